@@ -1,0 +1,119 @@
+/*
+ * mstm_b200.h -- C ABI of the B200 (sm_100a) multiple-sphere interaction solve.
+ *
+ * Drop-in boundary for MSTM's solver path (dmckwski/MSTM, december2023 tree).
+ * The reference has no FFI; its boundary is the Fortran subroutine interface.
+ * Each entry point below replaces one Fortran routine, called from Fortran
+ * through an ISO_C_BINDING interface module (INTEGRATION.md shows it):
+ *
+ *   mstmg_ctx_create         replaces the spheredata/mie module set-up:
+ *                            miecoefcalc (mstm-modules-33.f90:5301-5407) and
+ *                            the sphere arrays of spheredata (mstm-modules-33.f90:5088-5131)
+ *   mstmg_interaction        sphereinteraction (mstm-scatprops-26.f90:25-180)
+ *   mstmg_bicg               cbicg (mstm-solver-8.f90:654-949)
+ *   mstmg_planewave          sphereplanewavecoef (mstm-scatprops-26.f90:217-284)
+ *   mstmg_fixed_orientation  fixedorsoln (mstm-solver-8.f90:350-569) + qtotcalc
+ *                            (mstm-scatprops-26.f90:872-912)
+ *
+ * Conventions
+ *   - Complex arrays are interleaved (re, im) doubles, i.e. Fortran complex(8)
+ *     or C double _Complex; vectors use MSTM's layout: each sphere's block is
+ *     a(0:L+1,1:L,1:2) column-major, blocks in sphere order; multi-column
+ *     arrays are column-major with leading dimension neqns.
+ *   - Pointers may be host memory or device memory (detected per call).
+ *   - Every call returns an int status: 0 ok; 1 not converged (MSTM's istat=1,
+ *     mstm-solver-8.f90:524); negative values are errors (see MSTMG_ERR_*),
+ *     with a message from mstmg_last_error().  Nothing calls exit().
+ *   - One host thread per context.  The context replaces MSTM's module globals.
+ *   - Lengths are dimensionless (k = 1): a sphere's radius is its size parameter.
+ */
+#ifndef MSTM_B200_H
+#define MSTM_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MSTMG_OK 0
+#define MSTMG_NOT_CONVERGED 1
+#define MSTMG_ERR_ARG (-1)
+#define MSTMG_ERR_CUDA (-2)
+#define MSTMG_ERR_UNSUPPORTED (-3)
+#define MSTMG_ERR_BREAKDOWN (-4)
+
+#define MSTMG_PRECISION_FP64 0    /* drop-in: FP64 operators and BiCG, the reference's iteration */
+#define MSTMG_PRECISION_MIXED 1   /* FP32 inner BiCG + FP64 iterative refinement, polarisations batched */
+
+typedef struct mstmg_ctx mstmg_ctx;
+
+typedef struct {
+    int precision;                 /* MSTMG_PRECISION_* */
+    int device;                    /* CUDA device ordinal */
+    double medium_re, medium_im;   /* host medium refractive index (MSTM layer_ref_index(0)); 1 in free space */
+    int translation_switch_order;  /* MSTM translation_switch_order (mstm-modules-33.f90:5126), default 3 */
+    double inner_eps;              /* mixed mode: squared residual reduction per inner solve (default 1e-8) */
+    int max_outer;                 /* mixed mode: refinement steps cap (default 30) */
+} mstmg_opts;
+
+/* Fill opts with the defaults above. */
+void mstmg_default_opts(mstmg_opts *opts);
+
+/* Create a context for nsphere external spheres.
+ * pos: 3*nsphere (x,y,z per sphere); radius: nsphere; ref_index: 2*nsphere (re,im).
+ * mie_epsilon as MSTM's mie_epsilon: >0 converge orders, <0 force order ceil(-mie_epsilon).
+ * Replaces miecoefcalc (mstm-modules-33.f90:5301-5407) and the spheredata set-up. */
+int mstmg_ctx_create(mstmg_ctx **ctx, int nsphere, const double *pos, const double *radius, const double *ref_index,
+                     double mie_epsilon, const mstmg_opts *opts);
+void mstmg_ctx_destroy(mstmg_ctx *ctx);
+
+/* Replace the sphere positions (same count, radii and indices) without
+ * reallocating; operators are regenerated on the next solve. */
+int mstmg_ctx_set_positions(mstmg_ctx *ctx, const double *pos);
+
+int mstmg_neqns(const mstmg_ctx *ctx);
+int mstmg_npairs(const mstmg_ctx *ctx);
+/* order: nsphere sphere orders; offset: nsphere+1 sphere_offset values (complex units). */
+int mstmg_sphere_orders(const mstmg_ctx *ctx, int *order, int *offset);
+/* an: 2 * 4*sum(L) doubles (MSTM an_mie layout); qext, qabs: nsphere (may be NULL). */
+int mstmg_mie_coefficients(const mstmg_ctx *ctx, double *an, double *qext, double *qabs);
+/* (sum r^3)^.333333 as MSTM forms vol_radius (mstm-input-37.f90:1219-1225). */
+double mstmg_vol_radius(const mstmg_ctx *ctx);
+
+/* sphereinteraction (mstm-scatprops-26.f90:25-180).  ain, aout: neqns x nrhs complex.
+ * con_tran[r] != 0: column r gets conj((Mie*H)^T conj(x)); mie_mult[r] == 0 skips the
+ * Mie multiply.  Either array may be NULL (all 0 / all 1).  initial_run != 0
+ * (re)generates the stored pair operators. */
+int mstmg_interaction(mstmg_ctx *ctx, int nrhs, const double *ain, double *aout, const int *con_tran, const int *mie_mult,
+                      int initial_run);
+
+/* cbicg (mstm-solver-8.f90:654-949), FP64.  Solves (I - Mie*H) x = pnp from the
+ * initial guess in anp; stops when ||r||^2/||pnp||^2 < eps.  iter, err as cbicg's. */
+int mstmg_bicg(mstmg_ctx *ctx, int niter, double eps, const double *pnp, double *anp, int initialize, int *iter, double *err);
+
+/* sphereplanewavecoef (mstm-scatprops-26.f90:217-284), no plane boundaries: pmnp neqns x 2. */
+int mstmg_planewave(mstmg_ctx *ctx, double alpha, double sinc, int dir, double *pmnp);
+
+/* fixedorsoln (mstm-solver-8.f90:350-569) and qtotcalc.  amnp: neqns x 2 (out);
+ * qeff: 3 x 3 x nsphere (out, may be NULL); qtot: 3 x 3 (out, may be NULL):
+ * [ext, abs, sca] x [unpolarised, par, perp].  maxerr/maxiter as fixedorsoln's. */
+int mstmg_fixed_orientation(mstmg_ctx *ctx, double alpha, double sinc, int dir, double eps, int niter, double *amnp,
+                            double *qeff, double *qtot, double *maxerr, int *maxiter);
+
+/* Statistics of the last solve: iterations per polarisation, refinement steps,
+ * FP64 and FP32 operator passes. */
+int mstmg_last_stats(const mstmg_ctx *ctx, int *iters2, int *outer, int *passes64, int *passes32);
+
+/* Bytes of one FP64 (prec=0) or FP32 (prec=1) operator pass, and the
+ * reference's canonical per-pass operator bytes (translation_data layout). */
+int mstmg_operator_bytes(const mstmg_ctx *ctx, int prec, double *stored_bytes, double *canonical_bytes);
+
+/* Time `reps` translation passes (nrhs right-hand sides, FP64 or FP32) with CUDA
+ * events on the context stream; returns the average milliseconds per pass. */
+int mstmg_time_translation(mstmg_ctx *ctx, int prec, int nrhs, int reps, double *ms_per_pass);
+
+/* Message of the last error on this thread. */
+const char *mstmg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,70 @@
+"""ctypes binding of libmstm_b200.so (the C ABI in include/mstm_b200.h).
+
+The library is built in-tree (mstm_b200/libmstm_b200.so).  There is no CPU
+fallback: if the library is missing or cannot be loaded, ``lib()`` raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmstm_b200.so")
+_lib = None
+
+c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+P = ctypes.POINTER
+
+# Every symbol include/mstm_b200.h declares, with (restype, argtypes).
+SIGNATURES = {
+    "mstmg_default_opts": (None, [c_void_p]),
+    "mstmg_ctx_create": (c_int, [P(c_void_p), c_int, c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
+    "mstmg_ctx_destroy": (None, [c_void_p]),
+    "mstmg_ctx_set_positions": (c_int, [c_void_p, c_void_p]),
+    "mstmg_neqns": (c_int, [c_void_p]),
+    "mstmg_npairs": (c_int, [c_void_p]),
+    "mstmg_sphere_orders": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "mstmg_mie_coefficients": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mstmg_vol_radius": (c_double, [c_void_p]),
+    "mstmg_interaction": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
+    "mstmg_bicg": (c_int, [c_void_p, c_int, c_double, c_void_p, c_void_p, c_int, P(c_int), P(c_double)]),
+    "mstmg_planewave": (c_int, [c_void_p, c_double, c_double, c_int, c_void_p]),
+    "mstmg_fixed_orientation": (c_int, [c_void_p, c_double, c_double, c_int, c_double, c_int, c_void_p, c_void_p, c_void_p,
+                                        P(c_double), P(c_int)]),
+    "mstmg_last_stats": (c_int, [c_void_p, c_void_p, P(c_int), P(c_int), P(c_int)]),
+    "mstmg_operator_bytes": (c_int, [c_void_p, c_int, P(c_double), P(c_double)]),
+    "mstmg_time_translation": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),
+    "mstmg_last_error": (ctypes.c_char_p, []),
+}
+
+
+class MstmgOpts(ctypes.Structure):
+    _fields_ = [("precision", c_int), ("device", c_int), ("medium_re", c_double), ("medium_im", c_double),
+                ("translation_switch_order", c_int), ("inner_eps", c_double), ("max_outer", c_int)]
+
+
+class MstmgError(RuntimeError):
+    def __init__(self, code, where):
+        msg = lib().mstmg_last_error().decode(errors="replace")
+        super().__init__("%s failed with status %d: %s" % (where, code, msg))
+        self.code = code
+
+
+def lib():
+    """Load the CUDA library; raises if it was not built (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libmstm_b200.so is not built; run `python -m mstm_b200.build` "
+                               "(the CUDA extension is required, there is no CPU path)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code, where):
+    if code < 0:
+        raise MstmgError(code, where)
+    return code

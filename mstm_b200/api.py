@@ -1,0 +1,166 @@
+"""Host-side mirror of MSTM's solver call surface, backed by the CUDA library.
+
+Names and argument meanings follow the Fortran routines they replace
+(dmckwski/MSTM, december2023 tree):
+
+=====================  ==========================================================
+``SphereCluster``      spheredata + mie module state, miecoefcalc
+                       (mstm-modules-33.f90:5088-5131, 5301-5407)
+``sphereinteraction``  sphereinteraction (mstm-scatprops-26.f90:25-180)
+``cbicg``              cbicg (mstm-solver-8.f90:654-949)
+``sphereplanewavecoef``sphereplanewavecoef (mstm-scatprops-26.f90:217-284)
+``fixedorsoln``        fixedorsoln (mstm-solver-8.f90:350-569)
+``qtotcalc``           qtotcalc (mstm-scatprops-26.f90:872-912)
+=====================  ==========================================================
+
+Vectors are complex128 numpy arrays in MSTM's layout (each sphere block is
+a(0:L+1,1:L,1:2) column-major).  All arithmetic runs on the GPU; the status
+conventions match the reference (istat 0 converged, 1 not converged) and
+errors raise ``MstmgError``.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import c_double, c_int, check
+
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class SphereCluster:
+    """One cluster of external spheres in a medium (free space by default).
+
+    positions: (N,3); radii: (N,) size parameters; ref_index: (N,) complex or scalar.
+    mie_epsilon: MSTM's mie_epsilon (negative -L forces order L).
+    precision: "fp64" (drop-in) or "mixed" (FP32 inner BiCG, FP64 refinement).
+    """
+
+    def __init__(self, positions, radii, ref_index, mie_epsilon=1.0e-6, precision="fp64", device=0,
+                 medium_index=1.0, inner_eps=1.0e-8, max_outer=30):
+        self._L = _lib.lib()
+        pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
+        rad = np.ascontiguousarray(np.asarray(radii, np.float64).reshape(-1))
+        n = len(rad)
+        ri = np.asarray(ref_index, np.complex128)
+        if ri.ndim == 0:
+            ri = np.full(n, ri)
+        ri2 = np.ascontiguousarray(np.stack([ri.real, ri.imag], axis=1))
+        opts = _lib.MstmgOpts()
+        self._L.mstmg_default_opts(ctypes.byref(opts))
+        opts.precision = PRECISIONS[precision]
+        opts.device = device
+        opts.medium_re = float(np.real(medium_index))
+        opts.medium_im = float(np.imag(medium_index))
+        opts.inner_eps = inner_eps
+        opts.max_outer = max_outer
+        self.ctx = ctypes.c_void_p()
+        check(self._L.mstmg_ctx_create(ctypes.byref(self.ctx), n, _ptr(pos), _ptr(rad), _ptr(ri2), float(mie_epsilon),
+                                       ctypes.byref(opts)), "mstmg_ctx_create")
+        self.number_spheres = n
+        self.positions, self.radii = pos, rad
+        self.number_eqns = self._L.mstmg_neqns(self.ctx)
+        self.sphere_order = np.zeros(n, np.int32)
+        self.sphere_offset = np.zeros(n + 1, np.int32)
+        check(self._L.mstmg_sphere_orders(self.ctx, _ptr(self.sphere_order), _ptr(self.sphere_offset)), "orders")
+        self.precision = precision
+
+    def close(self):
+        if self.ctx:
+            self._L.mstmg_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def vol_radius(self):
+        return self._L.mstmg_vol_radius(self.ctx)
+
+    def set_positions(self, positions):
+        pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
+        check(self._L.mstmg_ctx_set_positions(self.ctx, _ptr(pos)), "set_positions")
+        self.positions = pos
+
+    def miecoefcalc(self):
+        nt = int(4 * self.sphere_order.sum())
+        an = np.zeros(nt, np.complex128)
+        qe = np.zeros(self.number_spheres)
+        qa = np.zeros(self.number_spheres)
+        check(self._L.mstmg_mie_coefficients(self.ctx, _ptr(an), _ptr(qe), _ptr(qa)), "mie")
+        return an, qe, qa
+
+    def sphereinteraction(self, ain, con_tran=None, mie_mult=None, initial_run=False):
+        ain = np.asfortranarray(np.asarray(ain, np.complex128).reshape(self.number_eqns, -1, order="F"))
+        nrhs = ain.shape[1]
+        out = np.zeros((self.number_eqns, nrhs), np.complex128, order="F")
+        ct = np.array(con_tran if con_tran is not None else [0] * nrhs, np.int32)
+        mm = np.array(mie_mult if mie_mult is not None else [1] * nrhs, np.int32)
+        check(self._L.mstmg_interaction(self.ctx, nrhs, _ptr(ain), _ptr(out), _ptr(ct), _ptr(mm), int(initial_run)),
+              "sphereinteraction")
+        return out
+
+    def cbicg(self, pnp, anp, niter=10000, eps=1.0e-6, initialize=True):
+        pnp = np.ascontiguousarray(pnp, np.complex128)
+        x = np.array(anp, np.complex128, copy=True)
+        it = c_int(0)
+        err = c_double(0.0)
+        rc = check(self._L.mstmg_bicg(self.ctx, niter, eps, _ptr(pnp), _ptr(x), int(initialize), ctypes.byref(it),
+                                      ctypes.byref(err)), "cbicg")
+        return x, it.value, err.value
+
+    def sphereplanewavecoef(self, alpha=0.0, sinc=0.0, direction=1):
+        out = np.zeros((self.number_eqns, 2), np.complex128, order="F")
+        check(self._L.mstmg_planewave(self.ctx, alpha, sinc, direction, _ptr(out)), "sphereplanewavecoef")
+        return out
+
+    def fixedorsoln(self, eps=1.0e-6, niter=10000, alpha=0.0, sinc=0.0, direction=1):
+        """Returns dict(amnp, qeff (3,3,N), qtot (3,3), maxerr, maxiter, istat, iterations)."""
+        amnp = np.zeros((self.number_eqns, 2), np.complex128, order="F")
+        qeff = np.zeros((3, 3, self.number_spheres), np.float64, order="F")
+        qtot = np.zeros((3, 3), np.float64, order="F")
+        me = c_double(0.0)
+        mi = c_int(0)
+        st = check(self._L.mstmg_fixed_orientation(self.ctx, alpha, sinc, direction, eps, niter, _ptr(amnp), _ptr(qeff),
+                                                   _ptr(qtot), ctypes.byref(me), ctypes.byref(mi)), "fixedorsoln")
+        stats = self.last_stats()
+        return dict(amnp=amnp, qeff=qeff, qtot=qtot, maxerr=me.value, maxiter=mi.value, istat=st, **stats)
+
+    def last_stats(self):
+        it = np.zeros(2, np.int32)
+        outer, p64, p32 = c_int(0), c_int(0), c_int(0)
+        check(self._L.mstmg_last_stats(self.ctx, _ptr(it), ctypes.byref(outer), ctypes.byref(p64), ctypes.byref(p32)),
+              "stats")
+        return dict(iterations=it.tolist(), outer=outer.value, passes64=p64.value, passes32=p32.value)
+
+    def operator_bytes(self, precision="fp64"):
+        s, c = c_double(0.0), c_double(0.0)
+        check(self._L.mstmg_operator_bytes(self.ctx, PRECISIONS[precision], ctypes.byref(s), ctypes.byref(c)), "bytes")
+        return s.value, c.value
+
+    def time_translation(self, precision="fp64", nrhs=2, reps=10):
+        ms = c_double(0.0)
+        check(self._L.mstmg_time_translation(self.ctx, PRECISIONS[precision], nrhs, reps, ctypes.byref(ms)), "time")
+        return ms.value
+
+
+def qtotcalc(qeff, radii, vol_radius):
+    """qtotcalc (mstm-scatprops-26.f90:872-912) for external spheres: area-weighted
+    totals with Qsca = Qext + Qinc - Qabs.  qeff: (3,3,N)."""
+    q = np.einsum("kpi,i->kp", qeff, np.asarray(radii) ** 2) / vol_radius ** 2
+    q = q.copy()
+    q[2, :] = q[0, :] + q[2, :] - q[1, :]
+    return q

@@ -1,0 +1,51 @@
+// kernels.cuh -- argument blocks and launchers shared by the .cu files.
+#pragma once
+#include "common.cuh"
+
+struct OpGenArgs {
+    int npairs;
+    const int2* pairs;       // (i, j), i < j
+    const double* pos;       // 3N
+    const int* order;        // N
+    const long long* opoff;  // per pair, in storage units
+    double* op64;            // may be null
+    float* op32;             // may be null
+    const double* vcc;       // vcc_const(vn, vn(vn+2), 0:2vn)
+    int vnmax;
+    const double* fnm1;      // (-vn:vn, 1:vn)
+    const double* fnc;
+    const double* fnp1;
+    const double* fnr;       // sqrt table
+    const double* bcofd;     // bcof(n,n)
+    double rimed_re, rimed_im;
+    int* err;
+};
+
+#include "oplayout.cuh"
+void launch_opgen(const OpGenArgs& a, int nsm, cudaStream_t st);
+
+template <typename T> struct TransArgs {
+    int npairs;
+    const int2* pairs;
+    const int* order;
+    const int* offset;       // sphere_offset (complex units)
+    const T* ops;
+    const long long* opoff;  // storage units
+    const cpx<T>* x;         // ld x nrhs
+    cpx<T>* y;               // ld x nrhs, accumulated
+    int ld;
+    int nrhs;
+    unsigned contran;        // bit r set: rhs r is a conjugate-transpose product
+    int lmax;                // largest order (smem strides)
+    int maxrec;              // largest operator record, storage units
+    int* err;
+};
+template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cudaStream_t st);
+template <typename T> size_t translate_smem_bytes(int lmax, int nrhs, int maxrec);
+
+// Mie multiply over all spheres: y(:,r) = A x(:,r) (idir=1) or A^T x(:,r);
+// optional conjugation of the input.  slot_sphere maps each (row, column)
+// slot of the first mode half of every sphere block to its sphere.
+template <typename T> void launch_mie(int nslots, const int* slot_sphere, const int* order, const int* offset,
+                                      const int* mie_offset, const cpx<T>* an, int idir, int conj_in,
+                                      const cpx<T>* x, cpx<T>* y, cudaStream_t st);

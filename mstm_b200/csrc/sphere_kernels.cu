@@ -1,0 +1,412 @@
+// sphere_kernels.cu -- per-sphere device kernels: Mie coefficients, incident
+// plane-wave coefficients, the Mie multiply, and the efficiency sums.  All
+// coefficient generation and the final cross-section sums run in FP64.
+#include "common.cuh"
+#include "special.cuh"
+#include "kernels.cuh"
+#include "sphere_kernels.cuh"
+
+#define MIE_NMAX 48   // largest Mie order a sphere may need (x up to ~30)
+
+// ---------------------------------------------------------------------------
+// mieoa for a non-optically-active sphere in a medium (december2023/
+// mstm-modules-33.f90:5438-5578).  mode 0: determine the order from qeps
+// (qeps>0 convergence test; qeps<0 forces ceiling(-qeps)); mode 1: write the
+// 2x2 LR-basis matrices anp(2,2,n) and their inverses for the given order.
+// ---------------------------------------------------------------------------
+__device__ void mie_one(double x, zd ri, zd rimed, double qeps, int mode, int* nodr_io, zd* anp, zd* anpinv,
+                        double* qext_o, double* qabs_o)
+{
+    int nstop;
+    if (mode == 0) {
+        if (qeps > 0.0) nstop = (int)llround(x + 4.0 * pow(x, (double)(1.0f / 3.0f))) + 5;
+        else if (qeps < 0.0) nstop = (int)ceil(-qeps);
+        else nstop = *nodr_io;
+    } else {
+        nstop = *nodr_io;
+    }
+    if (nstop > MIE_NMAX - 2) nstop = MIE_NMAX - 2;
+    const int nb = nstop + 1;
+    zd psi[2][MIE_NMAX], xi[2][MIE_NMAX], scr[2 * MIE_NMAX];
+    // both helicities share one index: rii(:,i) equal; i=0 medium, i=1 sphere
+    zd rii[2] = {rimed, ri};
+    zd ribulk[2] = {cdivr(2.0, cdivr(1.0, rii[0]) + cdivr(1.0, rii[0])), cdivr(2.0, cdivr(1.0, rii[1]) + cdivr(1.0, rii[1]))};
+    zd xri[2] = {x * rii[0], x * rii[1]};
+    for (int i = 0; i < 2; i++) {
+        mstm_cricbessel(nb, xri[i], psi[i], scr);
+        mstm_crichankel(nb, xri[i], xi[i], scr);
+    }
+    double qsca = 0.0, qext = 0.0;
+    double qext1[MIE_NMAX];
+    for (int n = 1; n <= nstop; n++) {
+        zd psip[2], xip[2], psipn[2];
+        for (int i = 0; i < 2; i++) {
+            psip[i] = psi[i][n - 1] - cdiv((double)n * psi[i][n], xri[i]);
+            xip[i] = xi[i][n - 1] - cdiv((double)n * xi[i][n], xri[i]);
+            psipn[i] = cdiv(psi[i][n - 1], psi[i][n]) - cdivr((double)n, xri[i]);
+        }
+        zd gmat[4], amat[4];
+        for (int s = 1; s <= 2; s++) {
+            double ss = pm1(s);
+            for (int t = 1; t <= 2; t++) {
+                double st = pm1(t);
+                zd pre = cdiv(ss * ribulk[0] + st * ribulk[1], rii[1] * rii[0]);
+                gmat[(s - 1) + 2 * (t - 1)] = pre * (psipn[1] * xi[0][n] - (ss * st) * xip[0]);
+                amat[(s - 1) + 2 * (t - 1)] = pre * (psipn[1] * psi[0][n] - (ss * st) * psip[0]);
+            }
+        }
+        zd ginv[4], am[4];
+        mstm_inv22(gmat, ginv);
+        for (int r = 1; r <= 2; r++)
+            for (int c = 1; c <= 2; c++)
+                am[(r - 1) + 2 * (c - 1)] = -(ginv[(r - 1)] * amat[2 * (c - 1)] + ginv[(r - 1) + 2] * amat[1 + 2 * (c - 1)]);
+        if (mode == 1) {
+            for (int k = 0; k < 4; k++) anp[4 * (n - 1) + k] = am[k];
+            mstm_inv22(am, anpinv + 4 * (n - 1));
+        }
+        qext1[n] = 0.0;
+        double fn1 = n + n + 1;
+        for (int p = 1; p <= 2; p++) {
+            for (int q = 1; q <= 2; q++) {
+                double ab = cabsd(am[(p - 1) + 2 * (q - 1)]);
+                qsca = qsca + fn1 * ab * ab;
+            }
+            qext1[n] = qext1[n] - fn1 * am[(p - 1) * 3].x;
+        }
+        qext = qext + qext1[n];
+    }
+    if (mode == 0) {
+        if (qeps > 0.0) {
+            double qextt = qext;
+            qext = 0.0;
+            int n;
+            for (n = 1; n <= nstop; n++) {
+                qext = qext + qext1[n];
+                if (fabs(1.0 - qext / qextt) < qeps || n == nstop) break;
+            }
+            *nodr_io = n;
+        } else {
+            *nodr_io = nstop;
+        }
+    }
+    qsca = 2.0 / x / x * qsca;
+    qext = 2.0 / x / x * qext;
+    if (qext_o) *qext_o = qext;
+    if (qabs_o) *qabs_o = qext - qsca;
+}
+
+__global__ void mie_order_kernel(int n, const double* radius, const double* ri, double rimed_re, double rimed_im, double qeps,
+                                 int* order)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int nodr = 0;
+    mie_one(radius[i], mk(ri[2 * i], ri[2 * i + 1]), mk(rimed_re, rimed_im), qeps, 0, &nodr, nullptr, nullptr, nullptr, nullptr);
+    order[i] = nodr;
+}
+
+__global__ void mie_coef_kernel(int n, const double* radius, const double* ri, double rimed_re, double rimed_im, const int* order,
+                                const int* mie_offset, zd* an, zd* an_inv, float* an32, double* qext, double* qabs)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int nodr = order[i];
+    mie_one(radius[i], mk(ri[2 * i], ri[2 * i + 1]), mk(rimed_re, rimed_im), 0.0, 1, &nodr, an + mie_offset[i],
+            an_inv + mie_offset[i], &qext[i], &qabs[i]);
+    for (int k = 0; k < 4 * order[i]; k++) {
+        an32[2 * (mie_offset[i] + k)] = (float)an[mie_offset[i] + k].x;
+        an32[2 * (mie_offset[i] + k) + 1] = (float)an[mie_offset[i] + k].y;
+    }
+}
+
+void launch_mie_orders(int n, const double* radius, const double* ri, double mre, double mim, double qeps, int* order,
+                       cudaStream_t st)
+{
+    mie_order_kernel<<<(n + 63) / 64, 64, 0, st>>>(n, radius, ri, mre, mim, qeps, order);
+}
+void launch_mie_coefs(int n, const double* radius, const double* ri, double mre, double mim, const int* order,
+                      const int* mie_offset, zd* an, zd* an_inv, float* an32, double* qext, double* qabs, cudaStream_t st)
+{
+    mie_coef_kernel<<<(n + 63) / 64, 64, 0, st>>>(n, radius, ri, mre, mim, order, mie_offset, an, an_inv, an32, qext, qabs);
+}
+
+// ---------------------------------------------------------------------------
+// Plane-wave coefficients: genplanewavecoef (modules:1453-1520) for order
+// lmax into pw0(nb(lmax), 2 polarisations), then per sphere the phase of
+// layerplanewavecoef without plane boundaries (modules:3901-3965).
+// ---------------------------------------------------------------------------
+__global__ void planewave_common_kernel(double alpha, zd cb, int nodr, zd* pw0, zd* drot /* 3*(nodr(nodr+2)+1) */)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    // crotcoef(cb, kmax=1, nodr) (modules:1187-1246)
+    const int kmax = 1, ld = 3;
+    int nd = nodr * (nodr + 2) + 1;
+    for (int k = 0; k < ld * nd; k++) drot[k] = mk(0.0, 0.0);
+#define DC(m, nk) drot[((m) + kmax) + ld * (nk)]
+    zd sbe = csqrtd((mk(1.0, 0.0) + cb) * (mk(1.0, 0.0) - cb));
+    zd cbe2 = 0.5 * (mk(1.0, 0.0) + cb), sbe2 = 0.5 * (mk(1.0, 0.0) - cb);
+    zd dk0s[2 * MSTMG_LMAX + 3], dk01s[2 * MSTMG_LMAX + 3];
+    zd* dk0 = dk0s + (MSTMG_LMAX + 1);
+    zd* dk01 = dk01s + (MSTMG_LMAX + 1);
+    for (int k = 0; k < 2 * MSTMG_LMAX + 3; k++) { dk0s[k] = mk(0.0, 0.0); dk01s[k] = mk(0.0, 0.0); }
+    int in = 1;
+    dk0[0] = mk(1.0, 0.0);
+    zd sben = mk(1.0, 0.0);
+    DC(0, 0) = mk(1.0, 0.0);
+    // bcof(n,n) = sqrt((2n)!/(n!)^2), built by the same recurrence as numconstants::init
+    double bnn = 1.0;
+    for (int n = 1; n <= nodr; n++) {
+        bnn = sqrt((double)(n + n)) * sqrt((double)(n + n - 1)) * bnn / sqrt((double)n) / sqrt((double)n);
+        int knmax = n < kmax ? n : kmax;
+        int nn1 = n * (n + 1);
+        in = -in;
+        {
+            zd tq = sben * sbe;   // sben = sben*sbe/2
+            sben = mk(tq.x / 2.0, tq.y / 2.0);
+        }
+        dk0[n] = ((double)in * sben) * bnn;
+        dk0[-n] = (double)in * dk0[n];
+        dk01[n] = mk(0.0, 0.0);
+        dk01[-n] = mk(0.0, 0.0);
+        DC(0, nn1 + n) = dk0[n];
+        DC(0, nn1 - n) = dk0[-n];
+        for (int k = -n + 1; k <= n - 1; k++) {
+            int kn = nn1 + k;
+            zd dkt = dk01[k];
+            dk01[k] = dk0[k];
+            double c1 = (double)(n + n - 1), c2 = sqrt((double)(n - k - 1)) * sqrt((double)(n + k - 1));
+            double c3 = sqrt((double)(n + k)) * sqrt((double)(n - k));
+            zd num = (cb * c1) * dk01[k] - c2 * dkt;
+            dk0[k] = mk(num.x / c3, num.y / c3);
+            DC(0, kn) = dk0[k];
+        }
+        int im = 1;
+        for (int m = 1; m <= knmax; m++) {
+            im = -im;
+            double fmn = 1.0 / sqrt((double)(n - m + 1)) / sqrt((double)(n + m));
+            int m1 = m - 1;
+            zd dkm0 = mk(0.0, 0.0);
+            for (int k = -n; k <= n; k++) {
+                int kn = nn1 + k;
+                zd dkm1 = dkm0;
+                dkm0 = DC(m1, kn);
+                zd dkn1 = (k == n) ? mk(0.0, 0.0) : DC(m1, kn + 1);
+                zd v = (sqrt((double)(n + k)) * sqrt((double)(n - k + 1))) * cbe2 * dkm1 -
+                       (sqrt((double)(n - k)) * sqrt((double)(n + k + 1))) * sbe2 * dkn1 - ((double)k * sbe) * DC(m1, kn);
+                DC(m, kn) = v * fmn;
+                DC(-m, nn1 - k) = DC(m, kn) * (pm1(k) * im);
+            }
+        }
+    }
+    int nb = 2 * nodr * (nodr + 2);
+    // tau(0:nodr+1,nodr,2) then the LR combination
+    for (int n = 1; n <= nodr; n++) {
+        int nn1 = n * (n + 1);
+        double fnm = sqrt((double)(n + n + 1) / 2.0) / 4.0;
+        zd cin;
+        {
+            int e = (n + 1) % 4;
+            zd ipw = (e == 0) ? mk(1.0, 0.0) : (e == 1 ? mk(0.0, 1.0) : (e == 2 ? mk(-1.0, 0.0) : mk(0.0, -1.0)));
+            cin = 4.0 * ipw;
+        }
+        for (int m = -n; m <= n; m++) {
+            int mn = nn1 + m;
+            zd tau1 = -fnm * (-DC(-1, mn) + DC(1, mn));
+            zd tau2 = -fnm * (DC(-1, mn) + DC(1, mn));
+            zd taulr[2] = {(tau1 + tau2) * 0.5, (tau1 - tau2) * 0.5};
+            // ealpham(-m): powers of e^{i alpha} as ephicoef builds them
+            zd ea;
+            zd ep = mk(cos(alpha), sin(alpha));
+            zd pw = mk(1.0, 0.0);
+            for (int q = 1; q <= (m < 0 ? -m : m); q++) pw = ep * pw;
+            ea = (m <= 0) ? pw : cj(pw);
+            for (int p = 1; p <= 2; p++) {
+                double sp = -pm1(p);
+                int ai = aidx(m, n, p - 1, nodr);
+                pw0[ai] = -(cin * taulr[p - 1] * ea);
+                pw0[nb + ai] = sp * imul(cin * taulr[p - 1] * ea);
+            }
+        }
+    }
+#undef DC
+}
+
+__global__ void planewave_phase_kernel(int nslots2, const int* slot_sphere, const int* order, const int* offset, const double* pos,
+                                       int lmax, const zd* pw0, zd cbinc, zd riinc, double sinc, double alpha, zd* pmnp, int ld)
+{
+    // nslots2 = neqns: every coefficient of every sphere block (both modes)
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nslots2) return;
+    int half = e;  // index in the full vector
+    // locate sphere via slot_sphere over the first-mode half of each block
+    int i = slot_sphere[e];
+    int L = order[i], off = offset[i];
+    int loc = half - off;
+    int hb = L * (L + 2);
+    int p = loc / hb, rem = loc % hb;
+    int row = rem % (L + 2), col = rem / (L + 2) + 1;
+    int m, n;
+    if (row <= col) { m = row; n = col; } else { n = row - 1; m = -col; }
+    zd phz = cexpd(imul(riinc * cbinc * mk(pos[3 * i + 2] - 0.0, 0.0)));
+    zd phl = cexpd(imul(mk(sinc * (cos(alpha) * pos[3 * i] + sin(alpha) * pos[3 * i + 1]), 0.0)));
+    int nbl = 2 * lmax * (lmax + 2);
+    int src = aidx(m, n, p, lmax);
+    for (int k = 0; k < 2; k++) pmnp[(size_t)k * ld + e] = (pw0[(size_t)k * nbl + src] * phz) * phl;
+}
+
+void launch_planewave(double alpha, double sinc, int dir, int lmax, int neqns, const int* slot_full, const int* order,
+                      const int* offset, const double* pos, zd* pw0, zd* drot, zd* pmnp, cudaStream_t st)
+{
+    zd riinc = mk(1.0, 0.0);
+    zd a = cdiv(mk(sinc, 0.0), riinc);
+    zd cbinc = csqrtd((mk(1.0, 0.0) - a) * (mk(1.0, 0.0) + a)) * (double)(3 - 2 * dir);
+    planewave_common_kernel<<<1, 32, 0, st>>>(alpha, cbinc, lmax, pw0, drot);
+    planewave_phase_kernel<<<(neqns + 255) / 256, 256, 0, st>>>(neqns, slot_full, order, offset, pos, lmax, pw0, cbinc, riinc,
+                                                                 sinc, alpha, pmnp, neqns);
+}
+
+// ---------------------------------------------------------------------------
+// Mie multiply (multmiecoeffmult, modules:5633-5751, external spheres):
+// y(m,n,p) = sum_q A(p,q,n) x(m,n,q)  (idir=1) or A(q,p,n) (idir!=1).
+// One thread per (m,n) slot of the first mode half; in-place is allowed.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void mie_kernel(int nslots, const int* slot_sphere, const int* order, const int* offset, const int* mie_offset,
+                           const cpx<T>* an, int idir, int conj_in, const cpx<T>* x, cpx<T>* y)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nslots) return;
+    int i = slot_sphere[e];
+    int L = order[i];
+    int hb = L * (L + 2);
+    int loc = e - offset[i] / 2;   // slot index inside the sphere's first half
+    int row = loc % (L + 2), col = loc / (L + 2) + 1;
+    int n = (row <= col) ? col : row - 1;
+    int base = offset[i] + loc;
+    cpx<T> x0 = x[base], x1 = x[base + hb];
+    if (conj_in) { x0 = cj(x0); x1 = cj(x1); }
+    const cpx<T>* A = an + mie_offset[i] + 4 * (n - 1);   // A(p,q) at (p-1)+2(q-1)
+    cpx<T> y0, y1;
+    if (idir == 1) {
+        y0 = A[0] * x0 + A[2] * x1;
+        y1 = A[1] * x0 + A[3] * x1;
+    } else {
+        y0 = A[0] * x0 + A[1] * x1;
+        y1 = A[2] * x0 + A[3] * x1;
+    }
+    y[base] = y0;
+    y[base + hb] = y1;
+}
+
+template <typename T>
+void launch_mie(int nslots, const int* slot_sphere, const int* order, const int* offset, const int* mie_offset, const cpx<T>* an,
+                int idir, int conj_in, const cpx<T>* x, cpx<T>* y, cudaStream_t st)
+{
+    mie_kernel<T><<<(nslots + 255) / 256, 256, 0, st>>>(nslots, slot_sphere, order, offset, mie_offset, an, idir, conj_in, x, y);
+}
+template void launch_mie<double>(int, const int*, const int*, const int*, const int*, const zd*, int, int, const zd*, zd*, cudaStream_t);
+template void launch_mie<float>(int, const int*, const int*, const int*, const int*, const zf*, int, int, const zf*, zf*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Efficiencies: lrsphereqeff (scatprops:676-776) per sphere, npol=2, with
+// g = A^{-1} a (qefficiencyfactors, scatprops:782-870, no host spheres).
+// qeff(3,3,N): qeff[q + 3*(pol + 3*i)].
+// ---------------------------------------------------------------------------
+__global__ void qeff_kernel(int nsph, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed,
+                            const zd* an_inv, const zd* amnp, const zd* pmnp0, int ld, double* qeff)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsph) return;
+    int L = order[i], off = offset[i];
+    double xsp = radius[i];
+    zd ri0 = rimed;
+    zd xri = xsp * ri0;
+    zd rib = cdivr(2.0, cdivr(1.0, ri0) + cdivr(1.0, ri0));
+    zd psi[MIE_NMAX], xi[MIE_NMAX], scr[2 * MIE_NMAX];
+    mstm_cricbessel(L, xri, psi, scr);
+    mstm_crichankel(L, xri, xi, scr);
+    double qe[3] = {0, 0, 0}, qa[3] = {0, 0, 0}, qi[3] = {0, 0, 0};
+    const zd* Ai = an_inv + mie_offset[i];
+    int hb = L * (L + 2);
+    for (int n = 1; n <= L; n++) {
+        zd psip = psi[n - 1] - cdiv((double)n * psi[n], xri);
+        zd xip = xi[n - 1] - cdiv((double)n * xi[n], xri);
+        zd aam[4], ggm[4], agm[4];
+        zd cterm = imul(cdiv(cj(cdivr(1.0, ri0)), ri0));
+        for (int s = 1; s <= 2; s++) {
+            double ss = pm1(s);
+            for (int t = 1; t <= 2; t++) {
+                double st = pm1(t);
+                int k = (s - 1) + 2 * (t - 1);
+                aam[k] = cterm * (xip * cj(xi[n]) - (ss * st) * (xi[n] * cj(xip)));
+                ggm[k] = cterm * (psip * cj(psi[n]) - (ss * st) * (psi[n] * cj(psip)));
+                agm[k] = cterm * (xip * cj(psi[n]) - (ss * st) * (xi[n] * cj(psip)));
+            }
+        }
+        const zd* Ain = Ai + 4 * (n - 1);
+        for (int m = -n; m <= n; m++) {
+            int a0 = aidx(m, n, 0, L);
+            zd av[2][2], gv[2][2], fv[2][2];   // [pol][mode]
+            for (int pol = 0; pol < 2; pol++) {
+                zd x0 = amnp[(size_t)pol * ld + off + a0], x1 = amnp[(size_t)pol * ld + off + a0 + hb];
+                av[pol][0] = x0;
+                av[pol][1] = x1;
+                // onemiecoeffmult with the inverse: g(p) = sum_q Ainv(p,q) a(q)
+                gv[pol][0] = Ain[0] * x0 + Ain[2] * x1;
+                gv[pol][1] = Ain[1] * x0 + Ain[3] * x1;
+                fv[pol][0] = pmnp0[(size_t)pol * ld + off + a0];
+                fv[pol][1] = pmnp0[(size_t)pol * ld + off + a0 + hb];
+            }
+            for (int p1 = 0; p1 < 2; p1++)
+                for (int p2 = 0; p2 < 2; p2++) {
+                    int k;
+                    double cst;
+                    if (p1 == 0 && p2 == 0) { k = 0; cst = 1.0; }
+                    else if (p1 == 1 && p2 == 1) { k = 1; cst = 1.0; }
+                    else { k = 2; cst = 0.5; }
+                    for (int s = 0; s < 2; s++)
+                        for (int t = 0; t < 2; t++) {
+                            int mk_ = s + 2 * t;
+                            double sgn = pm1(s + t);
+                            zd crib = cj(rib) + sgn * rib;
+                            qi[k] = qi[k] + (cst * (ggm[mk_] * fv[p1][s] * cj(rib * fv[p2][t]))).x;
+                            qa[k] = qa[k] + (cst * (aam[mk_] * av[p1][s] * cj(rib * av[p2][t]) + ggm[mk_] * gv[p1][s] * cj(rib * gv[p2][t]) +
+                                                    agm[mk_] * av[p1][s] * cj(gv[p2][t]) * crib)).x;
+                            qe[k] = qe[k] + (cst * (agm[mk_] * av[p1][s] * cj(fv[p2][t]) * crib)).x;
+                        }
+                }
+        }
+    }
+    double qeffi[3][3];
+    for (int k = 0; k < 3; k++) {
+        qi[k] = qi[k] * 2.0 / xsp / xsp;
+        qe[k] = qe[k] * 2.0 / xsp / xsp;
+        qa[k] = qa[k] * 2.0 / xsp / xsp;
+        qeffi[0][k] = qe[k];
+        qeffi[1][k] = qa[k];
+        qeffi[2][k] = qi[k];
+    }
+    for (int q = 0; q < 3; q++) {
+        qeff[q + 3 * (0 + 3 * i)] = 0.5 * (qeffi[q][0] + qeffi[q][1]);
+        qeff[q + 3 * (1 + 3 * i)] = qeffi[q][0];
+        qeff[q + 3 * (2 + 3 * i)] = qeffi[q][1];
+    }
+}
+
+// qtotcalc (scatprops:872-912), no host spheres, one block, fixed summation order.
+__global__ void qtot_kernel(int nsph, const double* radius, const double* qeff, double xg, double* qtot)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < nsph; i++)
+        for (int k = 0; k < 9; k++) s[k] = s[k] + qeff[k + 9 * i] * radius[i] * radius[i] / (xg * xg);
+    for (int pol = 0; pol < 3; pol++) s[2 + 3 * pol] = s[0 + 3 * pol] + s[2 + 3 * pol] - s[1 + 3 * pol];
+    for (int k = 0; k < 9; k++) qtot[k] = s[k];
+}
+
+void launch_qeff(int nsph, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed, const zd* an_inv,
+                 const zd* amnp, const zd* pmnp0, int ld, double* qeff, double xg, double* qtot, cudaStream_t st)
+{
+    qeff_kernel<<<(nsph + 63) / 64, 64, 0, st>>>(nsph, order, offset, mie_offset, radius, rimed, an_inv, amnp, pmnp0, ld, qeff);
+    qtot_kernel<<<1, 32, 0, st>>>(nsph, radius, qeff, xg, qtot);
+}

@@ -1,0 +1,232 @@
+"""ctypes front end of the CPU oracle (oracle/libmstm_oracle.so).
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker for the CUDA product; only
+tests/, __graft_entry__.smoke() and the CPU legs of bench.py import it.  The
+C restatement it wraps follows MSTM's Fortran routines line by line (see the
+citations in mstm_oracle.c).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libmstm_oracle.so")
+_lib = None
+
+c_int = ctypes.c_int
+c_double = ctypes.c_double
+c_void_p = ctypes.c_void_p
+P = ctypes.POINTER
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc, OpenMP)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_create.restype = c_void_p
+        L.orc_create.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_double, c_int, c_int]
+        L.orc_destroy.argtypes = [c_void_p]
+        L.orc_neqns.argtypes = [c_void_p]
+        L.orc_neqns.restype = c_int
+        L.orc_orders.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
+        L.orc_mie_coefs.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+        L.orc_sphereinteraction.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int]
+        L.orc_cbicg.argtypes = [c_void_p, c_int, c_double, c_void_p, c_void_p, c_int, P(c_int), P(c_double)]
+        L.orc_cbicg.restype = c_int
+        L.orc_planewave.argtypes = [c_void_p, c_double, c_double, c_int, c_void_p]
+        L.orc_fixedorsoln.argtypes = [c_void_p, c_double, c_double, c_int, c_double, c_int, c_void_p, c_void_p,
+                                      P(c_double), P(c_int), c_int]
+        L.orc_fixedorsoln.restype = c_int
+        L.orc_qtotcalc.argtypes = [c_void_p, c_void_p, c_void_p]
+        L.orc_vol_radius.argtypes = [c_void_p]
+        L.orc_vol_radius.restype = c_double
+        L.orc_x_rotcoef.argtypes = [c_double, c_int, c_int, c_void_p]
+        L.orc_x_vcfunc.argtypes = [c_int, c_int, c_int, c_int, c_void_p]
+        L.orc_x_atcdim.argtypes = [c_int, c_int]
+        L.orc_x_atcdim.restype = c_int
+        L.orc_x_moffset.argtypes = [c_int, c_int, c_int]
+        L.orc_x_moffset.restype = c_int
+        L.orc_x_axial.argtypes = [c_int, c_double, c_double, c_double, c_int, c_int, c_void_p]
+        L.orc_x_mieoa.argtypes = [c_double, c_double, c_double, c_double, P(c_int), P(c_double), P(c_double),
+                                  P(c_double), c_void_p, c_void_p]
+        L.orc_x_translate_rot.argtypes = [c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int, c_int]
+        L.orc_x_gentranmatrix.argtypes = [c_int, c_int, c_void_p, c_int, c_void_p]
+        L.orc_x_cspherebessel.argtypes = [c_int, c_double, c_double, c_void_p, c_void_p]
+        L.orc_x_crichankel.argtypes = [c_int, c_double, c_double, c_void_p]
+        L.orc_x_direct_solve.argtypes = [c_void_p, c_void_p, c_void_p]
+        L.orc_x_multmie.argtypes = [c_void_p, c_int, c_void_p, c_void_p]
+        L.orc_x_qeff.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(c_void_p)
+
+
+class Oracle:
+    """FP64 CPU restatement of one MSTM sphere cluster (free space, medium index 1).
+
+    positions (N,3), radii (N,), ref_index (N,) complex; mie_eps as the
+    reference's ``mie_epsilon`` (negative -L forces order L).
+    """
+
+    def __init__(self, positions, radii, ref_index, mie_eps=-7.0, store_matrix=True, nthreads=1):
+        self.L = lib()
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+        rad = np.ascontiguousarray(np.asarray(radii, dtype=np.float64))
+        ri = np.asarray(ref_index, dtype=np.complex128)
+        if ri.ndim == 0:
+            ri = np.full(len(rad), ri)
+        ri2 = np.ascontiguousarray(np.stack([ri.real, ri.imag], axis=1))
+        self.n = len(rad)
+        self.pos, self.rad = pos, rad
+        self.ctx = self.L.orc_create(self.n, _p(pos), _p(rad), _p(ri2), float(mie_eps), int(store_matrix),
+                                     int(nthreads))
+        self.neqns = self.L.orc_neqns(self.ctx)
+        self.order = np.zeros(self.n, np.int32)
+        self.offset = np.zeros(self.n + 1, np.int32)
+        self.mie_offset = np.zeros(self.n + 1, np.int32)
+        self.L.orc_orders(self.ctx, _p(self.order), _p(self.offset), _p(self.mie_offset))
+
+    def close(self):
+        if self.ctx:
+            self.L.orc_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def mie(self):
+        nt = int(self.mie_offset[-1])
+        an = np.zeros(nt, np.complex128)
+        ai = np.zeros(nt, np.complex128)
+        qe = np.zeros(self.n)
+        qa = np.zeros(self.n)
+        self.L.orc_mie_coefs(self.ctx, _p(an), _p(ai), _p(qe), _p(qa))
+        return an, ai, qe, qa
+
+    def sphereinteraction(self, ain, con_tran=None, mie_mult=None, initial_run=False):
+        ain = np.asfortranarray(np.asarray(ain, np.complex128).reshape(self.neqns, -1, order="F"))
+        nrhs = ain.shape[1]
+        out = np.zeros((self.neqns, nrhs), np.complex128, order="F")
+        ct = np.array(con_tran if con_tran is not None else [0] * nrhs, np.int32)
+        mm = np.array(mie_mult if mie_mult is not None else [1] * nrhs, np.int32)
+        self.L.orc_sphereinteraction(self.ctx, nrhs, _p(ain), _p(out), _p(ct), _p(mm), int(initial_run))
+        return out
+
+    def cbicg(self, pnp, x0, niter=10000, eps=1e-6, initialize=True):
+        pnp = np.ascontiguousarray(pnp, np.complex128)
+        x = np.array(x0, np.complex128, copy=True)
+        it = c_int(0)
+        err = c_double(0.0)
+        rc = self.L.orc_cbicg(self.ctx, niter, eps, _p(pnp), _p(x), int(initialize), ctypes.byref(it),
+                              ctypes.byref(err))
+        return x, it.value, err.value, rc
+
+    def planewave(self, alpha=0.0, sinc=0.0, direction=1):
+        out = np.zeros((self.neqns, 2), np.complex128, order="F")
+        self.L.orc_planewave(self.ctx, alpha, sinc, direction, _p(out))
+        return out
+
+    def fixedorsoln(self, eps=1e-6, niter=10000, alpha=0.0, sinc=0.0, direction=1, direct=False):
+        amnp = np.zeros((self.neqns, 2), np.complex128, order="F")
+        qeff = np.zeros((3, 3, self.n), np.float64, order="F")
+        maxerr = c_double(0.0)
+        maxiter = c_int(0)
+        st = self.L.orc_fixedorsoln(self.ctx, alpha, sinc, direction, eps, niter, _p(amnp), _p(qeff),
+                                    ctypes.byref(maxerr), ctypes.byref(maxiter), int(direct))
+        qtot = np.zeros((3, 3), np.float64, order="F")
+        self.L.orc_qtotcalc(self.ctx, _p(qeff), _p(qtot))
+        return dict(amnp=amnp, qeff=qeff, qtot=qtot, status=st, maxerr=maxerr.value, maxiter=maxiter.value)
+
+    def direct_solve(self, pnp):
+        pnp = np.ascontiguousarray(pnp, np.complex128)
+        out = np.zeros(self.neqns, np.complex128)
+        self.L.orc_x_direct_solve(self.ctx, _p(pnp), _p(out))
+        return out
+
+    def multmie(self, x, idir=1):
+        x = np.ascontiguousarray(x, np.complex128)
+        out = np.zeros(self.neqns, np.complex128)
+        self.L.orc_x_multmie(self.ctx, idir, _p(x), _p(out))
+        return out
+
+    def vol_radius(self):
+        return self.L.orc_vol_radius(self.ctx)
+
+
+def rotcoef(cbe, kmax, nmax):
+    L = lib()
+    dc = np.zeros((nmax * (nmax + 2) + 1, 2 * kmax + 1), np.float64)
+    L.orc_x_rotcoef(cbe, kmax, nmax, _p(dc))
+    return dc  # dc[nk, m+kmax]
+
+
+def vcfunc(m, n, k, l):
+    L = lib()
+    v = np.zeros(n + l + 1)
+    L.orc_x_vcfunc(m, n, k, l, _p(v))
+    return v
+
+
+def atcdim(n, l):
+    return lib().orc_x_atcdim(n, l)
+
+
+def moffset(m, n, l):
+    return lib().orc_x_moffset(m, n, l)
+
+
+def axial(itype, r, ri, nmax, lmax):
+    L = lib()
+    ac = np.zeros(atcdim(nmax, lmax), np.complex128)
+    L.orc_x_axial(itype, r, complex(ri).real, complex(ri).imag, nmax, lmax, _p(ac))
+    return ac
+
+
+def mieoa(x, ri, qeps):
+    L = lib()
+    nodr = c_int(0)
+    if qeps < 0:
+        n = int(np.ceil(-qeps))
+    else:
+        n = 200
+    anp = np.zeros(4 * max(n, 1) + 4 * 64, np.complex128)
+    ainv = np.zeros_like(anp)
+    qe, qs, qa = c_double(), c_double(), c_double()
+    L.orc_x_mieoa(x, complex(ri).real, complex(ri).imag, qeps, ctypes.byref(nodr), ctypes.byref(qe),
+                  ctypes.byref(qs), ctypes.byref(qa), _p(anp), _p(ainv))
+    nd = nodr.value
+    return dict(order=nd, qext=qe.value, qsca=qs.value, qabs=qa.value, anp=anp[:4 * nd].reshape(nd, 2, 2),
+                anp_inv=ainv[:4 * nd].reshape(nd, 2, 2))
+
+
+def translate_rot(ns, nt, rvec, a, vtype=3, sop=False, top=False):
+    L = lib()
+    rv = np.ascontiguousarray(rvec, np.float64)
+    a = np.ascontiguousarray(a, np.complex128)
+    g = np.zeros(2 * nt * (nt + 2), np.complex128)
+    L.orc_x_translate_rot(ns, nt, _p(rv), vtype, _p(a), _p(g), int(sop), int(top))
+    return g
+
+
+def gentranmatrix(ns, nt, rvec, vtype=3):
+    L = lib()
+    rv = np.ascontiguousarray(rvec, np.float64)
+    nbs, nbt = ns * (ns + 2), nt * (nt + 2)
+    ac = np.zeros(nbt * nbs * 2, np.complex128)
+    L.orc_x_gentranmatrix(ns, nt, _p(rv), vtype, _p(ac))
+    return ac.reshape(2, nbs, nbt).transpose(2, 1, 0)  # [row kla, col mna, mode]

@@ -1,0 +1,134 @@
+"""Pins of the CPU oracle (oracle/) by known answers and independent routes.
+
+MSTM ships no tests, golden vectors or expected outputs and cannot be compiled
+here (Fortran, no compiler), so the oracle is pinned by:
+  * Mie coefficients vs an independent Bohren-Huffman implementation (scipy),
+    from tests/golden/mie_bh.npz (made by tests/golden/make_golden.py);
+  * the rotation/axial pair translation vs MSTM's independent dense
+    translation matrix (gentranmatrix, mstm-modules-33.f90:1762-1888);
+  * Wigner-d orthogonality, table offsets, the N=1 cluster == Mie identity,
+    energy balance and BiCG == dense LU (mstm-solver-8.f90:571-642).
+"""
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_mie_matches_bohren_huffman(oracle_mod):
+    g = np.load(os.path.join(GOLDEN, "mie_bh.npz"))
+    for k in range(len(g["x"])):
+        x, m, L = float(g["x"][k]), complex(g["m"][k]), int(g["L"][k])
+        r = oracle_mod.mieoa(x, m, -L)
+        assert r["order"] == L
+        A = r["anp"].reshape(L, 4)  # (1,1),(2,1),(1,2),(2,2) per order
+        m11 = (A[:, 0] + A[:, 2] + A[:, 1] + A[:, 3]) / 2
+        m22 = (A[:, 0] - A[:, 2] - A[:, 1] + A[:, 3]) / 2
+        a, b = g["a"][k][:L], g["b"][k][:L]
+        assert np.allclose(m11, -a, rtol=0, atol=1e-13 * max(1, np.abs(a).max()))
+        assert np.allclose(m22, -b, rtol=0, atol=1e-13 * max(1, np.abs(b).max()))
+        assert abs(r["qext"] / g["qext"][k] - 1) < 1e-12
+        assert abs(r["qsca"] / g["qsca"][k] - 1) < 1e-12
+
+
+def test_mie_order_rule(oracle_mod):
+    # mie_epsilon > 0: nstop = nint(x + 4 x^(1/3)) + 5 then converge; forced order for <0
+    assert oracle_mod.mieoa(1.0, 1.5 + 0.01j, -7)["order"] == 7
+    r = oracle_mod.mieoa(2.0, 1.6 + 0.05j, 1e-6)
+    assert 5 <= r["order"] <= 12
+
+
+@pytest.mark.parametrize("ct", [0.9, 0.3, -0.55, 1.0, -1.0])
+def test_wigner_orthogonal(oracle_mod, ct):
+    L = 9
+    dc = oracle_mod.rotcoef(ct, L, L)
+    for n in range(1, L + 1):
+        D = np.array([[dc[n * (n + 1) + k, m + L] for k in range(-n, n + 1)] for m in range(-n, n + 1)])
+        assert np.allclose(D @ D.T, np.eye(2 * n + 1), atol=1e-12)
+
+
+def test_axial_offsets_match_moffset(oracle_mod):
+    for nt, ns in [(7, 7), (9, 9), (5, 8), (8, 5), (3, 10)]:
+        off = 0
+        nlmin = min(nt, ns)
+        for ma in range(0, nlmin + 1):
+            m1 = max(1, ma)
+            for m in ([0] if ma == 0 else [-ma, ma]):
+                assert oracle_mod.moffset(m, nt, ns) == off
+                off += 2 * (nt - m1 + 1) * (ns - m1 + 1)
+        assert off == oracle_mod.atcdim(nt, ns)
+
+
+@pytest.mark.parametrize("ns,nt", [(7, 7), (5, 8), (9, 4), (9, 9)])
+@pytest.mark.parametrize("r", [2.0, 4.5, 20.0])
+def test_rotation_translation_equals_dense(oracle_mod, ns, nt, r):
+    rng = np.random.default_rng(ns * 100 + nt)
+    d = rng.normal(size=3)
+    rv = d / np.linalg.norm(d) * r
+    a = rng.normal(size=2 * ns * (ns + 2)) + 1j * rng.normal(size=2 * ns * (ns + 2))
+    nbs = ns * (ns + 2)
+    H = oracle_mod.gentranmatrix(ns, nt, rv)
+    ref = np.concatenate([H[:, :, 0] @ a[:nbs], H[:, :, 1] @ a[nbs:]])
+    for sop in (False, True):
+        g = oracle_mod.translate_rot(ns, nt, rv, a, sop=sop)
+        assert np.abs(g - ref).max() <= 1e-12 * np.abs(ref).max()
+    Ht = oracle_mod.gentranmatrix(nt, ns, -rv)
+    reft = np.concatenate([Ht[:, :, 0].T @ a[:nbs], Ht[:, :, 1].T @ a[nbs:]])
+    for sop in (False, True):
+        g = oracle_mod.translate_rot(ns, nt, rv, a, sop=sop, top=True)
+        assert np.abs(g - reft).max() <= 1e-12 * np.abs(reft).max()
+
+
+def test_regular_translation_round_trip(oracle_mod):
+    # translate j->i then i->j with regular (J) functions: identity within truncation
+    L, Lbig = 4, 22
+    rng = np.random.default_rng(5)
+    a = np.zeros(2 * L * (L + 2), complex)
+    a[:] = rng.normal(size=a.size) + 1j * rng.normal(size=a.size)
+    rv = np.array([0.3, -0.2, 0.25])
+    g = oracle_mod.translate_rot(L, Lbig, rv, a, vtype=1)
+    back = oracle_mod.translate_rot(Lbig, L, -rv, g, vtype=1)
+    assert np.abs(back - a).max() < 1e-8 * np.abs(a).max()
+
+
+def test_single_sphere_equals_mie(oracle_mod):
+    o = oracle_mod.Oracle([[0.0, 0.0, 0.0]], [1.0], [1.5 + 0.01j], mie_eps=-7)
+    r = o.fixedorsoln()
+    m = oracle_mod.mieoa(1.0, 1.5 + 0.01j, -7)
+    assert abs(r["qtot"][0, 0] / m["qext"] - 1) < 1e-12
+    assert abs(r["qtot"][1, 0] / m["qabs"] - 1) < 1e-12
+    assert abs(r["qtot"][2, 0] / m["qsca"] - 1) < 1e-12
+
+
+def _small_cluster():
+    return np.array([[0, 0, 0], [2.5, 0.3, 0.1], [-0.4, 2.6, 0.5], [0.2, -0.3, 2.7], [2.4, 2.5, -0.2]], float)
+
+
+def test_bicg_equals_dense_lu(oracle_mod):
+    o = oracle_mod.Oracle(_small_cluster(), [1.0] * 5, [1.5 + 0.01j] * 5, mie_eps=-7)
+    r = o.fixedorsoln(eps=1e-14)
+    rd = o.fixedorsoln(direct=True)
+    assert np.allclose(r["qtot"], rd["qtot"], rtol=1e-7, atol=0)
+    assert np.abs(r["amnp"] - rd["amnp"]).max() < 1e-6 * np.abs(rd["amnp"]).max()
+
+
+def test_energy_balance_and_polarisation_mean(oracle_mod):
+    o = oracle_mod.Oracle(_small_cluster(), [1.0] * 5, [1.5 + 0.01j] * 5, mie_eps=-7)
+    r = o.fixedorsoln(eps=1e-10)
+    q = r["qtot"]
+    assert np.allclose(q[0] - q[1], q[2], rtol=1e-12)        # Qsca = Qext - Qabs (real medium)
+    assert np.allclose(q[:, 0], 0.5 * (q[:, 1] + q[:, 2]), rtol=1e-12)
+    assert np.all(q[1] > 0) and np.all(q[2] > 0)
+
+
+def test_store_and_recompute_modes_agree(oracle_mod):
+    pos = _small_cluster()
+    a = oracle_mod.Oracle(pos, [1.0] * 5, [1.5 + 0.01j] * 5, mie_eps=-7, store_matrix=True)
+    b = oracle_mod.Oracle(pos, [1.0] * 5, [1.5 + 0.01j] * 5, mie_eps=-7, store_matrix=False, nthreads=2)
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(a.neqns, 2)) + 1j * rng.normal(size=(a.neqns, 2))
+    ya = a.sphereinteraction(x, con_tran=[0, 1], initial_run=True)
+    yb = b.sphereinteraction(x, con_tran=[0, 1], initial_run=True)
+    assert np.abs(ya - yb).max() <= 1e-13 * np.abs(ya).max()
