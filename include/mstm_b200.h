@@ -110,6 +110,20 @@ int mstmg_operator_bytes(const mstmg_ctx *ctx, int prec, double *stored_bytes, d
  * events on the context stream; returns the average milliseconds per pass. */
 int mstmg_time_translation(mstmg_ctx *ctx, int prec, int nrhs, int reps, double *ms_per_pass);
 
+/* Run this context's work on the caller's CUDA stream (a cudaStream_t; NULL
+ * restores the context's own stream).  Lets a caller time a solve with its
+ * own events on the stream the kernels are launched on. */
+int mstmg_set_stream(mstmg_ctx *ctx, void *stream);
+
+/* Kernel timing: when enabled, every translation launch is bracketed by CUDA
+ * events; mstmg_kernel_time returns the summed milliseconds and launch counts
+ * of the FP64 and FP32 translation kernels since the last reset. */
+int mstmg_set_timing(mstmg_ctx *ctx, int enable);
+int mstmg_kernel_time(mstmg_ctx *ctx, double *ms64, int *n64, double *ms32, int *n32);
+
+/* Number of kernels this library has launched in the process so far. */
+long long mstmg_kernel_launches(void);
+
 /* Message of the last error on this thread. */
 const char *mstmg_last_error(void);
 

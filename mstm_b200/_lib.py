@@ -32,6 +32,10 @@ SIGNATURES = {
     "mstmg_last_stats": (c_int, [c_void_p, c_void_p, P(c_int), P(c_int), P(c_int)]),
     "mstmg_operator_bytes": (c_int, [c_void_p, c_int, P(c_double), P(c_double)]),
     "mstmg_time_translation": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),
+    "mstmg_set_stream": (c_int, [c_void_p, c_void_p]),
+    "mstmg_set_timing": (c_int, [c_void_p, c_int]),
+    "mstmg_kernel_time": (c_int, [c_void_p, P(c_double), P(c_int), P(c_double), P(c_int)]),
+    "mstmg_kernel_launches": (ctypes.c_longlong, []),
     "mstmg_last_error": (ctypes.c_char_p, []),
 }
 

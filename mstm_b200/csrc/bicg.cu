@@ -263,6 +263,7 @@ void launch_post(const SlotMaps& sm, const cpx<T>* an, const cpx<T>* p, const cp
     int g = grid_for(sm.nslots, nsm);
     post_kernel<T><<<g, RB, 0, st>>>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, an, p, w, y0, y1, cap, caw, part);
     fin_kernel<<<1, 32, 0, st>>>(1, g, part, sc, 0.0, 1);
+    launch_counter() += 2;
 }
 template <typename T>
 void launch_init(const SlotMaps& sm, const cpx<T>* an, const cpx<T>* b, const cpx<T>* x, const cpx<T>* y0, int have_y, cpx<T>* r,
@@ -271,6 +272,7 @@ void launch_init(const SlotMaps& sm, const cpx<T>* an, const cpx<T>* b, const cp
     int g = grid_for(sm.nslots, nsm);
     init_kernel<T><<<g, RB, 0, st>>>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, an, b, x, y0, have_y, r, p, w, q, part);
     fin_kernel<<<1, 32, 0, st>>>(0, g, part, sc, 0.0, normalize);
+    launch_counter() += 2;
 }
 template <typename T>
 void launch_upd(int n, cpx<T>* x, cpx<T>* r, cpx<T>* q, cpx<T>* p, cpx<T>* w, const cpx<T>* cap, const cpx<T>* caw, double* part,
@@ -280,6 +282,7 @@ void launch_upd(int n, cpx<T>* x, cpx<T>* r, cpx<T>* q, cpx<T>* p, cpx<T>* w, co
     upd1_kernel<T><<<g, RB, 0, st>>>(n, sc, x, r, q, p, cap, caw, part);
     fin_kernel<<<1, 32, 0, st>>>(2, g, part, sc, eps, 1);
     upd2_kernel<T><<<g, RB, 0, st>>>(n, sc, p, w, r, q);
+    launch_counter() += 3;
 }
 template <typename T, typename TB>
 void launch_resid(const SlotMaps& sm, const cpx<T>* an, const cpx<T>* b, const cpx<T>* x, const cpx<T>* y, cpx<TB>* rout, double* part,
@@ -288,11 +291,12 @@ void launch_resid(const SlotMaps& sm, const cpx<T>* an, const cpx<T>* b, const c
     int g = grid_for(sm.nslots, nsm);
     resid_kernel<T, TB><<<g, RB, 0, st>>>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, an, b, x, y, rout, part);
     sum2_kernel<<<1, 32, 0, st>>>(g, part, out2);
+    launch_counter() += 2;
 }
-void launch_add_correction_f(int n, zd* x, const zf* d, cudaStream_t st) { add_correction_kernel<float><<<296, 256, 0, st>>>(n, x, d); }
-void launch_add_correction_d(int n, zd* x, const zd* d, cudaStream_t st) { add_correction_kernel<double><<<296, 256, 0, st>>>(n, x, d); }
-template <typename T> void launch_conj_copy(int n, const cpx<T>* a, cpx<T>* b, cudaStream_t st) { conj_copy_kernel<T><<<296, 256, 0, st>>>(n, a, b); }
-void launch_d2f(int n, const zd* a, zf* b, cudaStream_t st) { d2f_kernel<<<296, 256, 0, st>>>(n, a, b); }
+void launch_add_correction_f(int n, zd* x, const zf* d, cudaStream_t st) { add_correction_kernel<float><<<296, 256, 0, st>>>(n, x, d); launch_counter() += 1; }
+void launch_add_correction_d(int n, zd* x, const zd* d, cudaStream_t st) { add_correction_kernel<double><<<296, 256, 0, st>>>(n, x, d); launch_counter() += 1; }
+template <typename T> void launch_conj_copy(int n, const cpx<T>* a, cpx<T>* b, cudaStream_t st) { conj_copy_kernel<T><<<296, 256, 0, st>>>(n, a, b); launch_counter() += 1; }
+void launch_d2f(int n, const zd* a, zf* b, cudaStream_t st) { d2f_kernel<<<296, 256, 0, st>>>(n, a, b); launch_counter() += 1; }
 
 template void launch_post<double>(const SlotMaps&, const zd*, const zd*, const zd*, const zd*, const zd*, zd*, zd*, double*, BicgScalars*, int, cudaStream_t);
 template void launch_post<float>(const SlotMaps&, const zf*, const zf*, const zf*, const zf*, const zf*, zf*, zf*, double*, BicgScalars*, int, cudaStream_t);

@@ -78,6 +78,13 @@ struct mstmg_ctx {
     BicgScalars* h_sc = nullptr;
     double* h_small = nullptr;
     int iters[2] = {0, 0}, outer = 0, passes64 = 0, passes32 = 0;
+    cudaStream_t own_st = nullptr;
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    struct Pending { cudaEvent_t a, b; int prec; };
+    std::vector<Pending> pending;
+    double kt_ms[2] = {0.0, 0.0};
+    int kt_n[2] = {0, 0};
     SlotMaps sm() const { return SlotMaps{neqns / 2, slot.p, d_order.p, d_offset.p, d_mie_offset.p}; }
 };
 
@@ -113,6 +120,25 @@ extern "C" void mstmg_default_opts(mstmg_opts* o)
 }
 
 extern "C" const char* mstmg_last_error(void) { return g_err.c_str(); }
+
+// Fold completed translation-kernel event pairs into the running totals.
+static void resolve_timing(mstmg_ctx* c)
+{
+    std::vector<mstmg_ctx::Pending> keep;
+    for (auto& p : c->pending) {
+        if (cudaEventQuery(p.b) == cudaSuccess) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, p.a, p.b);
+            c->kt_ms[p.prec] += ms;
+            c->kt_n[p.prec] += 1;
+            c->ev_pool.push_back(p.a);
+            c->ev_pool.push_back(p.b);
+        } else {
+            keep.push_back(p);
+        }
+    }
+    c->pending.swap(keep);
+}
 
 static int check_kernel_err(mstmg_ctx* c)
 {
@@ -191,20 +217,37 @@ static int setup_layout(mstmg_ctx* c)
         return MSTMG_ERR_UNSUPPORTED;
     }
     c->npairs = (int)np;
+    // Pair order: a round-robin tournament (circle method).  Each round holds
+    // floor(N/2) pairs with no sphere in common, so the pairs that concurrent
+    // CTAs work on touch disjoint output blocks and their atomic adds do not
+    // collide.  Pairs keep i < j, the reference's orientation of the operator.
     std::vector<int2> pr(np > 0 ? np : 1);
     std::vector<long long> off(np > 0 ? np : 1);
     long long u = 0;
     int maxrec = 4;
     long long t = 0;
-    for (int i = 0; i < n - 1; i++)
-        for (int j = i + 1; j < n; j++) {
-            pr[t] = make_int2(i, j);
-            off[t] = u;
-            int rec = op_record_units(c->order[i], c->order[j]);
-            maxrec = std::max(maxrec, rec);
-            u += rec;
-            t++;
+    {
+        int M = (n % 2 == 0) ? n : n + 1;   // with a dummy player when n is odd
+        for (int r = 0; r < M - 1 && n > 1; r++) {
+            for (int k = 0; k < M / 2; k++) {
+                int a_, b_;
+                if (k == 0) { a_ = M - 1; b_ = r; }
+                else { a_ = (r + k) % (M - 1); b_ = (r - k + (M - 1)) % (M - 1); }
+                if (a_ >= n || b_ >= n) continue;
+                int i = a_ < b_ ? a_ : b_, j = a_ < b_ ? b_ : a_;
+                pr[t] = make_int2(i, j);
+                off[t] = u;
+                int rec = op_record_units(c->order[i], c->order[j]);
+                maxrec = std::max(maxrec, rec);
+                u += rec;
+                t++;
+            }
         }
+    }
+    if (t != np) {
+        set_err("internal error: pair schedule incomplete");
+        return MSTMG_ERR_ARG;
+    }
     c->op_units = u;
     c->maxrec = maxrec;
     if (np > 0) {
@@ -279,7 +322,8 @@ extern "C" int mstmg_ctx_create(mstmg_ctx** out, int nsphere, const double* pos,
             return MSTMG_ERR_CUDA;
         }
         cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->opts.device);
-        e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+        e = cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking);
+        c->st = c->own_st;
         if (e != cudaSuccess) {
             set_err(std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
             delete c;
@@ -346,7 +390,9 @@ extern "C" void mstmg_ctx_destroy(mstmg_ctx* c)
     c->sc.release();
     if (c->h_sc) cudaFreeHost(c->h_sc);
     if (c->h_small) cudaFreeHost(c->h_small);
-    if (c->st) cudaStreamDestroy(c->st);
+    for (auto& p : c->pending) { c->ev_pool.push_back(p.a); c->ev_pool.push_back(p.b); }
+    for (auto ev : c->ev_pool) cudaEventDestroy(ev);
+    if (c->own_st) cudaStreamDestroy(c->own_st);
     delete c;
 }
 
@@ -440,8 +486,20 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
     a.lmax = c->lmax;
     a.maxrec = c->maxrec;
     a.err = c->err.p;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c->timing) {
+        for (cudaEvent_t* ev : {&e0, &e1}) {
+            if (!c->ev_pool.empty()) { *ev = c->ev_pool.back(); c->ev_pool.pop_back(); }
+            else CK(cudaEventCreate(ev));
+        }
+        CK(cudaEventRecord(e0, c->st));
+    }
     launch_translate<T>(a, c->nsm, c->st);
     CK(cudaGetLastError());
+    if (c->timing) {
+        CK(cudaEventRecord(e1, c->st));
+        c->pending.push_back({e0, e1, sizeof(T) == 8 ? 0 : 1});
+    }
     if (sizeof(T) == 8) c->passes64++;
     else c->passes32++;
     return MSTMG_OK;
@@ -804,6 +862,41 @@ extern "C" int mstmg_operator_bytes(const mstmg_ctx* c, int prec, double* stored
     }
     return MSTMG_OK;
 }
+
+extern "C" int mstmg_set_stream(mstmg_ctx* c, void* stream)
+{
+    if (!c) return MSTMG_ERR_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    c->st = stream ? (cudaStream_t)stream : c->own_st;
+    return MSTMG_OK;
+}
+
+extern "C" int mstmg_set_timing(mstmg_ctx* c, int enable)
+{
+    if (!c) return MSTMG_ERR_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    resolve_timing(c);
+    c->timing = enable != 0;
+    c->kt_ms[0] = c->kt_ms[1] = 0.0;
+    c->kt_n[0] = c->kt_n[1] = 0;
+    return MSTMG_OK;
+}
+
+extern "C" int mstmg_kernel_time(mstmg_ctx* c, double* ms64, int* n64, double* ms32, int* n32)
+{
+    if (!c) return MSTMG_ERR_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    resolve_timing(c);
+    if (ms64) *ms64 = c->kt_ms[0];
+    if (n64) *n64 = c->kt_n[0];
+    if (ms32) *ms32 = c->kt_ms[1];
+    if (n32) *n32 = c->kt_n[1];
+    c->kt_ms[0] = c->kt_ms[1] = 0.0;
+    c->kt_n[0] = c->kt_n[1] = 0;
+    return MSTMG_OK;
+}
+
+extern "C" long long mstmg_kernel_launches(void) { return launch_counter().load(); }
 
 extern "C" int mstmg_time_translation(mstmg_ctx* c, int prec, int nrhs, int reps, double* ms)
 {

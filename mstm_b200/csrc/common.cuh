@@ -5,6 +5,14 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <atomic>
+
+// Count of kernels launched by this library (all contexts, all threads).
+inline std::atomic<long long>& launch_counter()
+{
+    static std::atomic<long long> n{0};
+    return n;
+}
 
 #define MSTMG_LMAX 16          // largest sphere truncation order the kernels accept
 

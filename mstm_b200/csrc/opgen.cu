@@ -222,4 +222,5 @@ void launch_opgen(const OpGenArgs& a, int nsm, cudaStream_t st)
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     opgen_kernel<<<blocks, warps * 32, smem, st>>>(a);
+    launch_counter() += 1;
 }

@@ -123,11 +123,13 @@ void launch_mie_orders(int n, const double* radius, const double* ri, double mre
                        cudaStream_t st)
 {
     mie_order_kernel<<<(n + 63) / 64, 64, 0, st>>>(n, radius, ri, mre, mim, qeps, order);
+    launch_counter() += 1;
 }
 void launch_mie_coefs(int n, const double* radius, const double* ri, double mre, double mim, const int* order,
                       const int* mie_offset, zd* an, zd* an_inv, float* an32, double* qext, double* qabs, cudaStream_t st)
 {
     mie_coef_kernel<<<(n + 63) / 64, 64, 0, st>>>(n, radius, ri, mre, mim, order, mie_offset, an, an_inv, an32, qext, qabs);
+    launch_counter() += 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -263,6 +265,7 @@ void launch_planewave(double alpha, double sinc, int dir, int lmax, int neqns, c
     planewave_common_kernel<<<1, 32, 0, st>>>(alpha, cbinc, lmax, pw0, drot);
     planewave_phase_kernel<<<(neqns + 255) / 256, 256, 0, st>>>(neqns, slot_full, order, offset, pos, lmax, pw0, cbinc, riinc,
                                                                  sinc, alpha, pmnp, neqns);
+    launch_counter() += 2;
 }
 
 // ---------------------------------------------------------------------------
@@ -303,6 +306,7 @@ void launch_mie(int nslots, const int* slot_sphere, const int* order, const int*
                 int idir, int conj_in, const cpx<T>* x, cpx<T>* y, cudaStream_t st)
 {
     mie_kernel<T><<<(nslots + 255) / 256, 256, 0, st>>>(nslots, slot_sphere, order, offset, mie_offset, an, idir, conj_in, x, y);
+    launch_counter() += 1;
 }
 template void launch_mie<double>(int, const int*, const int*, const int*, const int*, const zd*, int, int, const zd*, zd*, cudaStream_t);
 template void launch_mie<float>(int, const int*, const int*, const int*, const int*, const zf*, int, int, const zf*, zf*, cudaStream_t);
@@ -409,4 +413,5 @@ void launch_qeff(int nsph, const int* order, const int* offset, const int* mie_o
 {
     qeff_kernel<<<(nsph + 63) / 64, 64, 0, st>>>(nsph, order, offset, mie_offset, radius, rimed, an_inv, amnp, pmnp0, ld, qeff);
     qtot_kernel<<<1, 32, 0, st>>>(nsph, radius, qeff, xg, qtot);
+    launch_counter() += 2;
 }

@@ -297,6 +297,7 @@ template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cuda
     if (blocks > a.npairs) blocks = a.npairs;
     if (blocks < 1) return;
     translate_kernel<T, NT><<<blocks, NT, smem, st>>>(a);
+    launch_counter() += 1;
 }
 
 template void launch_translate<double>(const TransArgs<double>&, int, cudaStream_t);
