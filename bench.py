@@ -368,7 +368,20 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-REF_ITERS = [60, 60]
+REF_ITERS = [79, 78]
+
+
+def run_translation_case(args):
+    """Operator generation + `--translation-passes` translation passes of one
+    workload, timed with CUDA events (the case the ncu captures use)."""
+    from mstm_b200 import api, configs as C
+    w = C.workload(args.workload)
+    g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=-w["order"], precision=args.precision)
+    ms = g.time_translation(args.precision, args.nrhs, args.translation_passes)
+    sb, cb = g.operator_bytes(args.precision)
+    print(json.dumps({"workload": args.workload, "precision": args.precision, "nrhs": args.nrhs, "ms_per_pass": ms,
+                      "operator_bytes": sb, "operator_gbs": sb / ms / 1e6}))
+    g.close()   # cbicg iterations of the FP64 solve of this workload (both polarisations)
 
 
 def main():
@@ -378,8 +391,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--translation-passes", type=int, default=0,
+                    help="profiling case: only run this many translation passes (no solve)")
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--nrhs", type=int, default=4)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.translation_passes:
+        run_translation_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
