@@ -52,6 +52,7 @@ typedef struct {
     int translation_switch_order;  /* MSTM translation_switch_order (mstm-modules-33.f90:5126), default 3 */
     double inner_eps;              /* mixed mode: squared residual reduction per inner solve (default 1e-8) */
     int max_outer;                 /* mixed mode: refinement steps cap (default 30) */
+    int generic_kernel;            /* 1: always use the order-generic translation kernel (default 0) */
 } mstmg_opts;
 
 /* Fill opts with the defaults above. */

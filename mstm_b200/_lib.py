@@ -42,7 +42,8 @@ SIGNATURES = {
 
 class MstmgOpts(ctypes.Structure):
     _fields_ = [("precision", c_int), ("device", c_int), ("medium_re", c_double), ("medium_im", c_double),
-                ("translation_switch_order", c_int), ("inner_eps", c_double), ("max_outer", c_int)]
+                ("translation_switch_order", c_int), ("inner_eps", c_double), ("max_outer", c_int),
+                ("generic_kernel", c_int)]
 
 
 class MstmgError(RuntimeError):

@@ -12,6 +12,7 @@
 #include "bicg.cuh"
 #include "sphere_kernels.cuh"
 #include "tables.h"
+#include "translate_tiled.cuh"
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
@@ -65,6 +66,9 @@ struct mstmg_ctx {
     DevBuf<float> an32;
     DevBuf<int2> pairs;
     DevBuf<long long> opoff;
+    DevBuf<int4> tiles;
+    int ntiles = 0;
+    bool tiled = false;   // monodisperse cluster: pairs stored in tile order for the fast kernel
     DevBuf<double> op64;
     DevBuf<float> op32;
     bool ops64_ready = false, ops32_ready = false;
@@ -117,6 +121,7 @@ extern "C" void mstmg_default_opts(mstmg_opts* o)
     o->translation_switch_order = 3;
     o->inner_eps = 1.0e-8;
     o->max_outer = 30;
+    o->generic_kernel = 0;
 }
 
 extern "C" const char* mstmg_last_error(void) { return g_err.c_str(); }
@@ -217,32 +222,64 @@ static int setup_layout(mstmg_ctx* c)
         return MSTMG_ERR_UNSUPPORTED;
     }
     c->npairs = (int)np;
-    // Pair order: a round-robin tournament (circle method).  Each round holds
-    // floor(N/2) pairs with no sphere in common, so the pairs that concurrent
-    // CTAs work on touch disjoint output blocks and their atomic adds do not
+    // Pair order.  Monodisperse clusters of a supported order use tiles of
+    // TILE_B x TILE_B sphere blocks (translate_tiled.cu); the block pairs are
+    // visited in round-robin tournament order (circle method), so tiles that
+    // run at the same time write mostly disjoint spheres.  Otherwise the pairs
+    // themselves follow the tournament order: each round holds floor(N/2)
+    // pairs with no sphere in common, so concurrent CTAs' atomic adds do not
     // collide.  Pairs keep i < j, the reference's orientation of the operator.
     std::vector<int2> pr(np > 0 ? np : 1);
     std::vector<long long> off(np > 0 ? np : 1);
     long long u = 0;
     int maxrec = 4;
     long long t = 0;
-    {
-        int M = (n % 2 == 0) ? n : n + 1;   // with a dummy player when n is odd
-        for (int r = 0; r < M - 1 && n > 1; r++) {
+    auto add_pair = [&](int i, int j) {
+        pr[t] = make_int2(i, j);
+        off[t] = u;
+        int rec = op_record_units(c->order[i], c->order[j]);
+        maxrec = std::max(maxrec, rec);
+        u += rec;
+        t++;
+    };
+    auto tournament = [](int n, std::vector<std::pair<int, int>>& out) {
+        int M = (n % 2 == 0) ? n : n + 1;
+        for (int r = 0; r < M - 1 && n > 1; r++)
             for (int k = 0; k < M / 2; k++) {
                 int a_, b_;
                 if (k == 0) { a_ = M - 1; b_ = r; }
                 else { a_ = (r + k) % (M - 1); b_ = (r - k + (M - 1)) % (M - 1); }
                 if (a_ >= n || b_ >= n) continue;
-                int i = a_ < b_ ? a_ : b_, j = a_ < b_ ? b_ : a_;
-                pr[t] = make_int2(i, j);
-                off[t] = u;
-                int rec = op_record_units(c->order[i], c->order[j]);
-                maxrec = std::max(maxrec, rec);
-                u += rec;
-                t++;
+                out.push_back({std::min(a_, b_), std::max(a_, b_)});
             }
+    };
+    c->tiled = !c->opts.generic_kernel && (lm == lmin) && tiled_supported(lm, 1) && n > 1 && n < 65536;
+    std::vector<int4> tl;
+    if (c->tiled) {
+        const int B = TILE_B;
+        int nb = (n + B - 1) / B;
+        std::vector<std::pair<int, int>> bp;
+        tournament(nb, bp);
+        for (int I = 0; I < nb; I++) bp.push_back({I, I});
+        for (auto& IJ : bp) {
+            int I = IJ.first, J = IJ.second;
+            int i0 = I * B, j0 = J * B;
+            int start = (int)t;
+            for (int i = i0; i < std::min(n, i0 + B); i++)
+                for (int j = j0; j < std::min(n, j0 + B); j++)
+                    if (i < j) add_pair(i, j);
+            int cnt = (int)t - start;
+            if (cnt > 0) tl.push_back(make_int4(start, cnt, (i0 << 16) | j0, I == J ? 1 : 0));
         }
+    } else {
+        std::vector<std::pair<int, int>> pp;
+        tournament(n, pp);
+        for (auto& ij : pp) add_pair(ij.first, ij.second);
+    }
+    c->ntiles = (int)tl.size();
+    if (c->ntiles > 0) {
+        CK(c->tiles.alloc(tl.size()));
+        CK(cudaMemcpyAsync(c->tiles.p, tl.data(), sizeof(int4) * tl.size(), cudaMemcpyHostToDevice, c->st));
     }
     if (t != np) {
         set_err("internal error: pair schedule incomplete");
@@ -386,6 +423,7 @@ extern "C" void mstmg_ctx_destroy(mstmg_ctx* c)
     c->an32.release();
     c->op32.release();
     c->pairs.release();
+    c->tiles.release();
     c->opoff.release();
     c->sc.release();
     if (c->h_sc) cudaFreeHost(c->h_sc);
@@ -486,6 +524,21 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
     a.lmax = c->lmax;
     a.maxrec = c->maxrec;
     a.err = c->err.p;
+    TiledArgs<T> ta;
+    bool use_tiled = c->tiled && tiled_supported(c->lmax, nrhs);
+    if (use_tiled) {
+        ta.ntiles = c->ntiles;
+        ta.tiles = c->tiles.p;
+        ta.pairs = c->pairs.p;
+        ta.ops = ops_ptr<T>(c);
+        ta.x = x;
+        ta.y = y;
+        ta.ld = c->neqns;
+        ta.nrhs = nrhs;
+        ta.nsph = c->n;
+        ta.contran = contran;
+        ta.err = c->err.p;
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->timing) {
         for (cudaEvent_t* ev : {&e0, &e1}) {
@@ -494,7 +547,7 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
         }
         CK(cudaEventRecord(e0, c->st));
     }
-    launch_translate<T>(a, c->nsm, c->st);
+    if (!use_tiled || launch_translate_tiled<T>(ta, c->lmax, c->nsm, c->st) != 0) launch_translate<T>(a, c->nsm, c->st);
     CK(cudaGetLastError());
     if (c->timing) {
         CK(cudaEventRecord(e1, c->st));

@@ -2,7 +2,7 @@
 // the layout).  Shared by the generator and the translation kernel.
 #pragma once
 
-__host__ __device__ inline int op_rot_size(int nmax, int nmin)
+__host__ __device__ constexpr int op_rot_size(int nmax, int nmin)
 {
     int s = 0;
     for (int n = 1; n <= nmax; n++) {
@@ -11,7 +11,7 @@ __host__ __device__ inline int op_rot_size(int nmax, int nmin)
     }
     return s;
 }
-__host__ __device__ inline int op_rot_offset(int n, int nmin)   // offset of E_n from the start of the rot section
+__host__ __device__ constexpr int op_rot_offset(int n, int nmin)   // offset of E_n from the start of the rot section
 {
     int s = 0;
     for (int q = 1; q < n; q++) {
@@ -20,7 +20,7 @@ __host__ __device__ inline int op_rot_offset(int n, int nmin)   // offset of E_n
     }
     return s;
 }
-__host__ __device__ inline int op_z_offset(int m, int nt, int ns)  // complex offset of block Z_m (mode 0)
+__host__ __device__ constexpr int op_z_offset(int m, int nt, int ns)  // complex offset of block Z_m (mode 0)
 {
     int s = 0;
     for (int q = 0; q < m; q++) {
@@ -29,7 +29,7 @@ __host__ __device__ inline int op_z_offset(int m, int nt, int ns)  // complex of
     }
     return s;
 }
-__host__ __device__ inline int op_record_units(int nt, int ns)
+__host__ __device__ constexpr int op_record_units(int nt, int ns)
 {
     int nmin = nt < ns ? nt : ns, nmax = nt > ns ? nt : ns;
     int units = 2 + op_rot_size(nmax, nmin) + 2 * op_z_offset(nmin + 1, nt, ns);

@@ -1,0 +1,440 @@
+// translate_tiled.cu -- the pair translation pass for clusters whose spheres
+// all have one order L (the fast path; mixed orders use translate.cu).
+//
+// Same mathematics as translate.cu (MSTM's coefficient_translation,
+// december2023/mstm-modules-33.f90:6610-6787, applied in both directions per
+// pair as in external_to_external_expansion, modules:6390-6525), organised for
+// throughput:
+//   * L and the number of right-hand sides NR are template parameters, so every
+//     index is a compile-time expression and every short loop unrolls;
+//   * pairs are grouped in tiles: all pairs (i, j) with i in sphere block I
+//     and j in block J (B spheres per block).  A CTA works through whole tiles
+//     and accumulates the outputs of the tile's 2B spheres in shared memory,
+//     flushing them to y with coalesced vector atomics once per tile;
+//   * per pair the work is four small dense products over C = 4*NR columns
+//     (direction x rhs x mode), each output computed from a matrix row or
+//     column held in registers:
+//        A  shift/phase/even-odd split of the sources          (C x L(L+3)/2)
+//        B  forward rotation  [P;Q] = [E;O] [S;T]               per degree n
+//        C  axial translation  g = Z a'  (Z^T a' for i -> j)     per degree m
+//        D  back rotation + phase + shift, accumulated in smem   per degree n
+//   * the operator record of the next pair streams in with a bulk TMA copy
+//     (cp.async.bulk + mbarrier) while the current one is applied.
+#include "common.cuh"
+#include "kernels.cuh"
+#include "translate_tiled.cuh"
+
+namespace {
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mb_init(uint64_t* bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mb_expect(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(su32(dst)),
+                 "l"(src), "r"(bytes), "r"(su32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mb_try(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok)
+                 : "r"(su32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mb_wait(uint64_t* bar, uint32_t parity)
+{
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mb_try(bar, parity)) return true;
+    return false;
+}
+
+template <typename T> __device__ __forceinline__ void red_add(cpx<T>* p, cpx<T> v);
+template <> __device__ __forceinline__ void red_add<float>(cpx<float>* p, cpx<float> v)
+{
+    atomicAdd(reinterpret_cast<float2*>(p), make_float2(v.x, v.y));
+}
+template <> __device__ __forceinline__ void red_add<double>(cpx<double>* p, cpx<double> v)
+{
+    atomicAdd(&p->x, v.x);
+    atomicAdd(&p->y, v.y);
+}
+
+// degree offsets in the packed per-column arrays
+__host__ __device__ constexpr int sofs(int n) { return (n - 1) * (n + 2) / 2; }   // S/P: m = 0..n
+__host__ __device__ constexpr int tofs(int n) { return (n - 1) * n / 2; }         // T/Q: m = 1..n
+// half-block (one mode) slot of degree m, order n: MSTM's a(0:L+1,1:L) index
+template <int L> __host__ __device__ constexpr int hidx(int m, int n) { return m >= 0 ? m + (L + 2) * (n - 1) : (n + 1) + (L + 2) * (-m - 1); }
+
+}  // namespace
+
+template <typename T, int L, int NR, int B>
+__global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
+{
+    constexpr int NT = 256;
+    constexpr int C = 4 * NR;            // columns: ((dir*NR)+r)*2+p
+    constexpr int CB = 4;                // columns per item
+    constexpr int NG = C / CB;
+    constexpr int NS = L * (L + 3) / 2;
+    constexpr int NQ = L * (L + 1) / 2;
+    constexpr int NB2 = L * (L + 2);     // NS + NQ
+    constexpr int NB = 2 * NB2;
+    constexpr int REC = op_record_units(L, L);
+    constexpr int RS = op_rot_size(L, L);
+    constexpr int NSLOT = 2 * B;
+
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+    short2* tabS = reinterpret_cast<short2*>(sm + 64);                     // NS entries: (n, m)
+    short2* tabQ = tabS + NS;                                               // NQ entries: (n, m>=1)
+    short4* tabZ = reinterpret_cast<short4*>(tabQ + NQ + (((NS + NQ) & 1) ? 1 : 0));   // NB2 entries: (m, q, line, zoff)
+    size_t off = 64 + sizeof(short2) * (NS + NQ + 1) + sizeof(short4) * NB2;
+    off = (off + 127) & ~(size_t)127;
+    cpx<T>* ephm = reinterpret_cast<cpx<T>*>(sm + off);                     // 2L+1
+    off += sizeof(cpx<T>) * (2 * L + 1);
+    off = (off + 127) & ~(size_t)127;
+    T* opb = reinterpret_cast<T*>(sm + off);                                // 2 x REC
+    off += sizeof(T) * 2 * REC;
+    off = (off + 127) & ~(size_t)127;
+    cpx<T>* W1 = reinterpret_cast<cpx<T>*>(sm + off);                       // C x NB2: S/T, then G
+    cpx<T>* W2 = W1 + C * NB2;                                              // C x NB2: P/Q
+    cpx<T>* ACC = W2 + C * NB2;                                             // NSLOT x NR x NB
+
+    const int tid = threadIdx.x;
+    // ---- one-time tables ----
+    for (int e = tid; e < NS; e += NT) {
+        int n = 1;
+        while (sofs(n + 1) <= e) n++;
+        tabS[e] = make_short2((short)n, (short)(e - sofs(n)));
+    }
+    for (int e = tid; e < NQ; e += NT) {
+        int n = 1;
+        while (tofs(n + 1) <= e) n++;
+        tabQ[e] = make_short2((short)n, (short)(e - tofs(n) + 1));
+    }
+    if (tid == 0) {
+        int e = 0;
+        for (int m = 0; m <= L; m++) {
+            int m1 = m < 1 ? 1 : m;
+            int nq = (m == 0) ? 1 : 2;
+            int zo = 2 + RS + 2 * op_z_offset(m, L, L);
+            for (int q = 0; q < nq; q++)
+                for (int line = m1; line <= L; line++) tabZ[e++] = make_short4((short)m, (short)q, (short)line, (short)zo);
+        }
+    }
+    for (int e = tid; e < NSLOT * NR * NB; e += NT) ACC[e] = mk((T)0, (T)0);
+    if (tid == 0) {
+        mb_init(&bar[0], 1);
+        mb_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int G = gridDim.x;
+    int tcur = blockIdx.x;
+    if (tcur >= a.ntiles) return;
+    // prefetch iterator (thread 0)
+    int pf_t = tcur, pf_q = a.tiles[tcur].x;
+    bool pf_ok = true;
+    auto pf_adv = [&]() {
+        pf_q++;
+        if (pf_q >= a.tiles[pf_t].x + a.tiles[pf_t].y) {
+            pf_t += G;
+            if (pf_t >= a.ntiles) { pf_ok = false; return; }
+            pf_q = a.tiles[pf_t].x;
+        }
+    };
+    constexpr uint32_t RECB = (uint32_t)(REC * sizeof(T));
+    if (tid == 0) {
+        for (int b = 0; b < 2 && pf_ok; b++) {
+            mb_expect(&bar[b], RECB);
+            bulk_copy(opb + b * REC, a.ops + (size_t)pf_q * REC, RECB, &bar[b]);
+            pf_adv();
+        }
+    }
+    int q = a.tiles[tcur].x;
+    int t = 0;
+    while (true) {
+        const int4 tinfo = make_int4(a.tiles[tcur].x, a.tiles[tcur].y, a.tiles[tcur].z, a.tiles[tcur].w);
+        const int i0 = tinfo.z >> 16, j0 = tinfo.z & 0xffff;   // block starts
+        const int diag = tinfo.w;
+        const int b = t & 1;
+        if (!mb_wait(&bar[b], (t >> 1) & 1)) {
+            if (tid == 0) atomicExch(a.err, MSTMG_ERR_CUDA);
+            mb_wait(&bar[b ^ 1], ((t + 1) >> 1) & 1);
+            return;
+        }
+        const T* rec = opb + b * REC;
+        const int2 pr = a.pairs[q];
+        const int pi = pr.x, pj = pr.y;
+        const int si = pi - i0;
+        const int sj = diag ? (pj - i0) : (B + pj - j0);
+        if (tid == 0) {
+            cpx<T> ep = mk(rec[0], rec[1]);
+            cpx<T>* e = ephm + L;
+            e[0] = mk((T)1, (T)0);
+#pragma unroll
+            for (int m = 1; m <= L; m++) {
+                e[m] = ep * e[m - 1];
+                e[-m] = cj(e[m]);
+            }
+        }
+        __syncthreads();
+        const cpx<T>* e = ephm + L;
+
+        // ---- A: shift, phase, even/odd split ----
+        for (int idx = tid; idx < C * NS; idx += NT) {
+            const int c = idx / NS, jj = idx - c * NS;
+            const short2 nm = tabS[jj];
+            const int n = nm.x, m = nm.y;
+            const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
+            const int src = dir ? pi : pj;
+            const bool swp = (dir != (int)((a.contran >> r) & 1u));
+            const cpx<T>* xs = a.x + (size_t)r * a.ld + (size_t)src * NB + p * NB2;
+            cpx<T>* st = W1 + c * NB2;
+            cpx<T> u = xs[hidx<L>(m, n)];
+            if (m == 0) {
+                st[sofs(n)] = (T)2 * u;
+            } else {
+                cpx<T> v = xs[hidx<L>(-m, n)];
+                const T sg = (m & 1) ? (T)-1 : (T)1;
+                if (swp) { cpx<T> tt = u; u = sg * v; v = sg * tt; }
+                const int im = dir ? -m : m;
+                cpx<T> uu = u * e[im], vv = v * e[-im];
+                st[sofs(n) + m] = uu + sg * vv;
+                st[NS + tofs(n) + m - 1] = uu - sg * vv;
+            }
+        }
+        __syncthreads();
+
+        // ---- B: forward rotation, P = E s (rows k=0..n), Q = O t (rows k=1..n) ----
+        for (int idx = tid; idx < NB2 * NG; idx += NT) {
+            const int row = idx / NG, g = idx - row * NG;
+            const T* mrow;
+            int n, k, soff, doff, base, m0;
+            if (row < NS) {
+                short2 nk = tabS[row];
+                n = nk.x; k = nk.y;
+                mrow = rec + 2 + op_rot_offset(n, L) + k * (n + 1);   // E_n[k][0..n]
+                soff = sofs(n); doff = sofs(n) + k; m0 = 0; base = 0;
+            } else {
+                short2 nk = tabQ[row - NS];
+                n = nk.x; k = nk.y;
+                mrow = rec + 2 + op_rot_offset(n, L) + (n + 1) * (n + 1) + (k - 1) * n;   // O_n[k][1..n]
+                soff = NS + tofs(n); doff = NS + tofs(n) + k - 1; m0 = 1; base = 1;
+            }
+            const int len = n + 1 - m0;
+            T rv[L + 1];
+#pragma unroll
+            for (int mm = 0; mm <= L; mm++) rv[mm] = (mm < len) ? mrow[mm] : (T)0;
+            (void)base;
+#pragma unroll
+            for (int cc = 0; cc < CB; cc++) {
+                const int c = g * CB + cc;
+                const cpx<T>* sv = W1 + c * NB2 + soff;
+                cpx<T> acc = mk((T)0, (T)0);
+#pragma unroll
+                for (int mm = 0; mm <= L; mm++)
+                    if (mm < len) acc = acc + rv[mm] * sv[mm];
+                W2[c * NB2 + doff] = acc;
+            }
+        }
+        __syncthreads();
+
+        // ---- C: axial translation per degree m (Z row for j->i, Z column for i->j) ----
+        for (int idx = tid; idx < 2 * NB2; idx += NT) {
+            const int dir = idx >= NB2 ? 1 : 0;
+            const short4 zi = tabZ[idx - dir * NB2];
+            const int m = zi.x, qz = zi.y, line = zi.z;
+            const int m1 = m < 1 ? 1 : m;
+            const int dim = L - m1 + 1;
+            const T* zb = rec + zi.w + 2 * qz * dim * dim;
+            cpx<T> zv[L];
+#pragma unroll
+            for (int u = 0; u < L; u++) {
+                if (u < dim) {
+                    const T* zz = dir ? (zb + 2 * (u * dim + (line - m1))) : (zb + 2 * ((line - m1) * dim + u));
+                    zv[u] = mk(zz[0], zz[1]);
+                } else {
+                    zv[u] = mk((T)0, (T)0);
+                }
+            }
+            const int nout = 2;   // (m=0: p=0,1) or (+m: p=q ; -m: p=1-q)
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+#pragma unroll
+                for (int o = 0; o < nout; o++) {
+                    int p, sgnm;
+                    if (m == 0) { p = o; sgnm = 1; }
+                    else if (o == 0) { p = qz; sgnm = 1; }
+                    else { p = 1 - qz; sgnm = -1; }
+                    const int c = ((dir * NR) + r) * 2 + p;
+                    const cpx<T>* P = W2 + c * NB2;
+                    const cpx<T>* Q = W2 + c * NB2 + NS;
+                    const T sgm = (sgnm < 0 && (m & 1)) ? (T)-1 : (T)1;
+                    cpx<T> acc = mk((T)0, (T)0);
+#pragma unroll
+                    for (int u = 0; u < L; u++) {
+                        if (u < dim) {
+                            const int l = m1 + u;
+                            cpx<T> av;
+                            if (m == 0) av = P[sofs(l)];
+                            else {
+                                cpx<T> pp = P[sofs(l) + m], qq = Q[tofs(l) + m - 1];
+                                av = (sgnm > 0) ? (pp + qq) : (sgm * (pp - qq));
+                            }
+                            acc = acc + zv[u] * av;
+                        }
+                    }
+                    W1[c * NB2 + hidx<L>(sgnm * m, line)] = acc;
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- D: back rotation, phase, shift, accumulate into the tile's smem outputs ----
+        for (int idx = tid; idx < NS * NG; idx += NT) {
+            const int jj = idx / NG, g = idx - jj * NG;
+            const short2 nk = tabS[jj];
+            const int n = nk.x, k = nk.y;
+            const T* E = rec + 2 + op_rot_offset(n, L);
+            const T* O = E + (n + 1) * (n + 1);
+            T ec[L + 1], oc[L + 1];
+#pragma unroll
+            for (int mm = 0; mm <= L; mm++) {
+                ec[mm] = (mm <= n) ? E[mm * (n + 1) + k] : (T)0;
+                oc[mm] = (mm >= 1 && mm <= n && k >= 1) ? O[(mm - 1) * n + (k - 1)] : (T)0;
+            }
+#pragma unroll
+            for (int cc = 0; cc < CB; cc++) {
+                const int c = g * CB + cc;
+                const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
+                const cpx<T>* gv = W1 + c * NB2;
+                cpx<T> P = gv[hidx<L>(0, n)] * ec[0];
+                cpx<T> Q = mk((T)0, (T)0);
+#pragma unroll
+                for (int mm = 1; mm <= L; mm++) {
+                    if (mm <= n) {
+                        const T sg = (mm & 1) ? (T)-1 : (T)1;
+                        cpx<T> gp = gv[hidx<L>(mm, n)], gm = sg * gv[hidx<L>(-mm, n)];
+                        P = P + ec[mm] * (gp + gm);
+                        Q = Q + oc[mm] * (gp - gm);
+                    }
+                }
+                const int slot = dir ? sj : si;
+                cpx<T>* acc = ACC + (slot * NR + r) * NB + p * NB2;
+                if (k == 0) {
+                    cpx<T> v = (T)2 * P;
+                    acc[hidx<L>(0, n)] = acc[hidx<L>(0, n)] + v;
+                } else {
+                    const T sk = (k & 1) ? (T)-1 : (T)1;
+                    const int im = dir ? -k : k;
+                    cpx<T> outk = (P + Q) * e[-im];
+                    cpx<T> outmk = (sk * (P - Q)) * e[im];
+                    const bool swp = (dir != (int)((a.contran >> r) & 1u));
+                    if (swp) { cpx<T> tt = outk; outk = sk * outmk; outmk = sk * tt; }
+                    acc[hidx<L>(k, n)] = acc[hidx<L>(k, n)] + outk;
+                    acc[hidx<L>(-k, n)] = acc[hidx<L>(-k, n)] + outmk;
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- refill this buffer with the pair after next ----
+        if (tid == 0 && pf_ok) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mb_expect(&bar[b], RECB);
+            bulk_copy(opb + b * REC, a.ops + (size_t)pf_q * REC, RECB, &bar[b]);
+            pf_adv();
+        }
+        // ---- end of tile: flush the tile's outputs ----
+        const bool last = (q + 1 == tinfo.x + tinfo.y);
+        if (last) {
+            for (int idx = tid; idx < NSLOT * NR * NB; idx += NT) {
+                const int slot = idx / (NR * NB);
+                const int rem = idx - slot * (NR * NB);
+                const int r = rem / NB, el = rem - r * NB;
+                int sph = (slot < B) ? (i0 + slot) : (diag ? -1 : (j0 + slot - B));
+                if (sph >= 0 && sph < a.nsph && !(diag && slot >= B)) {
+                    cpx<T> v = ACC[idx];
+                    if (v.x != (T)0 || v.y != (T)0) red_add<T>(a.y + (size_t)r * a.ld + (size_t)sph * NB + el, v);
+                }
+                ACC[idx] = mk((T)0, (T)0);
+            }
+            __syncthreads();
+            tcur += G;
+            if (tcur >= a.ntiles) break;
+            q = a.tiles[tcur].x;
+        } else {
+            q++;
+        }
+        t++;
+    }
+}
+
+template <typename T, int L, int NR, int B> static size_t tiled_smem()
+{
+    constexpr int NS = L * (L + 3) / 2, NQ = L * (L + 1) / 2, NB2 = L * (L + 2), NB = 2 * NB2, C = 4 * NR;
+    size_t off = 64 + sizeof(short2) * (NS + NQ + 1) + sizeof(short4) * NB2;
+    off = (off + 127) & ~(size_t)127;
+    off += sizeof(cpx<T>) * (2 * L + 1);
+    off = (off + 127) & ~(size_t)127;
+    off += sizeof(T) * 2 * op_record_units(L, L);
+    off = (off + 127) & ~(size_t)127;
+    off += sizeof(cpx<T>) * ((size_t)2 * C * NB2 + (size_t)2 * B * NR * NB);
+    return off;
+}
+
+template <typename T, int L, int NR, int B> static int launch_one(const TiledArgs<T>& a, int nsm, cudaStream_t st)
+{
+    size_t smem = tiled_smem<T, L, NR, B>();
+    if (smem > 227 * 1024) return -1;
+    auto kern = translate_tiled_kernel<T, L, NR, B>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = (int)((228 * 1024) / (smem + 1024));
+    if (per_sm < 1) per_sm = 1;
+    if (per_sm > 2) per_sm = 2;
+    int blocks = nsm * per_sm;
+    if (blocks > a.ntiles) blocks = a.ntiles;
+    if (blocks < 1) return 0;
+    kern<<<blocks, 256, smem, st>>>(a);
+    launch_counter() += 1;
+    return 0;
+}
+
+template <typename T, int L> static int launch_L(const TiledArgs<T>& a, int nsm, cudaStream_t st)
+{
+    switch (a.nrhs) {
+    case 1: return launch_one<T, L, 1, TILE_B>(a, nsm, st);
+    case 2: return launch_one<T, L, 2, TILE_B>(a, nsm, st);
+    case 4:
+        if constexpr (sizeof(T) == 8) return -1;   // FP64 with four columns: the generic kernel
+        else return launch_one<T, L, 4, TILE_B>(a, nsm, st);
+    default: return -1;
+    }
+}
+
+template <typename T> int launch_translate_tiled(const TiledArgs<T>& a, int L, int nsm, cudaStream_t st)
+{
+    switch (L) {
+    case 5: return launch_L<T, 5>(a, nsm, st);
+    case 6: return launch_L<T, 6>(a, nsm, st);
+    case 7: return launch_L<T, 7>(a, nsm, st);
+    case 8: return launch_L<T, 8>(a, nsm, st);
+    case 9: return launch_L<T, 9>(a, nsm, st);
+    case 10: return launch_L<T, 10>(a, nsm, st);
+    default: return -1;
+    }
+}
+bool tiled_supported(int L, int nrhs) { return L >= 5 && L <= 10 && (nrhs == 1 || nrhs == 2 || nrhs == 4); }
+
+template int launch_translate_tiled<double>(const TiledArgs<double>&, int, int, cudaStream_t);
+template int launch_translate_tiled<float>(const TiledArgs<float>&, int, int, cudaStream_t);

@@ -1,0 +1,20 @@
+// translate_tiled.cuh -- tiled fast path of the pair translation pass.
+#pragma once
+#include "common.cuh"
+
+#define TILE_B 4   // spheres per block: a tile holds the pairs of two blocks
+
+template <typename T> struct TiledArgs {
+    int ntiles;
+    const int4* tiles;       // (pair start, pair count, (i0<<16)|j0, diagonal)
+    const int2* pairs;       // tile-ordered pairs, i < j
+    const T* ops;            // records in pair order, op_record_units(L,L) each
+    const cpx<T>* x;         // ld x nrhs
+    cpx<T>* y;               // ld x nrhs, accumulated
+    int ld, nrhs, nsph;
+    unsigned contran;
+    int* err;
+};
+
+bool tiled_supported(int L, int nrhs);
+template <typename T> int launch_translate_tiled(const TiledArgs<T>& a, int L, int nsm, cudaStream_t st);

@@ -83,6 +83,20 @@ def test_sphereinteraction(api, oracle_mod, name):
             assert np.abs(yg[:, r] - yo[:, r]).max() <= 1e-11 * scale, (name, ct, mm, r)
 
 
+@pytest.mark.parametrize("name,nrhs", [("cluster20", 1), ("fractal60", 2), ("fractal60", 4)])
+def test_tiled_and_generic_kernels_agree(api, name, nrhs):
+    pos, rad, ri, em = _cluster(name)
+    for prec in ("fp64", "mixed"):
+        a = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision=prec)
+        b = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision=prec, generic_kernel=True)
+        rng = np.random.default_rng(3)
+        x = rng.normal(size=(a.number_eqns, nrhs)) + 1j * rng.normal(size=(a.number_eqns, nrhs))
+        ct = [r % 2 for r in range(nrhs)]
+        ya = a.sphereinteraction(x, con_tran=ct, initial_run=True)
+        yb = b.sphereinteraction(x, con_tran=ct, initial_run=True)
+        assert np.abs(ya - yb).max() <= 1e-11 * np.abs(yb).max()
+
+
 def test_cbicg_same_iterations(api, oracle_mod):
     pos, rad, ri, em = _cluster("cluster20")
     g, o = _pair(api, oracle_mod, pos, rad, ri, em)
