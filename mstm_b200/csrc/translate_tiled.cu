@@ -81,47 +81,45 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR;            // columns: ((dir*NR)+r)*2+p
-    constexpr int CB = 4;                // columns per item
+    constexpr int CB = 4;                // columns per item in the rotations
     constexpr int NG = C / CB;
-    constexpr int NS = L * (L + 3) / 2;
+    constexpr int NS = L * (L + 3) / 2;  // (n, k>=0) rows
     constexpr int NQ = L * (L + 1) / 2;
-    constexpr int NB2 = L * (L + 2);     // NS + NQ
+    constexpr int NB2 = L * (L + 2);     // NS + NQ: one mode of a sphere block
     constexpr int NB = 2 * NB2;
     constexpr int REC = op_record_units(L, L);
     constexpr int RS = op_rot_size(L, L);
     constexpr int NSLOT = 2 * B;
+    constexpr uint32_t RECB = (uint32_t)(REC * sizeof(T));
+    constexpr uint32_t XB = (uint32_t)(NB * sizeof(cpx<T>));   // one sphere block of one rhs
 
     extern __shared__ __align__(128) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
-    short2* tabS = reinterpret_cast<short2*>(sm + 64);                     // NS entries: (n, m)
-    short2* tabQ = tabS + NS;                                               // NQ entries: (n, m>=1)
-    short4* tabZ = reinterpret_cast<short4*>(tabQ + NQ + (((NS + NQ) & 1) ? 1 : 0));   // NB2 entries: (m, q, line, zoff)
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm);          // [0],[1] operators, [2] sources
+    short2* tabS = reinterpret_cast<short2*>(sm + 64);        // NS entries (n, k), n descending
+    short2* tabQ = tabS + NS;                                  // NQ entries (n, m>=1)
+    short4* tabZ = reinterpret_cast<short4*>(tabQ + NQ + (((NS + NQ) & 1) ? 1 : 0));   // NB2 entries (m, q, line, zoff)
     size_t off = 64 + sizeof(short2) * (NS + NQ + 1) + sizeof(short4) * NB2;
     off = (off + 127) & ~(size_t)127;
-    cpx<T>* ephm = reinterpret_cast<cpx<T>*>(sm + off);                     // 2L+1
+    cpx<T>* ephm = reinterpret_cast<cpx<T>*>(sm + off);       // 2L+1
     off += sizeof(cpx<T>) * (2 * L + 1);
     off = (off + 127) & ~(size_t)127;
-    T* opb = reinterpret_cast<T*>(sm + off);                                // 2 x REC
+    T* opb = reinterpret_cast<T*>(sm + off);                  // 2 x REC
     off += sizeof(T) * 2 * REC;
     off = (off + 127) & ~(size_t)127;
-    cpx<T>* W1 = reinterpret_cast<cpx<T>*>(sm + off);                       // C x NB2: S/T, then G
-    cpx<T>* W2 = W1 + C * NB2;                                              // C x NB2: P/Q
-    cpx<T>* ACC = W2 + C * NB2;                                             // NSLOT x NR x NB
+    cpx<T>* W1 = reinterpret_cast<cpx<T>*>(sm + off);         // C x NB2: S/T, then g
+    cpx<T>* W2 = W1 + C * NB2;                                // C x NB2: sources x (2 spheres x NR x NB), then a'
+    cpx<T>* ACC = W2 + C * NB2;                               // NSLOT x NR x NB
 
     const int tid = threadIdx.x;
-    // ---- one-time tables ----
-    for (int e = tid; e < NS; e += NT) {
-        int n = 1;
-        while (sofs(n + 1) <= e) n++;
-        tabS[e] = make_short2((short)n, (short)(e - sofs(n)));
-    }
-    for (int e = tid; e < NQ; e += NT) {
-        int n = 1;
-        while (tofs(n + 1) <= e) n++;
-        tabQ[e] = make_short2((short)n, (short)(e - tofs(n) + 1));
-    }
     if (tid == 0) {
+        // (n, k) rows with the longest first so the work of a phase spreads evenly
         int e = 0;
+        for (int n = L; n >= 1; n--)
+            for (int k = 0; k <= n; k++) tabS[e++] = make_short2((short)n, (short)k);
+        e = 0;
+        for (int n = 1; n <= L; n++)
+            for (int m = 1; m <= n; m++) tabQ[e++] = make_short2((short)n, (short)m);
+        e = 0;
         for (int m = 0; m <= L; m++) {
             int m1 = m < 1 ? 1 : m;
             int nq = (m == 0) ? 1 : 2;
@@ -134,6 +132,7 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
     if (tid == 0) {
         mb_init(&bar[0], 1);
         mb_init(&bar[1], 1);
+        mb_init(&bar[2], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -141,7 +140,7 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
     const int G = gridDim.x;
     int tcur = blockIdx.x;
     if (tcur >= a.ntiles) return;
-    // prefetch iterator (thread 0)
+    // thread 0's iterators: operators two pairs ahead, sources one pair ahead
     int pf_t = tcur, pf_q = a.tiles[tcur].x;
     bool pf_ok = true;
     auto pf_adv = [&]() {
@@ -152,8 +151,16 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
             pf_q = a.tiles[pf_t].x;
         }
     };
-    constexpr uint32_t RECB = (uint32_t)(REC * sizeof(T));
+    auto load_sources = [&](int qq) {
+        const int2 pr = a.pairs[qq];
+        mb_expect(&bar[2], 2u * NR * XB);
+        for (int r = 0; r < NR; r++) {
+            bulk_copy(W2 + (size_t)(0 * NR + r) * NB, a.x + (size_t)r * a.ld + (size_t)pr.y * NB, XB, &bar[2]);   // source of j -> i
+            bulk_copy(W2 + (size_t)(1 * NR + r) * NB, a.x + (size_t)r * a.ld + (size_t)pr.x * NB, XB, &bar[2]);   // source of i -> j
+        }
+    };
     if (tid == 0) {
+        load_sources(pf_q);
         for (int b = 0; b < 2 && pf_ok; b++) {
             mb_expect(&bar[b], RECB);
             bulk_copy(opb + b * REC, a.ops + (size_t)pf_q * REC, RECB, &bar[b]);
@@ -163,20 +170,20 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
     int q = a.tiles[tcur].x;
     int t = 0;
     while (true) {
-        const int4 tinfo = make_int4(a.tiles[tcur].x, a.tiles[tcur].y, a.tiles[tcur].z, a.tiles[tcur].w);
+        const int4 tinfo = a.tiles[tcur];
         const int i0 = tinfo.z >> 16, j0 = tinfo.z & 0xffff;   // block starts
         const int diag = tinfo.w;
         const int b = t & 1;
-        if (!mb_wait(&bar[b], (t >> 1) & 1)) {
+        if (!mb_wait(&bar[b], (t >> 1) & 1) || !mb_wait(&bar[2], t & 1)) {
             if (tid == 0) atomicExch(a.err, MSTMG_ERR_CUDA);
             mb_wait(&bar[b ^ 1], ((t + 1) >> 1) & 1);
+            mb_wait(&bar[2], t & 1);
             return;
         }
         const T* rec = opb + b * REC;
         const int2 pr = a.pairs[q];
-        const int pi = pr.x, pj = pr.y;
-        const int si = pi - i0;
-        const int sj = diag ? (pj - i0) : (B + pj - j0);
+        const int si = pr.x - i0;
+        const int sj = diag ? (pr.y - i0) : (B + pr.y - j0);
         if (tid == 0) {
             cpx<T> ep = mk(rec[0], rec[1]);
             cpx<T>* e = ephm + L;
@@ -190,15 +197,14 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
         __syncthreads();
         const cpx<T>* e = ephm + L;
 
-        // ---- A: shift, phase, even/odd split ----
+        // ---- A: shift, phase, even/odd split of the staged sources ----
         for (int idx = tid; idx < C * NS; idx += NT) {
             const int c = idx / NS, jj = idx - c * NS;
             const short2 nm = tabS[jj];
             const int n = nm.x, m = nm.y;
             const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
-            const int src = dir ? pi : pj;
             const bool swp = (dir != (int)((a.contran >> r) & 1u));
-            const cpx<T>* xs = a.x + (size_t)r * a.ld + (size_t)src * NB + p * NB2;
+            const cpx<T>* xs = W2 + (size_t)(dir * NR + r) * NB + p * NB2;
             cpx<T>* st = W1 + c * NB2;
             cpx<T> u = xs[hidx<L>(m, n)];
             if (m == 0) {
@@ -215,90 +221,85 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
         }
         __syncthreads();
 
-        // ---- B: forward rotation, P = E s (rows k=0..n), Q = O t (rows k=1..n) ----
-        for (int idx = tid; idx < NB2 * NG; idx += NT) {
-            const int row = idx / NG, g = idx - row * NG;
-            const T* mrow;
-            int n, k, soff, doff, base, m0;
-            if (row < NS) {
-                short2 nk = tabS[row];
-                n = nk.x; k = nk.y;
-                mrow = rec + 2 + op_rot_offset(n, L) + k * (n + 1);   // E_n[k][0..n]
-                soff = sofs(n); doff = sofs(n) + k; m0 = 0; base = 0;
-            } else {
-                short2 nk = tabQ[row - NS];
-                n = nk.x; k = nk.y;
-                mrow = rec + 2 + op_rot_offset(n, L) + (n + 1) * (n + 1) + (k - 1) * n;   // O_n[k][1..n]
-                soff = NS + tofs(n); doff = NS + tofs(n) + k - 1; m0 = 1; base = 1;
-            }
-            const int len = n + 1 - m0;
-            T rv[L + 1];
+        // ---- B: forward rotation: a'(k) = P+Q, a'(-k) = (-1)^k (P-Q),
+        //      P = E_n[k][:] s, Q = O_n[k][:] t ----
+        for (int idx = tid; idx < NS * NG; idx += NT) {
+            const int jj = idx / NG, g = idx - jj * NG;
+            const short2 nk = tabS[jj];
+            const int n = nk.x, k = nk.y;
+            const T* Er = rec + 2 + op_rot_offset(n, L) + k * (n + 1);
+            const T* Or = rec + 2 + op_rot_offset(n, L) + (n + 1) * (n + 1) + (k - 1) * n;
+            T er[L + 1], orr[L];
 #pragma unroll
-            for (int mm = 0; mm <= L; mm++) rv[mm] = (mm < len) ? mrow[mm] : (T)0;
-            (void)base;
+            for (int mm = 0; mm <= L; mm++) er[mm] = (mm <= n) ? Er[mm] : (T)0;
+#pragma unroll
+            for (int mm = 0; mm < L; mm++) orr[mm] = (k >= 1 && mm < n) ? Or[mm] : (T)0;
 #pragma unroll
             for (int cc = 0; cc < CB; cc++) {
                 const int c = g * CB + cc;
-                const cpx<T>* sv = W1 + c * NB2 + soff;
-                cpx<T> acc = mk((T)0, (T)0);
+                const cpx<T>* sv = W1 + c * NB2 + sofs(n);
+                const cpx<T>* tv = W1 + c * NB2 + NS + tofs(n);
+                cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
 #pragma unroll
                 for (int mm = 0; mm <= L; mm++)
-                    if (mm < len) acc = acc + rv[mm] * sv[mm];
-                W2[c * NB2 + doff] = acc;
+                    if (mm <= n) P = P + er[mm] * sv[mm];
+#pragma unroll
+                for (int mm = 0; mm < L; mm++)
+                    if (mm < n) Q = Q + orr[mm] * tv[mm];
+                cpx<T>* ap = W2 + c * NB2;
+                if (k == 0) {
+                    ap[hidx<L>(0, n)] = P;
+                } else {
+                    const T sk = (k & 1) ? (T)-1 : (T)1;
+                    ap[hidx<L>(k, n)] = P + Q;
+                    ap[hidx<L>(-k, n)] = sk * (P - Q);
+                }
             }
         }
         __syncthreads();
 
-        // ---- C: axial translation per degree m (Z row for j->i, Z column for i->j) ----
-        for (int idx = tid; idx < 2 * NB2; idx += NT) {
-            const int dir = idx >= NB2 ? 1 : 0;
-            const short4 zi = tabZ[idx - dir * NB2];
+        // ---- C: axial translation per degree m; one item = one Z row (j -> i)
+        //      or column (i -> j) applied to the two columns that use it ----
+        for (int idx = tid; idx < NB2 * 2 * NR; idx += NT) {
+            const int zr = idx / (2 * NR), dr = idx - zr * (2 * NR);
+            const int dir = dr / NR, r = dr - dir * NR;
+            const short4 zi = tabZ[zr];
             const int m = zi.x, qz = zi.y, line = zi.z;
             const int m1 = m < 1 ? 1 : m;
             const int dim = L - m1 + 1;
-            const T* zb = rec + zi.w + 2 * qz * dim * dim;
-            cpx<T> zv[L];
-#pragma unroll
-            for (int u = 0; u < L; u++) {
-                if (u < dim) {
-                    const T* zz = dir ? (zb + 2 * (u * dim + (line - m1))) : (zb + 2 * ((line - m1) * dim + u));
-                    zv[u] = mk(zz[0], zz[1]);
-                } else {
-                    zv[u] = mk((T)0, (T)0);
-                }
+            const T* zb = rec + zi.w + 2 * qz * dim * dim + (dir ? 2 * (line - m1) : 2 * (line - m1) * dim);
+            const int zs = dir ? 2 * dim : 2;
+            int p0, p1, m0s, m1s;
+            if (m == 0) { p0 = 0; p1 = 1; m0s = 0; m1s = 0; }
+            else { p0 = qz; p1 = 1 - qz; m0s = m; m1s = -m; }
+            const cpx<T>* a0 = W2 + (((dir * NR) + r) * 2 + p0) * NB2;
+            const cpx<T>* a1 = W2 + (((dir * NR) + r) * 2 + p1) * NB2;
+            cpx<T> g0 = mk((T)0, (T)0), g1 = mk((T)0, (T)0);
+            for (int u = 0; u < dim; u++) {
+                const cpx<T> z = mk(zb[u * zs], zb[u * zs + 1]);
+                const int l = m1 + u;
+                g0 = g0 + z * a0[hidx<L>(m0s, l)];
+                g1 = g1 + z * a1[hidx<L>(m1s, l)];
             }
-            const int nout = 2;   // (m=0: p=0,1) or (+m: p=q ; -m: p=1-q)
-#pragma unroll
-            for (int r = 0; r < NR; r++) {
-#pragma unroll
-                for (int o = 0; o < nout; o++) {
-                    int p, sgnm;
-                    if (m == 0) { p = o; sgnm = 1; }
-                    else if (o == 0) { p = qz; sgnm = 1; }
-                    else { p = 1 - qz; sgnm = -1; }
-                    const int c = ((dir * NR) + r) * 2 + p;
-                    const cpx<T>* P = W2 + c * NB2;
-                    const cpx<T>* Q = W2 + c * NB2 + NS;
-                    const T sgm = (sgnm < 0 && (m & 1)) ? (T)-1 : (T)1;
-                    cpx<T> acc = mk((T)0, (T)0);
-#pragma unroll
-                    for (int u = 0; u < L; u++) {
-                        if (u < dim) {
-                            const int l = m1 + u;
-                            cpx<T> av;
-                            if (m == 0) av = P[sofs(l)];
-                            else {
-                                cpx<T> pp = P[sofs(l) + m], qq = Q[tofs(l) + m - 1];
-                                av = (sgnm > 0) ? (pp + qq) : (sgm * (pp - qq));
-                            }
-                            acc = acc + zv[u] * av;
-                        }
-                    }
-                    W1[c * NB2 + hidx<L>(sgnm * m, line)] = acc;
-                }
-            }
+            W1[(((dir * NR) + r) * 2 + p0) * NB2 + hidx<L>(m0s, line)] = g0;
+            W1[(((dir * NR) + r) * 2 + p1) * NB2 + hidx<L>(m1s, line)] = g1;
         }
         __syncthreads();
+
+        // ---- the next pair's sources stream into W2 while D runs ----
+        if (tid == 0) {
+            int nq = q + 1;
+            bool have = true;
+            if (nq >= tinfo.x + tinfo.y) {
+                int nt = tcur + G;
+                if (nt < a.ntiles) nq = a.tiles[nt].x;
+                else have = false;
+            }
+            if (have) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                load_sources(nq);
+            }
+        }
 
         // ---- D: back rotation, phase, shift, accumulate into the tile's smem outputs ----
         for (int idx = tid; idx < NS * NG; idx += NT) {
@@ -332,8 +333,7 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
                 const int slot = dir ? sj : si;
                 cpx<T>* acc = ACC + (slot * NR + r) * NB + p * NB2;
                 if (k == 0) {
-                    cpx<T> v = (T)2 * P;
-                    acc[hidx<L>(0, n)] = acc[hidx<L>(0, n)] + v;
+                    acc[hidx<L>(0, n)] = acc[hidx<L>(0, n)] + (T)2 * P;
                 } else {
                     const T sk = (k & 1) ? (T)-1 : (T)1;
                     const int im = dir ? -k : k;
@@ -348,24 +348,24 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
         }
         __syncthreads();
 
-        // ---- refill this buffer with the pair after next ----
+        // ---- refill this operator buffer with the pair after next ----
         if (tid == 0 && pf_ok) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mb_expect(&bar[b], RECB);
             bulk_copy(opb + b * REC, a.ops + (size_t)pf_q * REC, RECB, &bar[b]);
             pf_adv();
         }
-        // ---- end of tile: flush the tile's outputs ----
+        // ---- end of tile: flush the tile's outputs with coalesced atomics ----
         const bool last = (q + 1 == tinfo.x + tinfo.y);
         if (last) {
             for (int idx = tid; idx < NSLOT * NR * NB; idx += NT) {
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int r = rem / NB, el = rem - r * NB;
-                int sph = (slot < B) ? (i0 + slot) : (diag ? -1 : (j0 + slot - B));
-                if (sph >= 0 && sph < a.nsph && !(diag && slot >= B)) {
+                const int sph = (slot < B) ? (i0 + slot) : (j0 + slot - B);
+                if (!(diag && slot >= B) && sph < a.nsph) {
                     cpx<T> v = ACC[idx];
-                    if (v.x != (T)0 || v.y != (T)0) red_add<T>(a.y + (size_t)r * a.ld + (size_t)sph * NB + el, v);
+                    red_add<T>(a.y + (size_t)r * a.ld + (size_t)sph * NB + el, v);
                 }
                 ACC[idx] = mk((T)0, (T)0);
             }
