@@ -90,7 +90,7 @@ template <int N, int L, typename F> __device__ __forceinline__ void with_n(int n
 }  // namespace
 
 template <typename T, int L, int NR, int B>
-__global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1)) translate_tiled_kernel(TiledArgs<T> a)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR;            // columns: ((dir*NR)+r)*2+p
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
 #pragma unroll
                     for (int mm = 0; mm < N; mm++) orr[mm] = Or[mm];
                 }
-#pragma unroll
+#pragma unroll 1
                 for (int cc = 0; cc < CB; cc++) {
                     const int c = g * CB + cc;
                     const cpx<T>* sv = W1 + c * NB2 + sofs(N);
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
                 if (m == 0) {
                     // Z_0 is shared by both modes
                     cpx<T> g0 = mk((T)0, (T)0), g1 = mk((T)0, (T)0);
-#pragma unroll
+#pragma unroll 3
                     for (int u = 0; u < D; u++) {
                         const cpx<T> z = mk(z0[u * zst], z0[u * zst + 1]);
                         const int h = hidx<L>(0, 1 + u);
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
                     // mode p: +m uses Z_m[p], -m uses Z_m[1-p]
                     cpx<T> gp0 = mk((T)0, (T)0), gm0 = gp0, gp1 = gp0, gm1 = gp0;
                     const int hp0 = hidx<L>(m, m1), hm0 = hidx<L>(-m, m1);
-#pragma unroll
+#pragma unroll 3
                     for (int u = 0; u < D; u++) {
                         const cpx<T> za = mk(z0[u * zst], z0[u * zst + 1]);
                         const cpx<T> zb = mk(z1[u * zst], z1[u * zst + 1]);
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
 #pragma unroll
                     for (int mm = 0; mm < N; mm++) oc[mm] = O[mm * N + (k - 1)];
                 }
-#pragma unroll
+#pragma unroll 1
                 for (int cc = 0; cc < CB; cc++) {
                     const int c = g * CB + cc;
                     const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
