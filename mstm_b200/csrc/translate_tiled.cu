@@ -23,7 +23,6 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "translate_tiled.cuh"
-#include <type_traits>
 
 namespace {
 
@@ -75,22 +74,10 @@ __host__ __device__ constexpr int tofs(int n) { return (n - 1) * n / 2; }       
 // half-block (one mode) slot of degree m, order n: MSTM's a(0:L+1,1:L) index
 template <int L> __host__ __device__ constexpr int hidx(int m, int n) { return m >= 0 ? m + (L + 2) * (n - 1) : (n + 1) + (L + 2) * (-m - 1); }
 
-// Call f(integral_constant<N>) for the runtime value n in [N, L].
-template <int N, int L, typename F> __device__ __forceinline__ void with_n(int n, F&& f)
-{
-    if constexpr (N <= L) {
-        if (n == N) {
-            f(std::integral_constant<int, N>{});
-            return;
-        }
-        with_n<N + 1, L>(n, f);
-    }
-}
-
 }  // namespace
 
 template <typename T, int L, int NR, int B>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1)) translate_tiled_kernel(TiledArgs<T> a)
+__global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR;            // columns: ((dir*NR)+r)*2+p
@@ -105,14 +92,13 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1)) translate_tiled
     constexpr int NSLOT = 2 * B;
     constexpr uint32_t RECB = (uint32_t)(REC * sizeof(T));
     constexpr uint32_t XB = (uint32_t)(NB * sizeof(cpx<T>));   // one sphere block of one rhs
-    constexpr int NCI = NS;              // (m, line) items of the axial phase: m = 0..L, line = max(1,m)..L
 
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm);          // [0],[1] operators, [2] sources
     short2* tabS = reinterpret_cast<short2*>(sm + 64);        // NS entries (n, k), n descending
     short2* tabQ = tabS + NS;                                  // NQ entries (n, m>=1)
-    short2* tabC = tabQ + NQ;                                  // NCI entries (m, line)
-    size_t off = 64 + sizeof(short2) * (NS + NQ + NCI);
+    short2* tabC = tabQ + NQ;                                  // NS entries (m, line), m = 0..L, line = max(1,m)..L
+    size_t off = 64 + sizeof(short2) * (NS + NQ + NS);
     off = (off + 127) & ~(size_t)127;
     cpx<T>* ephm = reinterpret_cast<cpx<T>*>(sm + off);       // 2L+1
     off += sizeof(cpx<T>) * (2 * L + 1);
@@ -208,136 +194,115 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1)) translate_tiled
         __syncthreads();
         const cpx<T>* e = ephm + L;
 
-        // ---- A: shift, phase, even/odd split of the staged sources; one item
-        //      = one (direction, n, m) for all right-hand sides and modes ----
-        for (int idx = tid; idx < 2 * NS; idx += NT) {
-            const int dir = idx >= NS ? 1 : 0;
-            const short2 nm = tabS[idx - dir * NS];
+        // ---- A: shift, phase, even/odd split of the staged sources ----
+        for (int idx = tid; idx < C * NS; idx += NT) {
+            const int c = idx / NS, jj = idx - c * NS;
+            const short2 nm = tabS[jj];
             const int n = nm.x, m = nm.y;
-            const int im = dir ? -m : m;
-            const cpx<T> ep = e[im], emn = e[-im];
-            const T sg = (m & 1) ? (T)-1 : (T)1;
-            const int hp = hidx<L>(m, n), hm = hidx<L>(-m, n);
-            const int so = sofs(n) + m, to = NS + tofs(n) + m - 1;
-#pragma unroll
-            for (int r = 0; r < NR; r++) {
-                const bool swp = (dir != (int)((a.contran >> r) & 1u));
-#pragma unroll
-                for (int p = 0; p < 2; p++) {
-                    const cpx<T>* xs = W2 + (size_t)(dir * NR + r) * NB + p * NB2;
-                    cpx<T>* st = W1 + (((dir * NR) + r) * 2 + p) * NB2;
-                    cpx<T> u = xs[hp];
-                    if (m == 0) {
-                        st[so] = (T)2 * u;
-                    } else {
-                        cpx<T> v = xs[hm];
-                        if (swp) { cpx<T> tt = u; u = sg * v; v = sg * tt; }
-                        cpx<T> uu = u * ep, vv = v * emn;
-                        st[so] = uu + sg * vv;
-                        st[to] = uu - sg * vv;
-                    }
-                }
+            const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
+            const bool swp = (dir != (int)((a.contran >> r) & 1u));
+            const cpx<T>* xs = W2 + (size_t)(dir * NR + r) * NB + p * NB2;
+            cpx<T>* st = W1 + c * NB2;
+            cpx<T> u = xs[hidx<L>(m, n)];
+            if (m == 0) {
+                st[sofs(n)] = (T)2 * u;
+            } else {
+                cpx<T> v = xs[hidx<L>(-m, n)];
+                const T sg = (m & 1) ? (T)-1 : (T)1;
+                if (swp) { cpx<T> tt = u; u = sg * v; v = sg * tt; }
+                const int im = dir ? -m : m;
+                cpx<T> uu = u * e[im], vv = v * e[-im];
+                st[sofs(n) + m] = uu + sg * vv;
+                st[NS + tofs(n) + m - 1] = uu - sg * vv;
             }
         }
         __syncthreads();
 
         // ---- B: forward rotation: a'(k) = P+Q, a'(-k) = (-1)^k (P-Q),
-        //      P = E_n[k][:] s, Q = O_n[k][:] t  (exact loop lengths per degree) ----
+        //      P = E_n[k][:] s, Q = O_n[k][:] t ----
         for (int idx = tid; idx < NS * NG; idx += NT) {
             const int jj = idx / NG, g = idx - jj * NG;
             const short2 nk = tabS[jj];
-            const int k = nk.y;
-            with_n<1, L>(nk.x, [&](auto NC) {
-                constexpr int N = decltype(NC)::value;
-                const T* Er = rec + 2 + op_rot_offset(N, L) + k * (N + 1);
-                const T* Or = rec + 2 + op_rot_offset(N, L) + (N + 1) * (N + 1) + (k - 1) * N;
-                T er[N + 1], orr[N];
+            const int n = nk.x, k = nk.y;
+            const T* Er = rec + 2 + op_rot_offset(n, L) + k * (n + 1);
+            const T* Or = rec + 2 + op_rot_offset(n, L) + (n + 1) * (n + 1) + (k - 1) * n;
+            T er[L + 1], orr[L];
 #pragma unroll
-                for (int mm = 0; mm <= N; mm++) er[mm] = Er[mm];
-                if (k > 0) {
+            for (int mm = 0; mm <= L; mm++) er[mm] = (mm <= n) ? Er[mm] : (T)0;
 #pragma unroll
-                    for (int mm = 0; mm < N; mm++) orr[mm] = Or[mm];
+            for (int mm = 0; mm < L; mm++) orr[mm] = (k >= 1 && mm < n) ? Or[mm] : (T)0;
+#pragma unroll
+            for (int cc = 0; cc < CB; cc++) {
+                const int c = g * CB + cc;
+                const cpx<T>* sv = W1 + c * NB2 + sofs(n);
+                const cpx<T>* tv = W1 + c * NB2 + NS + tofs(n);
+                cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
+#pragma unroll
+                for (int mm = 0; mm <= L; mm++)
+                    if (mm <= n) P = P + er[mm] * sv[mm];
+#pragma unroll
+                for (int mm = 0; mm < L; mm++)
+                    if (mm < n) Q = Q + orr[mm] * tv[mm];
+                cpx<T>* ap = W2 + c * NB2;
+                if (k == 0) {
+                    ap[hidx<L>(0, n)] = P;
+                } else {
+                    const T sk = (k & 1) ? (T)-1 : (T)1;
+                    ap[hidx<L>(k, n)] = P + Q;
+                    ap[hidx<L>(-k, n)] = sk * (P - Q);
                 }
-#pragma unroll 1
-                for (int cc = 0; cc < CB; cc++) {
-                    const int c = g * CB + cc;
-                    const cpx<T>* sv = W1 + c * NB2 + sofs(N);
-                    const cpx<T>* tv = W1 + c * NB2 + NS + tofs(N);
-                    cpx<T> P = er[0] * sv[0];
-#pragma unroll
-                    for (int mm = 1; mm <= N; mm++) P = P + er[mm] * sv[mm];
-                    cpx<T>* ap = W2 + c * NB2;
-                    if (k == 0) {
-                        ap[hidx<L>(0, N)] = P;
-                    } else {
-                        cpx<T> Q = orr[0] * tv[0];
-#pragma unroll
-                        for (int mm = 1; mm < N; mm++) Q = Q + orr[mm] * tv[mm];
-                        const T sk = (k & 1) ? (T)-1 : (T)1;
-                        ap[hidx<L>(k, N)] = P + Q;
-                        ap[hidx<L>(-k, N)] = sk * (P - Q);
-                    }
-                }
-            });
+            }
         }
         __syncthreads();
 
         // ---- C: axial translation per degree m.  One item = one (m, line,
-        //      direction, rhs) applying rows (j -> i) or columns (i -> j) of
-        //      Z_m[0] and Z_m[1]; it writes the back rotation's inputs
-        //      s'(m) = g(m) + (-1)^m g(-m), t'(m) = g(m) - (-1)^m g(-m)
-        //      (s'(0) = g(0)) into W1 in the packed S/T layout ----
-        for (int idx = tid; idx < NCI * 2 * NR; idx += NT) {
+        //      direction, rhs): rows (j -> i) or columns (i -> j) of Z_m[0] and
+        //      Z_m[1] applied to both modes, written as the back rotation's
+        //      inputs s'(m) = g(m) + (-1)^m g(-m), t'(m) = g(m) - (-1)^m g(-m)
+        //      (s'(0) = g(0)) in the packed S/T layout of W1 ----
+        for (int idx = tid; idx < NS * 2 * NR; idx += NT) {
             const int zr = idx / (2 * NR), dr = idx - zr * (2 * NR);
             const int dir = dr / NR, r = dr - dir * NR;
             const short2 ml = tabC[zr];
             const int m = ml.x, line = ml.y;
             const int m1 = m < 1 ? 1 : m;
-            with_n<1, L>(L - m1 + 1, [&](auto DC) {
-                constexpr int D = decltype(DC)::value;
-                const int zo = 2 + RS + 2 * op_z_offset(m, L, L);
-                const T* z0 = rec + zo + (dir ? 2 * (line - m1) : 2 * (line - m1) * D);
-                const T* z1 = z0 + 2 * D * D;
-                constexpr int zs = 2;
-                const int zst = dir ? 2 * D : zs;
-                const cpx<T>* a0 = W2 + (((dir * NR) + r) * 2 + 0) * NB2;
-                const cpx<T>* a1 = W2 + (((dir * NR) + r) * 2 + 1) * NB2;
-                cpx<T>* o0 = W1 + (((dir * NR) + r) * 2 + 0) * NB2;
-                cpx<T>* o1 = W1 + (((dir * NR) + r) * 2 + 1) * NB2;
-                if (m == 0) {
-                    // Z_0 is shared by both modes
-                    cpx<T> g0 = mk((T)0, (T)0), g1 = mk((T)0, (T)0);
-#pragma unroll 3
-                    for (int u = 0; u < D; u++) {
-                        const cpx<T> z = mk(z0[u * zst], z0[u * zst + 1]);
-                        const int h = hidx<L>(0, 1 + u);
-                        g0 = g0 + z * a0[h];
-                        g1 = g1 + z * a1[h];
-                    }
-                    o0[sofs(line)] = g0;
-                    o1[sofs(line)] = g1;
-                } else {
-                    // mode p: +m uses Z_m[p], -m uses Z_m[1-p]
-                    cpx<T> gp0 = mk((T)0, (T)0), gm0 = gp0, gp1 = gp0, gm1 = gp0;
-                    const int hp0 = hidx<L>(m, m1), hm0 = hidx<L>(-m, m1);
-#pragma unroll 3
-                    for (int u = 0; u < D; u++) {
-                        const cpx<T> za = mk(z0[u * zst], z0[u * zst + 1]);
-                        const cpx<T> zb = mk(z1[u * zst], z1[u * zst + 1]);
-                        const int hp = hp0 + (L + 2) * u, hm = hm0 + u;
-                        gp0 = gp0 + za * a0[hp];
-                        gm0 = gm0 + zb * a0[hm];
-                        gp1 = gp1 + zb * a1[hp];
-                        gm1 = gm1 + za * a1[hm];
-                    }
-                    const T sg = (m & 1) ? (T)-1 : (T)1;
-                    const int so = sofs(line) + m, to = NS + tofs(line) + m - 1;
-                    o0[so] = gp0 + sg * gm0;
-                    o0[to] = gp0 - sg * gm0;
-                    o1[so] = gp1 + sg * gm1;
-                    o1[to] = gp1 - sg * gm1;
+            const int dim = L - m1 + 1;
+            const T* z0 = rec + 2 + RS + 2 * op_z_offset(m, L, L) + (dir ? 2 * (line - m1) : 2 * (line - m1) * dim);
+            const T* z1 = z0 + 2 * dim * dim;
+            const int zst = dir ? 2 * dim : 2;
+            const cpx<T>* a0 = W2 + (((dir * NR) + r) * 2 + 0) * NB2;
+            const cpx<T>* a1 = W2 + (((dir * NR) + r) * 2 + 1) * NB2;
+            cpx<T>* o0 = W1 + (((dir * NR) + r) * 2 + 0) * NB2;
+            cpx<T>* o1 = W1 + (((dir * NR) + r) * 2 + 1) * NB2;
+            if (m == 0) {
+                cpx<T> g0 = mk((T)0, (T)0), g1 = mk((T)0, (T)0);
+                for (int u = 0; u < dim; u++) {
+                    const cpx<T> z = mk(z0[u * zst], z0[u * zst + 1]);
+                    const int h = (L + 2) * u;   // hidx(0, 1+u)
+                    g0 = g0 + z * a0[h];
+                    g1 = g1 + z * a1[h];
                 }
-            });
+                o0[sofs(line)] = g0;
+                o1[sofs(line)] = g1;
+            } else {
+                cpx<T> gp0 = mk((T)0, (T)0), gm0 = gp0, gp1 = gp0, gm1 = gp0;
+                const int hp0 = hidx<L>(m, m1), hm0 = hidx<L>(-m, m1);
+                for (int u = 0; u < dim; u++) {
+                    const cpx<T> za = mk(z0[u * zst], z0[u * zst + 1]);
+                    const cpx<T> zb = mk(z1[u * zst], z1[u * zst + 1]);
+                    const int hp = hp0 + (L + 2) * u, hm = hm0 + u;
+                    gp0 = gp0 + za * a0[hp];   // mode 0, +m: Z_m[0]
+                    gm0 = gm0 + zb * a0[hm];   // mode 0, -m: Z_m[1]
+                    gp1 = gp1 + zb * a1[hp];   // mode 1, +m: Z_m[1]
+                    gm1 = gm1 + za * a1[hm];   // mode 1, -m: Z_m[0]
+                }
+                const T sg = (m & 1) ? (T)-1 : (T)1;
+                const int so = sofs(line) + m, to = NS + tofs(line) + m - 1;
+                o0[so] = gp0 + sg * gm0;
+                o0[to] = gp0 - sg * gm0;
+                o1[so] = gp1 + sg * gm1;
+                o1[to] = gp1 - sg * gm1;
+            }
         }
         __syncthreads();
 
@@ -356,51 +321,47 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1)) translate_tiled
             }
         }
 
-        // ---- D: back rotation  g'(k) = sum_m s'(m) E_n[m][k] (+/-) sum_m t'(m) O_n[m][k],
+        // ---- D: back rotation g'(k) = sum_m s'(m) E_n[m][k] +/- sum_m t'(m) O_n[m][k],
         //      phase, shift, accumulate into the tile's smem outputs ----
         for (int idx = tid; idx < NS * NG; idx += NT) {
             const int jj = idx / NG, g = idx - jj * NG;
             const short2 nk = tabS[jj];
-            const int k = nk.y;
-            with_n<1, L>(nk.x, [&](auto NC) {
-                constexpr int N = decltype(NC)::value;
-                const T* E = rec + 2 + op_rot_offset(N, L);
-                const T* O = E + (N + 1) * (N + 1);
-                T ec[N + 1], oc[N];
+            const int n = nk.x, k = nk.y;
+            const T* E = rec + 2 + op_rot_offset(n, L);
+            const T* O = E + (n + 1) * (n + 1);
+            T ec[L + 1], oc[L];
 #pragma unroll
-                for (int mm = 0; mm <= N; mm++) ec[mm] = E[mm * (N + 1) + k];
-                if (k > 0) {
+            for (int mm = 0; mm <= L; mm++) ec[mm] = (mm <= n) ? E[mm * (n + 1) + k] : (T)0;
 #pragma unroll
-                    for (int mm = 0; mm < N; mm++) oc[mm] = O[mm * N + (k - 1)];
+            for (int mm = 0; mm < L; mm++) oc[mm] = (mm < n && k >= 1) ? O[mm * n + (k - 1)] : (T)0;
+#pragma unroll
+            for (int cc = 0; cc < CB; cc++) {
+                const int c = g * CB + cc;
+                const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
+                const cpx<T>* sv = W1 + c * NB2 + sofs(n);
+                const cpx<T>* tv = W1 + c * NB2 + NS + tofs(n);
+                cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
+#pragma unroll
+                for (int mm = 0; mm <= L; mm++)
+                    if (mm <= n) P = P + ec[mm] * sv[mm];
+#pragma unroll
+                for (int mm = 0; mm < L; mm++)
+                    if (mm < n) Q = Q + oc[mm] * tv[mm];
+                const int slot = dir ? sj : si;
+                cpx<T>* acc = ACC + (slot * NR + r) * NB + p * NB2;
+                if (k == 0) {
+                    acc[hidx<L>(0, n)] = acc[hidx<L>(0, n)] + (T)2 * P;
+                } else {
+                    const T sk = (k & 1) ? (T)-1 : (T)1;
+                    const int im = dir ? -k : k;
+                    cpx<T> outk = (P + Q) * e[-im];
+                    cpx<T> outmk = (sk * (P - Q)) * e[im];
+                    const bool swp = (dir != (int)((a.contran >> r) & 1u));
+                    if (swp) { cpx<T> tt = outk; outk = sk * outmk; outmk = sk * tt; }
+                    acc[hidx<L>(k, n)] = acc[hidx<L>(k, n)] + outk;
+                    acc[hidx<L>(-k, n)] = acc[hidx<L>(-k, n)] + outmk;
                 }
-#pragma unroll 1
-                for (int cc = 0; cc < CB; cc++) {
-                    const int c = g * CB + cc;
-                    const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
-                    const cpx<T>* sv = W1 + c * NB2 + sofs(N);
-                    const cpx<T>* tv = W1 + c * NB2 + NS + tofs(N);
-                    cpx<T> P = ec[0] * sv[0];
-#pragma unroll
-                    for (int mm = 1; mm <= N; mm++) P = P + ec[mm] * sv[mm];
-                    const int slot = dir ? sj : si;
-                    cpx<T>* acc = ACC + (slot * NR + r) * NB + p * NB2;
-                    if (k == 0) {
-                        acc[hidx<L>(0, N)] = acc[hidx<L>(0, N)] + (T)2 * P;
-                    } else {
-                        cpx<T> Q = oc[0] * tv[0];
-#pragma unroll
-                        for (int mm = 1; mm < N; mm++) Q = Q + oc[mm] * tv[mm];
-                        const T sk = (k & 1) ? (T)-1 : (T)1;
-                        const int im = dir ? -k : k;
-                        cpx<T> outk = (P + Q) * e[-im];
-                        cpx<T> outmk = (sk * (P - Q)) * e[im];
-                        const bool swp = (dir != (int)((a.contran >> r) & 1u));
-                        if (swp) { cpx<T> tt = outk; outk = sk * outmk; outmk = sk * tt; }
-                        acc[hidx<L>(k, N)] = acc[hidx<L>(k, N)] + outk;
-                        acc[hidx<L>(-k, N)] = acc[hidx<L>(-k, N)] + outmk;
-                    }
-                }
-            });
+            }
         }
         __syncthreads();
 
