@@ -16,6 +16,7 @@
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
+void mstmg_internal_set_error(const std::string& msg) { set_err(msg); }
 
 #define CK(call)                                                                                  \
     do {                                                                                          \
