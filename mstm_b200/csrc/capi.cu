@@ -468,11 +468,13 @@ extern "C" int mstmg_mie_coefficients(const mstmg_ctx* c, double* an, double* qe
 // ---------------------------------------------------------------------------
 // operators and the translation pass
 // ---------------------------------------------------------------------------
-static int ensure_ops(mstmg_ctx* c, int prec, bool force)
+// Generate the stored pair operators.  want64 / want32 select the FP64 and
+// FP32 records; both come out of one pass of the generator when both are due.
+static int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
 {
     if (c->npairs == 0) return MSTMG_OK;
-    bool need64 = (prec == 0) && (force || !c->ops64_ready);
-    bool need32 = (prec == 1) && (force || !c->ops32_ready);
+    bool need64 = want64 && (force || !c->ops64_ready);
+    bool need32 = want32 && (force || !c->ops32_ready);
     if (!need64 && !need32) return MSTMG_OK;
     if (need64) CK(c->op64.alloc(c->op_units));
     if (need32) CK(c->op32.alloc(c->op_units));
@@ -500,6 +502,7 @@ static int ensure_ops(mstmg_ctx* c, int prec, bool force)
     if (need32) c->ops32_ready = true;
     return MSTMG_OK;
 }
+static int ensure_ops(mstmg_ctx* c, int prec, bool force) { return ensure_ops_both(c, prec == 0, prec == 1, force); }
 
 template <typename T> static const T* ops_ptr(mstmg_ctx* c);
 template <> const double* ops_ptr<double>(mstmg_ctx* c) { return c->op64.p; }
@@ -827,12 +830,8 @@ extern "C" int mstmg_fixed_orientation(mstmg_ctx* c, double alpha, double sinc, 
     c->passes64 = c->passes32 = 0;
     c->outer = 0;
     // operators are (re)generated for this configuration: the reference's initial_run
-    int rc = ensure_ops(c, 0, true);
+    int rc = ensure_ops_both(c, true, c->opts.precision == MSTMG_PRECISION_MIXED, true);
     if (rc) return rc;
-    if (c->opts.precision == MSTMG_PRECISION_MIXED) {
-        rc = ensure_ops(c, 1, true);
-        if (rc) return rc;
-    }
     launch_planewave(alpha, sinc, dir, c->lmax, ne, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p,
                      c->pmnp.p, c->st);
     zd* bvec = c->bvec64.p;   // pmnpan for both polarisations: 2 x ne
