@@ -99,6 +99,22 @@ int mstmg_planewave(mstmg_ctx *ctx, double alpha, double sinc, int dir, double *
 int mstmg_fixed_orientation(mstmg_ctx *ctx, double alpha, double sinc, int dir, double eps, int niter, double *amnp,
                             double *qeff, double *qtot, double *maxerr, int *maxiter);
 
+/* Scattering post-processing of a fixed-orientation solution, the free-space
+ * single-origin branch of main_calling_program (mstm-input-37.f90:1159-1197,
+ * 1497-1532): translation orders of each sphere to the cluster origin
+ * (tranordertest, mstm-modules-33.f90:1896-1942) with trans_eps
+ * (translation_epsilon) and cap max_t_order (max_t_matrix_order); the merge to
+ * the common origin (merge_to_common_origin, mstm-scatprops-26.f90:447-559);
+ * the GSF expansion of the azimuth-averaged scattering matrix (fosmexpansion,
+ * mstm-scatprops-26.f90:1820-1951) and its values at nangles polar angles
+ * evenly spaced over 0..180 degrees (fosmcalc, mstm-scatprops-26.f90:1750-1810,
+ * as scattering_matrix_calculation, mstm-input-37.f90:3015-3118, calls it).
+ *   amnp: neqns x 2 (the fixed_orientation output); smat: 16 x nangles
+ *   (Fortran sm(4,4) per angle, may be NULL); g = s00(1,1,1)/(3 s00(1,1,0));
+ *   amnp0: optional 2*T(T+2) x 2 common-origin coefficients if amnp0_cap >= 2*T(T+2). */
+int mstmg_scattering(mstmg_ctx *ctx, const double *amnp, double trans_eps, int max_t_order, int nangles, double *smat, double *g,
+                     int *t_matrix_order, double *amnp0, int amnp0_cap);
+
 /* Statistics of the last solve: iterations per polarisation, refinement steps,
  * FP64 and FP32 operator passes. */
 int mstmg_last_stats(const mstmg_ctx *ctx, int *iters2, int *outer, int *passes64, int *passes32);

@@ -29,6 +29,8 @@ SIGNATURES = {
     "mstmg_planewave": (c_int, [c_void_p, c_double, c_double, c_int, c_void_p]),
     "mstmg_fixed_orientation": (c_int, [c_void_p, c_double, c_double, c_int, c_double, c_int, c_void_p, c_void_p, c_void_p,
                                         P(c_double), P(c_int)]),
+    "mstmg_scattering": (c_int, [c_void_p, c_void_p, c_double, c_int, c_int, c_void_p, P(c_double), P(c_int), c_void_p,
+                                 c_int]),
     "mstmg_last_stats": (c_int, [c_void_p, c_void_p, P(c_int), P(c_int), P(c_int)]),
     "mstmg_operator_bytes": (c_int, [c_void_p, c_int, P(c_double), P(c_double)]),
     "mstmg_time_translation": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),

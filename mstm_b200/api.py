@@ -140,6 +140,16 @@ class SphereCluster:
         stats = self.last_stats()
         return dict(amnp=amnp, qeff=qeff, qtot=qtot, maxerr=me.value, maxiter=mi.value, istat=st, **stats)
 
+    def scattering(self, amnp, trans_eps=1.0e-5, max_t_order=100, nangles=181):
+        """Azimuth-averaged scattering matrix (nangles, 4, 4), asymmetry parameter
+        g and t_matrix_order of a fixed-orientation solution amnp (neqns, 2)."""
+        amnp = np.asfortranarray(amnp, np.complex128)
+        smat = np.zeros(16 * nangles)
+        g, tmo = c_double(0.0), c_int(0)
+        check(self._L.mstmg_scattering(self.ctx, _ptr(amnp), trans_eps, max_t_order, nangles, _ptr(smat), ctypes.byref(g),
+                                       ctypes.byref(tmo), None, 0), "scattering")
+        return dict(smat=smat.reshape(nangles, 4, 4).transpose(0, 2, 1).copy(), g=g.value, t_matrix_order=tmo.value)
+
     def last_stats(self):
         it = np.zeros(2, np.int32)
         outer, p64, p32 = c_int(0), c_int(0), c_int(0)

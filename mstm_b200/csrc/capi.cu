@@ -13,6 +13,7 @@
 #include "sphere_kernels.cuh"
 #include "tables.h"
 #include "translate_tiled.cuh"
+#include "postproc.cuh"
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
@@ -61,6 +62,7 @@ struct mstmg_ctx {
     double xg = 1.0;
     std::vector<int> order, offset, mie_offset;
     std::vector<double> radius;
+    std::vector<double> hpos;   // host copy of the positions (cluster origin)
     DevBuf<double> pos, rad, ri, qext, qabs;
     DevBuf<int> d_order, d_offset, d_mie_offset, slot, slot_full;
     DevBuf<zd> an, an_inv;
@@ -383,6 +385,12 @@ extern "C" int mstmg_ctx_create(mstmg_ctx** out, int nsphere, const double* pos,
         return fail(MSTMG_ERR_CUDA);
     }
     c->radius.assign(radius, radius + nsphere);
+    c->hpos.assign(3 * (size_t)nsphere, 0.0);
+    if (is_dev(pos)) {
+        if (cudaMemcpy(c->hpos.data(), pos, sizeof(double) * 3 * nsphere, cudaMemcpyDeviceToHost)) return fail(MSTMG_ERR_CUDA);
+    } else {
+        memcpy(c->hpos.data(), pos, sizeof(double) * 3 * nsphere);
+    }
     if (copy_in(c->pos.p, pos, sizeof(double) * 3 * nsphere, c->st) || copy_in(c->rad.p, radius, sizeof(double) * nsphere, c->st) ||
         copy_in(c->ri.p, ref_index, sizeof(double) * 2 * nsphere, c->st) || cudaMemsetAsync(c->err.p, 0, sizeof(int), c->st)) {
         set_err("copy of sphere data failed");
@@ -439,6 +447,8 @@ extern "C" int mstmg_ctx_set_positions(mstmg_ctx* c, const double* pos)
 {
     if (!c || !pos) return MSTMG_ERR_ARG;
     CK(copy_in(c->pos.p, pos, sizeof(double) * 3 * c->n, c->st));
+    if (is_dev(pos)) CK(cudaMemcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n, cudaMemcpyDeviceToHost));
+    else memcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n);
     c->ops64_ready = c->ops32_ready = false;
     return MSTMG_OK;
 }
@@ -914,6 +924,163 @@ extern "C" int mstmg_operator_bytes(const mstmg_ctx* c, int prec, double* stored
         *canonical = s;
     }
     return MSTMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Scattering post-processing of a solution (main_calling_program,
+// mstm-input-37.f90:1159-1197 and 1497-1532): translation orders and
+// t_matrix_order, merge to the common origin, GSF expansion, azimuth-averaged
+// scattering matrix on nangles polar angles 0..180 deg, and g.
+// ---------------------------------------------------------------------------
+extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_eps, int max_t_order, int nangles, double* smat,
+                                double* g, int* t_matrix_order, double* amnp0, int amnp0_cap)
+{
+    if (!c || !amnp || nangles < 2 || max_t_order < 1) {
+        set_err("mstmg_scattering: bad arguments");
+        return MSTMG_ERR_ARG;
+    }
+    const int n = c->n, L = c->lmax;
+    const int NBC = 420;
+    // cluster origin: mean position of the external spheres
+    double r0[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->hpos[3 * (size_t)i + k];
+    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)n;
+    static thread_local mstmg::Tables* big = nullptr;
+    if (!big) big = new mstmg::Tables(NBC);
+    DevBuf<double> dbc, dfnr;
+    CK(dbc.alloc(big->bcof.size()));
+    CK(dfnr.alloc(big->fnr.size()));
+    CK(cudaMemcpyAsync(dbc.p, big->bcof.data(), sizeof(double) * big->bcof.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dfnr.p, big->fnr.data(), sizeof(double) * big->fnr.size(), cudaMemcpyHostToDevice, c->st));
+    // translation orders (tranordertest) on the device
+    DevBuf<int> dtord;
+    DevBuf<zd> tscr;
+    const int sstride = 3 * (200 + MSTMG_LMAX + 4);
+    CK(dtord.alloc(n));
+    CK(tscr.alloc((size_t)n * sstride));
+    launch_tranorder(n, c->pos.p, c->d_order.p, r0, c->opts.medium_re, trans_eps, max_t_order, dbc.p, dfnr.p, NBC, tscr.p, sstride,
+                     dtord.p, c->st);
+    std::vector<int> tord(n);
+    CK(cudaMemcpyAsync(tord.data(), dtord.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int T = std::min(L, max_t_order);
+    for (int i = 0; i < n; i++) T = std::max(T, tord[i]);
+    if (T > 200) {
+        set_err("mstmg_scattering: t_matrix_order above 200 is not supported");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    // axial constants for regular translation up to order T (host, FP64)
+    std::vector<double> vcc((size_t)T * L * (L + 2) * (T + L + 1), 0.0), f1, f2, f3, vc1(2 * (T + L) + 4), vc2(2 * (T + L) + 4);
+    for (int nn = 1; nn <= T; nn++)
+        for (int l = 1; l <= L; l++) {
+            double c1 = big->fnr[nn + nn + 1] * big->fnr[l + l + 1];
+            big->vcfunc(-1, nn, 1, l, vc2.data());
+            int wmin = std::abs(nn - l), wmax = nn + l, nlmin = std::min(l, nn);
+            for (int m = -nlmin; m <= nlmin; m++) {
+                int ml = l * (l + 1) + m;
+                double c2 = -c1 * ((m & 1) ? -1.0 : 1.0);
+                big->vcfunc(-m, nn, m, l, vc1.data());
+                for (int w = wmin; w <= wmax; w++) {
+                    int e = ((nn - l + w) % 4 + 4) % 4;
+                    double ri = (e == 0 || e == 1) ? 1.0 : -1.0;
+                    vcc[(size_t)(nn - 1) + (size_t)T * ((size_t)(ml - 1) + (size_t)L * (L + 2) * w)] = c2 * vc1[w] * vc2[w] * ri;
+                }
+            }
+        }
+    int FN = std::max(T, L);
+    {
+        std::vector<double> tmpv;
+        mstmg::Tables small(6 * FN + 6 < NBC ? 6 * FN + 6 : NBC);
+        size_t nf = (size_t)(2 * FN + 1) * FN;
+        f1.assign(nf, 0.0);
+        f2.assign(nf, 0.0);
+        f3.assign(nf, 0.0);
+        const std::vector<double>& fr = big->fnr;
+        for (int m = -FN; m <= FN; m++)
+            for (int l = std::max(1, std::abs(m)); l <= FN; l++) {
+                size_t ix = (size_t)(m + FN) + (2 * FN + 1) * (size_t)(l - 1);
+                int lp1 = l + 1, lm1 = l - 1;
+                f1[ix] = fr[lm1] * fr[lp1] * fr[l - m] * fr[l + m] / fr[lm1 + l] / fr[l + lp1] / (double)l;
+                f2[ix] = (double)m / (double)l / (double)lp1;
+                f3[ix] = fr[l] * fr[l + 2] * fr[lp1 - m] * fr[lp1 + m] / fr[l + lp1] / fr[l + l + 3] / (double)lp1;
+            }
+    }
+    DevBuf<double> dvcc, df1, df2, df3, dbcd;
+    CK(dvcc.alloc(vcc.size()));
+    CK(df1.alloc(f1.size()));
+    CK(df2.alloc(f2.size()));
+    CK(df3.alloc(f3.size()));
+    std::vector<double> bd(T + L + 4);
+    for (int k = 0; k < (int)bd.size(); k++) bd[k] = big->bc(k, k);
+    CK(dbcd.alloc(bd.size()));
+    CK(cudaMemcpyAsync(dvcc.p, vcc.data(), sizeof(double) * vcc.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(df1.p, f1.data(), sizeof(double) * f1.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(df2.p, f2.data(), sizeof(double) * f2.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(df3.p, f3.data(), sizeof(double) * f3.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dbcd.p, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice, c->st));
+    // merge to the common origin
+    const int ne = c->neqns, nb0 = 2 * T * (T + 2);
+    DevBuf<zd> dsrc, da0, mscr;
+    CK(dsrc.alloc(2 * (size_t)ne));
+    CK(copy_in(dsrc.p, amnp, sizeof(zd) * 2 * (size_t)ne, c->st));
+    CK(da0.alloc(2 * (size_t)nb0));
+    CK(cudaMemsetAsync(da0.p, 0, sizeof(zd) * 2 * (size_t)nb0, c->st));
+    int grid = std::min(n, c->nsm * 2);
+    size_t stride = merge_scratch_per_cta(T, L);
+    CK(mscr.alloc((size_t)grid * stride));
+    MergeArgs ma;
+    ma.nsph = n;
+    ma.pos = c->pos.p;
+    ma.order = c->d_order.p;
+    ma.offset = c->d_offset.p;
+    ma.tord = dtord.p;
+    ma.T = T;
+    ma.r0[0] = r0[0];
+    ma.r0[1] = r0[1];
+    ma.r0[2] = r0[2];
+    ma.rimed_re = c->opts.medium_re;
+    ma.rimed_im = c->opts.medium_im;
+    ma.amnp = dsrc.p;
+    ma.ld = ne;
+    ma.npol = 2;
+    ma.amnp0 = da0.p;
+    ma.ld0 = nb0;
+    ma.vcc = dvcc.p;
+    ma.vcT = T;
+    ma.vcML = L * (L + 2);
+    ma.fnm1 = df1.p;
+    ma.fnc = df2.p;
+    ma.fnp1 = df3.p;
+    ma.fcN = FN;
+    ma.fnr = dfnr.p;
+    ma.bcofd = dbcd.p;
+    ma.scratch = mscr.p;
+    ma.scratch_stride = stride;
+    launch_merge(ma, grid, c->st);
+    CK(cudaGetLastError());
+    // GSF expansion and scattering matrix
+    const int W = 2 * T + 1;
+    DevBuf<double> ds, fscr, cscr, dsm;
+    CK(ds.alloc(4 * 16 * (size_t)W));
+    CK(cudaMemsetAsync(ds.p, 0, sizeof(double) * 4 * 16 * (size_t)W, c->st));
+    CK(fscr.alloc(fosm_scratch_doubles(T)));
+    launch_fosm(T, da0.p, dbc.p, dfnr.p, NBC, ds.p, ds.p + 16 * W, ds.p + 32 * W, ds.p + 48 * W, fscr.p, c->st);
+    CK(cscr.alloc(fosmcalc_scratch_doubles(T, nangles)));
+    CK(dsm.alloc(16 * (size_t)nangles));
+    launch_fosmcalc(T, nangles, ds.p, ds.p + 16 * W, ds.p + 32 * W, ds.p + 48 * W, dfnr.p, dbcd.p, cscr.p, dsm.p, c->st);
+    CK(cudaGetLastError());
+    double s0[2];
+    CK(cudaMemcpyAsync(&s0[0], ds.p + 0, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&s0[1], ds.p + 16, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    if (smat) CK(copy_out(smat, dsm.p, sizeof(double) * 16 * (size_t)nangles, c->st));
+    if (amnp0 && amnp0_cap >= nb0) CK(copy_out(amnp0, da0.p, sizeof(zd) * 2 * (size_t)nb0, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (g) *g = s0[1] / (3.0 * s0[0]);
+    if (t_matrix_order) *t_matrix_order = T;
+    dbc.release(); dfnr.release(); dtord.release(); tscr.release(); dvcc.release(); df1.release(); df2.release(); df3.release();
+    dbcd.release(); dsrc.release(); da0.release(); mscr.release(); ds.release(); fscr.release(); cscr.release(); dsm.release();
+    return check_kernel_err(c);
 }
 
 extern "C" int mstmg_set_stream(mstmg_ctx* c, void* stream)

@@ -1,0 +1,598 @@
+// postproc.cu -- FP64 device post-processing of a solved cluster:
+//   * translation orders of each sphere to the cluster origin
+//     (tranordertest, december2023/mstm-modules-33.f90:1896-1942);
+//   * merge to the common origin: regular (J) translation of every sphere's
+//     expansion to the origin, converted from the LR to the TE/TM basis and
+//     summed (merge_to_common_origin, mstm-scatprops-26.f90:447-559);
+//   * GSF expansion of the azimuth-averaged scattering matrix
+//     (fosmexpansion, mstm-scatprops-26.f90:1820-1951);
+//   * its evaluation at polar angles (fosmcalc, mstm-scatprops-26.f90:1750-1810).
+// Orders reach t_matrix_order (up to 100), so the per-sphere translation keeps
+// its Wigner-d rows, Bessel values and axial blocks in global scratch.
+#include "common.cuh"
+#include "special.cuh"
+#include "postproc.cuh"
+#include <algorithm>
+
+#define PP_NT 128
+
+// ---------------------------------------------------------------------------
+// vector-coupling coefficients on the device (vcfunc / vcfuncuprec,
+// modules:950-1056), from a bcof/fnr table of side nbc+1
+// ---------------------------------------------------------------------------
+struct VCTab {
+    const double* bcof;  // (nbc+1)^2
+    const double* fnr;   // 0..2*nbc
+    int nbc;
+    __device__ double bc(int n, int l) const { return bcof[(size_t)n * (nbc + 1) + l]; }
+    __device__ double fr(int n) const { return fnr[n]; }
+};
+
+__device__ void vc_uprec(const VCTab& t, int m, int n, int k, int l, int wmax, double* vcn)
+{
+    int mk = abs(m + k), nl = abs(n - l), w, m1, l1, k1;
+    double vc1;
+    if (nl >= mk) {
+        w = nl;
+        if (n >= l) { m1 = m; l1 = l; k1 = k; }
+        else { m1 = k; k1 = m; l1 = n; }
+        vc1 = pm1(k1 + l1) * t.bc(l1 + k1, w - m1 - k1) * t.bc(l1 - k1, w + m1 + k1) / t.bc(l1 + l1, w + w + 1);
+    } else {
+        w = mk;
+        if (m + k >= 0) vc1 = pm1(n + m) * t.bc(n - l + w, l - k) * t.bc(l - n + w, n - m) / t.bc(w + w + 1, n + l - w);
+        else vc1 = pm1(l + k) * t.bc(n - l + w, l + k) * t.bc(l - n + w, n + m) / t.bc(w + w + 1, n + l - w);
+    }
+    int w1 = w;
+    vcn[w] = vc1;
+    w = w1 + 1;
+    mk = m + k;
+    int w2 = min(wmax, n + l);
+    if (w2 > w1) {
+        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
+                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
+        double t2 = (w1 == 0) ? 0.5 * (double)(m - k)
+                              : (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
+        vcn[w] = t1 * t2 * vcn[w1];
+    }
+    for (w = w1 + 2; w <= w2; w++) {
+        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
+                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
+        double t2 = (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
+        double t3 = t.fr(w - mk - 1) * t.fr(w + mk - 1) * t.fr(l - n + w - 1) * t.fr(n - l + w - 1) * t.fr(n + l - w + 2) * t.fr(n + l + w) /
+                    ((double)(2 * (w - 1)) * t.fr(2 * w - 3) * t.fr(2 * w - 1));
+        vcn[w] = t1 * (t2 * vcn[w - 1] - t3 * vcn[w - 2]);
+    }
+}
+
+__device__ void vc_func(const VCTab& t, int m, int n, int k, int l, double* vcn)
+{
+    for (int w = 0; w <= n + l; w++) vcn[w] = 0.0;
+    int wmax = n + l;
+    int wmin = max(abs(n - l), abs(m + k));
+    vcn[wmax] = t.bc(n + m, l + k) * t.bc(n - m, l - k) / t.bc(n + n, l + l);
+    if (wmin == wmax) return;
+    vcn[wmax - 1] = vcn[wmax] * (l * m - k * n) * t.fr(2 * (l + n) - 1) / t.fr(l) / t.fr(n) / t.fr(n + l + m + k) / t.fr(n + l - m - k);
+    if (wmin == wmax - 1) return;
+    int mk = m + k;
+    double vcmax = fabs(vcn[wmax]) + fabs(vcn[wmax - 1]);
+    int w;
+    for (w = wmax; w >= wmin + 2; w--) {
+        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
+                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
+        double t2 = (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
+        double t3 = t.fr(w - mk - 1) * t.fr(w + mk - 1) * t.fr(l - n + w - 1) * t.fr(n - l + w - 1) * t.fr(n + l - w + 2) * t.fr(n + l + w) /
+                    ((double)(2 * (w - 1)) * t.fr(2 * w - 3) * t.fr(2 * w - 1));
+        vcn[w - 2] = (t2 * vcn[w - 1] - vcn[w] / t1) / t3;
+        if ((wmax - w) % 2 == 1) {
+            double vctest = fabs(vcn[w - 2]) + fabs(vcn[w - 1]);
+            vcmax = vcmax > vctest ? vcmax : vctest;
+            if (vctest / vcmax < 0.01) break;
+        }
+    }
+    if (w - 2 > wmin) vc_uprec(t, m, n, k, l, w - 3, vcn);
+}
+
+__device__ __forceinline__ zd ipow_z(int k)
+{
+    int e = ((k % 4) + 4) % 4;
+    return (e == 0) ? mk(1.0, 0.0) : (e == 1 ? mk(0.0, 1.0) : (e == 2 ? mk(-1.0, 0.0) : mk(0.0, -1.0)));
+}
+
+// ---------------------------------------------------------------------------
+// tranordertest per sphere
+// ---------------------------------------------------------------------------
+__global__ void tranorder_kernel(int nsph, const double* pos, const int* order, double ox, double oy, double oz, double rire, double eps,
+                                 int maxt, VCTab tab, zd* scratch, int sstride, int* tord)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsph) return;
+    const int nlim = 200;
+    int lmax = order[i];
+    double dx = pos[3 * i] - ox, dy = pos[3 * i + 1] - oy, dz = pos[3 * i + 2] - oz;
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    int nmax;
+    if (r == 0.0) {
+        nmax = lmax;
+    } else {
+        zd* xi = scratch + (size_t)i * sstride;
+        zd* scr = xi + (nlim + lmax + 2);
+        double* vc1 = (double*)(scr + (nlim + lmax + 2));
+        zd z = mk(r * rire, 0.0);
+        double sum = 0.0;
+        int n;
+        for (n = 1; n <= nlim; n++) {
+            mstm_cricbessel(n + lmax, z, xi, scr);
+            for (int l = 0; l <= n + lmax; l++) xi[l] = cdiv(xi[l], z) * ipow_z(l);
+            int l = lmax;
+            zd c = (tab.fr(n + n + 1) * tab.fr(l + l + 1)) * ipow_z(n - l);
+            vc_func(tab, -1, n, 1, l, vc1);
+            int wmin = abs(n - l), wmax = n + l;
+            zd a = mk(0.0, 0.0), b = mk(0.0, 0.0);
+            for (int w = wmin; w <= wmax; w++) {
+                double alnw = vc1[w] * vc1[w];
+                if ((n + l + w) % 2 == 0) a = a + alnw * xi[w];
+                else b = b + alnw * xi[w];
+            }
+            a = c * a;
+            b = c * b;
+            sum = sum + (a * cj(a) + b * cj(b)).x;
+            if (fabs(1.0 - sum) < eps) break;
+        }
+        nmax = min(n, nlim);
+        nmax = max(nmax, lmax);
+    }
+    tord[i] = min(nmax, maxt);
+}
+
+// ---------------------------------------------------------------------------
+// merge to the common origin: one CTA per sphere (grid-stride), scratch per CTA
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int tid = threadIdx.x;
+    const int T = a.T;
+    zd* base = a.scratch + (size_t)blockIdx.x * a.scratch_stride;
+    for (int i = blockIdx.x; i < a.nsph; i += gridDim.x) {
+        const int L = a.order[i];
+        const int nt = min(T, a.tord[i]);
+        const int nmin = min(L, nt), nmax = max(L, nt);
+        const double rv0 = a.r0[0] - a.pos[3 * i], rv1 = a.r0[1] - a.pos[3 * i + 1], rv2 = a.r0[2] - a.pos[3 * i + 2];
+        const double rr = rv0 * rv0 + rv1 * rv1 + rv2 * rv2;
+        // scratch layout
+        zd* xi = base;                                        // nt+L+2
+        zd* hs = xi + (nmax + L + 4);                         // Bessel scratch 2*(nt+L+2)
+        double* D = (double*)(hs + 2 * (nmax + L + 4));       // Wigner rows: per degree n, (2nmin+1) x (2n+1), restricted index first
+        size_t dsz = 0;
+        for (int n = 0; n <= nmax; n++) dsz += (size_t)(2 * nmin + 1) * (2 * n + 1);
+        zd* Z = (zd*)(D + dsz + 1);                           // one axial block: 2 x nt x L
+        zd* G = Z + 2 * (size_t)nt * L;                       // g(m, n, p): 2 x nt x (2nmin+1)
+        zd* AP = G + 2 * (size_t)nt * (2 * nmin + 1);         // a'(k, l, p): 2 x L x (2nmin+1)
+        double* dk0 = (double*)(AP + 2 * (size_t)L * (2 * nmin + 1)) + (nmax + 1);
+        double* dk01 = dk0 + (2 * nmax + 3);
+        const zd* src = a.amnp;
+        __syncthreads();
+        if (rr < 1.0e-12) {
+            // zero translation of regular functions: copy the overlapping orders (mtransfer)
+            int nc = min(L, nt);
+            for (int p = 0; p < a.npol; p++)
+                for (int e = tid; e < nc * (nc + 2); e += PP_NT) {
+                    int n = 1;
+                    while (n * (n + 2) <= e) n++;
+                    int m = e - (n * n - 1) - n;   // e = n(n+1)-1+m ... -> m in -n..n
+                    zd v1 = src[(size_t)p * a.ld + a.offset[i] + aidx(m, n, 0, L)];
+                    zd v2 = src[(size_t)p * a.ld + a.offset[i] + aidx(m, n, 1, L)];
+                    int s = aidx(m, n, 0, T);
+                    atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s].x, v1.x + v2.x);
+                    atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s].y, v1.y + v2.y);
+                    atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s + T * (T + 2)].x, v1.x - v2.x);
+                    atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s + T * (T + 2)].y, v1.y - v2.y);
+                }
+            __syncthreads();
+            continue;
+        }
+        const double r = sqrt(rr);
+        const double ct = rv2 / r;
+        zd ephi = (rv0 == 0.0 && rv1 == 0.0) ? mk(1.0, 0.0) : mk(rv0 / sqrt(rv0 * rv0 + rv1 * rv1), rv1 / sqrt(rv0 * rv0 + rv1 * rv1));
+        // Bessel functions psi_n(r)/r (cricbessel), n = 0..nt+L
+        if (tid == 0) {
+            zd z = mk(r * a.rimed_re, r * a.rimed_im);
+            mstm_cricbessel(nt + L, z, xi, hs);
+            for (int k = 0; k <= nt + L; k++) xi[k] = cdiv(xi[k], z);
+        }
+        // Wigner-d rows by the rotcoef recurrence (kmax = nmin, nmax)
+        {
+            double sbe = (fabs(ct) >= 1.0) ? 0.0 : sqrt(fabs((1.0 + ct) * (1.0 - ct)));
+            double cbe2 = 0.5 * (1.0 + ct), sbe2 = 0.5 * (1.0 - ct);
+            for (int k = tid; k < 2 * nmax + 3; k += PP_NT) { dk0[k - (nmax + 1)] = 0.0; dk01[k - (nmax + 1)] = 0.0; }
+            __syncthreads();
+            if (tid == 0) { dk0[0] = 1.0; D[0] = 1.0; }
+            __syncthreads();
+            int sgn = 1;
+            double sben = 1.0;
+            size_t doff = 1;   // degree 0 occupies (2nmin+1) x 1 but only its centre matters
+            doff = (size_t)(2 * nmin + 1);
+            for (int n = 1; n <= nmax; n++) {
+                int kk = min(n, nmin);
+                int ld = 2 * n + 1;
+                double* Dn = D + doff;
+                sgn = -sgn;
+                sben = sben * sbe / 2.0;
+                if (sben < 1.0e-30) sben = 0.0;
+                double newv[4];
+                int cnt = 0;
+                for (int k = -n + 1 + tid; k <= n - 1; k += PP_NT) {
+                    newv[cnt++] = (ct * (double)(n + n - 1) * dk0[k] - a.fnr[n - k - 1] * a.fnr[n + k - 1] * dk01[k]) / (a.fnr[n + k] * a.fnr[n - k]);
+                }
+                __syncthreads();
+                cnt = 0;
+                for (int k = -n + 1 + tid; k <= n - 1; k += PP_NT) {
+                    dk01[k] = dk0[k];
+                    dk0[k] = newv[cnt++];
+                }
+                if (tid == 0) {
+                    dk0[n] = sgn * sben * a.bcofd[n];
+                    dk0[-n] = sgn * dk0[n];
+                    dk01[n] = 0.0;
+                    dk01[-n] = 0.0;
+                }
+                __syncthreads();
+                for (int k = -n + tid; k <= n; k += PP_NT) Dn[(0 + nmin) * ld + (k + n)] = dk0[k];
+                __syncthreads();
+                int im = 1;
+                for (int m = 1; m <= kk; m++) {
+                    im = -im;
+                    double fmn = 1.0 / a.fnr[n - m + 1] / a.fnr[n + m];
+                    for (int k = -n + tid; k <= n; k += PP_NT) {
+                        double dkm1 = (k == -n) ? 0.0 : Dn[(m - 1 + nmin) * ld + (k - 1 + n)];
+                        double dkn1 = (k == n) ? 0.0 : Dn[(m - 1 + nmin) * ld + (k + 1 + n)];
+                        double v = (a.fnr[n + k] * a.fnr[n - k + 1] * cbe2 * dkm1 - a.fnr[n - k] * a.fnr[n + k + 1] * sbe2 * dkn1 -
+                                    (double)k * sbe * Dn[(m - 1 + nmin) * ld + (k + n)]) * fmn;
+                        Dn[(m + nmin) * ld + (k + n)] = v;
+                        Dn[(-m + nmin) * ld + (-k + n)] = v * pm1(k) * im;
+                    }
+                    __syncthreads();
+                }
+                doff += (size_t)(2 * nmin + 1) * ld;
+            }
+        }
+        __syncthreads();
+        // degree offsets of D
+        auto dofs = [&](int n) -> size_t {
+            size_t o = (size_t)(2 * nmin + 1);
+            for (int q = 1; q < n; q++) o += (size_t)(2 * nmin + 1) * (2 * q + 1);
+            return o;
+        };
+        for (int p = 0; p < a.npol; p++) {
+            const zd* x = src + (size_t)p * a.ld + a.offset[i];
+            // phase (shift_op = F: e^{+i m phi} on the source) and forward rotation of degrees l <= L
+            for (int e = tid; e < 2 * L * (2 * nmin + 1); e += PP_NT) {
+                int q = e / (L * (2 * nmin + 1));
+                int rem = e - q * L * (2 * nmin + 1);
+                int l = rem / (2 * nmin + 1) + 1;
+                int k = rem % (2 * nmin + 1) - nmin;
+                int n1 = min(l, nt);
+                zd acc = mk(0.0, 0.0);
+                if (abs(k) <= n1) {
+                    const double* Dl = D + dofs(l);
+                    zd ep = mk(1.0, 0.0);
+                    // a_tt(m) = a(m) e^{i m phi}; sum over m = -l..l
+                    for (int m = -l; m <= l; m++) {
+                        zd em = mk(1.0, 0.0);
+                        int am = m < 0 ? -m : m;
+                        for (int s = 0; s < am; s++) em = ephi * em;
+                        if (m < 0) em = cj(em);
+                        zd v = x[aidx(m, l, q, L)] * em;
+                        acc = acc + Dl[(k + nmin) * (2 * l + 1) + (m + l)] * v;
+                    }
+                    (void)ep;
+                }
+                AP[(q * L + (l - 1)) * (2 * nmin + 1) + (k + nmin)] = acc;
+            }
+            __syncthreads();
+            // axial translation per degree m (regular functions), both signs of m
+            for (int ma = 0; ma <= nmin; ma++) {
+                int m1 = max(1, ma);
+                int rows = nt - m1 + 1, cols = L - m1 + 1;
+                // first row n = m1 and last column l = L
+                for (int e = tid; e < cols + (rows - 1); e += PP_NT) {
+                    int n, l;
+                    if (e < cols) { n = m1; l = m1 + e; }
+                    else { n = m1 + 1 + (e - cols); l = L; }
+                    int wmin = abs(n - l), wmax = n + l, ml = l * (l + 1) + ma;
+                    zd s1 = mk(0.0, 0.0), s2 = mk(0.0, 0.0);
+                    for (int w = wmin; w <= wmax; w += 2) s1 = s1 + a.vcc[(n - 1) + (size_t)a.vcT * ((ml - 1) + (size_t)a.vcML * w)] * xi[w];
+                    for (int w = wmin + 1; w <= wmax - 1; w += 2) s2 = s2 + a.vcc[(n - 1) + (size_t)a.vcT * ((ml - 1) + (size_t)a.vcML * w)] * xi[w];
+                    s2 = imul(s2);
+                    Z[(0 * nt + (n - 1)) * L + (l - 1)] = s1 + s2;
+                    Z[(1 * nt + (n - 1)) * L + (l - 1)] = s1 - s2;
+                }
+                __syncthreads();
+                if (m1 < min(nt, L)) {
+                    for (int n = m1; n <= nt - 1; n++) {
+                        for (int e = tid; e < 2 * (L - m1); e += PP_NT) {
+                            int pp = e / (L - m1), l = m1 + e % (L - m1);
+                            double sp = (pp == 0) ? 1.0 : -1.0;
+#define ZA(nn, ll) Z[(pp * nt + ((nn) - 1)) * L + ((ll) - 1)]
+#define FC(arr, mm, ll) arr[((mm) + a.fcN) + (2 * a.fcN + 1) * ((ll) - 1)]
+                            zd v = -(ZA(n, l + 1) * FC(a.fnp1, ma, l)) + imul(sp * (FC(a.fnc, ma, l) - FC(a.fnc, ma, n)) * ZA(n, l));
+                            if (l >= m1 + 1) v = v + ZA(n, l - 1) * FC(a.fnm1, ma, l);
+                            if (n > m1) v = v + ZA(n - 1, l) * FC(a.fnm1, ma, n);
+                            double dd = FC(a.fnp1, ma, n);
+                            ZA(n + 1, l) = mk(v.x / dd, v.y / dd);
+#undef ZA
+#undef FC
+                        }
+                        __syncthreads();
+                    }
+                }
+                // g(+ma, n, p) = Z[mode p] a'(+ma) ; g(-ma, n, p) = Z[mode 1-p] a'(-ma)
+                for (int e = tid; e < 2 * 2 * rows; e += PP_NT) {
+                    int sg = e / (2 * rows);
+                    int rem = e - sg * 2 * rows;
+                    int pm = rem / rows, n = m1 + rem % rows;
+                    if (ma == 0 && sg == 1) continue;
+                    int mm = sg ? -ma : ma;
+                    int pz = (ma == 0) ? 0 : (sg == 0 ? pm : 1 - pm);
+                    zd acc = mk(0.0, 0.0);
+                    for (int l = m1; l <= L; l++)
+                        acc = acc + Z[(pz * nt + (n - 1)) * L + (l - 1)] * AP[(pm * L + (l - 1)) * (2 * nmin + 1) + (mm + nmin)];
+                    G[(pm * nt + (n - 1)) * (2 * nmin + 1) + (mm + nmin)] = acc;
+                }
+                __syncthreads();
+            }
+            // back rotation per target degree n, phase back, LR -> TE/TM, accumulate
+            for (int e = tid; e < nt * (nt + 2); e += PP_NT) {
+                int n = 1;
+                while (n * (n + 2) <= e) n++;
+                int k = e - (n * n - 1) - n;   // -n..n
+                int n1 = min(n, L);
+                const double* Dn = D + dofs(n);
+                zd gq[2];
+                for (int pm = 0; pm < 2; pm++) {
+                    zd acc = mk(0.0, 0.0);
+                    for (int m = -n1; m <= n1; m++) acc = acc + Dn[(m + nmin) * (2 * n + 1) + (k + n)] * G[(pm * nt + (n - 1)) * (2 * nmin + 1) + (m + nmin)];
+                    // phase back: e^{-i k phi}
+                    zd em = mk(1.0, 0.0);
+                    int ak = k < 0 ? -k : k;
+                    for (int s = 0; s < ak; s++) em = ephi * em;
+                    if (k > 0) em = cj(em);
+                    gq[pm] = acc * em;
+                }
+                int s = aidx(k, n, 0, T);
+                zd* o = a.amnp0 + (size_t)p * a.ld0;
+                atomicAdd(&o[s].x, gq[0].x + gq[1].x);
+                atomicAdd(&o[s].y, gq[0].y + gq[1].y);
+                atomicAdd(&o[s + T * (T + 2)].x, gq[0].x - gq[1].x);
+                atomicAdd(&o[s + T * (T + 2)].y, gq[0].y - gq[1].y);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fosmexpansion: one CTA per (n, l); threads over m; atomics into s arrays
+// ---------------------------------------------------------------------------
+__global__ void fosm_kernel(int ntot, const zd* a0, VCTab tab, double* s00, double* s02, double* sp22, double* sm22, double* vscr)
+{
+  double* base = vscr + ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 5 * (2 * ntot + 2);
+  for (int nl = blockIdx.x; nl < ntot * ntot; nl += gridDim.x) {
+    int n = nl / ntot + 1, l = nl % ntot + 1;
+    const int nb = 2 * ntot * (ntot + 2);
+    const int half = ntot * (ntot + 2);
+    int wmin = abs(n - l), wmax = n + l;
+    zd fnl = sqrt((double)((n + n + 1) * (l + l + 1))) * ipow_z(l - n);
+    int mm = min(n, l + 2);
+    for (int m = -mm + (int)threadIdx.x; m <= mm; m += blockDim.x) {
+        double* cm1p1 = base;
+        double* cm1m1 = cm1p1 + (2 * ntot + 2);
+        double* cmmpm = cm1m1 + (2 * ntot + 2);
+        double* cmmm2pm = cmmpm + (2 * ntot + 2);
+        double* cmmp2pm = cmmm2pm + (2 * ntot + 2);
+        vc_func(tab, -1, n, 1, l, cm1p1);
+        vc_func(tab, -1, n, -1, l, cm1m1);
+        if (abs(m) <= l) vc_func(tab, -m, n, m, l, cmmpm);
+        else for (int w = 0; w <= n + l; w++) cmmpm[w] = 0.0;
+        if (abs(-2 + m) <= l) vc_func(tab, -m, n, -2 + m, l, cmmm2pm);
+        else for (int w = 0; w <= n + l; w++) cmmm2pm[w] = 0.0;
+        if (abs(2 + m) <= l) vc_func(tab, -m, n, 2 + m, l, cmmp2pm);
+        else for (int w = 0; w <= n + l; w++) cmmp2pm[w] = 0.0;
+        double m1m = pm1(m);
+        auto A = [&](int pol, int mq, int nq, int p) -> zd {
+            if (mq < -nq || mq > nq) return mk(0.0, 0.0);
+            return a0[(size_t)pol * nb + aidx(mq, nq, 0, ntot) + (size_t)half * p];
+        };
+        for (int p = 1; p <= 2; p++)
+            for (int q = 1; q <= 2; q++) {
+                double m1mq = pm1(m + q);
+                double m1mnpl = pm1(m + n + p + l);
+                zd a1n = A(0, m, n, p - 1), a2n = A(1, m, n, p - 1);
+                zd a1l = A(0, m, l, q - 1), a2l = A(1, m, l, q - 1);
+                zd a1122 = a1n * cj(a1l) + a2n * cj(a2l);
+                zd a2112 = a2n * cj(a1l) - a1n * cj(a2l);
+                zd a1p2 = (a1n + imul(a2n)) * cj(A(0, m - 2, l, q - 1) - imul(A(1, m - 2, l, q - 1)));
+                zd a1m2 = (a1n - imul(a2n)) * cj(A(0, m + 2, l, q - 1) + imul(A(1, m + 2, l, q - 1)));
+                for (int w = wmin; w <= wmax; w++) {
+                    double m1w = pm1(w);
+                    bool ev = ((n + l + w + p + q) % 2 == 0);
+#define SS(arr, i, j) (&arr[((i) - 1) + 4 * ((j) - 1) + 16 * w])
+                    if (ev) atomicAdd(SS(s00, 1, 1), -((m1m * fnl) * a1122 * (cm1p1[w] * cmmpm[w])).x / 2.0);
+                    else atomicAdd(SS(s00, 4, 4), (imul(mk(0.5, 0.0)) * (m1m * fnl) * a2112 * (cm1p1[w] * cmmpm[w])).x);
+                    if (w < 2) continue;
+                    if (ev) {
+                        atomicAdd(SS(s02, 2, 1), -((m1mq * a1122) * fnl * (cm1m1[w] * cmmpm[w])).x / 2.0);
+                        atomicAdd(SS(s02, 1, 2), -((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).x / 4.0);
+                        atomicAdd(SS(s02, 1, 2), -((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).x / 4.0);
+                    } else {
+                        atomicAdd(SS(s02, 3, 4), (imul(mk(-0.5, 0.0)) * (m1mq * a2112) * fnl * (cm1m1[w] * cmmpm[w])).y);
+                        atomicAdd(SS(s02, 4, 3), ((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).y / 4.0);
+                        atomicAdd(SS(s02, 4, 3), -((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).y / 4.0);
+                    }
+                    atomicAdd(SS(sm22, 2, 2), -((m1mnpl * m1w * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0);
+                    atomicAdd(SS(sp22, 2, 2), -((m1mq * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0);
+                    atomicAdd(SS(sm22, 2, 2), -((m1mq * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0);
+                    atomicAdd(SS(sp22, 2, 2), -((m1mnpl * m1w * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0);
+#undef SS
+                }
+            }
+    }
+  }
+}
+
+// the sign patches and the 1/(2 m_medium) factor of fosmexpansion
+__global__ void fosm_patch_kernel(int ntot, double* s00, double* s02, double* sp22, double* sm22, double scale)
+{
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w > 2 * ntot) return;
+    double* S[4] = {s00, s02, sm22, sp22};
+    for (int k = 0; k < 4; k++)
+        for (int i = 3; i <= 4; i++)
+            for (int j = 1; j <= i; j++) S[k][(j - 1) + 4 * (i - 1) + 16 * w] = -S[k][(j - 1) + 4 * (i - 1) + 16 * w];
+    sm22[(3 - 1) + 4 * (3 - 1) + 16 * w] = -sm22[(2 - 1) + 4 * (2 - 1) + 16 * w];
+    sp22[(3 - 1) + 4 * (3 - 1) + 16 * w] = sp22[(2 - 1) + 4 * (2 - 1) + 16 * w];
+    for (int k = 0; k < 4; k++)
+        for (int e = 0; e < 16; e++) S[k][e + 16 * w] = 0.5 * S[k][e + 16 * w] / scale;
+}
+
+// fosmcalc at each angle: one CTA per angle; rotcoef(ct, 2, 2ntot) by the
+// degree recurrence, then the sum over w and the element patches
+__global__ void fosmcalc_kernel(int ntot, int nang, const double* s00, const double* s02, const double* sp22,
+                                const double* sm22, const double* fnr, const double* bcofd, double* dscr, double* smat)
+{
+    int ia = blockIdx.x;
+    if (ia >= nang) return;
+    const int nmax = 2 * ntot, kmax = 2;
+    // polar angle as scattering_matrix_calculation forms it (input:3039-3043), pi as MSTM stores it
+    double ct = cos(MSTMG_REF_PI / 180.0 * (0.0 + (180.0 - 0.0) * (double)ia / (double)(nang - 1)));
+    if (ct == 1.0) ct = 0.9999999;
+    if (ct == -1.0) ct = -0.9999999;
+    double* dk0 = dscr + (size_t)ia * (16 * nmax + 40) + (nmax + 1);
+    double* dk01 = dk0 + (2 * nmax + 3);
+    double* dc = dk01 + (2 * nmax + 3);   // rows m = -2..2 of the current degree, columns k = -nmax..nmax
+    const int W = 2 * nmax + 1;
+#define DCR(m, k) dc[((m) + 2) * W + ((k) + nmax)]
+    __shared__ double acc[16];
+    if (threadIdx.x < 16) acc[threadIdx.x] = 0.0;
+    double sbe = (fabs(ct) >= 1.0) ? 0.0 : sqrt(fabs((1.0 + ct) * (1.0 - ct)));
+    double cbe2 = 0.5 * (1.0 + ct), sbe2 = 0.5 * (1.0 - ct);
+    for (int k = threadIdx.x; k < 2 * nmax + 3; k += blockDim.x) { dk0[k - (nmax + 1)] = 0.0; dk01[k - (nmax + 1)] = 0.0; }
+    __syncthreads();
+    if (threadIdx.x == 0) dk0[0] = 1.0;
+    __syncthreads();
+    // degree 0: dc(0,0) = 1 -> the w = 0 term
+    if (threadIdx.x < 16) acc[threadIdx.x] += s00[threadIdx.x] * 1.0;
+    int sgn = 1;
+    double sben = 1.0;
+    for (int n = 1; n <= nmax; n++) {
+        int kk = min(n, kmax);
+        sgn = -sgn;
+        sben = sben * sbe / 2.0;
+        if (sben < 1.0e-30) sben = 0.0;
+        double newv[8];
+        int cnt = 0;
+        for (int k = -n + 1 + (int)threadIdx.x; k <= n - 1; k += blockDim.x)
+            newv[cnt++] = (ct * (double)(n + n - 1) * dk0[k] - fnr[n - k - 1] * fnr[n + k - 1] * dk01[k]) / (fnr[n + k] * fnr[n - k]);
+        __syncthreads();
+        cnt = 0;
+        for (int k = -n + 1 + (int)threadIdx.x; k <= n - 1; k += blockDim.x) {
+            dk01[k] = dk0[k];
+            dk0[k] = newv[cnt++];
+        }
+        if (threadIdx.x == 0) {
+            dk0[n] = sgn * sben * bcofd[n];
+            dk0[-n] = sgn * dk0[n];
+            dk01[n] = 0.0;
+            dk01[-n] = 0.0;
+        }
+        __syncthreads();
+        for (int k = -n + (int)threadIdx.x; k <= n; k += blockDim.x) DCR(0, k) = dk0[k];
+        __syncthreads();
+        int im = 1;
+        for (int m = 1; m <= kk; m++) {
+            im = -im;
+            double fmn = 1.0 / fnr[n - m + 1] / fnr[n + m];
+            for (int k = -n + (int)threadIdx.x; k <= n; k += blockDim.x) {
+                double dkm1 = (k == -n) ? 0.0 : DCR(m - 1, k - 1);
+                double dkn1 = (k == n) ? 0.0 : DCR(m - 1, k + 1);
+                double v = (fnr[n + k] * fnr[n - k + 1] * cbe2 * dkm1 - fnr[n - k] * fnr[n + k + 1] * sbe2 * dkn1 -
+                            (double)k * sbe * DCR(m - 1, k)) * fmn;
+                DCR(m, k) = v;
+                DCR(-m, -k) = v * pm1(k) * im;
+            }
+            __syncthreads();
+        }
+        // terms: w = n uses dc(0, n(n+1)) [k=0 column]; dc(0,n(n+1)+2), dc(+-2, n(n+1)+2) [k=2]
+        if (threadIdx.x < 16) {
+            int e = threadIdx.x;
+            double v = s00[e + 16 * n] * DCR(0, 0);
+            if (n >= 2) v += s02[e + 16 * n] * DCR(0, 2) + sp22[e + 16 * n] * DCR(2, 2) + sm22[e + 16 * n] * DCR(-2, 2);
+            acc[e] += v;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double sm[16];
+        for (int e = 0; e < 16; e++) sm[e] = acc[e];
+#define SM(i, j) sm[((i) - 1) + 4 * ((j) - 1)]
+        SM(3, 1) = -SM(3, 1);
+        SM(1, 3) = -SM(1, 3);
+        SM(4, 3) = -SM(4, 3);
+        double temp = SM(4, 1);
+        SM(4, 1) = SM(4, 2);
+        SM(4, 2) = temp;
+        SM(1, 2) = (SM(1, 2) + SM(2, 1)) / 2.0;
+        SM(2, 1) = SM(1, 2);
+        SM(3, 4) = (SM(3, 4) - SM(4, 3)) / 2.0;
+        SM(4, 3) = -SM(3, 4);
+#undef SM
+        for (int e = 0; e < 16; e++) smat[(size_t)ia * 16 + e] = sm[e];
+    }
+#undef DCR
+}
+
+void launch_tranorder(int nsph, const double* pos, const int* order, const double* origin, double rire, double eps, int maxt,
+                      const double* bcof, const double* fnr, int nbc, zd* scratch, int sstride, int* tord, cudaStream_t st)
+{
+    VCTab t{bcof, fnr, nbc};
+    tranorder_kernel<<<(nsph + 63) / 64, 64, 0, st>>>(nsph, pos, order, origin[0], origin[1], origin[2], rire, eps, maxt, t, scratch,
+                                                      sstride, tord);
+    launch_counter() += 1;
+}
+
+size_t merge_scratch_per_cta(int T, int L)
+{
+    int nmin = std::min(T, L), nmax = std::max(T, L);
+    size_t dsz = 0;
+    for (int n = 0; n <= nmax; n++) dsz += (size_t)(2 * nmin + 1) * (2 * n + 1);
+    size_t z = (size_t)(nmax + L + 4) * 3;                       // xi + Bessel scratch
+    size_t dbl = dsz + 1 + 2 * (2 * nmax + 3) + 8;                // D + dk arrays
+    size_t zz = 2 * (size_t)T * L + 2 * (size_t)T * (2 * nmin + 1) + 2 * (size_t)L * (2 * nmin + 1);
+    return z + (dbl + 1) / 2 + zz + 8;                            // in zd units
+}
+
+void launch_merge(const MergeArgs& a, int grid, cudaStream_t st)
+{
+    merge_kernel<<<grid, PP_NT, 0, st>>>(a);
+    launch_counter() += 1;
+}
+
+int fosm_grid(int ntot) { return std::min(ntot * ntot, 148 * 8); }
+size_t fosm_scratch_doubles(int ntot) { return (size_t)fosm_grid(ntot) * 32 * 5 * (2 * ntot + 2); }
+size_t fosmcalc_scratch_doubles(int ntot, int nang) { return (size_t)nang * (16 * (2 * ntot) + 40); }
+
+void launch_fosm(int ntot, const zd* a0, const double* bcof, const double* fnr, int nbc, double* s00, double* s02, double* sp22,
+                 double* sm22, double* vscr, cudaStream_t st)
+{
+    VCTab t{bcof, fnr, nbc};
+    fosm_kernel<<<fosm_grid(ntot), 32, 0, st>>>(ntot, a0, t, s00, s02, sp22, sm22, vscr);
+    fosm_patch_kernel<<<(2 * ntot + 1 + 63) / 64, 64, 0, st>>>(ntot, s00, s02, sp22, sm22, 1.0);
+    launch_counter() += 2;
+}
+
+void launch_fosmcalc(int ntot, int nang, const double* s00, const double* s02, const double* sp22, const double* sm22,
+                     const double* fnr, const double* bcofd, double* dscr, double* smat, cudaStream_t st)
+{
+    fosmcalc_kernel<<<nang, 128, 0, st>>>(ntot, nang, s00, s02, sp22, sm22, fnr, bcofd, dscr, smat);
+    launch_counter() += 1;
+}

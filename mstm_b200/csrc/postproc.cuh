@@ -1,0 +1,41 @@
+// postproc.cuh -- device post-processing launchers (see postproc.cu).
+#pragma once
+#include "common.cuh"
+#include <cstddef>
+
+struct MergeArgs {
+    int nsph;
+    const double* pos;
+    const int* order;
+    const int* offset;
+    const int* tord;        // translation order per sphere (already capped)
+    int T;                  // t_matrix_order
+    double r0[3];
+    double rimed_re, rimed_im;
+    const zd* amnp;         // ld x npol, LR basis
+    int ld, npol;
+    zd* amnp0;              // ld0 x npol, TE/TM basis, accumulated (zeroed by the caller)
+    int ld0;
+    const double* vcc;      // vcc_const slice (n <= vcT, ml <= vcML, w <= vcT + L)
+    int vcT, vcML;
+    const double* fnm1;     // (-fcN..fcN, 1..fcN)
+    const double* fnc;
+    const double* fnp1;
+    int fcN;
+    const double* fnr;
+    const double* bcofd;
+    zd* scratch;
+    size_t scratch_stride;  // zd units per CTA
+};
+
+void launch_tranorder(int nsph, const double* pos, const int* order, const double* origin, double rire, double eps, int maxt,
+                      const double* bcof, const double* fnr, int nbc, zd* scratch, int sstride, int* tord, cudaStream_t st);
+size_t merge_scratch_per_cta(int T, int L);
+void launch_merge(const MergeArgs& a, int grid, cudaStream_t st);
+int fosm_grid(int ntot);
+size_t fosm_scratch_doubles(int ntot);
+size_t fosmcalc_scratch_doubles(int ntot, int nang);
+void launch_fosm(int ntot, const zd* a0, const double* bcof, const double* fnr, int nbc, double* s00, double* s02, double* sp22,
+                 double* sm22, double* vscr, cudaStream_t st);
+void launch_fosmcalc(int ntot, int nang, const double* s00, const double* s02, const double* sp22, const double* sm22,
+                     const double* fnr, const double* bcofd, double* dscr, double* smat, cudaStream_t st);

@@ -1603,3 +1603,227 @@ void orc_x_crichankel(int n, double zr, double zi, cplx *xi) { crichankel(n, zr 
 void orc_x_direct_solve(orc_ctx *c, const cplx *pnp, cplx *anp) { direct_solve(c, pnp, anp); }
 void orc_x_multmie(orc_ctx *c, int idir, const cplx *ain, cplx *aout) { multmiecoeffmult(c, idir, ain, aout, c->an); }
 void orc_x_qeff(orc_ctx *c, const cplx *amnp, const cplx *pmnp0, double *qeff) { qefficiencyfactors(c, amnp, pmnp0, qeff); }
+
+/* ======================================================================== */
+/* Post-processing: common-origin expansion, GSF expansion, scattering matrix */
+/* ======================================================================== */
+static cplx ipow(int k) /* i**k for any integer k */
+{
+    int e = ((k % 4) + 4) % 4;
+    return (e == 0) ? 1.0 : (e == 1 ? CI : (e == 2 ? -1.0 : -CI));
+}
+
+/* tranordertest (modules:1896-1942): order needed to translate a sphere of
+ * order lmax over distance r with regular functions to accuracy eps. */
+int orc_tranordertest(double r, double ri_re, int lmax, double eps)
+{
+    tables_init();
+    const int nlim = 200;
+    if (r == 0.0) return lmax;
+    cplx z = r * ri_re;
+    double sum = 0.0;
+    cplx *xi = (cplx *)malloc(sizeof(cplx) * (nlim + lmax + 2));
+    double *vc1 = (double *)malloc(sizeof(double) * (nlim + lmax + 2));
+    int n;
+    for (n = 1; n <= nlim; n++) {
+        cricbessel(n + lmax, z, xi);
+        for (int l = 0; l <= n + lmax; l++) xi[l] = xi[l] / z * ipow(l);
+        int n21 = n + n + 1, l = lmax;
+        cplx c = FNR(n21) * FNR(l + l + 1) * ipow(n - l);
+        vcfunc(-1, n, 1, l, vc1);
+        int wmin = iabs_(n - l), wmax = n + l;
+        cplx a = 0, b = 0;
+        for (int w = wmin; w <= wmax; w++) {
+            double alnw = vc1[w] * vc1[w];
+            if ((n + l + w) % 2 == 0) a = a + alnw * xi[w];
+            else b = b + alnw * xi[w];
+        }
+        a = c * a;
+        b = c * b;
+        sum = creal(sum + a * conj(a) + b * conj(b));
+        if (fabs(1.0 - sum) < eps) break;
+    }
+    free(xi); free(vc1);
+    int nmax = n < nlim ? n : nlim;
+    return nmax > lmax ? nmax : lmax;
+}
+
+/* cluster origin, translation orders and t_matrix_order as main_calling_program
+ * sets them (input:1159-1197): origin = mean external position, orders from
+ * tranordertest with translation_epsilon, capped at max_t_matrix_order. */
+int orc_t_matrix_order(const orc_ctx *c, double trans_eps, int maxt, double *origin, int *trans_order)
+{
+    double r0[3] = {0, 0, 0};
+    for (int i = 0; i < c->n; i++)
+        for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->pos[3 * i + k];
+    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)c->n;
+    int tmo = imin(c->max_order, maxt);
+    for (int i = 0; i < c->n; i++) {
+        double d2 = 0.0;
+        for (int k = 0; k < 3; k++) d2 += (c->pos[3 * i + k] - r0[k]) * (c->pos[3 * i + k] - r0[k]);
+        int to = orc_tranordertest(sqrt(d2), creal(c->rimed), c->order[i], trans_eps);
+        to = imin(to, maxt);
+        trans_order[i] = to;
+        tmo = imax(tmo, to);
+    }
+    for (int k = 0; k < 3; k++) origin[k] = r0[k];
+    return tmo;
+}
+
+/* merge_to_common_origin (scatprops:447-559), one right-hand side: regular (J)
+ * translation of each sphere's expansion to r0, converted LR -> TE/TM.
+ * amnp0 is the nodrt block a(0:nodrt+1,1:nodrt,1:2). */
+void orc_merge_to_common_origin(const orc_ctx *c, int nodrt, const cplx *amnp, const double *r0, const int *trans_order,
+                                cplx *amnp0)
+{
+    int nb0 = 2 * nodrt * (nodrt + 2);
+    for (int k = 0; k < nb0; k++) amnp0[k] = 0;
+    axialtrancoefinit(imax(nodrt, c->max_order));
+    for (int i = 0; i < c->n; i++) {
+        int noi = c->order[i];
+        int ntrani = imin(nodrt, trans_order[i]);
+        int nbt = 2 * ntrani * (ntrani + 2);
+        cplx *amnpt = (cplx *)calloc(nbt, sizeof(cplx));
+        double rv[3] = {r0[0] - c->pos[3 * i], r0[1] - c->pos[3 * i + 1], r0[2] - c->pos[3 * i + 2]};
+        pairop_t op;
+        pairop_compute(&op, ntrani, noi, rv, 1, c->rimed);
+        coefficient_translation(noi, ntrani, amnp + c->offset[i], amnpt, &op, 0, 0);
+        pairop_free(&op);
+        for (int n = 1; n <= ntrani; n++)
+            for (int m = 0; m <= ntrani + 1; m++) {
+                cplx t1 = amnpt[m + (ntrani + 2) * (n - 1)];
+                cplx t2 = amnpt[m + (ntrani + 2) * (n - 1) + (ntrani + 2) * ntrani];
+                amnp0[m + (nodrt + 2) * (n - 1)] = amnp0[m + (nodrt + 2) * (n - 1)] + t1 + t2;
+                amnp0[m + (nodrt + 2) * (n - 1) + (nodrt + 2) * nodrt] = amnp0[m + (nodrt + 2) * (n - 1) + (nodrt + 2) * nodrt] + t1 - t2;
+            }
+        free(amnpt);
+    }
+}
+
+/* fosmexpansion (scatprops:1820-1951): GSF expansion coefficients of the
+ * azimuth-averaged scattering matrix.  amnp0: (nb(ntot), 2 polarisations).
+ * s00..sm22: 16*(2ntot+1) each, Fortran (4,4,0:2ntot) order. */
+void orc_fosmexpansion(int ntot, const cplx *amnp0, double *s00, double *s02, double *sp22, double *sm22)
+{
+    tables_init();
+    int nb = 2 * ntot * (ntot + 2);
+    int W = 2 * ntot + 1;
+    int ldm = 2 * ntot + 5;   /* m from -ntot-2..ntot+2 */
+    cplx *a1 = (cplx *)calloc((size_t)ldm * ntot * 2, sizeof(cplx));
+    cplx *a2 = (cplx *)calloc((size_t)ldm * ntot * 2, sizeof(cplx));
+#define AA(arr, m, n, p) arr[((m) + ntot + 2) + ldm * (((n) - 1) + ntot * (p))]
+    for (int n = 1; n <= ntot; n++)
+        for (int p = 0; p < 2; p++)
+            for (int m = -n; m <= n; m++) {
+                int s = (m < 0) ? ((n + 1) + (ntot + 2) * (-m - 1)) : (m + (ntot + 2) * (n - 1));
+                AA(a1, m, n, p) = amnp0[s + (ntot + 2) * ntot * p];
+                AA(a2, m, n, p) = amnp0[nb + s + (ntot + 2) * ntot * p];
+            }
+    for (int k = 0; k < 16 * W; k++) { s00[k] = 0; s02[k] = 0; sp22[k] = 0; sm22[k] = 0; }
+#define SS(arr, i, j, w) arr[((i) - 1) + 4 * ((j) - 1) + 16 * (w)]
+    double *cm1p1 = (double *)malloc(sizeof(double) * (2 * ntot + 2));
+    double *cm1m1 = (double *)malloc(sizeof(double) * (2 * ntot + 2));
+    double *cmmpm = (double *)malloc(sizeof(double) * (2 * ntot + 2));
+    double *cmmm2pm = (double *)malloc(sizeof(double) * (2 * ntot + 2));
+    double *cmmp2pm = (double *)malloc(sizeof(double) * (2 * ntot + 2));
+    for (int n = 1; n <= ntot; n++)
+        for (int l = 1; l <= ntot; l++) {
+            int wmin = iabs_(n - l), wmax = n + l;
+            cplx fnl = sqrt((double)((n + n + 1) * (l + l + 1))) * ipow(l - n);
+            vcfunc(-1, n, 1, l, cm1p1);
+            vcfunc(-1, n, -1, l, cm1m1);
+            int mm = imin(n, l + 2);
+            for (int m = -mm; m <= mm; m++) {
+                double m1m = pm1(m);
+                if (iabs_(m) <= l) vcfunc(-m, n, m, l, cmmpm);
+                else for (int w = 0; w <= n + l; w++) cmmpm[w] = 0.0;
+                if (iabs_(-2 + m) <= l) vcfunc(-m, n, -2 + m, l, cmmm2pm);
+                else for (int w = 0; w <= n + l; w++) cmmm2pm[w] = 0.0;
+                if (iabs_(2 + m) <= l) vcfunc(-m, n, 2 + m, l, cmmp2pm);
+                else for (int w = 0; w <= n + l; w++) cmmp2pm[w] = 0.0;
+                for (int p = 1; p <= 2; p++)
+                    for (int q = 1; q <= 2; q++) {
+                        double m1mq = pm1(m + q);
+                        double m1mnpl = pm1(m + n + p + l);
+                        cplx a1122 = AA(a1, m, n, p - 1) * conj(AA(a1, m, l, q - 1)) + AA(a2, m, n, p - 1) * conj(AA(a2, m, l, q - 1));
+                        cplx a2112 = AA(a2, m, n, p - 1) * conj(AA(a1, m, l, q - 1)) - AA(a1, m, n, p - 1) * conj(AA(a2, m, l, q - 1));
+                        cplx a1p2 = (AA(a1, m, n, p - 1) + CI * AA(a2, m, n, p - 1)) * conj(AA(a1, m - 2, l, q - 1) - CI * AA(a2, m - 2, l, q - 1));
+                        cplx a1m2 = (AA(a1, m, n, p - 1) - CI * AA(a2, m, n, p - 1)) * conj(AA(a1, m + 2, l, q - 1) + CI * AA(a2, m + 2, l, q - 1));
+                        for (int w = wmin; w <= wmax; w++) {
+                            double m1w = pm1(w);
+                            int ev = ((n + l + w + p + q) % 2 == 0);
+                            if (ev) SS(s00, 1, 1, w) = SS(s00, 1, 1, w) - creal(m1m * fnl * a1122 * cm1p1[w] * cmmpm[w]) / 2.0;
+                            else SS(s00, 4, 4, w) = SS(s00, 4, 4, w) + creal(CI / 2.0 * m1m * fnl * a2112 * cm1p1[w] * cmmpm[w]);
+                            if (w < 2) continue;
+                            if (ev) {
+                                SS(s02, 2, 1, w) = SS(s02, 2, 1, w) - creal(m1mq * a1122 * fnl * cm1m1[w] * cmmpm[w]) / 2.0;
+                                SS(s02, 1, 2, w) = SS(s02, 1, 2, w) - creal(m1m * a1p2 * fnl * cm1p1[w] * cmmm2pm[w]) / 4.0;
+                                SS(s02, 1, 2, w) = SS(s02, 1, 2, w) - creal(m1m * a1m2 * fnl * cm1p1[w] * cmmp2pm[w]) / 4.0;
+                            } else {
+                                SS(s02, 3, 4, w) = SS(s02, 3, 4, w) + cimag(-CI / 2.0 * m1mq * a2112 * fnl * cm1m1[w] * cmmpm[w]);
+                                SS(s02, 4, 3, w) = SS(s02, 4, 3, w) + cimag(m1m * a1p2 * fnl * cm1p1[w] * cmmm2pm[w]) / 4.0;
+                                SS(s02, 4, 3, w) = SS(s02, 4, 3, w) - cimag(m1m * a1m2 * fnl * cm1p1[w] * cmmp2pm[w]) / 4.0;
+                            }
+                            SS(sm22, 2, 2, w) = SS(sm22, 2, 2, w) - creal(m1mnpl * m1w * a1p2 * fnl * cm1m1[w] * cmmm2pm[w]) / 8.0;
+                            SS(sp22, 2, 2, w) = SS(sp22, 2, 2, w) - creal(m1mq * a1p2 * fnl * cm1m1[w] * cmmm2pm[w]) / 8.0;
+                            SS(sm22, 2, 2, w) = SS(sm22, 2, 2, w) - creal(m1mq * a1m2 * fnl * cm1m1[w] * cmmp2pm[w]) / 8.0;
+                            SS(sp22, 2, 2, w) = SS(sp22, 2, 2, w) - creal(m1mnpl * m1w * a1m2 * fnl * cm1m1[w] * cmmp2pm[w]) / 8.0;
+                        }
+                    }
+            }
+        }
+    for (int i = 3; i <= 4; i++)
+        for (int j = 1; j <= i; j++)
+            for (int w = 0; w < W; w++) {
+                SS(s00, j, i, w) = -SS(s00, j, i, w);
+                SS(s02, j, i, w) = -SS(s02, j, i, w);
+                SS(sm22, j, i, w) = -SS(sm22, j, i, w);
+                SS(sp22, j, i, w) = -SS(sp22, j, i, w);
+            }
+    for (int w = 0; w < W; w++) {
+        SS(sm22, 3, 3, w) = -SS(sm22, 2, 2, w);
+        SS(sp22, 3, 3, w) = SS(sp22, 2, 2, w);
+    }
+    for (int k = 0; k < 16 * W; k++) {
+        s00[k] = 0.5 * s00[k] / 1.0;
+        s02[k] = 0.5 * s02[k] / 1.0;
+        sm22[k] = 0.5 * sm22[k] / 1.0;
+        sp22[k] = 0.5 * sp22[k] / 1.0;
+    }
+#undef AA
+#undef SS
+    free(a1); free(a2); free(cm1p1); free(cm1m1); free(cmmpm); free(cmmm2pm); free(cmmp2pm);
+}
+
+/* fosmcalc (scatprops:1750-1810), normalize_s11 = .false.: sm(4,4) Fortran order. */
+void orc_fosmcalc(int ntot, const double *s00, const double *s02, const double *sp22, const double *sm22, double ct, double *sm)
+{
+    tables_init();
+    int kmax = 2, nmax = 2 * ntot;
+    double *dc = (double *)malloc(sizeof(double) * 5 * (nmax * (nmax + 2) + 1));
+    rotcoef(ct, kmax, nmax, dc);
+#define DC(m, nk) dc[((m) + 2) + 5 * (nk)]
+    for (int k = 0; k < 16; k++) sm[k] = 0.0;
+    for (int w = 0; w <= 2 * ntot; w++) {
+        int ww1 = w * (w + 1);
+        for (int k = 0; k < 16; k++) {
+            double v = s00[k + 16 * w] * DC(0, ww1);
+            v = v + s02[k + 16 * w] * DC(0, ww1 + 2) + sp22[k + 16 * w] * DC(2, ww1 + 2) + sm22[k + 16 * w] * DC(-2, ww1 + 2);
+            sm[k] = sm[k] + v;
+        }
+    }
+#undef DC
+#define SM(i, j) sm[((i) - 1) + 4 * ((j) - 1)]
+    SM(3, 1) = -SM(3, 1);
+    SM(1, 3) = -SM(1, 3);
+    SM(4, 3) = -SM(4, 3);
+    double temp = SM(4, 1);
+    SM(4, 1) = SM(4, 2);
+    SM(4, 2) = temp;
+    SM(1, 2) = (SM(1, 2) + SM(2, 1)) / 2.0;
+    SM(2, 1) = SM(1, 2);
+    SM(3, 4) = (SM(3, 4) - SM(4, 3)) / 2.0;
+    SM(4, 3) = -SM(3, 4);
+#undef SM
+    free(dc);
+}

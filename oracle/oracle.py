@@ -65,6 +65,13 @@ def lib():
         L.orc_x_direct_solve.argtypes = [c_void_p, c_void_p, c_void_p]
         L.orc_x_multmie.argtypes = [c_void_p, c_int, c_void_p, c_void_p]
         L.orc_x_qeff.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
+        L.orc_tranordertest.argtypes = [c_double, c_double, c_int, c_double]
+        L.orc_tranordertest.restype = c_int
+        L.orc_t_matrix_order.argtypes = [c_void_p, c_double, c_int, c_void_p, c_void_p]
+        L.orc_t_matrix_order.restype = c_int
+        L.orc_merge_to_common_origin.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]
+        L.orc_fosmexpansion.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+        L.orc_fosmcalc.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_void_p]
         _lib = L
     return _lib
 
@@ -166,6 +173,54 @@ class Oracle:
 
     def vol_radius(self):
         return self.L.orc_vol_radius(self.ctx)
+
+    def t_matrix_order(self, trans_eps=1.0e-5, maxt=100):
+        origin = np.zeros(3)
+        to = np.zeros(self.n, np.int32)
+        nt = self.L.orc_t_matrix_order(self.ctx, trans_eps, maxt, _p(origin), _p(to))
+        return nt, origin, to
+
+    def merge_to_common_origin(self, amnp, nodrt, origin, trans_order):
+        """amnp: (neqns, npol) -> (nb(nodrt), npol) common-origin TE/TM coefficients."""
+        amnp = np.asfortranarray(amnp, np.complex128)
+        nb = 2 * nodrt * (nodrt + 2)
+        out = np.zeros((nb, amnp.shape[1]), np.complex128, order="F")
+        to = np.ascontiguousarray(trans_order, np.int32)
+        r0 = np.ascontiguousarray(origin, np.float64)
+        for p in range(amnp.shape[1]):
+            col = np.ascontiguousarray(amnp[:, p])
+            o = np.zeros(nb, np.complex128)
+            self.L.orc_merge_to_common_origin(self.ctx, nodrt, _p(col), _p(r0), _p(to), _p(o))
+            out[:, p] = o
+        return out
+
+    def scattering(self, amnp, trans_eps=1.0e-5, maxt=100, nangles=181):
+        """fosmexpansion + fosmcalc: returns dict(ntot, s00.., g, smat (nangles,4,4))."""
+        nt, origin, to = self.t_matrix_order(trans_eps, maxt)
+        a0 = self.merge_to_common_origin(amnp, nt, origin, to)
+        return gsf_scattering(nt, a0, nangles) | dict(t_matrix_order=nt, amnp0=a0)
+
+
+def gsf_scattering(nt, a0, nangles=181):
+    L = lib()
+    W = 2 * nt + 1
+    s = [np.zeros(16 * W) for _ in range(4)]
+    a0 = np.asfortranarray(a0, np.complex128)
+    L.orc_fosmexpansion(nt, _p(a0), _p(s[0]), _p(s[1]), _p(s[2]), _p(s[3]))
+    smat = np.zeros((nangles, 4, 4))
+    pi_ref = float(np.float32(np.pi))
+    for i in range(nangles):
+        ct = np.cos(pi_ref / 180.0 * (0.0 + 180.0 * (i / (nangles - 1))))
+        if ct == 1.0:
+            ct = 0.9999999
+        if ct == -1.0:
+            ct = -0.9999999
+        sm = np.zeros(16)
+        L.orc_fosmcalc(nt, _p(s[0]), _p(s[1]), _p(s[2]), _p(s[3]), ct, _p(sm))
+        smat[i] = sm.reshape(4, 4, order="F")
+    s00 = s[0].reshape(W, 4, 4).transpose(0, 2, 1)   # [w][i][j]
+    g = s00[1, 0, 0] / (3.0 * s00[0, 0, 0])
+    return dict(s00=s[0], s02=s[1], sp22=s[2], sm22=s[3], g=g, smat=smat)
 
 
 def rotcoef(cbe, kmax, nmax):

@@ -179,3 +179,26 @@ def _mie_times(g, f):
                 y[1, col - 1, row] = a[0, 1] * blk[0, col - 1, row] + a[1, 1] * blk[1, col - 1, row]
         out[off[i]:off[i + 1]] = y.reshape(-1, f.shape[1])
     return out
+
+
+@pytest.mark.parametrize("name", ["cluster20", "fractal60"])
+def test_scattering_postprocessing(api, oracle_mod, name):
+    """merge_to_common_origin + fosmexpansion + fosmcalc on the device vs the
+    oracle, fed the same solution, then end to end (device solve + device
+    post-processing vs oracle solve + oracle post-processing)."""
+    pos, rad, ri, em = _cluster(name)
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em)
+    ro = o.fixedorsoln(eps=1e-12, niter=4000)
+    so = o.scattering(ro["amnp"])
+    sg = g.scattering(ro["amnp"])
+    assert sg["t_matrix_order"] == so["t_matrix_order"]
+    s11max = np.abs(so["smat"][:, 0, 0]).max()
+    assert np.abs(sg["smat"] - so["smat"]).max() <= 1e-9 * s11max
+    assert abs(sg["g"] - so["g"]) <= 1e-10
+    rg = g.fixedorsoln(eps=1e-12, niter=4000)
+    sge = g.scattering(rg["amnp"])
+    assert np.abs(sge["smat"] - so["smat"]).max() <= 1e-8 * s11max
+    gm = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed")
+    sgm = gm.scattering(gm.fixedorsoln(eps=1e-12, niter=4000)["amnp"])
+    assert np.abs(sgm["smat"] - so["smat"]).max() <= 1e-4 * s11max
+    assert abs(sgm["g"] - so["g"]) <= 1e-6

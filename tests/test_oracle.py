@@ -132,3 +132,60 @@ def test_store_and_recompute_modes_agree(oracle_mod):
     ya = a.sphereinteraction(x, con_tran=[0, 1], initial_run=True)
     yb = b.sphereinteraction(x, con_tran=[0, 1], initial_run=True)
     assert np.abs(ya - yb).max() <= 1e-13 * np.abs(ya).max()
+
+
+def _bh_ab(x, m, N):
+    from scipy.special import spherical_jn, spherical_yn
+    n = np.arange(1, N + 1)
+    psi = lambda z: z * spherical_jn(n, z)
+    dpsi = lambda z: spherical_jn(n, z) + z * spherical_jn(n, z, derivative=True)
+    xi = lambda z: z * (spherical_jn(n, z) + 1j * spherical_yn(n, z))
+    dxi = lambda z: (spherical_jn(n, z) + 1j * spherical_yn(n, z)) + z * (
+        spherical_jn(n, z, derivative=True) + 1j * spherical_yn(n, z, derivative=True))
+    mx = m * x
+    a = (m * psi(mx) * dpsi(x) - psi(x) * dpsi(mx)) / (m * psi(mx) * dxi(x) - xi(x) * dpsi(mx))
+    b = (psi(mx) * dpsi(x) - m * psi(x) * dpsi(mx)) / (psi(mx) * dxi(x) - m * xi(x) * dpsi(mx))
+    return a, b
+
+
+def test_single_sphere_scattering_matrix_and_g_equal_mie(oracle_mod):
+    """fosmexpansion/fosmcalc of a lone sphere: S11 = (|S1|^2+|S2|^2)/2 and g of Mie theory."""
+    x, m, L = 1.0, 1.5 + 0.01j, 7
+    o = oracle_mod.Oracle([[0.0, 0.0, 0.0]], [x], [m], mie_eps=-L)
+    r = o.fixedorsoln()
+    sc = o.scattering(r["amnp"])
+    a, b = _bh_ab(x, m, L)
+    n = np.arange(1, L + 1)
+    qs = 2 / x ** 2 * np.sum((2 * n + 1) * (abs(a) ** 2 + abs(b) ** 2))
+    g = 4 / (x ** 2 * qs) * (np.sum(n[:-1] * (n[:-1] + 2) / (n[:-1] + 1) * np.real(a[:-1] * np.conj(a[1:]) + b[:-1] * np.conj(b[1:])))
+                             + np.sum((2 * n + 1) / (n * (n + 1)) * np.real(a * np.conj(b))))
+    assert abs(sc["g"] / g - 1) < 1e-12
+    pi_ref = float(np.float32(np.pi))
+    for i in [0, 30, 90, 150, 180]:
+        ct = np.cos(pi_ref / 180.0 * (180.0 * (i / 180.0)))   # scattering_matrix_calculation's angle
+        ct = 0.9999999 if ct == 1.0 else (-0.9999999 if ct == -1.0 else ct)
+        # Mie S1, S2 by the pi/tau recurrences
+        pi0, pi1 = 0.0, 1.0
+        S1 = S2 = 0.0
+        for k in range(1, L + 1):
+            if k > 1:
+                pk = ((2 * k - 1) * ct * pi1 - k * pi0) / (k - 1)
+                pi0, pi1 = pi1, pk
+            tau = k * ct * pi1 - (k + 1) * pi0
+            S1 += (2 * k + 1) / (k * (k + 1)) * (a[k - 1] * pi1 + b[k - 1] * tau)
+            S2 += (2 * k + 1) / (k * (k + 1)) * (a[k - 1] * tau + b[k - 1] * pi1)
+        s11 = 0.5 * (abs(S1) ** 2 + abs(S2) ** 2)
+        assert abs(sc["smat"][i, 0, 0] / s11 - 1) < 1e-9
+        s12 = 0.5 * (abs(S2) ** 2 - abs(S1) ** 2)
+        assert abs(sc["smat"][i, 0, 1] - s12) < 1e-9 * s11
+
+
+def test_scattering_invariant_under_cluster_shift(oracle_mod):
+    pos = _small_cluster()
+    o1 = oracle_mod.Oracle(pos, [1.0] * 5, [1.5 + 0.01j] * 5, mie_eps=-7)
+    o2 = oracle_mod.Oracle(pos + np.array([0.0, 0.0, 3.7]), [1.0] * 5, [1.5 + 0.01j] * 5, mie_eps=-7)
+    s1 = o1.scattering(o1.fixedorsoln(eps=1e-14)["amnp"])
+    s2 = o2.scattering(o2.fixedorsoln(eps=1e-14)["amnp"])
+    assert s1["t_matrix_order"] == s2["t_matrix_order"]
+    assert abs(s1["g"] - s2["g"]) < 1e-9
+    assert np.abs(s1["smat"] - s2["smat"]).max() < 1e-8 * np.abs(s1["smat"][:, 0, 0]).max()
