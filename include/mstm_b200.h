@@ -115,6 +115,44 @@ int mstmg_fixed_orientation(mstmg_ctx *ctx, double alpha, double sinc, int dir, 
 int mstmg_scattering(mstmg_ctx *ctx, const double *amnp, double trans_eps, int max_t_order, int nangles, double *smat, double *g,
                      int *t_matrix_order, double *amnp0, int amnp0_cap);
 
+/* Order of the cluster T matrix about the cluster origin (the mean sphere
+ * position): replaces the t_matrix_order set-up of main_calling_program
+ * (mstm-input-37.f90:1179-1197), tranordertest (mstm-modules-33.f90:1896-1942)
+ * per sphere with trans_eps (translation_epsilon), capped at max_t_order
+ * (max_t_matrix_order).  Keeps each sphere's translation order in the context
+ * for mstmg_tmatrix. */
+int mstmg_t_matrix_order(mstmg_ctx *ctx, double trans_eps, int max_t_order, int *t_matrix_order);
+
+/* Replaces tmatrix_solution (mstm-solver-8.f90:22-332) with the iterative
+ * solver, one process: for l = 1..t_matrix_order the 2(2l+1) unit TE/TM
+ * common-origin fields of order l are distributed to the spheres
+ * (distribute_from_common_origin, mstm-scatprops-26.f90:561-669), multiplied by
+ * the Mie coefficients and solved together (each column stops where cbicg
+ * stops it, solution_eps, max_iterations), merged back to the origin
+ * (merge_to_common_origin) and stored as T-matrix columns; the order loop stops
+ * after the order at which the summed extinction changes by less than
+ * convergence_eps (signed difference, as the reference; <= 0 disables).
+ * mstmg_t_matrix_order must have been called on the context.  With
+ * MSTMG_PRECISION_MIXED the column solves are FP32 BiCG inside FP64
+ * refinement.
+ *   tmat: nblkt x nblkt complex, column-major, nblkt = 2 T (T+2), T =
+ *     t_matrix_order: column 2(l(l+1)+k-1)+q-1, row 2(n(n+1)+m-1)+p-1, rows with
+ *     n > l zero (the entries the reference's T-matrix file holds);
+ *   sphere_qeff: 3 x N (ext, abs, sca) summed over the columns (the
+ *     reference's sphere_qeff); qtot[3]: their area-weighted totals with
+ *     Qsca = Qext + Qinc - Qabs (qtotcalc); order_used: the order kept;
+ *   maxiter, maxerr: over all column solves.
+ * Returns 0, MSTMG_NOT_CONVERGED (solution_status = 1) or an error. */
+int mstmg_tmatrix(mstmg_ctx *ctx, int t_matrix_order, double solution_eps, double convergence_eps, int max_iterations,
+                  double *tmat, double *sphere_qeff, double *qtot, int *order_used, int *maxiter, double *maxerr);
+
+/* Orientation-averaged Qext and Qsca from a T matrix as ranorientscatmatrix
+ * forms them after reading the T-matrix file (mstm-scatprops-26.f90:2031-2122):
+ * entries rounded to single precision, rows of order n > l filled by the
+ * T-matrix symmetry, Qext = -2/xv^2 sum Re T(q,kl,q,kl), Qsca = 2/xv^2 sum |T|^2,
+ * xv = the context's volume-equivalent radius (cross_section_radius). */
+int mstmg_tmatrix_qext_qsca(mstmg_ctx *ctx, int t_matrix_order, const double *tmat, double *qext, double *qsca);
+
 /* Statistics of the last solve: iterations per polarisation, refinement steps,
  * FP64 and FP32 operator passes. */
 int mstmg_last_stats(const mstmg_ctx *ctx, int *iters2, int *outer, int *passes64, int *passes32);

@@ -31,6 +31,10 @@ SIGNATURES = {
                                         P(c_double), P(c_int)]),
     "mstmg_scattering": (c_int, [c_void_p, c_void_p, c_double, c_int, c_int, c_void_p, P(c_double), P(c_int), c_void_p,
                                  c_int]),
+    "mstmg_t_matrix_order": (c_int, [c_void_p, c_double, c_int, P(c_int)]),
+    "mstmg_tmatrix": (c_int, [c_void_p, c_int, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p, P(c_int), P(c_int),
+                              P(c_double)]),
+    "mstmg_tmatrix_qext_qsca": (c_int, [c_void_p, c_int, c_void_p, P(c_double), P(c_double)]),
     "mstmg_last_stats": (c_int, [c_void_p, c_void_p, P(c_int), P(c_int), P(c_int)]),
     "mstmg_operator_bytes": (c_int, [c_void_p, c_int, P(c_double), P(c_double)]),
     "mstmg_time_translation": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),

@@ -150,6 +150,48 @@ class SphereCluster:
                                        ctypes.byref(tmo), None, 0), "scattering")
         return dict(smat=smat.reshape(nangles, 4, 4).transpose(0, 2, 1).copy(), g=g.value, t_matrix_order=tmo.value)
 
+    def t_matrix_order(self, trans_eps=1.0e-5, max_t_order=100):
+        """Order of the cluster T matrix about the cluster origin (tranordertest for
+        every sphere, mstm-modules-33.f90:1896-1942); also fixes the per-sphere
+        translation orders that tmatrix_solution uses."""
+        t = c_int(0)
+        check(self._L.mstmg_t_matrix_order(self.ctx, trans_eps, max_t_order, ctypes.byref(t)), "t_matrix_order")
+        return t.value
+
+    def tmatrix_solution(self, t_matrix_order=None, solution_eps=1.0e-6, convergence_eps=1.0e-6, max_iterations=10000,
+                         trans_eps=1.0e-5, max_t_order=100):
+        """tmatrix_solution (mstm-solver-8.f90:22-332): the cluster T matrix,
+        (nblkt, nblkt) complex with nblkt = 2 T (T+2), column 2(l(l+1)+k-1)+q-1 for
+        the unit TE (q=1) / TM (q=2) field of degree k and order l, rows
+        2(n(n+1)+m-1)+p-1 (rows of order n > l are left zero, as the reference
+        writes them); plus the per-sphere efficiencies summed over the columns
+        (3, N), the orientation-averaged (Qext, Qabs, Qsca), the order kept
+        (the loop stops once Qext changes by less than convergence_eps), and
+        the largest iteration count and residual of the column solves."""
+        if t_matrix_order is None:
+            t_matrix_order = self.t_matrix_order(trans_eps, max_t_order)
+        T = int(t_matrix_order)
+        nb = 2 * T * (T + 2)
+        tm = np.zeros((nb, nb), np.complex128, order="F")
+        sq = np.zeros((3, self.number_spheres), np.float64, order="F")
+        qt = np.zeros(3)
+        used, mi, me = c_int(0), c_int(0), c_double(0.0)
+        st = self._L.mstmg_tmatrix(self.ctx, T, solution_eps, convergence_eps, max_iterations, _ptr(tm), _ptr(sq), _ptr(qt),
+                                   ctypes.byref(used), ctypes.byref(mi), ctypes.byref(me))
+        if st < 0:
+            check(st, "tmatrix")
+        return dict(tmat=tm, t_matrix_order=T, order=used.value, sphere_qeff=sq, qtot=qt, istat=st, maxiter=mi.value,
+                    maxerr=me.value, outer=self.last_stats()["outer"])
+
+    def tmatrix_qext_qsca(self, tmat, t_matrix_order):
+        """Orientation-averaged Qext, Qsca from the T matrix as the random-orientation
+        reader forms them (mstm-scatprops-26.f90:2103-2122)."""
+        tmat = np.asfortranarray(tmat, np.complex128)
+        qe, qs = c_double(0.0), c_double(0.0)
+        check(self._L.mstmg_tmatrix_qext_qsca(self.ctx, int(t_matrix_order), _ptr(tmat), ctypes.byref(qe), ctypes.byref(qs)),
+              "tmatrix_qext_qsca")
+        return qe.value, qs.value
+
     def last_stats(self):
         it = np.zeros(2, np.int32)
         outer, p64, p32 = c_int(0), c_int(0), c_int(0)

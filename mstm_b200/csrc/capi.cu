@@ -14,6 +14,7 @@
 #include "tables.h"
 #include "translate_tiled.cuh"
 #include "postproc.cuh"
+#include "mrhs.cuh"
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
@@ -28,9 +29,14 @@ void mstmg_internal_set_error(const std::string& msg) { set_err(msg); }
         }                                                                                         \
     } while (0)
 
+// Owning device buffer (freed on destruction, not copyable).
 template <typename T> struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
     cudaError_t alloc(size_t count)
     {
         if (count <= n && p) return cudaSuccess;
@@ -85,6 +91,7 @@ struct mstmg_ctx {
     BicgScalars* h_sc = nullptr;
     double* h_small = nullptr;
     int iters[2] = {0, 0}, outer = 0, passes64 = 0, passes32 = 0;
+    std::vector<int> tord;   // translation order of each sphere to the cluster origin (mstmg_t_matrix_order)
     cudaStream_t own_st = nullptr;
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -518,10 +525,11 @@ template <typename T> static const T* ops_ptr(mstmg_ctx* c);
 template <> const double* ops_ptr<double>(mstmg_ctx* c) { return c->op64.p; }
 template <> const float* ops_ptr<float>(mstmg_ctx* c) { return c->op32.p; }
 
-// y[:, 0:nrhs] = H x[:, 0:nrhs]  (y zeroed here)
-template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran)
+// y[:, 0:nrhs*nchunk] = H x[:, 0:nrhs*nchunk]  (y zeroed here).  nchunk > 1
+// only on the tiled path: contran then applies to column r of every chunk.
+template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran, int nchunk = 1)
 {
-    CK(cudaMemsetAsync(y, 0, sizeof(cpx<T>) * (size_t)c->neqns * nrhs, c->st));
+    CK(cudaMemsetAsync(y, 0, sizeof(cpx<T>) * (size_t)c->neqns * nrhs * nchunk, c->st));
     if (c->npairs == 0) return MSTMG_OK;
     TransArgs<T> a;
     a.npairs = c->npairs;
@@ -549,10 +557,12 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
         ta.y = y;
         ta.ld = c->neqns;
         ta.nrhs = nrhs;
+        ta.nchunk = nchunk;
         ta.nsph = c->n;
         ta.contran = contran;
         ta.err = c->err.p;
     }
+    if (nchunk > 1 && !use_tiled) return MSTMG_ERR_UNSUPPORTED;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->timing) {
         for (cudaEvent_t* ev : {&e0, &e1}) {
@@ -561,7 +571,14 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
         }
         CK(cudaEventRecord(e0, c->st));
     }
-    if (!use_tiled || launch_translate_tiled<T>(ta, c->lmax, c->nsm, c->st) != 0) launch_translate<T>(a, c->nsm, c->st);
+    if (!use_tiled || launch_translate_tiled<T>(ta, c->lmax, c->nsm, c->st) != 0) {
+        if (nchunk > 1) {
+            if (e0) c->ev_pool.push_back(e0);
+            if (e1) c->ev_pool.push_back(e1);
+            return MSTMG_ERR_UNSUPPORTED;
+        }
+        launch_translate<T>(a, c->nsm, c->st);
+    }
     CK(cudaGetLastError());
     if (c->timing) {
         CK(cudaEventRecord(e1, c->st));
@@ -569,6 +586,34 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
     }
     if (sizeof(T) == 8) c->passes64++;
     else c->passes32++;
+    return MSTMG_OK;
+}
+
+// Many columns: y[:, 0:ncols] = H x[:, 0:ncols], where column k is a
+// conjugate-transpose product when bit (k & 1) of pattern2 is set (BiCG packs
+// [p_1, w_1, p_2, w_2, ...]: pattern2 = 2).  On the tiled path the columns go
+// in chunks of 4 (FP32) or 2 (FP64) through one launch; otherwise in groups of
+// up to 4 columns, one launch each.
+template <typename T> static int translate_many(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int ncols, unsigned pattern2)
+{
+    auto expand = [&](int w) {
+        unsigned m = 0;
+        for (int r = 0; r < w; r++)
+            if ((pattern2 >> (r & 1)) & 1u) m |= 1u << r;
+        return m;
+    };
+    const int NR = sizeof(T) == 4 ? 4 : 2;
+    if (c->tiled && ncols > NR && ncols % NR == 0 && tiled_supported(c->lmax, NR)) {
+        int rc = translate<T>(c, x, y, NR, expand(NR), ncols / NR);
+        if (rc != MSTMG_ERR_UNSUPPORTED) return rc;
+    }
+    if (ncols <= 4) return translate<T>(c, x, y, ncols, expand(ncols));
+    const size_t ld = (size_t)c->neqns;
+    for (int k = 0; k < ncols; k += 4) {
+        int w = std::min(4, ncols - k);
+        int rc = translate<T>(c, x + (size_t)k * ld, y + (size_t)k * ld, w, expand(w));
+        if (rc) return rc;
+    }
     return MSTMG_OK;
 }
 
@@ -932,6 +977,146 @@ extern "C" int mstmg_operator_bytes(const mstmg_ctx* c, int prec, double* stored
 // t_matrix_order, merge to the common origin, GSF expansion, azimuth-averaged
 // scattering matrix on nangles polar angles 0..180 deg, and g.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Cluster-origin post-processing and the T matrix
+// ---------------------------------------------------------------------------
+
+static mstmg::Tables& big_tables()
+{
+    static thread_local mstmg::Tables* big = nullptr;
+    if (!big) big = new mstmg::Tables(420);
+    return *big;
+}
+
+// Device copies of the bcof / sqrt tables of big_tables().
+struct BigTablesDev {
+    DevBuf<double> bc, fnr;
+    int nbc = 420;
+};
+static int upload_big(mstmg_ctx* c, BigTablesDev& d)
+{
+    mstmg::Tables& big = big_tables();
+    CK(d.bc.alloc(big.bcof.size()));
+    CK(d.fnr.alloc(big.fnr.size()));
+    CK(cudaMemcpyAsync(d.bc.p, big.bcof.data(), sizeof(double) * big.bcof.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(d.fnr.p, big.fnr.data(), sizeof(double) * big.fnr.size(), cudaMemcpyHostToDevice, c->st));
+    return MSTMG_OK;
+}
+
+// Cluster origin (mean position of the spheres) and the order each sphere
+// needs to reach it (tranordertest, modules:1896-1942, capped at max_t_order);
+// T = max(min(L, max_t_order), those orders)  (input:1179-1197).
+static int origin_orders(mstmg_ctx* c, const BigTablesDev& bt, double trans_eps, int max_t_order, double* r0, DevBuf<int>& dtord,
+                         std::vector<int>& tord, int* T)
+{
+    const int n = c->n;
+    r0[0] = r0[1] = r0[2] = 0.0;
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->hpos[3 * (size_t)i + k];
+    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)n;
+    DevBuf<zd> tscr;
+    const int sstride = 3 * (200 + MSTMG_LMAX + 4);
+    CK(dtord.alloc(n));
+    CK(tscr.alloc((size_t)n * sstride));
+    launch_tranorder(n, c->pos.p, c->d_order.p, r0, c->opts.medium_re, trans_eps, max_t_order, bt.bc.p, bt.fnr.p, bt.nbc, tscr.p, sstride,
+                     dtord.p, c->st);
+    tord.resize(n);
+    CK(cudaMemcpyAsync(tord.data(), dtord.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int t = std::min(c->lmax, max_t_order);
+    for (int i = 0; i < n; i++) t = std::max(t, tord[i]);
+    if (t > 200) {
+        set_err("t_matrix_order above 200 is not supported");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    *T = t;
+    return MSTMG_OK;
+}
+
+// Constant tables of a regular translation from source orders <= Ls to target
+// orders <= Tt (the vcc_const combination of axialtrancoefinit, modules:1680-1722,
+// the recurrence factors of axialtrancoefrecurrence up to max(Tt, Ls), and bcof(n,n)).
+struct RegTables {
+    DevBuf<double> vcc, f1, f2, f3, bcd;
+    int vcT = 0, vcML = 0, FN = 0;
+};
+static int build_reg_tables(mstmg_ctx* c, int Tt, int Ls, RegTables& r)
+{
+    mstmg::Tables& big = big_tables();
+    std::vector<double> vcc((size_t)Tt * Ls * (Ls + 2) * (Tt + Ls + 1), 0.0), vc1(2 * (Tt + Ls) + 4), vc2(2 * (Tt + Ls) + 4);
+    for (int nn = 1; nn <= Tt; nn++)
+        for (int l = 1; l <= Ls; l++) {
+            double c1 = big.fnr[nn + nn + 1] * big.fnr[l + l + 1];
+            big.vcfunc(-1, nn, 1, l, vc2.data());
+            int wmin = std::abs(nn - l), wmax = nn + l, nlmin = std::min(l, nn);
+            for (int m = -nlmin; m <= nlmin; m++) {
+                int ml = l * (l + 1) + m;
+                double c2 = -c1 * ((m & 1) ? -1.0 : 1.0);
+                big.vcfunc(-m, nn, m, l, vc1.data());
+                for (int w = wmin; w <= wmax; w++) {
+                    int e = ((nn - l + w) % 4 + 4) % 4;
+                    double ri = (e == 0 || e == 1) ? 1.0 : -1.0;
+                    vcc[(size_t)(nn - 1) + (size_t)Tt * ((size_t)(ml - 1) + (size_t)Ls * (Ls + 2) * w)] = c2 * vc1[w] * vc2[w] * ri;
+                }
+            }
+        }
+    const int FN = std::max(Tt, Ls);
+    size_t nf = (size_t)(2 * FN + 1) * FN;
+    std::vector<double> f1(nf, 0.0), f2(nf, 0.0), f3(nf, 0.0);
+    const std::vector<double>& fr = big.fnr;
+    for (int m = -FN; m <= FN; m++)
+        for (int l = std::max(1, std::abs(m)); l <= FN; l++) {
+            size_t ix = (size_t)(m + FN) + (2 * FN + 1) * (size_t)(l - 1);
+            int lp1 = l + 1, lm1 = l - 1;
+            f1[ix] = fr[lm1] * fr[lp1] * fr[l - m] * fr[l + m] / fr[lm1 + l] / fr[l + lp1] / (double)l;
+            f2[ix] = (double)m / (double)l / (double)lp1;
+            f3[ix] = fr[l] * fr[l + 2] * fr[lp1 - m] * fr[lp1 + m] / fr[l + lp1] / fr[l + l + 3] / (double)lp1;
+        }
+    std::vector<double> bd(Tt + Ls + 4);
+    for (int k = 0; k < (int)bd.size(); k++) bd[k] = big.bc(k, k);
+    auto up = [&](DevBuf<double>& d, const std::vector<double>& h) -> int {
+        CK(d.alloc(h.size()));
+        CK(cudaMemcpyAsync(d.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->st));
+        return MSTMG_OK;
+    };
+    int rc;
+    if ((rc = up(r.vcc, vcc)) || (rc = up(r.f1, f1)) || (rc = up(r.f2, f2)) || (rc = up(r.f3, f3)) || (rc = up(r.bcd, bd))) return rc;
+    // the host vectors are freed on return: wait for the copies
+    CK(cudaStreamSynchronize(c->st));
+    r.vcT = Tt;
+    r.vcML = Ls * (Ls + 2);
+    r.FN = FN;
+    return MSTMG_OK;
+}
+
+static MergeArgs merge_args(mstmg_ctx* c, const RegTables& rt, const BigTablesDev& bt, const double* r0, const int* dtord)
+{
+    MergeArgs ma;
+    ma.mode = 0;
+    ma.out = nullptr;
+    ma.ldo = 0;
+    ma.nsph = c->n;
+    ma.pos = c->pos.p;
+    ma.order = c->d_order.p;
+    ma.offset = c->d_offset.p;
+    ma.tord = dtord;
+    ma.r0[0] = r0[0];
+    ma.r0[1] = r0[1];
+    ma.r0[2] = r0[2];
+    ma.rimed_re = c->opts.medium_re;
+    ma.rimed_im = c->opts.medium_im;
+    ma.vcc = rt.vcc.p;
+    ma.vcT = rt.vcT;
+    ma.vcML = rt.vcML;
+    ma.fnm1 = rt.f1.p;
+    ma.fnc = rt.f2.p;
+    ma.fnp1 = rt.f3.p;
+    ma.fcN = rt.FN;
+    ma.fnr = bt.fnr.p;
+    ma.bcofd = rt.bcd.p;
+    return ma;
+}
+
 extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_eps, int max_t_order, int nangles, double* smat,
                                 double* g, int* t_matrix_order, double* amnp0, int amnp0_cap)
 {
@@ -940,85 +1125,16 @@ extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_e
         return MSTMG_ERR_ARG;
     }
     const int n = c->n, L = c->lmax;
-    const int NBC = 420;
-    // cluster origin: mean position of the external spheres
-    double r0[3] = {0.0, 0.0, 0.0};
-    for (int i = 0; i < n; i++)
-        for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->hpos[3 * (size_t)i + k];
-    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)n;
-    static thread_local mstmg::Tables* big = nullptr;
-    if (!big) big = new mstmg::Tables(NBC);
-    DevBuf<double> dbc, dfnr;
-    CK(dbc.alloc(big->bcof.size()));
-    CK(dfnr.alloc(big->fnr.size()));
-    CK(cudaMemcpyAsync(dbc.p, big->bcof.data(), sizeof(double) * big->bcof.size(), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(dfnr.p, big->fnr.data(), sizeof(double) * big->fnr.size(), cudaMemcpyHostToDevice, c->st));
-    // translation orders (tranordertest) on the device
+    BigTablesDev bt;
+    int rc = upload_big(c, bt);
+    if (rc) return rc;
+    double r0[3];
     DevBuf<int> dtord;
-    DevBuf<zd> tscr;
-    const int sstride = 3 * (200 + MSTMG_LMAX + 4);
-    CK(dtord.alloc(n));
-    CK(tscr.alloc((size_t)n * sstride));
-    launch_tranorder(n, c->pos.p, c->d_order.p, r0, c->opts.medium_re, trans_eps, max_t_order, dbc.p, dfnr.p, NBC, tscr.p, sstride,
-                     dtord.p, c->st);
-    std::vector<int> tord(n);
-    CK(cudaMemcpyAsync(tord.data(), dtord.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    int T = std::min(L, max_t_order);
-    for (int i = 0; i < n; i++) T = std::max(T, tord[i]);
-    if (T > 200) {
-        set_err("mstmg_scattering: t_matrix_order above 200 is not supported");
-        return MSTMG_ERR_UNSUPPORTED;
-    }
-    // axial constants for regular translation up to order T (host, FP64)
-    std::vector<double> vcc((size_t)T * L * (L + 2) * (T + L + 1), 0.0), f1, f2, f3, vc1(2 * (T + L) + 4), vc2(2 * (T + L) + 4);
-    for (int nn = 1; nn <= T; nn++)
-        for (int l = 1; l <= L; l++) {
-            double c1 = big->fnr[nn + nn + 1] * big->fnr[l + l + 1];
-            big->vcfunc(-1, nn, 1, l, vc2.data());
-            int wmin = std::abs(nn - l), wmax = nn + l, nlmin = std::min(l, nn);
-            for (int m = -nlmin; m <= nlmin; m++) {
-                int ml = l * (l + 1) + m;
-                double c2 = -c1 * ((m & 1) ? -1.0 : 1.0);
-                big->vcfunc(-m, nn, m, l, vc1.data());
-                for (int w = wmin; w <= wmax; w++) {
-                    int e = ((nn - l + w) % 4 + 4) % 4;
-                    double ri = (e == 0 || e == 1) ? 1.0 : -1.0;
-                    vcc[(size_t)(nn - 1) + (size_t)T * ((size_t)(ml - 1) + (size_t)L * (L + 2) * w)] = c2 * vc1[w] * vc2[w] * ri;
-                }
-            }
-        }
-    int FN = std::max(T, L);
-    {
-        std::vector<double> tmpv;
-        mstmg::Tables small(6 * FN + 6 < NBC ? 6 * FN + 6 : NBC);
-        size_t nf = (size_t)(2 * FN + 1) * FN;
-        f1.assign(nf, 0.0);
-        f2.assign(nf, 0.0);
-        f3.assign(nf, 0.0);
-        const std::vector<double>& fr = big->fnr;
-        for (int m = -FN; m <= FN; m++)
-            for (int l = std::max(1, std::abs(m)); l <= FN; l++) {
-                size_t ix = (size_t)(m + FN) + (2 * FN + 1) * (size_t)(l - 1);
-                int lp1 = l + 1, lm1 = l - 1;
-                f1[ix] = fr[lm1] * fr[lp1] * fr[l - m] * fr[l + m] / fr[lm1 + l] / fr[l + lp1] / (double)l;
-                f2[ix] = (double)m / (double)l / (double)lp1;
-                f3[ix] = fr[l] * fr[l + 2] * fr[lp1 - m] * fr[lp1 + m] / fr[l + lp1] / fr[l + l + 3] / (double)lp1;
-            }
-    }
-    DevBuf<double> dvcc, df1, df2, df3, dbcd;
-    CK(dvcc.alloc(vcc.size()));
-    CK(df1.alloc(f1.size()));
-    CK(df2.alloc(f2.size()));
-    CK(df3.alloc(f3.size()));
-    std::vector<double> bd(T + L + 4);
-    for (int k = 0; k < (int)bd.size(); k++) bd[k] = big->bc(k, k);
-    CK(dbcd.alloc(bd.size()));
-    CK(cudaMemcpyAsync(dvcc.p, vcc.data(), sizeof(double) * vcc.size(), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(df1.p, f1.data(), sizeof(double) * f1.size(), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(df2.p, f2.data(), sizeof(double) * f2.size(), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(df3.p, f3.data(), sizeof(double) * f3.size(), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(dbcd.p, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice, c->st));
+    std::vector<int> tord;
+    int T = 0;
+    if ((rc = origin_orders(c, bt, trans_eps, max_t_order, r0, dtord, tord, &T))) return rc;
+    RegTables rt;
+    if ((rc = build_reg_tables(c, T, L, rt))) return rc;
     // merge to the common origin
     const int ne = c->neqns, nb0 = 2 * T * (T + 2);
     DevBuf<zd> dsrc, da0, mscr;
@@ -1029,32 +1145,13 @@ extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_e
     int grid = std::min(n, c->nsm * 2);
     size_t stride = merge_scratch_per_cta(T, L);
     CK(mscr.alloc((size_t)grid * stride));
-    MergeArgs ma;
-    ma.nsph = n;
-    ma.pos = c->pos.p;
-    ma.order = c->d_order.p;
-    ma.offset = c->d_offset.p;
-    ma.tord = dtord.p;
+    MergeArgs ma = merge_args(c, rt, bt, r0, dtord.p);
     ma.T = T;
-    ma.r0[0] = r0[0];
-    ma.r0[1] = r0[1];
-    ma.r0[2] = r0[2];
-    ma.rimed_re = c->opts.medium_re;
-    ma.rimed_im = c->opts.medium_im;
     ma.amnp = dsrc.p;
     ma.ld = ne;
     ma.npol = 2;
     ma.amnp0 = da0.p;
     ma.ld0 = nb0;
-    ma.vcc = dvcc.p;
-    ma.vcT = T;
-    ma.vcML = L * (L + 2);
-    ma.fnm1 = df1.p;
-    ma.fnc = df2.p;
-    ma.fnp1 = df3.p;
-    ma.fcN = FN;
-    ma.fnr = dfnr.p;
-    ma.bcofd = dbcd.p;
     ma.scratch = mscr.p;
     ma.scratch_stride = stride;
     launch_merge(ma, grid, c->st);
@@ -1065,10 +1162,10 @@ extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_e
     CK(ds.alloc(4 * 16 * (size_t)W));
     CK(cudaMemsetAsync(ds.p, 0, sizeof(double) * 4 * 16 * (size_t)W, c->st));
     CK(fscr.alloc(fosm_scratch_doubles(T)));
-    launch_fosm(T, da0.p, dbc.p, dfnr.p, NBC, ds.p, ds.p + 16 * W, ds.p + 32 * W, ds.p + 48 * W, fscr.p, c->st);
+    launch_fosm(T, da0.p, bt.bc.p, bt.fnr.p, bt.nbc, ds.p, ds.p + 16 * W, ds.p + 32 * W, ds.p + 48 * W, fscr.p, c->st);
     CK(cscr.alloc(fosmcalc_scratch_doubles(T, nangles)));
     CK(dsm.alloc(16 * (size_t)nangles));
-    launch_fosmcalc(T, nangles, ds.p, ds.p + 16 * W, ds.p + 32 * W, ds.p + 48 * W, dfnr.p, dbcd.p, cscr.p, dsm.p, c->st);
+    launch_fosmcalc(T, nangles, ds.p, ds.p + 16 * W, ds.p + 32 * W, ds.p + 48 * W, bt.fnr.p, rt.bcd.p, cscr.p, dsm.p, c->st);
     CK(cudaGetLastError());
     double s0[2];
     CK(cudaMemcpyAsync(&s0[0], ds.p + 0, sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -1078,9 +1175,366 @@ extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_e
     CK(cudaStreamSynchronize(c->st));
     if (g) *g = s0[1] / (3.0 * s0[0]);
     if (t_matrix_order) *t_matrix_order = T;
-    dbc.release(); dfnr.release(); dtord.release(); tscr.release(); dvcc.release(); df1.release(); df2.release(); df3.release();
-    dbcd.release(); dsrc.release(); da0.release(); mscr.release(); ds.release(); fscr.release(); cscr.release(); dsm.release();
     return check_kernel_err(c);
+}
+
+// ---- many systems at once ----
+
+template <typename T> struct MultiWork {
+    int S = 0;
+    DevBuf<cpx<T>> vec, XP, YP;
+    DevBuf<double> part, epsv;
+    DevBuf<BicgScalars> sc;
+    DevBuf<int> act;
+    std::vector<BicgScalars> hsc;
+    std::vector<int> hact;
+    MultiVecs<T> v(int ne) const
+    {
+        MultiVecs<T> m;
+        cpx<T>* b = vec.p;
+        size_t cs = (size_t)ne * S;
+        m.X = b;
+        m.R = b + cs;
+        m.P = b + 2 * cs;
+        m.W = b + 3 * cs;
+        m.Q = b + 4 * cs;
+        m.CAP = b + 5 * cs;
+        m.CAW = b + 6 * cs;
+        return m;
+    }
+    // vectors = false: only the packed translation buffers (FP64 residuals of the refinement)
+    int init(int S_, int ne, int nsm, bool vectors)
+    {
+        S = S_;
+        int spad = S + 3;
+        if (vectors) CK(vec.alloc((size_t)7 * ne * S));
+        CK(XP.alloc((size_t)2 * ne * spad));
+        CK(YP.alloc((size_t)2 * ne * spad));
+        CK(part.alloc((size_t)3 * (4 * nsm + spad)));
+        CK(epsv.alloc(S));
+        CK(sc.alloc(S));
+        CK(act.alloc(S));
+        hsc.resize(S);
+        hact.resize(S);
+        return MSTMG_OK;
+    }
+};
+
+// cbicg for the systems listed in sys (columns of B and of the work vectors),
+// all advanced together; system s stops where cbicg would stop it.  X (w.v().X)
+// holds the initial guesses when have_x0.  iters/errs/status are indexed by
+// system; status 2 = breakdown.
+template <typename T>
+static int bicg_multi(mstmg_ctx* c, MultiWork<T>& w, const cpx<T>* B, const std::vector<int>& sys, bool have_x0, int niter,
+                      const std::vector<double>& eps, std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status)
+{
+    const int ne = c->neqns;
+    SlotMaps sm = c->sm();
+    const cpx<T>* an = (sizeof(T) == 8) ? (const cpx<T>*)c->an.p : (const cpx<T>*)c->an32.p;
+    MultiVecs<T> v = w.v(ne);
+    const int per_chunk = (sizeof(T) == 4) ? 2 : 1;   // systems per translation chunk ([p, w] column pairs)
+    const int NR = 2 * per_chunk;
+    iters.assign(w.S, 0);
+    errs.assign(w.S, 0.0);
+    status.assign(w.S, 0);
+    int a = (int)sys.size();
+    if (a == 0) return MSTMG_OK;
+    for (int k = 0; k < a; k++) w.hact[k] = sys[k];
+    CK(cudaMemcpyAsync(w.act.p, w.hact.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(w.epsv.p, eps.data(), sizeof(double) * w.S, cudaMemcpyHostToDevice, c->st));
+    int rc;
+    if (have_x0) {
+        int apad = ((a + NR - 1) / NR) * NR;
+        launch_m_gather<T>(ne, a, apad, w.act.p, v.X, w.XP.p, c->nsm, c->st);
+        if ((rc = translate_many<T>(c, w.XP.p, w.YP.p, apad, 0u))) return rc;
+    } else {
+        for (int k = 0; k < a; k++) CK(cudaMemsetAsync(v.X + (size_t)sys[k] * ne, 0, sizeof(cpx<T>) * ne, c->st));
+    }
+    launch_m_init<T>(sm, an, ne, a, w.act.p, B, v, w.YP.p, have_x0 ? 1 : 0, w.part.p, w.sc.p, c->nsm, c->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(w.hsc.data(), w.sc.p, sizeof(BicgScalars) * w.S, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    auto compact = [&]() -> int {
+        int na = 0;
+        for (int k = 0; k < a; k++) {
+            int s = w.hact[k];
+            const BicgScalars& q = w.hsc[s];
+            if (q.breakdown) status[s] = 2;
+            else if (!q.stop) w.hact[na++] = s;
+        }
+        bool changed = (na != a);
+        a = na;
+        if (changed && a > 0) CK(cudaMemcpyAsync(w.act.p, w.hact.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+        return MSTMG_OK;
+    };
+    if ((rc = compact())) return rc;
+    for (int it = 1; it <= niter && a > 0; it++) {
+        int apad = ((a + per_chunk - 1) / per_chunk) * per_chunk;
+        launch_m_pack<T>(sm, an, ne, a, apad, w.act.p, v.P, v.W, w.XP.p, c->nsm, c->st);
+        if ((rc = translate_many<T>(c, w.XP.p, w.YP.p, 2 * apad, 2u))) return rc;
+        launch_m_post<T>(sm, an, ne, a, w.act.p, v, w.YP.p, w.part.p, w.sc.p, c->nsm, c->st);
+        launch_m_upd<T>(ne, a, w.act.p, v, w.part.p, w.sc.p, w.epsv.p, c->nsm, c->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(w.hsc.data(), w.sc.p, sizeof(BicgScalars) * w.S, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        for (int k = 0; k < a; k++) {
+            int s = w.hact[k];
+            iters[s] = it;
+            errs[s] = w.hsc[s].eerr;
+        }
+        if ((rc = compact())) return rc;
+    }
+    for (int k = 0; k < a; k++) iters[w.hact[k]] = niter + 1;   // Fortran DO-loop exit value when the cap is reached
+    return check_kernel_err(c);
+}
+
+// Mixed precision for S systems: FP64 outer refinement (true residual with the
+// FP64 operators), FP32 inner BiCG on the residual systems, all systems in
+// lockstep.  X (FP64, ne x S) holds the initial guesses on entry.
+static int solve_multi_mixed(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>& w32, DevBuf<zf>& B32, DevBuf<double>& rr,
+                             DevBuf<int>& idx, int S, const zd* B, zd* X, double eps, int niter, std::vector<int>& iters,
+                             std::vector<double>& errs, std::vector<int>& status, int* outer_count)
+{
+    const int ne = c->neqns;
+    SlotMaps sm = c->sm();
+    std::vector<int> act(S), total(S, 0);
+    for (int s = 0; s < S; s++) act[s] = s;
+    iters.assign(S, 0);
+    errs.assign(S, 1.0);
+    status.assign(S, 0);
+    std::vector<double> hrr(2 * (size_t)S), ieps(w32.S, 1.0);
+    std::vector<int> it2, st2, map(2 * (size_t)S);
+    std::vector<double> e2;
+    int rc;
+    *outer_count = 0;
+    for (int outer = 0; outer < c->opts.max_outer && !act.empty(); outer++) {
+        int a = (int)act.size();
+        int apad = ((a + 1) / 2) * 2;
+        CK(cudaMemcpyAsync(w64.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+        launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
+        if ((rc = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u))) return rc;
+        launch_m_resid<float>(sm, c->an.p, ne, a, w64.act.p, B, X, w64.YP.p, B32.p, w64.part.p, rr.p, c->nsm, c->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hrr.data(), rr.p, sizeof(double) * 2 * S, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        *outer_count = outer + 1;
+        std::vector<int> inner, keep;   // inner: residual columns k to refine; keep: their systems
+        int cap = niter;
+        for (int k = 0; k < a; k++) {
+            int s = act[k];
+            double bb = hrr[2 * s + 1];
+            errs[s] = bb > 0.0 ? hrr[2 * s] / bb : 0.0;
+            if (errs[s] < eps || total[s] >= niter) continue;
+            inner.push_back(k);
+            keep.push_back(s);
+            ieps[k] = std::max(eps / errs[s] * 0.01, c->opts.inner_eps);
+            cap = std::min(cap, niter - total[s]);
+        }
+        if (inner.empty()) break;
+        if (cap < 1) cap = 1;
+        if ((rc = bicg_multi<float>(c, w32, B32.p, inner, false, cap, ieps, it2, e2, st2))) return rc;
+        const int ni = (int)inner.size();
+        for (int j = 0; j < ni; j++) {
+            int k = inner[j], s = keep[j];
+            total[s] += std::min(it2[k], cap);
+            if (st2[k] == 2) status[s] = 2;
+            map[j] = s;
+            map[S + j] = k;
+        }
+        CK(cudaMemcpyAsync(idx.p, map.data(), sizeof(int) * 2 * S, cudaMemcpyHostToDevice, c->st));
+        launch_m_addcorr<float>(ne, ni, idx.p, idx.p + S, X, w32.v(ne).X, c->st);
+        CK(cudaGetLastError());
+        act = keep;
+    }
+    for (int s = 0; s < S; s++) iters[s] = total[s];
+    return check_kernel_err(c);
+}
+
+extern "C" int mstmg_t_matrix_order(mstmg_ctx* c, double trans_eps, int max_t_order, int* t_matrix_order)
+{
+    if (!c || max_t_order < 1 || !t_matrix_order) {
+        set_err("mstmg_t_matrix_order: bad arguments");
+        return MSTMG_ERR_ARG;
+    }
+    BigTablesDev bt;
+    int rc = upload_big(c, bt);
+    if (rc) return rc;
+    double r0[3];
+    DevBuf<int> dtord;
+    int T = 0;
+    if ((rc = origin_orders(c, bt, trans_eps, max_t_order, r0, dtord, c->tord, &T))) {
+        c->tord.clear();
+        return rc;
+    }
+    *t_matrix_order = T;
+    return MSTMG_OK;
+}
+
+extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_eps, double convergence_eps, int max_iterations,
+                             double* tmat, double* sphere_qeff, double* qtot, int* order_used, int* maxiter, double* maxerr)
+{
+    if (!c || t_matrix_order < 1 || t_matrix_order > 200 || !tmat || max_iterations < 1) {
+        set_err("mstmg_tmatrix: bad arguments (1 <= t_matrix_order <= 200, max_iterations >= 1, tmat required)");
+        return MSTMG_ERR_ARG;
+    }
+    if ((int)c->tord.size() != c->n) {
+        set_err("mstmg_tmatrix: call mstmg_t_matrix_order first (it sets the translation orders)");
+        return MSTMG_ERR_ARG;
+    }
+    const bool mixed = c->opts.precision == MSTMG_PRECISION_MIXED;
+    int rc = ensure_ops_both(c, true, mixed, false);
+    if (rc) return rc;
+    const int n = c->n, L = c->lmax, ne = c->neqns, TM = t_matrix_order;
+    const int nblkt = 2 * TM * (TM + 2), Smax = 2 * (2 * TM + 1);
+    BigTablesDev bt;
+    if ((rc = upload_big(c, bt))) return rc;
+    double r0[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->hpos[3 * (size_t)i + k];
+    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)n;
+    DevBuf<int> dtord;
+    CK(dtord.alloc(n));
+    CK(cudaMemcpyAsync(dtord.p, c->tord.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+    RegTables rtm, rtd;   // merge: spheres -> origin; distribute: origin -> spheres
+    if ((rc = build_reg_tables(c, TM, L, rtm)) || (rc = build_reg_tables(c, L, TM, rtd))) return rc;
+    const int grid = std::min(n, c->nsm * 2);
+    const size_t strm = merge_scratch_per_cta(TM, L), strd = merge_scratch_per_cta(L, TM);
+    DevBuf<zd> mscr, P0, PK, B64, A0, dT, X64;
+    DevBuf<double> qcol, dsq, qsum, rr;
+    DevBuf<zf> B32;
+    DevBuf<int> idx;
+    CK(mscr.alloc((size_t)grid * std::max(strm, strd)));
+    CK(P0.alloc((size_t)2 * TM * (TM + 2) * Smax));
+    CK(A0.alloc((size_t)2 * TM * (TM + 2) * Smax));
+    CK(PK.alloc((size_t)ne * Smax));
+    CK(B64.alloc((size_t)ne * Smax));
+    CK(dT.alloc((size_t)nblkt * nblkt));
+    CK(cudaMemsetAsync(dT.p, 0, sizeof(zd) * (size_t)nblkt * nblkt, c->st));
+    CK(qcol.alloc((size_t)3 * n * Smax));
+    CK(dsq.alloc((size_t)3 * n));
+    CK(cudaMemsetAsync(dsq.p, 0, sizeof(double) * 3 * n, c->st));
+    CK(qsum.alloc(3));
+    MultiWork<double> w64;
+    MultiWork<float> w32;
+    if ((rc = w64.init(Smax, ne, c->nsm, !mixed))) return rc;
+    if (mixed) {
+        if ((rc = w32.init(Smax, ne, c->nsm, true))) return rc;
+        CK(X64.alloc((size_t)ne * Smax));
+        CK(B32.alloc((size_t)ne * Smax));
+        CK(rr.alloc(2 * (size_t)Smax));
+        CK(idx.alloc(2 * (size_t)Smax));
+    }
+    zd* X = mixed ? X64.p : w64.v(ne).X;
+    SlotMaps sm = c->sm();
+    const zd rimed = mk(c->opts.medium_re, c->opts.medium_im);
+    int istat = 0, mit = 0, used = TM, outer_total = 0;
+    double merr = 0.0, qold = 0.0, hq[3] = {0.0, 0.0, 0.0};
+    int l;
+    for (l = 1; l <= TM; l++) {
+        const int S = 2 * (2 * l + 1), nb = 2 * l * (l + 2);
+        // right-hand sides: unit TE/TM fields of order l at the origin, distributed to the spheres
+        launch_tm_rhs(l, P0.p, c->st);
+        CK(cudaMemsetAsync(PK.p, 0, sizeof(zd) * (size_t)ne * S, c->st));
+        MergeArgs md = merge_args(c, rtd, bt, r0, dtord.p);
+        md.mode = 1;
+        md.out = PK.p;
+        md.ldo = ne;
+        md.T = l;
+        md.amnp = P0.p;
+        md.ld = nb;
+        md.npol = S;
+        md.amnp0 = nullptr;
+        md.ld0 = 0;
+        md.scratch = mscr.p;
+        md.scratch_stride = strd;
+        launch_merge(md, grid, c->st);
+        // b = Mie f, initial guess b (solver:185-187)
+        launch_m_mie(sm, c->an.p, ne, S, PK.p, B64.p, c->st);
+        CK(cudaMemcpyAsync(X, B64.p, sizeof(zd) * (size_t)ne * S, cudaMemcpyDeviceToDevice, c->st));
+        CK(cudaGetLastError());
+        std::vector<int> its;
+        std::vector<double> errs;
+        std::vector<int> sts;
+        if (mixed) {
+            int oc = 0;
+            rc = solve_multi_mixed(c, w64, w32, B32, rr, idx, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
+            outer_total += oc;
+        } else {
+            std::vector<int> sys(S);
+            for (int s = 0; s < S; s++) sys[s] = s;
+            std::vector<double> ev(Smax, solution_eps);
+            w64.S = Smax;
+            rc = bicg_multi<double>(c, w64, B64.p, sys, true, max_iterations, ev, its, errs, sts);
+        }
+        if (rc) return rc;
+        for (int s = 0; s < S; s++) {
+            mit = std::max(mit, its[s]);
+            merr = std::max(merr, errs[s]);
+            if (its[s] > max_iterations || errs[s] > solution_eps || sts[s] == 2) istat = 1;
+        }
+        // per-sphere efficiencies of every column, summed
+        launch_tm_qeff(n, S, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, rimed, c->an_inv.p, X, PK.p, ne, qcol.p, c->st);
+        launch_tm_qsum(n, S, qcol.p, c->rad.p, c->xg, dsq.p, qsum.p, c->st);
+        // merge the solutions to the origin: T-matrix columns of order l
+        CK(cudaMemsetAsync(A0.p, 0, sizeof(zd) * (size_t)nb * S, c->st));
+        MergeArgs mm = merge_args(c, rtm, bt, r0, dtord.p);
+        mm.T = l;
+        mm.amnp = X;
+        mm.ld = ne;
+        mm.npol = S;
+        mm.amnp0 = A0.p;
+        mm.ld0 = nb;
+        mm.scratch = mscr.p;
+        mm.scratch_stride = strm;
+        launch_merge(mm, grid, c->st);
+        launch_tm_store(l, TM, A0.p, dT.p, c->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hq, qsum.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        double converr = hq[0] - qold;
+        qold = hq[0];
+        if (convergence_eps > 0.0 && converr < convergence_eps) break;
+    }
+    used = l < TM ? l : TM;
+    c->outer = outer_total;
+    CK(copy_out(tmat, dT.p, sizeof(zd) * (size_t)nblkt * nblkt, c->st));
+    if (sphere_qeff) CK(copy_out(sphere_qeff, dsq.p, sizeof(double) * 3 * n, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (qtot) {
+        qtot[0] = hq[0];
+        qtot[1] = hq[1];
+        qtot[2] = hq[0] + hq[2] - hq[1];   // qtotcalc: Qsca = Qext + Qinc - Qabs
+    }
+    if (order_used) *order_used = used;
+    if (maxiter) *maxiter = mit;
+    if (maxerr) *maxerr = merr;
+    rc = check_kernel_err(c);
+    if (rc) return rc;
+    return istat ? MSTMG_NOT_CONVERGED : MSTMG_OK;
+}
+
+extern "C" int mstmg_tmatrix_qext_qsca(mstmg_ctx* c, int t_matrix_order, const double* tmat, double* qext, double* qsca)
+{
+    if (!c || t_matrix_order < 1 || t_matrix_order > 200 || !tmat) {
+        set_err("mstmg_tmatrix_qext_qsca: bad arguments");
+        return MSTMG_ERR_ARG;
+    }
+    const size_t nblkt = 2 * (size_t)t_matrix_order * (t_matrix_order + 2);
+    DevBuf<zd> dT;
+    DevBuf<float> tc;
+    DevBuf<double> out;
+    CK(dT.alloc(nblkt * nblkt));
+    CK(tc.alloc(2 * nblkt * nblkt));
+    CK(out.alloc(2));
+    CK(copy_in(dT.p, tmat, sizeof(zd) * nblkt * nblkt, c->st));
+    launch_tm_qext_qsca(t_matrix_order, dT.p, c->xg, tc.p, out.p, c->st);
+    CK(cudaGetLastError());
+    double h[2];
+    CK(cudaMemcpyAsync(h, out.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (qext) *qext = h[0];
+    if (qsca) *qsca = h[1];
+    return MSTMG_OK;
 }
 
 extern "C" int mstmg_set_stream(mstmg_ctx* c, void* stream)

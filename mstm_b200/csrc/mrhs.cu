@@ -1,0 +1,616 @@
+// mrhs.cu -- MSTM's BiCG iteration (cbicg, december2023/mstm-solver-8.f90:654-949)
+// for many independent systems at once, and the T-matrix helpers of
+// tmatrix_solution (solver:22-332).
+//
+// Each system keeps exactly the reference's recurrence; systems only share
+// launches.  A launch covers the a active systems act[0..a) in grid rows, so
+// one iteration of any number of systems is a fixed handful of launches (pack,
+// translation, post, upd1, upd2 and three scalar finishes) instead of a handful
+// per system.  Dot products accumulate in FP64 per CTA and are summed per
+// system in a fixed order, so results do not depend on the other systems.
+#include "mrhs.cuh"
+#include "special.cuh"
+
+#define MB 256
+
+namespace {
+
+__device__ __forceinline__ double mwarp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+template <int K> __device__ __forceinline__ void mblock_store(double (&v)[K], double* out)
+{
+    __shared__ double sh[K][MB / 32];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double s = mwarp_sum(v[k]);
+        if (lane == 0) sh[k][w] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            double s = 0.0;
+            for (int q = 0; q < MB / 32; q++) s += sh[k][q];
+            out[k] = s;
+        }
+    }
+}
+template <typename T> __device__ __forceinline__ cpx<double> upd_(cpx<T> a) { return mk((double)a.x, (double)a.y); }
+
+// slot e of the first mode half -> (element of mode 1, element of mode 2, Mie row n, sphere)
+struct SlotPos { int b0, b1, n, i; };
+__device__ __forceinline__ SlotPos slot_pos(const SlotMaps& sm, int e)
+{
+    SlotPos r;
+    r.i = sm.slot[e];
+    int L = sm.order[r.i], hb = L * (L + 2);
+    int loc = e - sm.offset[r.i] / 2;
+    int row = loc % (L + 2), col = loc / (L + 2) + 1;
+    r.n = (row <= col) ? col : row - 1;
+    r.b0 = sm.offset[r.i] + loc;
+    r.b1 = r.b0 + hb;
+    return r;
+}
+
+}  // namespace
+
+int multi_grid(int nslots, int a, int nsm)
+{
+    int want = (4 * nsm + a - 1) / (a > 0 ? a : 1);
+    int most = (nslots + MB - 1) / MB;
+    int g = want < most ? want : most;
+    return g < 1 ? 1 : g;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MB) m_gather_kernel(int ld, int a, const int* act, const cpx<T>* X, cpx<T>* XP)
+{
+    const int k = blockIdx.y;
+    cpx<T>* dst = XP + (size_t)k * ld;
+    if (k >= a) {
+        for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) dst[e] = mk((T)0, (T)0);
+        return;
+    }
+    const cpx<T>* src = X + (size_t)act[k] * ld;
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) dst[e] = src[e];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MB) m_pack_kernel(SlotMaps sm, const cpx<T>* an, int ld, int a, const int* act, const cpx<T>* P,
+                                                    const cpx<T>* W, cpx<T>* XP)
+{
+    const int k = blockIdx.y;
+    cpx<T>* xp = XP + (size_t)(2 * k) * ld;
+    cpx<T>* xw = xp + ld;
+    if (k >= a) {
+        for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+            xp[e] = mk((T)0, (T)0);
+            xw[e] = mk((T)0, (T)0);
+        }
+        return;
+    }
+    const int s = act[k];
+    const cpx<T>* p = P + (size_t)s * ld;
+    const cpx<T>* w = W + (size_t)s * ld;
+    for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
+        SlotPos q = slot_pos(sm, e);
+        xp[q.b0] = p[q.b0];
+        xp[q.b1] = p[q.b1];
+        // A^T conj(w)  (multmiecoeffmult with idir /= 1 on the conjugated vector)
+        const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        cpx<T> x0 = cj(w[q.b0]), x1 = cj(w[q.b1]);
+        xw[q.b0] = A[0] * x0 + A[1] * x1;
+        xw[q.b1] = A[2] * x0 + A[3] * x1;
+    }
+}
+
+// cr = b - x + M y ; cp = cr ; cq = cw = conj(cr); partials sum cr*cr, sum |b|^2
+template <typename T>
+__global__ void __launch_bounds__(MB) m_init_kernel(SlotMaps sm, const cpx<T>* an, int ld, const int* act, const cpx<T>* B,
+                                                    MultiVecs<T> v, const cpx<T>* YP, int have_y, double* part)
+{
+    const int k = blockIdx.y, s = act[k];
+    const size_t o = (size_t)s * ld;
+    const cpx<T>* y = YP + (size_t)k * ld;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
+        SlotPos q = slot_pos(sm, e);
+        cpx<T> m[2] = {mk((T)0, (T)0), mk((T)0, (T)0)};
+        if (have_y) {
+            const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+            cpx<T> u0 = y[q.b0], u1 = y[q.b1];
+            m[0] = A[0] * u0 + A[2] * u1;
+            m[1] = A[1] * u0 + A[3] * u1;
+        }
+        const int bb[2] = {q.b0, q.b1};
+        for (int h = 0; h < 2; h++) {
+            size_t g = o + bb[h];
+            cpx<T> bv = B[g];
+            cpx<T> rv = have_y ? (bv - v.X[g]) + m[h] : bv;
+            v.R[g] = rv;
+            v.P[g] = rv;
+            v.Q[g] = cj(rv);
+            v.W[g] = cj(rv);
+            cpx<double> rd = upd_(rv), bd = upd_(bv);
+            acc[0] += rd.x * rd.x - rd.y * rd.y;
+            acc[1] += 2.0 * rd.x * rd.y;
+            acc[2] += bd.x * bd.x + bd.y * bd.y;
+        }
+    }
+    mblock_store<3>(acc, part + 3 * ((size_t)k * gridDim.x + blockIdx.x));
+}
+
+// cap = p - M y0 ; caw = w - conj(y1) ; partial sum conj(w) cap
+template <typename T>
+__global__ void __launch_bounds__(MB) m_post_kernel(SlotMaps sm, const cpx<T>* an, int ld, const int* act, MultiVecs<T> v,
+                                                    const cpx<T>* YP, double* part)
+{
+    const int k = blockIdx.y, s = act[k];
+    const size_t o = (size_t)s * ld;
+    const cpx<T>* y0 = YP + (size_t)(2 * k) * ld;
+    const cpx<T>* y1 = y0 + ld;
+    double acc[2] = {0.0, 0.0};
+    for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
+        SlotPos q = slot_pos(sm, e);
+        const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        cpx<T> u0 = y0[q.b0], u1 = y0[q.b1];
+        cpx<T> m0 = A[0] * u0 + A[2] * u1;
+        cpx<T> m1 = A[1] * u0 + A[3] * u1;
+        cpx<T> c0 = v.P[o + q.b0] - m0, c1 = v.P[o + q.b1] - m1;
+        v.CAP[o + q.b0] = c0;
+        v.CAP[o + q.b1] = c1;
+        cpx<T> w0 = v.W[o + q.b0], w1 = v.W[o + q.b1];
+        v.CAW[o + q.b0] = w0 - cj(y1[q.b0]);
+        v.CAW[o + q.b1] = w1 - cj(y1[q.b1]);
+        cpx<double> wd0 = upd_(w0), wd1 = upd_(w1), d0 = upd_(c0), d1 = upd_(c1);
+        acc[0] += wd0.x * d0.x + wd0.y * d0.y + wd1.x * d1.x + wd1.y * d1.y;
+        acc[1] += wd0.x * d0.y - wd0.y * d0.x + wd1.x * d1.y - wd1.y * d1.x;
+    }
+    mblock_store<2>(acc, part + 2 * ((size_t)k * gridDim.x + blockIdx.x));
+}
+
+// x += a p ; r -= a cap ; q -= conj(a) caw ; partials sum conj(q) r, sum |r|^2
+template <typename T>
+__global__ void __launch_bounds__(MB) m_upd1_kernel(int ld, const int* act, const BicgScalars* sc, MultiVecs<T> v, double* part)
+{
+    const int k = blockIdx.y, s = act[k];
+    const size_t o = (size_t)s * ld;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (!sc[s].breakdown) {
+        cpx<T> al = mk((T)sc[s].alpha[0], (T)sc[s].alpha[1]);
+        cpx<T> ac = cj(al);
+        for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+            size_t g = o + e;
+            v.X[g] = v.X[g] + al * v.P[g];
+            cpx<T> rv = v.R[g] - al * v.CAP[g];
+            cpx<T> qv = v.Q[g] - ac * v.CAW[g];
+            v.R[g] = rv;
+            v.Q[g] = qv;
+            cpx<double> rd = upd_(rv), qd = upd_(qv);
+            acc[0] += qd.x * rd.x + qd.y * rd.y;
+            acc[1] += qd.x * rd.y - qd.y * rd.x;
+            acc[2] += rd.x * rd.x + rd.y * rd.y;
+        }
+    }
+    mblock_store<3>(acc, part + 3 * ((size_t)k * gridDim.x + blockIdx.x));
+}
+
+// p = r + b p ; w = q + conj(b) w  (skipped once the system stopped)
+template <typename T>
+__global__ void __launch_bounds__(MB) m_upd2_kernel(int ld, const int* act, const BicgScalars* sc, MultiVecs<T> v)
+{
+    const int k = blockIdx.y, s = act[k];
+    if (sc[s].stop || sc[s].breakdown) return;
+    const size_t o = (size_t)s * ld;
+    cpx<T> b = mk((T)sc[s].beta[0], (T)sc[s].beta[1]);
+    cpx<T> bc = cj(b);
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+        size_t g = o + e;
+        v.P[g] = v.R[g] + b * v.P[g];
+        v.W[g] = v.Q[g] + bc * v.W[g];
+    }
+}
+
+// Per-system finish, one thread per active system (same logic as cbicg's
+// scalar steps): mode 0 after init, 1 after post, 2 after upd1.
+__global__ void m_fin_kernel(int mode, int a, int G, const int* act, const double* part, BicgScalars* scs, const double* epsv)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a) return;
+    BicgScalars* sc = scs + act[k];
+    const double eps = epsv ? epsv[act[k]] : 0.0;
+    const int K = (mode == 1) ? 2 : 3;
+    double s[3] = {0.0, 0.0, 0.0};
+    const double* pk = part + (size_t)K * G * k;
+    for (int b = 0; b < G; b++)
+        for (int j = 0; j < K; j++) s[j] += pk[K * b + j];
+    if (mode == 0) {
+        sc->csk[0] = s[0];
+        sc->csk[1] = s[1];
+        sc->enorm = s[2];
+        sc->stop = (s[0] == 0.0 && s[1] == 0.0) ? 1 : 0;
+        sc->breakdown = 0;
+        sc->eerr = 0.0;
+    } else if (mode == 1) {
+        zd cak = mk(s[0], s[1]);
+        if (cabsd(cak) != 0.0) {
+            zd al = cdiv(mk(sc->csk[0], sc->csk[1]), cak);
+            sc->alpha[0] = al.x;
+            sc->alpha[1] = al.y;
+        } else {
+            sc->breakdown = 1;
+        }
+    } else {
+        if (sc->breakdown) return;
+        double eerr = s[2] / sc->enorm;
+        sc->eerr = eerr;
+        zd csk = mk(sc->csk[0], sc->csk[1]);
+        if (eerr < eps || cabsd(csk) == 0.0) {
+            sc->stop = 1;
+        } else {
+            zd csk2 = mk(s[0], s[1]);
+            zd b = cdiv(csk2, csk);
+            sc->beta[0] = b.x;
+            sc->beta[1] = b.y;
+            sc->csk[0] = csk2.x;
+            sc->csk[1] = csk2.y;
+        }
+    }
+}
+
+template <typename TB>
+__global__ void __launch_bounds__(MB) m_resid_kernel(SlotMaps sm, const zd* an, int ld, const int* act, const zd* B, const zd* X,
+                                                     const zd* YP, cpx<TB>* Rout, double* part)
+{
+    const int k = blockIdx.y, s = act[k];
+    const size_t o = (size_t)s * ld;
+    const zd* y = YP + (size_t)k * ld;
+    cpx<TB>* ro = Rout + (size_t)k * ld;
+    double acc[2] = {0.0, 0.0};
+    for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
+        SlotPos q = slot_pos(sm, e);
+        const zd* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        zd u0 = y[q.b0], u1 = y[q.b1];
+        zd m[2] = {A[0] * u0 + A[2] * u1, A[1] * u0 + A[3] * u1};
+        const int bb[2] = {q.b0, q.b1};
+        for (int h = 0; h < 2; h++) {
+            zd bv = B[o + bb[h]];
+            zd rv = (bv - X[o + bb[h]]) + m[h];
+            ro[bb[h]] = mk((TB)rv.x, (TB)rv.y);
+            acc[0] += rv.x * rv.x + rv.y * rv.y;
+            acc[1] += bv.x * bv.x + bv.y * bv.y;
+        }
+    }
+    mblock_store<2>(acc, part + 2 * ((size_t)k * gridDim.x + blockIdx.x));
+}
+
+__global__ void m_sum2_kernel(int a, int G, const int* act, const double* part, double* out2)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a) return;
+    double s0 = 0.0, s1 = 0.0;
+    const double* pk = part + (size_t)2 * G * k;
+    for (int b = 0; b < G; b++) {
+        s0 += pk[2 * b];
+        s1 += pk[2 * b + 1];
+    }
+    out2[2 * act[k]] = s0;
+    out2[2 * act[k] + 1] = s1;
+}
+
+template <typename TL>
+__global__ void m_addcorr_kernel(int ld, const int* dst, const int* src, zd* X, const cpx<TL>* D)
+{
+    const int k = blockIdx.y;
+    zd* x = X + (size_t)dst[k] * ld;
+    const cpx<TL>* d = D + (size_t)src[k] * ld;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ld; e += gridDim.x * blockDim.x)
+        x[e] = x[e] + mk((double)d[e].x, (double)d[e].y);
+}
+
+__global__ void m_mie_kernel(SlotMaps sm, const zd* an, int ld, const zd* X, zd* Y)
+{
+    const int k = blockIdx.y;
+    const zd* x = X + (size_t)k * ld;
+    zd* y = Y + (size_t)k * ld;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < sm.nslots; e += gridDim.x * blockDim.x) {
+        SlotPos q = slot_pos(sm, e);
+        const zd* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        zd x0 = x[q.b0], x1 = x[q.b1];
+        y[q.b0] = A[0] * x0 + A[2] * x1;
+        y[q.b1] = A[1] * x0 + A[3] * x1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// T matrix helpers
+// ---------------------------------------------------------------------------
+
+// Column kq-1 (kq = 1..2(2l+1)) of the order-l right-hand sides: degree
+// k = -l + (kq-1)/2, mode q = mod(kq-1,2)+1; a(k,l,1) = 1/2, a(k,l,2) = -(-1)^q/2
+// (solver:166-178; the T matrix is TE-TM based).
+__global__ void tm_rhs_kernel(int l, zd* P0)
+{
+    const int nb = 2 * l * (l + 2), ncol = 2 * (2 * l + 1);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nb * ncol; e += gridDim.x * blockDim.x) {
+        int col = e / nb, el = e - col * nb;
+        int k = -l + col / 2, q = col % 2 + 1;
+        zd v = mk(0.0, 0.0);
+        if (el == aidx(k, l, 0, l)) v = mk(0.5, 0.0);
+        if (el == aidx(k, l, 1, l)) v = mk(-0.5 * pm1(q), 0.0);
+        P0[e] = v;
+    }
+}
+
+// lrsphereqeff (scatprops:676-776) with npol = 1 for one (sphere, column);
+// g = A^{-1} a as in qefficiencyfactors (scatprops:782-870, no host spheres).
+__global__ void tm_qeff_kernel(int nsph, int ncols, const int* order, const int* offset, const int* mie_offset, const double* radius,
+                               zd rimed, const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nsph * ncols) return;
+    const int c = t / nsph, i = t - c * nsph;
+    const int L = order[i], off = offset[i], hb = L * (L + 2);
+    const double xsp = radius[i];
+    const zd ri0 = rimed;
+    const zd xri = xsp * ri0;
+    const zd rib = cdivr(2.0, cdivr(1.0, ri0) + cdivr(1.0, ri0));
+    zd psi[MSTMG_LMAX + 2], xi[MSTMG_LMAX + 2], scr[2 * (MSTMG_LMAX + 2)];   // sphere orders are at most MSTMG_LMAX
+    mstm_cricbessel(L, xri, psi, scr);
+    mstm_crichankel(L, xri, xi, scr);
+    const zd* a = A + (size_t)c * ld + off;
+    const zd* f = P + (size_t)c * ld + off;
+    const zd* Ai = an_inv + mie_offset[i];
+    double qe = 0.0, qa = 0.0, qi = 0.0;
+    const zd cterm = imul(cdiv(cj(cdivr(1.0, ri0)), ri0));
+    for (int n = 1; n <= L; n++) {
+        zd psip = psi[n - 1] - cdiv((double)n * psi[n], xri);
+        zd xip = xi[n - 1] - cdiv((double)n * xi[n], xri);
+        zd aam[4], ggm[4], agm[4];
+        for (int s = 1; s <= 2; s++)
+            for (int u = 1; u <= 2; u++) {
+                double sg = pm1(s) * pm1(u);
+                int kk = (s - 1) + 2 * (u - 1);
+                aam[kk] = cterm * (xip * cj(xi[n]) - sg * (xi[n] * cj(xip)));
+                ggm[kk] = cterm * (psip * cj(psi[n]) - sg * (psi[n] * cj(psip)));
+                agm[kk] = cterm * (xip * cj(psi[n]) - sg * (xi[n] * cj(psip)));
+            }
+        const zd* Ain = Ai + 4 * (n - 1);
+        for (int m = -n; m <= n; m++) {
+            int a0 = aidx(m, n, 0, L);
+            zd av[2] = {a[a0], a[a0 + hb]};
+            zd gv[2] = {Ain[0] * av[0] + Ain[2] * av[1], Ain[1] * av[0] + Ain[3] * av[1]};
+            zd fv[2] = {f[a0], f[a0 + hb]};
+            for (int s = 0; s < 2; s++)
+                for (int u = 0; u < 2; u++) {
+                    int kk = s + 2 * u;
+                    zd crib = cj(rib) + pm1(s + u) * rib;
+                    qi += (ggm[kk] * fv[s] * cj(rib * fv[u])).x;
+                    qa += (aam[kk] * av[s] * cj(rib * av[u]) + ggm[kk] * gv[s] * cj(rib * gv[u]) + agm[kk] * av[s] * cj(gv[u]) * crib).x;
+                    qe += (agm[kk] * av[s] * cj(fv[u]) * crib).x;
+                }
+        }
+    }
+    double* q = qcol + 3 * ((size_t)i + (size_t)nsph * c);
+    q[0] = qe * 2.0 / xsp / xsp;
+    q[1] = qa * 2.0 / xsp / xsp;
+    q[2] = qi * 2.0 / xsp / xsp;   // qs = qi (the reference's 10-22 patch)
+}
+
+// One block: per sphere add the columns in order, then the weighted total in sphere order.
+__global__ void tm_qsum_kernel(int nsph, int ncols, const double* qcol, const double* radius, double xv, double* sq, double* qsum)
+{
+    for (int i = threadIdx.x; i < nsph; i += blockDim.x)
+        for (int c = 0; c < ncols; c++)
+            for (int j = 0; j < 3; j++) sq[3 * i + j] += qcol[3 * ((size_t)i + (size_t)nsph * c) + j];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < nsph; i++)
+            for (int j = 0; j < 3; j++) s[j] = s[j] + sq[3 * i + j] * radius[i] * radius[i] / (xv * xv);
+        for (int j = 0; j < 3; j++) qsum[j] = s[j];
+    }
+}
+
+__global__ void tm_store_kernel(int l, int tmo, const zd* A0, zd* tmat)
+{
+    const int nb = 2 * l * (l + 2), ncol = 2 * (2 * l + 1), nblkt = 2 * tmo * (tmo + 2);
+    const int nrow = l * (l + 2);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * nrow * ncol; e += gridDim.x * blockDim.x) {
+        int cc = e / (2 * nrow), rr = e - cc * 2 * nrow;
+        int mn = rr / 2 + 1, p = rr % 2;
+        int n = 1;
+        while (n * (n + 2) < mn) n++;
+        int m = mn - n * (n + 1);
+        int k = -l + cc / 2, q = cc % 2;
+        size_t col = (size_t)(2 * (l * (l + 1) + k - 1) + q);
+        tmat[(size_t)(2 * (mn - 1) + p) + (size_t)nblkt * col] = A0[(size_t)cc * nb + aidx(m, n, p, l)];
+    }
+}
+
+// ranorientscatmatrix's reader (scatprops:2031-2075): complex(4) copy with the
+// entries of rows n > l filled from tc(q,l(l+1)-k,p,n(n+1)-m) = (-1)^(m+k) tc(p,n(n+1)+m,q,l(l+1)+k).
+__global__ void tm_symm_kernel(int tmo, const zd* tmat, float* tc)
+{
+    const int nblk = tmo * (tmo + 2), nblkt = 2 * nblk;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)nblkt * nblkt; e += (size_t)gridDim.x * blockDim.x) {
+        int row = (int)(e % nblkt), col = (int)(e / nblkt);
+        int mn = row / 2 + 1, p = row % 2 + 1, kl = col / 2 + 1, q = col % 2 + 1;
+        int n = 1;
+        while (n * (n + 2) < mn) n++;
+        int l = 1;
+        while (l * (l + 2) < kl) l++;
+        float re, im;
+        if (n <= l) {
+            zd t = tmat[e];
+            re = (float)t.x;
+            im = (float)t.y;
+        } else {
+            // entry (p, mn, q, kl) with n > l is the image of (q, l(l+1)-k, p, n(n+1)-m) of column order n
+            int m = mn - n * (n + 1), k = kl - l * (l + 1);
+            int srow = 2 * (l * (l + 1) - k - 1) + (q - 1), scol = 2 * (n * (n + 1) - m - 1) + (p - 1);
+            zd t = tmat[(size_t)srow + (size_t)nblkt * scol];
+            float s = (float)pm1(m + k);
+            re = (float)t.x * s;
+            im = (float)t.y * s;
+        }
+        tc[2 * e] = re;
+        tc[2 * e + 1] = im;
+    }
+}
+
+// qextt = -sum Re tc(q,kl,q,kl), qscatt = sum |tc|^2 (single-precision terms,
+// double sums in the reader's order), both times 2/xv^2 (scatprops:2103-2122).
+__global__ void tm_qextsca_kernel(int tmo, const float* tc, double xv, double* out2)
+{
+    const int nblkt = 2 * tmo * (tmo + 2);
+    __shared__ double colsum[256];
+    double qe = 0.0, qs = 0.0;
+    for (int c0 = 0; c0 < nblkt; c0 += blockDim.x) {
+        int col = c0 + threadIdx.x;
+        double s = 0.0;
+        if (col < nblkt)
+            for (int row = 0; row < nblkt; row++) {
+                float re = tc[2 * ((size_t)row + (size_t)nblkt * col)], im = tc[2 * ((size_t)row + (size_t)nblkt * col) + 1];
+                // cabs of a complex(4) value: the modulus formed in double, rounded once to single
+                float a = (float)sqrt((double)re * re + (double)im * im);
+                s = s + (double)(a * a);
+            }
+        colsum[threadIdx.x] = s;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int j = 0; j < (int)blockDim.x && c0 + j < nblkt; j++) {
+                qs = qs + colsum[j];
+                int cj_ = c0 + j;
+                qe = qe - (double)tc[2 * ((size_t)cj_ + (size_t)nblkt * cj_)];
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out2[0] = qe * 2.0 / (xv * xv);
+        out2[1] = qs * 2.0 / (xv * xv);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <typename T> void launch_m_gather(int ld, int a, int apad, const int* act, const cpx<T>* X, cpx<T>* XP, int nsm, cudaStream_t st)
+{
+    dim3 g(multi_grid(ld, apad, nsm), apad);
+    m_gather_kernel<T><<<g, MB, 0, st>>>(ld, a, act, X, XP);
+    launch_counter() += 1;
+}
+template <typename T>
+void launch_m_pack(const SlotMaps& sm, const cpx<T>* an, int ld, int a, int apad, const int* act, const cpx<T>* P, const cpx<T>* W,
+                   cpx<T>* XP, int nsm, cudaStream_t st)
+{
+    dim3 g(multi_grid(sm.nslots, apad, nsm), apad);
+    m_pack_kernel<T><<<g, MB, 0, st>>>(sm, an, ld, a, act, P, W, XP);
+    launch_counter() += 1;
+}
+template <typename T>
+void launch_m_init(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const int* act, const cpx<T>* B, const MultiVecs<T>& v,
+                   const cpx<T>* YP, int have_y, double* part, BicgScalars* sc, int nsm, cudaStream_t st)
+{
+    int G = multi_grid(sm.nslots, a, nsm);
+    m_init_kernel<T><<<dim3(G, a), MB, 0, st>>>(sm, an, ld, act, B, v, YP, have_y, part);
+    m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(0, a, G, act, part, sc, nullptr);
+    launch_counter() += 2;
+}
+template <typename T>
+void launch_m_post(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const int* act, const MultiVecs<T>& v, const cpx<T>* YP,
+                   double* part, BicgScalars* sc, int nsm, cudaStream_t st)
+{
+    int G = multi_grid(sm.nslots, a, nsm);
+    m_post_kernel<T><<<dim3(G, a), MB, 0, st>>>(sm, an, ld, act, v, YP, part);
+    m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(1, a, G, act, part, sc, nullptr);
+    launch_counter() += 2;
+}
+template <typename T>
+void launch_m_upd(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, const double* epsv, int nsm,
+                  cudaStream_t st)
+{
+    int G = multi_grid(ld, a, nsm);
+    m_upd1_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v, part);
+    m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(2, a, G, act, part, sc, epsv);
+    m_upd2_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v);
+    launch_counter() += 3;
+}
+template <typename TB>
+void launch_m_resid(const SlotMaps& sm, const zd* an, int ld, int a, const int* act, const zd* B, const zd* X, const zd* YP, cpx<TB>* Rout,
+                    double* part, double* out2, int nsm, cudaStream_t st)
+{
+    int G = multi_grid(sm.nslots, a, nsm);
+    m_resid_kernel<TB><<<dim3(G, a), MB, 0, st>>>(sm, an, ld, act, B, X, YP, Rout, part);
+    m_sum2_kernel<<<(a + 63) / 64, 64, 0, st>>>(a, G, act, part, out2);
+    launch_counter() += 2;
+}
+template <typename TL> void launch_m_addcorr(int ld, int a, const int* dst, const int* src, zd* X, const cpx<TL>* D, cudaStream_t st)
+{
+    dim3 g(multi_grid(ld, a, 148), a);
+    m_addcorr_kernel<TL><<<g, MB, 0, st>>>(ld, dst, src, X, D);
+    launch_counter() += 1;
+}
+void launch_m_mie(const SlotMaps& sm, const zd* an, int ld, int ncols, const zd* X, zd* Y, cudaStream_t st)
+{
+    dim3 g(multi_grid(sm.nslots, ncols, 148), ncols);
+    m_mie_kernel<<<g, MB, 0, st>>>(sm, an, ld, X, Y);
+    launch_counter() += 1;
+}
+
+void launch_tm_rhs(int l, zd* P0, cudaStream_t st)
+{
+    int tot = 2 * l * (l + 2) * 2 * (2 * l + 1);
+    tm_rhs_kernel<<<(tot + 255) / 256, 256, 0, st>>>(l, P0);
+    launch_counter() += 1;
+}
+void launch_tm_qeff(int nsph, int ncols, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed,
+                    const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol, cudaStream_t st)
+{
+    int tot = nsph * ncols;
+    tm_qeff_kernel<<<(tot + 63) / 64, 64, 0, st>>>(nsph, ncols, order, offset, mie_offset, radius, rimed, an_inv, A, P, ld, qcol);
+    launch_counter() += 1;
+}
+void launch_tm_qsum(int nsph, int ncols, const double* qcol, const double* radius, double xv, double* sq, double* qsum, cudaStream_t st)
+{
+    tm_qsum_kernel<<<1, 256, 0, st>>>(nsph, ncols, qcol, radius, xv, sq, qsum);
+    launch_counter() += 1;
+}
+void launch_tm_store(int l, int tmo, const zd* A0, zd* tmat, cudaStream_t st)
+{
+    int tot = 2 * l * (l + 2) * 2 * (2 * l + 1);
+    tm_store_kernel<<<(tot + 255) / 256, 256, 0, st>>>(l, tmo, A0, tmat);
+    launch_counter() += 1;
+}
+void launch_tm_qext_qsca(int tmo, const zd* tmat, double xv, float* tc, double* out2, cudaStream_t st)
+{
+    size_t nblkt = 2 * (size_t)tmo * (tmo + 2);
+    int g = (int)std::min<size_t>((nblkt * nblkt + 255) / 256, 148 * 16);
+    tm_symm_kernel<<<g, 256, 0, st>>>(tmo, tmat, tc);
+    tm_qextsca_kernel<<<1, 256, 0, st>>>(tmo, tc, xv, out2);
+    launch_counter() += 2;
+}
+
+#define INST(T)                                                                                                                     \
+    template void launch_m_gather<T>(int, int, int, const int*, const cpx<T>*, cpx<T>*, int, cudaStream_t);                             \
+    template void launch_m_pack<T>(const SlotMaps&, const cpx<T>*, int, int, int, const int*, const cpx<T>*, const cpx<T>*, cpx<T>*, \
+                                   int, cudaStream_t);                                                                              \
+    template void launch_m_init<T>(const SlotMaps&, const cpx<T>*, int, int, const int*, const cpx<T>*, const MultiVecs<T>&,         \
+                                   const cpx<T>*, int, double*, BicgScalars*, int, cudaStream_t);                                   \
+    template void launch_m_post<T>(const SlotMaps&, const cpx<T>*, int, int, const int*, const MultiVecs<T>&, const cpx<T>*, double*, \
+                                   BicgScalars*, int, cudaStream_t);                                                                \
+    template void launch_m_upd<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, const double*, int, cudaStream_t);
+INST(double)
+INST(float)
+#undef INST
+template void launch_m_resid<double>(const SlotMaps&, const zd*, int, int, const int*, const zd*, const zd*, const zd*, zd*, double*, double*,
+                                     int, cudaStream_t);
+template void launch_m_resid<float>(const SlotMaps&, const zd*, int, int, const int*, const zd*, const zd*, const zd*, zf*, double*, double*,
+                                    int, cudaStream_t);
+template void launch_m_addcorr<float>(int, int, const int*, const int*, zd*, const zf*, cudaStream_t);
+template void launch_m_addcorr<double>(int, int, const int*, const int*, zd*, const zd*, cudaStream_t);

@@ -1,0 +1,50 @@
+// mrhs.cuh -- many-system BiCG vector kernels and T-matrix helpers (mrhs.cu).
+#pragma once
+#include "common.cuh"
+#include "bicg.cuh"
+
+// S systems are the columns of ld x S column-major blocks.  A launch works on
+// the a active systems listed in act[0..a) (device), system act[k] in grid row k.
+template <typename T> struct MultiVecs {
+    cpx<T> *X, *R, *P, *W, *Q, *CAP, *CAW;   // ld x S each
+};
+
+int multi_grid(int nslots, int a, int nsm);   // CTAs per system
+// XP[:, k] = X[:, act[k]] for k < a, zero for a <= k < apad
+template <typename T> void launch_m_gather(int ld, int a, int apad, const int* act, const cpx<T>* X, cpx<T>* XP, int nsm, cudaStream_t st);
+// XP[:, 2k] = P[:, act[k]], XP[:, 2k+1] = A^T conj(W[:, act[k]]); columns 2a .. 2apad-1 zeroed
+template <typename T>
+void launch_m_pack(const SlotMaps& sm, const cpx<T>* an, int ld, int a, int apad, const int* act, const cpx<T>* P, const cpx<T>* W,
+                   cpx<T>* XP, int nsm, cudaStream_t st);
+template <typename T>
+void launch_m_init(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const int* act, const cpx<T>* B, const MultiVecs<T>& v,
+                   const cpx<T>* YP, int have_y, double* part, BicgScalars* sc, int nsm, cudaStream_t st);
+template <typename T>
+void launch_m_post(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const int* act, const MultiVecs<T>& v, const cpx<T>* YP,
+                   double* part, BicgScalars* sc, int nsm, cudaStream_t st);
+template <typename T>
+void launch_m_upd(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, const double* epsv, int nsm,
+                  cudaStream_t st);   // epsv[s]: stopping threshold of system s (device)
+// FP64 true residual of system act[k]: Rout[:, k] = B - X + M YP[:, k] (rounded to TB);
+// out2[2 act[k]] = |r|^2, out2[2 act[k] + 1] = |b|^2
+template <typename TB>
+void launch_m_resid(const SlotMaps& sm, const zd* an, int ld, int a, const int* act, const zd* B, const zd* X, const zd* YP, cpx<TB>* Rout,
+                    double* part, double* out2, int nsm, cudaStream_t st);
+// X[:, dst[k]] += D[:, src[k]], k < a
+template <typename TL> void launch_m_addcorr(int ld, int a, const int* dst, const int* src, zd* X, const cpx<TL>* D, cudaStream_t st);
+// Y[:, k] = M X[:, k] for k < ncols (Mie multiply, idir = 1)
+void launch_m_mie(const SlotMaps& sm, const zd* an, int ld, int ncols, const zd* X, zd* Y, cudaStream_t st);
+
+// ---- T matrix (tmatrix_solution, mstm-solver-8.f90:22-332) ----
+// columns of order l: unit TE (q=1) / TM (q=2) field of degree k in the LR basis
+void launch_tm_rhs(int l, zd* P0, cudaStream_t st);
+// per-column, per-sphere efficiencies (qefficiencyfactors with npol = 1): qcol[3 (i + N c)]
+void launch_tm_qeff(int nsph, int ncols, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed,
+                    const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol, cudaStream_t st);
+// sphere_qeff(3,N) += sum over the columns (fixed order); qsum[0..2] = sum_i sphere_qeff r_i^2 / xv^2
+void launch_tm_qsum(int nsph, int ncols, const double* qcol, const double* radius, double xv, double* sphere_qeff, double* qsum,
+                    cudaStream_t st);
+// T-matrix columns of order l from the merged TE/TM coefficients A0 (nb(l) x 2(2l+1))
+void launch_tm_store(int l, int tmo, const zd* A0, zd* tmat, cudaStream_t st);
+// orientation-averaged Qext, Qsca from the single-precision symmetrised T matrix
+void launch_tm_qext_qsca(int tmo, const zd* tmat, double xv, float* tc, double* out2, cudaStream_t st);

@@ -3,7 +3,9 @@
 //     (tranordertest, december2023/mstm-modules-33.f90:1896-1942);
 //   * merge to the common origin: regular (J) translation of every sphere's
 //     expansion to the origin, converted from the LR to the TE/TM basis and
-//     summed (merge_to_common_origin, mstm-scatprops-26.f90:447-559);
+//     summed (merge_to_common_origin, mstm-scatprops-26.f90:447-559), and the
+//     reverse translation of an origin expansion to every sphere
+//     (distribute_from_common_origin, mstm-scatprops-26.f90:561-669);
 //   * GSF expansion of the azimuth-averaged scattering matrix
 //     (fosmexpansion, mstm-scatprops-26.f90:1820-1951);
 //   * its evaluation at polar angles (fosmcalc, mstm-scatprops-26.f90:1750-1810).
@@ -153,11 +155,15 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
     const int tid = threadIdx.x;
     const int T = a.T;
     zd* base = a.scratch + (size_t)blockIdx.x * a.scratch_stride;
+    const bool dist = (a.mode == 1);
     for (int i = blockIdx.x; i < a.nsph; i += gridDim.x) {
-        const int L = a.order[i];
-        const int nt = min(T, a.tord[i]);
+        const int Li = a.order[i];
+        const int L = dist ? T : Li;                       // source order
+        const int nt = dist ? Li : min(T, a.tord[i]);      // target order
         const int nmin = min(L, nt), nmax = max(L, nt);
-        const double rv0 = a.r0[0] - a.pos[3 * i], rv1 = a.r0[1] - a.pos[3 * i + 1], rv2 = a.r0[2] - a.pos[3 * i + 2];
+        const double sv = dist ? -1.0 : 1.0;               // translation vector: target - source
+        const double rv0 = sv * (a.r0[0] - a.pos[3 * i]), rv1 = sv * (a.r0[1] - a.pos[3 * i + 1]), rv2 = sv * (a.r0[2] - a.pos[3 * i + 2]);
+        const size_t soff = dist ? 0 : (size_t)a.offset[i];
         const double rr = rv0 * rv0 + rv1 * rv1 + rv2 * rv2;
         // scratch layout
         zd* xi = base;                                        // nt+L+2
@@ -180,8 +186,14 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
                     int n = 1;
                     while (n * (n + 2) <= e) n++;
                     int m = e - (n * n - 1) - n;   // e = n(n+1)-1+m ... -> m in -n..n
-                    zd v1 = src[(size_t)p * a.ld + a.offset[i] + aidx(m, n, 0, L)];
-                    zd v2 = src[(size_t)p * a.ld + a.offset[i] + aidx(m, n, 1, L)];
+                    zd v1 = src[(size_t)p * a.ld + soff + aidx(m, n, 0, L)];
+                    zd v2 = src[(size_t)p * a.ld + soff + aidx(m, n, 1, L)];
+                    if (dist) {
+                        zd* o = a.out + (size_t)p * a.ldo + a.offset[i];
+                        o[aidx(m, n, 0, nt)] = v1;
+                        o[aidx(m, n, 1, nt)] = v2;
+                        continue;
+                    }
                     int s = aidx(m, n, 0, T);
                     atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s].x, v1.x + v2.x);
                     atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s].y, v1.y + v2.y);
@@ -264,7 +276,7 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
             return o;
         };
         for (int p = 0; p < a.npol; p++) {
-            const zd* x = src + (size_t)p * a.ld + a.offset[i];
+            const zd* x = src + (size_t)p * a.ld + soff;
             // phase (shift_op = F: e^{+i m phi} on the source) and forward rotation of degrees l <= L
             for (int e = tid; e < 2 * L * (2 * nmin + 1); e += PP_NT) {
                 int q = e / (L * (2 * nmin + 1));
@@ -358,6 +370,12 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
                     for (int s = 0; s < ak; s++) em = ephi * em;
                     if (k > 0) em = cj(em);
                     gq[pm] = acc * em;
+                }
+                if (dist) {
+                    zd* od = a.out + (size_t)p * a.ldo + a.offset[i];
+                    od[aidx(k, n, 0, nt)] = gq[0];
+                    od[aidx(k, n, 1, nt)] = gq[1];
+                    continue;
                 }
                 int s = aidx(k, n, 0, T);
                 zd* o = a.amnp0 + (size_t)p * a.ld0;

@@ -3,7 +3,15 @@
 #include "common.cuh"
 #include <cstddef>
 
+// Regular (J) translation between the cluster origin and every sphere.
+// mode 0 (merge_to_common_origin): sphere block (order L_i, LR) -> origin block
+//   of order min(T, tord_i), converted to TE/TM and accumulated into amnp0;
+// mode 1 (distribute_from_common_origin): origin block of order T (LR, column p
+//   of amnp, leading dimension ld) -> sphere block of order L_i written to out.
 struct MergeArgs {
+    int mode;
+    zd* out;                // mode 1: ldo x npol sphere blocks (zeroed by the caller)
+    int ldo;
     int nsph;
     const double* pos;
     const int* order;

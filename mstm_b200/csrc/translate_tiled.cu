@@ -19,7 +19,11 @@
 //        C  axial translation  g = Z a'  (Z^T a' for i -> j)     per degree m
 //        D  back rotation + phase + shift, accumulated in smem   per degree n
 //   * the operator record of the next pair streams in with a bulk TMA copy
-//     (cp.async.bulk + mbarrier) while the current one is applied.
+//     (cp.async.bulk + mbarrier) while the current one is applied;
+//   * more than NR right-hand sides are split in chunks of NR columns; a work
+//     item is (tile, chunk) with the chunk varying fastest, so the CTAs that
+//     run the chunks of one tile at the same time read its operator records
+//     from L2 after the first one brought them from HBM.
 #include "common.cuh"
 #include "kernels.cuh"
 #include "translate_tiled.cuh"
@@ -135,39 +139,44 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
     __syncthreads();
 
     const int G = gridDim.x;
+    const int NI = a.ntiles * a.nchunk;   // work items (tile, chunk), chunk fastest
     int tcur = blockIdx.x;
-    if (tcur >= a.ntiles) return;
+    if (tcur >= NI) return;
+    auto tile_of = [&](int it) { return it / a.nchunk; };
+    auto col0 = [&](int it) { return (size_t)(it % a.nchunk) * NR * (size_t)a.ld; };
     // thread 0's iterators: operators two pairs ahead, sources one pair ahead
-    int pf_t = tcur, pf_q = a.tiles[tcur].x;
+    int pf_t = tcur, pf_q = a.tiles[tile_of(tcur)].x;
     bool pf_ok = true;
     auto pf_adv = [&]() {
         pf_q++;
-        if (pf_q >= a.tiles[pf_t].x + a.tiles[pf_t].y) {
+        const int4 ti = a.tiles[tile_of(pf_t)];
+        if (pf_q >= ti.x + ti.y) {
             pf_t += G;
-            if (pf_t >= a.ntiles) { pf_ok = false; return; }
-            pf_q = a.tiles[pf_t].x;
+            if (pf_t >= NI) { pf_ok = false; return; }
+            pf_q = a.tiles[tile_of(pf_t)].x;
         }
     };
-    auto load_sources = [&](int qq) {
+    auto load_sources = [&](int qq, int it) {
         const int2 pr = a.pairs[qq];
+        const cpx<T>* xs = a.x + col0(it);
         mb_expect(&bar[2], 2u * NR * XB);
         for (int r = 0; r < NR; r++) {
-            bulk_copy(W2 + (size_t)(0 * NR + r) * NB, a.x + (size_t)r * a.ld + (size_t)pr.y * NB, XB, &bar[2]);   // source of j -> i
-            bulk_copy(W2 + (size_t)(1 * NR + r) * NB, a.x + (size_t)r * a.ld + (size_t)pr.x * NB, XB, &bar[2]);   // source of i -> j
+            bulk_copy(W2 + (size_t)(0 * NR + r) * NB, xs + (size_t)r * a.ld + (size_t)pr.y * NB, XB, &bar[2]);   // source of j -> i
+            bulk_copy(W2 + (size_t)(1 * NR + r) * NB, xs + (size_t)r * a.ld + (size_t)pr.x * NB, XB, &bar[2]);   // source of i -> j
         }
     };
     if (tid == 0) {
-        load_sources(pf_q);
+        load_sources(pf_q, tcur);
         for (int b = 0; b < 2 && pf_ok; b++) {
             mb_expect(&bar[b], RECB);
             bulk_copy(opb + b * REC, a.ops + (size_t)pf_q * REC, RECB, &bar[b]);
             pf_adv();
         }
     }
-    int q = a.tiles[tcur].x;
+    int q = a.tiles[tile_of(tcur)].x;
     int t = 0;
     while (true) {
-        const int4 tinfo = a.tiles[tcur];
+        const int4 tinfo = a.tiles[tile_of(tcur)];
         const int i0 = tinfo.z >> 16, j0 = tinfo.z & 0xffff;   // block starts
         const int diag = tinfo.w;
         const int b = t & 1;
@@ -308,16 +317,16 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
 
         // ---- the next pair's sources stream into W2 while D runs ----
         if (tid == 0) {
-            int nq = q + 1;
+            int nq = q + 1, nit = tcur;
             bool have = true;
             if (nq >= tinfo.x + tinfo.y) {
-                int nt = tcur + G;
-                if (nt < a.ntiles) nq = a.tiles[nt].x;
+                nit = tcur + G;
+                if (nit < NI) nq = a.tiles[tile_of(nit)].x;
                 else have = false;
             }
             if (have) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                load_sources(nq);
+                load_sources(nq, nit);
             }
         }
 
@@ -375,6 +384,7 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
         // ---- end of tile: flush the tile's outputs with coalesced atomics ----
         const bool last = (q + 1 == tinfo.x + tinfo.y);
         if (last) {
+            cpx<T>* yc = a.y + col0(tcur);
             for (int idx = tid; idx < NSLOT * NR * NB; idx += NT) {
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
@@ -382,14 +392,14 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
                 const int sph = (slot < B) ? (i0 + slot) : (j0 + slot - B);
                 if (!(diag && slot >= B) && sph < a.nsph) {
                     cpx<T> v = ACC[idx];
-                    red_add<T>(a.y + (size_t)r * a.ld + (size_t)sph * NB + el, v);
+                    red_add<T>(yc + (size_t)r * a.ld + (size_t)sph * NB + el, v);
                 }
                 ACC[idx] = mk((T)0, (T)0);
             }
             __syncthreads();
             tcur += G;
-            if (tcur >= a.ntiles) break;
-            q = a.tiles[tcur].x;
+            if (tcur >= NI) break;
+            q = a.tiles[tile_of(tcur)].x;
         } else {
             q++;
         }
@@ -420,7 +430,7 @@ template <typename T, int L, int NR, int B> static int launch_one(const TiledArg
     if (per_sm < 1) per_sm = 1;
     if (per_sm > 2) per_sm = 2;
     int blocks = nsm * per_sm;
-    if (blocks > a.ntiles) blocks = a.ntiles;
+    if (blocks > a.ntiles * a.nchunk) blocks = a.ntiles * a.nchunk;
     if (blocks < 1) return 0;
     kern<<<blocks, 256, smem, st>>>(a);
     launch_counter() += 1;

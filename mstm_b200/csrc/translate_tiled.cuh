@@ -11,8 +11,9 @@ template <typename T> struct TiledArgs {
     const T* ops;            // records in pair order, op_record_units(L,L) each
     const cpx<T>* x;         // ld x nrhs
     cpx<T>* y;               // ld x nrhs, accumulated
-    int ld, nrhs, nsph;
-    unsigned contran;
+    int ld, nrhs, nsph;      // nrhs: columns per chunk (the kernel's NR)
+    int nchunk;              // chunks of nrhs columns: x and y hold nrhs * nchunk columns
+    unsigned contran;        // bit r: column r of every chunk is a conjugate-transpose product
     int* err;
 };
 

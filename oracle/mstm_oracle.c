@@ -1700,6 +1700,151 @@ void orc_merge_to_common_origin(const orc_ctx *c, int nodrt, const cplx *amnp, c
     }
 }
 
+/* distribute_from_common_origin (scatprops:561-669), one right-hand side,
+ * regular (J, vswf_type=1) functions: amnp (neqns) = translation of the
+ * nodrt common-origin block amnp0 (LR basis) from r0 to every sphere. */
+void orc_distribute_from_common_origin(const orc_ctx *c, int nodrt, const cplx *amnp0, const double *r0, cplx *amnp)
+{
+    for (int k = 0; k < c->neqns; k++) amnp[k] = 0;
+    axialtrancoefinit(imax(nodrt, c->max_order));
+    for (int i = 0; i < c->n; i++) {
+        int noi = c->order[i];
+        double rv[3] = {c->pos[3 * i] - r0[0], c->pos[3 * i + 1] - r0[1], c->pos[3 * i + 2] - r0[2]};
+        pairop_t op;
+        pairop_compute(&op, noi, nodrt, rv, 1, c->rimed);
+        coefficient_translation(nodrt, noi, amnp0, amnp + c->offset[i], &op, 0, 0);
+        pairop_free(&op);
+    }
+}
+
+/* tmatrix_solution (solver:22-332) on one process with the iterative solver:
+ * for l = 1..tmo and the 2(2l+1) columns (k, q) of order l, the unit
+ * common-origin field of degree k, order l and TE (q=1) / TM (q=2) mode is
+ * distributed to the spheres, multiplied by the Mie coefficients, solved by
+ * cbicg (initial guess = right-hand side), merged back to the origin, and
+ * stored as T-matrix column 2(l(l+1)+k-1)+q-1 (rows 2(n(n+1)+m-1)+p-1, n <= l;
+ * tmat is nblkt x nblkt column-major, nblkt = 2 tmo (tmo+2)).  The per-sphere
+ * efficiencies of every column (qefficiencyfactors with npol=1) are summed in
+ * sphere_qeff(3,N); the order loop stops after the order at which the
+ * summed extinction changes by less than conveps (qeff(1) - qeffold(1), signed).
+ * Returns istat; *order_used = the T-matrix order kept (t_matrix_order). */
+int orc_tmatrix_solution(orc_ctx *c, int tmo, const int *trans_order, const double *r0, double solneps, double conveps,
+                         int niter, cplx *tmat, double *sphere_qeff, int *order_used, int *maxiter_o, double *maxerr_o)
+{
+    int neq = c->neqns, nblkt = 2 * tmo * (tmo + 2), istat = 0, initialize = 1, maxiter = 0;
+    double maxerr = 0.0, qeffold = 0.0, xv = orc_vol_radius(c);
+    for (size_t k = 0; k < (size_t)nblkt * nblkt; k++) tmat[k] = 0;
+    for (int k = 0; k < 3 * c->n; k++) sphere_qeff[k] = 0.0;
+    cplx *pmnpkq = (cplx *)malloc(sizeof(cplx) * neq), *pmnpan = (cplx *)malloc(sizeof(cplx) * neq);
+    cplx *amnpkq = (cplx *)malloc(sizeof(cplx) * neq), *gmnp = (cplx *)malloc(sizeof(cplx) * neq);
+    int l;
+    for (l = 1; l <= tmo; l++) {
+        int nb = 2 * l * (l + 2);
+        cplx *pmnp0 = (cplx *)malloc(sizeof(cplx) * nb), *amnp0 = (cplx *)malloc(sizeof(cplx) * nb);
+        for (int kq = 1; kq <= 2 * (2 * l + 1); kq++) {
+            int k = -l + (kq - 1) / 2, q = (kq - 1) % 2 + 1;
+            for (int e = 0; e < nb; e++) pmnp0[e] = 0;
+            /* the T matrix is TE-TM based: unit TE / TM field in the LR basis */
+            pmnp0[AIDX(k < 0 ? l + 1 : k, k < 0 ? -k : l, 0, l)] = 0.5;
+            pmnp0[AIDX(k < 0 ? l + 1 : k, k < 0 ? -k : l, 1, l)] = -0.5 * pm1(q);
+            orc_distribute_from_common_origin(c, l, pmnp0, r0, pmnpkq);
+            multmiecoeffmult(c, 1, pmnpkq, pmnpan, c->an);
+            memcpy(amnpkq, pmnpan, sizeof(cplx) * neq);
+            if (niter != 0) {
+                int iter = 0;
+                double serr = 0.0;
+                orc_cbicg(c, niter, solneps, pmnpan, amnpkq, initialize, &iter, &serr);
+                maxiter = imax(iter, maxiter);
+                maxerr = serr > maxerr ? serr : maxerr;
+                if (iter > niter || serr > solneps) istat = 1;
+            }
+            initialize = 0;
+            /* qefficiencyfactors(npol=1): the first-polarisation terms of lrsphereqeff */
+            for (int i = 0; i < c->n; i++)
+                mie_mult_sphere(c->an_inv + c->mie_offset[i], c->order[i], 1, amnpkq + c->offset[i], gmnp + c->offset[i]);
+            for (int i = 0; i < c->n; i++) {
+                double qe[3], qs[3], qa[3];
+                int off = c->offset[i];
+                lrsphereqeff(c->rimed, c->order[i], c->rad[i], amnpkq + off, 0, pmnpkq + off, gmnp + off, qe, qs, qa);
+                sphere_qeff[3 * i] += qe[0];
+                sphere_qeff[3 * i + 1] += qa[0];
+                sphere_qeff[3 * i + 2] += qs[0];
+            }
+            orc_merge_to_common_origin(c, l, amnpkq, r0, trans_order, amnp0);
+            int col = 2 * (l * (l + 1) + k - 1) + q - 1;
+            for (int n = 1; n <= l; n++)
+                for (int m = -n; m <= n; m++)
+                    for (int p = 0; p < 2; p++)
+                        tmat[(size_t)(2 * (n * (n + 1) + m - 1) + p) + (size_t)nblkt * col] =
+                            amnp0[AIDX(m < 0 ? n + 1 : m, m < 0 ? -m : n, p, l)];
+        }
+        free(pmnp0);
+        free(amnp0);
+        double qext = 0.0;
+        for (int i = 0; i < c->n; i++) qext = qext + sphere_qeff[3 * i] * c->rad[i] * c->rad[i] / (xv * xv);
+        double converr = qext - qeffold;
+        qeffold = qext;
+        if (conveps > 0.0 && converr < conveps) break;
+    }
+    *order_used = l < tmo ? l : tmo;
+    *maxiter_o = maxiter;
+    *maxerr_o = maxerr;
+    free(pmnpkq); free(pmnpan); free(amnpkq); free(gmnp);
+    return istat;
+}
+
+/* The T matrix as ranorientscatmatrix holds it after reading the file
+ * (scatprops:2031-2075): complex(4) storage tc(2,nblk,2,nblk) with the
+ * computed entries (rows of order n <= l in the column of order l) and the
+ * rest from the symmetry tc(q,l(l+1)-k,p,n(n+1)-m) = (-1)^(m+k) tc(p,n(n+1)+m,q,l(l+1)+k)
+ * for n < l.  tmat: nblkt x nblkt column-major as orc_tmatrix_solution
+ * writes it; tc: the same layout in single precision. */
+void orc_tmatrix_symmetrize(int tmo, const cplx *tmat, float _Complex *tc)
+{
+    int nblkt = 2 * tmo * (tmo + 2);
+    for (size_t k = 0; k < (size_t)nblkt * nblkt; k++) tc[k] = 0;
+#define TIX(p, mn, q, kl) ((size_t)(2 * ((mn) - 1) + (p) - 1) + (size_t)nblkt * (size_t)(2 * ((kl) - 1) + (q) - 1))
+    for (int l = 1; l <= tmo; l++)
+        for (int k = -l; k <= l; k++) {
+            int kl = l * (l + 1) + k, klm = l * (l + 1) - k;
+            for (int q = 1; q <= 2; q++)
+                for (int n = 1; n <= l; n++)
+                    for (int m = -n; m <= n; m++) {
+                        int mn = n * (n + 1) + m, mnm = n * (n + 1) - m;
+                        for (int p = 1; p <= 2; p++) {
+                            cplx t = tmat[TIX(p, mn, q, kl)];
+                            tc[TIX(p, mn, q, kl)] = (float)creal(t) + I * (float)cimag(t);
+                        }
+                        if (n < l) {
+                            float ikm = (float)pm1(m + k);
+                            for (int p = 1; p <= 2; p++) tc[TIX(q, klm, p, mnm)] = tc[TIX(p, mn, q, kl)] * ikm;
+                        }
+                    }
+        }
+#undef TIX
+}
+
+/* Orientation-averaged extinction and scattering efficiencies from the T
+ * matrix (ranorientscatmatrix, scatprops:2103-2122), summed over the
+ * single-precision symmetrised matrix; xv = cross_section_radius. */
+void orc_tmatrix_qext_qsca(int tmo, const cplx *tmat, double xv, double *qext, double *qsca)
+{
+    int nblkt = 2 * tmo * (tmo + 2);
+    float _Complex *tc = (float _Complex *)malloc(sizeof(float _Complex) * (size_t)nblkt * nblkt);
+    orc_tmatrix_symmetrize(tmo, tmat, tc);
+    double qe = 0.0, qs = 0.0;
+    for (int col = 0; col < nblkt; col++) {
+        for (int row = 0; row < nblkt; row++) {
+            float a = cabsf(tc[(size_t)row + (size_t)nblkt * col]);
+            qs = qs + (double)(a * a);
+        }
+        qe = qe - (double)crealf(tc[(size_t)col + (size_t)nblkt * col]);
+    }
+    free(tc);
+    *qext = qe * 2.0 / (xv * xv);
+    *qsca = qs * 2.0 / (xv * xv);
+}
+
 /* fosmexpansion (scatprops:1820-1951): GSF expansion coefficients of the
  * azimuth-averaged scattering matrix.  amnp0: (nb(ntot), 2 polarisations).
  * s00..sm22: 16*(2ntot+1) each, Fortran (4,4,0:2ntot) order. */

@@ -72,6 +72,12 @@ def lib():
         L.orc_merge_to_common_origin.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]
         L.orc_fosmexpansion.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
         L.orc_fosmcalc.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_void_p]
+        L.orc_distribute_from_common_origin.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p]
+        L.orc_tmatrix_solution.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_int, c_void_p,
+                                           c_void_p, P(c_int), P(c_int), P(c_double)]
+        L.orc_tmatrix_solution.restype = c_int
+        L.orc_tmatrix_symmetrize.argtypes = [c_int, c_void_p, c_void_p]
+        L.orc_tmatrix_qext_qsca.argtypes = [c_int, c_void_p, c_double, P(c_double), P(c_double)]
         _lib = L
     return _lib
 
@@ -194,6 +200,39 @@ class Oracle:
             out[:, p] = o
         return out
 
+    def distribute_from_common_origin(self, amnp0, nodrt, origin):
+        """amnp0: (nb(nodrt), nrhs) LR common-origin coefficients -> (neqns, nrhs) regular expansions about each sphere."""
+        amnp0 = np.asfortranarray(amnp0, np.complex128)
+        out = np.zeros((self.neqns, amnp0.shape[1]), np.complex128, order="F")
+        r0 = np.ascontiguousarray(origin, np.float64)
+        for p in range(amnp0.shape[1]):
+            col = np.ascontiguousarray(amnp0[:, p])
+            o = np.zeros(self.neqns, np.complex128)
+            self.L.orc_distribute_from_common_origin(self.ctx, nodrt, _p(col), _p(r0), _p(o))
+            out[:, p] = o
+        return out
+
+    def tmatrix_solution(self, tmo=None, trans_eps=1.0e-5, maxt=100, solution_eps=1.0e-6, convergence_eps=1.0e-6,
+                         max_iterations=10000):
+        """tmatrix_solution: dict(tmat (nblkt, nblkt), order, sphere_qeff (3, N), qtot (ext, abs, sca),
+        status, maxiter, maxerr, origin, trans_order)."""
+        nt, origin, to = self.t_matrix_order(trans_eps, maxt)
+        if tmo is None:
+            tmo = nt
+        nblkt = 2 * tmo * (tmo + 2)
+        tmat = np.zeros((nblkt, nblkt), np.complex128, order="F")
+        sq = np.zeros((3, self.n), np.float64, order="F")
+        used, mi, me = c_int(0), c_int(0), c_double(0.0)
+        st = self.L.orc_tmatrix_solution(self.ctx, tmo, _p(np.ascontiguousarray(to, np.int32)), _p(origin), solution_eps,
+                                         convergence_eps, max_iterations, _p(tmat), _p(sq), ctypes.byref(used),
+                                         ctypes.byref(mi), ctypes.byref(me))
+        xv = self.vol_radius()
+        r2 = np.asarray(self.rad) ** 2 / xv ** 2
+        qt = (sq * r2[None, :]).sum(axis=1)
+        qtot = np.array([qt[0], qt[1], qt[0] + qt[2] - qt[1]])
+        return dict(tmat=tmat, order=used.value, tmo=tmo, sphere_qeff=sq, qtot=qtot, status=st, maxiter=mi.value,
+                    maxerr=me.value, origin=origin, trans_order=to)
+
     def scattering(self, amnp, trans_eps=1.0e-5, maxt=100, nangles=181):
         """fosmexpansion + fosmcalc: returns dict(ntot, s00.., g, smat (nangles,4,4))."""
         nt, origin, to = self.t_matrix_order(trans_eps, maxt)
@@ -285,3 +324,19 @@ def gentranmatrix(ns, nt, rvec, vtype=3):
     ac = np.zeros(nbt * nbs * 2, np.complex128)
     L.orc_x_gentranmatrix(ns, nt, _p(rv), vtype, _p(ac))
     return ac.reshape(2, nbs, nbt).transpose(2, 1, 0)  # [row kla, col mna, mode]
+
+
+def tmatrix_symmetrize(tmo, tmat):
+    """The complex(4) T matrix as the random-orientation reader fills it."""
+    nblkt = 2 * tmo * (tmo + 2)
+    tmat = np.asfortranarray(tmat, np.complex128)
+    tc = np.zeros((nblkt, nblkt), np.complex64, order="F")
+    lib().orc_tmatrix_symmetrize(tmo, _p(tmat), _p(tc))
+    return tc
+
+
+def tmatrix_qext_qsca(tmo, tmat, xv):
+    tmat = np.asfortranarray(tmat, np.complex128)
+    qe, qs = c_double(0.0), c_double(0.0)
+    lib().orc_tmatrix_qext_qsca(tmo, _p(tmat), xv, ctypes.byref(qe), ctypes.byref(qs))
+    return qe.value, qs.value

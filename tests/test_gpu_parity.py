@@ -202,3 +202,38 @@ def test_scattering_postprocessing(api, oracle_mod, name):
     sgm = gm.scattering(gm.fixedorsoln(eps=1e-12, niter=4000)["amnp"])
     assert np.abs(sgm["smat"] - so["smat"]).max() <= 1e-4 * s11max
     assert abs(sgm["g"] - so["g"]) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["cluster8", "cluster20"])
+def test_tmatrix_fp64(api, oracle_mod, name):
+    """tmatrix_solution: the many-column FP64 solve follows cbicg per column, so
+    the T matrix, the per-sphere sums and the order kept match the oracle."""
+    pos, rad, ri, em = _cluster(name)
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em)
+    ro = o.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-10)
+    T = g.t_matrix_order()
+    assert T == ro["tmo"]
+    rg = g.tmatrix_solution(T, solution_eps=1e-10, convergence_eps=1e-6)
+    assert rg["istat"] == 0 and rg["order"] == ro["order"]
+    assert abs(rg["maxiter"] - ro["maxiter"]) <= 1
+    assert np.abs(rg["tmat"] - ro["tmat"]).max() <= RTOL_FP64 * np.abs(ro["tmat"]).max()
+    assert np.allclose(rg["qtot"], ro["qtot"], rtol=RTOL_FP64)
+    assert np.abs(rg["sphere_qeff"] - ro["sphere_qeff"]).max() <= RTOL_FP64 * np.abs(ro["sphere_qeff"]).max()
+    qe, qs = g.tmatrix_qext_qsca(rg["tmat"], T)
+    qe_o, qs_o = oracle_mod.tmatrix_qext_qsca(T, rg["tmat"], o.vol_radius())
+    assert abs(qe / qe_o - 1) < 1e-12 and abs(qs / qs_o - 1) < 1e-12
+    # the two routes to the orientation averages agree (single-precision T entries)
+    assert abs(qe / rg["qtot"][0] - 1) < 1e-6 and abs(qs / rg["qtot"][2] - 1) < 1e-6
+
+
+def test_tmatrix_mixed(api, oracle_mod):
+    """FP32 column solves inside FP64 refinement, all columns together: the
+    orientation-averaged efficiencies within 1e-6 of the FP64 oracle."""
+    pos, rad, ri, em = _cluster("cluster20")
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em, precision="mixed")
+    ro = o.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-14)
+    T = g.t_matrix_order()
+    rg = g.tmatrix_solution(T, solution_eps=1e-14, convergence_eps=1e-6)
+    assert rg["istat"] == 0 and rg["order"] == ro["order"] and rg["outer"] >= 1
+    assert np.allclose(rg["qtot"], ro["qtot"], rtol=RTOL_MIXED)
+    assert np.abs(rg["tmat"] - ro["tmat"]).max() <= 1e-6 * np.abs(ro["tmat"]).max()

@@ -14,6 +14,8 @@ import os
 import numpy as np
 import pytest
 
+from mstm_b200 import configs as C
+
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
@@ -189,3 +191,70 @@ def test_scattering_invariant_under_cluster_shift(oracle_mod):
     assert s1["t_matrix_order"] == s2["t_matrix_order"]
     assert abs(s1["g"] - s2["g"]) < 1e-9
     assert np.abs(s1["smat"] - s2["smat"]).max() < 1e-8 * np.abs(s1["smat"][:, 0, 0]).max()
+
+
+def _te_tm_rows(col, T):
+    """LR block a(0:T+1,1:T,1:2) -> T-matrix row order 2(n(n+1)+m-1)+p-1 in the TE/TM basis (L+R, L-R)."""
+    h = T * (T + 2)
+    v = np.zeros(2 * h, complex)
+    for n in range(1, T + 1):
+        for m in range(-n, n + 1):
+            s = (m + (T + 2) * (n - 1)) if m >= 0 else ((n + 1) + (T + 2) * (-m - 1))
+            v[2 * (n * (n + 1) + m - 1)] = col[s] + col[s + h]
+            v[2 * (n * (n + 1) + m - 1) + 1] = col[s] - col[s + h]
+    return v
+
+
+def _rows(col, T):
+    """TE/TM block a(0:T+1,1:T,1:2) -> T-matrix row order."""
+    h = T * (T + 2)
+    v = np.zeros(2 * h, complex)
+    for n in range(1, T + 1):
+        for m in range(-n, n + 1):
+            s = (m + (T + 2) * (n - 1)) if m >= 0 else ((n + 1) + (T + 2) * (-m - 1))
+            v[2 * (n * (n + 1) + m - 1)] = col[s]
+            v[2 * (n * (n + 1) + m - 1) + 1] = col[s + h]
+    return v
+
+
+def test_tmatrix_single_sphere_is_mie(oracle_mod):
+    """tmatrix_solution of one sphere at the origin: a diagonal T matrix whose
+    orientation averages equal the sphere's Mie efficiencies."""
+    o = oracle_mod.Oracle([[0.0, 0.0, 0.0]], [1.0], [1.5 + 0.01j], mie_eps=-7)
+    r = o.tmatrix_solution(tmo=7, convergence_eps=0.0, solution_eps=1e-12)
+    T = r["tmat"]
+    assert np.abs(T - np.diag(np.diag(T))).max() == 0.0
+    f = o.fixedorsoln(eps=1e-12)
+    assert np.allclose(r["qtot"], f["qtot"][:, 0], rtol=1e-12)
+    qe, qs = oracle_mod.tmatrix_qext_qsca(7, T, o.vol_radius())
+    assert abs(qe / f["qtot"][0, 0] - 1) < 1e-6 and abs(qs / f["qtot"][2, 0] - 1) < 1e-6
+
+
+def test_tmatrix_reproduces_fixed_orientation(oracle_mod):
+    """The symmetrised T matrix applied to the plane wave's expansion at the
+    cluster origin gives the merged fixed-orientation solution (the T-matrix
+    and the direct route meet; single-precision T entries bound the match)."""
+    w = C.workload("cluster8")
+    o = oracle_mod.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-w["order"])
+    r = o.tmatrix_solution(convergence_eps=0.0, solution_eps=1e-12)
+    T = r["tmo"]
+    f = o.fixedorsoln(eps=1e-12)
+    a0 = o.merge_to_common_origin(f["amnp"], T, r["origin"], r["trans_order"])
+    p = oracle_mod.Oracle([r["origin"]], [1.0], [1.5], mie_eps=-T).planewave()
+    full = oracle_mod.tmatrix_symmetrize(T, r["tmat"]).astype(complex)
+    for pol in range(2):
+        y = full @ _te_tm_rows(p[:, pol], T)
+        ref = _rows(a0[:, pol], T)
+        assert np.abs(y - ref).max() < 5e-6 * np.abs(ref).max()
+
+
+def test_tmatrix_efficiency_sum_rule(oracle_mod):
+    """Orientation-averaged Qext/Qsca from the T-matrix trace equal the sums of
+    the per-column sphere efficiencies (two independent routes)."""
+    w = C.workload("cluster8")
+    o = oracle_mod.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-w["order"])
+    r = o.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-10)
+    assert 1 <= r["order"] < r["tmo"]
+    qe, qs = oracle_mod.tmatrix_qext_qsca(r["tmo"], r["tmat"], o.vol_radius())
+    assert abs(qe / r["qtot"][0] - 1) < 1e-6
+    assert abs(qs / r["qtot"][2] - 1) < 1e-6
