@@ -153,6 +153,21 @@ int mstmg_tmatrix(mstmg_ctx *ctx, int t_matrix_order, double solution_eps, doubl
  * xv = the context's volume-equivalent radius (cross_section_radius). */
 int mstmg_tmatrix_qext_qsca(mstmg_ctx *ctx, int t_matrix_order, const double *tmat, double *qext, double *qsca);
 
+/* Replaces ranorientscatmatrix (mstm-scatprops-26.f90:1963-2530, no Gaussian
+ * beam) and its evaluation ranorienscatmatrixcalc (:2538-2592) as
+ * main_calling_program calls them (mstm-input-37.f90:1431-1445): the GSF
+ * expansion of the orientation-averaged scattering matrix from a T matrix of
+ * order t_matrix_order (<= 60; layout as mstmg_tmatrix writes it), with the
+ * entries rounded to single precision and the symmetric rows filled as the
+ * reference's T-matrix reader does.
+ *   sm, smcf: 16 x (2T+1) expansion coefficients, Fortran sm(4,4,0:2T), total
+ *     and coherent part (either may be NULL); smcf(1,1,0) is the coherent
+ *     scattering ratio;
+ *   smat: 16 x nangles elements at theta_i = i pi/(nangles-1) (may be NULL,
+ *     nangles 0 to skip). */
+int mstmg_ranorient_scattering(mstmg_ctx *ctx, int t_matrix_order, const double *tmat, int nangles, double *sm, double *smcf,
+                               double *smat);
+
 /* Statistics of the last solve: iterations per polarisation, refinement steps,
  * FP64 and FP32 operator passes. */
 int mstmg_last_stats(const mstmg_ctx *ctx, int *iters2, int *outer, int *passes64, int *passes32);

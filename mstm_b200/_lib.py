@@ -35,6 +35,7 @@ SIGNATURES = {
     "mstmg_tmatrix": (c_int, [c_void_p, c_int, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p, P(c_int), P(c_int),
                               P(c_double)]),
     "mstmg_tmatrix_qext_qsca": (c_int, [c_void_p, c_int, c_void_p, P(c_double), P(c_double)]),
+    "mstmg_ranorient_scattering": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "mstmg_last_stats": (c_int, [c_void_p, c_void_p, P(c_int), P(c_int), P(c_int)]),
     "mstmg_operator_bytes": (c_int, [c_void_p, c_int, P(c_double), P(c_double)]),
     "mstmg_time_translation": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),

@@ -192,6 +192,26 @@ class SphereCluster:
               "tmatrix_qext_qsca")
         return qe.value, qs.value
 
+    def ranorientscatmatrix(self, tmat, t_matrix_order, nangles=181):
+        """Orientation-averaged scattering matrix from the T matrix: GSF expansion
+        coefficients sm, smcf (2T+1, 4, 4) [w][i][j] (total and coherent part),
+        the elements smat (nangles, 4, 4) at theta_i = i*pi/(nangles-1), and the
+        coherent scattering ratio smcf[0,0,0]."""
+        T = int(t_matrix_order)
+        W = 2 * T + 1
+        tmat = np.asfortranarray(tmat, np.complex128)
+        sm = np.zeros(16 * W)
+        cf = np.zeros(16 * W)
+        smat = np.zeros(16 * max(nangles, 1))
+        check(self._L.mstmg_ranorient_scattering(self.ctx, T, _ptr(tmat), nangles, _ptr(sm), _ptr(cf), _ptr(smat)),
+              "ranorientscatmatrix")
+        sm3 = sm.reshape(W, 4, 4).transpose(0, 2, 1).copy()
+        cf3 = cf.reshape(W, 4, 4).transpose(0, 2, 1).copy()
+        out = dict(sm=sm3, smcf=cf3, coherent=cf3[0, 0, 0])
+        if nangles > 0:
+            out["smat"] = smat.reshape(nangles, 4, 4).transpose(0, 2, 1).copy()
+        return out
+
     def last_stats(self):
         it = np.zeros(2, np.int32)
         outer, p64, p32 = c_int(0), c_int(0), c_int(0)

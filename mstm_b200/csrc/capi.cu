@@ -15,6 +15,7 @@
 #include "translate_tiled.cuh"
 #include "postproc.cuh"
 #include "mrhs.cuh"
+#include "ranorient.cuh"
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
@@ -1535,6 +1536,66 @@ extern "C" int mstmg_tmatrix_qext_qsca(mstmg_ctx* c, int t_matrix_order, const d
     if (qext) *qext = h[0];
     if (qsca) *qsca = h[1];
     return MSTMG_OK;
+}
+
+extern "C" int mstmg_ranorient_scattering(mstmg_ctx* c, int t_matrix_order, const double* tmat, int nangles, double* sm, double* smcf,
+                                          double* smat)
+{
+    const int T = t_matrix_order;
+    if (!c || T < 1 || T > 60 || !tmat || (nangles > 0 && nangles < 2)) {
+        set_err("mstmg_ranorient_scattering: bad arguments (1 <= t_matrix_order <= 60, nangles 0 or >= 2)");
+        return MSTMG_ERR_ARG;
+    }
+    BigTablesDev bt;
+    int rc = upload_big(c, bt);
+    if (rc) return rc;
+    const size_t nblkt = 2 * (size_t)T * (T + 2);
+    const int W = 2 * T + 1;
+    DevBuf<zd> dT, trace, dm, dmcf, fm;
+    DevBuf<float2> tc;
+    DevBuf<double> dsm, dsmat, vscr, dscr, dbcd;
+    CK(dT.alloc(nblkt * nblkt));
+    CK(copy_in(dT.p, tmat, sizeof(zd) * nblkt * nblkt, c->st));
+    CK(tc.alloc(nblkt * nblkt));
+    CK(trace.alloc(4 * (size_t)T));
+    CK(dm.alloc(ro_dm_elems(T)));
+    CK(dmcf.alloc(ro_dm_elems(T)));
+    CK(cudaMemsetAsync(dm.p, 0, sizeof(zd) * ro_dm_elems(T), c->st));
+    CK(cudaMemsetAsync(dmcf.p, 0, sizeof(zd) * ro_dm_elems(T), c->st));
+    CK(fm.alloc((size_t)W * 2 * 3 * T * 2 * T * 2));
+    CK(dsm.alloc(2 * 16 * (size_t)W));
+    CK(vscr.alloc(ro_vscr_doubles(T, c->nsm)));
+    const int nang = nangles > 0 ? nangles : 1;
+    CK(dscr.alloc((size_t)nang * (16 * (2 * T) + 40)));
+    CK(dsmat.alloc(16 * (size_t)nang));
+    std::vector<double> bd(2 * T + 4);
+    for (int k = 0; k < (int)bd.size(); k++) bd[k] = big_tables().bc(k, k);
+    CK(dbcd.alloc(bd.size()));
+    CK(cudaMemcpyAsync(dbcd.p, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice, c->st));
+    RoArgs a;
+    a.nodr = T;
+    a.tc = tc.p;
+    a.trace = trace.p;
+    a.dm = dm.p;
+    a.dmcf = dmcf.p;
+    a.fm = fm.p;
+    a.sm = dsm.p;
+    a.smcf = dsm.p + 16 * W;
+    a.bcof = bt.bc.p;
+    a.fnr = bt.fnr.p;
+    a.nbc = bt.nbc;
+    a.vscr = vscr.p;
+    a.rimed_re = c->opts.medium_re;
+    if (launch_ranorient(a, dT.p, nangles, dbcd.p, dscr.p, dsmat.p, c->nsm, c->st) != 0) {
+        set_err("mstmg_ranorient_scattering: t_matrix_order too large for the shared-memory layout");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    CK(cudaGetLastError());
+    if (sm) CK(copy_out(sm, dsm.p, sizeof(double) * 16 * W, c->st));
+    if (smcf) CK(copy_out(smcf, dsm.p + 16 * W, sizeof(double) * 16 * W, c->st));
+    if (smat && nangles > 0) CK(copy_out(smat, dsmat.p, sizeof(double) * 16 * (size_t)nangles, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return check_kernel_err(c);
 }
 
 extern "C" int mstmg_set_stream(mstmg_ctx* c, void* stream)

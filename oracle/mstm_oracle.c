@@ -1845,6 +1845,270 @@ void orc_tmatrix_qext_qsca(int tmo, const cplx *tmat, double xv, double *qext, d
     *qsca = qs * 2.0 / (xv * xv);
 }
 
+/* ranorientscatmatrix (scatprops:1963-2530), beam_width 0, one process:
+ * GSF expansion coefficients sm(4,4,0:2nodr) and smcf (the coherent part)
+ * of the orientation-averaged scattering matrix from the T matrix of order
+ * nodr (tmat as orc_tmatrix_solution stores it; read into complex(4) and
+ * symmetrised exactly as the reference's file reader does), divided by
+ * 2 Re(medium index).  sm, smcf: 16 * (2 nodr + 1), Fortran (4,4,0:2nodr). */
+void orc_ranorientscatmatrix(int nodr, const cplx *tmat, double rimed_re, double *sm, double *smcf)
+{
+    tables_init();
+    const int nodr2 = 2 * nodr, nodrw = nodr2, nblk = nodr * (nodr + 2), nblkt = 2 * nblk;
+    float _Complex *tc = (float _Complex *)malloc(sizeof(float _Complex) * (size_t)nblkt * nblkt);
+    orc_tmatrix_symmetrize(nodr, tmat, tc);
+#define TC(p, mn, q, kl) tc[(size_t)(2 * ((mn) - 1) + (p) - 1) + (size_t)nblkt * (size_t)(2 * ((kl) - 1) + (q) - 1)]
+    /* the GB-modified T matrix (no beam: gbn = 1), stored back in single precision */
+    for (int n = 1; n <= nodr; n++)
+        for (int m = -n; m <= n; m++) {
+            int mn = n * (n + 1) + m;
+            for (int p = 1; p <= 2; p++)
+                for (int l = 1; l <= nodr; l++) {
+                    cplx pp11 = -0.5 * ipow(l + 1) * FNR(l + l + 1);
+                    cplx pp21 = -pp11, pp12 = -pp11, pp22 = pp21;
+                    for (int k = -l; k <= l; k++) {
+                        int kl = l * (l + 1) + k;
+                        cplx a = TC(p, mn, 1, kl);
+                        cplx t1 = (cplx)TC(p, mn, 1, kl) * pp11 + (cplx)TC(p, mn, 2, kl) * pp12;
+                        TC(p, mn, 1, kl) = (float)creal(t1) + I * (float)cimag(t1);
+                        cplx t2 = a * pp21 + (cplx)TC(p, mn, 2, kl) * pp22;
+                        TC(p, mn, 2, kl) = (float)creal(t2) + I * (float)cimag(t2);
+                    }
+                }
+        }
+    const int U = nodr + 1, ldu = 2 * U + 1;
+    size_t dmsz = (size_t)ldu * 3 * nodr * 2 * nodr * 2;
+    cplx *dm = (cplx *)calloc(dmsz, sizeof(cplx)), *dmcf = (cplx *)calloc(dmsz, sizeof(cplx));
+#define DM(arr, u, ku, n, p, n1, p1) arr[((u) + U) + (size_t)ldu * ((ku) - 1 + 3 * (((n) - 1) + nodr * (((p) - 1) + 2 * (((n1) - 1) + nodr * ((p1) - 1)))))]
+    cplx *bm = (cplx *)malloc(sizeof(cplx) * 2 * nblk * 2), *bmcf = (cplx *)malloc(sizeof(cplx) * 2 * nblk * 2);
+    cplx *am = (cplx *)malloc(sizeof(cplx) * 2 * (nodr + 1) * 2), *amcf = (cplx *)malloc(sizeof(cplx) * 2 * (nodr + 1) * 2);
+#define BM(arr, k, mn, p) arr[((k) - 1) + 2 * (((mn) - 1) + nblk * ((p) - 1))]
+#define AM(arr, k, l, p) arr[((k) - 1) + 2 * (((l) - 1) + (nodr + 1) * ((p) - 1))]
+    double *vc = (double *)malloc(sizeof(double) * (4 * nodr + 3));
+    for (int w = 0; w <= nodr2; w++)
+        for (int v = -w; v <= w; v++) {
+            for (size_t e = 0; e < (size_t)2 * nblk * 2; e++) { bm[e] = 0; bmcf[e] = 0; }
+            for (int n = 1; n <= nodr; n++) {
+                int nn1 = n * (n + 1);
+                for (int l = imax(1, iabs_(w - n)); l <= imin(nodr, w + n); l++)
+                    for (int k = 1; k <= 2; k++)
+                        for (int p = 1; p <= 2; p++) { AM(am, k, l, p) = 0; AM(amcf, k, l, p) = 0; }
+                for (int t = -n; t <= n; t++) {
+                    int tn = nn1 + t, lmax = imin(nodr, w + n);
+                    vcfunc(v, w, -t, n, vc);
+                    for (int l = imax(imax(1, iabs_(v - t)), iabs_(n - w)); l <= lmax; l++) {
+                        int tvl = l * (l + 1) + t - v;
+                        for (int k = 1; k <= 2; k++)
+                            for (int p = 1; p <= 2; p++) {
+                                AM(am, k, l, p) += vc[l] * (cplx)TC(p, tn, k, tvl);
+                                if (l == n && v == 0) {
+                                    cplx tct = 0;
+                                    for (int kt = -n; kt <= n; kt++) tct += (cplx)TC(p, nn1 + kt, k, nn1 + kt);
+                                    AM(amcf, k, l, p) += vc[l] * tct / (double)(n + n + 1);
+                                }
+                            }
+                    }
+                }
+                for (int m = -n; m <= n; m++) {
+                    int mn = nn1 + m;
+                    for (int k = 1; k <= 2; k++) {
+                        int u = m - (-3 + 2 * k);
+                        if (iabs_(u) > w) continue;
+                        int lmax = imin(nodr, w + n);
+                        vcfunc(-u, w, m, n, vc);
+                        for (int l = imax(1, iabs_(w - n)); l <= lmax; l++) {
+                            double fl = -pm1(l) * vc[l] / (double)(l + l + 1);
+                            for (int p = 1; p <= 2; p++) {
+                                BM(bm, k, mn, p) += AM(am, k, l, p) * fl;
+                                if (v == 0) BM(bmcf, k, mn, p) += AM(amcf, k, l, p) * fl;
+                            }
+                        }
+                    }
+                }
+            }
+            int umax = imin(w, nodr + 1);
+            for (int u = -umax; u <= umax; u++)
+                for (int ku = 1; ku <= 3; ku++) {
+                    int k = (ku == 1) ? -1 : 1, k1 = (ku == 2) ? 1 : -1;
+                    int m = u + k, m1 = u + k1, ns = imax(1, iabs_(m));
+                    int ik = (k + 1) / 2 + 1, ik1 = (k1 + 1) / 2 + 1;
+                    for (int n = ns; n <= nodr; n++) {
+                        int nu = n * (n + 1) + m;
+                        int n1s = imax(imax(1, iabs_(m1)), n - nodrw), n1e = imin(nodr, n + nodrw);
+                        for (int n1 = n1s; n1 <= n1e; n1++) {
+                            cplx cin = ipow(n - n1);
+                            int nu1 = n1 * (n1 + 1) + m1;
+                            double fl = -FNR(n + n + 1) * FNR(n1 + n1 + 1) * (double)(w + w + 1);
+                            for (int p = 1; p <= 2; p++)
+                                for (int p1 = 1; p1 <= 2; p1++) {
+                                    DM(dm, u, ku, n, p, n1, p1) += BM(bm, ik, nu, p) * cin * fl * conj(BM(bm, ik1, nu1, p1));
+                                    if (v == 0) DM(dmcf, u, ku, n, p, n1, p1) += BM(bmcf, ik, nu, p) * cin * fl * conj(BM(bmcf, ik1, nu1, p1));
+                                }
+                        }
+                    }
+                }
+        }
+    /* expansion coefficients */
+    cplx *aw = (cplx *)calloc(3 * 3 * (nodrw + 1), sizeof(cplx)), *bw = (cplx *)calloc(3 * 3 * (nodrw + 1), sizeof(cplx));
+    cplx *awcf = (cplx *)calloc(3 * 3 * (nodrw + 1), sizeof(cplx)), *bwcf = (cplx *)calloc(3 * 3 * (nodrw + 1), sizeof(cplx));
+    cplx *cw = (cplx *)calloc(nodrw + 1, sizeof(cplx)), *dw = (cplx *)calloc(nodrw + 1, sizeof(cplx));
+    cplx *cwcf = (cplx *)calloc(nodrw + 1, sizeof(cplx)), *dwcf = (cplx *)calloc(nodrw + 1, sizeof(cplx));
+#define AW(arr, i, k, w) arr[(i) + 3 * (((k) + 1) + 3 * (w))]
+    cplx *fm = (cplx *)malloc(sizeof(cplx) * 3 * nodr * 2 * nodr * 2), *fmcf = (cplx *)malloc(sizeof(cplx) * 3 * nodr * 2 * nodr * 2);
+#define FM(arr, k, n, p, n1, p1) arr[((k) - 1) + 3 * (((n) - 1) + nodr * (((p) - 1) + 2 * (((n1) - 1) + nodr * ((p1) - 1))))]
+    for (int w = 0; w <= nodrw; w++) {
+        for (size_t e = 0; e < (size_t)3 * nodr * 2 * nodr * 2; e++) { fm[e] = 0; fmcf[e] = 0; }
+        for (int u = -nodr - 1; u <= nodr + 1; u++) {
+            for (int k = -1; k <= 1; k += 2) {
+                int m = u + k, ik = (k + 1) / 2 + 1, ns = imax(1, iabs_(m));
+                for (int n = ns; n <= nodr; n++) {
+                    vcfunc(m, n, 0, w, vc);
+                    for (int n1 = ns; n1 <= nodr; n1++) {
+                        if (n + n1 < w || iabs_(n - n1) > w) continue;
+                        double fl = -pm1(n) * vc[n1] * FNR(w + w + 1) / FNR(n1 + n1 + 1);
+                        for (int p = 1; p <= 2; p++)
+                            for (int p1 = 1; p1 <= 2; p1++) {
+                                FM(fm, ik, n, p, n1, p1) += DM(dm, u, ik, n, p, n1, p1) * fl;
+                                FM(fmcf, ik, n, p, n1, p1) += DM(dmcf, u, ik, n, p, n1, p1) * fl;
+                            }
+                    }
+                }
+            }
+            if (w < 2) continue;
+            int m = u + 1, m1 = u - 1, ns = imax(1, iabs_(m)), n1s = imax(1, iabs_(m1));
+            for (int n = ns; n <= nodr; n++) {
+                vcfunc(m, n, -2, w, vc);
+                for (int n1 = n1s; n1 <= nodr; n1++) {
+                    if (n + n1 < w || iabs_(n - n1) > w) continue;
+                    double fl = -pm1(n) * vc[n1] * FNR(w + w + 1) / FNR(n1 + n1 + 1);
+                    for (int p = 1; p <= 2; p++)
+                        for (int p1 = 1; p1 <= 2; p1++) {
+                            FM(fm, 3, n, p, n1, p1) += DM(dm, u, 3, n, p, n1, p1) * fl;
+                            FM(fmcf, 3, n, p, n1, p1) += DM(dmcf, u, 3, n, p, n1, p1) * fl;
+                        }
+                }
+            }
+        }
+        for (int n = 1; n <= nodr; n++) {
+            int n1s = imax(1, iabs_(n - w)), n1e = imin(nodr, n + w);
+            double in = pm1(n);
+            vcfunc(1, n, 0, w, vc);
+            for (int n1 = n1s; n1 <= n1e; n1++) {
+                double fl = 2.0 * in * vc[n1] * FNR(w + w + 1) / FNR(n1 + n1 + 1);
+                int i = (n + n1 - w) % 2 + 1;
+                for (int p = 1; p <= 2; p++) {
+                    int p1 = (2 - i) * p + (i - 1) * (3 - p);
+                    for (int k = -1; k <= 1; k += 2) {
+                        int ik = (k + 1) / 2 + 1;
+                        AW(aw, 0, k, w) += FM(fm, ik, n, p, n1, p1) * fl;
+                        AW(bw, 0, k, w) += FM(fm, ik, n, p, n1, 3 - p1) * fl;
+                        AW(awcf, 0, k, w) += FM(fmcf, ik, n, p, n1, p1) * fl;
+                        AW(bwcf, 0, k, w) += FM(fmcf, ik, n, p, n1, 3 - p1) * fl;
+                    }
+                    AW(bw, 2, 0, w) += FM(fm, 3, n, p, n1, 3 - p1) * fl;
+                    AW(aw, 2, 0, w) += FM(fm, 3, n, p, n1, p1) * fl;
+                    AW(bwcf, 2, 0, w) += FM(fmcf, 3, n, p, n1, 3 - p1) * fl;
+                    AW(awcf, 2, 0, w) += FM(fmcf, 3, n, p, n1, p1) * fl;
+                }
+            }
+            if (w < 2) continue;
+            vcfunc(1, n, -2, w, vc);
+            for (int n1 = n1s; n1 <= n1e; n1++) {
+                double fl = 2.0 * in * vc[n1] * FNR(w + w + 1) / FNR(n1 + n1 + 1);
+                int i = (n + n1 - w) % 2 + 1;
+                for (int p = 1; p <= 2; p++) {
+                    int p1 = (2 - i) * p + (i - 1) * (3 - p);
+                    for (int k = -1; k <= 1; k += 2) {
+                        int ik = (k + 1) / 2 + 1;
+                        AW(aw, 2, k, w) += FM(fm, ik, n, p, n1, p1) * fl * pm1(p1);
+                        AW(bw, 2, k, w) += FM(fm, ik, n, p, n1, 3 - p1) * fl * pm1(3 - p1);
+                        AW(awcf, 2, k, w) += FM(fmcf, ik, n, p, n1, p1) * fl * pm1(p1);
+                        AW(bwcf, 2, k, w) += FM(fmcf, ik, n, p, n1, 3 - p1) * fl * pm1(3 - p1);
+                    }
+                }
+                double fl2 = 2.0 * pm1(n1 + w) * vc[n1] * FNR(w + w + 1) / FNR(n1 + n1 + 1);
+                for (int p = 1; p <= 2; p++)
+                    for (int p1 = 1; p1 <= 2; p1++) {
+                        cw[w] += FM(fm, 3, n, p, n1, p1) * fl * pm1(p1);
+                        dw[w] += FM(fm, 3, n, p, n1, p1) * fl2 * pm1(p);
+                        cwcf[w] += FM(fmcf, 3, n, p, n1, p1) * fl * pm1(p1);
+                        dwcf[w] += FM(fmcf, 3, n, p, n1, p1) * fl2 * pm1(p);
+                    }
+            }
+        }
+    }
+#define SMX(arr, i, j, n) arr[((i) - 1) + 4 * ((j) - 1) + 16 * (n)]
+    for (int k = 0; k < 16 * (nodrw + 1); k++) { sm[k] = 0.0; smcf[k] = 0.0; }
+    for (int pass = 0; pass < 2; pass++) {
+        double *o = pass ? smcf : sm;
+        cplx *A = pass ? awcf : aw, *B = pass ? bwcf : bw, *Cc = pass ? cwcf : cw, *D = pass ? dwcf : dw;
+        for (int n = 0; n <= nodrw; n++) {
+            SMX(o, 1, 1, n) = creal(AW(A, 0, -1, n) + AW(A, 0, 1, n));
+            SMX(o, 1, 2, n) = creal(AW(A, 2, -1, n) + AW(A, 2, 1, n));
+            SMX(o, 1, 3, n) = 2.0 * cimag(AW(A, 2, 0, n));
+            SMX(o, 1, 4, n) = creal(AW(A, 0, 1, n) - AW(A, 0, -1, n));
+            SMX(o, 2, 2, n) = creal(D[n]);
+            SMX(o, 2, 3, n) = cimag(D[n]);
+            SMX(o, 2, 4, n) = creal(AW(A, 2, 1, n) - AW(A, 2, -1, n));
+            SMX(o, 3, 1, n) = -cimag(AW(B, 2, -1, n) + AW(B, 2, 1, n));
+            SMX(o, 3, 2, n) = cimag(Cc[n]);
+            SMX(o, 3, 3, n) = creal(Cc[n]);
+            SMX(o, 3, 4, n) = cimag(AW(B, 2, -1, n) - AW(B, 2, 1, n));
+            SMX(o, 4, 1, n) = creal(AW(B, 0, -1, n) + AW(B, 0, 1, n));
+            SMX(o, 4, 2, n) = 2.0 * creal(AW(B, 2, 0, n));
+            SMX(o, 4, 4, n) = creal(AW(B, 0, 1, n) - AW(B, 0, -1, n));
+        }
+        for (int k = 0; k < 16 * (nodrw + 1); k++) o[k] = o[k] / rimed_re / 2.0;
+    }
+#undef TC
+#undef DM
+#undef BM
+#undef AM
+#undef AW
+#undef FM
+    free(tc); free(dm); free(dmcf); free(bm); free(bmcf); free(am); free(amcf); free(vc);
+    free(aw); free(bw); free(awcf); free(bwcf); free(cw); free(dw); free(cwcf); free(dwcf); free(fm); free(fmcf);
+}
+
+/* ranorienscatmatrixcalc (scatprops:2538-2592): the 16 elements at cos(theta)
+ * = ct from the expansion smc(4,4,0:nodrexp); the reference's assignment
+ * sm(3,1) = sm(1,3) + ... is kept as written. */
+void orc_ranorienscatmatrixcalc(double ct, const double *smc, int nodrexp, double *smo)
+{
+    tables_init();
+    double *dc = (double *)malloc(sizeof(double) * 5 * (nodrexp * (nodrexp + 2) + 1));
+    rotcoef(ct, 2, nodrexp, dc);
+#define DCX(k, nm) dc[((k) + 2) + 5 * (nm)]
+#define SC(i, j, n) smc[((i) - 1) + 4 * ((j) - 1) + 16 * (n)]
+#define SO(i, j) smo[((i) - 1) + 4 * ((j) - 1)]
+    for (int k = 0; k < 16; k++) smo[k] = 0.0;
+    for (int n = 0; n <= nodrexp; n++) {
+        int nn0 = n * (n + 1), nnp2 = nn0 + 2, nnm2 = nn0 - 2;
+        SO(1, 1) = SO(1, 1) + DCX(0, nn0) * SC(1, 1, n);
+        SO(1, 4) = SO(1, 4) + DCX(0, nn0) * SC(1, 4, n);
+        SO(4, 1) = SO(4, 1) + DCX(0, nn0) * SC(4, 1, n);
+        SO(4, 4) = SO(4, 4) + DCX(0, nn0) * SC(4, 4, n);
+        if (n >= 2) {
+            SO(1, 2) = SO(1, 2) + DCX(2, nn0) * SC(1, 2, n);
+            SO(2, 4) = SO(2, 4) + DCX(2, nn0) * SC(2, 4, n);
+            SO(3, 4) = SO(3, 4) + DCX(2, nn0) * SC(3, 4, n);
+            SO(1, 3) = SO(1, 3) + DCX(2, nn0) * SC(1, 3, n);
+            SO(3, 1) = SO(1, 3) + DCX(2, nn0) * SC(3, 1, n);
+            SO(4, 2) = SO(4, 2) + DCX(2, nn0) * SC(4, 2, n);
+            SO(2, 2) = SO(2, 2) + DCX(2, nnm2) * SC(2, 2, n) + DCX(2, nnp2) * SC(3, 3, n);
+            SO(2, 3) = SO(2, 3) + DCX(2, nnp2) * SC(2, 3, n) + DCX(2, nnp2) * SC(3, 2, n);
+            SO(3, 3) = SO(3, 3) - DCX(2, nnm2) * SC(2, 2, n) + DCX(2, nnp2) * SC(3, 3, n);
+            SO(3, 2) = SO(3, 2) + DCX(2, nnp2) * SC(2, 3, n) - DCX(2, nnp2) * SC(3, 2, n);
+        }
+    }
+    SO(2, 1) = SO(1, 2);
+    SO(4, 3) = -SO(3, 4);
+#undef DCX
+#undef SC
+#undef SO
+    free(dc);
+}
+
 /* fosmexpansion (scatprops:1820-1951): GSF expansion coefficients of the
  * azimuth-averaged scattering matrix.  amnp0: (nb(ntot), 2 polarisations).
  * s00..sm22: 16*(2ntot+1) each, Fortran (4,4,0:2ntot) order. */

@@ -78,6 +78,8 @@ def lib():
         L.orc_tmatrix_solution.restype = c_int
         L.orc_tmatrix_symmetrize.argtypes = [c_int, c_void_p, c_void_p]
         L.orc_tmatrix_qext_qsca.argtypes = [c_int, c_void_p, c_double, P(c_double), P(c_double)]
+        L.orc_ranorientscatmatrix.argtypes = [c_int, c_void_p, c_double, c_void_p, c_void_p]
+        L.orc_ranorienscatmatrixcalc.argtypes = [c_double, c_void_p, c_int, c_void_p]
         _lib = L
     return _lib
 
@@ -340,3 +342,25 @@ def tmatrix_qext_qsca(tmo, tmat, xv):
     qe, qs = c_double(0.0), c_double(0.0)
     lib().orc_tmatrix_qext_qsca(tmo, _p(tmat), xv, ctypes.byref(qe), ctypes.byref(qs))
     return qe.value, qs.value
+
+
+def ranorientscatmatrix(tmo, tmat, rimed_re=1.0, nangles=181):
+    """Orientation-averaged scattering matrix from the T matrix: dict(sm, smcf
+    (2tmo+1, 4, 4) expansion coefficients [w][i][j], smat (nangles, 4, 4) at
+    theta_i = i*pi/(nangles-1) with the reference's pi, coherent = smcf[0,0,0])."""
+    L_ = lib()
+    W = 2 * tmo + 1
+    sm = np.zeros(16 * W)
+    smcf = np.zeros(16 * W)
+    tmat = np.asfortranarray(tmat, np.complex128)
+    L_.orc_ranorientscatmatrix(tmo, _p(tmat), rimed_re, _p(sm), _p(smcf))
+    pi_ref = float(np.float32(np.pi))
+    smat = np.zeros((nangles, 4, 4))
+    for i in range(nangles):
+        ct = np.cos(float(i) * pi_ref / float(nangles - 1))
+        o = np.zeros(16)
+        L_.orc_ranorienscatmatrixcalc(ct, _p(sm), 2 * tmo, _p(o))
+        smat[i] = o.reshape(4, 4, order="F")
+    sm3 = sm.reshape(W, 4, 4).transpose(0, 2, 1)
+    cf3 = smcf.reshape(W, 4, 4).transpose(0, 2, 1)
+    return dict(sm=sm3, smcf=cf3, smat=smat, coherent=cf3[0, 0, 0], sm_raw=sm, smcf_raw=smcf)

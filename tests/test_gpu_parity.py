@@ -237,3 +237,21 @@ def test_tmatrix_mixed(api, oracle_mod):
     assert rg["istat"] == 0 and rg["order"] == ro["order"] and rg["outer"] >= 1
     assert np.allclose(rg["qtot"], ro["qtot"], rtol=RTOL_MIXED)
     assert np.abs(rg["tmat"] - ro["tmat"]).max() <= 1e-6 * np.abs(ro["tmat"]).max()
+
+
+def test_ranorient_scattering(api, oracle_mod):
+    """Orientation-averaged scattering matrix from the T matrix on the device
+    against the oracle's restatement (same single-precision T, FP64 sums)."""
+    pos, rad, ri, em = _cluster("cluster8")
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em)
+    r = o.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-10)
+    T = r["order"]
+    nb = 2 * T * (T + 2)
+    tm = np.asfortranarray(r["tmat"][:nb, :nb])
+    ro = oracle_mod.ranorientscatmatrix(T, tm)
+    rg = g.ranorientscatmatrix(tm, T)
+    scale = np.abs(ro["sm"]).max()
+    assert np.abs(rg["sm"] - ro["sm"]).max() <= 1e-9 * scale
+    assert np.abs(rg["smcf"] - ro["smcf"]).max() <= 1e-9 * scale
+    s11 = np.abs(ro["smat"][:, 0, 0]).max()
+    assert np.abs(rg["smat"] - ro["smat"]).max() <= 1e-9 * s11

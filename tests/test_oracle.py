@@ -258,3 +258,56 @@ def test_tmatrix_efficiency_sum_rule(oracle_mod):
     qe, qs = oracle_mod.tmatrix_qext_qsca(r["tmo"], r["tmat"], o.vol_radius())
     assert abs(qe / r["qtot"][0] - 1) < 1e-6
     assert abs(qs / r["qtot"][2] - 1) < 1e-6
+
+
+def test_ranorient_single_sphere_is_mie(oracle_mod):
+    """Orientation averaging a lone sphere changes nothing: the random-orientation
+    scattering matrix equals the fixed-orientation (Mie) one, to the single
+    precision of the stored T matrix."""
+    o = oracle_mod.Oracle([[0.0, 0.0, 0.0]], [1.0], [1.5 + 0.01j], mie_eps=-7)
+    r = o.tmatrix_solution(tmo=7, convergence_eps=0.0, solution_eps=1e-12)
+    ro = oracle_mod.ranorientscatmatrix(7, r["tmat"])
+    sc = o.scattering(o.fixedorsoln(eps=1e-12)["amnp"])
+    s11 = sc["smat"][:, 0, 0]
+    for i in range(0, 181, 10):
+        assert abs(ro["smat"][i, 0, 0] / s11[i] - 1) < 1e-6
+        assert abs(ro["smat"][i, 0, 1] - sc["smat"][i, 0, 1]) < 1e-6 * s11[i]
+        assert abs(ro["smat"][i, 2, 2] - sc["smat"][i, 2, 2]) < 1e-6 * s11[i]
+    # a sphere scatters coherently: the coherent part is all of it
+    assert abs(ro["coherent"] / ro["sm"][0, 0, 0] - 1) < 1e-12
+
+
+def test_ranorient_cluster_sum_rule(oracle_mod):
+    """sm(1,1,0) of the expansion is Qsca xv^2 / 4: the D-matrix route and the
+    T-matrix norm route give the same orientation-averaged scattering."""
+    w = C.workload("cluster8")
+    o = oracle_mod.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-w["order"])
+    r = o.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-10)
+    T = r["order"]
+    nb = 2 * T * (T + 2)
+    tm = np.asfortranarray(r["tmat"][:nb, :nb])
+    ro = oracle_mod.ranorientscatmatrix(T, tm)
+    xv = o.vol_radius()
+    qe, qs = oracle_mod.tmatrix_qext_qsca(T, tm, xv)
+    assert abs(ro["sm"][0, 0, 0] * 4 / xv ** 2 / qs - 1) < 1e-6
+    assert 0.0 < ro["coherent"] < ro["sm"][0, 0, 0]
+
+
+def test_tmatrix_file_roundtrip(oracle_mod, tmp_path):
+    """The T-matrix text file (tmatrix_solution's writer, ranorientscatmatrix's
+    reader): header, column order, E18.10 entries."""
+    from mstm_b200.tmatrix_file import read_tmatrix_file, write_tmatrix_file
+    w = C.workload("cluster8")
+    o = oracle_mod.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-w["order"])
+    r = o.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-10)
+    fn = tmp_path / "tmatrix.dat"
+    write_tmatrix_file(fn, r["tmat"], r["tmo"], r["order"])
+    first = open(fn).readline()
+    assert first == f"{r['order']:4d}{r['order']:4d}\n"
+    T, tm = read_tmatrix_file(fn)
+    nb = 2 * T * (T + 2)
+    assert T == r["order"]
+    assert np.abs(tm - r["tmat"][:nb, :nb]).max() < 1e-9 * np.abs(tm).max()
+    # entries a file holds: rows of order n <= l only
+    lines = sum(1 for _ in open(fn)) - 1
+    assert lines == sum(2 * (2 * l + 1) * 2 * l * (l + 2) for l in range(1, T + 1))
