@@ -168,6 +168,24 @@ int mstmg_tmatrix_qext_qsca(mstmg_ctx *ctx, int t_matrix_order, const double *tm
 int mstmg_ranorient_scattering(mstmg_ctx *ctx, int t_matrix_order, const double *tmat, int nangles, double *sm, double *smcf,
                                double *smat);
 
+/* Switch the context to MSTM's FFT translation (fft_translation_option=t;
+ * node_selection, fft_translation-5.f90:654-825, with the target box spanned
+ * by the sphere centres, as main_calling_program sets it up,
+ * mstm-input-37.f90:1238-1261): spheres are binned in cubic cells; pairs in
+ * cells within the neighbour stencil (neighbor_node_model 0/1/2: 1/7/19 cells)
+ * are translated directly, all other interactions go through regular
+ * expansions of order node_order about the cell centres and the node-to-node
+ * outgoing translation, applied as an FFT convolution on the zero-padded
+ * (2 cell_dim)^3 grid with kernels stored in single precision, as the
+ * reference stores them (fft:72-336, 827-974).  d_cell > 0 fixes the cell
+ * edge, otherwise cell_volume_fraction (<= 0: from the spheres' volume) sets
+ * it; node_order <= 0 means -node_order + ceiling(d_cell).  Every later
+ * interaction, BiCG, fixed-orientation and T-matrix call uses it (positions
+ * set later rebuild it).
+ *   cell_dim[3], d_cell_out, node_order_out, near_pairs: the chosen grid. */
+int mstmg_fft_setup(mstmg_ctx *ctx, double cell_volume_fraction, double d_cell, int node_order, int neighbor_node_model, int *cell_dim,
+                    double *d_cell_out, int *node_order_out, int *near_pairs);
+
 /* Statistics of the last solve: iterations per polarisation, refinement steps,
  * FP64 and FP32 operator passes. */
 int mstmg_last_stats(const mstmg_ctx *ctx, int *iters2, int *outer, int *passes64, int *passes32);

@@ -36,6 +36,7 @@ SIGNATURES = {
                               P(c_double)]),
     "mstmg_tmatrix_qext_qsca": (c_int, [c_void_p, c_int, c_void_p, P(c_double), P(c_double)]),
     "mstmg_ranorient_scattering": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "mstmg_fft_setup": (c_int, [c_void_p, c_double, c_double, c_int, c_int, c_void_p, P(c_double), P(c_int), P(c_int)]),
     "mstmg_last_stats": (c_int, [c_void_p, c_void_p, P(c_int), P(c_int), P(c_int)]),
     "mstmg_operator_bytes": (c_int, [c_void_p, c_int, P(c_double), P(c_double)]),
     "mstmg_time_translation": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),

@@ -150,6 +150,16 @@ class SphereCluster:
                                        ctypes.byref(tmo), None, 0), "scattering")
         return dict(smat=smat.reshape(nangles, 4, 4).transpose(0, 2, 1).copy(), g=g.value, t_matrix_order=tmo.value)
 
+    def fft_setup(self, cell_volume_fraction=0.2, d_cell=0.0, node_order=-1, neighbor_node_model=2):
+        """Use MSTM's FFT translation (fft_translation_option): near pairs direct,
+        the rest through cell nodes and an FFT convolution.  Returns the grid
+        chosen: dict(cell_dim, d_cell, node_order, near_pairs)."""
+        cd = np.zeros(3, np.int32)
+        dc, no, npair = c_double(0.0), c_int(0), c_int(0)
+        check(self._L.mstmg_fft_setup(self.ctx, cell_volume_fraction, d_cell, node_order, neighbor_node_model, _ptr(cd),
+                                      ctypes.byref(dc), ctypes.byref(no), ctypes.byref(npair)), "fft_setup")
+        return dict(cell_dim=cd.tolist(), d_cell=dc.value, node_order=no.value, near_pairs=npair.value)
+
     def t_matrix_order(self, trans_eps=1.0e-5, max_t_order=100):
         """Order of the cluster T matrix about the cluster origin (tranordertest for
         every sphere, mstm-modules-33.f90:1896-1942); also fixes the per-sphere

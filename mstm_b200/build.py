@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmstm_b200.so")
-SOURCES = ["opgen.cu", "translate.cu", "translate_tiled.cu", "sphere_kernels.cu", "bicg.cu", "mrhs.cu", "ranorient.cu", "postproc.cu", "capi.cu", "noalloc.cu", "tables.cpp"]
+SOURCES = ["opgen.cu", "translate.cu", "translate_tiled.cu", "sphere_kernels.cu", "bicg.cu", "mrhs.cu", "ranorient.cu", "fftpath.cu", "postproc.cu", "capi.cu", "noalloc.cu", "tables.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -38,6 +38,7 @@ def build(force=False, verbose=False, extra=()):
            "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(os.path.dirname(HERE), "include"), *extra,
            "-o", LIB + ".tmp"]
     cmd += [os.path.join(CSRC, s) for s in SOURCES]
+    cmd += ["-lcufft"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

@@ -16,6 +16,9 @@
 #include "postproc.cuh"
 #include "mrhs.cuh"
 #include "ranorient.cuh"
+#include "fftpath.cuh"
+#include <cufft.h>
+#include <memory>
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
@@ -60,6 +63,34 @@ template <typename T> struct BicgVecs {
     cpx<T>*x, *r, *p, *w, *q, *cap, *caw;
 };
 
+// FFT translation state (fft_translation-5.f90): cells, node translations,
+// kernel spectra, cuFFT plans and the node work arrays.
+struct FftState {
+    bool on = false;
+    double fv_in = 0.2, d_in = 0.0;
+    int no_in = -1, model_in = 2;
+    int No = 0, nbN = 0, cd[3] = {0, 0, 0}, nnb = 0, nbv[81] = {0};
+    double dcell = 0.0, cb[3] = {0.0, 0.0, 0.0};
+    size_t N8 = 0;
+    DevBuf<int> snode, slot;
+    DevBuf<long long> joff;
+    DevBuf<zd> Jsn64, Jns64, A64, G64;
+    DevBuf<zf> Jsn32, Jns32, A32, G32;
+    DevBuf<float2> H;
+    cufftHandle plan[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};   // [FP64, FP32][columns]
+    bool have[2][5] = {{false, false, false, false, false}, {false, false, false, false, false}};
+    void drop_plans()
+    {
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 5; b++)
+                if (have[a][b]) {
+                    cufftDestroy(plan[a][b]);
+                    have[a][b] = false;
+                }
+    }
+    ~FftState() { drop_plans(); }
+};
+
 struct mstmg_ctx {
     int dev = 0, nsm = 148;
     cudaStream_t st = nullptr;
@@ -93,6 +124,7 @@ struct mstmg_ctx {
     double* h_small = nullptr;
     int iters[2] = {0, 0}, outer = 0, passes64 = 0, passes32 = 0;
     std::vector<int> tord;   // translation order of each sphere to the cluster origin (mstmg_t_matrix_order)
+    std::unique_ptr<FftState> fft;   // set by mstmg_fft_setup
     cudaStream_t own_st = nullptr;
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -102,6 +134,9 @@ struct mstmg_ctx {
     int kt_n[2] = {0, 0};
     SlotMaps sm() const { return SlotMaps{neqns / 2, slot.p, d_order.p, d_offset.p, d_mie_offset.p}; }
 };
+
+template <typename T> static int fft_far(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int ncols, unsigned contran);
+static int fft_build(mstmg_ctx* c);
 
 static bool is_dev(const void* p)
 {
@@ -168,6 +203,38 @@ static int check_kernel_err(mstmg_ctx* c)
         cudaStreamSynchronize(c->st);
         return herr;
     }
+    return MSTMG_OK;
+}
+
+// Install a pair list (i < j) and, for the tiled kernel, its tiles: operator
+// record offsets, the device copies, and invalidated operators.
+static int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const std::vector<int4>& tl)
+{
+    std::vector<long long> off(np > 0 ? np : 1);
+    long long u = 0;
+    int maxrec = 4;
+    for (int t = 0; t < np; t++) {
+        off[t] = u;
+        int rec = op_record_units(c->order[pr[t].x], c->order[pr[t].y]);
+        maxrec = std::max(maxrec, rec);
+        u += rec;
+    }
+    c->npairs = np;
+    c->ntiles = (int)tl.size();
+    if (c->ntiles > 0) {
+        CK(c->tiles.alloc(tl.size()));
+        CK(cudaMemcpyAsync(c->tiles.p, tl.data(), sizeof(int4) * tl.size(), cudaMemcpyHostToDevice, c->st));
+    }
+    c->op_units = u;
+    c->maxrec = maxrec;
+    if (np > 0) {
+        CK(c->pairs.alloc(np));
+        CK(c->opoff.alloc(np));
+        CK(cudaMemcpyAsync(c->pairs.p, pr.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->opoff.p, off.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));   // host vectors are freed on return
+    }
+    c->ops64_ready = c->ops32_ready = false;
     return MSTMG_OK;
 }
 
@@ -287,23 +354,14 @@ static int setup_layout(mstmg_ctx* c)
         tournament(n, pp);
         for (auto& ij : pp) add_pair(ij.first, ij.second);
     }
-    c->ntiles = (int)tl.size();
-    if (c->ntiles > 0) {
-        CK(c->tiles.alloc(tl.size()));
-        CK(cudaMemcpyAsync(c->tiles.p, tl.data(), sizeof(int4) * tl.size(), cudaMemcpyHostToDevice, c->st));
-    }
     if (t != np) {
         set_err("internal error: pair schedule incomplete");
         return MSTMG_ERR_ARG;
     }
-    c->op_units = u;
-    c->maxrec = maxrec;
-    if (np > 0) {
-        CK(c->pairs.alloc(np));
-        CK(c->opoff.alloc(np));
-        CK(cudaMemcpyAsync(c->pairs.p, pr.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(c->opoff.p, off.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, c->st));
-    }
+    (void)off;
+    (void)maxrec;
+    int rc_ = upload_pairs(c, pr, (int)np, tl);
+    if (rc_) return rc_;
     // constant tables
     mstmg::Tables tb(6 * lm + 6);
     std::vector<double> vcc, f1, f2, f3;
@@ -458,6 +516,11 @@ extern "C" int mstmg_ctx_set_positions(mstmg_ctx* c, const double* pos)
     if (is_dev(pos)) CK(cudaMemcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n, cudaMemcpyDeviceToHost));
     else memcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n);
     c->ops64_ready = c->ops32_ready = false;
+    if (c->fft && c->fft->on) {
+        c->fft->drop_plans();
+        c->fft->on = false;
+        return fft_build(c);
+    }
     return MSTMG_OK;
 }
 
@@ -526,12 +589,13 @@ template <typename T> static const T* ops_ptr(mstmg_ctx* c);
 template <> const double* ops_ptr<double>(mstmg_ctx* c) { return c->op64.p; }
 template <> const float* ops_ptr<float>(mstmg_ctx* c) { return c->op32.p; }
 
+
 // y[:, 0:nrhs*nchunk] = H x[:, 0:nrhs*nchunk]  (y zeroed here).  nchunk > 1
 // only on the tiled path: contran then applies to column r of every chunk.
 template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran, int nchunk = 1)
 {
     CK(cudaMemsetAsync(y, 0, sizeof(cpx<T>) * (size_t)c->neqns * nrhs * nchunk, c->st));
-    if (c->npairs == 0) return MSTMG_OK;
+    if (c->npairs == 0) return (c->fft && c->fft->on) ? fft_far<T>(c, x, y, nrhs * nchunk, contran) : MSTMG_OK;
     TransArgs<T> a;
     a.npairs = c->npairs;
     a.pairs = c->pairs.p;
@@ -587,6 +651,7 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
     }
     if (sizeof(T) == 8) c->passes64++;
     else c->passes32++;
+    if (c->fft && c->fft->on) return fft_far<T>(c, x, y, nrhs * nchunk, contran);
     return MSTMG_OK;
 }
 
@@ -1596,6 +1661,294 @@ extern "C" int mstmg_ranorient_scattering(mstmg_ctx* c, int t_matrix_order, cons
     if (smat && nangles > 0) CK(copy_out(smat, dsmat.p, sizeof(double) * 16 * (size_t)nangles, c->st));
     CK(cudaStreamSynchronize(c->st));
     return check_kernel_err(c);
+}
+
+// ---------------------------------------------------------------------------
+// FFT translation (fft_translation-5.f90)
+// ---------------------------------------------------------------------------
+
+static int check235(int n) /* fft:1052-1066 */
+{
+    int nn = n, ifac = 2;
+    for (int ll = 1; ll <= 3; ll++) {
+        while (nn % ifac == 0) nn /= ifac;
+        ifac += ll;
+    }
+    return nn == 1;
+}
+static int correct235(int n) /* fft:1068-1076 (n >= 1: a flat extent gives one cell) */
+{
+    int n1 = n < 1 ? 1 : n;
+    while (!check235(n1)) n1++;
+    return n1;
+}
+
+// Far part: y += S Jns conv(Jsn S x) for up to 4 columns per pass.
+template <typename T> static int fft_far(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int ncols, unsigned contran)
+{
+    FftState& F = *c->fft;
+    const int pi = sizeof(T) == 8 ? 0 : 1;
+    const size_t per = (size_t)2 * F.nbN * F.N8;
+    DevBuf<cpx<T>>& A = *reinterpret_cast<DevBuf<cpx<T>>*>(sizeof(T) == 8 ? (void*)&F.A64 : (void*)&F.A32);
+    DevBuf<cpx<T>>& G = *reinterpret_cast<DevBuf<cpx<T>>*>(sizeof(T) == 8 ? (void*)&F.G64 : (void*)&F.G32);
+    const cpx<T>* Jsn = sizeof(T) == 8 ? (const cpx<T>*)F.Jsn64.p : (const cpx<T>*)F.Jsn32.p;
+    const cpx<T>* Jns = sizeof(T) == 8 ? (const cpx<T>*)F.Jns64.p : (const cpx<T>*)F.Jns32.p;
+    if (!Jsn || !Jns) {
+        set_err("FFT translation: node translations missing for this precision");
+        return MSTMG_ERR_CUDA;
+    }
+    CK(A.alloc(4 * per));
+    CK(G.alloc(4 * per));
+    FftMArgs m;
+    m.nsph = c->n;
+    m.No = F.No;
+    m.nbmax = c->lmax * (c->lmax + 2);
+    m.N8 = F.N8;
+    m.order = c->d_order.p;
+    m.offset = c->d_offset.p;
+    m.joff = F.joff.p;
+    m.slot = F.slot.p;
+    const size_t ld = (size_t)c->neqns;
+    for (int k0 = 0; k0 < ncols; k0 += 4) {
+        const int w = std::min(4, ncols - k0);
+        const unsigned mask = (contran >> k0) & 0xFu;
+        if (!F.have[pi][w]) {
+            int nn[3] = {2 * F.cd[2], 2 * F.cd[1], 2 * F.cd[0]};
+            if (cufftPlanMany(&F.plan[pi][w], 3, nn, nullptr, 1, (int)F.N8, nullptr, 1, (int)F.N8, sizeof(T) == 8 ? CUFFT_Z2Z : CUFFT_C2C,
+                              w * 2 * F.nbN) != CUFFT_SUCCESS) {
+                set_err("FFT translation: cufftPlanMany failed");
+                return MSTMG_ERR_CUDA;
+            }
+            F.have[pi][w] = true;
+        }
+        cufftSetStream(F.plan[pi][w], c->st);
+        CK(cudaMemsetAsync(A.p, 0, sizeof(cpx<T>) * w * per, c->st));
+        launch_fft_s2n<T>(m, Jsn, x + (size_t)k0 * ld, (int)ld, w, mask, A.p, c->st);
+        cufftResult fr;
+        if (sizeof(T) == 8) fr = cufftExecZ2Z(F.plan[pi][w], (cufftDoubleComplex*)A.p, (cufftDoubleComplex*)A.p, CUFFT_FORWARD);
+        else fr = cufftExecC2C(F.plan[pi][w], (cufftComplex*)A.p, (cufftComplex*)A.p, CUFFT_FORWARD);
+        if (fr != CUFFT_SUCCESS) {
+            set_err("FFT translation: forward transform failed");
+            return MSTMG_ERR_CUDA;
+        }
+        launch_fft_mul<T>(F.nbN, F.N8, w, F.H.p, A.p, G.p, c->nsm, c->st);
+        if (sizeof(T) == 8) fr = cufftExecZ2Z(F.plan[pi][w], (cufftDoubleComplex*)G.p, (cufftDoubleComplex*)G.p, CUFFT_INVERSE);
+        else fr = cufftExecC2C(F.plan[pi][w], (cufftComplex*)G.p, (cufftComplex*)G.p, CUFFT_INVERSE);
+        if (fr != CUFFT_SUCCESS) {
+            set_err("FFT translation: inverse transform failed");
+            return MSTMG_ERR_CUDA;
+        }
+        launch_fft_n2s<T>(m, Jns, G.p, w, mask, y + (size_t)k0 * ld, (int)ld, c->st);
+        CK(cudaGetLastError());
+    }
+    return MSTMG_OK;
+}
+
+// node_selection (fft:654-825) with target box = the sphere-centre extents,
+// the near-pair list, the node translations and the kernel spectra.
+static int fft_build(mstmg_ctx* c)
+{
+    FftState& F = *c->fft;
+    const int n = c->n;
+    double tmin[3] = {1e10, 1e10, 1e10}, tmax[3] = {-1e10, -1e10, -1e10};
+    for (int i = 0; i < n; i++)
+        for (int m = 0; m < 3; m++) {
+            tmin[m] = std::min(tmin[m], c->hpos[3 * (size_t)i + m]);
+            tmax[m] = std::max(tmax[m], c->hpos[3 * (size_t)i + m]);
+        }
+    double amean = 0.0, svol = 0.0;
+    for (int i = 0; i < n; i++) {
+        amean += c->radius[i];
+        svol += c->radius[i] * c->radius[i] * c->radius[i];
+    }
+    svol = std::pow(svol, 1.0 / 3.0);
+    amean = amean / (double)n;
+    double tvol = 1.0;
+    for (int m = 0; m < 3; m++) tvol *= std::max(tmax[m] - tmin[m], amean);
+    double dc = F.d_in;
+    if (!(F.d_in > 0.0)) {
+        double fv = F.fv_in;
+        if (fv <= 0.0) {
+            fv = 4.0 * MSTMG_REF_PI / 3.0 * svol * svol * svol / tvol;
+            fv = std::min(fv, 1.0);
+            fv = std::max(fv, 0.02);
+        }
+        dc = std::pow(4.0 * MSTMG_REF_PI / 3.0 / fv / (double)n, 1.0 / 3.0) * svol;
+    }
+    for (int m = 0; m < 3; m++) F.cd[m] = correct235((int)std::ceil((tmax[m] - tmin[m]) / dc));
+    dc = 0.0;
+    for (int m = 0; m < 3; m++) dc = std::max(dc, (tmax[m] - tmin[m]) / (double)F.cd[m]);
+    F.dcell = dc;
+    for (int m = 0; m < 3; m++) F.cb[m] = tmin[m];
+    F.No = F.no_in > 0 ? F.no_in : -F.no_in + (int)std::ceil(dc);
+    F.nbN = F.No * (F.No + 2);
+    if (F.No < 1 || F.nbN > FFT_NBN_MAX || 2 * F.No > GT_WMAX || F.No + c->lmax > GT_WMAX) {
+        set_err("FFT translation: node order out of range (1..20)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    F.N8 = (size_t)8 * F.cd[0] * F.cd[1] * F.cd[2];
+    const double hr_bytes = 16.0 * 2.0 * F.nbN * F.nbN * (double)F.N8;
+    if (hr_bytes > 16.0e9) {
+        set_err("FFT translation: kernel table above 16 GB (grid or node order too large)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    // cells of the spheres, stencil, near pairs (j > i in neighbouring cells, the reference's order)
+    std::vector<int> snode(3 * (size_t)n), slot(n);
+    const int N0 = 2 * F.cd[0], N1 = 2 * F.cd[1];
+    std::vector<std::vector<int>> members((size_t)F.cd[0] * F.cd[1] * F.cd[2]);
+    for (int i = 0; i < n; i++) {
+        int cc[3];
+        for (int m = 0; m < 3; m++) {
+            int nd = (int)std::floor((c->hpos[3 * (size_t)i + m] - tmin[m]) / dc) + 1;
+            nd = std::min(nd, F.cd[m]);
+            cc[m] = std::max(nd, 1);
+            snode[3 * (size_t)i + m] = cc[m];
+        }
+        slot[i] = (cc[0] - 1) + N0 * ((cc[1] - 1) + N1 * (cc[2] - 1));
+        members[(size_t)(cc[0] - 1) + (size_t)F.cd[0] * ((cc[1] - 1) + (size_t)F.cd[1] * (cc[2] - 1))].push_back(i);
+    }
+    F.nnb = 0;
+    for (int iz = -1; iz <= 1; iz++)
+        for (int iy = -1; iy <= 1; iy++)
+            for (int ix = -1; ix <= 1; ix++) {
+                int ir = ix * ix + iy * iy + iz * iz;
+                if ((F.model_in == 0 && ir > 0) || (F.model_in == 1 && ir > 1) || (F.model_in == 2 && ir > 2)) continue;
+                F.nbv[3 * F.nnb] = ix;
+                F.nbv[3 * F.nnb + 1] = iy;
+                F.nbv[3 * F.nnb + 2] = iz;
+                F.nnb++;
+            }
+    std::vector<int2> pr;
+    for (int i = 0; i < n; i++)
+        for (int q = 0; q < F.nnb; q++) {
+            int sx = snode[3 * (size_t)i] - F.nbv[3 * q], sy = snode[3 * (size_t)i + 1] - F.nbv[3 * q + 1], sz = snode[3 * (size_t)i + 2] - F.nbv[3 * q + 2];
+            if (sx < 1 || sy < 1 || sz < 1 || sx > F.cd[0] || sy > F.cd[1] || sz > F.cd[2]) continue;
+            for (int j : members[(size_t)(sx - 1) + (size_t)F.cd[0] * ((sy - 1) + (size_t)F.cd[1] * (sz - 1))])
+                if (j > i) pr.push_back(make_int2(i, j));
+        }
+    c->tiled = false;
+    int rc = upload_pairs(c, pr, (int)pr.size(), std::vector<int4>());
+    if (rc) return rc;
+    // node translations
+    std::vector<long long> joff(n + 1);
+    long long tot = 0;
+    for (int i = 0; i < n; i++) {
+        joff[i] = tot;
+        tot += 2LL * F.nbN * c->order[i] * (c->order[i] + 2);
+    }
+    joff[n] = tot;
+    CK(F.snode.alloc(3 * (size_t)n));
+    CK(F.slot.alloc(n));
+    CK(F.joff.alloc(n + 1));
+    CK(cudaMemcpyAsync(F.snode.p, snode.data(), sizeof(int) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(F.slot.p, slot.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(F.joff.p, joff.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, c->st));
+    const int nmax = std::max(F.No, c->lmax);
+    std::vector<double> tcv, bd(GT_WMAX + 2);
+    gentran_constants(nmax, tcv);
+    mstmg::Tables& big = big_tables();
+    for (int k = 0; k < (int)bd.size(); k++) bd[k] = big.bc(k, k);
+    DevBuf<double> dtc, dbd, dfnr;
+    CK(dtc.alloc(tcv.size()));
+    CK(dbd.alloc(bd.size()));
+    CK(dfnr.alloc(big.fnr.size()));
+    CK(cudaMemcpyAsync(dtc.p, tcv.data(), sizeof(double) * tcv.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dbd.p, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dfnr.p, big.fnr.data(), sizeof(double) * big.fnr.size(), cudaMemcpyHostToDevice, c->st));
+    GtConst g;
+    g.tc = dtc.p;
+    g.nmax = nmax;
+    g.nd = nmax * (nmax + 2);
+    g.fnr = dfnr.p;
+    g.bcd = dbd.p;
+    CK(F.Jsn64.alloc(tot));
+    CK(F.Jns64.alloc(tot));
+    FftJArgs ja;
+    ja.nsph = n;
+    ja.No = F.No;
+    ja.order = c->d_order.p;
+    ja.pos = c->pos.p;
+    ja.snode = F.snode.p;
+    ja.dcell = dc;
+    for (int m = 0; m < 3; m++) ja.cb[m] = F.cb[m];
+    ja.joff = F.joff.p;
+    ja.Jsn = F.Jsn64.p;
+    ja.Jns = F.Jns64.p;
+    ja.rimed_re = c->opts.medium_re;
+    ja.rimed_im = c->opts.medium_im;
+    ja.g = g;
+    launch_fft_j(ja, c->st);
+    CK(cudaGetLastError());
+    CK(F.Jsn32.alloc(tot));
+    CK(F.Jns32.alloc(tot));
+    launch_d2f((int)tot, F.Jsn64.p, F.Jsn32.p, c->st);
+    launch_d2f((int)tot, F.Jns64.p, F.Jns32.p, c->st);
+    // kernel spectra: real-space kernels (single-precision sums), double FFT, stored in single precision
+    {
+        DevBuf<zd> hr;
+        const size_t nel = (size_t)2 * F.nbN * F.nbN;
+        CK(hr.alloc(nel * F.N8));
+        FftHArgs ha;
+        for (int m = 0; m < 3; m++) ha.cd[m] = F.cd[m];
+        ha.No = F.No;
+        ha.nnb = F.nnb;
+        for (int q = 0; q < 81; q++) ha.nbv[q] = F.nbv[q];
+        ha.dcell = dc;
+        ha.rimed_re = c->opts.medium_re;
+        ha.rimed_im = c->opts.medium_im;
+        ha.hr = hr.p;
+        ha.g = g;
+        launch_fft_hbuild(ha, c->nsm, c->st);
+        CK(cudaGetLastError());
+        cufftHandle hp;
+        int nn[3] = {2 * F.cd[2], 2 * F.cd[1], 2 * F.cd[0]};
+        // in batches of at most 1225 transforms (one mode of a node order 5 kernel)
+        const int chunk = std::min<int>((int)nel, F.nbN * F.nbN);
+        if (cufftPlanMany(&hp, 3, nn, nullptr, 1, (int)F.N8, nullptr, 1, (int)F.N8, CUFFT_Z2Z, chunk) != CUFFT_SUCCESS) {
+            set_err("FFT translation: kernel plan failed");
+            return MSTMG_ERR_CUDA;
+        }
+        cufftSetStream(hp, c->st);
+        bool ok = true;
+        for (size_t b = 0; b + (size_t)chunk <= nel && ok; b += chunk)
+            ok = cufftExecZ2Z(hp, (cufftDoubleComplex*)(hr.p + b * F.N8), (cufftDoubleComplex*)(hr.p + b * F.N8), CUFFT_FORWARD) == CUFFT_SUCCESS;
+        cufftDestroy(hp);
+        if (!ok) {
+            set_err("FFT translation: kernel transform failed");
+            return MSTMG_ERR_CUDA;
+        }
+        CK(F.H.alloc(nel * F.N8));
+        launch_fft_round(nel * F.N8, hr.p, F.H.p, c->st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(c->st));
+    }
+    F.on = true;
+    return check_kernel_err(c);
+}
+
+extern "C" int mstmg_fft_setup(mstmg_ctx* c, double cell_volume_fraction, double d_cell, int node_order, int neighbor_node_model,
+                               int* cell_dim, double* d_cell_out, int* node_order_out, int* near_pairs)
+{
+    if (!c || c->n < 2 || neighbor_node_model < 0 || neighbor_node_model > 2) {
+        set_err("mstmg_fft_setup: bad arguments (two or more spheres, neighbor_node_model 0..2)");
+        return MSTMG_ERR_ARG;
+    }
+    if (!c->fft) c->fft.reset(new FftState());
+    FftState& F = *c->fft;
+    F.drop_plans();
+    F.on = false;
+    F.fv_in = cell_volume_fraction;
+    F.d_in = d_cell;
+    F.no_in = node_order;
+    F.model_in = neighbor_node_model;
+    int rc = fft_build(c);
+    if (rc) return rc;
+    if (cell_dim)
+        for (int m = 0; m < 3; m++) cell_dim[m] = F.cd[m];
+    if (d_cell_out) *d_cell_out = F.dcell;
+    if (node_order_out) *node_order_out = F.No;
+    if (near_pairs) *near_pairs = c->npairs;
+    return MSTMG_OK;
 }
 
 extern "C" int mstmg_set_stream(mstmg_ctx* c, void* stream)

@@ -981,6 +981,13 @@ struct orc_ctx {
     int *pi_, *pj_;
     pairop_t *ops;     /* stored operators (store_translation_matrix) */
     int ops_ready;
+    /* FFT translation (fft_translation-5.f90): set by orc_fft_setup */
+    int fft, No, cd[3], nnb, nb_vec[27][3];
+    double dcell, cb[3];
+    int *snode;            /* 3N, 1-based cell of each sphere */
+    cplx *Jsn, *Jns;       /* per sphere: dense J(node - pos) (nbN x nb_i x 2) and J(pos - node) (nb_i x nbN x 2) */
+    size_t *joff;
+    cplx *Hc;              /* dense H at every node offset (2cd-1)^3 x nbN x nbN x 2, zero inside the hole */
 };
 
 orc_ctx *orc_create(int nsphere, const double *pos, const double *radius, const double *ri,
@@ -1045,6 +1052,7 @@ void orc_destroy(orc_ctx *c)
     if (c->ops) { for (int k = 0; k < c->npairs; k++) pairop_free(&c->ops[k]); free(c->ops); }
     free(c->pos); free(c->rad); free(c->ri); free(c->order); free(c->offset); free(c->mie_offset);
     free(c->an); free(c->an_inv); free(c->qext_mie); free(c->qabs_mie); free(c->pi_); free(c->pj_);
+    free(c->snode); free(c->Jsn); free(c->Jns); free(c->joff); free(c->Hc);
     free(c);
 }
 
@@ -1091,6 +1099,228 @@ static void multmiecoeffmult(const orc_ctx *c, int idir, const cplx *ain, cplx *
  * split over threads with a private output each and a final sum, the
  * single-node analogue of the reference's round-robin MPI task split plus
  * allreduce (scatprops:152-156). */
+/* ------------------------------------------------------------------------ */
+/* FFT translation (fft_translation-5.f90): spheres binned in cubic cells;    */
+/* pairs in neighbouring cells are translated directly, all others through    */
+/* regular expansions about the cell nodes and the node-to-node outgoing      */
+/* translation, which the reference evaluates as an FFT convolution on the    */
+/* zero-padded (2 cell_dim)^3 grid (fft:827-899) with kernels built at every  */
+/* node offset outside the neighbour stencil (fft:901-974).  Here the         */
+/* convolution is summed directly over node pairs: for offsets inside the     */
+/* grid it is the same linear map (the padded grid's wrap-around slots are    */
+/* never reached), without the kernels' single-precision rounding.            */
+/* ------------------------------------------------------------------------ */
+
+static int checkn235(int n) /* fft:1052-1066 */
+{
+    int nn = n, ifac = 2;
+    for (int ll = 1; ll <= 3; ll++) {
+        while (nn % ifac == 0) nn /= ifac;
+        ifac += ll;
+    }
+    return nn == 1;
+}
+static int correctn235(int n) /* fft:1068-1076; n >= 1 */
+{
+    int n1 = n < 1 ? 1 : n;
+    while (!checkn235(n1)) n1++;
+    return n1;
+}
+
+/* node_selection (fft:654-825) for free-space external spheres with target
+ * box [tmin, tmax] (the sphere-centre extents), and the near-pair list j > i
+ * in neighbouring cells; then the dense node translations per sphere and
+ * the node-offset kernels.  d_cell > 0 fixes the cell edge (d_cell
+ * specified), else cell_volume_fraction (<= 0: from the spheres' volume)
+ * sets it; node_order <= 0 means -node_order + ceiling(d_cell)
+ * (input:1256-1260).  Returns the node order. */
+int orc_fft_setup(orc_ctx *c, double cell_volume_fraction, double d_cell, int node_order, int neighbor_node_model,
+                  int *cell_dim_out, double *d_cell_out)
+{
+    tables_init();
+    const int n = c->n;
+    double tmin[3] = {1e10, 1e10, 1e10}, tmax[3] = {-1e10, -1e10, -1e10};
+    for (int i = 0; i < n; i++)
+        for (int m = 0; m < 3; m++) {
+            tmin[m] = fmin(tmin[m], c->pos[3 * i + m]);
+            tmax[m] = fmax(tmax[m], c->pos[3 * i + m]);
+        }
+    double amean = 0.0, svol = 0.0;
+    for (int i = 0; i < n; i++) { amean += c->rad[i]; svol += c->rad[i] * c->rad[i] * c->rad[i]; }
+    svol = pow(svol, 1.0 / 3.0);
+    amean = amean / (double)n;
+    double tvol = 1.0;
+    for (int m = 0; m < 3; m++) tvol *= fmax(tmax[m] - tmin[m], amean);
+    double dc = d_cell;
+    if (!(d_cell > 0.0)) {
+        double fv = cell_volume_fraction;
+        if (fv <= 0.0) {
+            fv = 4.0 * ORC_REF_PI / 3.0 * svol * svol * svol / tvol;
+            fv = fmin(fv, 1.0);
+            fv = fmax(fv, 0.02);
+        }
+        dc = pow(4.0 * ORC_REF_PI / 3.0 / fv / (double)n, 1.0 / 3.0) * svol;
+    }
+    for (int m = 0; m < 3; m++) c->cd[m] = correctn235((int)ceil((tmax[m] - tmin[m]) / dc));
+    dc = 0.0;
+    for (int m = 0; m < 3; m++) dc = fmax(dc, (tmax[m] - tmin[m]) / (double)c->cd[m]);
+    c->dcell = dc;
+    for (int m = 0; m < 3; m++) c->cb[m] = tmin[m];
+    c->No = node_order > 0 ? node_order : -node_order + (int)ceil(dc);
+    free(c->snode);
+    c->snode = (int *)malloc(sizeof(int) * 3 * n);
+    for (int i = 0; i < n; i++)
+        for (int m = 0; m < 3; m++) {
+            int nd = (int)floor((c->pos[3 * i + m] - tmin[m]) / dc) + 1;
+            nd = nd < c->cd[m] ? nd : c->cd[m];
+            c->snode[3 * i + m] = nd > 1 ? nd : 1;
+        }
+    c->nnb = 0;
+    for (int iz = -1; iz <= 1; iz++)
+        for (int iy = -1; iy <= 1; iy++)
+            for (int ix = -1; ix <= 1; ix++) {
+                int ir = ix * ix + iy * iy + iz * iz;
+                if (neighbor_node_model == 0 && ir > 0) continue;
+                if (neighbor_node_model == 1 && ir > 1) continue;
+                if (neighbor_node_model == 2 && ir > 2) continue;
+                c->nb_vec[c->nnb][0] = ix; c->nb_vec[c->nnb][1] = iy; c->nb_vec[c->nnb][2] = iz;
+                c->nnb++;
+            }
+    /* near pairs: for sphere i, cells node(i) - neighbour, members j > i in sphere order */
+    int cap = 16, np = 0;
+    int *pi = (int *)malloc(sizeof(int) * cap), *pj = (int *)malloc(sizeof(int) * cap);
+    for (int i = 0; i < n; i++)
+        for (int cell = 0; cell < c->nnb; cell++) {
+            int sx = c->snode[3 * i] - c->nb_vec[cell][0], sy = c->snode[3 * i + 1] - c->nb_vec[cell][1], sz = c->snode[3 * i + 2] - c->nb_vec[cell][2];
+            if (sx < 1 || sy < 1 || sz < 1 || sx > c->cd[0] || sy > c->cd[1] || sz > c->cd[2]) continue;
+            for (int j = i + 1; j < n; j++)
+                if (c->snode[3 * j] == sx && c->snode[3 * j + 1] == sy && c->snode[3 * j + 2] == sz) {
+                    if (np == cap) { cap *= 2; pi = (int *)realloc(pi, sizeof(int) * cap); pj = (int *)realloc(pj, sizeof(int) * cap); }
+                    pi[np] = i; pj[np] = j; np++;
+                }
+        }
+    if (c->ops) { for (int k = 0; k < c->npairs; k++) pairop_free(&c->ops[k]); free(c->ops); c->ops = NULL; }
+    c->ops_ready = 0;
+    free(c->pi_); free(c->pj_);
+    c->pi_ = pi; c->pj_ = pj; c->npairs = np;
+    /* dense regular translations sphere <-> node (vswf_type 1); a translation
+     * shorter than 1e-3 is the identity on the shared orders, as the
+     * reference's zero_translation (r^2 < 1e-6) makes it */
+    const int No = c->No, nbN = No * (No + 2);
+    free(c->joff); free(c->Jsn); free(c->Jns);
+    c->joff = (size_t *)malloc(sizeof(size_t) * (n + 1));
+    size_t tot = 0;
+    for (int i = 0; i < n; i++) { c->joff[i] = tot; tot += (size_t)2 * nbN * c->order[i] * (c->order[i] + 2); }
+    c->joff[n] = tot;
+    c->Jsn = (cplx *)calloc(tot, sizeof(cplx));
+    c->Jns = (cplx *)calloc(tot, sizeof(cplx));
+    for (int i = 0; i < n; i++) {
+        double rv[3], r2 = 0.0;
+        for (int m = 0; m < 3; m++) {
+            rv[m] = dc * ((double)c->snode[3 * i + m] - 0.5) - c->pos[3 * i + m] + c->cb[m];
+            r2 += rv[m] * rv[m];
+        }
+        int L = c->order[i], nb = L * (L + 2);
+        if (r2 < 1.0e-6) {
+            for (int k = 1; k <= imin(nb, nbN); k++)
+                for (int p = 0; p < 2; p++) {
+                    c->Jsn[c->joff[i] + (k - 1) + (size_t)nbN * ((k - 1) + (size_t)nb * p)] = 1.0;
+                    c->Jns[c->joff[i] + (k - 1) + (size_t)nb * ((k - 1) + (size_t)nbN * p)] = 1.0;
+                }
+            continue;
+        }
+        gentranmatrix(L, No, rv, c->rimed, 1, c->Jsn + c->joff[i]);
+        double rm[3] = {-rv[0], -rv[1], -rv[2]};
+        gentranmatrix(No, L, rm, c->rimed, 1, c->Jns + c->joff[i]);
+    }
+    /* node-offset kernels H((t - s) d_cell), zero inside the neighbour stencil */
+    int ox = 2 * c->cd[0] - 1, oy = 2 * c->cd[1] - 1, oz = 2 * c->cd[2] - 1;
+    size_t hsz = (size_t)nbN * nbN * 2;
+    free(c->Hc);
+    c->Hc = (cplx *)calloc((size_t)ox * oy * oz * hsz, sizeof(cplx));
+#pragma omp parallel for schedule(dynamic, 4) num_threads(c->nthreads)
+    for (int e = 0; e < ox * oy * oz; e++) {
+        int dx = e % ox - (c->cd[0] - 1), dy = (e / ox) % oy - (c->cd[1] - 1), dz = e / (ox * oy) - (c->cd[2] - 1);
+        int hole = 0;   /* the stencil is symmetric: offsets equal to a neighbour vector */
+        for (int k = 0; k < c->nnb; k++)
+            if (dx == c->nb_vec[k][0] && dy == c->nb_vec[k][1] && dz == c->nb_vec[k][2]) hole = 1;
+        if (hole) continue;
+        double xp[3] = {dc * dx, dc * dy, dc * dz};
+        gentranmatrix(No, No, xp, c->rimed, 3, c->Hc + (size_t)e * hsz);
+    }
+    c->fft = 1;
+    if (cell_dim_out) for (int m = 0; m < 3; m++) cell_dim_out[m] = c->cd[m];
+    if (d_cell_out) *d_cell_out = dc;
+    return No;
+}
+
+int orc_fft_near_pairs(const orc_ctx *c, int *pi, int *pj)
+{
+    if (pi) memcpy(pi, c->pi_, sizeof(int) * c->npairs);
+    if (pj) memcpy(pj, c->pj_, sizeof(int) * c->npairs);
+    return c->npairs;
+}
+
+/* far part of fft_external_to_external_expansion (fft:72-336): with
+ * S = shiftcoefficient(-1,-1) for conjugate-transpose columns,
+ * g += S Jns conv(Jsn S a). */
+static void fft_far_field(orc_ctx *c, int nrhs, const cplx *ain, cplx *gout, const int *contran)
+{
+    const int n = c->n, No = c->No, nbN = No * (No + 2), neq = c->neqns;
+    const int ncell = c->cd[0] * c->cd[1] * c->cd[2];
+    const int ox = 2 * c->cd[0] - 1, oy = 2 * c->cd[1] - 1;
+    const size_t hsz = (size_t)nbN * nbN * 2;
+    cplx *anode = (cplx *)malloc(sizeof(cplx) * (size_t)ncell * nbN * 2);
+    cplx *gnode = (cplx *)malloc(sizeof(cplx) * (size_t)ncell * nbN * 2);
+    cplx *xt = (cplx *)malloc(sizeof(cplx) * 2 * c->max_order * (c->max_order + 2));
+    cplx *yt = (cplx *)malloc(sizeof(cplx) * 2 * c->max_order * (c->max_order + 2));
+    for (int r = 0; r < nrhs; r++) {
+        const int sv = contran[r] ? -1 : 1;
+        for (size_t k = 0; k < (size_t)ncell * nbN * 2; k++) { anode[k] = 0; gnode[k] = 0; }
+        for (int i = 0; i < n; i++) {
+            int L = c->order[i], nb = L * (L + 2);
+            shiftcoefficient(L, sv, sv, ain + (size_t)neq * r + c->offset[i], xt);
+            int cell = (c->snode[3 * i] - 1) + c->cd[0] * ((c->snode[3 * i + 1] - 1) + c->cd[1] * (c->snode[3 * i + 2] - 1));
+            const cplx *J = c->Jsn + c->joff[i];
+            for (int p = 0; p < 2; p++)
+                for (int k = 0; k < nbN; k++) {
+                    cplx s_ = 0;
+                    for (int m = 0; m < nb; m++) s_ += J[k + (size_t)nbN * (m + (size_t)nb * p)] * xt[m + nb * p];
+                    anode[(size_t)cell * nbN * 2 + (size_t)nbN * p + k] += s_;
+                }
+        }
+#pragma omp parallel for schedule(static) num_threads(c->nthreads)
+        for (int t = 0; t < ncell; t++) {
+            int tx = t % c->cd[0], ty = (t / c->cd[0]) % c->cd[1], tz = t / (c->cd[0] * c->cd[1]);
+            for (int s_ = 0; s_ < ncell; s_++) {
+                int sx = s_ % c->cd[0], sy = (s_ / c->cd[0]) % c->cd[1], sz = s_ / (c->cd[0] * c->cd[1]);
+                int e = (tx - sx + c->cd[0] - 1) + ox * ((ty - sy + c->cd[1] - 1) + oy * (tz - sz + c->cd[2] - 1));
+                const cplx *H = c->Hc + (size_t)e * hsz;
+                for (int p = 0; p < 2; p++)
+                    for (int l = 0; l < nbN; l++) {
+                        cplx acc = 0;
+                        for (int k = 0; k < nbN; k++) acc += H[l + (size_t)nbN * (k + (size_t)nbN * p)] * anode[(size_t)s_ * nbN * 2 + (size_t)nbN * p + k];
+                        gnode[(size_t)t * nbN * 2 + (size_t)nbN * p + l] += acc;
+                    }
+            }
+        }
+        for (int i = 0; i < n; i++) {
+            int L = c->order[i], nb = L * (L + 2);
+            int cell = (c->snode[3 * i] - 1) + c->cd[0] * ((c->snode[3 * i + 1] - 1) + c->cd[1] * (c->snode[3 * i + 2] - 1));
+            const cplx *J = c->Jns + c->joff[i];
+            for (int p = 0; p < 2; p++)
+                for (int m = 0; m < nb; m++) {
+                    cplx s_ = 0;
+                    for (int k = 0; k < nbN; k++) s_ += J[m + (size_t)nb * (k + (size_t)nbN * p)] * gnode[(size_t)cell * nbN * 2 + (size_t)nbN * p + k];
+                    yt[m + nb * p] = s_;
+                }
+            shiftcoefficient(L, sv, sv, yt, xt);
+            for (int k = 0; k < 2 * nb; k++) gout[(size_t)neq * r + c->offset[i] + k] += xt[k];
+        }
+    }
+    free(anode); free(gnode); free(xt); free(yt);
+}
+
 static void external_to_external(orc_ctx *c, int nrhs, const cplx *ain, cplx *gout, const int *contran, int initial_run)
 {
     int neq = c->neqns;
@@ -1137,6 +1367,7 @@ static void external_to_external(orc_ctx *c, int nrhs, const cplx *ain, cplx *go
     for (int t = 0; t < nth; t++)
         for (size_t k = 0; k < (size_t)neq * nrhs; k++) gout[k] += priv[(size_t)neq * nrhs * t + k];
     free(priv);
+    if (c->fft) fft_far_field(c, nrhs, ain, gout, contran);
 }
 
 /* sphereinteraction (scatprops:25-180), free-space external spheres */

@@ -79,6 +79,10 @@ def lib():
         L.orc_tmatrix_symmetrize.argtypes = [c_int, c_void_p, c_void_p]
         L.orc_tmatrix_qext_qsca.argtypes = [c_int, c_void_p, c_double, P(c_double), P(c_double)]
         L.orc_ranorientscatmatrix.argtypes = [c_int, c_void_p, c_double, c_void_p, c_void_p]
+        L.orc_fft_setup.argtypes = [c_void_p, c_double, c_double, c_int, c_int, c_void_p, P(c_double)]
+        L.orc_fft_setup.restype = c_int
+        L.orc_fft_near_pairs.argtypes = [c_void_p, c_void_p, c_void_p]
+        L.orc_fft_near_pairs.restype = c_int
         L.orc_ranorienscatmatrixcalc.argtypes = [c_double, c_void_p, c_int, c_void_p]
         _lib = L
     return _lib
@@ -201,6 +205,16 @@ class Oracle:
             self.L.orc_merge_to_common_origin(self.ctx, nodrt, _p(col), _p(r0), _p(to), _p(o))
             out[:, p] = o
         return out
+
+    def fft_setup(self, cell_volume_fraction=0.2, d_cell=0.0, node_order=-1, neighbor_node_model=2):
+        """Switch to the FFT translation (fft_translation-5.f90): near pairs direct,
+        the rest through cell nodes.  Returns dict(cell_dim, d_cell, node_order, npairs)."""
+        cd = np.zeros(3, np.int32)
+        dc = c_double(0.0)
+        no = self.L.orc_fft_setup(self.ctx, cell_volume_fraction, d_cell, node_order, neighbor_node_model, _p(cd),
+                                  ctypes.byref(dc))
+        npair = self.L.orc_fft_near_pairs(self.ctx, None, None)
+        return dict(cell_dim=cd.tolist(), d_cell=dc.value, node_order=no, npairs=npair)
 
     def distribute_from_common_origin(self, amnp0, nodrt, origin):
         """amnp0: (nb(nodrt), nrhs) LR common-origin coefficients -> (neqns, nrhs) regular expansions about each sphere."""

@@ -311,3 +311,25 @@ def test_tmatrix_file_roundtrip(oracle_mod, tmp_path):
     # entries a file holds: rows of order n <= l only
     lines = sum(1 for _ in open(fn)) - 1
     assert lines == sum(2 * (2 * l + 1) * 2 * l * (l + 2) for l in range(1, T + 1))
+
+
+def test_fft_far_field_exact_at_cell_centres(oracle_mod):
+    """FFT translation oracle: for spheres at cell centres the node expansions
+    are the spheres' own, so the far interactions equal the direct ones."""
+    pos = np.array([[0, 0, 0], [16, 16, 16], [2, 2, 2], [2, 2, 14], [10, 6, 2]], float)
+    L = 3
+    o1 = oracle_mod.Oracle(pos, [1.0] * 5, [1.31] * 5, mie_eps=-L)
+    o2 = oracle_mod.Oracle(pos, [1.0] * 5, [1.31] * 5, mie_eps=-L)
+    info = o2.fft_setup(d_cell=4.0, node_order=3)
+    assert info["cell_dim"] == [4, 4, 4] and info["d_cell"] == 4.0
+    nb = 2 * L * (L + 2)
+    rng = np.random.default_rng(0)
+    for src in (2, 3, 4):
+        x = np.zeros((o1.neqns, 1), complex)
+        x[src * nb:(src + 1) * nb, 0] = rng.standard_normal(nb) + 1j * rng.standard_normal(nb)
+        y1 = o1.sphereinteraction(x, mie_mult=[0])
+        y2 = o2.sphereinteraction(x, mie_mult=[0])
+        for i in (2, 3, 4):
+            if i != src:
+                blk = slice(i * nb, (i + 1) * nb)
+                assert np.abs(y2[blk] - y1[blk]).max() < 1e-12 * np.abs(y1[blk]).max()
