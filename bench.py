@@ -36,6 +36,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 EPS = 1.0e-12          # squared-norm criterion: ||r||/||b|| < 1e-6
+# DRAM bytes per algorithmic byte of the FP32 tiled translation pass, from the
+# ncu capture of the 200-sphere aggregate (163.95 MB of 158.9 MB)
+TRAFFIC_PER_ALG_BYTE = 163.95 / 158.9
 NITER = 10000
 WORKLOAD = "fractal500"
 METRIC = "solves/s at 1e-6 residual (fractal aggregate N=500, x=2, both polarisations)"
@@ -220,8 +223,11 @@ def run_gpu(args):
                                   d2h=(amnp_h.numel() + qeff_h.numel() + qtot_h.numel()) * 8)
         g.close()
 
+    extras = run_extras(args, dev, stream) if (rank == 0 and ws == 1 and not args.no_extras) else None
     if rank == 0:
         line = report_line(args, ws, results, ne)
+        if extras:
+            line["other_workloads"] = extras
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline_sample(results["fp64"]["stats"]["iterations"], threads=os.cpu_count() or 1)
@@ -231,6 +237,76 @@ def run_gpu(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_extras(args, dev, stream):
+    """Secondary workloads of the same path, each timed with CUDA events on the
+    library's stream after one untimed warm-up: the FFT-translation cluster
+    (5000 spheres in a cylinder, cell edge 4), one configuration of the
+    T-matrix ensemble (100 spheres, x = 1.5), and the small 20-sphere cluster."""
+    import torch
+    from mstm_b200 import _lib, api
+    from mstm_b200 import configs as C
+    L = _lib.lib()
+    out = {}
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = None
+        for _ in range(reps):
+            r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps, r
+
+    def cluster(pos, x, m, prec):
+        n = len(pos)
+        g = api.SphereCluster(pos, np.full(n, x), np.full(n, m), mie_epsilon=-C.truncation_order(x), precision=prec)
+        _lib.check(L.mstmg_set_stream(g.ctx, ctypes.c_void_p(stream.cuda_stream)), "set_stream")
+        return g
+
+    # FFT translation cluster
+    pos = C.rsa_cylinder(5000, 1.0, 0.25, 1.0, seed=3)
+    pos = pos[0] if isinstance(pos, tuple) else pos
+    row = {"workload": "5000 spheres, x=1.0, m=1.31, RSA in a cylinder (aspect 1) at fv 0.25, FFT translation, d_cell 4",
+           "metric": "solves/s at 1e-6 residual (both polarisations)"}
+    for prec in ("mixed", "fp64"):
+        g = cluster(pos, 1.0, 1.31 + 0j, prec)
+        grid = g.fft_setup(d_cell=4.0)
+        ms, r = timed(lambda: g.fixedorsoln(eps=EPS, niter=NITER), 2)
+        row[prec] = {"solves_per_s": round(1000.0 / ms, 3), "ms": round(ms, 2), "qext": r["qtot"][0, 0], "iterations": r["iterations"]}
+        row["grid"] = grid
+        g.close()
+    row["qext_rel_diff"] = abs(row["mixed"]["qext"] / row["fp64"]["qext"] - 1)
+    out["fft_cylinder5000"] = row
+    # one T-matrix configuration of the ensemble
+    pos, _ = C.rsa_sphere(100, 1.5, 0.20, seed=4)
+    row = {"workload": "100 spheres, x=1.5, m=1.6+0.005i, RSA in a sphere at fv 0.20: cluster T matrix, "
+                       "all 2Lc(Lc+2) columns, solution_eps 1e-6, t_matrix_convergence 1e-6",
+           "metric": "T matrices/s"}
+    for prec in ("mixed", "fp64"):
+        g = cluster(pos, 1.5, 1.6 + 0.005j, prec)
+        T = g.t_matrix_order()
+        ms, r = timed(lambda: g.tmatrix_solution(T, solution_eps=1e-6, convergence_eps=1e-6), 1)
+        row[prec] = {"tmatrices_per_s": round(1000.0 / ms, 4), "ms": round(ms, 1), "order": r["order"], "t_matrix_order": T,
+                     "columns": 2 * r["order"] * (r["order"] + 2), "qext": r["qtot"][0], "maxiter": r["maxiter"]}
+        g.close()
+    row["qext_rel_diff"] = abs(row["mixed"]["qext"] / row["fp64"]["qext"] - 1)
+    out["tmatrix_cluster100"] = row
+    # the 20-sphere cluster (the reference's CPU-sized case)
+    w = C.workload("cluster20")
+    row = {"workload": "20 spheres, x=1.0, m=1.5+0.01i, RSA in a sphere at fv 0.10, both polarisations",
+           "metric": "solves/s at 1e-6 residual"}
+    for prec in ("mixed", "fp64"):
+        g = cluster(w["pos"], 1.0, 1.5 + 0.01j, prec)
+        ms, r = timed(lambda: g.fixedorsoln(eps=EPS, niter=NITER), 5)
+        row[prec] = {"solves_per_s": round(1000.0 / ms, 2), "ms": round(ms, 3), "qext": r["qtot"][0, 0]}
+        g.close()
+    out["cluster20"] = row
+    return out
 
 
 def report_line(args, ws, R, ne):
@@ -289,7 +365,10 @@ def report_line(args, ws, R, ne):
                   "qext_rel_diff": abs(m["qtot"][0, 0] / p["qtot"][0, 0] - 1)},
         "roofline": {"kernel": "translate_kernel<float> (pair translation pass)", "bound": "hbm",
                      "achieved": round(achieved, 1) if achieved else None, "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 4) if achieved else None, "traffic": None,
+                     "frac": round(achieved / hbm, 4) if achieved else None,
+                     "traffic": round(TRAFFIC_PER_ALG_BYTE * alg),
+                     "traffic_source": "ncu dram__bytes_read+write of this kernel on the 200-sphere aggregate "
+                                       "(profiles/translate_tiled_fp32_fractal200.md), scaled by algorithmic bytes",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": alg, "launch_ms": round(dur, 4), "launches": n32,
                      "canonical_equiv_gbs": round((canon64 / 2 + vec_bytes) / (dur * 1e-3) / 1e9, 1) if n32 else None},
@@ -391,6 +470,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--translation-passes", type=int, default=0,
                     help="profiling case: only run this many translation passes (no solve)")
     ap.add_argument("--workload", default=WORKLOAD)
