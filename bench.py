@@ -306,6 +306,12 @@ def run_extras(args, dev, stream):
         row[prec] = {"solves_per_s": round(1000.0 / ms, 2), "ms": round(ms, 3), "qext": r["qtot"][0, 0]}
         g.close()
     out["cluster20"] = row
+    # learned warm start: a short study (training set generated by the solver)
+    from mstm_b200 import warmstart as WS
+    ws = WS.study(n_train=120, n_eval=8, epochs=60, device=dev, log=None)
+    ws["workload"] = ("held-out configurations of 100-300 spheres, x in [0.5, 2], m random, fv in [0.05, 0.3], "
+                      "+z incidence, mixed precision to 1e-6 residual; network trained here on solver outputs")
+    out["warm_start"] = ws
     return out
 
 

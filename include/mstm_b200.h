@@ -186,6 +186,43 @@ int mstmg_ranorient_scattering(mstmg_ctx *ctx, int t_matrix_order, const double 
 int mstmg_fft_setup(mstmg_ctx *ctx, double cell_volume_fraction, double d_cell, int node_order, int neighbor_node_model, int *cell_dim,
                     double *d_cell_out, int *node_order_out, int *near_pairs);
 
+/* mstmg_fixed_orientation from a caller's initial guess x0 (neqns x 2, the
+ * learned warm start) instead of MSTM's Mie-solution start (fixedorsoln,
+ * mstm-solver-8.f90:482-483).  Each polarisation's guess is used only if its
+ * FP64 relative residual ||b - (I - M H) x0|| / ||b|| is at most
+ * fallback_residual, else that polarisation starts from the Mie solution.
+ * used_guess[2], guess_residual[2]: the decision and the residuals (may be
+ * NULL).  No counterpart in MSTM. */
+int mstmg_fixed_orientation_guess(mstmg_ctx *ctx, double alpha, double sinc, int dir, double eps, int niter, const double *x0,
+                                  double fallback_residual, int *used_guess, double *guess_residual, double *amnp, double *qeff,
+                                  double *qtot, double *maxerr, int *maxiter);
+
+/* Learned warm start network primitives (warmstart.cu), all on device memory
+ * and the given stream; no counterpart in MSTM.
+ *   gemm: C[M x N] (+)= op(A)[M x K] op(B)[K x N]; A FP32 (lda), B BF16
+ *         (b_bf16 = 1) or FP32 (ldb), FP32 accumulation; op = transpose if set;
+ *   bias_act: Y = act(Z + b), act 0 identity / 1 SiLU; act_back: dZ = dY act'(Z + b);
+ *   colsum: db = column sums; edge_concat: rows [h_dst, h_src, ef] and its
+ *   backward (atomic); scatter_add: out[dst[e]] += in[e]; gather: out[e] = in[idx[e]];
+ *   mse: masked mean-square loss (*loss) and gradient; adam: Adam step on FP32
+ *   weights with an optional BF16 copy; to_bf16; knn: k <= 32 nearest
+ *   neighbours of each sphere within its configuration. */
+int mstmg_nn_gemm(int M, int N, int K, const float *A, int lda, int transA, const void *B, int ldb, int transB, int b_bf16, float *C,
+                  int ldc, int accumulate, void *stream);
+int mstmg_nn_bias_act(int M, int N, const float *Z, const float *b, float *Y, int act, void *stream);
+int mstmg_nn_act_back(int M, int N, const float *Z, const float *b, const float *dY, float *dZ, int act, void *stream);
+int mstmg_nn_colsum(int M, int N, const float *dZ, float *db, void *stream);
+int mstmg_nn_edge_concat(int E, int H, int F, const int *dst, const int *src, const float *h, const float *ef, float *Z, void *stream);
+int mstmg_nn_edge_concat_back(int E, int H, int F, const int *dst, const int *src, const float *dZ, float *dh, void *stream);
+int mstmg_nn_scatter_add(int E, int H, const int *dst, const float *in, float *out, void *stream);
+int mstmg_nn_gather(int E, int H, const int *idx, const float *in, float *out, int accumulate, void *stream);
+int mstmg_nn_mse(long long n, const float *y, const float *t, const float *mask, float msum, float *dy, double *loss, void *stream);
+int mstmg_nn_adam(long long n, float *p, const float *g, float *m, float *v, void *pb, float lr, float b1, float b2, float eps, int step,
+                  void *stream);
+int mstmg_nn_to_bf16(long long n, const float *p, void *pb, void *stream);
+int mstmg_nn_axpy(long long n, float a, const float *x, float *y, void *stream);   /* y += a x */
+int mstmg_nn_knn(int n, int k, const int *cfg_start, const int *sphere_cfg, const double *pos, int *nbr, void *stream);
+
 /* Statistics of the last solve: iterations per polarisation, refinement steps,
  * FP64 and FP32 operator passes. */
 int mstmg_last_stats(const mstmg_ctx *ctx, int *iters2, int *outer, int *passes64, int *passes32);

@@ -37,6 +37,23 @@ SIGNATURES = {
     "mstmg_tmatrix_qext_qsca": (c_int, [c_void_p, c_int, c_void_p, P(c_double), P(c_double)]),
     "mstmg_ranorient_scattering": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "mstmg_fft_setup": (c_int, [c_void_p, c_double, c_double, c_int, c_int, c_void_p, P(c_double), P(c_int), P(c_int)]),
+    "mstmg_fixed_orientation_guess": (c_int, [c_void_p, c_double, c_double, c_int, c_double, c_int, c_void_p, c_double, c_void_p,
+                                              c_void_p, c_void_p, c_void_p, c_void_p, P(c_double), P(c_int)]),
+    "mstmg_nn_gemm": (c_int, [c_int, c_int, c_int, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int,
+                              c_void_p]),
+    "mstmg_nn_bias_act": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "mstmg_nn_act_back": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "mstmg_nn_colsum": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "mstmg_nn_edge_concat": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mstmg_nn_edge_concat_back": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mstmg_nn_scatter_add": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mstmg_nn_gather": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "mstmg_nn_mse": (c_int, [ctypes.c_longlong, c_void_p, c_void_p, c_void_p, ctypes.c_float, c_void_p, c_void_p, c_void_p]),
+    "mstmg_nn_adam": (c_int, [ctypes.c_longlong, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_float, ctypes.c_float,
+                              ctypes.c_float, ctypes.c_float, c_int, c_void_p]),
+    "mstmg_nn_to_bf16": (c_int, [ctypes.c_longlong, c_void_p, c_void_p, c_void_p]),
+    "mstmg_nn_axpy": (c_int, [ctypes.c_longlong, ctypes.c_float, c_void_p, c_void_p, c_void_p]),
+    "mstmg_nn_knn": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mstmg_last_stats": (c_int, [c_void_p, c_void_p, P(c_int), P(c_int), P(c_int)]),
     "mstmg_operator_bytes": (c_int, [c_void_p, c_int, P(c_double), P(c_double)]),
     "mstmg_time_translation": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),

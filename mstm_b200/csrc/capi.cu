@@ -942,8 +942,29 @@ static int solve_mixed(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, int
     return MSTMG_OK;
 }
 
+static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, const double* x0, double fallback,
+                                  int* used_guess, double* guess_res, double* amnp, double* qeff, double* qtot, double* maxerr, int* maxiter);
+
 extern "C" int mstmg_fixed_orientation(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, double* amnp,
                                        double* qeff, double* qtot, double* maxerr, int* maxiter)
+{
+    return fixed_orientation_impl(c, alpha, sinc, dir, eps, niter, nullptr, 0.0, nullptr, nullptr, amnp, qeff, qtot, maxerr, maxiter);
+}
+
+extern "C" int mstmg_fixed_orientation_guess(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, const double* x0,
+                                             double fallback_residual, int* used_guess, double* guess_residual, double* amnp, double* qeff,
+                                             double* qtot, double* maxerr, int* maxiter)
+{
+    if (!x0) {
+        set_err("mstmg_fixed_orientation_guess: x0 required");
+        return MSTMG_ERR_ARG;
+    }
+    return fixed_orientation_impl(c, alpha, sinc, dir, eps, niter, x0, fallback_residual, used_guess, guess_residual, amnp, qeff, qtot,
+                                  maxerr, maxiter);
+}
+
+static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, const double* x0, double fallback,
+                                  int* used_guess, double* guess_res, double* amnp, double* qeff, double* qtot, double* maxerr, int* maxiter)
 {
     if (!c || !amnp) return MSTMG_ERR_ARG;
     const int ne = c->neqns;
@@ -963,20 +984,48 @@ extern "C" int mstmg_fixed_orientation(mstmg_ctx* c, double alpha, double sinc, 
     int istat = 0;
     int it[2] = {0, 0}, st[2] = {0, 0};
     double er[2] = {0.0, 0.0};
-    if (niter == 0) {
+    // initial guesses: MSTM's Mie solution (solver:482-483), or the caller's
+    // guess where its FP64 relative residual is at most `fallback`
+    zd* xinit = bvec;
+    if (x0) {
+        zd* g = c->X64.p + 2 * (size_t)ne;   // columns 2, 3 of the work block
+        CK(copy_in(g, x0, sizeof(zd) * 2 * (size_t)ne, c->st));
+        CK(cudaMemcpyAsync(c->X64.p, g, sizeof(zd) * 2 * (size_t)ne, cudaMemcpyDeviceToDevice, c->st));
+        rc = translate<double>(c, c->X64.p, c->Y64.p, 2, 0u);
+        if (rc) return rc;
         for (int p = 0; p < 2; p++)
-            CK(cudaMemcpyAsync(c->amnp.p + (size_t)p * ne, bvec + (size_t)p * ne, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+            launch_resid<double, double>(sm, c->an.p, bvec + (size_t)p * ne, g + (size_t)p * ne, c->Y64.p + (size_t)p * ne,
+                                         c->Y64.p + (size_t)(2 + p) * ne, c->part.p, c->small.p + 2 * p, c->nsm, c->st);
+        CK(cudaMemcpyAsync(c->h_small, c->small.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        for (int p = 0; p < 2; p++) {
+            double rr = c->h_small[2 * p], bb = c->h_small[2 * p + 1];
+            double res = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+            bool use = res <= fallback;
+            if (guess_res) guess_res[p] = res;
+            if (used_guess) used_guess[p] = use ? 1 : 0;
+            if (!use) CK(cudaMemcpyAsync(g + (size_t)p * ne, bvec + (size_t)p * ne, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+        }
+        // the BiCG work below reuses X64/Y64; keep the guesses in the amnp buffer
+        CK(cudaMemcpyAsync(c->amnp.p, g, sizeof(zd) * 2 * (size_t)ne, cudaMemcpyDeviceToDevice, c->st));
+        xinit = c->amnp.p;
+    }
+    if (niter == 0) {
+        if (xinit != c->amnp.p)
+            for (int p = 0; p < 2; p++)
+                CK(cudaMemcpyAsync(c->amnp.p + (size_t)p * ne, bvec + (size_t)p * ne, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
     } else if (c->opts.precision == MSTMG_PRECISION_MIXED) {
         zd* xs[2] = {c->amnp.p, c->amnp.p + ne};
         zd* bs[2] = {bvec, bvec + ne};
-        for (int p = 0; p < 2; p++) CK(cudaMemcpyAsync(xs[p], bs[p], sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+        if (xinit != c->amnp.p)
+            for (int p = 0; p < 2; p++) CK(cudaMemcpyAsync(xs[p], bs[p], sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
         rc = solve_mixed(c, bs, xs, eps, niter, it, er, st);
         if (rc) return rc;
     } else {
         // the reference's order: polarisation 1 then 2, each from x0 = Mie*f
         for (int p = 0; p < 2; p++) {
             BicgVecs<double> v = vecs_at<double>(c->vec64.p, ne, 0);
-            CK(cudaMemcpyAsync(v.x, bvec + (size_t)p * ne, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+            CK(cudaMemcpyAsync(v.x, xinit + (size_t)p * ne, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
             const zd* bb[1] = {bvec + (size_t)p * ne};
             rc = bicg_batched<double>(c, 1, bb, &v, true, niter, &eps, &it[p], &er[p], &st[p]);
             if (rc) return rc;

@@ -333,3 +333,35 @@ def test_fft_far_field_exact_at_cell_centres(oracle_mod):
             if i != src:
                 blk = slice(i * nb, (i + 1) * nb)
                 assert np.abs(y2[blk] - y1[blk]).max() < 1e-12 * np.abs(y1[blk]).max()
+
+
+def test_warmstart_restatement_gradients_by_finite_differences():
+    """The CPU restatement of the warm-start network (the checker of the device
+    kernels) differentiates correctly: central differences on a small network."""
+    from oracle import warmstart_ref as R
+    rng = np.random.default_rng(0)
+    H, NF, EF, NOUT, L = 8, 5, 3, 6, 3
+    P = {"enc_w": rng.standard_normal((NF, H)) * 0.3, "enc_b": rng.standard_normal(H) * 0.1,
+         "out_w": rng.standard_normal((H, NOUT)) * 0.3, "out_b": rng.standard_normal(NOUT) * 0.1}
+    for t in range(L):
+        P[f"m{t}_w"] = rng.standard_normal((2 * H + EF, H)) * 0.3
+        P[f"m{t}_b"] = rng.standard_normal(H) * 0.1
+        P[f"u{t}_w1"] = rng.standard_normal((H, H)) * 0.3
+        P[f"u{t}_w2"] = rng.standard_normal((H, H)) * 0.3
+        P[f"u{t}_b"] = rng.standard_normal(H) * 0.1
+    Nn, E = 7, 20
+    X, ef = rng.standard_normal((Nn, NF)), rng.standard_normal((E, EF))
+    dst, src = rng.integers(0, Nn, E), rng.integers(0, Nn, E)
+    tg, mask = rng.standard_normal((Nn, NOUT)), (rng.random((Nn, NOUT)) < 0.7).astype(float)
+    _, G = R.forward_backward(P, X, ef, dst, src, tg, mask, layers=L)
+    for name in P:
+        for _ in range(3):
+            idx = tuple(rng.integers(0, s) for s in P[name].shape)
+            h = 1e-6
+            P[name][idx] += h
+            lp, _ = R.forward_backward(P, X, ef, dst, src, tg, mask, layers=L)
+            P[name][idx] -= 2 * h
+            lm, _ = R.forward_backward(P, X, ef, dst, src, tg, mask, layers=L)
+            P[name][idx] += h
+            fd = (lp - lm) / (2 * h)
+            assert abs(fd - G[name][idx]) <= 1e-5 * (abs(fd) + abs(G[name][idx])) + 1e-10
