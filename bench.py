@@ -317,6 +317,20 @@ def run_extras(args, dev, stream):
     ws["workload"] = ("held-out configurations of 100-300 spheres, x in [0.5, 2], m random, fv in [0.05, 0.3], "
                       "+z incidence, mixed precision to 1e-6 residual; network trained here on solver outputs")
     out["warm_start"] = ws
+    # batched ensemble of T matrices (uneven sizes), concurrent and autotuned, against one at a time
+    from mstm_b200 import ensemble as EN
+    cfgs = EN.ensemble_configs(6, seed=4, nmin=50, nmax=150)
+    seq = EN.solve_ensemble(cfgs, precision="mixed", workers=1)
+    tuner = EN.Autotuner(reps=2)
+    bat = EN.solve_ensemble(cfgs, precision="mixed", workers=4, tuner=tuner)
+    out["ensemble_tmatrix"] = {
+        "workload": "6 configurations, 50-150 spheres (seeded), x=1.5, m=1.6+0.005i, RSA at fv 0.20: cluster T matrices, "
+                    "orientation-averaged Qext/Qsca and scattering matrix, ensemble means",
+        "metric": "T matrices/s (mixed precision)",
+        "one_at_a_time": round(seq["tmatrices_per_s"], 4), "batched_autotuned": round(bat["tmatrices_per_s"], 4),
+        "tuning_s": round(bat["tune_s"], 2), "qext_mean": bat["qext"], "qsca_mean": bat["qsca"],
+        "chosen": [dict(size=l["key"][0], order=l["key"][1], best=l["best"], ms=round(l["best_ms"], 3)) for l in tuner.log],
+    }
     return out
 
 
@@ -466,12 +480,13 @@ def run_translation_case(args):
     workload, timed with CUDA events (the case the ncu captures use)."""
     from mstm_b200 import api, configs as C
     w = C.workload(args.workload)
-    g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=-w["order"], precision=args.precision)
+    g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=-w["order"], precision=args.precision,
+                          fp32_chunk=args.fp32_chunk, tile_ctas_per_sm=args.ctas_per_sm)
     ms = g.time_translation(args.precision, args.nrhs, args.translation_passes)
     sb, cb = g.operator_bytes(args.precision)
-    print(json.dumps({"workload": args.workload, "precision": args.precision, "nrhs": args.nrhs, "ms_per_pass": ms,
-                      "operator_bytes": sb, "operator_gbs": sb / ms / 1e6}))
-    g.close()   # cbicg iterations of the FP64 solve of this workload (both polarisations)
+    print(json.dumps({"workload": args.workload, "precision": args.precision, "nrhs": args.nrhs, "fp32_chunk": args.fp32_chunk,
+                      "ctas_per_sm": args.ctas_per_sm, "ms_per_pass": ms, "operator_bytes": sb, "operator_gbs": sb / ms / 1e6}))
+    g.close()
 
 
 def main():
@@ -486,6 +501,8 @@ def main():
                     help="profiling case: only run this many translation passes (no solve)")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--fp32-chunk", type=int, default=0, help="profiling case: FP32 column chunk (2 or 4; 0 default)")
+    ap.add_argument("--ctas-per-sm", type=int, default=0, help="profiling case: tiled kernel CTAs per SM (0 default)")
     ap.add_argument("--nrhs", type=int, default=4)
     args = ap.parse_args()
     if args.translation_passes:

@@ -53,6 +53,8 @@ typedef struct {
     double inner_eps;              /* mixed mode: squared residual reduction per inner solve (default 1e-8) */
     int max_outer;                 /* mixed mode: refinement steps cap (default 30) */
     int generic_kernel;            /* 1: always use the order-generic translation kernel (default 0) */
+    int tile_ctas_per_sm;          /* tiled kernel CTAs per SM, 1 or 2 (0: as many as shared memory allows, at most 2) */
+    int fp32_chunk;                /* columns per chunk of FP32 many-column passes, 2 or 4 (0: 4) */
 } mstmg_opts;
 
 /* Fill opts with the defaults above. */

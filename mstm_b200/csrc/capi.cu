@@ -168,6 +168,8 @@ extern "C" void mstmg_default_opts(mstmg_opts* o)
     o->inner_eps = 1.0e-8;
     o->max_outer = 30;
     o->generic_kernel = 0;
+    o->tile_ctas_per_sm = 0;
+    o->fp32_chunk = 0;
 }
 
 extern "C" const char* mstmg_last_error(void) { return g_err.c_str(); }
@@ -626,6 +628,7 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
         ta.nsph = c->n;
         ta.contran = contran;
         ta.err = c->err.p;
+        ta.ctas_per_sm = c->opts.tile_ctas_per_sm;
     }
     if (nchunk > 1 && !use_tiled) return MSTMG_ERR_UNSUPPORTED;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -668,7 +671,7 @@ template <typename T> static int translate_many(mstmg_ctx* c, const cpx<T>* x, c
             if ((pattern2 >> (r & 1)) & 1u) m |= 1u << r;
         return m;
     };
-    const int NR = sizeof(T) == 4 ? 4 : 2;
+    const int NR = sizeof(T) == 4 ? (c->opts.fp32_chunk == 2 ? 2 : 4) : 2;
     if (c->tiled && ncols > NR && ncols % NR == 0 && tiled_supported(c->lmax, NR)) {
         int rc = translate<T>(c, x, y, NR, expand(NR), ncols / NR);
         if (rc != MSTMG_ERR_UNSUPPORTED) return rc;
@@ -2035,31 +2038,48 @@ extern "C" int mstmg_kernel_time(mstmg_ctx* c, double* ms64, int* n64, double* m
 
 extern "C" long long mstmg_kernel_launches(void) { return launch_counter().load(); }
 
+// One translation pass over nrhs columns laid out as BiCG packs them
+// ([p, A^T conj w] pairs, odd columns conjugate-transpose products), timed with
+// CUDA events on the context's stream (mean of reps after one warm-up).
 extern "C" int mstmg_time_translation(mstmg_ctx* c, int prec, int nrhs, int reps, double* ms)
 {
-    if (!c || nrhs < 1 || nrhs > 4 || reps < 1) return MSTMG_ERR_ARG;
+    if (!c || nrhs < 1 || nrhs > 256 || reps < 1) return MSTMG_ERR_ARG;
     int rc = ensure_ops(c, prec, false);
     if (rc) return rc;
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    unsigned mask = (nrhs >= 2) ? 0xAu : 0u;
-    // warm-up
-    if (prec == 0) rc = translate<double>(c, c->X64.p, c->Y64.p, nrhs, mask);
-    else rc = translate<float>(c, c->X32.p, c->Y32.p, nrhs, mask);
-    if (rc) return rc;
-    CK(cudaEventRecord(e0, c->st));
-    for (int k = 0; k < reps; k++) {
-        if (prec == 0) rc = translate<double>(c, c->X64.p, c->Y64.p, nrhs, mask);
-        else rc = translate<float>(c, c->X32.p, c->Y32.p, nrhs, mask);
-        if (rc) return rc;
+    DevBuf<zd> x64, y64;
+    DevBuf<zf> x32, y32;
+    const size_t cols = (size_t)c->neqns * nrhs;
+    if (prec == 0) {
+        CK(x64.alloc(cols));
+        CK(y64.alloc(cols));
+        CK(cudaMemsetAsync(x64.p, 0, sizeof(zd) * cols, c->st));
+    } else {
+        CK(x32.alloc(cols));
+        CK(y32.alloc(cols));
+        CK(cudaMemsetAsync(x32.p, 0, sizeof(zf) * cols, c->st));
     }
-    CK(cudaEventRecord(e1, c->st));
-    CK(cudaEventSynchronize(e1));
+    auto pass = [&]() -> int {
+        if (prec == 0) return translate_many<double>(c, x64.p, y64.p, nrhs, nrhs >= 2 ? 2u : 0u);
+        return translate_many<float>(c, x32.p, y32.p, nrhs, nrhs >= 2 ? 2u : 0u);
+    };
+    if ((rc = pass())) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        set_err("mstmg_time_translation: cudaEventCreate failed");
+        return MSTMG_ERR_CUDA;
+    }
+    cudaEventRecord(e0, c->st);
+    for (int k = 0; k < reps && rc == 0; k++) rc = pass();
+    cudaEventRecord(e1, c->st);
+    cudaError_t es = cudaEventSynchronize(e1);
     float t = 0.f;
-    CK(cudaEventElapsedTime(&t, e0, e1));
+    if (es == cudaSuccess) es = cudaEventElapsedTime(&t, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (rc) return rc;
+    CK(es);
     if (ms) *ms = t / reps;
     return check_kernel_err(c);
 }

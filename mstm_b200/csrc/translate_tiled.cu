@@ -429,6 +429,7 @@ template <typename T, int L, int NR, int B> static int launch_one(const TiledArg
     int per_sm = (int)((228 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
     if (per_sm > 2) per_sm = 2;
+    if (a.ctas_per_sm >= 1 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
     int blocks = nsm * per_sm;
     if (blocks > a.ntiles * a.nchunk) blocks = a.ntiles * a.nchunk;
     if (blocks < 1) return 0;

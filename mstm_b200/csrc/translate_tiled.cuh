@@ -14,6 +14,7 @@ template <typename T> struct TiledArgs {
     int ld, nrhs, nsph;      // nrhs: columns per chunk (the kernel's NR)
     int nchunk;              // chunks of nrhs columns: x and y hold nrhs * nchunk columns
     unsigned contran;        // bit r: column r of every chunk is a conjugate-transpose product
+    int ctas_per_sm;         // 0: as many as shared memory allows (at most 2)
     int* err;
 };
 

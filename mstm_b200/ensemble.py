@@ -1,0 +1,148 @@
+"""Ensembles of random configurations (the random-orientation workflow of
+main_calling_program, mstm-input-37.f90:1411-1448, repeated over
+configurations): each configuration's cluster T matrix (tmatrix_solution),
+its orientation-averaged efficiencies and scattering matrix
+(ranorientscatmatrix), and the ensemble means.
+
+Configurations of uneven size are solved concurrently: worker threads each
+drive their own contexts, and every context launches on its own CUDA stream,
+so small configurations fill the GPU together (the C calls release the
+interpreter lock).  Kernel settings are chosen per size class by `Autotuner`,
+which times one many-column translation pass -- the operation that dominates
+a T-matrix solve -- under each candidate setting and keeps the fastest.
+"""
+import ctypes
+import threading
+import time
+
+import numpy as np
+
+from . import _lib
+from . import api
+from . import configs as C
+
+
+def ensemble_configs(count, seed=4, nmin=50, nmax=400, x=1.5, m=1.6 + 0.005j, fv=0.20):
+    """Seeded ensemble: sphere counts uniform in [nmin, nmax], identical spheres
+    of size parameter x and index m, RSA in a bounding sphere at volume fraction fv."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(rng.integers(nmin, nmax + 1))
+        pos, _ = C.rsa_sphere(n, x, fv, seed=int(rng.integers(0, 2 ** 31 - 1)))
+        out.append(dict(pos=np.asarray(pos, np.float64), x=x, m=m, n=n, order=C.truncation_order(x)))
+    return out
+
+
+class Autotuner:
+    """Per size class (sphere count rounded to 50, sphere order, precision), the
+    tiled kernel's CTAs per SM, the FP32 column chunk and the kernel family
+    (tiled or order-generic), chosen by timing a translation pass over the
+    column count of the largest T-matrix order's batch."""
+
+    CANDIDATES = [dict(tile_ctas_per_sm=c, fp32_chunk=k, generic_kernel=0) for c in (1, 2) for k in (2, 4)] + \
+                 [dict(tile_ctas_per_sm=0, fp32_chunk=0, generic_kernel=1)]
+
+    def __init__(self, reps=3):
+        self.reps = reps
+        self.table = {}
+        self.lock = threading.Lock()
+        self.log = []
+
+    @staticmethod
+    def size_class(n):
+        return int(50 * round(n / 50.0))
+
+    def choose(self, cfg, precision, columns):
+        key = (self.size_class(len(cfg["pos"])), cfg["order"], precision, columns)
+        with self.lock:
+            if key in self.table:
+                return self.table[key]
+        L = _lib.lib()
+        best, best_ms, trials = None, float("inf"), []
+        n = len(cfg["pos"])
+        for cand in self.CANDIDATES:
+            g = api.SphereCluster(cfg["pos"], np.full(n, cfg["x"]), np.full(n, cfg["m"]), mie_epsilon=-cfg["order"],
+                                  precision=precision, **cand)
+            ms = ctypes.c_double(0.0)
+            prec = 0 if precision == "fp64" else 1
+            rc = L.mstmg_time_translation(g.ctx, prec, columns, self.reps, ctypes.byref(ms))
+            err = L.mstmg_last_error().decode() if rc != 0 else ""
+            g.close()
+            if rc != 0:
+                trials.append((dict(cand), None, f"status {rc}: {err}"))
+                continue
+            trials.append((dict(cand), ms.value, ""))
+            if ms.value < best_ms:
+                best, best_ms = dict(cand), ms.value
+        with self.lock:
+            if best is not None:
+                self.table[key] = best
+            self.log.append(dict(key=key, trials=trials, best=best, best_ms=best_ms))
+        return best
+
+
+def solve_one(cfg, precision="mixed", settings=None, solution_eps=1e-6, convergence_eps=1e-6, nangles=181, trans_eps=1e-5):
+    """T matrix, orientation-averaged efficiencies and scattering matrix of one configuration."""
+    n = len(cfg["pos"])
+    g = api.SphereCluster(cfg["pos"], np.full(n, cfg["x"]), np.full(n, cfg["m"]), mie_epsilon=-cfg["order"], precision=precision,
+                          **(settings or {}))
+    T = g.t_matrix_order(trans_eps=trans_eps)
+    r = g.tmatrix_solution(T, solution_eps=solution_eps, convergence_eps=convergence_eps)
+    u = r["order"]
+    nb = 2 * u * (u + 2)
+    tm = np.asfortranarray(r["tmat"][:nb, :nb])
+    ro = g.ranorientscatmatrix(tm, u, nangles=nangles)
+    qe, qs = g.tmatrix_qext_qsca(tm, u)
+    g.close()
+    return dict(n=n, t_matrix_order=T, order=u, qtot=r["qtot"], qext_t=qe, qsca_t=qs, smat=ro["smat"], coherent=ro["coherent"],
+                maxiter=r["maxiter"], istat=r["istat"])
+
+
+def solve_ensemble(cfgs, precision="mixed", workers=4, tuner=None, **kw):
+    """Solve every configuration (largest first, over `workers` threads) and
+    return per-configuration results, ensemble means and throughput."""
+    order = sorted(range(len(cfgs)), key=lambda k: -len(cfgs[k]["pos"]))
+    results = [None] * len(cfgs)
+    tune_cols = 2 * (2 * 25 + 1)   # column count of a large order's batch, the tuning case
+    t_tune = time.time()
+    if tuner is not None:
+        # one representative per size class, timed alone before any solve runs
+        seen = set()
+        for k in order:
+            key = (Autotuner.size_class(len(cfgs[k]["pos"])), cfgs[k]["order"])
+            if key not in seen:
+                seen.add(key)
+                tuner.choose(cfgs[k], precision, tune_cols)
+    t_tune = time.time() - t_tune
+    errors = []
+    nxt = [0]
+    lock = threading.Lock()
+
+    def worker():
+        while True:
+            with lock:
+                if nxt[0] >= len(order):
+                    return
+                k = order[nxt[0]]
+                nxt[0] += 1
+            cfg = cfgs[k]
+            try:
+                settings = tuner.choose(cfg, precision, tune_cols) if tuner is not None else None
+                results[k] = solve_one(cfg, precision, settings, **kw)
+            except Exception as e:   # reported after the join
+                errors.append((k, repr(e)))
+
+    t0 = time.time()
+    threads = [threading.Thread(target=worker) for _ in range(max(1, workers))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    wall = time.time() - t0
+    if errors:
+        raise RuntimeError(f"ensemble: {len(errors)} configurations failed, first: {errors[0]}")
+    q = np.array([r["qtot"] for r in results])
+    smat = np.mean([r["smat"] for r in results], axis=0)
+    return dict(per_config=results, qext=float(q[:, 0].mean()), qabs=float(q[:, 1].mean()), qsca=float(q[:, 2].mean()),
+                smat=smat, wall_s=wall, tune_s=t_tune, tmatrices_per_s=len(cfgs) / wall)
