@@ -17,6 +17,7 @@
 #include "mrhs.cuh"
 #include "ranorient.cuh"
 #include "fftpath.cuh"
+#include "densepair.cuh"
 #include <cufft.h>
 #include <memory>
 
@@ -125,6 +126,15 @@ struct mstmg_ctx {
     int iters[2] = {0, 0}, outer = 0, passes64 = 0, passes32 = 0;
     std::vector<int> tord;   // translation order of each sphere to the cluster origin (mstmg_t_matrix_order)
     std::unique_ptr<FftState> fft;   // set by mstmg_fft_setup
+    // pairs below translation_switch_order: dense gentranmatrix records (densepair.cu)
+    int ndense = 0;
+    long long dense_units = 0;
+    DevBuf<int2> dpairs;
+    DevBuf<long long> doff;
+    DevBuf<zd> dop64;
+    DevBuf<zf> dop32;
+    DevBuf<double> gt_tc, gt_bcd, gt_fnr;
+    int gt_nmax = 0;
     cudaStream_t own_st = nullptr;
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -262,9 +272,8 @@ static int setup_layout(mstmg_ctx* c)
         set_err("sphere order " + std::to_string(lm) + " exceeds the kernels' limit " + std::to_string(MSTMG_LMAX));
         return MSTMG_ERR_UNSUPPORTED;
     }
-    if (n > 1 && lmin < c->opts.translation_switch_order) {
-        set_err("pairs with min order below translation_switch_order use MSTM's dense gentranmatrix path, "
-                "which this library does not implement");
+    if (2 * lm > GT_WMAX) {
+        set_err("sphere orders above 20 are not supported");
         return MSTMG_ERR_UNSUPPORTED;
     }
     c->neqns = (int)ne;
@@ -295,8 +304,44 @@ static int setup_layout(mstmg_ctx* c)
     launch_mie_coefs(n, c->rad.p, c->ri.p, c->opts.medium_re, c->opts.medium_im, c->d_order.p, c->d_mie_offset.p, c->an.p,
                      c->an_inv.p, c->an32.p, c->qext.p, c->qabs.p, c->st);
     CK(cudaGetLastError());
+    // pairs whose smaller order is below translation_switch_order take the
+    // reference's dense path (coefficient_translation, rot_op false)
+    const int tso = c->opts.translation_switch_order;
+    auto dense_pair = [&](int i, int j) { return std::min(c->order[i], c->order[j]) < tso; };
+    {
+        std::vector<int2> dp;
+        std::vector<long long> doff;
+        long long du = 0;
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++)
+                if (dense_pair(i, j)) {
+                    dp.push_back(make_int2(i, j));
+                    doff.push_back(du);
+                    du += 2LL * c->order[i] * (c->order[i] + 2) * c->order[j] * (c->order[j] + 2);
+                }
+        c->ndense = (int)dp.size();
+        c->dense_units = du;
+        if (c->ndense > 0) {
+            CK(c->dpairs.alloc(dp.size()));
+            CK(c->doff.alloc(doff.size()));
+            CK(cudaMemcpyAsync(c->dpairs.p, dp.data(), sizeof(int2) * dp.size(), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(c->doff.p, doff.data(), sizeof(long long) * doff.size(), cudaMemcpyHostToDevice, c->st));
+            std::vector<double> tcv, bd(GT_WMAX + 2);
+            gentran_constants(lm, tcv);
+            mstmg::Tables tb(6 * GT_WMAX + 6);
+            for (int k = 0; k < (int)bd.size(); k++) bd[k] = tb.bc(k, k);
+            CK(c->gt_tc.alloc(tcv.size()));
+            CK(c->gt_bcd.alloc(bd.size()));
+            CK(c->gt_fnr.alloc(tb.fnr.size()));
+            CK(cudaMemcpyAsync(c->gt_tc.p, tcv.data(), sizeof(double) * tcv.size(), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(c->gt_bcd.p, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(c->gt_fnr.p, tb.fnr.data(), sizeof(double) * tb.fnr.size(), cudaMemcpyHostToDevice, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            c->gt_nmax = lm;
+        }
+    }
     // pair list (i < j, the reference's loop order) and operator offsets
-    long long np = (long long)n * (n - 1) / 2;
+    long long np = (long long)n * (n - 1) / 2 - c->ndense;
     if (np > 2000000000LL) {
         set_err("too many sphere pairs for the direct translation path");
         return MSTMG_ERR_UNSUPPORTED;
@@ -333,7 +378,7 @@ static int setup_layout(mstmg_ctx* c)
                 out.push_back({std::min(a_, b_), std::max(a_, b_)});
             }
     };
-    c->tiled = !c->opts.generic_kernel && (lm == lmin) && tiled_supported(lm, 1) && n > 1 && n < 65536;
+    c->tiled = !c->opts.generic_kernel && (lm == lmin) && lmin >= tso && tiled_supported(lm, 1) && n > 1 && n < 65536;
     std::vector<int4> tl;
     if (c->tiled) {
         const int B = TILE_B;
@@ -354,7 +399,8 @@ static int setup_layout(mstmg_ctx* c)
     } else {
         std::vector<std::pair<int, int>> pp;
         tournament(n, pp);
-        for (auto& ij : pp) add_pair(ij.first, ij.second);
+        for (auto& ij : pp)
+            if (!dense_pair(ij.first, ij.second)) add_pair(ij.first, ij.second);
     }
     if (t != np) {
         set_err("internal error: pair schedule incomplete");
@@ -553,12 +599,51 @@ extern "C" int mstmg_mie_coefficients(const mstmg_ctx* c, double* an, double* qe
 // ---------------------------------------------------------------------------
 // Generate the stored pair operators.  want64 / want32 select the FP64 and
 // FP32 records; both come out of one pass of the generator when both are due.
+static DenseArgs dense_args(mstmg_ctx* c)
+{
+    DenseArgs d;
+    d.npairs = c->ndense;
+    d.pairs = c->dpairs.p;
+    d.order = c->d_order.p;
+    d.offset = c->d_offset.p;
+    d.pos = c->pos.p;
+    d.off = c->doff.p;
+    d.rec64 = nullptr;
+    d.rec32 = nullptr;
+    d.rimed_re = c->opts.medium_re;
+    d.rimed_im = c->opts.medium_im;
+    d.g.tc = c->gt_tc.p;
+    d.g.nmax = c->gt_nmax;
+    d.g.nd = c->gt_nmax * (c->gt_nmax + 2);
+    d.g.fnr = c->gt_fnr.p;
+    d.g.bcd = c->gt_bcd.p;
+    return d;
+}
+
 static int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
 {
-    if (c->npairs == 0) return MSTMG_OK;
+    if (c->npairs == 0 && c->ndense == 0) return MSTMG_OK;
     bool need64 = want64 && (force || !c->ops64_ready);
     bool need32 = want32 && (force || !c->ops32_ready);
     if (!need64 && !need32) return MSTMG_OK;
+    if (c->ndense > 0) {
+        DenseArgs d = dense_args(c);
+        if (need64) {
+            CK(c->dop64.alloc(c->dense_units));
+            d.rec64 = c->dop64.p;
+        }
+        if (need32) {
+            CK(c->dop32.alloc(c->dense_units));
+            d.rec32 = c->dop32.p;
+        }
+        launch_dense_gen(d, c->st);
+        CK(cudaGetLastError());
+    }
+    if (c->npairs == 0) {
+        if (need64) c->ops64_ready = true;
+        if (need32) c->ops32_ready = true;
+        return MSTMG_OK;
+    }
     if (need64) CK(c->op64.alloc(c->op_units));
     if (need32) CK(c->op32.alloc(c->op_units));
     OpGenArgs a;
@@ -597,6 +682,12 @@ template <> const float* ops_ptr<float>(mstmg_ctx* c) { return c->op32.p; }
 template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran, int nchunk = 1)
 {
     CK(cudaMemsetAsync(y, 0, sizeof(cpx<T>) * (size_t)c->neqns * nrhs * nchunk, c->st));
+    if (c->ndense > 0) {
+        if (nchunk > 1) return MSTMG_ERR_UNSUPPORTED;
+        const T* drec = sizeof(T) == 8 ? (const T*)c->dop64.p : (const T*)c->dop32.p;
+        launch_dense_apply<T>(dense_args(c), drec, x, y, c->neqns, nrhs, contran, c->st);
+        CK(cudaGetLastError());
+    }
     if (c->npairs == 0) return (c->fft && c->fft->on) ? fft_far<T>(c, x, y, nrhs * nchunk, contran) : MSTMG_OK;
     TransArgs<T> a;
     a.npairs = c->npairs;
@@ -1836,6 +1927,10 @@ static int fft_build(mstmg_ctx* c)
     F.nbN = F.No * (F.No + 2);
     if (F.No < 1 || F.nbN > FFT_NBN_MAX || 2 * F.No > GT_WMAX || F.No + c->lmax > GT_WMAX) {
         set_err("FFT translation: node order out of range (1..20)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    if (c->ndense > 0) {
+        set_err("FFT translation: spheres below translation_switch_order are not supported on this path");
         return MSTMG_ERR_UNSUPPORTED;
     }
     F.N8 = (size_t)8 * F.cd[0] * F.cd[1] * F.cd[2];

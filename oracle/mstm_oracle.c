@@ -1321,6 +1321,46 @@ static void fft_far_field(orc_ctx *c, int nrhs, const cplx *ain, cplx *gout, con
     free(anode); free(gnode); free(xt); free(yt);
 }
 
+/* Dense pair translation (coefficient_translation with rot_op false): gen_mat
+ * = gentranmatrix(L_j -> L_i, r_i - r_j); j -> i uses gen_mat, i -> j its
+ * transpose; shiftcoefficient(-1,-1) on input and output when shift_op
+ * differs from tran_op. */
+static void dense_pair_apply(const orc_ctx *c, int i, int j, int nrhs, const cplx *ain, cplx *g, const int *contran)
+{
+    int Li = c->order[i], Lj = c->order[j], nbi = Li * (Li + 2), nbj = Lj * (Lj + 2), neq = c->neqns;
+    cplx *H = (cplx *)malloc(sizeof(cplx) * (size_t)nbi * nbj * 2);
+    double rv[3] = {c->pos[3 * i] - c->pos[3 * j], c->pos[3 * i + 1] - c->pos[3 * j + 1], c->pos[3 * i + 2] - c->pos[3 * j + 2]};
+    gentranmatrix(Lj, Li, rv, c->rimed, 3, H);
+    cplx *a = (cplx *)malloc(sizeof(cplx) * 2 * (nbi > nbj ? nbi : nbj));
+    cplx *o = (cplx *)malloc(sizeof(cplx) * 2 * (nbi > nbj ? nbi : nbj));
+    for (int r = 0; r < nrhs; r++) {
+        int top = contran[r] != 0;
+        /* j -> i: shift when tran_op (shift_op false) */
+        int sv = top ? -1 : 1;
+        shiftcoefficient(Lj, sv, sv, ain + (size_t)neq * r + c->offset[j], a);
+        for (int p = 0; p < 2; p++)
+            for (int t = 0; t < nbi; t++) {
+                cplx acc = 0;
+                for (int s_ = 0; s_ < nbj; s_++) acc += H[t + (size_t)nbi * (s_ + (size_t)nbj * p)] * a[s_ + nbj * p];
+                o[t + nbi * p] = acc;
+            }
+        shiftcoefficient(Li, sv, sv, o, o);
+        for (int k = 0; k < 2 * nbi; k++) g[(size_t)neq * r + c->offset[i] + k] += o[k];
+        /* i -> j: shift when not tran_op (shift_op true) */
+        sv = top ? 1 : -1;
+        shiftcoefficient(Li, sv, sv, ain + (size_t)neq * r + c->offset[i], a);
+        for (int p = 0; p < 2; p++)
+            for (int s_ = 0; s_ < nbj; s_++) {
+                cplx acc = 0;
+                for (int t = 0; t < nbi; t++) acc += a[t + nbi * p] * H[t + (size_t)nbi * (s_ + (size_t)nbj * p)];
+                o[s_ + nbj * p] = acc;
+            }
+        shiftcoefficient(Lj, sv, sv, o, o);
+        for (int k = 0; k < 2 * nbj; k++) g[(size_t)neq * r + c->offset[j] + k] += o[k];
+    }
+    free(H); free(a); free(o);
+}
+
 static void external_to_external(orc_ctx *c, int nrhs, const cplx *ain, cplx *gout, const int *contran, int initial_run)
 {
     int neq = c->neqns;
@@ -1356,6 +1396,12 @@ static void external_to_external(orc_ctx *c, int nrhs, const cplx *ain, cplx *go
                 double rv[3] = {c->pos[3 * i] - c->pos[3 * j], c->pos[3 * i + 1] - c->pos[3 * j + 1], c->pos[3 * i + 2] - c->pos[3 * j + 2]};
                 pairop_compute(&local, noi, noj, rv, 3, c->rimed);
                 op = &local;
+            }
+            if (imin(noi, noj) < 3) {
+                /* dense branch of coefficient_translation (modules:6751-6780), translation_switch_order 3 */
+                dense_pair_apply(c, i, j, nrhs, ain, g, contran);
+                if (!c->store) pairop_free(&local);
+                continue;
             }
             for (int r = 0; r < nrhs; r++) {
                 coefficient_translation(noj, noi, ain + (size_t)neq * r + c->offset[j], g + (size_t)neq * r + c->offset[i], op, 0, contran[r]);

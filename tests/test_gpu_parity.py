@@ -294,3 +294,31 @@ def test_fft_translation_solve(api, oracle_mod):
         g.fft_setup(d_cell=4.0)
         rg = g.fixedorsoln(eps=1e-12)
         assert np.allclose(rg["qtot"], ro["qtot"], rtol=tol)
+
+
+def test_dense_pairs_below_switch_order(api, oracle_mod):
+    """Spheres of order 2 among order-4 spheres: their pairs use the dense
+    gentranmatrix records on the device; matvec (both product orientations)
+    and the FP64 / mixed solves against the oracle."""
+    rng = np.random.default_rng(3)
+    pos = []
+    while len(pos) < 12:
+        p = rng.uniform(-6, 6, 3)
+        if all(np.linalg.norm(p - q) > 2.2 for q in pos):
+            pos.append(p)
+    pos = np.array(pos)
+    rad = np.array([1.0] * 8 + [0.05] * 4)
+    ri = np.array([1.5 + 0.01j] * 8 + [1.6 + 0.1j] * 4)
+    g, o = _pair(api, oracle_mod, pos, rad, ri, 1e-6)
+    assert np.array_equal(g.sphere_order, o.order) and min(o.order) < 3
+    rng2 = np.random.default_rng(4)
+    x = rng2.standard_normal((g.number_eqns, 2)) + 1j * rng2.standard_normal((g.number_eqns, 2))
+    yg = g.sphereinteraction(x, con_tran=[0, 1])
+    yo = o.sphereinteraction(x, con_tran=[0, 1])
+    assert np.abs(yg - yo).max() <= 1e-12 * np.abs(yo).max()
+    ro = o.fixedorsoln(eps=1e-12)
+    rg = g.fixedorsoln(eps=1e-12)
+    assert rg["iterations"][1] == ro["maxiter"]
+    assert np.allclose(rg["qtot"], ro["qtot"], rtol=RTOL_FP64)
+    gm = api.SphereCluster(pos, rad, ri, mie_epsilon=1e-6, precision="mixed")
+    assert np.allclose(gm.fixedorsoln(eps=1e-12)["qtot"], o.fixedorsoln(eps=1e-16)["qtot"], rtol=RTOL_MIXED)

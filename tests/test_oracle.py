@@ -365,3 +365,26 @@ def test_warmstart_restatement_gradients_by_finite_differences():
             P[name][idx] += h
             fd = (lp - lm) / (2 * h)
             assert abs(fd - G[name][idx]) <= 1e-5 * (abs(fd) + abs(G[name][idx])) + 1e-10
+
+
+def _small_order_cluster():
+    rng = np.random.default_rng(3)
+    pos = []
+    while len(pos) < 12:
+        p = rng.uniform(-6, 6, 3)
+        if all(np.linalg.norm(p - q) > 2.2 for q in pos):
+            pos.append(p)
+    return np.array(pos), np.array([1.0] * 8 + [0.05] * 4), np.array([1.5 + 0.01j] * 8 + [1.6 + 0.1j] * 4)
+
+
+def test_dense_pairs_below_switch_order_match_direct_solver(oracle_mod):
+    """Pairs with an order below translation_switch_order (3) take the dense
+    gentranmatrix branch, transposed and shifted for the reverse direction; the
+    BiCG solution agrees with the dense LU solve, which builds every block
+    directly."""
+    pos, rad, ri = _small_order_cluster()
+    o = oracle_mod.Oracle(pos, rad, ri, mie_eps=1e-6)
+    assert min(o.order) < 3 <= max(o.order)
+    f = o.fixedorsoln(eps=1e-16)
+    d = o.fixedorsoln(eps=1e-16, direct=True)
+    assert np.allclose(f["qtot"], d["qtot"], rtol=1e-7)
