@@ -180,6 +180,7 @@ extern "C" void mstmg_default_opts(mstmg_opts* o)
     o->generic_kernel = 0;
     o->tile_ctas_per_sm = 0;
     o->fp32_chunk = 0;
+    o->mixed_solver = 0;
 }
 
 extern "C" const char* mstmg_last_error(void) { return g_err.c_str(); }
@@ -1036,6 +1037,148 @@ static int solve_mixed(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, int
     return MSTMG_OK;
 }
 
+// Mixed precision by residual replacement ("reliable updates"): one FP32
+// BiCG per system, never restarted.  Its iterate accumulates in FP32 and is
+// folded into the FP64 solution x whenever the recursive FP32 residual has
+// dropped by `drop` since the last true residual, or claims convergence; the
+// true residual b - (I - M H) x is then computed with the FP64 operators,
+// replaces the BiCG residual (FP32), and beta and the shadow product are
+// recomputed from it.  A system stops when its true residual meets eps, so the
+// answer carries the reference's criterion in FP64 while every Krylov step
+// runs in FP32.  Both polarisations advance in lockstep (4 FP32 columns per
+// pass).  x holds the initial guesses (FP64) on entry.
+static int solve_mixed_rr(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, int niter, int* iters, double* errs, int* status)
+{
+    const int ne = c->neqns, S = 2;
+    SlotMaps sm = c->sm();
+    int rc = ensure_ops(c, 0, false);
+    if (rc) return rc;
+    if ((rc = ensure_ops(c, 1, false))) return rc;
+    const zf* an32 = (const zf*)c->an32.p;
+    const double drop = 1.0e-5;   // replacement once the FP32 residual fell by this factor (squared norms)
+    double base[2] = {1.0, 1.0};  // true squared residual ratio at the last replacement
+    bool act[2] = {true, true};
+    int tot[2] = {0, 0};
+    c->outer = 0;
+    for (int s = 0; s < S; s++) status[s] = 0;
+    // true residual of the active systems in FP64, rounded into the FP32 BiCG residual
+    auto true_residual = [&](const bool* which, double* ratio) -> int {
+        int slots[2], a = 0;
+        for (int s = 0; s < S; s++)
+            if (which[s]) slots[a++] = s;
+        if (a == 0) return MSTMG_OK;
+        for (int k = 0; k < a; k++)
+            CK(cudaMemcpyAsync(c->X64.p + (size_t)k * ne, x[slots[k]], sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+        int r2 = translate<double>(c, c->X64.p, c->Y64.p, a, 0u);
+        if (r2) return r2;
+        for (int k = 0; k < a; k++) {
+            int s = slots[k];
+            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
+            launch_resid<double, float>(sm, c->an.p, b[s], x[s], c->Y64.p + (size_t)k * ne, v.r, c->part.p, c->small.p + 2 * s, c->nsm,
+                                        c->st);
+        }
+        CK(cudaMemcpyAsync(c->h_small, c->small.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        c->outer++;
+        for (int k = 0; k < a; k++) {
+            int s = slots[k];
+            double rr = c->h_small[2 * s], bb = c->h_small[2 * s + 1];
+            ratio[s] = bb > 0.0 ? rr / bb : 0.0;
+        }
+        return MSTMG_OK;
+    };
+    double ratio[2] = {0.0, 0.0};
+    if ((rc = true_residual(act, ratio))) return rc;
+    for (int s = 0; s < S; s++) {
+        base[s] = ratio[s];
+        errs[s] = ratio[s];
+        if (ratio[s] < eps) act[s] = false;
+    }
+    // FP32 BiCG start from the true residual: r = r_true, p = r, q = w = conj(r), x32 = 0
+    for (int s = 0; s < S; s++) {
+        if (!act[s]) continue;
+        BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
+        CK(cudaMemsetAsync(v.x, 0, sizeof(zf) * ne, c->st));
+        CK(cudaMemcpyAsync(c->rvec32.p + (size_t)s * ne, v.r, sizeof(zf) * ne, cudaMemcpyDeviceToDevice, c->st));
+        launch_init<float>(sm, an32, c->rvec32.p + (size_t)s * ne, v.x, nullptr, 0, v.r, v.p, v.w, v.q, c->part.p, c->sc.p + s, 1, c->nsm,
+                           c->st);
+    }
+    CK(cudaGetLastError());
+    for (int it = 1; it <= niter && (act[0] || act[1]); it++) {
+        int slots[2], a = 0;
+        for (int s = 0; s < S; s++)
+            if (act[s]) slots[a++] = s;
+        unsigned mask = 0;
+        for (int k = 0; k < a; k++) {
+            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, slots[k]);
+            CK(cudaMemcpyAsync(c->X32.p + (size_t)(2 * k) * ne, v.p, sizeof(zf) * ne, cudaMemcpyDeviceToDevice, c->st));
+            launch_mie<float>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, an32, -1, 1, v.w, c->X32.p + (size_t)(2 * k + 1) * ne,
+                              c->st);
+            mask |= 2u << (2 * k);
+        }
+        if ((rc = translate<float>(c, c->X32.p, c->Y32.p, 2 * a, mask))) return rc;
+        for (int k = 0; k < a; k++) {
+            int s = slots[k];
+            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
+            launch_post<float>(sm, an32, v.p, v.w, c->Y32.p + (size_t)(2 * k) * ne, c->Y32.p + (size_t)(2 * k + 1) * ne, v.cap, v.caw,
+                               c->part.p, c->sc.p + s, c->nsm, c->st);
+            launch_upd1_only<float>(ne, v.x, v.r, v.q, v.p, v.cap, v.caw, c->part.p, c->sc.p + s, c->nsm, c->st);
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->h_sc, c->sc.p, sizeof(BicgScalars) * S, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        bool repl[2] = {false, false};
+        for (int k = 0; k < a; k++) {
+            int s = slots[k];
+            tot[s] = it;
+            if (c->h_sc[s].breakdown) {
+                status[s] = 2;
+                act[s] = false;
+                continue;
+            }
+            double rec = c->h_sc[s].eerr * base[s];   // recursive residual relative to ||b||^2
+            if (rec < eps || c->h_sc[s].eerr < drop) repl[s] = true;
+        }
+        if (repl[0] || repl[1]) {
+            for (int s = 0; s < S; s++)
+                if (repl[s]) {
+                    BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
+                    launch_add_correction_f(ne, x[s], v.x, c->st);
+                    CK(cudaMemsetAsync(v.x, 0, sizeof(zf) * ne, c->st));
+                }
+            if ((rc = true_residual(repl, ratio))) return rc;
+            for (int s = 0; s < S; s++) {
+                if (!repl[s]) continue;
+                errs[s] = ratio[s];
+                base[s] = ratio[s];
+                if (ratio[s] < eps) {
+                    act[s] = false;
+                    continue;
+                }
+                BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
+                launch_rr_fix<float>(ne, v.q, v.r, c->part.p, c->sc.p + s, c->nsm, c->st);
+            }
+        }
+        for (int k = 0; k < a; k++) {
+            int s = slots[k];
+            if (!act[s]) continue;
+            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
+            launch_upd2_only<float>(ne, v.p, v.w, v.r, v.q, c->sc.p + s, c->nsm, c->st);
+        }
+        CK(cudaGetLastError());
+    }
+    for (int s = 0; s < S; s++) {
+        if (act[s]) {
+            // iteration cap: fold the last FP32 steps in
+            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
+            launch_add_correction_f(ne, x[s], v.x, c->st);
+            tot[s] = niter + 1;
+        }
+        iters[s] = tot[s];
+    }
+    return check_kernel_err(c);
+}
+
 static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, const double* x0, double fallback,
                                   int* used_guess, double* guess_res, double* amnp, double* qeff, double* qtot, double* maxerr, int* maxiter);
 
@@ -1113,7 +1256,7 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
         zd* bs[2] = {bvec, bvec + ne};
         if (xinit != c->amnp.p)
             for (int p = 0; p < 2; p++) CK(cudaMemcpyAsync(xs[p], bs[p], sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
-        rc = solve_mixed(c, bs, xs, eps, niter, it, er, st);
+        rc = c->opts.mixed_solver == 1 ? solve_mixed(c, bs, xs, eps, niter, it, er, st) : solve_mixed_rr(c, bs, xs, eps, niter, it, er, st);
         if (rc) return rc;
     } else {
         // the reference's order: polarisation 1 then 2, each from x0 = Mie*f
