@@ -290,12 +290,12 @@ def run_extras(args, dev, stream):
     # one T-matrix configuration of the ensemble
     pos, _ = C.rsa_sphere(100, 1.5, 0.20, seed=4)
     row = {"workload": "100 spheres, x=1.5, m=1.6+0.005i, RSA in a sphere at fv 0.20: cluster T matrix, "
-                       "all 2Lc(Lc+2) columns, solution_eps 1e-6, t_matrix_convergence 1e-6",
+                       "all 2Lc(Lc+2) columns to residual 1e-6 (solution_eps 1e-12), t_matrix_convergence 1e-6",
            "metric": "T matrices/s"}
     for prec in ("mixed", "fp64"):
         g = cluster(pos, 1.5, 1.6 + 0.005j, prec)
         T = g.t_matrix_order()
-        ms, r = timed(lambda: g.tmatrix_solution(T, solution_eps=1e-6, convergence_eps=1e-6), 1)
+        ms, r = timed(lambda: g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6), 1)
         row[prec] = {"tmatrices_per_s": round(1000.0 / ms, 4), "ms": round(ms, 1), "order": r["order"], "t_matrix_order": T,
                      "columns": 2 * r["order"] * (r["order"] + 2), "qext": r["qtot"][0], "maxiter": r["maxiter"]}
         g.close()
@@ -320,9 +320,9 @@ def run_extras(args, dev, stream):
     # batched ensemble of T matrices (uneven sizes), concurrent and autotuned, against one at a time
     from mstm_b200 import ensemble as EN
     cfgs = EN.ensemble_configs(6, seed=4, nmin=50, nmax=150)
-    seq = EN.solve_ensemble(cfgs, precision="mixed", workers=1)
+    seq = EN.solve_ensemble(cfgs, precision="mixed", workers=1, solution_eps=1e-12)
     tuner = EN.Autotuner(reps=2)
-    bat = EN.solve_ensemble(cfgs, precision="mixed", workers=4, tuner=tuner)
+    bat = EN.solve_ensemble(cfgs, precision="mixed", workers=4, tuner=tuner, solution_eps=1e-12)
     out["ensemble_tmatrix"] = {
         "workload": "6 configurations, 50-150 spheres (seeded), x=1.5, m=1.6+0.005i, RSA at fv 0.20: cluster T matrices, "
                     "orientation-averaged Qext/Qsca and scattering matrix, ensemble means",
