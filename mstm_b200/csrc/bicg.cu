@@ -206,6 +206,13 @@ __global__ void __launch_bounds__(RB) rr_dot_kernel(int n, const cpx<T>* q, cons
     }
     block_reduce_store<3>(acc, part + 3 * blockIdx.x);
 }
+__global__ void sum3_last_kernel(int nparts, const double* part, double* out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0.0;
+    for (int b = 0; b < nparts; b++) s += part[3 * b + 2];
+    out[0] = s;
+}
 __global__ void rr_fin_kernel(int nparts, const double* part, BicgScalars* sc)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -352,6 +359,14 @@ template <typename T> void launch_rr_fix(int n, const cpx<T>* q, const cpx<T>* r
     int g = grid_for(n, nsm);
     rr_dot_kernel<T><<<g, RB, 0, st>>>(n, q, r, part);
     rr_fin_kernel<<<1, 32, 0, st>>>(g, part, sc);
+    launch_counter() += 2;
+}
+// out[0] = sum |v|^2 (one block-reduction pass and a fixed-order finish)
+void launch_rr_dot_norm(int n, const zd* v, double* part, double* out, int nsm, cudaStream_t st)
+{
+    int g = grid_for(n, nsm);
+    rr_dot_kernel<double><<<g, RB, 0, st>>>(n, v, v, part);
+    sum3_last_kernel<<<1, 32, 0, st>>>(g, part, out);
     launch_counter() += 2;
 }
 template void launch_rr_fix<float>(int, const zf*, const zf*, double*, BicgScalars*, int, cudaStream_t);

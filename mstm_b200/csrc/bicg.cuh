@@ -41,5 +41,6 @@ template <typename T> void launch_upd2_only(int n, cpx<T>* p, cpx<T>* w, const c
 // csk = sum conj(q) r, beta = csk / csk_prev, enorm = sum |r|^2 (the new base).
 template <typename T> void launch_rr_fix(int n, const cpx<T>* q, const cpx<T>* r, double* part, BicgScalars* sc, int nsm, cudaStream_t st);
 void launch_add_correction_d(int n, zd* x, const zd* d, cudaStream_t st);
+void launch_rr_dot_norm(int n, const zd* v, double* part, double* out, int nsm, cudaStream_t st);   // out[0] = sum |v|^2
 template <typename T> void launch_conj_copy(int n, const cpx<T>* a, cpx<T>* b, cudaStream_t st);
 void launch_d2f(int n, const zd* a, zf* b, cudaStream_t st);

@@ -918,6 +918,42 @@ template <typename T> static BicgVecs<T> vecs_at(cpx<T>* base, int ne, int s)
     return v;
 }
 
+// cbicg with niter < 0: the order-of-scattering iteration (mstm-solver-8.f90:787-822),
+// x += M H p, p = M H p, until ||M H p||^2 / ||b||^2 < eps or -niter steps.
+// *err keeps the reference's value: the error at the exit, 0 when the count ran out.
+static int oos_solve(mstmg_ctx* c, const zd* b, zd* x, int niter, double eps, int* iter, double* err)
+{
+    const int ne = c->neqns;
+    SlotMaps sm = c->sm();
+    zd* cp = c->X64.p + 2 * (size_t)ne;
+    zd* cr = c->Y64.p + 2 * (size_t)ne;
+    launch_rr_dot_norm(ne, b, c->part.p, c->small.p, c->nsm, c->st);
+    CK(cudaMemcpyAsync(c->h_small, c->small.p, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double enorm = c->h_small[0];
+    CK(cudaMemcpyAsync(cp, x, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+    int it;
+    double emax = 0.0;
+    for (it = 1; it <= -niter; it++) {
+        int rc = translate<double>(c, cp, c->Y64.p, 1, 0u);
+        if (rc) return rc;
+        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, 1, 0, c->Y64.p, cr, c->st);
+        launch_add_correction_d(ne, x, cr, c->st);
+        CK(cudaMemcpyAsync(cp, cr, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+        launch_rr_dot_norm(ne, cr, c->part.p, c->small.p, c->nsm, c->st);
+        CK(cudaMemcpyAsync(c->h_small, c->small.p, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        double eerr = enorm > 0.0 ? c->h_small[0] / enorm : 0.0;
+        if (eerr < eps) {
+            emax = eerr;
+            break;
+        }
+    }
+    *iter = it;
+    *err = emax;
+    return check_kernel_err(c);
+}
+
 extern "C" int mstmg_bicg(mstmg_ctx* c, int niter, double eps, const double* pnp, double* anp, int initialize, int* iter, double* err)
 {
     if (!c || !pnp || !anp) return MSTMG_ERR_ARG;
@@ -930,11 +966,12 @@ extern "C" int mstmg_bicg(mstmg_ctx* c, int niter, double eps, const double* pnp
     const zd* bb[1] = {c->bvec64.p};
     int it = 0, st = 0;
     double e = 0.0;
-    if (niter <= 0) {
-        set_err("mstmg_bicg: niter must be positive (MSTM's niter<=0 modes are not on this path)");
+    if (niter == 0) {
+        set_err("mstmg_bicg: niter = 0 (the reference's Mie-multiply-only mode) is not on this path");
         return MSTMG_ERR_UNSUPPORTED;
     }
-    rc = bicg_batched<double>(c, 1, bb, &v, true, niter, &eps, &it, &e, &st);
+    if (niter < 0) rc = oos_solve(c, c->bvec64.p, v.x, niter, eps, &it, &e);
+    else rc = bicg_batched<double>(c, 1, bb, &v, true, niter, &eps, &it, &e, &st);
     if (rc) return rc;
     CK(copy_out(anp, v.x, sizeof(zd) * ne, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -1247,7 +1284,14 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
         CK(cudaMemcpyAsync(c->amnp.p, g, sizeof(zd) * 2 * (size_t)ne, cudaMemcpyDeviceToDevice, c->st));
         xinit = c->amnp.p;
     }
-    if (niter == 0) {
+    if (niter < 0) {
+        for (int p = 0; p < 2; p++) {
+            if (xinit != c->amnp.p)
+                CK(cudaMemcpyAsync(c->amnp.p + (size_t)p * ne, xinit + (size_t)p * ne, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+            rc = oos_solve(c, bvec + (size_t)p * ne, c->amnp.p + (size_t)p * ne, niter, eps, &it[p], &er[p]);
+            if (rc) return rc;
+        }
+    } else if (niter == 0) {
         if (xinit != c->amnp.p)
             for (int p = 0; p < 2; p++)
                 CK(cudaMemcpyAsync(c->amnp.p + (size_t)p * ne, bvec + (size_t)p * ne, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));

@@ -1474,6 +1474,20 @@ int orc_cbicg(orc_ctx *c, int niter, double eps, const cplx *pnp, cplx *anp, int
     double enorm = creal(dotc(pnp, pnp, neq));   /* normalize_solution_error = T */
     double errmin = 1.0e10, errmax = 0.0;
     int one0 = 0, rc = 0, iter;
+    if (niter < 0) {
+        /* order-of-scattering iteration (solver:787-822): x += M H p, p = M H p */
+        memcpy(cp, anp, sizeof(cplx) * neq);
+        for (iter = 1; iter <= -niter; iter++) {
+            orc_sphereinteraction(c, 1, cp, cr, &one0, NULL, iter == 1 ? initialize : 0);
+            for (int k = 0; k < neq; k++) { anp[k] += cr[k]; cp[k] = cr[k]; }
+            double eerr = creal(dotc(cr, cr, neq)) / enorm;
+            if (eerr < eps) { errmax = eerr; break; }
+        }
+        *iter_o = iter;
+        *err_o = errmax;
+        free(cr); free(cp); free(cw); free(cq); free(cap); free(caw); free(ctin); free(ctout);
+        return 0;
+    }
     orc_sphereinteraction(c, 1, anp, cr, &one0, NULL, initialize);
     for (int k = 0; k < neq; k++) cr[k] = pnp[k] - anp[k] + cr[k];
     for (int k = 0; k < neq; k++) { cq[k] = conj(cr[k]); cw[k] = cq[k]; cp[k] = cr[k]; }

@@ -322,3 +322,14 @@ def test_dense_pairs_below_switch_order(api, oracle_mod):
     assert np.allclose(rg["qtot"], ro["qtot"], rtol=RTOL_FP64)
     gm = api.SphereCluster(pos, rad, ri, mie_epsilon=1e-6, precision="mixed")
     assert np.allclose(gm.fixedorsoln(eps=1e-12)["qtot"], o.fixedorsoln(eps=1e-16)["qtot"], rtol=RTOL_MIXED)
+
+
+def test_order_of_scattering_mode(api, oracle_mod):
+    """cbicg's niter < 0 mode (order-of-scattering iteration) on the device:
+    same iteration count and solution as the oracle."""
+    pos, rad, ri, em = _cluster("cluster20")
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em)
+    fo = o.fixedorsoln(eps=1e-10, niter=-100)
+    fg = g.fixedorsoln(eps=1e-10, niter=-100)
+    assert fg["iterations"][1] == fo["maxiter"]
+    assert np.allclose(fg["qtot"], fo["qtot"], rtol=RTOL_FP64)

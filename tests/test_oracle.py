@@ -388,3 +388,14 @@ def test_dense_pairs_below_switch_order_match_direct_solver(oracle_mod):
     f = o.fixedorsoln(eps=1e-16)
     d = o.fixedorsoln(eps=1e-16, direct=True)
     assert np.allclose(f["qtot"], d["qtot"], rtol=1e-7)
+
+
+def test_order_of_scattering_mode_converges_to_bicg_solution(oracle_mod):
+    """cbicg with niter < 0 runs the order-of-scattering iteration; for a dilute
+    cluster it converges to the BiCG solution."""
+    w = C.workload("cluster8")
+    o = oracle_mod.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-w["order"])
+    f_b = o.fixedorsoln(eps=1e-14)
+    f_o = o.fixedorsoln(eps=1e-14, niter=-200)
+    assert f_o["maxiter"] < 200 and f_o["maxerr"] < 1e-14
+    assert np.allclose(f_o["qtot"], f_b["qtot"], rtol=1e-7)
