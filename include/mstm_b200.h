@@ -119,6 +119,21 @@ int mstmg_fixed_orientation(mstmg_ctx *ctx, double alpha, double sinc, int dir, 
 int mstmg_scattering(mstmg_ctx *ctx, const double *amnp, double trans_eps, int max_t_order, int nangles, double *smat, double *g,
                      int *t_matrix_order, double *amnp0, int amnp0_cap);
 
+/* The scattering matrix of the common-origin expansion at single directions,
+ * without azimuthal averaging (azimuthal_average = .false., the reference's
+ * default for fixed orientation): scatteringmatrix
+ * (mstm-scatprops-26.f90:1498-1573) with normalize_s11 = .false., at the
+ * directions of scattering_matrix_calculation (mstm-input-37.f90:3038-3061):
+ * i = ldim..udim, theta_i = amin + (amax - amin)(i - ldim)/(udim - ldim)
+ * degrees, azimuth alpha + pi for i < 0 and alpha otherwise (the reference
+ * takes udim = floor(180.00001/scattering_map_increment), ldim = -udim,
+ * amin = -180, amax = 180).
+ *   amnp0: 2T(T+2) x 2 TE/TM coefficients (mstmg_scattering's amnp0 output),
+ *   T = t_matrix_order <= 200; sm: 16 x (udim - ldim + 1), Fortran sm(4,4)
+ *   per direction, divided by the medium's real index as the reference does. */
+int mstmg_scattering_plane(mstmg_ctx *ctx, int t_matrix_order, const double *amnp0, int ldim, int udim, double amin, double amax,
+                           double alpha, int rotate_plane, double *sm);
+
 /* Order of the cluster T matrix about the cluster origin (the mean sphere
  * position): replaces the t_matrix_order set-up of main_calling_program
  * (mstm-input-37.f90:1179-1197), tranordertest (mstm-modules-33.f90:1896-1942)

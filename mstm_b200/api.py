@@ -146,13 +146,41 @@ class SphereCluster:
 
     def scattering(self, amnp, trans_eps=1.0e-5, max_t_order=100, nangles=181):
         """Azimuth-averaged scattering matrix (nangles, 4, 4), asymmetry parameter
-        g and t_matrix_order of a fixed-orientation solution amnp (neqns, 2)."""
+        g, t_matrix_order and the common-origin expansion amnp0 (2T(T+2), 2;
+        TE/TM) of a fixed-orientation solution amnp (neqns, 2)."""
         amnp = np.asfortranarray(amnp, np.complex128)
         smat = np.zeros(16 * nangles)
         g, tmo = c_double(0.0), c_int(0)
+        tcap = max(max_t_order, int(self.sphere_order.max()))
+        cap = 2 * tcap * (tcap + 2)
+        a0 = np.zeros((cap, 2), np.complex128, order="F")
         check(self._L.mstmg_scattering(self.ctx, _ptr(amnp), trans_eps, max_t_order, nangles, _ptr(smat), ctypes.byref(g),
-                                       ctypes.byref(tmo), None, 0), "scattering")
-        return dict(smat=smat.reshape(nangles, 4, 4).transpose(0, 2, 1).copy(), g=g.value, t_matrix_order=tmo.value)
+                                       ctypes.byref(tmo), _ptr(a0), cap), "scattering")
+        T = tmo.value
+        nb0 = 2 * T * (T + 2)
+        amnp0 = np.asfortranarray(a0.reshape(-1, order="F")[:2 * nb0].reshape(nb0, 2, order="F"))
+        return dict(smat=smat.reshape(nangles, 4, 4).transpose(0, 2, 1).copy(), g=g.value, t_matrix_order=T, amnp0=amnp0)
+
+    def scattering_plane(self, amnp0, t_matrix_order, increment=1.0, alpha=0.0, rotate_plane=False):
+        """Scattering matrix without azimuthal averaging (scatteringmatrix,
+        mstm-scatprops-26.f90:1498-1573, normalize_s11 false) at the directions
+        scattering_matrix_calculation uses when azimuthal_average is false:
+        theta = -180..180 degrees in steps of 180/udim, udim =
+        floor(180.00001/increment), in the plane of azimuth alpha (theta < 0
+        on the far side).  Returns (theta (2udim+1,), smat (2udim+1, 4, 4))."""
+        T = int(t_matrix_order)
+        udim = int(np.floor(180.00001 / increment))
+        ldim, amax = -udim, 180.0
+        amin = -amax
+        a0 = np.asfortranarray(amnp0, np.complex128)
+        if a0.shape != (2 * T * (T + 2), 2):
+            raise ValueError(f"amnp0 must be ({2 * T * (T + 2)}, 2), got {a0.shape}")
+        n = udim - ldim + 1
+        sm = np.zeros(16 * n)
+        check(self._L.mstmg_scattering_plane(self.ctx, T, _ptr(a0), ldim, udim, amin, amax, alpha, int(bool(rotate_plane)),
+                                             _ptr(sm)), "scattering_plane")
+        theta = np.array([amin + (i - ldim) / (udim - ldim) * (amax - amin) for i in range(ldim, udim + 1)])
+        return theta, sm.reshape(n, 4, 4).transpose(0, 2, 1).copy()
 
     def fft_setup(self, cell_volume_fraction=0.2, d_cell=0.0, node_order=-1, neighbor_node_model=2):
         """Use MSTM's FFT translation (fft_translation_option): near pairs direct,

@@ -1574,6 +1574,52 @@ extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_e
     return check_kernel_err(c);
 }
 
+extern "C" int mstmg_scattering_plane(mstmg_ctx* c, int t_matrix_order, const double* amnp0, int ldim, int udim, double amin, double amax,
+                                      double alpha, int rotate_plane, double* sm)
+{
+    const int T = t_matrix_order;
+    if (!c || !amnp0 || !sm || T < 1 || udim <= ldim) {
+        set_err("mstmg_scattering_plane: bad arguments");
+        return MSTMG_ERR_ARG;
+    }
+    if (T > PS_TMAX) {
+        set_err("mstmg_scattering_plane: t_matrix_order above 200 is not supported");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    mstmg::Tables& big = big_tables();
+    std::vector<double> bd(T + 1);
+    for (int k = 0; k <= T; k++) bd[k] = big.bc(k, k);
+    const size_t nb0 = 2 * (size_t)T * (T + 2);
+    const int nang = udim - ldim + 1;
+    DevBuf<double> dfnr, dbd, dsm;
+    DevBuf<zd> da0;
+    CK(dfnr.alloc(2 * T + 2));
+    CK(dbd.alloc(T + 1));
+    CK(da0.alloc(2 * nb0));
+    CK(dsm.alloc(16 * (size_t)nang));
+    CK(cudaMemcpyAsync(dfnr.p, big.fnr.data(), sizeof(double) * (2 * T + 2), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dbd.p, bd.data(), sizeof(double) * (T + 1), cudaMemcpyHostToDevice, c->st));
+    CK(copy_in(da0.p, amnp0, sizeof(zd) * 2 * nb0, c->st));
+    PlaneSmArgs a;
+    a.T = T;
+    a.a0 = da0.p;
+    a.ldim = ldim;
+    a.udim = udim;
+    a.amin = amin;
+    a.amax = amax;
+    a.alpha = alpha;
+    a.rotate = rotate_plane ? 1 : 0;
+    a.rimed_re = c->opts.medium_re;
+    a.fnr = dfnr.p;
+    a.bcofd = dbd.p;
+    a.smat = dsm.p;
+    launch_planesm(a, c->st);
+    CK(cudaGetLastError());
+    CK(copy_out(sm, dsm.p, sizeof(double) * 16 * (size_t)nang, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return check_kernel_err(c);
+}
+
 // ---- many systems at once ----
 
 template <typename T> struct MultiWork {

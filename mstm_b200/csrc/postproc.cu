@@ -8,7 +8,9 @@
 //     (distribute_from_common_origin, mstm-scatprops-26.f90:561-669);
 //   * GSF expansion of the azimuth-averaged scattering matrix
 //     (fosmexpansion, mstm-scatprops-26.f90:1820-1951);
-//   * its evaluation at polar angles (fosmcalc, mstm-scatprops-26.f90:1750-1810).
+//   * its evaluation at polar angles (fosmcalc, mstm-scatprops-26.f90:1750-1810);
+//   * the scattering matrix at single directions without azimuthal averaging
+//     (scatteringmatrix, mstm-scatprops-26.f90:1498-1573).
 // Orders reach t_matrix_order (up to 100), so the per-sphere translation keeps
 // its Wigner-d rows, Bessel values and axial blocks in global scratch.
 #include "common.cuh"
@@ -569,6 +571,153 @@ __global__ void fosmcalc_kernel(int ntot, int nang, const double* s00, const dou
 #undef DCR
 }
 
+// scatteringmatrix (scatprops:1498-1573) with normalize_s11 = .false. at the
+// directions of scattering_matrix_calculation (input:3038-3061): one CTA per
+// direction.  rotcoef(ct, 1, T) advances degree by degree in shared memory;
+// per degree the threads take the orders m = -n..n, form the two tau
+// functions of taufunc (modules:1324-1344) and add their terms to the four
+// amplitude sums, which are reduced over the CTA at the end; thread 0 forms
+// the 4x4 matrix (amplitude_to_scattering_matrix, scatprops:1410-1436).
+#define PS_NT 128
+__global__ void __launch_bounds__(PS_NT) planesm_kernel(PlaneSmArgs a)
+{
+    const int ia = blockIdx.x;
+    const int i = a.ldim + ia;
+    if (i > a.udim) return;
+    const int T = a.T;
+    __shared__ double dk0s[2 * PS_TMAX + 3], dk01s[2 * PS_TMAX + 3], dcs[3 * (2 * PS_TMAX + 1)];
+    __shared__ double red[8][PS_NT / 32];
+    double* dk0 = dk0s + (T + 1);
+    double* dk01 = dk01s + (T + 1);
+    const int W = 2 * T + 1;
+#define DCR(m, k) dcs[((m) + 1) * W + ((k) + T)]
+    double ct = cos(MSTMG_REF_PI / 180.0 * (a.amin + (a.amax - a.amin) * (double)(i - a.ldim) / (double)(a.udim - a.ldim)));
+    if (ct == 1.0) ct = 0.9999999;
+    if (ct == -1.0) ct = -0.9999999;
+    const double phi = (i < 0) ? a.alpha + MSTMG_REF_PI : a.alpha;
+    double cphi, sphi;
+    sincos(phi, &sphi, &cphi);
+    const double* fnr = a.fnr;
+    double sbe = (fabs(ct) >= 1.0) ? 0.0 : sqrt(fabs((1.0 + ct) * (1.0 - ct)));
+    double cbe2 = 0.5 * (1.0 + ct), sbe2 = 0.5 * (1.0 - ct);
+    for (int k = threadIdx.x; k < 2 * T + 3; k += blockDim.x) { dk0s[k] = 0.0; dk01s[k] = 0.0; }
+    __syncthreads();
+    if (threadIdx.x == 0) dk0[0] = 1.0;
+    __syncthreads();
+    zd sa[4];
+    for (int e = 0; e < 4; e++) sa[e] = mk(0.0, 0.0);
+    const size_t ld = 2 * (size_t)T * (T + 2);
+    int sgn = 1;
+    double sben = 1.0;
+    for (int n = 1; n <= T; n++) {
+        sgn = -sgn;
+        sben = sben * sbe / 2.0;
+        if (sben < 1.0e-30) sben = 0.0;
+        double newv[(2 * PS_TMAX + PS_NT - 1) / PS_NT];
+        int cnt = 0;
+        for (int k = -n + 1 + (int)threadIdx.x; k <= n - 1; k += blockDim.x)
+            newv[cnt++] = (ct * (double)(n + n - 1) * dk0[k] - fnr[n - k - 1] * fnr[n + k - 1] * dk01[k]) / (fnr[n + k] * fnr[n - k]);
+        __syncthreads();
+        cnt = 0;
+        for (int k = -n + 1 + (int)threadIdx.x; k <= n - 1; k += blockDim.x) {
+            dk01[k] = dk0[k];
+            dk0[k] = newv[cnt++];
+        }
+        if (threadIdx.x == 0) {
+            dk0[n] = sgn * sben * a.bcofd[n];
+            dk0[-n] = sgn * dk0[n];
+            dk01[n] = 0.0;
+            dk01[-n] = 0.0;
+        }
+        __syncthreads();
+        for (int k = -n + (int)threadIdx.x; k <= n; k += blockDim.x) DCR(0, k) = dk0[k];
+        __syncthreads();
+        {
+            const double fmn = 1.0 / fnr[n] / fnr[n + 1];
+            for (int k = -n + (int)threadIdx.x; k <= n; k += blockDim.x) {
+                double dkm1 = (k == -n) ? 0.0 : DCR(0, k - 1);
+                double dkn1 = (k == n) ? 0.0 : DCR(0, k + 1);
+                double v = (fnr[n + k] * fnr[n - k + 1] * cbe2 * dkm1 - fnr[n - k] * fnr[n + k + 1] * sbe2 * dkn1 -
+                            (double)k * sbe * DCR(0, k)) * fmn;
+                DCR(1, k) = v;
+                DCR(-1, -k) = -v * pm1(k);
+            }
+        }
+        __syncthreads();
+        // (-i)^n
+        const zd cin = (n & 3) == 0 ? mk(1.0, 0.0) : (n & 3) == 1 ? mk(0.0, -1.0) : (n & 3) == 2 ? mk(-1.0, 0.0) : mk(0.0, 1.0);
+        const double fnm = sqrt((double)(n + n + 1) / 2.0) / 4.0;
+        for (int m = -n + (int)threadIdx.x; m <= n; m += blockDim.x) {
+            const double tau[2] = {-fnm * (-DCR(-1, m) + DCR(1, m)), -fnm * (DCR(-1, m) + DCR(1, m))};
+            const int m1 = (m <= -1) ? n + 1 : m, n1 = (m <= -1) ? -m : n;
+            double sm_, cm_;
+            sincos((double)m * phi, &sm_, &cm_);
+            const zd ce = cin * mk(cm_, sm_);
+            for (int p = 0; p < 2; p++) {
+                const size_t ix = (size_t)aidx(m1, n1, p, T);
+                const zd a1 = a.a0[ix], a2 = a.a0[ix + ld];
+                zd av, bv;
+                if (a.rotate) {
+                    av = cphi * a1 + sphi * a2;
+                    bv = sphi * a1 - cphi * a2;
+                } else {
+                    av = a1;
+                    bv = -a2;
+                }
+                const zd tb = ce * bv, ta = ce * av;
+                sa[0] = sa[0] + tau[1 - p] * tb;
+                sa[1] = sa[1] + tau[p] * imul(ta);
+                sa[2] = sa[2] + tau[p] * imul(tb);
+                sa[3] = sa[3] + tau[1 - p] * ta;
+            }
+        }
+        __syncthreads();
+    }
+#undef DCR
+    // CTA reduction of the 8 doubles
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double v8[8] = {sa[0].x, sa[0].y, sa[1].x, sa[1].y, sa[2].x, sa[2].y, sa[3].x, sa[3].y};
+    for (int e = 0; e < 8; e++) {
+        double v = v8[e];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[e][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        zd s[4];
+        for (int e = 0; e < 4; e++) {
+            double re = 0.0, im = 0.0;
+            for (int w = 0; w < PS_NT / 32; w++) { re += red[2 * e][w]; im += red[2 * e + 1][w]; }
+            s[e] = (4.0 / sqrt(2.0 * (1.0 / MSTMG_REF_PI))) * mk(re, im);
+        }
+        zd sp[4][4];
+        for (int r = 0; r < 4; r++)
+            for (int q = 0; q < 4; q++) sp[r][q] = s[r] * cj(s[q]);
+        double sm[16];
+#define SP(r, q) sp[(r) - 1][(q) - 1]
+#define SM(r, q) sm[((r) - 1) + 4 * ((q) - 1)]
+        SM(1, 1) = (SP(1, 1) + SP(2, 2) + SP(3, 3) + SP(4, 4)).x;
+        SM(1, 2) = (-SP(1, 1) + SP(2, 2) - SP(3, 3) + SP(4, 4)).x;
+        SM(2, 1) = (-SP(1, 1) + SP(2, 2) + SP(3, 3) - SP(4, 4)).x;
+        SM(2, 2) = (SP(1, 1) + SP(2, 2) - SP(3, 3) - SP(4, 4)).x;
+        SM(3, 3) = 2.0 * (SP(1, 2) + SP(3, 4)).x;
+        SM(3, 4) = 2.0 * (SP(2, 1) + SP(4, 3)).y;
+        SM(4, 3) = 2.0 * (SP(1, 2) - SP(3, 4)).y;
+        SM(4, 4) = 2.0 * (SP(1, 2) - SP(3, 4)).x;
+        SM(1, 3) = 2.0 * (SP(2, 3) + SP(1, 4)).x;
+        SM(3, 1) = 2.0 * (SP(2, 4) + SP(1, 3)).x;
+        SM(1, 4) = -2.0 * (SP(2, 3) - SP(1, 4)).y;
+        SM(4, 1) = -2.0 * (SP(4, 2) + SP(1, 3)).y;
+        SM(2, 3) = -2.0 * (SP(2, 3) - SP(1, 4)).x;
+        SM(3, 2) = -2.0 * (SP(2, 4) - SP(1, 3)).x;
+        SM(2, 4) = -2.0 * (SP(2, 3) + SP(1, 4)).y;
+        SM(4, 2) = -2.0 * (SP(4, 2) - SP(1, 3)).y;
+#undef SP
+#undef SM
+        for (int e = 0; e < 16; e++) a.smat[(size_t)ia * 16 + e] = sm[e] / (4.0 * MSTMG_REF_PI) / a.rimed_re;
+    }
+}
+
 void launch_tranorder(int nsph, const double* pos, const int* order, const double* origin, double rire, double eps, int maxt,
                       const double* bcof, const double* fnr, int nbc, zd* scratch, int sstride, int* tord, cudaStream_t st)
 {
@@ -612,5 +761,11 @@ void launch_fosmcalc(int ntot, int nang, const double* s00, const double* s02, c
                      const double* fnr, const double* bcofd, double* dscr, double* smat, cudaStream_t st)
 {
     fosmcalc_kernel<<<nang, 128, 0, st>>>(ntot, nang, s00, s02, sp22, sm22, fnr, bcofd, dscr, smat);
+    launch_counter() += 1;
+}
+
+void launch_planesm(const PlaneSmArgs& a, cudaStream_t st)
+{
+    planesm_kernel<<<a.udim - a.ldim + 1, PS_NT, 0, st>>>(a);
     launch_counter() += 1;
 }

@@ -47,3 +47,19 @@ void launch_fosm(int ntot, const zd* a0, const double* bcof, const double* fnr, 
                  double* sm22, double* vscr, cudaStream_t st);
 void launch_fosmcalc(int ntot, int nang, const double* s00, const double* s02, const double* sp22, const double* sm22,
                      const double* fnr, const double* bcofd, double* dscr, double* smat, cudaStream_t st);
+
+// scatteringmatrix at the directions i = ldim..udim of scattering_matrix_calculation
+#define PS_TMAX 200
+struct PlaneSmArgs {
+    int T;                  // order of the origin expansion (<= PS_TMAX)
+    const zd* a0;           // 2T(T+2) x 2, TE/TM basis
+    int ldim, udim;         // udim > ldim
+    double amin, amax;      // degrees
+    double alpha;           // incident azimuth (radians)
+    int rotate;             // rotate_plane
+    double rimed_re;
+    const double* fnr;      // sqrt table, indices 0..2T+1
+    const double* bcofd;    // bcof(n, n), n = 0..T
+    double* smat;           // 16 x (udim - ldim + 1)
+};
+void launch_planesm(const PlaneSmArgs& a, cudaStream_t st);

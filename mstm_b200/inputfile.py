@@ -53,6 +53,7 @@ OPTIONS = {
     "incident_alpha_deg": ("r", 0.0),
     "calculate_scattering_matrix": ("l", True),
     "azimuthal_average": ("l", False),
+    "scattering_map_increment": ("r", 1.0),
     "store_translation_matrix": ("l", True),
     "solution_method": ("a", "iterative"),
     "t_matrix_output_file": ("a", ""),
@@ -67,6 +68,10 @@ RESTRICTED = {
     "random_configuration_host": ("l", False),
     "configuration_average": ("l", False),
     "incidence_average": ("l", False),
+    "incident_frame": ("l", False),
+    "scattering_map_model": ("i", 0),
+    "single_origin_expansion": ("l", True),
+    "numerical_azimuthal_average": ("l", False),
 }
 
 
@@ -231,10 +236,16 @@ def incidence(run, medium):
     return run["incident_alpha_deg"] * REF_PI / 180.0, sinc, direction
 
 
-def execute(run, precision="fp64", nangles=181):
-    """Run one deck entry on the GPU; returns a dict of results."""
+def execute(run, precision="fp64"):
+    """Run one deck entry on the GPU; returns a dict of results.  The
+    scattering-matrix directions follow main_calling_program
+    (input:1300-1363): udim = floor(180.00001/scattering_map_increment) steps
+    over 0..180 degrees for random orientation and for the azimuth-averaged
+    fixed-orientation matrix, -180..180 in the plane of incidence otherwise."""
     from . import api
     check_supported(run)
+    udim = int(math.floor(180.00001 / run["scattering_map_increment"]))
+    nangles = udim + 1
     pos, rad, ri = cluster_arrays(run)
     med = medium_index(run)
     g = api.SphereCluster(pos, rad, ri, mie_epsilon=run["mie_epsilon"], precision=precision, medium_index=med)
@@ -258,7 +269,7 @@ def execute(run, precision="fp64", nangles=181):
                 write_tmatrix_file(run["t_matrix_output_file"], r["tmat"], T, u)
             if run["calculate_scattering_matrix"]:
                 ro = g.ranorientscatmatrix(tm, u, nangles=nangles)
-                out.update(smat=ro["smat"], sm_coef=ro["sm"], coherent_ratio=ro["coherent"],
+                out.update(theta=np.linspace(0.0, 180.0, nangles), smat=ro["smat"], sm_coef=ro["sm"], coherent_ratio=ro["coherent"],
                            g_asym=ro["sm"][1, 0, 0] / (3.0 * ro["sm"][0, 0, 0]))
         else:
             alpha, sinc, direction = incidence(run, med)
@@ -268,7 +279,13 @@ def execute(run, precision="fp64", nangles=181):
             if run["calculate_scattering_matrix"]:
                 sc = g.scattering(r["amnp"], trans_eps=run["translation_epsilon"], max_t_order=run["max_t_matrix_order"],
                                   nangles=nangles)
-                out.update(smat=sc["smat"], g_asym=sc["g"], t_matrix_order=sc["t_matrix_order"])
+                out.update(g_asym=sc["g"], t_matrix_order=sc["t_matrix_order"])
+                if run["azimuthal_average"]:
+                    out.update(theta=np.linspace(0.0, 180.0, nangles), smat=sc["smat"])
+                else:
+                    theta, sm = g.scattering_plane(sc["amnp0"], sc["t_matrix_order"], increment=run["scattering_map_increment"],
+                                                   alpha=alpha)
+                    out.update(theta=theta, smat=sm, amnp0=sc["amnp0"])
     finally:
         g.close()
     return out
@@ -293,11 +310,10 @@ def report(out):
     if "smat" in out:
         L.append(f"asymmetry parameter {out['g_asym']:.8f}")
         L.append("scattering matrix (theta, S11, S12, S33, S34):")
-        sm = out["smat"]
+        sm, theta = out["smat"], out["theta"]
         n = sm.shape[0]
         for i in range(0, n, max(1, (n - 1) // 18)):
-            th = 180.0 * i / (n - 1)
-            L.append(f"  {th:7.2f} {sm[i, 0, 0]:.6e} {sm[i, 0, 1]:.6e} {sm[i, 2, 2]:.6e} {sm[i, 2, 3]:.6e}")
+            L.append(f"  {theta[i]:7.2f} {sm[i, 0, 0]:.6e} {sm[i, 0, 1]:.6e} {sm[i, 2, 2]:.6e} {sm[i, 2, 3]:.6e}")
     return "\n".join(L)
 
 

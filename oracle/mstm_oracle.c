@@ -2527,3 +2527,102 @@ void orc_fosmcalc(int ntot, const double *s00, const double *s02, const double *
 #undef SM
     free(dc);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Scattering matrix at one direction from the common-origin expansion,     */
+/* not azimuth-averaged: scatteringmatrix (scatprops:1498-1573) with        */
+/* normalize_s11 = .false., its tau functions (taufunc, modules:1324-1344)  */
+/* and amplitude_to_scattering_matrix (scatprops:1410-1436).                */
+/* amn0: 2*nodrt*(nodrt+2) x 2 (TE/TM, index model 2, two polarizations).   */
+/* ------------------------------------------------------------------------ */
+static void amplitude_to_sm(const cplx *sa, double *sm)
+{
+    cplx sp[4][4];
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) sp[i][j] = sa[i] * conj(sa[j]);
+#define SP(i, j) sp[(i) - 1][(j) - 1]
+#define SM(i, j) sm[((i) - 1) + 4 * ((j) - 1)]
+    SM(1, 1) = creal(SP(1, 1) + SP(2, 2) + SP(3, 3) + SP(4, 4));
+    SM(1, 2) = creal(-SP(1, 1) + SP(2, 2) - SP(3, 3) + SP(4, 4));
+    SM(2, 1) = creal(-SP(1, 1) + SP(2, 2) + SP(3, 3) - SP(4, 4));
+    SM(2, 2) = creal(SP(1, 1) + SP(2, 2) - SP(3, 3) - SP(4, 4));
+    SM(3, 3) = 2.0 * creal(SP(1, 2) + SP(3, 4));
+    SM(3, 4) = 2.0 * cimag(SP(2, 1) + SP(4, 3));
+    SM(4, 3) = 2.0 * cimag(SP(1, 2) - SP(3, 4));
+    SM(4, 4) = 2.0 * creal(SP(1, 2) - SP(3, 4));
+    SM(1, 3) = 2.0 * creal(SP(2, 3) + SP(1, 4));
+    SM(3, 1) = 2.0 * creal(SP(2, 4) + SP(1, 3));
+    SM(1, 4) = -2.0 * cimag(SP(2, 3) - SP(1, 4));
+    SM(4, 1) = -2.0 * cimag(SP(4, 2) + SP(1, 3));
+    SM(2, 3) = -2.0 * creal(SP(2, 3) - SP(1, 4));
+    SM(3, 2) = -2.0 * creal(SP(2, 4) - SP(1, 3));
+    SM(2, 4) = -2.0 * cimag(SP(2, 3) + SP(1, 4));
+    SM(4, 2) = -2.0 * cimag(SP(4, 2) - SP(1, 3));
+#undef SP
+#undef SM
+}
+
+void orc_scatteringmatrix(int nodrt, const cplx *amn0, double ct, double phi, int rotate, double rimed_re, cplx *sa, double *sm)
+{
+    tables_init();
+    const int nb = nodrt * (nodrt + 2);
+    const int ld = 2 * nb;
+    double *dc = (double *)malloc(sizeof(double) * 3 * (nb + 1));
+    rotcoef(ct, 1, nodrt, dc);
+#define DC(k, mn) dc[((k) + 1) + 3 * (mn)]
+    double cphi = cos(phi), sphi = sin(phi);
+    cplx *ephim = (cplx *)malloc(sizeof(cplx) * (2 * nodrt + 1));
+    ephicoef(cphi + CI * sphi, nodrt, ephim);
+    for (int k = 0; k < 4; k++) sa[k] = 0.0;
+    cplx cin = 1.0;
+    for (int n = 1; n <= nodrt; n++) {
+        cin = cin * (-CI);
+        double fnm = sqrt((double)(n + n + 1) / 2.0) / 4.0;
+        for (int m = -n; m <= n; m++) {
+            int mn = n * (n + 1) + m;
+            double tau[2] = {-fnm * (-DC(-1, mn) + DC(1, mn)), -fnm * (DC(-1, mn) + DC(1, mn))};
+            int m1 = (m <= -1) ? n + 1 : m, n1 = (m <= -1) ? -m : n;
+            cplx e = ephim[m + nodrt];
+            for (int p = 1; p <= 2; p++) {
+                int ia = AIDX(m1, n1, p - 1, nodrt);
+                cplx a1 = amn0[ia], a2 = amn0[ia + ld], a, b;
+                if (rotate) {
+                    a = a1 * cphi + a2 * sphi;
+                    b = a1 * sphi - a2 * cphi;
+                } else {
+                    a = a1;
+                    b = -a2;
+                }
+                sa[0] += cin * tau[2 - p] * b * e;
+                sa[1] += CI * cin * tau[p - 1] * a * e;
+                sa[2] += CI * cin * tau[p - 1] * b * e;
+                sa[3] += cin * tau[2 - p] * a * e;
+            }
+        }
+    }
+#undef DC
+    double qsca = 1.0 / ORC_REF_PI;
+    for (int k = 0; k < 4; k++) sa[k] = sa[k] * 4.0 / sqrt(2.0 * qsca);
+    amplitude_to_sm(sa, sm);
+    for (int k = 0; k < 16; k++) sm[k] = sm[k] / (4.0 * ORC_REF_PI) / rimed_re;
+    free(dc);
+    free(ephim);
+}
+
+/* The angle loop of scattering_matrix_calculation (input:3038-3061) for a
+ * single-origin expansion without azimuthal averaging: i = ldim..udim,
+ * theta_i = amin + (amax - amin)(i - ldim)/(udim - ldim) degrees, cos theta
+ * kept off +-1, azimuth alpha + pi for i < 0 and alpha otherwise.
+ * sm: 16 x (udim - ldim + 1). */
+void orc_incident_plane_scattering(int nodrt, const cplx *amn0, int ldim, int udim, double amin, double amax, double alpha,
+                                   int rotate, double rimed_re, double *sm)
+{
+    cplx sa[4];
+    for (int i = ldim; i <= udim; i++) {
+        double ct = cos(ORC_REF_PI / 180.0 * (amin + (amax - amin) * (double)(i - ldim) / (double)(udim - ldim)));
+        if (ct == 1.0) ct = 0.9999999;
+        if (ct == -1.0) ct = -0.9999999;
+        double phi = (i < 0) ? alpha + ORC_REF_PI : alpha;
+        orc_scatteringmatrix(nodrt, amn0, ct, phi, rotate, rimed_re, sa, sm + 16 * (size_t)(i - ldim));
+    }
+}

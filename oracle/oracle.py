@@ -84,6 +84,9 @@ def lib():
         L.orc_fft_near_pairs.argtypes = [c_void_p, c_void_p, c_void_p]
         L.orc_fft_near_pairs.restype = c_int
         L.orc_ranorienscatmatrixcalc.argtypes = [c_double, c_void_p, c_int, c_void_p]
+        L.orc_scatteringmatrix.argtypes = [c_int, c_void_p, c_double, c_double, c_int, c_double, c_void_p, c_void_p]
+        L.orc_incident_plane_scattering.argtypes = [c_int, c_void_p, c_int, c_int, c_double, c_double, c_double, c_int,
+                                                    c_double, c_void_p]
         _lib = L
     return _lib
 
@@ -378,3 +381,27 @@ def ranorientscatmatrix(tmo, tmat, rimed_re=1.0, nangles=181):
     sm3 = sm.reshape(W, 4, 4).transpose(0, 2, 1)
     cf3 = smcf.reshape(W, 4, 4).transpose(0, 2, 1)
     return dict(sm=sm3, smcf=cf3, smat=smat, coherent=cf3[0, 0, 0], sm_raw=sm, smcf_raw=smcf)
+
+
+def scatteringmatrix(nodrt, amn0, ct, phi, rotate=False, rimed_re=1.0):
+    """scatteringmatrix (normalize_s11 false) at one direction: (sa[4], sm (4,4))."""
+    a0 = np.asfortranarray(amn0, np.complex128)
+    sa = np.zeros(4, np.complex128)
+    sm = np.zeros(16)
+    lib().orc_scatteringmatrix(nodrt, _p(a0), ct, phi, int(rotate), rimed_re, _p(sa), _p(sm))
+    return sa, sm.reshape(4, 4, order="F")
+
+
+def incident_plane_scattering(nodrt, amn0, increment=1.0, alpha=0.0, rotate=False, rimed_re=1.0):
+    """The non-azimuth-averaged scattering matrix of a single-origin expansion
+    over theta = -180..180 degrees (udim = floor(180.00001/increment)):
+    returns (theta (2udim+1,), smat (2udim+1, 4, 4))."""
+    udim = int(np.floor(180.00001 / increment))
+    ldim, amax = -udim, 180.0
+    amin = amax * (-1 if udim > 0 else 0)
+    a0 = np.asfortranarray(amn0, np.complex128)
+    n = udim - ldim + 1
+    sm = np.zeros(16 * n)
+    lib().orc_incident_plane_scattering(nodrt, _p(a0), ldim, udim, amin, amax, alpha, int(rotate), rimed_re, _p(sm))
+    theta = np.array([amin + (i - ldim) / (udim - ldim) * (amax - amin) for i in range(ldim, udim + 1)])
+    return theta, sm.reshape(n, 4, 4).transpose(0, 2, 1)

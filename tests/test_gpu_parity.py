@@ -204,6 +204,27 @@ def test_scattering_postprocessing(api, oracle_mod, name):
     assert abs(sgm["g"] - so["g"]) <= 1e-6
 
 
+@pytest.mark.parametrize("alpha,rotate", [(0.0, False), (0.4, True)])
+def test_incident_plane_scattering(api, oracle_mod, alpha, rotate):
+    """scatteringmatrix over the directions scattering_matrix_calculation uses
+    without azimuthal averaging (theta = -180..180, 1 degree): device vs oracle
+    on the same common-origin expansion, which the device merge produced and
+    which matches the oracle's merge."""
+    pos, rad, ri, em = _cluster("cluster20")
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em)
+    ro = o.fixedorsoln(eps=1e-12, niter=4000)
+    so = o.scattering(ro["amnp"])
+    sg = g.scattering(ro["amnp"])
+    T = sg["t_matrix_order"]
+    assert T == so["t_matrix_order"]
+    assert np.abs(sg["amnp0"] - so["amnp0"]).max() <= 1e-10 * np.abs(so["amnp0"]).max()
+    th_g, sm_g = g.scattering_plane(sg["amnp0"], T, increment=1.0, alpha=alpha, rotate_plane=rotate)
+    th_o, sm_o = oracle_mod.incident_plane_scattering(T, sg["amnp0"], increment=1.0, alpha=alpha, rotate=rotate)
+    assert sm_g.shape == (361, 4, 4)
+    assert np.array_equal(th_g, th_o)
+    assert np.abs(sm_g - sm_o).max() <= 1e-11 * np.abs(sm_o[:, 0, 0]).max()
+
+
 @pytest.mark.parametrize("name", ["cluster8", "cluster20"])
 def test_tmatrix_fp64(api, oracle_mod, name):
     """tmatrix_solution: the many-column FP64 solve follows cbicg per column, so

@@ -66,6 +66,14 @@ def test_deck_runs_match_oracle(oracle_mod, tmp_path):
     assert np.allclose(fixed["qtot"], ro["qtot"], rtol=1e-9)
     sc = o.scattering(ro["amnp"])
     assert abs(fixed["g_asym"] - sc["g"]) < 1e-9
+    # azimuthal_average false (the default): the plane of incidence, -180..180
+    th, sm = oracle_mod.incident_plane_scattering(sc["t_matrix_order"], sc["amnp0"], increment=1.0)
+    assert fixed["smat"].shape == (361, 4, 4) and np.array_equal(fixed["theta"], th)
+    assert np.abs(fixed["smat"] - sm).max() <= 1e-8 * np.abs(sm[:, 0, 0]).max()
+    avg = dict(runs[0], azimuthal_average=True, scattering_map_increment=5.0)
+    fa = I.execute(avg, "fp64")
+    ga = oracle_mod.gsf_scattering(sc["t_matrix_order"], sc["amnp0"], nangles=37)["smat"]
+    assert fa["smat"].shape == (37, 4, 4) and np.abs(fa["smat"] - ga).max() <= 1e-8 * np.abs(ga[:, 0, 0]).max()
     rand = I.execute(runs[1], "fp64")
     rt = o.tmatrix_solution(convergence_eps=1e-8, solution_eps=1e-12)
     assert rand["t_matrix_order"] == rt["order"]

@@ -182,6 +182,51 @@ def test_single_sphere_scattering_matrix_and_g_equal_mie(oracle_mod):
         assert abs(sc["smat"][i, 0, 1] - s12) < 1e-9 * s11
 
 
+def test_incident_plane_scattering_single_sphere_equals_azimuth_average(oracle_mod):
+    """scatteringmatrix (normalize_s11 false) of a lone sphere does not depend on
+    the azimuth: the theta >= 0 half of the incident-plane matrix equals the
+    GSF (fosmcalc) matrix, which the Mie test above pins."""
+    x, m, L = 2.0, 1.5 + 0.01j, 9
+    o = oracle_mod.Oracle([[0.0, 0.0, 0.0]], [x], [m], mie_eps=-L)
+    sc = o.scattering(o.fixedorsoln(eps=1e-14)["amnp"])
+    T = sc["t_matrix_order"]
+    theta, sm = oracle_mod.incident_plane_scattering(T, sc["amnp0"], increment=5.0)
+    assert len(theta) == 73 and theta[0] == -180.0 and theta[36] == 0.0 and theta[-1] == 180.0
+    fs = oracle_mod.gsf_scattering(T, sc["amnp0"], nangles=37)["smat"]
+    assert np.abs(sm[36:] - fs).max() < 1e-12 * np.abs(fs[:, 0, 0]).max()
+    # the far half (azimuth alpha + pi) mirrors it; the reference's single
+    # precision pi tilts that plane by 8.7e-8 rad, hence the 1e-6 bound
+    assert np.abs(sm[:36][::-1] - sm[37:]).max() < 1e-6 * np.abs(fs[:, 0, 0]).max()
+
+
+def test_incident_plane_scattering_averages_to_gsf_matrix(oracle_mod):
+    """For a cluster, the azimuthal mean of scatteringmatrix with rotate_plane
+    (numerical_sm_azimuthal_average_so, mstm-scatprops-26.f90) equals the GSF
+    matrix on the elements fosmcalc keeps: the diagonal, (S12+S21)/2 and
+    (S34-S43)/2.  64 azimuths integrate the band-limited products exactly."""
+    pos = _small_cluster()
+    o = oracle_mod.Oracle(pos, [1.0] * 5, [1.5 + 0.01j] * 5, mie_eps=-7)
+    sc = o.scattering(o.fixedorsoln(eps=1e-14)["amnp"])
+    T, a0 = sc["t_matrix_order"], sc["amnp0"]
+    assert 2 * T + 4 < 64
+    fs = oracle_mod.gsf_scattering(T, a0, nangles=19)["smat"]
+    pi_ref = float(np.float32(np.pi))
+    scale = np.abs(fs[:, 0, 0]).max()
+    for k in (0, 3, 9, 14, 18):
+        ct = np.cos(pi_ref / 180.0 * (180.0 * k / 18))
+        ct = 0.9999999 if ct == 1.0 else (-0.9999999 if ct == -1.0 else ct)
+        acc = sum(oracle_mod.scatteringmatrix(T, a0, ct, 2 * np.pi * j / 64, rotate=True)[1] for j in range(64)) / 64
+        for i in range(4):
+            assert abs(acc[i, i] - fs[k][i, i]) < 1e-12 * scale
+        assert abs(0.5 * (acc[0, 1] + acc[1, 0]) - fs[k][0, 1]) < 1e-12 * scale
+        assert abs(0.5 * (acc[2, 3] - acc[3, 2]) - fs[k][2, 3]) < 1e-12 * scale
+    # rotate_plane changes nothing in the plane of incidence (azimuth 0)
+    ct = np.cos(0.7)
+    s0 = oracle_mod.scatteringmatrix(T, a0, ct, 0.0, rotate=False)[1]
+    s1 = oracle_mod.scatteringmatrix(T, a0, ct, 0.0, rotate=True)[1]
+    assert np.abs(s0 - s1).max() < 1e-14 * scale
+
+
 def test_scattering_invariant_under_cluster_shift(oracle_mod):
     pos = _small_cluster()
     o1 = oracle_mod.Oracle(pos, [1.0] * 5, [1.5 + 0.01j] * 5, mie_eps=-7)
