@@ -250,6 +250,13 @@ int mstmg_last_stats(const mstmg_ctx *ctx, int *iters2, int *outer, int *passes6
  * reference's canonical per-pass operator bytes (translation_data layout). */
 int mstmg_operator_bytes(const mstmg_ctx *ctx, int prec, double *stored_bytes, double *canonical_bytes);
 
+/* The pair translation pass alone, y = H x (external_to_external_expansion,
+ * mstm-modules-33.f90:6390-6525, no Mie multiply): ncols columns (<= 256) of
+ * neqns complex values, column k a conjugate-transpose product when
+ * con_tran[k] != 0 (NULL: none), with the FP64 (prec 0) or FP32 (prec 1)
+ * operators and kernels the solvers use; FP32 results are returned widened. */
+int mstmg_translation_pass(mstmg_ctx *ctx, int prec, int ncols, const int *con_tran, const double *x, double *y);
+
 /* Time `reps` translation passes (nrhs right-hand sides, FP64 or FP32) with CUDA
  * events on the context stream; returns the average milliseconds per pass. */
 int mstmg_time_translation(mstmg_ctx *ctx, int prec, int nrhs, int reps, double *ms_per_pass);

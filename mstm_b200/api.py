@@ -161,6 +161,17 @@ class SphereCluster:
         amnp0 = np.asfortranarray(a0.reshape(-1, order="F")[:2 * nb0].reshape(nb0, 2, order="F"))
         return dict(smat=smat.reshape(nangles, 4, 4).transpose(0, 2, 1).copy(), g=g.value, t_matrix_order=T, amnp0=amnp0)
 
+    def translation_pass(self, x, con_tran=None, precision="fp64"):
+        """y = H x, the pair translation pass alone (external_to_external_expansion,
+        mstm-modules-33.f90:6390-6525) with the FP64 or FP32 ("fp32") operators."""
+        x = np.asfortranarray(np.asarray(x, np.complex128).reshape(self.number_eqns, -1))
+        ncols = x.shape[1]
+        y = np.zeros_like(x, order="F")
+        ct = None if con_tran is None else np.ascontiguousarray(np.asarray(con_tran, np.int32))
+        check(self._L.mstmg_translation_pass(self.ctx, 0 if precision == "fp64" else 1, ncols, None if ct is None else _ptr(ct),
+                                             _ptr(x), _ptr(y)), "translation_pass")
+        return y
+
     def scattering_plane(self, amnp0, t_matrix_order, increment=1.0, alpha=0.0, rotate_plane=False):
         """Scattering matrix without azimuthal averaging (scatteringmatrix,
         mstm-scatprops-26.f90:1498-1573, normalize_s11 false) at the directions

@@ -20,6 +20,7 @@
 #include "densepair.cuh"
 #include <cufft.h>
 #include <memory>
+#include <type_traits>
 
 static thread_local std::string g_err;
 static void set_err(const std::string& s) { g_err = s; }
@@ -2369,6 +2370,60 @@ extern "C" long long mstmg_kernel_launches(void) { return launch_counter().load(
 // One translation pass over nrhs columns laid out as BiCG packs them
 // ([p, A^T conj w] pairs, odd columns conjugate-transpose products), timed with
 // CUDA events on the context's stream (mean of reps after one warm-up).
+extern "C" int mstmg_translation_pass(mstmg_ctx* c, int prec, int ncols, const int* con_tran, const double* x, double* y)
+{
+    if (!c || ncols < 1 || ncols > 256 || !x || !y || (prec != 0 && prec != 1)) {
+        set_err("mstmg_translation_pass: bad arguments");
+        return MSTMG_ERR_ARG;
+    }
+    int rc = ensure_ops(c, prec, false);
+    if (rc) return rc;
+    const size_t ne = (size_t)c->neqns, cols = ne * ncols;
+    // a period-2 con_tran pattern goes through the many-column path; anything
+    // else in groups of up to 4 columns with their own masks
+    bool per2 = true;
+    for (int k = 2; k < ncols; k++) per2 = per2 && ((con_tran ? con_tran[k] != 0 : false) == (con_tran ? con_tran[k - 2] != 0 : false));
+    unsigned pattern2 = 0;
+    if (con_tran && con_tran[0]) pattern2 |= 1u;
+    if (con_tran && ncols > 1 && con_tran[1]) pattern2 |= 2u;
+    DevBuf<zd> x64, y64;
+    CK(x64.alloc(cols));
+    CK(y64.alloc(cols));
+    CK(copy_in(x64.p, x, sizeof(zd) * cols, c->st));
+    auto groups = [&](auto* xp, auto* yp) -> int {
+        using TT = std::remove_pointer_t<decltype(xp)>;
+        using T = decltype(TT::x);
+        if (per2) return translate_many<T>(c, xp, yp, ncols, pattern2);
+        for (int k = 0; k < ncols; k += 4) {
+            int w = std::min(4, ncols - k);
+            unsigned m = 0;
+            for (int r = 0; r < w; r++)
+                if (con_tran && con_tran[k + r]) m |= 1u << r;
+            int rr = translate<T>(c, xp + k * ne, yp + k * ne, w, m);
+            if (rr) return rr;
+        }
+        return MSTMG_OK;
+    };
+    if (prec == 0) {
+        if ((rc = groups(x64.p, y64.p))) return rc;
+    } else {
+        DevBuf<zf> x32, y32;
+        CK(x32.alloc(cols));
+        CK(y32.alloc(cols));
+        launch_d2f((int)cols, x64.p, x32.p, c->st);
+        if ((rc = groups(x32.p, y32.p))) return rc;
+        CK(cudaMemsetAsync(y64.p, 0, sizeof(zd) * cols, c->st));
+        launch_add_correction_f((int)cols, y64.p, y32.p, c->st);
+        CK(cudaGetLastError());
+        CK(copy_out(y, y64.p, sizeof(zd) * cols, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        return check_kernel_err(c);
+    }
+    CK(copy_out(y, y64.p, sizeof(zd) * cols, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return check_kernel_err(c);
+}
+
 extern "C" int mstmg_time_translation(mstmg_ctx* c, int prec, int nrhs, int reps, double* ms)
 {
     if (!c || nrhs < 1 || nrhs > 256 || reps < 1) return MSTMG_ERR_ARG;

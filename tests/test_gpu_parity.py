@@ -97,6 +97,28 @@ def test_tiled_and_generic_kernels_agree(api, name, nrhs):
         assert np.abs(ya - yb).max() <= 1e-11 * np.abs(yb).max()
 
 
+@pytest.mark.parametrize("name", ["fractal60", "cluster20"])
+def test_translation_pass_kernels_agree(api, name):
+    """The translation pass alone through the C ABI: the tiled kernel (uniform
+    orders) against the order-generic kernel, FP64 to 1e-12 and FP32 to 2e-6
+    of the largest output, for 2, 4 and 8 columns (8: many-column chunks) and
+    several con_tran patterns."""
+    pos, rad, ri, em = _cluster(name)
+    til = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed")
+    gen = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", generic_kernel=True)
+    rng = np.random.default_rng(5)
+    for ct in ([0, 1], [1, 0], [0, 0], [0, 1, 0, 1], [1, 1, 0, 0], [0, 1] * 4, [1, 0] * 4):
+        x = rng.normal(size=(til.number_eqns, len(ct))) + 1j * rng.normal(size=(til.number_eqns, len(ct)))
+        y64 = [k.translation_pass(x, ct, "fp64") for k in (til, gen)]
+        s = np.abs(y64[1]).max()
+        assert np.abs(y64[0] - y64[1]).max() <= 1e-12 * s, ct
+        y32 = [k.translation_pass(x, ct, "fp32") for k in (til, gen)]
+        assert np.abs(y32[0] - y64[1]).max() <= 2e-6 * s, ct
+        assert np.abs(y32[1] - y64[1]).max() <= 2e-6 * s, ct
+    til.close()
+    gen.close()
+
+
 def test_cbicg_same_iterations(api, oracle_mod):
     pos, rad, ri, em = _cluster("cluster20")
     g, o = _pair(api, oracle_mod, pos, rad, ri, em)
