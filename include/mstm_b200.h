@@ -54,7 +54,8 @@ typedef struct {
     int max_outer;                 /* mixed mode: refinement steps cap (default 30) */
     int generic_kernel;            /* 1: always use the order-generic translation kernel (default 0) */
     int tile_ctas_per_sm;          /* tiled kernel CTAs per SM, 1 or 2 (0: as many as shared memory allows, at most 2) */
-    int fp32_chunk;                /* columns per chunk of FP32 many-column passes, 2 or 4 (0: 4) */
+    int fp32_chunk;                /* columns per chunk of FP32 tiled passes, 2 or 4 (0: chosen per context by
+                                      timing one pass of each on the first pass of 4 or more columns) */
     int mixed_solver;              /* MSTMG_PRECISION_MIXED fixed-orientation solver: 0 FP32 BiCG with FP64
                                       residual replacement (default), 1 restarted FP32 BiCG inside FP64 refinement */
 } mstmg_opts;

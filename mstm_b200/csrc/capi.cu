@@ -20,6 +20,7 @@
 #include "densepair.cuh"
 #include <cufft.h>
 #include <memory>
+#include <algorithm>
 #include <type_traits>
 
 static thread_local std::string g_err;
@@ -115,6 +116,7 @@ struct mstmg_ctx {
     DevBuf<double> op64;
     DevBuf<float> op32;
     bool ops64_ready = false, ops32_ready = false;
+    int chunk32 = 0;   // FP32 columns per tiled chunk chosen by timing (0: not yet)
     DevBuf<double> vcc, fnm1, fnc, fnp1, fnr, bcofd;
     int vn = 0;
     DevBuf<int> err;
@@ -751,11 +753,55 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
     return MSTMG_OK;
 }
 
+// Columns per chunk of FP32 tiled passes: opts.fp32_chunk when set (2 or 4),
+// otherwise chosen once per context by timing one pass over the caller's
+// columns in chunks of 4 and of 2 (each run twice, the second timed), which
+// depends on the order and the cluster size (4 wins at L = 9, 2 at L = 8 and
+// for small column counts).  The timing passes write y, which the caller's
+// own pass then overwrites.
+static int fp32_chunk(mstmg_ctx* c, const zf* x, zf* y, int ncols, unsigned pattern2)
+{
+    if (c->opts.fp32_chunk == 2 || c->opts.fp32_chunk == 4) return c->opts.fp32_chunk;
+    if (c->chunk32 > 0) return c->chunk32;
+    if (!c->tiled || ncols < 4 || ncols % 4 != 0 || !tiled_supported(c->lmax, 2) || !tiled_supported(c->lmax, 4)) return 4;
+    auto expand = [&](int w) {
+        unsigned m = 0;
+        for (int r = 0; r < w; r++)
+            if ((pattern2 >> (r & 1)) & 1u) m |= 1u << r;
+        return m;
+    };
+    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    for (auto& ev : e)
+        if (cudaEventCreate(&ev) != cudaSuccess) {
+            for (auto& f : e)
+                if (f) cudaEventDestroy(f);
+            return 4;
+        }
+    float ms[2] = {0.f, 0.f};
+    const int nr[2] = {4, 2};
+    const bool timing = c->timing;
+    c->timing = false;
+    bool ok = true;
+    for (int v = 0; v < 2 && ok; v++) {
+        ok = translate<float>(c, x, y, nr[v], expand(nr[v]), ncols / nr[v]) == MSTMG_OK;
+        cudaEventRecord(e[0], c->st);
+        ok = ok && translate<float>(c, x, y, nr[v], expand(nr[v]), ncols / nr[v]) == MSTMG_OK;
+        cudaEventRecord(e[1], c->st);
+        ok = ok && cudaEventSynchronize(e[1]) == cudaSuccess && cudaEventElapsedTime(&ms[v], e[0], e[1]) == cudaSuccess;
+    }
+    c->timing = timing;
+    for (auto& f : e) cudaEventDestroy(f);
+    if (!ok) return 4;
+    c->passes32 -= 4;   // the timing passes are not the caller's
+    c->chunk32 = ms[1] < ms[0] ? 2 : 4;
+    return c->chunk32;
+}
+
 // Many columns: y[:, 0:ncols] = H x[:, 0:ncols], where column k is a
 // conjugate-transpose product when bit (k & 1) of pattern2 is set (BiCG packs
 // [p_1, w_1, p_2, w_2, ...]: pattern2 = 2).  On the tiled path the columns go
-// in chunks of 4 (FP32) or 2 (FP64) through one launch; otherwise in groups of
-// up to 4 columns, one launch each.
+// in chunks of 4 or 2 (FP32, fp32_chunk) or 2 (FP64) through one launch;
+// otherwise in groups of up to 4 columns, one launch each.
 template <typename T> static int translate_many(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int ncols, unsigned pattern2)
 {
     auto expand = [&](int w) {
@@ -764,7 +810,8 @@ template <typename T> static int translate_many(mstmg_ctx* c, const cpx<T>* x, c
             if ((pattern2 >> (r & 1)) & 1u) m |= 1u << r;
         return m;
     };
-    const int NR = sizeof(T) == 4 ? (c->opts.fp32_chunk == 2 ? 2 : 4) : 2;
+    int NR = 2;
+    if constexpr (sizeof(T) == 4) NR = fp32_chunk(c, x, y, ncols, pattern2);
     if (c->tiled && ncols > NR && ncols % NR == 0 && tiled_supported(c->lmax, NR)) {
         int rc = translate<T>(c, x, y, NR, expand(NR), ncols / NR);
         if (rc != MSTMG_ERR_UNSUPPORTED) return rc;
@@ -1154,7 +1201,8 @@ static int solve_mixed_rr(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, 
                               c->st);
             mask |= 2u << (2 * k);
         }
-        if ((rc = translate<float>(c, c->X32.p, c->Y32.p, 2 * a, mask))) return rc;
+        (void)mask;   // [p, A^T conj w] pairs: the odd columns are the transpose products
+        if ((rc = translate_many<float>(c, c->X32.p, c->Y32.p, 2 * a, 2u))) return rc;
         for (int k = 0; k < a; k++) {
             int s = slots[k];
             BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
@@ -1793,6 +1841,143 @@ static int solve_multi_mixed(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<flo
     return check_kernel_err(c);
 }
 
+// Mixed precision for S systems by residual replacement (the many-system form
+// of solve_mixed_rr): one FP32 BiCG per system, never restarted; whenever a
+// system's recursive residual has fallen by `drop` since its last replacement,
+// or claims convergence, its FP32 iterate is folded into the FP64 solution X,
+// the FP64 true residual replaces r, and csk/beta are recomputed.  The same
+// FP64 pass also replaces every other system whose residual has fallen by
+// `drop_soft`, so the systems of one order share their FP64 passes.  A system
+// stops when its true residual ratio is below eps.  X holds the initial
+// guesses on entry.
+static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>& w32, DevBuf<double>& rr, DevBuf<int>& idx, int S,
+                          const zd* B, zd* X, double eps, int niter, std::vector<int>& iters, std::vector<double>& errs,
+                          std::vector<int>& status, int* outer_count)
+{
+    const int ne = c->neqns;
+    SlotMaps sm = c->sm();
+    const zf* an32 = (const zf*)c->an32.p;
+    MultiVecs<float> v = w32.v(ne);
+    const double drop = 1.0e-5, drop_soft = 1.0e-3;
+    std::vector<int> act(S), tot(S, 0);
+    std::vector<double> base(S, 1.0), ratio(S, 0.0), hrr(2 * (size_t)S);
+    for (int s = 0; s < S; s++) act[s] = s;
+    iters.assign(S, 0);
+    errs.assign(S, 1.0);
+    status.assign(S, 0);
+    *outer_count = 0;
+    int rc;
+    // FP64 true residual of the systems in L, rounded into their FP32 r
+    auto true_residual = [&](const std::vector<int>& Ls) -> int {
+        const int a = (int)Ls.size();
+        if (a == 0) return MSTMG_OK;
+        const int apad = ((a + 1) / 2) * 2;
+        CK(cudaMemcpyAsync(w64.act.p, Ls.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+        launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
+        int r2 = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u);
+        if (r2) return r2;
+        launch_m_resid<float>(sm, c->an.p, ne, a, w64.act.p, B, X, w64.YP.p, v.R, w64.part.p, rr.p, c->nsm, c->st, 1);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hrr.data(), rr.p, sizeof(double) * 2 * S, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        (*outer_count)++;
+        for (int s : Ls) ratio[s] = hrr[2 * s + 1] > 0.0 ? hrr[2 * s] / hrr[2 * s + 1] : 0.0;
+        return MSTMG_OK;
+    };
+    auto upload_act = [&]() -> int {
+        if (!act.empty()) CK(cudaMemcpyAsync(w32.act.p, act.data(), sizeof(int) * act.size(), cudaMemcpyHostToDevice, c->st));
+        return MSTMG_OK;
+    };
+    if ((rc = true_residual(act))) return rc;
+    {
+        std::vector<int> keep;
+        for (int s : act) {
+            base[s] = errs[s] = ratio[s];
+            if (ratio[s] >= eps && niter > 0) keep.push_back(s);
+        }
+        act = keep;
+    }
+    if (act.empty()) return check_kernel_err(c);
+    // FP32 BiCG from the true residual: x32 = 0, p = r, q = w = conj(r)
+    if ((rc = upload_act())) return rc;
+    for (int s : act) CK(cudaMemsetAsync(v.X + (size_t)s * ne, 0, sizeof(zf) * ne, c->st));
+    launch_m_init<float>(sm, an32, ne, (int)act.size(), w32.act.p, v.R, v, nullptr, 0, w32.part.p, w32.sc.p, c->nsm, c->st);
+    CK(cudaGetLastError());
+    const int per_chunk = 2;   // systems per FP32 translation chunk ([p, w] column pairs)
+    for (int it = 1; it <= niter && !act.empty(); it++) {
+        const int a = (int)act.size();
+        const int apad = ((a + per_chunk - 1) / per_chunk) * per_chunk;
+        launch_m_pack<float>(sm, an32, ne, a, apad, w32.act.p, v.P, v.W, w32.XP.p, c->nsm, c->st);
+        if ((rc = translate_many<float>(c, w32.XP.p, w32.YP.p, 2 * apad, 2u))) return rc;
+        launch_m_post<float>(sm, an32, ne, a, w32.act.p, v, w32.YP.p, w32.part.p, w32.sc.p, c->nsm, c->st);
+        launch_m_upd1<float>(ne, a, w32.act.p, v, w32.part.p, w32.sc.p, c->nsm, c->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(w32.hsc.data(), w32.sc.p, sizeof(BicgScalars) * S, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        std::vector<int> repl, keep;
+        bool trigger = false;
+        for (int s : act) {
+            tot[s] = it;
+            const BicgScalars& q = w32.hsc[s];
+            if (q.breakdown) {
+                // breakdown: fold the iterate in and report it
+                status[s] = 2;
+                continue;
+            }
+            if (q.stop || q.eerr * base[s] < eps || q.eerr < drop) trigger = true;
+            keep.push_back(s);
+        }
+        // one FP64 pass serves every system close to its next replacement
+        if (trigger)
+            for (int s : keep) {
+                const BicgScalars& q = w32.hsc[s];
+                if (q.stop || q.eerr * base[s] < eps || q.eerr < drop_soft) repl.push_back(s);
+            }
+        for (int s : act)
+            if (status[s] == 2) {
+                std::vector<int> one{s};
+                CK(cudaMemcpyAsync(idx.p, one.data(), sizeof(int), cudaMemcpyHostToDevice, c->st));
+                launch_m_addcorr<float>(ne, 1, idx.p, idx.p, X, v.X, c->st);
+            }
+        if (!repl.empty()) {
+            const int nr = (int)repl.size();
+            CK(cudaMemcpyAsync(idx.p, repl.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, c->st));
+            launch_m_addcorr<float>(ne, nr, idx.p, idx.p, X, v.X, c->st);
+            for (int s : repl) CK(cudaMemsetAsync(v.X + (size_t)s * ne, 0, sizeof(zf) * ne, c->st));
+            if ((rc = true_residual(repl))) return rc;
+            std::vector<int> fix, keep2;
+            for (int s : keep) {
+                bool replaced = std::find(repl.begin(), repl.end(), s) != repl.end();
+                if (replaced) {
+                    errs[s] = base[s] = ratio[s];
+                    if (ratio[s] < eps) continue;   // converged
+                    fix.push_back(s);
+                }
+                keep2.push_back(s);
+            }
+            if (!fix.empty()) {
+                CK(cudaMemcpyAsync(idx.p, fix.data(), sizeof(int) * fix.size(), cudaMemcpyHostToDevice, c->st));
+                launch_m_rrfix<float>(ne, (int)fix.size(), idx.p, v, w32.part.p, w32.sc.p, c->nsm, c->st);
+            }
+            keep = keep2;
+        }
+        if (keep.size() != act.size()) {
+            act = keep;
+            if ((rc = upload_act())) return rc;
+        }
+        if (!act.empty()) launch_m_upd2<float>(ne, (int)act.size(), w32.act.p, v, w32.sc.p, c->nsm, c->st);
+        CK(cudaGetLastError());
+    }
+    if (!act.empty()) {
+        // iteration cap: fold the last FP32 steps in
+        CK(cudaMemcpyAsync(idx.p, act.data(), sizeof(int) * act.size(), cudaMemcpyHostToDevice, c->st));
+        launch_m_addcorr<float>(ne, (int)act.size(), idx.p, idx.p, X, v.X, c->st);
+        for (int s : act) tot[s] = niter + 1;
+    }
+    for (int s = 0; s < S; s++) iters[s] = tot[s];
+    return check_kernel_err(c);
+}
+
 extern "C" int mstmg_t_matrix_order(mstmg_ctx* c, double trans_eps, int max_t_order, int* t_matrix_order)
 {
     if (!c || max_t_order < 1 || !t_matrix_order) {
@@ -1900,7 +2085,10 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
         std::vector<int> sts;
         if (mixed) {
             int oc = 0;
-            rc = solve_multi_mixed(c, w64, w32, B32, rr, idx, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
+            if (c->opts.mixed_solver == 1)
+                rc = solve_multi_mixed(c, w64, w32, B32, rr, idx, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
+            else
+                rc = solve_multi_rr(c, w64, w32, rr, idx, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
             outer_total += oc;
         } else {
             std::vector<int> sys(S);

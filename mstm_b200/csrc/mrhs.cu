@@ -256,20 +256,65 @@ __global__ void m_fin_kernel(int mode, int a, int G, const int* act, const doubl
             zd b = cdiv(csk2, csk);
             sc->beta[0] = b.x;
             sc->beta[1] = b.y;
+            sc->csk_prev[0] = csk.x;
+            sc->csk_prev[1] = csk.y;
             sc->csk[0] = csk2.x;
             sc->csk[1] = csk2.y;
         }
     }
 }
 
+// Residual replacement of the systems in act: r was replaced by the true
+// residual; csk = sum conj(q) r, beta = csk / csk_prev, enorm = sum |r|^2
+// (the new base of eerr).  part: 3 partials per CTA per system.
+__global__ void m_rrfin_kernel(int a, int G, const int* act, const double* part, BicgScalars* scs)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a) return;
+    BicgScalars* sc = scs + act[k];
+    double s[3] = {0.0, 0.0, 0.0};
+    const double* pk = part + (size_t)3 * G * k;
+    for (int b = 0; b < G; b++)
+        for (int j = 0; j < 3; j++) s[j] += pk[3 * b + j];
+    zd csk2 = mk(s[0], s[1]), prev = mk(sc->csk_prev[0], sc->csk_prev[1]);
+    if (cabsd(prev) == 0.0) {
+        sc->breakdown = 1;
+        return;
+    }
+    zd b = cdiv(csk2, prev);
+    sc->beta[0] = b.x;
+    sc->beta[1] = b.y;
+    sc->csk[0] = csk2.x;
+    sc->csk[1] = csk2.y;
+    sc->enorm = s[2];
+    sc->eerr = 1.0;
+    sc->stop = (s[0] == 0.0 && s[1] == 0.0) ? 1 : 0;
+}
+
+// partials sum conj(q) r, sum |r|^2 of the systems in act
+template <typename T>
+__global__ void __launch_bounds__(MB) m_rrdot_kernel(int ld, const int* act, MultiVecs<T> v, double* part)
+{
+    const int k = blockIdx.y, s = act[k];
+    const size_t o = (size_t)s * ld;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+        cpx<double> rd = upd_(v.R[o + e]), qd = upd_(v.Q[o + e]);
+        acc[0] += qd.x * rd.x + qd.y * rd.y;
+        acc[1] += qd.x * rd.y - qd.y * rd.x;
+        acc[2] += rd.x * rd.x + rd.y * rd.y;
+    }
+    mblock_store<3>(acc, part + 3 * ((size_t)k * gridDim.x + blockIdx.x));
+}
+
 template <typename TB>
 __global__ void __launch_bounds__(MB) m_resid_kernel(SlotMaps sm, const zd* an, int ld, const int* act, const zd* B, const zd* X,
-                                                     const zd* YP, cpx<TB>* Rout, double* part)
+                                                     const zd* YP, cpx<TB>* Rout, int by_sys, double* part)
 {
     const int k = blockIdx.y, s = act[k];
     const size_t o = (size_t)s * ld;
     const zd* y = YP + (size_t)k * ld;
-    cpx<TB>* ro = Rout + (size_t)k * ld;
+    cpx<TB>* ro = Rout + (size_t)(by_sys ? s : k) * ld;
     double acc[2] = {0.0, 0.0};
     for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
         SlotPos q = slot_pos(sm, e);
@@ -541,12 +586,34 @@ void launch_m_upd(int ld, int a, const int* act, const MultiVecs<T>& v, double* 
     m_upd2_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v);
     launch_counter() += 3;
 }
+template <typename T>
+void launch_m_upd1(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, int nsm, cudaStream_t st)
+{
+    int G = multi_grid(ld, a, nsm);
+    m_upd1_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v, part);
+    m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(2, a, G, act, part, sc, nullptr);
+    launch_counter() += 2;
+}
+template <typename T> void launch_m_upd2(int ld, int a, const int* act, const MultiVecs<T>& v, const BicgScalars* sc, int nsm, cudaStream_t st)
+{
+    int G = multi_grid(ld, a, nsm);
+    m_upd2_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v);
+    launch_counter() += 1;
+}
+template <typename T> void launch_m_rrfix(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, int nsm,
+                                          cudaStream_t st)
+{
+    int G = multi_grid(ld, a, nsm);
+    m_rrdot_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, v, part);
+    m_rrfin_kernel<<<(a + 63) / 64, 64, 0, st>>>(a, G, act, part, sc);
+    launch_counter() += 2;
+}
 template <typename TB>
 void launch_m_resid(const SlotMaps& sm, const zd* an, int ld, int a, const int* act, const zd* B, const zd* X, const zd* YP, cpx<TB>* Rout,
-                    double* part, double* out2, int nsm, cudaStream_t st)
+                    double* part, double* out2, int nsm, cudaStream_t st, int by_sys)
 {
     int G = multi_grid(sm.nslots, a, nsm);
-    m_resid_kernel<TB><<<dim3(G, a), MB, 0, st>>>(sm, an, ld, act, B, X, YP, Rout, part);
+    m_resid_kernel<TB><<<dim3(G, a), MB, 0, st>>>(sm, an, ld, act, B, X, YP, Rout, by_sys, part);
     m_sum2_kernel<<<(a + 63) / 64, 64, 0, st>>>(a, G, act, part, out2);
     launch_counter() += 2;
 }
@@ -604,13 +671,16 @@ void launch_tm_qext_qsca(int tmo, const zd* tmat, double xv, float* tc, double* 
                                    const cpx<T>*, int, double*, BicgScalars*, int, cudaStream_t);                                   \
     template void launch_m_post<T>(const SlotMaps&, const cpx<T>*, int, int, const int*, const MultiVecs<T>&, const cpx<T>*, double*, \
                                    BicgScalars*, int, cudaStream_t);                                                                \
-    template void launch_m_upd<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, const double*, int, cudaStream_t);
+    template void launch_m_upd<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, const double*, int, cudaStream_t); \
+    template void launch_m_upd1<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, int, cudaStream_t);            \
+    template void launch_m_upd2<T>(int, int, const int*, const MultiVecs<T>&, const BicgScalars*, int, cudaStream_t);               \
+    template void launch_m_rrfix<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, int, cudaStream_t);
 INST(double)
 INST(float)
 #undef INST
 template void launch_m_resid<double>(const SlotMaps&, const zd*, int, int, const int*, const zd*, const zd*, const zd*, zd*, double*, double*,
-                                     int, cudaStream_t);
+                                     int, cudaStream_t, int);
 template void launch_m_resid<float>(const SlotMaps&, const zd*, int, int, const int*, const zd*, const zd*, const zd*, zf*, double*, double*,
-                                    int, cudaStream_t);
+                                    int, cudaStream_t, int);
 template void launch_m_addcorr<float>(int, int, const int*, const int*, zd*, const zf*, cudaStream_t);
 template void launch_m_addcorr<double>(int, int, const int*, const int*, zd*, const zd*, cudaStream_t);

@@ -25,11 +25,19 @@ void launch_m_post(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const in
 template <typename T>
 void launch_m_upd(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, const double* epsv, int nsm,
                   cudaStream_t st);   // epsv[s]: stopping threshold of system s (device)
-// FP64 true residual of system act[k]: Rout[:, k] = B - X + M YP[:, k] (rounded to TB);
-// out2[2 act[k]] = |r|^2, out2[2 act[k] + 1] = |b|^2
+// the two halves of launch_m_upd for residual replacement: x, r, q update and
+// the scalar finish with no stopping threshold (csk_prev kept), then p, w
+template <typename T>
+void launch_m_upd1(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, int nsm, cudaStream_t st);
+template <typename T> void launch_m_upd2(int ld, int a, const int* act, const MultiVecs<T>& v, const BicgScalars* sc, int nsm, cudaStream_t st);
+// residual replacement of the systems in act: csk, beta = csk / csk_prev and enorm from the replaced r
+template <typename T>
+void launch_m_rrfix(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, int nsm, cudaStream_t st);
+// FP64 true residual of system act[k]: Rout[:, k] (Rout[:, act[k]] when by_sys)
+// = B - X + M YP[:, k] (rounded to TB); out2[2 act[k]] = |r|^2, out2[2 act[k] + 1] = |b|^2
 template <typename TB>
 void launch_m_resid(const SlotMaps& sm, const zd* an, int ld, int a, const int* act, const zd* B, const zd* X, const zd* YP, cpx<TB>* Rout,
-                    double* part, double* out2, int nsm, cudaStream_t st);
+                    double* part, double* out2, int nsm, cudaStream_t st, int by_sys = 0);
 // X[:, dst[k]] += D[:, src[k]], k < a
 template <typename TL> void launch_m_addcorr(int ld, int a, const int* dst, const int* src, zd* X, const cpx<TL>* D, cudaStream_t st);
 // Y[:, k] = M X[:, k] for k < ncols (Mie multiply, idir = 1)

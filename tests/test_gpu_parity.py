@@ -269,15 +269,24 @@ def test_tmatrix_fp64(api, oracle_mod, name):
     assert abs(qe / rg["qtot"][0] - 1) < 1e-6 and abs(qs / rg["qtot"][2] - 1) < 1e-6
 
 
-def test_tmatrix_mixed(api, oracle_mod):
-    """FP32 column solves inside FP64 refinement, all columns together: the
-    orientation-averaged efficiencies within 1e-6 of the FP64 oracle."""
+@pytest.mark.parametrize("solver", [0, 1])
+def test_tmatrix_mixed(api, oracle_mod, solver):
+    """FP32 column solves with FP64 true residuals, all columns together
+    (solver 0: residual replacement, 1: restarts inside FP64 refinement): the
+    orientation-averaged efficiencies within 1e-6 of the FP64 oracle; residual
+    replacement needs at most 10 % more iterations than the FP64 column solves."""
     pos, rad, ri, em = _cluster("cluster20")
     g, o = _pair(api, oracle_mod, pos, rad, ri, em, precision="mixed")
+    g.close()
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", mixed_solver=solver)
     ro = o.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-14)
     T = g.t_matrix_order()
     rg = g.tmatrix_solution(T, solution_eps=1e-14, convergence_eps=1e-6)
     assert rg["istat"] == 0 and rg["order"] == ro["order"] and rg["outer"] >= 1
+    if solver == 0:
+        g64 = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="fp64")
+        r64 = g64.tmatrix_solution(g64.t_matrix_order(), solution_eps=1e-14, convergence_eps=1e-6)
+        assert rg["maxiter"] <= 1.1 * r64["maxiter"] + 2
     assert np.allclose(rg["qtot"], ro["qtot"], rtol=RTOL_MIXED)
     assert np.abs(rg["tmat"] - ro["tmat"]).max() <= 1e-6 * np.abs(ro["tmat"]).max()
 
