@@ -1141,6 +1141,7 @@ static int solve_mixed_rr(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, 
     if ((rc = ensure_ops(c, 1, false))) return rc;
     const zf* an32 = (const zf*)c->an32.p;
     const double drop = 1.0e-5;   // replacement once the FP32 residual fell by this factor (squared norms)
+    const double drop_soft = 1.0e-3;   // ... or by this one when the other polarisation's replacement is due
     double base[2] = {1.0, 1.0};  // true squared residual ratio at the last replacement
     bool act[2] = {true, true};
     int tot[2] = {0, 0};
@@ -1213,7 +1214,7 @@ static int solve_mixed_rr(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, 
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(c->h_sc, c->sc.p, sizeof(BicgScalars) * S, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
-        bool repl[2] = {false, false};
+        bool repl[2] = {false, false}, trigger = false;
         for (int k = 0; k < a; k++) {
             int s = slots[k];
             tot[s] = it;
@@ -1223,7 +1224,14 @@ static int solve_mixed_rr(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, 
                 continue;
             }
             double rec = c->h_sc[s].eerr * base[s];   // recursive residual relative to ||b||^2
-            if (rec < eps || c->h_sc[s].eerr < drop) repl[s] = true;
+            if (rec < eps || c->h_sc[s].eerr < drop) trigger = true;
+        }
+        // one FP64 pass serves both polarisations when the other is close to its replacement
+        for (int k = 0; k < a && trigger; k++) {
+            int s = slots[k];
+            if (!act[s]) continue;
+            double rec = c->h_sc[s].eerr * base[s];
+            if (rec < eps || c->h_sc[s].eerr < drop_soft) repl[s] = true;
         }
         if (repl[0] || repl[1]) {
             for (int s = 0; s < S; s++)

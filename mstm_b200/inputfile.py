@@ -19,6 +19,7 @@ clear error rather than ignored.
     python -m mstm_b200.inputfile run.inp [--precision fp64|mixed]
 """
 import math
+import time
 import re
 import sys
 
@@ -54,6 +55,8 @@ OPTIONS = {
     "calculate_scattering_matrix": ("l", True),
     "azimuthal_average": ("l", False),
     "scattering_map_increment": ("r", 1.0),
+    "print_sphere_data": ("l", True),
+    "normalize_s11": ("l", True),
     "store_translation_matrix": ("l", True),
     "solution_method": ("a", "iterative"),
     "t_matrix_output_file": ("a", ""),
@@ -72,6 +75,7 @@ RESTRICTED = {
     "scattering_map_model": ("i", 0),
     "single_origin_expansion": ("l", True),
     "numerical_azimuthal_average": ("l", False),
+    "interaction_radius": ("r", 1.0e10),
 }
 
 
@@ -149,6 +153,7 @@ def parse(text):
     runs inherit earlier settings, as the reference's option variables do."""
     lines = [ln.rstrip("\n") for ln in text.splitlines()]
     runs, cur = [], {k: v for k, (t, v) in OPTIONS.items()}
+    cur["_specified"] = ()
     cur.update({k: v for k, (t, v) in RESTRICTED.items()})
     spheres = []
     i = 0
@@ -186,6 +191,7 @@ def parse(text):
             continue
         if key in OPTIONS:
             cur[key] = _convert(OPTIONS[key][0], nextval())
+            cur["_specified"] = tuple(sorted(set(cur.get("_specified", ())) | {key}))
         elif key in RESTRICTED:
             cur[key] = _convert(RESTRICTED[key][0], nextval())
         else:
@@ -249,7 +255,12 @@ def execute(run, precision="fp64"):
     pos, rad, ri = cluster_arrays(run)
     med = medium_index(run)
     g = api.SphereCluster(pos, rad, ri, mie_epsilon=run["mie_epsilon"], precision=precision, medium_index=med)
-    out = dict(number_spheres=len(rad), neqns=g.number_eqns, vol_radius=g.vol_radius, medium=med)
+    out = dict(number_spheres=len(rad), neqns=g.number_eqns, vol_radius=g.vol_radius, medium=med,
+               max_mie_order=int(g.sphere_order.max()), run_number=run.get("_run_number", 1))
+    _, mqe, mqa = g.miecoefcalc()
+    from .output import mean_mie
+    out["mean_mie"] = mean_mie(rad, mqe, mqa)
+    t0 = time.perf_counter()
     try:
         if run["fft_translation_option"] and len(rad) >= run["min_fft_nsphere"]:
             d = run["d_cell"] if run["d_cell"] is not None else 0.0
@@ -259,6 +270,8 @@ def execute(run, precision="fp64"):
             T = g.t_matrix_order(trans_eps=run["translation_epsilon"], max_t_order=run["max_t_matrix_order"])
             r = g.tmatrix_solution(T, solution_eps=run["solution_epsilon"], convergence_eps=run["t_matrix_convergence_epsilon"],
                                    max_iterations=run["max_iterations"])
+            out.update(solution_time=time.perf_counter() - t0, iterations_max=r["maxiter"], error_max=r["maxerr"],
+                       t_matrix_order_estimate=T, sphere_qeff_unpol=np.asarray(r["sphere_qeff"]).T.copy())
             u = r["order"]
             nb = 2 * u * (u + 2)
             tm = np.asfortranarray(r["tmat"][:nb, :nb])
@@ -269,13 +282,14 @@ def execute(run, precision="fp64"):
                 write_tmatrix_file(run["t_matrix_output_file"], r["tmat"], T, u)
             if run["calculate_scattering_matrix"]:
                 ro = g.ranorientscatmatrix(tm, u, nangles=nangles)
-                out.update(theta=np.linspace(0.0, 180.0, nangles), smat=ro["smat"], sm_coef=ro["sm"], coherent_ratio=ro["coherent"],
-                           g_asym=ro["sm"][1, 0, 0] / (3.0 * ro["sm"][0, 0, 0]))
+                out.update(theta=np.linspace(0.0, 180.0, nangles), smat=ro["smat"], sm_coef=ro["sm"], smcf_coef=ro["smcf"],
+                           coherent_ratio=ro["coherent"], g_asym=ro["sm"][1, 0, 0] / (3.0 * ro["sm"][0, 0, 0]))
         else:
             alpha, sinc, direction = incidence(run, med)
             r = g.fixedorsoln(eps=run["solution_epsilon"], niter=run["max_iterations"], alpha=alpha, sinc=sinc, direction=direction)
             out.update(kind="fixed_orientation", qtot=r["qtot"], qeff=r["qeff"], iterations=r["iterations"], maxerr=r["maxerr"],
-                       istat=r["istat"], amnp=r["amnp"])
+                       istat=r["istat"], amnp=r["amnp"], sinc=sinc, direction=direction, solution_time=time.perf_counter() - t0,
+                       iterations_max=r["maxiter"], error_max=r["maxerr"], sphere_qeff_unpol=np.asarray(r["qeff"])[:, 0, :].T.copy())
             if run["calculate_scattering_matrix"]:
                 sc = g.scattering(r["amnp"], trans_eps=run["translation_epsilon"], max_t_order=run["max_t_matrix_order"],
                                   nangles=nangles)
@@ -325,12 +339,16 @@ def main(argv=None):
     a = ap.parse_args(argv)
     with open(a.input) as f:
         runs = parse(f.read())
+    from .output import write_output
+    written = set()
     for k, run in enumerate(runs):
+        run = dict(run, _run_number=k + 1)
         out = execute(run, a.precision)
-        text = report(out)
-        print(text)
-        with open(run["output_file"], "a" if k else "w") as f:
-            f.write(text + "\n")
+        print(report(out))
+        # the output file in the reference's layout (print_run_variables +
+        # print_calculation_results), one block per run
+        write_output(run["output_file"], [(run, out)], append=run["output_file"] in written)
+        written.add(run["output_file"])
 
 
 if __name__ == "__main__":

@@ -79,3 +79,59 @@ def test_deck_runs_match_oracle(oracle_mod, tmp_path):
     assert rand["t_matrix_order"] == rt["order"]
     assert np.allclose(rand["qtot"], rt["qtot"], rtol=1e-9)
     assert "asymmetry parameter" in I.report(rand) and "efficiencies" in I.report(fixed)
+    # the reference-layout output file of both runs
+    from mstm_b200.output import write_output, es
+    p = tmp_path / "out.dat"
+    write_output(str(p), [(dict(runs[0], _run_number=1), fixed), (dict(runs[1], _run_number=2), rand)])
+    text = p.read_text().splitlines()
+    assert text.count(" calculation results for run ") == 2
+    i = text.index(" total extinction, absorption, scattering efficiencies (unpol, par, perp incidence)")
+    assert text[i + 1][:12] == es(ro["qtot"][0, 0])
+    i = text.index(" total extinction, absorption, scattering efficiencies (unpolarized incidence)")
+    assert text[i + 1][:12] == es(rt["qtot"][0])
+
+
+def test_fortran_edit_descriptors():
+    from mstm_b200.output import es, fd, iw
+    assert es(0.0) == "  0.0000E+00" and es(-1.0) == " -1.0000E+00" and es(12.3456789) == "  1.2346E+01"
+    assert es(9.99996) == "  1.0000E+01" and es(1.0e100) == "  1.0000+100" and es(-2.5e-101) == " -2.5000-101"
+    assert es(1.23456789, 15, 7) == "  1.2345679E+00" and es(5.0, 14, 6) == "  5.000000E+00"
+    assert fd(-180.0, 8, 2) == " -180.00" and fd(3.14159, 8, 3) == "   3.142" and iw(42, 6) == "    42"
+
+
+def test_output_blocks_layout():
+    """The run-variable and result blocks in the reference's record layout
+    (labels, record order, field widths) for a synthetic fixed-orientation
+    and random-orientation result."""
+    from mstm_b200 import output as O
+    run = I.parse(DECK)[0]
+    n = 3
+    fixed = dict(kind="fixed_orientation", run_number=1, neqns=210, max_mie_order=5, mean_mie=(2.0, 0.1), vol_radius=1.44,
+                 sinc=0.0, direction=1, t_matrix_order=8, iterations_max=12, error_max=3e-13, solution_time=0.01,
+                 sphere_qeff_unpol=np.ones((n, 3)), qtot=np.arange(9.0).reshape(3, 3, order="F") + 1,
+                 theta=np.linspace(-180, 180, 361), smat=np.tile(np.eye(4), (361, 1, 1)))
+    L = O.run_variables(run, fixed) + O.calculation_results(run, fixed)
+    assert L[0] == "*" * 52 and L[1] == " input variables for run     1"
+    i = L.index(" number spheres")
+    assert L[i + 1] == "      3"
+    i = L.index(" calculation results for run ")
+    assert L[i + 1].strip() == "1"
+    i = L.index(" number iterations, error, solution time ")
+    assert L[i + 1] == "    12  3.0000E-13  1.0000E-02"
+    i = L.index(" total extinction, absorption, scattering efficiencies (unpol, par, perp incidence)")
+    assert L[i + 1] == "".join(O.es(v) for v in range(1, 10))
+    i = L.index(" scattering matrix in incident plane: 0 deg= z axis")
+    assert L[i + 2] == "   361    16" and L[i + 3].startswith("   theta     11          12     ")
+    assert L[i + 4].startswith(" -180.00") and len(L[i + 4]) == 8 + 16 * 12
+    # S11 scaled by 1/(pi r^2 Qsca), the rest divided by S11
+    assert abs(float(L[i + 4][8:20]) - 1.0 / (1.44 ** 2 * O.REF_PI * 3.0)) < 1e-4 / (1.44 ** 2 * O.REF_PI * 3.0)
+    rnd = dict(fixed, kind="random_orientation", t_matrix_order_estimate=9, qtot=np.array([3.0, 0.5, 2.5]),
+               theta=np.linspace(0, 180, 181), smat=np.tile(np.eye(4), (181, 1, 1)),
+               sm_coef=np.ones((17, 4, 4)), smcf_coef=np.ones((17, 4, 4)))
+    rrun = I.parse(DECK)[1]
+    L = O.run_variables(rrun, rnd) + O.calculation_results(rrun, rnd)
+    assert " random orientation, estimated t matrix order:" in L and " calculated t matrix order:" in L
+    i = L.index(" total scattering")
+    assert L[i + 2] == "   181     6" and L[i + 3] == "   theta     11          12          22          33          34          44     "
+    i = L.index(" orientation averaged scattering matrix expansion coefficients")
+    assert L[i + 2] == "    0" + O.es(1.0, 14, 6) * 6 and len(L) == i + 2 + 17 + 2 + 17
