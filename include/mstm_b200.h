@@ -120,6 +120,12 @@ int mstmg_fixed_orientation(mstmg_ctx *ctx, double alpha, double sinc, int dir, 
 int mstmg_scattering(mstmg_ctx *ctx, const double *amnp, double trans_eps, int max_t_order, int nangles, double *smat, double *g,
                      int *t_matrix_order, double *amnp0, int amnp0_cap);
 
+/* The GSF expansion of the azimuth-averaged scattering matrix of a
+ * common-origin expansion (fosmexpansion, mstm-scatprops-26.f90:1820-1951):
+ * coef = s00, s02, sp22, sm22 in turn, each 16 x (2T+1) (Fortran sm(4,4) per
+ * degree w = 0..2T).  amnp0 as for mstmg_scattering_plane. */
+int mstmg_gsf_coefficients(mstmg_ctx *ctx, int t_matrix_order, const double *amnp0, double *coef);
+
 /* The scattering matrix of the common-origin expansion at single directions,
  * without azimuthal averaging (azimuthal_average = .false., the reference's
  * default for fixed orientation): scatteringmatrix

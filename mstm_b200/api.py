@@ -172,6 +172,17 @@ class SphereCluster:
                                              _ptr(x), _ptr(y)), "translation_pass")
         return y
 
+    def gsf_coefficients(self, amnp0, t_matrix_order):
+        """fosmexpansion of a common-origin expansion: dict(s00, s02, sp22, sm22),
+        each (2T+1, 4, 4) [w][i][j]."""
+        T = int(t_matrix_order)
+        W = 2 * T + 1
+        a0 = np.asfortranarray(amnp0, np.complex128)
+        coef = np.zeros(4 * 16 * W)
+        check(self._L.mstmg_gsf_coefficients(self.ctx, T, _ptr(a0), _ptr(coef)), "gsf_coefficients")
+        c = coef.reshape(4, W, 4, 4).transpose(0, 1, 3, 2)
+        return dict(s00=c[0].copy(), s02=c[1].copy(), sp22=c[2].copy(), sm22=c[3].copy())
+
     def scattering_plane(self, amnp0, t_matrix_order, increment=1.0, alpha=0.0, rotate_plane=False):
         """Scattering matrix without azimuthal averaging (scatteringmatrix,
         mstm-scatprops-26.f90:1498-1573, normalize_s11 false) at the directions

@@ -1631,6 +1631,32 @@ extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_e
     return check_kernel_err(c);
 }
 
+extern "C" int mstmg_gsf_coefficients(mstmg_ctx* c, int t_matrix_order, const double* amnp0, double* coef)
+{
+    const int T = t_matrix_order;
+    if (!c || !amnp0 || !coef || T < 1 || T > 200) {
+        set_err("mstmg_gsf_coefficients: bad arguments");
+        return MSTMG_ERR_ARG;
+    }
+    BigTablesDev bt;
+    int rc = upload_big(c, bt);
+    if (rc) return rc;
+    const size_t nb0 = 2 * (size_t)T * (T + 2);
+    const int W = 2 * T + 1;
+    DevBuf<zd> da0;
+    DevBuf<double> ds, fscr;
+    CK(da0.alloc(2 * nb0));
+    CK(copy_in(da0.p, amnp0, sizeof(zd) * 2 * nb0, c->st));
+    CK(ds.alloc(4 * 16 * (size_t)W));
+    CK(cudaMemsetAsync(ds.p, 0, sizeof(double) * 4 * 16 * (size_t)W, c->st));
+    CK(fscr.alloc(fosm_scratch_doubles(T)));
+    launch_fosm(T, da0.p, bt.bc.p, bt.fnr.p, bt.nbc, ds.p, ds.p + 16 * W, ds.p + 32 * W, ds.p + 48 * W, fscr.p, c->st);
+    CK(cudaGetLastError());
+    CK(copy_out(coef, ds.p, sizeof(double) * 4 * 16 * (size_t)W, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return check_kernel_err(c);
+}
+
 extern "C" int mstmg_scattering_plane(mstmg_ctx* c, int t_matrix_order, const double* amnp0, int ldim, int udim, double amin, double amax,
                                       double alpha, int rotate_plane, double* sm)
 {

@@ -295,7 +295,8 @@ def execute(run, precision="fp64"):
                                   nangles=nangles)
                 out.update(g_asym=sc["g"], t_matrix_order=sc["t_matrix_order"])
                 if run["azimuthal_average"]:
-                    out.update(theta=np.linspace(0.0, 180.0, nangles), smat=sc["smat"])
+                    out.update(theta=np.linspace(0.0, 180.0, nangles), smat=sc["smat"],
+                               gsf=g.gsf_coefficients(sc["amnp0"], sc["t_matrix_order"]))
                 else:
                     theta, sm = g.scattering_plane(sc["amnp0"], sc["t_matrix_order"], increment=run["scattering_map_increment"],
                                                    alpha=alpha)

@@ -3,9 +3,7 @@ block of print_run_variables (mstm-input-37.f90:3137-3304) and the results
 block of print_calculation_results (mstm-input-37.f90:3340-3751), with the
 same labels, record order and Fortran edit descriptors, for the branches this
 library covers (no plane boundaries, periodic lattices, configuration or
-incidence averages, near fields or Gaussian beams).  The one block left out is
-the table of azimuth-averaged expansion coefficients that follows an
-azimuth-averaged fixed-orientation scattering matrix.
+incidence averages, near fields or Gaussian beams).
 """
 import math
 
@@ -181,6 +179,15 @@ def calculation_results(run, out):
             smt = scaled_scat_mat(np.asarray(sm[i]).reshape(4, 4).T.reshape(16))   # Fortran sm(4,4) order
             smt[0] *= s11scale
             L.append(fd(theta[i], 8, 2) + "".join(es(smt[k - 1]) for k in vec))
+        if (not random) and run["azimuthal_average"] and "gsf" in out:
+            c = out["gsf"]   # (2T+1, 4, 4) [w][i][j] each
+            L += [label("azimuthal averaged scattering matrix expansion coefficients, total field"),
+                  "    n         11            44            12            34           22p           22m"]
+            for nn in range(c["s00"].shape[0]):
+                L.append(iw(nn, 5) + es(c["s00"][nn, 0, 0], 14, 6) + es(c["s00"][nn, 3, 3], 14, 6)
+                         + es(0.5 * (c["s02"][nn, 1, 0] + c["s02"][nn, 0, 1]), 14, 6)
+                         + es(0.5 * (c["s02"][nn, 3, 2] + c["s02"][nn, 2, 3]), 14, 6)
+                         + es(c["sp22"][nn, 1, 1], 14, 6) + es(c["sm22"][nn, 1, 1], 14, 6))
         if random:
             hdr = "    n         11            44            12            34           22            33"
             for title, key in (("orientation averaged scattering matrix expansion coefficients", "sm_coef"),

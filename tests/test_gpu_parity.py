@@ -226,6 +226,22 @@ def test_scattering_postprocessing(api, oracle_mod, name):
     assert abs(sgm["g"] - so["g"]) <= 1e-6
 
 
+def test_gsf_coefficients(api, oracle_mod):
+    """fosmexpansion on the device (the azimuth-averaged expansion the output
+    file tabulates) against the oracle, same common-origin expansion."""
+    pos, rad, ri, em = _cluster("cluster20")
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em)
+    ro = o.fixedorsoln(eps=1e-12, niter=4000)
+    sg = g.scattering(ro["amnp"])
+    T = sg["t_matrix_order"]
+    c = g.gsf_coefficients(sg["amnp0"], T)
+    so = oracle_mod.gsf_scattering(T, sg["amnp0"], nangles=3)
+    W = 2 * T + 1
+    for k in ("s00", "s02", "sp22", "sm22"):
+        ref = np.asarray(so[k]).reshape(W, 4, 4).transpose(0, 2, 1)
+        assert np.abs(c[k] - ref).max() <= 1e-11 * np.abs(ref).max(), k
+
+
 @pytest.mark.parametrize("alpha,rotate", [(0.0, False), (0.4, True)])
 def test_incident_plane_scattering(api, oracle_mod, alpha, rotate):
     """scatteringmatrix over the directions scattering_matrix_calculation uses

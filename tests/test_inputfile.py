@@ -72,8 +72,14 @@ def test_deck_runs_match_oracle(oracle_mod, tmp_path):
     assert np.abs(fixed["smat"] - sm).max() <= 1e-8 * np.abs(sm[:, 0, 0]).max()
     avg = dict(runs[0], azimuthal_average=True, scattering_map_increment=5.0)
     fa = I.execute(avg, "fp64")
-    ga = oracle_mod.gsf_scattering(sc["t_matrix_order"], sc["amnp0"], nangles=37)["smat"]
+    gs = oracle_mod.gsf_scattering(sc["t_matrix_order"], sc["amnp0"], nangles=37)
+    ga = gs["smat"]
     assert fa["smat"].shape == (37, 4, 4) and np.abs(fa["smat"] - ga).max() <= 1e-8 * np.abs(ga[:, 0, 0]).max()
+    from mstm_b200.output import calculation_results, es
+    L = calculation_results(avg, fa)
+    i = L.index(" azimuthal averaged scattering matrix expansion coefficients, total field")
+    assert L[i + 2][:33] == "    0" + es(gs["s00"][0], 14, 6) + es(gs["s00"][15], 14, 6)
+    assert len(L) == i + 2 + 2 * sc["t_matrix_order"] + 1
     rand = I.execute(runs[1], "fp64")
     rt = o.tmatrix_solution(convergence_eps=1e-8, solution_eps=1e-12)
     assert rand["t_matrix_order"] == rt["order"]
