@@ -323,6 +323,17 @@ def run_extras(args, dev, stream):
     seq = EN.solve_ensemble(cfgs, precision="mixed", workers=1, solution_eps=1e-12)
     tuner = EN.Autotuner(reps=2)
     bat = EN.solve_ensemble(cfgs, precision="mixed", workers=4, tuner=tuner, solution_eps=1e-12)
+    # many small fixed-orientation configurations: one at a time against four streams
+    rng = np.random.default_rng(11)
+    small = [C.rsa_sphere(int(rng.integers(15, 41)), 1.0, 0.10, seed=300 + k)[0] for k in range(48)]
+    EN.solve_fixed_ensemble(small[:4], 1.0, 1.5 + 0.01j, workers=1)
+    f1 = EN.solve_fixed_ensemble(small, 1.0, 1.5 + 0.01j, workers=1)
+    f4 = EN.solve_fixed_ensemble(small, 1.0, 1.5 + 0.01j, workers=4)
+    out["ensemble_fixed_small"] = {
+        "workload": "48 configurations, 15-40 spheres (seeded), x=1.0, m=1.5+0.01i, RSA at fv 0.10: fixed orientation, "
+                    "both polarisations to residual 1e-6 (mixed precision)",
+        "metric": "solves/s", "one_at_a_time": round(f1["solves_per_s"], 1), "four_streams": round(f4["solves_per_s"], 1),
+        "qext_rel_diff": abs(f4["qext_mean"] / f1["qext_mean"] - 1)}
     out["ensemble_tmatrix"] = {
         "workload": "6 configurations, 50-150 spheres (seeded), x=1.5, m=1.6+0.005i, RSA at fv 0.20: cluster T matrices, "
                     "orientation-averaged Qext/Qsca and scattering matrix, ensemble means",

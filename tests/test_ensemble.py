@@ -28,3 +28,16 @@ def test_ensemble_concurrent_autotuned_matches_sequential_and_oracle(oracle_mod)
     nb = 2 * u * (u + 2)
     rr = oracle_mod.ranorientscatmatrix(u, np.asfortranarray(ro["tmat"][:nb, :nb]))
     assert np.abs(seq[0]["smat"] - rr["smat"]).max() <= 1e-8 * np.abs(rr["smat"][:, 0, 0]).max()
+
+
+def test_fixed_ensemble_concurrent_matches_fp64():
+    """Concurrent mixed-precision fixed-orientation solves of small clusters
+    (four streams) give the efficiencies of one-at-a-time FP64 solves."""
+    from mstm_b200 import ensemble as E
+    from mstm_b200 import configs as C
+    pos = [C.rsa_sphere(n, 1.0, 0.10, seed=200 + n)[0] for n in (12, 18, 25, 31, 16, 22)]
+    ens = E.solve_fixed_ensemble(pos, 1.0, 1.5 + 0.01j, precision="mixed", workers=4)
+    seq = E.solve_fixed_ensemble(pos, 1.0, 1.5 + 0.01j, precision="fp64", workers=1)
+    for a, b in zip(ens["per_config"], seq["per_config"]):
+        assert a["istat"] == 0 and b["istat"] == 0
+        assert np.allclose(a["qtot"], b["qtot"], rtol=1e-6)
