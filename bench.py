@@ -4,9 +4,12 @@ interaction solve on B200.
 Workload (one step = one solve): a seeded particle-cluster fractal aggregate,
 500 touching monomers, x = 2.0, m = 1.6+0.05i, Df = 1.8, kf = 1.3, incidence
 along +z, both polarisations, direct pair translation, sphere order L = 9
-(neqns = 99,000, 124,750 pairs).  A solve = pair-operator generation + incident
-coefficients + both polarisations solved to ||r||/||b|| < 1e-6 (MSTM
-solution_epsilon = 1e-12 in its squared-norm test) + efficiencies.
+(neqns = 99,000, 124,750 pairs).  A solve = incident coefficients + both
+polarisations solved to ||r||/||b|| < 1e-6 (MSTM solution_epsilon = 1e-12 in
+its squared-norm test) + efficiencies, on a context whose pair operators were
+generated in the warm-up (`value`); the end-to-end number (`e2e`) adds, every
+step, the positions copied in from pinned host memory, which regenerates the
+pair operators, and the solution and efficiencies copied back.
 
 Arms:
   default            tuned path (mixed precision, polarisations batched), with
@@ -500,6 +503,28 @@ def run_translation_case(args):
     g.close()
 
 
+def run_tmatrix_case(args):
+    """One cluster T matrix of the seeded `--tmatrix-case`-sphere cluster
+    (x = 1.5, m = 1.6+0.005i, RSA at fv 0.20, residual 1e-6), after one
+    untimed solve (the case the T-matrix launch-list capture uses)."""
+    import time
+    from mstm_b200 import _lib, api, configs as C
+    n = args.tmatrix_case
+    pos, _ = C.rsa_sphere(n, 1.5, 0.20, seed=4)
+    g = api.SphereCluster(pos, np.full(n, 1.5), np.full(n, 1.6 + 0.005j), mie_epsilon=-C.truncation_order(1.5),
+                          precision=args.precision)
+    T = g.t_matrix_order()
+    g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6)
+    L = _lib.lib()
+    l0 = L.mstmg_kernel_launches()
+    t0 = time.perf_counter()
+    r = g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6)
+    dt = time.perf_counter() - t0
+    print(json.dumps({"spheres": n, "precision": args.precision, "t_matrix_order": T, "order": r["order"], "s": dt,
+                      "launches": L.mstmg_kernel_launches() - l0, "maxiter": r["maxiter"], "outer": r["outer"]}))
+    g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -515,9 +540,12 @@ def main():
     ap.add_argument("--fp32-chunk", type=int, default=0, help="profiling case: FP32 column chunk (2 or 4; 0 default)")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="profiling case: tiled kernel CTAs per SM (0 default)")
     ap.add_argument("--nrhs", type=int, default=4)
+    ap.add_argument("--tmatrix-case", type=int, default=0, help="profiling case: one T matrix of this many spheres")
     args = ap.parse_args()
     if args.translation_passes:
         run_translation_case(args)
+    elif args.tmatrix_case:
+        run_tmatrix_case(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
