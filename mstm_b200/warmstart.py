@@ -4,9 +4,10 @@ A message-passing network over each sphere's k nearest neighbours predicts the
 sphere's interaction correction Delta a_i = a_i - a_i^0 to its isolated-sphere
 solution a_i^0 = Mie_i f_i (the reference's BiCG initial guess, fixedorsoln,
 mstm-solver-8.f90:482-483).  The BiCG then starts from a^0 + Delta a; a
-polarisation whose initial relative residual exceeds `fallback` (0.1) starts
-from a^0 as the reference does (mstmg_fixed_orientation_guess), so the
-converged residual, not the network, decides the answer.
+polarisation whose initial relative residual ||r||/||b|| exceeds `fallback`
+(default 1, the residual of a zero start) starts from a^0 as the reference
+does (mstmg_fixed_orientation_guess), so the converged residual, not the
+network, decides the answer.
 
 Network (sizes as in the cluster-ensemble study this targets):
   node features (41): x, Re m, log10 Im m, volume fraction, N/300, and the
@@ -455,7 +456,7 @@ def predict_guess(net, sample):
     return x0
 
 
-def solve_with_guess(cfg, x0, eps=1e-12, precision="mixed", fallback=0.1):
+def solve_with_guess(cfg, x0, eps=1e-12, precision="mixed", fallback=1.0):
     """Fixed-orientation solve from x0 (falls back per polarisation to the Mie start)."""
     g = solver_pair(cfg, precision)
     L = _lib.lib()
@@ -475,7 +476,7 @@ def solve_with_guess(cfg, x0, eps=1e-12, precision="mixed", fallback=0.1):
     return dict(amnp=amnp, qtot=qtot.reshape(3, 3, order="F"), used=used.tolist(), guess_residual=res.tolist(), **stats)
 
 
-def study(n_train=200, n_eval=16, epochs=60, seed=5, device=None, fallback=0.1, log=print):
+def study(n_train=200, n_eval=16, epochs=60, seed=5, device=None, fallback=1.0, log=print):
     """Generate, train, evaluate: the warm-start study on configurations drawn
     as sample_config draws them.  Returns a summary dict (iterations and
     initial residuals with and without the guess, timing, fallbacks)."""
@@ -494,7 +495,7 @@ def study(n_train=200, n_eval=16, epochs=60, seed=5, device=None, fallback=0.1, 
     t_train = time.time() - t0
     out = dict(n_train=n_train, n_eval=n_eval, epochs=epochs, gen_s=round(t_gen, 1), train_s=round(t_train, 1),
                loss_first=hist[0], loss_last=hist[-1])
-    for fb_name, fb in (("spec_fallback", fallback), ("guess_always", 10.0)):
+    for fb_name, fb in (("with_fallback", fallback), ("guess_always", 10.0)):
         it_p = it_w = nfb = 0
         rp_l, rw_l = [], []
         for s in held:
@@ -521,6 +522,6 @@ if __name__ == "__main__":
     ap.add_argument("--train", type=int, default=500)
     ap.add_argument("--eval", type=int, default=16)
     ap.add_argument("--epochs", type=int, default=150)
-    ap.add_argument("--fallback", type=float, default=0.1)
+    ap.add_argument("--fallback", type=float, default=1.0)
     a = ap.parse_args()
     print(json.dumps(study(a.train, a.eval, a.epochs, fallback=a.fallback, log=None)))
