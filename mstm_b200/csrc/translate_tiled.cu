@@ -203,26 +203,48 @@ __global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
         __syncthreads();
         const cpx<T>* e = ephm + L;
 
-        // ---- A: shift, phase, even/odd split of the staged sources ----
-        for (int idx = tid; idx < C * NS; idx += NT) {
-            const int c = idx / NS, jj = idx - c * NS;
-            const short2 nm = tabS[jj];
-            const int n = nm.x, m = nm.y;
-            const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
-            const bool swp = (dir != (int)((a.contran >> r) & 1u));
-            const cpx<T>* xs = W2 + (size_t)(dir * NR + r) * NB + p * NB2;
-            cpx<T>* st = W1 + c * NB2;
-            cpx<T> u = xs[hidx<L>(m, n)];
-            if (m == 0) {
-                st[sofs(n)] = (T)2 * u;
-            } else {
-                cpx<T> v = xs[hidx<L>(-m, n)];
-                const T sg = (m & 1) ? (T)-1 : (T)1;
-                if (swp) { cpx<T> tt = u; u = sg * v; v = sg * tt; }
-                const int im = dir ? -m : m;
-                cpx<T> uu = u * e[im], vv = v * e[-im];
-                st[sofs(n) + m] = uu + sg * vv;
-                st[NS + tofs(n) + m - 1] = uu - sg * vv;
+        // ---- A: shift, phase, even/odd split of the staged sources.  Each
+        //      thread takes IA items; all their loads are issued before any
+        //      arithmetic, so the shared-memory latencies overlap ----
+        {
+            constexpr int NA = C * NS, IA = (NA + NT - 1) / NT;
+            cpx<T> U[IA], V[IA], EU[IA];
+            int sdst[IA], tdst[IA], mm[IA];   // S and T slots; m, with the shift flag as -m-1
+#pragma unroll
+            for (int k = 0; k < IA; k++) {
+                const int idx = tid + k * NT;
+                sdst[k] = -1;
+                if (idx < NA) {
+                    const int c = idx / NS, jj = idx - c * NS;
+                    const short2 nm = tabS[jj];
+                    const int n = nm.x, m = nm.y;
+                    const int r = (c >> 1) % NR, dir = (c >> 1) / NR;
+                    const bool swp = (dir != (int)((a.contran >> r) & 1u));
+                    const cpx<T>* xs = W2 + (size_t)c * NB2;
+                    const int hp = hidx<L>(m, n), hm = m ? hidx<L>(-m, n) : hp;
+                    // with the shift the +m and -m sources trade places (and take the sign (-1)^m)
+                    U[k] = xs[swp ? hm : hp];
+                    V[k] = xs[swp ? hp : hm];
+                    EU[k] = e[dir ? -m : m];
+                    sdst[k] = c * NB2 + sofs(n) + m;
+                    tdst[k] = c * NB2 + NS + tofs(n) + m - 1;
+                    mm[k] = swp ? -m - 1 : m;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < IA; k++) {
+                if (sdst[k] < 0) continue;
+                const bool swp = mm[k] < 0;
+                const int m = swp ? -mm[k] - 1 : mm[k];
+                if (m == 0) {
+                    W1[sdst[k]] = (T)2 * U[k];
+                } else {
+                    const T sg = (m & 1) ? (T)-1 : (T)1;
+                    const T s2 = swp ? sg : (T)1;
+                    const cpx<T> uu = (s2 * U[k]) * EU[k], vv = (s2 * V[k]) * cj(EU[k]);
+                    W1[sdst[k]] = uu + sg * vv;
+                    W1[tdst[k]] = uu - sg * vv;
+                }
             }
         }
         __syncthreads();
