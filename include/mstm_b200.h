@@ -264,6 +264,14 @@ int mstmg_operator_bytes(const mstmg_ctx *ctx, int prec, double *stored_bytes, d
  * operators and kernels the solvers use; FP32 results are returned widened. */
 int mstmg_translation_pass(mstmg_ctx *ctx, int prec, int ncols, const int *con_tran, const double *x, double *y);
 
+/* Diagnostic, no counterpart in the reference: runs the bounded mbarrier
+ * wait that the translation kernels use on a barrier that no copy ever
+ * completes, with `limit` polls per thread (1 .. 4194304, the kernels' own
+ * limit), and stores the status the kernel records: MSTMG_ERR_CUDA when the
+ * wait gave up.  Returns MSTMG_OK when the launch ran and the device is still
+ * usable afterwards. */
+int mstmg_selftest_bounded_wait(int device, int limit, int *status);
+
 /* Time `reps` translation passes (nrhs right-hand sides, FP64 or FP32) with CUDA
  * events on the context stream; returns the average milliseconds per pass. */
 int mstmg_time_translation(mstmg_ctx *ctx, int prec, int nrhs, int reps, double *ms_per_pass);

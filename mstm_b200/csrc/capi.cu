@@ -18,6 +18,7 @@
 #include "ranorient.cuh"
 #include "fftpath.cuh"
 #include "densepair.cuh"
+#include <nvtx3/nvToolsExt.h>
 #include <cufft.h>
 #include <memory>
 #include <algorithm>
@@ -92,6 +93,15 @@ struct FftState {
                 }
     }
     ~FftState() { drop_plans(); }
+};
+
+// NVTX range over a C-ABI call or a pass, visible in Nsight timelines (a
+// no-op unless a tool is attached)
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
 struct mstmg_ctx {
@@ -467,6 +477,17 @@ extern "C" int mstmg_ctx_create(mstmg_ctx** out, int nsphere, const double* pos,
         return MSTMG_ERR_ARG;
     }
     *out = nullptr;
+    if (!is_dev(pos) && !is_dev(radius) && !is_dev(ref_index)) {
+        // host inputs are checked before anything reaches the GPU
+        for (int i = 0; i < nsphere; i++) {
+            bool ok = std::isfinite(radius[i]) && radius[i] > 0.0 && std::isfinite(ref_index[2 * i]) && std::isfinite(ref_index[2 * i + 1]);
+            for (int k = 0; k < 3; k++) ok = ok && std::isfinite(pos[3 * (size_t)i + k]);
+            if (!ok) {
+                set_err("mstmg_ctx_create: sphere " + std::to_string(i + 1) + " has a non-finite position or index, or a radius <= 0");
+                return MSTMG_ERR_ARG;
+            }
+        }
+    }
     mstmg_ctx* c = new mstmg_ctx();
     if (opts) c->opts = *opts;
     else mstmg_default_opts(&c->opts);
@@ -564,6 +585,12 @@ extern "C" void mstmg_ctx_destroy(mstmg_ctx* c)
 extern "C" int mstmg_ctx_set_positions(mstmg_ctx* c, const double* pos)
 {
     if (!c || !pos) return MSTMG_ERR_ARG;
+    if (!is_dev(pos))
+        for (int k = 0; k < 3 * c->n; k++)
+            if (!std::isfinite(pos[k])) {
+                set_err("mstmg_ctx_set_positions: non-finite position of sphere " + std::to_string(k / 3 + 1));
+                return MSTMG_ERR_ARG;
+            }
     CK(copy_in(c->pos.p, pos, sizeof(double) * 3 * c->n, c->st));
     if (is_dev(pos)) CK(cudaMemcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n, cudaMemcpyDeviceToHost));
     else memcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n);
@@ -650,6 +677,7 @@ static int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
     }
     if (need64) CK(c->op64.alloc(c->op_units));
     if (need32) CK(c->op32.alloc(c->op_units));
+    NvtxRange nvtx_("pair operator generation");
     OpGenArgs a;
     a.npairs = c->npairs;
     a.pairs = c->pairs.p;
@@ -685,6 +713,7 @@ template <> const float* ops_ptr<float>(mstmg_ctx* c) { return c->op32.p; }
 // only on the tiled path: contran then applies to column r of every chunk.
 template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran, int nchunk = 1)
 {
+    NvtxRange nvtx_(sizeof(T) == 8 ? "translation pass FP64" : "translation pass FP32");
     CK(cudaMemsetAsync(y, 0, sizeof(cpx<T>) * (size_t)c->neqns * nrhs * nchunk, c->st));
     if (c->ndense > 0) {
         if (nchunk > 1) return MSTMG_ERR_UNSUPPORTED;
@@ -829,6 +858,7 @@ template <typename T> static int translate_many(mstmg_ctx* c, const cpx<T>* x, c
 extern "C" int mstmg_interaction(mstmg_ctx* c, int nrhs, const double* ain, double* aout, const int* con_tran, const int* mie_mult,
                                  int initial_run)
 {
+    NvtxRange nvtx_("mstmg_interaction");
     if (!c || nrhs < 1 || nrhs > 4 || !ain || !aout) {
         set_err("mstmg_interaction: bad arguments (nrhs must be 1..4)");
         return MSTMG_ERR_ARG;
@@ -1004,6 +1034,7 @@ static int oos_solve(mstmg_ctx* c, const zd* b, zd* x, int niter, double eps, in
 
 extern "C" int mstmg_bicg(mstmg_ctx* c, int niter, double eps, const double* pnp, double* anp, int initialize, int* iter, double* err)
 {
+    NvtxRange nvtx_("mstmg_bicg");
     if (!c || !pnp || !anp) return MSTMG_ERR_ARG;
     int rc = ensure_ops(c, 0, initialize != 0);
     if (rc) return rc;
@@ -1017,6 +1048,16 @@ extern "C" int mstmg_bicg(mstmg_ctx* c, int niter, double eps, const double* pnp
     if (niter == 0) {
         set_err("mstmg_bicg: niter = 0 (the reference's Mie-multiply-only mode) is not on this path");
         return MSTMG_ERR_UNSUPPORTED;
+    }
+    // a zero right-hand side returns at once, anp untouched (cbicg, solver:694)
+    launch_rr_dot_norm(ne, c->bvec64.p, c->part.p, c->small.p, c->nsm, c->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->h_small, c->small.p, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (c->h_small[0] == 0.0) {
+        if (iter) *iter = 0;
+        if (err) *err = 0.0;
+        return MSTMG_OK;
     }
     if (niter < 0) rc = oos_solve(c, c->bvec64.p, v.x, niter, eps, &it, &e);
     else rc = bicg_batched<double>(c, 1, bb, &v, true, niter, &eps, &it, &e, &st);
@@ -1279,6 +1320,7 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
 extern "C" int mstmg_fixed_orientation(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, double* amnp,
                                        double* qeff, double* qtot, double* maxerr, int* maxiter)
 {
+    NvtxRange nvtx_("mstmg_fixed_orientation");
     return fixed_orientation_impl(c, alpha, sinc, dir, eps, niter, nullptr, 0.0, nullptr, nullptr, amnp, qeff, qtot, maxerr, maxiter);
 }
 
@@ -1573,6 +1615,7 @@ static MergeArgs merge_args(mstmg_ctx* c, const RegTables& rt, const BigTablesDe
 extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_eps, int max_t_order, int nangles, double* smat,
                                 double* g, int* t_matrix_order, double* amnp0, int amnp0_cap)
 {
+    NvtxRange nvtx_("mstmg_scattering");
     if (!c || !amnp || nangles < 2 || max_t_order < 1) {
         set_err("mstmg_scattering: bad arguments");
         return MSTMG_ERR_ARG;
@@ -2035,6 +2078,7 @@ extern "C" int mstmg_t_matrix_order(mstmg_ctx* c, double trans_eps, int max_t_or
 extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_eps, double convergence_eps, int max_iterations,
                              double* tmat, double* sphere_qeff, double* qtot, int* order_used, int* maxiter, double* maxerr)
 {
+    NvtxRange nvtx_("mstmg_tmatrix");
     if (!c || t_matrix_order < 1 || t_matrix_order > 200 || !tmat || max_iterations < 1) {
         set_err("mstmg_tmatrix: bad arguments (1 <= t_matrix_order <= 200, max_iterations >= 1, tmat required)");
         return MSTMG_ERR_ARG;
@@ -2205,6 +2249,7 @@ extern "C" int mstmg_tmatrix_qext_qsca(mstmg_ctx* c, int t_matrix_order, const d
 extern "C" int mstmg_ranorient_scattering(mstmg_ctx* c, int t_matrix_order, const double* tmat, int nangles, double* sm, double* smcf,
                                           double* smat)
 {
+    NvtxRange nvtx_("mstmg_ranorient_scattering");
     const int T = t_matrix_order;
     if (!c || T < 1 || T > 60 || !tmat || (nangles > 0 && nangles < 2)) {
         set_err("mstmg_ranorient_scattering: bad arguments (1 <= t_matrix_order <= 60, nangles 0 or >= 2)");
@@ -2532,6 +2577,7 @@ static int fft_build(mstmg_ctx* c)
 extern "C" int mstmg_fft_setup(mstmg_ctx* c, double cell_volume_fraction, double d_cell, int node_order, int neighbor_node_model,
                                int* cell_dim, double* d_cell_out, int* node_order_out, int* near_pairs)
 {
+    NvtxRange nvtx_("mstmg_fft_setup");
     if (!c || c->n < 2 || neighbor_node_model < 0 || neighbor_node_model > 2) {
         set_err("mstmg_fft_setup: bad arguments (two or more spheres, neighbor_node_model 0..2)");
         return MSTMG_ERR_ARG;
@@ -2592,8 +2638,32 @@ extern "C" long long mstmg_kernel_launches(void) { return launch_counter().load(
 // One translation pass over nrhs columns laid out as BiCG packs them
 // ([p, A^T conj w] pairs, odd columns conjugate-transpose products), timed with
 // CUDA events on the context's stream (mean of reps after one warm-up).
+extern "C" int mstmg_selftest_bounded_wait(int device, int limit, int* status)
+{
+    if (!status || limit < 1 || limit > (1 << 22)) {
+        set_err("mstmg_selftest_bounded_wait: bad arguments (limit 1..4194304)");
+        return MSTMG_ERR_ARG;
+    }
+    CK(cudaSetDevice(device));
+    int* d = nullptr;
+    CK(cudaMalloc((void**)&d, sizeof(int)));
+    int h = 0;
+    cudaError_t e = cudaMemset(d, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        launch_wait_selftest(limit, d, 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    CK(e);
+    *status = h;
+    return MSTMG_OK;
+}
+
 extern "C" int mstmg_translation_pass(mstmg_ctx* c, int prec, int ncols, const int* con_tran, const double* x, double* y)
 {
+    NvtxRange nvtx_("mstmg_translation_pass");
     if (!c || ncols < 1 || ncols > 256 || !x || !y || (prec != 0 && prec != 1)) {
         set_err("mstmg_translation_pass: bad arguments");
         return MSTMG_ERR_ARG;

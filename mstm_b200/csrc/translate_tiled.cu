@@ -54,9 +54,11 @@ __device__ __forceinline__ bool mb_try(uint64_t* bar, uint32_t parity)
                  : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mb_wait(uint64_t* bar, uint32_t parity)
+// bounded wait: gives up after `limit` polls (the kernels then record
+// MSTMG_ERR_CUDA and return instead of hanging)
+__device__ __forceinline__ bool mb_wait(uint64_t* bar, uint32_t parity, int limit = 1 << 22)
 {
-    for (int it = 0; it < (1 << 22); ++it)
+    for (int it = 0; it < limit; ++it)
         if (mb_try(bar, parity)) return true;
     return false;
 }
@@ -488,3 +490,30 @@ bool tiled_supported(int L, int nrhs) { return L >= 5 && L <= 10 && (nrhs == 1 |
 
 template int launch_translate_tiled<double>(const TiledArgs<double>&, int, int, cudaStream_t);
 template int launch_translate_tiled<float>(const TiledArgs<float>&, int, int, cudaStream_t);
+
+// Self-test of the bounded wait: one CTA waits on an mbarrier whose
+// transaction never arrives (an expected byte count with no copy issued), gives
+// up after `limit` polls per thread and records MSTMG_ERR_CUDA in *err -- the
+// path the translation kernel takes when a bulk copy does not complete.  No
+// asynchronous operation is in flight when it returns.
+__global__ void wait_selftest_kernel(int limit, int* err)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mb_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mb_expect(&bar, 16u);
+    __syncthreads();
+    if (!mb_wait(&bar, 0u, limit)) {
+        if (threadIdx.x == 0) atomicExch(err, MSTMG_ERR_CUDA);
+    }
+}
+
+int launch_wait_selftest(int limit, int* err, cudaStream_t st)
+{
+    wait_selftest_kernel<<<1, 64, 0, st>>>(limit, err);
+    launch_counter() += 1;
+    return 0;
+}

@@ -19,4 +19,6 @@ template <typename T> struct TiledArgs {
 };
 
 bool tiled_supported(int L, int nrhs);
+// one CTA runs the kernels' bounded mbarrier wait on a barrier no copy completes
+int launch_wait_selftest(int limit, int* err, cudaStream_t st);
 template <typename T> int launch_translate_tiled(const TiledArgs<T>& a, int L, int nsm, cudaStream_t st);

@@ -43,3 +43,33 @@ def test_missing_library_fails_loudly(monkeypatch):
     monkeypatch.setattr(_lib, "LIB_PATH", "/nonexistent/libmstm_b200.so")
     with pytest.raises(RuntimeError):
         _lib.lib()
+
+
+@pytest.mark.parametrize("bad", ["nan_position", "inf_index", "zero_radius"])
+def test_ctx_create_rejects_invalid_host_inputs(bad):
+    """Non-finite positions or indices and non-positive radii are rejected with
+    MSTMG_ERR_ARG before anything reaches a GPU (runs on a machine without one)."""
+    import ctypes
+
+    import numpy as np
+
+    from mstm_b200 import _lib
+    from mstm_b200 import build as B
+    if not os.path.exists(_lib.LIB_PATH):
+        B.build()
+    L = _lib.lib()
+    pos = np.array([[0.0, 0.0, 0.0], [3.0, 0.0, 0.0]])
+    rad = np.array([1.0, 1.0])
+    ri = np.array([[1.5, 0.01], [1.5, 0.01]])
+    if bad == "nan_position":
+        pos[1, 2] = np.nan
+    elif bad == "inf_index":
+        ri[0, 1] = np.inf
+    else:
+        rad[1] = 0.0
+    ctx = ctypes.c_void_p()
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = L.mstmg_ctx_create(ctypes.byref(ctx), 2, p(pos), p(rad), p(ri), -3.0, None)
+    assert rc == -1 and not ctx.value
+    msg = L.mstmg_last_error().decode()
+    assert ("sphere 2" if bad != "inf_index" else "sphere 1") in msg

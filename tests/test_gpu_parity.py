@@ -119,6 +119,43 @@ def test_translation_pass_kernels_agree(api, name):
     gen.close()
 
 
+def test_zero_rhs_and_iteration_cap(api, oracle_mod):
+    """Failure paths as the reference takes them: a zero right-hand side returns
+    at once with the guess untouched (cbicg, solver:694); an iteration cap
+    below what the solve needs gives solution status 1 (fixedorsoln, solver:524),
+    with the same iteration count and error as the oracle."""
+    pos, rad, ri, em = _cluster("cluster20")
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em)
+    ne = g.number_eqns
+    guess = np.full(ne, 0.25 - 0.5j)
+    x, it, err = g.cbicg(np.zeros(ne, complex), guess, niter=50, eps=1e-10)
+    assert it == 0 and err == 0.0 and np.array_equal(x, guess)
+    xo, ito, eo, _ = o.cbicg(np.zeros(ne, complex), guess, niter=50, eps=1e-10)
+    assert ito == 0 and np.array_equal(xo, guess)
+    rg = g.fixedorsoln(eps=1e-12, niter=3)
+    ro = o.fixedorsoln(eps=1e-12, niter=3)
+    assert rg["istat"] == 1 and ro["status"] == 1
+    assert rg["maxiter"] == ro["maxiter"]
+    assert abs(rg["maxerr"] / ro["maxerr"] - 1) < 1e-6
+
+
+def test_bounded_wait_gives_up_and_device_stays_usable(api, oracle_mod):
+    """The translation kernels' bounded mbarrier wait, run on a barrier that no
+    copy completes, gives up and records MSTMG_ERR_CUDA instead of hanging; the
+    device then solves normally."""
+    import ctypes
+    from mstm_b200 import _lib
+    L = _lib.lib()
+    st = ctypes.c_int(0)
+    assert L.mstmg_selftest_bounded_wait(0, 1 << 12, ctypes.byref(st)) == 0
+    assert st.value == -2   # MSTMG_ERR_CUDA
+    pos, rad, ri, em = _cluster("cluster20")
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em)
+    r = g.fixedorsoln(eps=1e-10, niter=500)
+    assert r["istat"] == 0
+    assert np.allclose(r["qtot"], o.fixedorsoln(eps=1e-10, niter=500)["qtot"], rtol=RTOL_FP64)
+
+
 def test_cbicg_same_iterations(api, oracle_mod):
     pos, rad, ri, em = _cluster("cluster20")
     g, o = _pair(api, oracle_mod, pos, rad, ri, em)
