@@ -399,6 +399,11 @@ def test_fft_translation_solve(api, oracle_mod):
         g.fft_setup(d_cell=4.0)
         rg = g.fixedorsoln(eps=1e-12)
         assert np.allclose(rg["qtot"], ro["qtot"], rtol=tol)
+    # the FFT path's own approximation against the direct path: Qext within the
+    # 1-2 % the reference's paper reports for node order max(ceil(d+1), L)
+    gd = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="fp64")
+    rd = gd.fixedorsoln(eps=1e-12)
+    assert abs(rg["qtot"][0, 0] / rd["qtot"][0, 0] - 1) < 0.02
 
 
 def test_dense_pairs_below_switch_order(api, oracle_mod):

@@ -444,3 +444,25 @@ def test_order_of_scattering_mode_converges_to_bicg_solution(oracle_mod):
     f_o = o.fixedorsoln(eps=1e-14, niter=-200)
     assert f_o["maxiter"] < 200 and f_o["maxerr"] < 1e-14
     assert np.allclose(f_o["qtot"], f_b["qtot"], rtol=1e-7)
+
+
+def test_orientation_average_of_fixed_orientation_equals_tmatrix(oracle_mod):
+    """Known-answer identity: the orientation-averaged Qext and Qsca of the
+    cluster T matrix equal the average of fixed-orientation efficiencies over
+    incident directions (Gauss-Legendre in cos(beta) x uniform in alpha, enough
+    nodes to integrate the band-limited direction dependence exactly)."""
+    w = C.workload("cluster8")
+    o = oracle_mod.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-w["order"])
+    rt = o.tmatrix_solution(convergence_eps=1e-9, solution_eps=1e-14)
+    T = rt["tmo"]
+    nb, na = T + 4, 2 * T + 4
+    xg, wg = np.polynomial.legendre.leggauss(nb)
+    acc = np.zeros(3)
+    for cb, wb in zip(xg, wg):
+        beta = np.arccos(cb)
+        sinc, direction = np.sin(beta), (1 if cb >= 0 else 2)
+        for k in range(na):
+            r = o.fixedorsoln(eps=1e-14, alpha=2 * np.pi * k / na, sinc=sinc, direction=direction)
+            acc += 0.5 * wb / na * r["qtot"][:, 0]
+    assert abs(acc[0] / rt["qtot"][0] - 1) < 1e-6
+    assert abs(acc[2] / rt["qtot"][2] - 1) < 1e-6
