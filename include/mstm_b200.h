@@ -91,6 +91,18 @@ double mstmg_vol_radius(const mstmg_ctx *ctx);
 int mstmg_interaction(mstmg_ctx *ctx, int nrhs, const double *ain, double *aout, const int *con_tran, const int *mie_mult,
                       int initial_run);
 
+/* sphereinteraction with the rest of its optional arguments
+ * (mstm-scatprops-26.f90:25-27): rhs_list[r] == 0 leaves column r out (its
+ * output is zero; NULL: all columns); fft_option -1 uses the context's set-up,
+ * 0 / 1 demand the direct / FFT path and return MSTMG_ERR_UNSUPPORTED when the
+ * context was set up the other way; store_matrix_option is accepted and ignored
+ * (the operators are always stored); skip_external_translation != 0 skips the
+ * pair translation, which leaves a zero interaction on this path (no host
+ * spheres or plane boundaries). */
+int mstmg_interaction_ex(mstmg_ctx *ctx, int nrhs, const double *ain, double *aout, const int *con_tran, const int *mie_mult,
+                         int initial_run, const int *rhs_list, int fft_option, int store_matrix_option,
+                         int skip_external_translation);
+
 /* cbicg (mstm-solver-8.f90:654-949), FP64.  Solves (I - Mie*H) x = pnp from the
  * initial guess in anp; stops when ||r||^2/||pnp||^2 < eps.  iter, err as cbicg's. */
 int mstmg_bicg(mstmg_ctx *ctx, int niter, double eps, const double *pnp, double *anp, int initialize, int *iter, double *err);

@@ -32,6 +32,7 @@ SIGNATURES = {
     "mstmg_scattering": (c_int, [c_void_p, c_void_p, c_double, c_int, c_int, c_void_p, P(c_double), P(c_int), c_void_p,
                                  c_int]),
     "mstmg_selftest_bounded_wait": (c_int, [c_int, c_int, P(c_int)]),
+    "mstmg_interaction_ex": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int]),
     "mstmg_translation_pass": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "mstmg_gsf_coefficients": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "mstmg_scattering_plane": (c_int, [c_void_p, c_int, c_void_p, c_int, c_int, c_double, c_double, c_double, c_int, c_void_p]),

@@ -118,6 +118,21 @@ class SphereCluster:
               "sphereinteraction")
         return out
 
+    def sphereinteraction_ex(self, ain, con_tran=None, mie_mult=None, initial_run=False, rhs_list=None, fft_option=-1,
+                             store_matrix_option=True, skip_external_translation=False):
+        """sphereinteraction with rhs_list, fft_option (-1: as set up),
+        store_matrix_option and skip_external_translation."""
+        ain = np.asfortranarray(np.asarray(ain, np.complex128).reshape(self.number_eqns, -1, order="F"))
+        nrhs = ain.shape[1]
+        out = np.zeros((self.number_eqns, nrhs), np.complex128, order="F")
+        ct = np.array(con_tran if con_tran is not None else [0] * nrhs, np.int32)
+        mm = np.array(mie_mult if mie_mult is not None else [1] * nrhs, np.int32)
+        rl = None if rhs_list is None else np.array(rhs_list, np.int32)
+        check(self._L.mstmg_interaction_ex(self.ctx, nrhs, _ptr(ain), _ptr(out), _ptr(ct), _ptr(mm), int(initial_run),
+                                           None if rl is None else _ptr(rl), int(fft_option), int(bool(store_matrix_option)),
+                                           int(bool(skip_external_translation))), "sphereinteraction_ex")
+        return out
+
     def cbicg(self, pnp, anp, niter=10000, eps=1.0e-6, initialize=True):
         pnp = np.ascontiguousarray(pnp, np.complex128)
         x = np.array(anp, np.complex128, copy=True)

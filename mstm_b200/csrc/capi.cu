@@ -855,20 +855,23 @@ template <typename T> static int translate_many(mstmg_ctx* c, const cpx<T>* x, c
     return MSTMG_OK;
 }
 
-extern "C" int mstmg_interaction(mstmg_ctx* c, int nrhs, const double* ain, double* aout, const int* con_tran, const int* mie_mult,
-                                 int initial_run)
+static int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, const int* con_tran, const int* mie_mult,
+                            int initial_run, const int* rhs_list, int skip_external)
 {
-    NvtxRange nvtx_("mstmg_interaction");
     if (!c || nrhs < 1 || nrhs > 4 || !ain || !aout) {
         set_err("mstmg_interaction: bad arguments (nrhs must be 1..4)");
         return MSTMG_ERR_ARG;
     }
-    int rc = ensure_ops(c, 0, initial_run != 0);
+    int rc = skip_external ? MSTMG_OK : ensure_ops(c, 0, initial_run != 0);
     if (rc) return rc;
     const int ne = c->neqns;
     SlotMaps sm = c->sm();
     unsigned mask = 0;
     CK(copy_in(c->X64.p, ain, sizeof(zd) * (size_t)ne * nrhs, c->st));
+    // columns left out of rhs_list are not translated: their output is zero
+    if (rhs_list)
+        for (int r = 0; r < nrhs; r++)
+            if (!rhs_list[r]) CK(cudaMemsetAsync(c->X64.p + (size_t)r * ne, 0, sizeof(zd) * ne, c->st));
     for (int r = 0; r < nrhs; r++) {
         int ct = con_tran ? con_tran[r] : 0;
         int mm = mie_mult ? mie_mult[r] : 1;
@@ -879,8 +882,14 @@ extern "C" int mstmg_interaction(mstmg_ctx* c, int nrhs, const double* ain, doub
             else launch_conj_copy<double>(ne, col, col, c->st);
         }
     }
-    rc = translate<double>(c, c->X64.p, c->Y64.p, nrhs, mask);
-    if (rc) return rc;
+    if (skip_external) {
+        // no pair translation (and, on this path, no host spheres or plane
+        // boundaries): the interaction is zero
+        CK(cudaMemsetAsync(c->Y64.p, 0, sizeof(zd) * (size_t)ne * nrhs, c->st));
+    } else {
+        rc = translate<double>(c, c->X64.p, c->Y64.p, nrhs, mask);
+        if (rc) return rc;
+    }
     for (int r = 0; r < nrhs; r++) {
         int ct = con_tran ? con_tran[r] : 0;
         int mm = mie_mult ? mie_mult[r] : 1;
@@ -895,6 +904,28 @@ extern "C" int mstmg_interaction(mstmg_ctx* c, int nrhs, const double* ain, doub
     CK(copy_out(aout, c->Y64.p, sizeof(zd) * (size_t)ne * nrhs, c->st));
     CK(cudaStreamSynchronize(c->st));
     return check_kernel_err(c);
+}
+
+extern "C" int mstmg_interaction(mstmg_ctx* c, int nrhs, const double* ain, double* aout, const int* con_tran, const int* mie_mult,
+                                 int initial_run)
+{
+    NvtxRange nvtx_("mstmg_interaction");
+    return interaction_impl(c, nrhs, ain, aout, con_tran, mie_mult, initial_run, nullptr, 0);
+}
+
+extern "C" int mstmg_interaction_ex(mstmg_ctx* c, int nrhs, const double* ain, double* aout, const int* con_tran, const int* mie_mult,
+                                    int initial_run, const int* rhs_list, int fft_option, int store_matrix_option,
+                                    int skip_external_translation)
+{
+    NvtxRange nvtx_("mstmg_interaction_ex");
+    if (!c) return MSTMG_ERR_ARG;
+    const bool fft_on = c->fft && c->fft->on;
+    if ((fft_option == 1 && !fft_on) || (fft_option == 0 && fft_on)) {
+        set_err("mstmg_interaction_ex: fft_option differs from the context's set-up (mstmg_fft_setup decides it per context)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    (void)store_matrix_option;   // the pair operators are always stored
+    return interaction_impl(c, nrhs, ain, aout, con_tran, mie_mult, initial_run, rhs_list, skip_external_translation);
 }
 
 // ---------------------------------------------------------------------------

@@ -83,6 +83,25 @@ def test_sphereinteraction(api, oracle_mod, name):
             assert np.abs(yg[:, r] - yo[:, r]).max() <= 1e-11 * scale, (name, ct, mm, r)
 
 
+def test_sphereinteraction_optional_arguments(api, oracle_mod):
+    """rhs_list zeroes the columns it leaves out and leaves the others as
+    sphereinteraction gives them; skip_external_translation gives zero; an
+    fft_option the context was not set up for is refused."""
+    pos, rad, ri, em = _cluster("cluster20")
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=em)
+    rng = np.random.default_rng(2)
+    x = rng.normal(size=(g.number_eqns, 3)) + 1j * rng.normal(size=(g.number_eqns, 3))
+    ct = [0, 1, 0]
+    full = g.sphereinteraction(x, con_tran=ct, initial_run=True)
+    part = g.sphereinteraction_ex(x, con_tran=ct, rhs_list=[1, 0, 1])
+    assert np.array_equal(part[:, 1], np.zeros(g.number_eqns))
+    assert np.abs(part[:, [0, 2]] - full[:, [0, 2]]).max() <= 1e-14 * np.abs(full).max()
+    assert np.abs(g.sphereinteraction_ex(x, con_tran=ct, skip_external_translation=True)).max() == 0.0
+    from mstm_b200._lib import MstmgError
+    with pytest.raises(MstmgError):
+        g.sphereinteraction_ex(x, fft_option=1)
+
+
 @pytest.mark.parametrize("name,nrhs", [("cluster20", 1), ("fractal60", 2), ("fractal60", 4)])
 def test_tiled_and_generic_kernels_agree(api, name, nrhs):
     pos, rad, ri, em = _cluster(name)
