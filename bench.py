@@ -4,12 +4,13 @@ interaction solve on B200.
 Workload (one step = one solve): a seeded particle-cluster fractal aggregate,
 500 touching monomers, x = 2.0, m = 1.6+0.05i, Df = 1.8, kf = 1.3, incidence
 along +z, both polarisations, direct pair translation, sphere order L = 9
-(neqns = 99,000, 124,750 pairs).  A solve = incident coefficients + both
+(neqns = 99,000, 124,750 pairs).  A solve = pair-operator generation (FP64,
+and FP32 for the tuned arm: every fixed-orientation solve regenerates them, as
+the reference's initial_run does) + incident coefficients + both
 polarisations solved to ||r||/||b|| < 1e-6 (MSTM solution_epsilon = 1e-12 in
-its squared-norm test) + efficiencies, on a context whose pair operators were
-generated in the warm-up (`value`); the end-to-end number (`e2e`) adds, every
-step, the positions copied in from pinned host memory, which regenerates the
-pair operators, and the solution and efficiencies copied back.
+its squared-norm test) + efficiencies (`value`); the end-to-end number
+(`e2e`) adds, every step, the positions copied in from pinned host memory and
+the solution and efficiencies copied back.
 
 Arms:
   default            tuned path (mixed precision, polarisations batched), with
