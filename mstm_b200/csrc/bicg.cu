@@ -213,26 +213,6 @@ __global__ void sum3_last_kernel(int nparts, const double* part, double* out)
     for (int b = 0; b < nparts; b++) s += part[3 * b + 2];
     out[0] = s;
 }
-__global__ void rr_fin_kernel(int nparts, const double* part, BicgScalars* sc)
-{
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double s[3] = {0.0, 0.0, 0.0};
-    for (int b = 0; b < nparts; b++)
-        for (int k = 0; k < 3; k++) s[k] += part[3 * b + k];
-    zd csk2 = mk(s[0], s[1]), prev = mk(sc->csk_prev[0], sc->csk_prev[1]);
-    if (cabsd(prev) == 0.0) {
-        sc->breakdown = 1;
-        return;
-    }
-    zd b = cdiv(csk2, prev);
-    sc->beta[0] = b.x;
-    sc->beta[1] = b.y;
-    sc->csk[0] = csk2.x;
-    sc->csk[1] = csk2.y;
-    sc->enorm = s[2];
-    sc->eerr = 1.0;
-    sc->stop = (s[0] == 0.0 && s[1] == 0.0) ? 1 : 0;
-}
 
 // r = b - x + M*y (FP64 true residual of the refinement loop); partials |r|^2, |b|^2
 template <typename T, typename TB>
@@ -327,23 +307,6 @@ void launch_upd(int n, cpx<T>* x, cpx<T>* r, cpx<T>* q, cpx<T>* p, cpx<T>* w, co
     upd2_kernel<T><<<g, RB, 0, st>>>(n, sc, p, w, r, q);
     launch_counter() += 3;
 }
-template <typename T>
-void launch_upd1_only(int n, cpx<T>* x, cpx<T>* r, cpx<T>* q, const cpx<T>* p, const cpx<T>* cap, const cpx<T>* caw, double* part,
-                      BicgScalars* sc, int nsm, cudaStream_t st)
-{
-    int g = grid_for(n, nsm);
-    upd1_kernel<T><<<g, RB, 0, st>>>(n, sc, x, r, q, p, cap, caw, part);
-    fin_kernel<<<1, 32, 0, st>>>(2, g, part, sc, 0.0, 1);
-    launch_counter() += 2;
-}
-template <typename T> void launch_upd2_only(int n, cpx<T>* p, cpx<T>* w, const cpx<T>* r, const cpx<T>* q, BicgScalars* sc, int nsm, cudaStream_t st)
-{
-    int g = grid_for(n, nsm);
-    upd2_kernel<T><<<g, RB, 0, st>>>(n, sc, p, w, r, q);
-    launch_counter() += 1;
-}
-template void launch_upd1_only<float>(int, zf*, zf*, zf*, const zf*, const zf*, const zf*, double*, BicgScalars*, int, cudaStream_t);
-template void launch_upd2_only<float>(int, zf*, zf*, const zf*, const zf*, BicgScalars*, int, cudaStream_t);
 
 template <typename T, typename TB>
 void launch_resid(const SlotMaps& sm, const cpx<T>* an, const cpx<T>* b, const cpx<T>* x, const cpx<T>* y, cpx<TB>* rout, double* part,
@@ -354,13 +317,6 @@ void launch_resid(const SlotMaps& sm, const cpx<T>* an, const cpx<T>* b, const c
     sum2_kernel<<<1, 32, 0, st>>>(g, part, out2);
     launch_counter() += 2;
 }
-template <typename T> void launch_rr_fix(int n, const cpx<T>* q, const cpx<T>* r, double* part, BicgScalars* sc, int nsm, cudaStream_t st)
-{
-    int g = grid_for(n, nsm);
-    rr_dot_kernel<T><<<g, RB, 0, st>>>(n, q, r, part);
-    rr_fin_kernel<<<1, 32, 0, st>>>(g, part, sc);
-    launch_counter() += 2;
-}
 // out[0] = sum |v|^2 (one block-reduction pass and a fixed-order finish)
 void launch_rr_dot_norm(int n, const zd* v, double* part, double* out, int nsm, cudaStream_t st)
 {
@@ -369,8 +325,6 @@ void launch_rr_dot_norm(int n, const zd* v, double* part, double* out, int nsm, 
     sum3_last_kernel<<<1, 32, 0, st>>>(g, part, out);
     launch_counter() += 2;
 }
-template void launch_rr_fix<float>(int, const zf*, const zf*, double*, BicgScalars*, int, cudaStream_t);
-template void launch_rr_fix<double>(int, const zd*, const zd*, double*, BicgScalars*, int, cudaStream_t);
 void launch_add_correction_f(int n, zd* x, const zf* d, cudaStream_t st) { add_correction_kernel<float><<<296, 256, 0, st>>>(n, x, d); launch_counter() += 1; }
 void launch_add_correction_d(int n, zd* x, const zd* d, cudaStream_t st) { add_correction_kernel<double><<<296, 256, 0, st>>>(n, x, d); launch_counter() += 1; }
 template <typename T> void launch_conj_copy(int n, const cpx<T>* a, cpx<T>* b, cudaStream_t st) { conj_copy_kernel<T><<<296, 256, 0, st>>>(n, a, b); launch_counter() += 1; }

@@ -32,14 +32,6 @@ template <typename T, typename TB>
 void launch_resid(const SlotMaps& sm, const cpx<T>* an, const cpx<T>* b, const cpx<T>* x, const cpx<T>* y, cpx<TB>* rout, double* part,
                   double* out2, int nsm, cudaStream_t st);
 void launch_add_correction_f(int n, zd* x, const zf* d, cudaStream_t st);
-// the two halves of launch_upd (update + scalar finish with eps 0; direction update)
-template <typename T>
-void launch_upd1_only(int n, cpx<T>* x, cpx<T>* r, cpx<T>* q, const cpx<T>* p, const cpx<T>* cap, const cpx<T>* caw, double* part,
-                      BicgScalars* sc, int nsm, cudaStream_t st);
-template <typename T> void launch_upd2_only(int n, cpx<T>* p, cpx<T>* w, const cpx<T>* r, const cpx<T>* q, BicgScalars* sc, int nsm, cudaStream_t st);
-// Residual replacement: r was replaced by the true residual; recompute
-// csk = sum conj(q) r, beta = csk / csk_prev, enorm = sum |r|^2 (the new base).
-template <typename T> void launch_rr_fix(int n, const cpx<T>* q, const cpx<T>* r, double* part, BicgScalars* sc, int nsm, cudaStream_t st);
 void launch_add_correction_d(int n, zd* x, const zd* d, cudaStream_t st);
 void launch_rr_dot_norm(int n, const zd* v, double* part, double* out, int nsm, cudaStream_t st);   // out[0] = sum |v|^2
 template <typename T> void launch_conj_copy(int n, const cpx<T>* a, cpx<T>* b, cudaStream_t st);

@@ -104,6 +104,47 @@ struct NvtxRange {
     NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
+// work vectors of the many-system BiCG (mrhs.cu kernels): S systems in columns
+template <typename T> struct MultiWork {
+    int S = 0;
+    DevBuf<cpx<T>> vec, XP, YP;
+    DevBuf<double> part, epsv;
+    DevBuf<BicgScalars> sc;
+    DevBuf<int> act;
+    std::vector<BicgScalars> hsc;
+    std::vector<int> hact;
+    MultiVecs<T> v(int ne) const
+    {
+        MultiVecs<T> m;
+        cpx<T>* b = vec.p;
+        size_t cs = (size_t)ne * S;
+        m.X = b;
+        m.R = b + cs;
+        m.P = b + 2 * cs;
+        m.W = b + 3 * cs;
+        m.Q = b + 4 * cs;
+        m.CAP = b + 5 * cs;
+        m.CAW = b + 6 * cs;
+        return m;
+    }
+    // vectors = false: only the packed translation buffers (FP64 residuals of the refinement)
+    int init(int S_, int ne, int nsm, bool vectors)
+    {
+        S = S_;
+        int spad = S + 3;
+        if (vectors) CK(vec.alloc((size_t)7 * ne * S));
+        CK(XP.alloc((size_t)2 * ne * spad));
+        CK(YP.alloc((size_t)2 * ne * spad));
+        CK(part.alloc((size_t)3 * (4 * nsm + spad)));
+        CK(epsv.alloc(S));
+        CK(sc.alloc(S));
+        CK(act.alloc(S));
+        hsc.resize(S);
+        hact.resize(S);
+        return MSTMG_OK;
+    }
+};
+
 struct mstmg_ctx {
     int dev = 0, nsm = 148;
     cudaStream_t st = nullptr;
@@ -126,6 +167,13 @@ struct mstmg_ctx {
     DevBuf<double> op64;
     DevBuf<float> op32;
     bool ops64_ready = false, ops32_ready = false;
+    // mixed fixed-orientation solve: the two polarisations as a many-system
+    // residual-replacement solve, its work kept across solves
+    MultiWork<double> fo64;
+    MultiWork<float> fo32;
+    DevBuf<double> fo_rr;
+    DevBuf<int> fo_idx;
+    bool fo_ready = false;
     int chunk32 = 0;   // FP32 columns per tiled chunk chosen by timing (0: not yet)
     DevBuf<double> vcc, fnm1, fnc, fnp1, fnr, bcofd;
     int vn = 0;
@@ -1194,156 +1242,10 @@ static int solve_mixed(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, int
     return MSTMG_OK;
 }
 
-// Mixed precision by residual replacement ("reliable updates"): one FP32
-// BiCG per system, never restarted.  Its iterate accumulates in FP32 and is
-// folded into the FP64 solution x whenever the recursive FP32 residual has
-// dropped by `drop` since the last true residual, or claims convergence; the
-// true residual b - (I - M H) x is then computed with the FP64 operators,
-// replaces the BiCG residual (FP32), and beta and the shadow product are
-// recomputed from it.  A system stops when its true residual meets eps, so the
-// answer carries the reference's criterion in FP64 while every Krylov step
-// runs in FP32.  Both polarisations advance in lockstep (4 FP32 columns per
-// pass).  x holds the initial guesses (FP64) on entry.
-static int solve_mixed_rr(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, int niter, int* iters, double* errs, int* status)
-{
-    const int ne = c->neqns, S = 2;
-    SlotMaps sm = c->sm();
-    int rc = ensure_ops(c, 0, false);
-    if (rc) return rc;
-    if ((rc = ensure_ops(c, 1, false))) return rc;
-    const zf* an32 = (const zf*)c->an32.p;
-    const double drop = 1.0e-5;   // replacement once the FP32 residual fell by this factor (squared norms)
-    const double drop_soft = 1.0e-3;   // ... or by this one when the other polarisation's replacement is due
-    double base[2] = {1.0, 1.0};  // true squared residual ratio at the last replacement
-    bool act[2] = {true, true};
-    int tot[2] = {0, 0};
-    c->outer = 0;
-    for (int s = 0; s < S; s++) status[s] = 0;
-    // true residual of the active systems in FP64, rounded into the FP32 BiCG residual
-    auto true_residual = [&](const bool* which, double* ratio) -> int {
-        int slots[2], a = 0;
-        for (int s = 0; s < S; s++)
-            if (which[s]) slots[a++] = s;
-        if (a == 0) return MSTMG_OK;
-        for (int k = 0; k < a; k++)
-            CK(cudaMemcpyAsync(c->X64.p + (size_t)k * ne, x[slots[k]], sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
-        int r2 = translate<double>(c, c->X64.p, c->Y64.p, a, 0u);
-        if (r2) return r2;
-        for (int k = 0; k < a; k++) {
-            int s = slots[k];
-            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
-            launch_resid<double, float>(sm, c->an.p, b[s], x[s], c->Y64.p + (size_t)k * ne, v.r, c->part.p, c->small.p + 2 * s, c->nsm,
-                                        c->st);
-        }
-        CK(cudaMemcpyAsync(c->h_small, c->small.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-        c->outer++;
-        for (int k = 0; k < a; k++) {
-            int s = slots[k];
-            double rr = c->h_small[2 * s], bb = c->h_small[2 * s + 1];
-            ratio[s] = bb > 0.0 ? rr / bb : 0.0;
-        }
-        return MSTMG_OK;
-    };
-    double ratio[2] = {0.0, 0.0};
-    if ((rc = true_residual(act, ratio))) return rc;
-    for (int s = 0; s < S; s++) {
-        base[s] = ratio[s];
-        errs[s] = ratio[s];
-        if (ratio[s] < eps) act[s] = false;
-    }
-    // FP32 BiCG start from the true residual: r = r_true, p = r, q = w = conj(r), x32 = 0
-    for (int s = 0; s < S; s++) {
-        if (!act[s]) continue;
-        BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
-        CK(cudaMemsetAsync(v.x, 0, sizeof(zf) * ne, c->st));
-        CK(cudaMemcpyAsync(c->rvec32.p + (size_t)s * ne, v.r, sizeof(zf) * ne, cudaMemcpyDeviceToDevice, c->st));
-        launch_init<float>(sm, an32, c->rvec32.p + (size_t)s * ne, v.x, nullptr, 0, v.r, v.p, v.w, v.q, c->part.p, c->sc.p + s, 1, c->nsm,
-                           c->st);
-    }
-    CK(cudaGetLastError());
-    for (int it = 1; it <= niter && (act[0] || act[1]); it++) {
-        int slots[2], a = 0;
-        for (int s = 0; s < S; s++)
-            if (act[s]) slots[a++] = s;
-        unsigned mask = 0;
-        for (int k = 0; k < a; k++) {
-            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, slots[k]);
-            CK(cudaMemcpyAsync(c->X32.p + (size_t)(2 * k) * ne, v.p, sizeof(zf) * ne, cudaMemcpyDeviceToDevice, c->st));
-            launch_mie<float>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, an32, -1, 1, v.w, c->X32.p + (size_t)(2 * k + 1) * ne,
-                              c->st);
-            mask |= 2u << (2 * k);
-        }
-        (void)mask;   // [p, A^T conj w] pairs: the odd columns are the transpose products
-        if ((rc = translate_many<float>(c, c->X32.p, c->Y32.p, 2 * a, 2u))) return rc;
-        for (int k = 0; k < a; k++) {
-            int s = slots[k];
-            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
-            launch_post<float>(sm, an32, v.p, v.w, c->Y32.p + (size_t)(2 * k) * ne, c->Y32.p + (size_t)(2 * k + 1) * ne, v.cap, v.caw,
-                               c->part.p, c->sc.p + s, c->nsm, c->st);
-            launch_upd1_only<float>(ne, v.x, v.r, v.q, v.p, v.cap, v.caw, c->part.p, c->sc.p + s, c->nsm, c->st);
-        }
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(c->h_sc, c->sc.p, sizeof(BicgScalars) * S, cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-        bool repl[2] = {false, false}, trigger = false;
-        for (int k = 0; k < a; k++) {
-            int s = slots[k];
-            tot[s] = it;
-            if (c->h_sc[s].breakdown) {
-                status[s] = 2;
-                act[s] = false;
-                continue;
-            }
-            double rec = c->h_sc[s].eerr * base[s];   // recursive residual relative to ||b||^2
-            if (rec < eps || c->h_sc[s].eerr < drop) trigger = true;
-        }
-        // one FP64 pass serves both polarisations when the other is close to its replacement
-        for (int k = 0; k < a && trigger; k++) {
-            int s = slots[k];
-            if (!act[s]) continue;
-            double rec = c->h_sc[s].eerr * base[s];
-            if (rec < eps || c->h_sc[s].eerr < drop_soft) repl[s] = true;
-        }
-        if (repl[0] || repl[1]) {
-            for (int s = 0; s < S; s++)
-                if (repl[s]) {
-                    BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
-                    launch_add_correction_f(ne, x[s], v.x, c->st);
-                    CK(cudaMemsetAsync(v.x, 0, sizeof(zf) * ne, c->st));
-                }
-            if ((rc = true_residual(repl, ratio))) return rc;
-            for (int s = 0; s < S; s++) {
-                if (!repl[s]) continue;
-                errs[s] = ratio[s];
-                base[s] = ratio[s];
-                if (ratio[s] < eps) {
-                    act[s] = false;
-                    continue;
-                }
-                BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
-                launch_rr_fix<float>(ne, v.q, v.r, c->part.p, c->sc.p + s, c->nsm, c->st);
-            }
-        }
-        for (int k = 0; k < a; k++) {
-            int s = slots[k];
-            if (!act[s]) continue;
-            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
-            launch_upd2_only<float>(ne, v.p, v.w, v.r, v.q, c->sc.p + s, c->nsm, c->st);
-        }
-        CK(cudaGetLastError());
-    }
-    for (int s = 0; s < S; s++) {
-        if (act[s]) {
-            // iteration cap: fold the last FP32 steps in
-            BicgVecs<float> v = vecs_at<float>(c->vec32.p, ne, s);
-            launch_add_correction_f(ne, x[s], v.x, c->st);
-            tot[s] = niter + 1;
-        }
-        iters[s] = tot[s];
-    }
-    return check_kernel_err(c);
-}
+static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>& w32, DevBuf<double>& rr, DevBuf<int>& idx, int S,
+                          const zd* B, zd* X, double eps, int niter, std::vector<int>& iters, std::vector<double>& errs,
+                          std::vector<int>& status, int* outer_count);
+
 
 static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, const double* x0, double fallback,
                                   int* used_guess, double* guess_res, double* amnp, double* qeff, double* qtot, double* maxerr, int* maxiter);
@@ -1430,7 +1332,27 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
         zd* bs[2] = {bvec, bvec + ne};
         if (xinit != c->amnp.p)
             for (int p = 0; p < 2; p++) CK(cudaMemcpyAsync(xs[p], bs[p], sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
-        rc = c->opts.mixed_solver == 1 ? solve_mixed(c, bs, xs, eps, niter, it, er, st) : solve_mixed_rr(c, bs, xs, eps, niter, it, er, st);
+        if (c->opts.mixed_solver == 1) {
+            rc = solve_mixed(c, bs, xs, eps, niter, it, er, st);
+        } else {
+            // both polarisations as two systems of the many-system residual-replacement solver
+            if (!c->fo_ready) {
+                if ((rc = c->fo64.init(2, ne, c->nsm, false)) || (rc = c->fo32.init(2, ne, c->nsm, true))) return rc;
+                CK(c->fo_rr.alloc(4));
+                CK(c->fo_idx.alloc(4));
+                c->fo_ready = true;
+            }
+            std::vector<int> its, sts;
+            std::vector<double> ers;
+            int oc = 0;
+            rc = solve_multi_rr(c, c->fo64, c->fo32, c->fo_rr, c->fo_idx, 2, bvec, c->amnp.p, eps, niter, its, ers, sts, &oc);
+            c->outer = oc;
+            for (int p = 0; p < 2; p++) {
+                it[p] = its[p];
+                er[p] = ers[p];
+                st[p] = sts[p];
+            }
+        }
         if (rc) return rc;
     } else {
         // the reference's order: polarisation 1 then 2, each from x0 = Mie*f
@@ -1779,45 +1701,6 @@ extern "C" int mstmg_scattering_plane(mstmg_ctx* c, int t_matrix_order, const do
 
 // ---- many systems at once ----
 
-template <typename T> struct MultiWork {
-    int S = 0;
-    DevBuf<cpx<T>> vec, XP, YP;
-    DevBuf<double> part, epsv;
-    DevBuf<BicgScalars> sc;
-    DevBuf<int> act;
-    std::vector<BicgScalars> hsc;
-    std::vector<int> hact;
-    MultiVecs<T> v(int ne) const
-    {
-        MultiVecs<T> m;
-        cpx<T>* b = vec.p;
-        size_t cs = (size_t)ne * S;
-        m.X = b;
-        m.R = b + cs;
-        m.P = b + 2 * cs;
-        m.W = b + 3 * cs;
-        m.Q = b + 4 * cs;
-        m.CAP = b + 5 * cs;
-        m.CAW = b + 6 * cs;
-        return m;
-    }
-    // vectors = false: only the packed translation buffers (FP64 residuals of the refinement)
-    int init(int S_, int ne, int nsm, bool vectors)
-    {
-        S = S_;
-        int spad = S + 3;
-        if (vectors) CK(vec.alloc((size_t)7 * ne * S));
-        CK(XP.alloc((size_t)2 * ne * spad));
-        CK(YP.alloc((size_t)2 * ne * spad));
-        CK(part.alloc((size_t)3 * (4 * nsm + spad)));
-        CK(epsv.alloc(S));
-        CK(sc.alloc(S));
-        CK(act.alloc(S));
-        hsc.resize(S);
-        hact.resize(S);
-        return MSTMG_OK;
-    }
-};
 
 // cbicg for the systems listed in sys (columns of B and of the work vectors),
 // all advanced together; system s stops where cbicg would stop it.  X (w.v().X)
@@ -1979,7 +1862,7 @@ static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>
     auto true_residual = [&](const std::vector<int>& Ls) -> int {
         const int a = (int)Ls.size();
         if (a == 0) return MSTMG_OK;
-        const int apad = ((a + 1) / 2) * 2;
+        const int apad = a == 1 ? 1 : ((a + 1) / 2) * 2;   // whole FP64 chunks of 2; a lone column alone
         CK(cudaMemcpyAsync(w64.act.p, Ls.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
         launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
         int r2 = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u);
@@ -2014,7 +1897,7 @@ static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>
     const int per_chunk = 2;   // systems per FP32 translation chunk ([p, w] column pairs)
     for (int it = 1; it <= niter && !act.empty(); it++) {
         const int a = (int)act.size();
-        const int apad = ((a + per_chunk - 1) / per_chunk) * per_chunk;
+        const int apad = a == 1 ? 1 : ((a + per_chunk - 1) / per_chunk) * per_chunk;   // a lone system: its 2 columns alone
         launch_m_pack<float>(sm, an32, ne, a, apad, w32.act.p, v.P, v.W, w32.XP.p, c->nsm, c->st);
         if ((rc = translate_many<float>(c, w32.XP.p, w32.YP.p, 2 * apad, 2u))) return rc;
         launch_m_post<float>(sm, an32, ne, a, w32.act.p, v, w32.YP.p, w32.part.p, w32.sc.p, c->nsm, c->st);
