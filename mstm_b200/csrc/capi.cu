@@ -1832,15 +1832,17 @@ static int solve_multi_mixed(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<flo
     return check_kernel_err(c);
 }
 
-// Mixed precision for S systems by residual replacement (the many-system form
-// of solve_mixed_rr): one FP32 BiCG per system, never restarted; whenever a
-// system's recursive residual has fallen by `drop` since its last replacement,
-// or claims convergence, its FP32 iterate is folded into the FP64 solution X,
-// the FP64 true residual replaces r, and csk/beta are recomputed.  The same
+// Mixed precision for S systems by residual replacement ("reliable updates"):
+// one FP32 BiCG per system, never restarted, all systems advanced together
+// (one translation launch per step).  Whenever a system's recursive residual
+// has fallen by `drop` since its last replacement, or claims convergence, its
+// FP32 iterate is folded into the FP64 solution X, the FP64 true residual
+// b - (I - M H) x replaces r, and csk/beta are recomputed from it.  The same
 // FP64 pass also replaces every other system whose residual has fallen by
-// `drop_soft`, so the systems of one order share their FP64 passes.  A system
-// stops when its true residual ratio is below eps.  X holds the initial
-// guesses on entry.
+// `drop_soft`, so the systems share their FP64 passes.  A system stops when
+// its true residual ratio is below eps.  X holds the initial guesses on entry.
+// Used for the T-matrix columns and for the two polarisations of a
+// fixed-orientation solve.
 static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>& w32, DevBuf<double>& rr, DevBuf<int>& idx, int S,
                           const zd* B, zd* X, double eps, int niter, std::vector<int>& iters, std::vector<double>& errs,
                           std::vector<int>& status, int* outer_count)
