@@ -111,6 +111,7 @@ template <typename T> struct MultiWork {
     DevBuf<double> part, epsv;
     DevBuf<BicgScalars> sc;
     DevBuf<int> act;
+    DevBuf<unsigned> cnt;   // per active position: CTAs done with a reduction (the last one finishes it)
     std::vector<BicgScalars> hsc;
     std::vector<int> hact;
     MultiVecs<T> v(int ne) const
@@ -139,6 +140,8 @@ template <typename T> struct MultiWork {
         CK(epsv.alloc(S));
         CK(sc.alloc(S));
         CK(act.alloc(S));
+        CK(cnt.alloc(S));
+        CK(cudaMemset(cnt.p, 0, sizeof(unsigned) * S));
         hsc.resize(S);
         hact.resize(S);
         return MSTMG_OK;
@@ -1754,8 +1757,8 @@ static int bicg_multi(mstmg_ctx* c, MultiWork<T>& w, const cpx<T>* B, const std:
         int apad = ((a + per_chunk - 1) / per_chunk) * per_chunk;
         launch_m_pack<T>(sm, an, ne, a, apad, w.act.p, v.P, v.W, w.XP.p, c->nsm, c->st);
         if ((rc = translate_many<T>(c, w.XP.p, w.YP.p, 2 * apad, 2u))) return rc;
-        launch_m_post<T>(sm, an, ne, a, w.act.p, v, w.YP.p, w.part.p, w.sc.p, c->nsm, c->st);
-        launch_m_upd<T>(ne, a, w.act.p, v, w.part.p, w.sc.p, w.epsv.p, c->nsm, c->st);
+        launch_m_post<T>(sm, an, ne, a, w.act.p, v, w.YP.p, w.part.p, w.sc.p, c->nsm, c->st, w.cnt.p);
+        launch_m_upd<T>(ne, a, w.act.p, v, w.part.p, w.sc.p, w.epsv.p, c->nsm, c->st, w.cnt.p);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(w.hsc.data(), w.sc.p, sizeof(BicgScalars) * w.S, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
@@ -1902,8 +1905,8 @@ static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>
         const int apad = a == 1 ? 1 : ((a + per_chunk - 1) / per_chunk) * per_chunk;   // a lone system: its 2 columns alone
         launch_m_pack<float>(sm, an32, ne, a, apad, w32.act.p, v.P, v.W, w32.XP.p, c->nsm, c->st);
         if ((rc = translate_many<float>(c, w32.XP.p, w32.YP.p, 2 * apad, 2u))) return rc;
-        launch_m_post<float>(sm, an32, ne, a, w32.act.p, v, w32.YP.p, w32.part.p, w32.sc.p, c->nsm, c->st);
-        launch_m_upd1<float>(ne, a, w32.act.p, v, w32.part.p, w32.sc.p, c->nsm, c->st);
+        launch_m_post<float>(sm, an32, ne, a, w32.act.p, v, w32.YP.p, w32.part.p, w32.sc.p, c->nsm, c->st, w32.cnt.p);
+        launch_m_upd1<float>(ne, a, w32.act.p, v, w32.part.p, w32.sc.p, c->nsm, c->st, w32.cnt.p);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(w32.hsc.data(), w32.sc.p, sizeof(BicgScalars) * S, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));

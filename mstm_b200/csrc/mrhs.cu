@@ -144,90 +144,16 @@ __global__ void __launch_bounds__(MB) m_init_kernel(SlotMaps sm, const cpx<T>* a
     mblock_store<3>(acc, part + 3 * ((size_t)k * gridDim.x + blockIdx.x));
 }
 
-// cap = p - M y0 ; caw = w - conj(y1) ; partial sum conj(w) cap
-template <typename T>
-__global__ void __launch_bounds__(MB) m_post_kernel(SlotMaps sm, const cpx<T>* an, int ld, const int* act, MultiVecs<T> v,
-                                                    const cpx<T>* YP, double* part)
+// The scalar steps of one system after a reduction (same logic as cbicg's):
+// mode 0 after init, 1 after post, 2 after upd1.  pk: its G per-CTA partials
+// of K values, summed in CTA order; read through L2 (__ldcg), since the
+// partials of other CTAs may have been written after this SM cached them.
+__device__ void m_fin_one(int mode, int G, const double* pk, BicgScalars* sc, double eps)
 {
-    const int k = blockIdx.y, s = act[k];
-    const size_t o = (size_t)s * ld;
-    const cpx<T>* y0 = YP + (size_t)(2 * k) * ld;
-    const cpx<T>* y1 = y0 + ld;
-    double acc[2] = {0.0, 0.0};
-    for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
-        SlotPos q = slot_pos(sm, e);
-        const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
-        cpx<T> u0 = y0[q.b0], u1 = y0[q.b1];
-        cpx<T> m0 = A[0] * u0 + A[2] * u1;
-        cpx<T> m1 = A[1] * u0 + A[3] * u1;
-        cpx<T> c0 = v.P[o + q.b0] - m0, c1 = v.P[o + q.b1] - m1;
-        v.CAP[o + q.b0] = c0;
-        v.CAP[o + q.b1] = c1;
-        cpx<T> w0 = v.W[o + q.b0], w1 = v.W[o + q.b1];
-        v.CAW[o + q.b0] = w0 - cj(y1[q.b0]);
-        v.CAW[o + q.b1] = w1 - cj(y1[q.b1]);
-        cpx<double> wd0 = upd_(w0), wd1 = upd_(w1), d0 = upd_(c0), d1 = upd_(c1);
-        acc[0] += wd0.x * d0.x + wd0.y * d0.y + wd1.x * d1.x + wd1.y * d1.y;
-        acc[1] += wd0.x * d0.y - wd0.y * d0.x + wd1.x * d1.y - wd1.y * d1.x;
-    }
-    mblock_store<2>(acc, part + 2 * ((size_t)k * gridDim.x + blockIdx.x));
-}
-
-// x += a p ; r -= a cap ; q -= conj(a) caw ; partials sum conj(q) r, sum |r|^2
-template <typename T>
-__global__ void __launch_bounds__(MB) m_upd1_kernel(int ld, const int* act, const BicgScalars* sc, MultiVecs<T> v, double* part)
-{
-    const int k = blockIdx.y, s = act[k];
-    const size_t o = (size_t)s * ld;
-    double acc[3] = {0.0, 0.0, 0.0};
-    if (!sc[s].breakdown) {
-        cpx<T> al = mk((T)sc[s].alpha[0], (T)sc[s].alpha[1]);
-        cpx<T> ac = cj(al);
-        for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
-            size_t g = o + e;
-            v.X[g] = v.X[g] + al * v.P[g];
-            cpx<T> rv = v.R[g] - al * v.CAP[g];
-            cpx<T> qv = v.Q[g] - ac * v.CAW[g];
-            v.R[g] = rv;
-            v.Q[g] = qv;
-            cpx<double> rd = upd_(rv), qd = upd_(qv);
-            acc[0] += qd.x * rd.x + qd.y * rd.y;
-            acc[1] += qd.x * rd.y - qd.y * rd.x;
-            acc[2] += rd.x * rd.x + rd.y * rd.y;
-        }
-    }
-    mblock_store<3>(acc, part + 3 * ((size_t)k * gridDim.x + blockIdx.x));
-}
-
-// p = r + b p ; w = q + conj(b) w  (skipped once the system stopped)
-template <typename T>
-__global__ void __launch_bounds__(MB) m_upd2_kernel(int ld, const int* act, const BicgScalars* sc, MultiVecs<T> v)
-{
-    const int k = blockIdx.y, s = act[k];
-    if (sc[s].stop || sc[s].breakdown) return;
-    const size_t o = (size_t)s * ld;
-    cpx<T> b = mk((T)sc[s].beta[0], (T)sc[s].beta[1]);
-    cpx<T> bc = cj(b);
-    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
-        size_t g = o + e;
-        v.P[g] = v.R[g] + b * v.P[g];
-        v.W[g] = v.Q[g] + bc * v.W[g];
-    }
-}
-
-// Per-system finish, one thread per active system (same logic as cbicg's
-// scalar steps): mode 0 after init, 1 after post, 2 after upd1.
-__global__ void m_fin_kernel(int mode, int a, int G, const int* act, const double* part, BicgScalars* scs, const double* epsv)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= a) return;
-    BicgScalars* sc = scs + act[k];
-    const double eps = epsv ? epsv[act[k]] : 0.0;
     const int K = (mode == 1) ? 2 : 3;
     double s[3] = {0.0, 0.0, 0.0};
-    const double* pk = part + (size_t)K * G * k;
     for (int b = 0; b < G; b++)
-        for (int j = 0; j < K; j++) s[j] += pk[K * b + j];
+        for (int j = 0; j < K; j++) s[j] += __ldcg(pk + K * b + j);
     if (mode == 0) {
         sc->csk[0] = s[0];
         sc->csk[1] = s[1];
@@ -263,6 +189,112 @@ __global__ void m_fin_kernel(int mode, int a, int G, const int* act, const doubl
         }
     }
 }
+
+// Per-system finish, one thread per active system.
+__global__ void m_fin_kernel(int mode, int a, int G, const int* act, const double* part, BicgScalars* scs, const double* epsv)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a) return;
+    const int K = (mode == 1) ? 2 : 3;
+    m_fin_one(mode, G, part + (size_t)K * G * k, scs + act[k], epsv ? epsv[act[k]] : 0.0);
+}
+
+// After a CTA stored its partials: the last CTA of system k to finish (a
+// counter per system, reset here for the next launch) does the system's
+// finish, so no separate finish launch is needed.
+__device__ __forceinline__ void m_last_cta_fin(int mode, int k, int s, const double* part, BicgScalars* scs, const double* epsv,
+                                               unsigned* cnt)
+{
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&cnt[k], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const int K = (mode == 1) ? 2 : 3;
+        m_fin_one(mode, (int)gridDim.x, part + (size_t)K * gridDim.x * k, scs + s, epsv ? epsv[s] : 0.0);
+        cnt[k] = 0u;
+    }
+}
+
+// cap = p - M y0 ; caw = w - conj(y1) ; partial sum conj(w) cap
+template <typename T>
+__global__ void __launch_bounds__(MB) m_post_kernel(SlotMaps sm, const cpx<T>* an, int ld, const int* act, MultiVecs<T> v,
+                                                    const cpx<T>* YP, double* part, BicgScalars* scs, unsigned* cnt)
+{
+    const int k = blockIdx.y, s = act[k];
+    const size_t o = (size_t)s * ld;
+    const cpx<T>* y0 = YP + (size_t)(2 * k) * ld;
+    const cpx<T>* y1 = y0 + ld;
+    double acc[2] = {0.0, 0.0};
+    for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
+        SlotPos q = slot_pos(sm, e);
+        const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        cpx<T> u0 = y0[q.b0], u1 = y0[q.b1];
+        cpx<T> m0 = A[0] * u0 + A[2] * u1;
+        cpx<T> m1 = A[1] * u0 + A[3] * u1;
+        cpx<T> c0 = v.P[o + q.b0] - m0, c1 = v.P[o + q.b1] - m1;
+        v.CAP[o + q.b0] = c0;
+        v.CAP[o + q.b1] = c1;
+        cpx<T> w0 = v.W[o + q.b0], w1 = v.W[o + q.b1];
+        v.CAW[o + q.b0] = w0 - cj(y1[q.b0]);
+        v.CAW[o + q.b1] = w1 - cj(y1[q.b1]);
+        cpx<double> wd0 = upd_(w0), wd1 = upd_(w1), d0 = upd_(c0), d1 = upd_(c1);
+        acc[0] += wd0.x * d0.x + wd0.y * d0.y + wd1.x * d1.x + wd1.y * d1.y;
+        acc[1] += wd0.x * d0.y - wd0.y * d0.x + wd1.x * d1.y - wd1.y * d1.x;
+    }
+    mblock_store<2>(acc, part + 2 * ((size_t)k * gridDim.x + blockIdx.x));
+    if (cnt) m_last_cta_fin(1, k, s, part, scs, nullptr, cnt);
+}
+
+// x += a p ; r -= a cap ; q -= conj(a) caw ; partials sum conj(q) r, sum |r|^2
+template <typename T>
+__global__ void __launch_bounds__(MB) m_upd1_kernel(int ld, const int* act, BicgScalars* sc, MultiVecs<T> v, double* part, unsigned* cnt,
+                                                    const double* epsv)
+{
+    const int k = blockIdx.y, s = act[k];
+    const size_t o = (size_t)s * ld;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (!sc[s].breakdown) {
+        cpx<T> al = mk((T)sc[s].alpha[0], (T)sc[s].alpha[1]);
+        cpx<T> ac = cj(al);
+        for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+            size_t g = o + e;
+            v.X[g] = v.X[g] + al * v.P[g];
+            cpx<T> rv = v.R[g] - al * v.CAP[g];
+            cpx<T> qv = v.Q[g] - ac * v.CAW[g];
+            v.R[g] = rv;
+            v.Q[g] = qv;
+            cpx<double> rd = upd_(rv), qd = upd_(qv);
+            acc[0] += qd.x * rd.x + qd.y * rd.y;
+            acc[1] += qd.x * rd.y - qd.y * rd.x;
+            acc[2] += rd.x * rd.x + rd.y * rd.y;
+        }
+    }
+    mblock_store<3>(acc, part + 3 * ((size_t)k * gridDim.x + blockIdx.x));
+    if (cnt) m_last_cta_fin(2, k, s, part, sc, epsv, cnt);
+}
+
+// p = r + b p ; w = q + conj(b) w  (skipped once the system stopped)
+template <typename T>
+__global__ void __launch_bounds__(MB) m_upd2_kernel(int ld, const int* act, const BicgScalars* sc, MultiVecs<T> v)
+{
+    const int k = blockIdx.y, s = act[k];
+    if (sc[s].stop || sc[s].breakdown) return;
+    const size_t o = (size_t)s * ld;
+    cpx<T> b = mk((T)sc[s].beta[0], (T)sc[s].beta[1]);
+    cpx<T> bc = cj(b);
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+        size_t g = o + e;
+        v.P[g] = v.R[g] + b * v.P[g];
+        v.W[g] = v.Q[g] + bc * v.W[g];
+    }
+}
+
+// Per-system finish, one thread per active system (same logic as cbicg's
+// scalar steps): mode 0 after init, 1 after post, 2 after upd1.
 
 // Residual replacement of the systems in act: r was replaced by the true
 // residual; csk = sum conj(q) r, beta = csk / csk_prev, enorm = sum |r|^2
@@ -569,30 +601,41 @@ void launch_m_init(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const in
 }
 template <typename T>
 void launch_m_post(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const int* act, const MultiVecs<T>& v, const cpx<T>* YP,
-                   double* part, BicgScalars* sc, int nsm, cudaStream_t st)
+                   double* part, BicgScalars* sc, int nsm, cudaStream_t st, unsigned* cnt)
 {
     int G = multi_grid(sm.nslots, a, nsm);
-    m_post_kernel<T><<<dim3(G, a), MB, 0, st>>>(sm, an, ld, act, v, YP, part);
-    m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(1, a, G, act, part, sc, nullptr);
-    launch_counter() += 2;
+    m_post_kernel<T><<<dim3(G, a), MB, 0, st>>>(sm, an, ld, act, v, YP, part, sc, cnt);
+    launch_counter() += 1;
+    if (!cnt) {
+        m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(1, a, G, act, part, sc, nullptr);
+        launch_counter() += 1;
+    }
 }
 template <typename T>
 void launch_m_upd(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, const double* epsv, int nsm,
-                  cudaStream_t st)
+                  cudaStream_t st, unsigned* cnt)
 {
     int G = multi_grid(ld, a, nsm);
-    m_upd1_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v, part);
-    m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(2, a, G, act, part, sc, epsv);
+    m_upd1_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v, part, cnt, epsv);
+    launch_counter() += 1;
+    if (!cnt) {
+        m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(2, a, G, act, part, sc, epsv);
+        launch_counter() += 1;
+    }
     m_upd2_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v);
-    launch_counter() += 3;
+    launch_counter() += 1;
 }
 template <typename T>
-void launch_m_upd1(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, int nsm, cudaStream_t st)
+void launch_m_upd1(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, int nsm, cudaStream_t st,
+                   unsigned* cnt)
 {
     int G = multi_grid(ld, a, nsm);
-    m_upd1_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v, part);
-    m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(2, a, G, act, part, sc, nullptr);
-    launch_counter() += 2;
+    m_upd1_kernel<T><<<dim3(G, a), MB, 0, st>>>(ld, act, sc, v, part, cnt, nullptr);
+    launch_counter() += 1;
+    if (!cnt) {
+        m_fin_kernel<<<(a + 63) / 64, 64, 0, st>>>(2, a, G, act, part, sc, nullptr);
+        launch_counter() += 1;
+    }
 }
 template <typename T> void launch_m_upd2(int ld, int a, const int* act, const MultiVecs<T>& v, const BicgScalars* sc, int nsm, cudaStream_t st)
 {
@@ -670,9 +713,10 @@ void launch_tm_qext_qsca(int tmo, const zd* tmat, double xv, float* tc, double* 
     template void launch_m_init<T>(const SlotMaps&, const cpx<T>*, int, int, const int*, const cpx<T>*, const MultiVecs<T>&,         \
                                    const cpx<T>*, int, double*, BicgScalars*, int, cudaStream_t);                                   \
     template void launch_m_post<T>(const SlotMaps&, const cpx<T>*, int, int, const int*, const MultiVecs<T>&, const cpx<T>*, double*, \
-                                   BicgScalars*, int, cudaStream_t);                                                                \
-    template void launch_m_upd<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, const double*, int, cudaStream_t); \
-    template void launch_m_upd1<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, int, cudaStream_t);            \
+                                   BicgScalars*, int, cudaStream_t, unsigned*);                                                     \
+    template void launch_m_upd<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, const double*, int, cudaStream_t,  \
+                                  unsigned*);                                                                                       \
+    template void launch_m_upd1<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, int, cudaStream_t, unsigned*); \
     template void launch_m_upd2<T>(int, int, const int*, const MultiVecs<T>&, const BicgScalars*, int, cudaStream_t);               \
     template void launch_m_rrfix<T>(int, int, const int*, const MultiVecs<T>&, double*, BicgScalars*, int, cudaStream_t);
 INST(double)

@@ -21,14 +21,17 @@ void launch_m_init(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const in
                    const cpx<T>* YP, int have_y, double* part, BicgScalars* sc, int nsm, cudaStream_t st);
 template <typename T>
 void launch_m_post(const SlotMaps& sm, const cpx<T>* an, int ld, int a, const int* act, const MultiVecs<T>& v, const cpx<T>* YP,
-                   double* part, BicgScalars* sc, int nsm, cudaStream_t st);
+                   double* part, BicgScalars* sc, int nsm, cudaStream_t st, unsigned* cnt = nullptr);
 template <typename T>
 void launch_m_upd(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, const double* epsv, int nsm,
-                  cudaStream_t st);   // epsv[s]: stopping threshold of system s (device)
+                  cudaStream_t st, unsigned* cnt = nullptr);   // epsv[s]: stopping threshold of system s (device)
+// cnt (one zeroed counter per active position k, left zeroed): the last CTA of
+// each system does the scalar finish instead of a separate launch
 // the two halves of launch_m_upd for residual replacement: x, r, q update and
 // the scalar finish with no stopping threshold (csk_prev kept), then p, w
 template <typename T>
-void launch_m_upd1(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, int nsm, cudaStream_t st);
+void launch_m_upd1(int ld, int a, const int* act, const MultiVecs<T>& v, double* part, BicgScalars* sc, int nsm, cudaStream_t st,
+                   unsigned* cnt = nullptr);
 template <typename T> void launch_m_upd2(int ld, int a, const int* act, const MultiVecs<T>& v, const BicgScalars* sc, int nsm, cudaStream_t st);
 // residual replacement of the systems in act: csk, beta = csk / csk_prev and enorm from the replaced r
 template <typename T>
