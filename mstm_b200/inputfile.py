@@ -1,6 +1,7 @@
 """MSTM input files on this path: read the reference's input deck
 (keyword line, value line; `sphere_data` ... `end_of_sphere_data`;
-`end_of_options` between runs; `!` comments; Fortran literals such as
+`new_run` between runs, `end_of_options` at the end, `loop_variable`
+sweeps; `!` comments; Fortran literals such as
 `1.d-15`, `(1.6d0,0.d0)`, `t` / `f`), as variable_list_operation and
 inputdata read it (mstm-input-37.f90:148-933), and run the options of the
 solver path through the library:
@@ -60,6 +61,7 @@ OPTIONS = {
     "store_translation_matrix": ("l", True),
     "solution_method": ("a", "iterative"),
     "t_matrix_output_file": ("a", ""),
+    "append_output_file": ("l", False),
 }
 # options accepted only at values that keep the run on this path
 RESTRICTED = {
@@ -147,15 +149,40 @@ def parse_sphere_line(line):
     return x, y, z, r, ri
 
 
+def _loop_values(kind, start, stop, step, limit=100000):
+    """The values nested_loop (mstm-main-3.f90:110-179) gives a loop variable:
+    start, start+step, ... while |v - start| does not exceed |stop - start| by
+    more than 1e-6; returns (values, the value the variable is left with)."""
+    dist = (lambda a, b: abs(a - b))
+    maxdif = dist(stop, start)
+    if step == 0:
+        raise ValueError("loop_variable with a zero step")
+    vals, v = [], start
+    while True:
+        vals.append(v)
+        v = v + step
+        if dist(v, start) - maxdif > 1.0e-6:
+            return vals, v
+        if len(vals) >= limit:
+            raise ValueError("loop_variable gives more than %d runs" % limit)
+
+
 def parse(text):
-    """A list of runs (one per `end_of_options` block), each a dict of options
-    plus `spheres` (N x 4 positions/radii) and `ref_index` (N complex).  Later
-    runs inherit earlier settings, as the reference's option variables do."""
+    """The runs of an input deck, each a dict of options plus `spheres` (the
+    sphere_data lines).  As inputdata reads it (mstm-input-37.f90:736-933):
+    `new_run` ends a run and the next one starts from the same settings;
+    `end_of_options` ends the input (anything after it is not read);
+    `loop_variable name` + `start, stop, step` repeats the run over the
+    values (nested loops in the order declared, the first outermost; the
+    variable keeps the value past the end, as the reference leaves it);
+    `run_file` names the run log."""
     lines = [ln.rstrip("\n") for ln in text.splitlines()]
     runs, cur = [], {k: v for k, (t, v) in OPTIONS.items()}
     cur["_specified"] = ()
     cur.update({k: v for k, (t, v) in RESTRICTED.items()})
+    cur["run_file"] = ""
     spheres = []
+    loops = []
     i = 0
 
     def nextval():
@@ -167,13 +194,50 @@ def parse(text):
                 return v
         raise ValueError("unexpected end of input file")
 
+    def finish_run():
+        nonlocal loops
+        base = dict(cur, spheres=list(spheres))
+        combos = [dict()]
+        for name, kind, start, stop, step in loops:
+            vals, after = _loop_values(kind, start, stop, step)
+            combos = [dict(c, **{name: v}) for c in combos for v in vals]
+            cur[name] = after
+        for c in combos:
+            r = dict(base, **c)
+            if c:
+                r["_loop"] = dict(c)
+            runs.append(r)
+        loops = []
+
+    ended = False
     while i < len(lines):
         key = lines[i].strip().lower()
         i += 1
         if not key or key[0] in "!%":
             continue
+        if key == "new_run":
+            finish_run()
+            continue
         if key == "end_of_options":
-            runs.append(dict(cur, spheres=list(spheres)))
+            finish_run()
+            ended = True
+            break
+        if key == "run_file":
+            cur["run_file"] = nextval()
+            continue
+        if key == "loop_variable":
+            name = nextval().lower()
+            if name == "sphere_number":
+                raise NotImplementedError("loop_variable over a per-sphere quantity is outside this path")
+            if name not in OPTIONS or OPTIONS[name][0] not in "irc":
+                raise NotImplementedError(f"loop_variable {name!r}: not a numeric option of this path")
+            kind = OPTIONS[name][0]
+            it = _split_items(nextval())
+            if len(it) < 3:
+                raise ValueError(f"loop_variable {name}: needs start, stop, step")
+            start, stop, step = (_convert(kind, v) for v in it[:3])
+            loops.append((name, kind, start, stop, step))
+            cur["_specified"] = tuple(sorted(set(cur.get("_specified", ())) | {name}))
             continue
         if key == "sphere_data":
             spheres = []
@@ -196,8 +260,8 @@ def parse(text):
             cur[key] = _convert(RESTRICTED[key][0], nextval())
         else:
             raise NotImplementedError(f"input option {key!r} is outside the multiple-sphere solve this library replaces")
-    if not runs or runs[-1]["spheres"] != spheres or cur != {k: v for k, v in runs[-1].items() if k != "spheres"}:
-        runs.append(dict(cur, spheres=list(spheres)))
+    if not ended:
+        finish_run()   # a file without end_of_options ends as if it had one (mstm-main-3.f90:47)
     return runs
 
 
@@ -340,16 +404,24 @@ def main(argv=None):
     a = ap.parse_args(argv)
     with open(a.input) as f:
         runs = parse(f.read())
-    from .output import write_output
-    written = set()
-    for k, run in enumerate(runs):
-        run = dict(run, _run_number=k + 1)
+    from .output import output_header, write_output
+    # run numbers restart, and a file starts with the header, whenever the
+    # output file changes (mstm-main-3.f90:63-80)
+    old, number = None, 0
+    for run in runs:
+        first = run["output_file"] != old
+        if first:
+            old, number = run["output_file"], 0
+        number += 1
+        run = dict(run, _run_number=number)
         out = execute(run, a.precision)
         print(report(out))
-        # the output file in the reference's layout (print_run_variables +
-        # print_calculation_results), one block per run
-        write_output(run["output_file"], [(run, out)], append=run["output_file"] in written)
-        written.add(run["output_file"])
+        if first:
+            with open(run["output_file"], "a" if run["append_output_file"] else "w") as f:
+                f.write("\n".join(output_header(a.input)) + "\n")
+        # the run's blocks in the reference's layout (print_run_variables +
+        # print_calculation_results)
+        write_output(run["output_file"], [(run, out)], append=True)
 
 
 if __name__ == "__main__":

@@ -92,6 +92,15 @@ SMVEC0 = (1, 5, 9, 13, 2, 6, 10, 14, 3, 7, 11, 15, 4, 8, 12, 16)
 SMLABEL = ("11", "21", "31", "41", "12", "22", "32", "42", "13", "23", "33", "43", "14", "24", "34", "44")
 
 
+def output_header(input_file, when=None):
+    """output_header (mstm-input-37.f90:3120-3135): written once at the top of
+    an output file."""
+    import datetime
+    t = when or datetime.datetime.now()
+    stamp = t.strftime("%Y%m%d") + " " + t.strftime("%H%M%S.") + "%03d" % (t.microsecond // 1000)
+    return ["*" * 52, "*" * 52, label("mstm calculation results"), label("date, time:"), stamp, label("input file:"), input_file]
+
+
 def run_variables(run, out):
     """print_run_variables for one run: a list of records."""
     from .inputfile import cluster_arrays, medium_index

@@ -24,12 +24,13 @@ incident_beta_deg
 0.d0
 calculate_scattering_matrix
 t
-end_of_options
+new_run
 random_orientation
 t
 t_matrix_convergence_epsilon
 1.d-8
 end_of_options
+this line is after the end and is not read
 """
 
 
@@ -45,6 +46,25 @@ def test_parse_deck_and_literals():
     assert I._complex("(1.6d0,0.d0)") == 1.6 + 0j and I._real("1.d-15") == 1e-15
     alpha, sinc, d = I.incidence(dict(incident_beta_deg=120.0, incident_alpha_deg=30.0), 1.0 + 0j)
     assert d == 2 and abs(sinc - np.sin(120 * I.REF_PI / 180)) < 1e-15
+
+
+def test_run_structure_and_loop_variable():
+    """new_run separates runs that inherit settings, end_of_options ends the
+    input, loop_variable repeats a run over start..stop (stop included within
+    1e-6) in nested order, and leaves the variable one step past the end."""
+    deck = ("number_spheres\n1\nsphere_data\n0 0 0 1 1.5 0\nend_of_sphere_data\n"
+            "loop_variable\nincident_beta_deg\n0.d0,90.d0,45.d0\n"
+            "loop_variable\nmax_iterations\n10 20 10\n"
+            "new_run\nmie_epsilon\n-3\nend_of_options\nbogus_option\n1\n")
+    runs = I.parse(deck)
+    assert [(r["incident_beta_deg"], r["max_iterations"]) for r in runs[:6]] == \
+        [(0.0, 10), (0.0, 20), (45.0, 10), (45.0, 20), (90.0, 10), (90.0, 20)]
+    assert len(runs) == 7 and runs[6]["mie_epsilon"] == -3.0
+    assert runs[6]["incident_beta_deg"] == 135.0 and runs[6]["max_iterations"] == 30
+    vals, after = I._loop_values("r", 1.0, 0.0, -0.25)
+    assert vals == [1.0, 0.75, 0.5, 0.25, 0.0] and after == -0.25
+    with pytest.raises(NotImplementedError):
+        I.parse("loop_variable\nsphere_number\n2\nsphere_radius\n1 2 1\nend_of_options\n")
 
 
 def test_options_outside_the_path_are_rejected():
