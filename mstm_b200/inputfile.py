@@ -62,6 +62,10 @@ OPTIONS = {
     "solution_method": ("a", "iterative"),
     "t_matrix_output_file": ("a", ""),
     "append_output_file": ("l", False),
+    # accepted; their output blocks are not written (see output.py)
+    "calculate_up_down_scattering": ("l", True),
+    "print_timings": ("l", True),
+    "number_configurations": ("i", 0),   # used only with configuration_average (rejected)
 }
 # options accepted only at values that keep the run on this path
 RESTRICTED = {
@@ -78,6 +82,7 @@ RESTRICTED = {
     "single_origin_expansion": ("l", True),
     "numerical_azimuthal_average": ("l", False),
     "interaction_radius": ("r", 1.0e10),
+    "normalize_solution_error": ("l", True),
 }
 
 

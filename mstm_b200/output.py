@@ -3,7 +3,11 @@ block of print_run_variables (mstm-input-37.f90:3137-3304) and the results
 block of print_calculation_results (mstm-input-37.f90:3340-3751), with the
 same labels, record order and Fortran edit descriptors, for the branches this
 library covers (no plane boundaries, periodic lattices, configuration or
-incidence averages, near fields or Gaussian beams).
+incidence averages, near fields or Gaussian beams).  Not written: the down and
+up hemispherical scattering efficiencies (`calculate_up_down_scattering`,
+default on in the reference), which the reference computes with its
+plane-boundary routines (sphere_boundary_scattering), outside this path; a
+deck with `calculate_up_down_scattering f` gives the reference's records.
 """
 import math
 

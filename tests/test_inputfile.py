@@ -73,7 +73,7 @@ def test_options_outside_the_path_are_rejected():
     with pytest.raises(NotImplementedError):
         I.check_supported(run)
     with pytest.raises(NotImplementedError):
-        I.parse("calculate_up_down_scattering\nt\n")
+        I.parse("calculate_near_field_plane\nt\n")
 
 
 @pytest.mark.gpu
