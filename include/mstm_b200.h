@@ -56,8 +56,11 @@ typedef struct {
     int tile_ctas_per_sm;          /* tiled kernel CTAs per SM, 1 or 2 (0: as many as shared memory allows, at most 2) */
     int fp32_chunk;                /* columns per chunk of FP32 tiled passes, 2 or 4 (0: chosen per context by
                                       timing one pass of each on the first pass of 4 or more columns) */
-    int mixed_solver;              /* MSTMG_PRECISION_MIXED fixed-orientation solver: 0 FP32 BiCG with FP64
-                                      residual replacement (default), 1 restarted FP32 BiCG inside FP64 refinement */
+    int mixed_solver;              /* MSTMG_PRECISION_MIXED solver of the fixed-orientation and T-matrix
+                                      systems: 2 restarted GMRES, FP32 Arnoldi cycles from FP64 true
+                                      residuals (default; iterations then count Arnoldi steps in pairs);
+                                      0 FP32 BiCG with FP64 residual replacement; 1 restarted FP32 BiCG
+                                      inside FP64 refinement */
 } mstmg_opts;
 
 /* Fill opts with the defaults above. */

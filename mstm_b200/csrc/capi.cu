@@ -1,6 +1,8 @@
 // capi.cu -- the C ABI (include/mstm_b200.h): context set-up, the translation
 // matvec driver (sphereinteraction), the device BiCG (cbicg), the
 // fixed-orientation solve (fixedorsoln) and its mixed-precision variant.
+#include <algorithm>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <cmath>
@@ -148,6 +150,68 @@ template <typename T> struct MultiWork {
     }
 };
 
+// work of the many-system restarted GMRES (mrhs.cu gm_* kernels): basis
+// vector i of system s at V + (s (m + 1) + i) ne, up to m steps per cycle
+struct GmresWork {
+    int S = 0, m = 0, ne = 0;
+    DevBuf<zf> V, W, XP, Y, R;
+    // h: S squared norms (padded to even), then two Gram-Schmidt passes of (m + 1) S complex
+    DevBuf<double> h, rr;
+    DevBuf<int> act;
+    double* hh = nullptr;   // pinned host copy of the norms and the first pass
+    std::vector<std::complex<double>> Rm, g, sn;   // per system: rotated Hessenberg (m x (m + 1)), rhs, rotations
+    std::vector<double> cs, target, ybuf;
+    std::vector<int> kk;
+    std::vector<char> frozen;
+    GmresWork() = default;
+    GmresWork(const GmresWork&) = delete;
+    GmresWork& operator=(const GmresWork&) = delete;
+    ~GmresWork()
+    {
+        if (hh) cudaFreeHost(hh);
+    }
+    size_t off1() const { return (size_t)(S + (S & 1)); }
+    size_t hpass() const { return (size_t)(m + 1) * S * 2; }
+    // basis length from the free device memory: at most mmax vectors a system,
+    // the basis within a quarter of the free memory
+    static int pick_m(int S, int ne, int mmax)
+    {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
+        const size_t per = sizeof(zf) * (size_t)S * ne;
+        const size_t fit = fr / 4 / (per ? per : 1);
+        return (int)std::min<size_t>(mmax, fit > 1 ? fit - 1 : 0);
+    }
+    int init(int S_, int ne_, int m_)
+    {
+        if (S_ == S && ne_ == ne && m_ == m && hh) return MSTMG_OK;
+        S = S_;
+        ne = ne_;
+        m = m_;
+        const int spad = ((S + 3) / 4) * 4;
+        CK(V.alloc((size_t)(m + 1) * S * ne));
+        CK(W.alloc((size_t)S * ne));
+        CK(XP.alloc((size_t)spad * ne));
+        CK(Y.alloc((size_t)spad * ne));
+        CK(R.alloc((size_t)S * ne));
+        CK(h.alloc(off1() + 2 * hpass()));
+        CK(rr.alloc(2 * (size_t)S));
+        CK(act.alloc(S));
+        if (hh) cudaFreeHost(hh);
+        hh = nullptr;
+        CK(cudaMallocHost((void**)&hh, sizeof(double) * (off1() + hpass())));
+        Rm.assign((size_t)S * m * (m + 1), 0.0);
+        g.assign((size_t)S * (m + 1), 0.0);
+        sn.assign((size_t)S * m, 0.0);
+        cs.assign((size_t)S * m, 0.0);
+        target.assign(S, 0.0);
+        ybuf.assign(hpass(), 0.0);
+        kk.assign(S, 0);
+        frozen.assign(S, 0);
+        return MSTMG_OK;
+    }
+};
+
 struct mstmg_ctx {
     int dev = 0, nsm = 148;
     cudaStream_t st = nullptr;
@@ -177,6 +241,8 @@ struct mstmg_ctx {
     DevBuf<double> fo_rr;
     DevBuf<int> fo_idx;
     bool fo_ready = false;
+    GmresWork fo_gm;   // mixed_solver 2
+    bool fo_gm_ready = false;
     int chunk32 = 0;   // FP32 columns per tiled chunk chosen by timing (0: not yet)
     DevBuf<double> vcc, fnm1, fnc, fnp1, fnr, bcofd;
     int vn = 0;
@@ -244,7 +310,7 @@ extern "C" void mstmg_default_opts(mstmg_opts* o)
     o->generic_kernel = 0;
     o->tile_ctas_per_sm = 0;
     o->fp32_chunk = 0;
-    o->mixed_solver = 0;
+    o->mixed_solver = 2;
 }
 
 extern "C" const char* mstmg_last_error(void) { return g_err.c_str(); }
@@ -1248,6 +1314,8 @@ static int solve_mixed(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, int
 static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>& w32, DevBuf<double>& rr, DevBuf<int>& idx, int S,
                           const zd* B, zd* X, double eps, int niter, std::vector<int>& iters, std::vector<double>& errs,
                           std::vector<int>& status, int* outer_count);
+static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S, const zd* B, zd* X, double eps, int niter,
+                             std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count);
 
 
 static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, const double* x0, double fallback,
@@ -1337,6 +1405,27 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
             for (int p = 0; p < 2; p++) CK(cudaMemcpyAsync(xs[p], bs[p], sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
         if (c->opts.mixed_solver == 1) {
             rc = solve_mixed(c, bs, xs, eps, niter, it, er, st);
+        } else if (c->opts.mixed_solver == 2) {
+            // both polarisations as two systems of the restarted GMRES
+            if (!c->fo_gm_ready) {
+                const int m = GmresWork::pick_m(2, ne, 200);
+                if (m < 8) {
+                    set_err("mixed GMRES: no device memory for the basis");
+                    return MSTMG_ERR_CUDA;
+                }
+                if ((rc = c->fo64.init(2, ne, c->nsm, false)) || (rc = c->fo_gm.init(2, ne, m))) return rc;
+                c->fo_gm_ready = true;
+            }
+            std::vector<int> its, sts;
+            std::vector<double> ers;
+            int oc = 0;
+            rc = solve_multi_gmres(c, c->fo64, c->fo_gm, 2, bvec, c->amnp.p, eps, niter, its, ers, sts, &oc);
+            c->outer = oc;
+            for (int p = 0; p < 2; p++) {
+                it[p] = its[p];
+                er[p] = ers[p];
+                st[p] = sts[p];
+            }
         } else {
             // both polarisations as two systems of the many-system residual-replacement solver
             if (!c->fo_ready) {
@@ -1974,6 +2063,166 @@ static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>
     return check_kernel_err(c);
 }
 
+// Mixed precision for S systems by restarted GMRES.  A cycle starts from the
+// FP64 true residuals of its systems (one shared pass) and runs FP32 Arnoldi
+// steps: one translation pass over the basis vectors of the systems still
+// active, classical Gram-Schmidt applied twice with FP64 sums, and the
+// Givens-rotated least-squares residual of each system tracked on the host.
+// A system leaves the cycle when that estimate falls below its target
+// (eps |b|^2 / 4, but no deeper than inner_eps times the cycle's starting
+// residual; squared norms) or its Krylov space is invariant; the cycle ends
+// when no system is left or after m steps.  Each system's correction is then
+// summed into the FP64 solution X, and the next cycle's true residuals tell
+// which systems are done: squared residual ratio below eps, the cbicg test
+// of the reference.  iters counts Arnoldi steps in pairs (a BiCG iteration
+// is two matvecs), so the cap niter allows 2 niter steps.  X holds the
+// initial guesses on entry.
+static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S, const zd* B, zd* X, double eps, int niter,
+                             std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count)
+{
+    using C = std::complex<double>;
+    NvtxRange nvtx_("mixed GMRES");
+    const int ne = c->neqns, m = gw.m, m1 = gw.m + 1;
+    SlotMaps sm = c->sm();
+    const zf* an32 = (const zf*)c->an32.p;
+    const size_t O1 = gw.off1(), HP = gw.hpass();
+    double* h1 = gw.h.p + O1;
+    double* h2 = h1 + HP;
+    const long long cap = 2LL * std::max(niter, 0);
+    std::vector<int> act(S), cur;
+    std::vector<long long> steps(S, 0);
+    std::vector<double> hrr(2 * (size_t)S);
+    for (int s = 0; s < S; s++) act[s] = s;
+    iters.assign(S, 0);
+    errs.assign(S, 1.0);
+    status.assign(S, 0);
+    *outer_count = 0;
+    int rc;
+    auto rot = [&](int s) { return (size_t)s * m; };
+    auto colR = [&](int s, int j) { return &gw.Rm[((size_t)s * m + j) * m1]; };
+    for (int cyc = 0; cyc <= c->opts.max_outer && !act.empty(); cyc++) {
+        // FP64 true residuals of the cycle's systems into R (FP32, by system)
+        int a = (int)act.size();
+        const int apad = a == 1 ? 1 : ((a + 1) / 2) * 2;
+        CK(cudaMemcpyAsync(w64.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+        launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
+        if ((rc = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u))) return rc;
+        launch_m_resid<float>(sm, c->an.p, ne, a, w64.act.p, B, X, w64.YP.p, gw.R.p, w64.part.p, gw.rr.p, c->nsm, c->st, 1);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hrr.data(), gw.rr.p, sizeof(double) * 2 * S, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        (*outer_count)++;
+        std::vector<int> keep;
+        for (int s : act) {
+            const double bb = hrr[2 * s + 1];
+            errs[s] = bb > 0.0 ? hrr[2 * s] / bb : 0.0;
+            if (errs[s] >= eps && steps[s] < cap && status[s] != 2) keep.push_back(s);
+        }
+        act = keep;
+        a = (int)act.size();
+        if (a == 0 || cyc == c->opts.max_outer) break;
+        CK(cudaMemcpyAsync(gw.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+        // v_0 = r / |r|
+        launch_gm_scale(ne, m1, 0, a, gw.act.p, 1, gw.R.p, gw.rr.p, 2, 1.0e-35, gw.V.p, c->nsm, c->st);
+        long long room = cap;
+        for (int s : act) {
+            const double beta2 = hrr[2 * s];
+            gw.target[s] = std::max(0.25 * eps * hrr[2 * s + 1], c->opts.inner_eps * beta2);
+            std::fill(gw.g.begin() + (size_t)s * m1, gw.g.begin() + (size_t)(s + 1) * m1, C(0.0));
+            gw.g[(size_t)s * m1] = C(std::sqrt(beta2));
+            gw.kk[s] = 0;
+            gw.frozen[s] = 0;
+            room = std::min(room, cap - steps[s]);
+        }
+        cur = act;
+        const int jmax = (int)std::min<long long>(m, room);
+        for (int j = 0; j < jmax && !cur.empty(); j++) {
+            const int na = (int)cur.size();
+            const int npad = na <= 2 ? na : ((na + 3) / 4) * 4;   // whole FP32 chunks
+            launch_gm_gather(ne, m1, j, na, npad, gw.act.p, gw.V.p, gw.XP.p, c->nsm, c->st);
+            if ((rc = translate_many<float>(c, gw.XP.p, gw.Y.p, npad, 0u))) return rc;
+            launch_gm_apply(sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+            const size_t hn = (size_t)(j + 1) * S * 2;
+            CK(cudaMemsetAsync(gw.h.p, 0, sizeof(double) * (O1 + hn), c->st));
+            CK(cudaMemsetAsync(h2, 0, sizeof(double) * hn, c->st));
+            launch_gm_dots(ne, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h1, nullptr, c->nsm, c->st);
+            launch_gm_update(ne, S, m1, j + 1, na, gw.act.p, gw.V.p, h1, gw.W.p, nullptr, c->nsm, c->st);
+            launch_gm_dots(ne, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h2, h1, c->nsm, c->st);
+            launch_gm_update(ne, S, m1, j + 1, na, gw.act.p, gw.V.p, h2, gw.W.p, gw.h.p, c->nsm, c->st);
+            launch_gm_scale(ne, m1, j + 1, na, gw.act.p, 0, gw.W.p, gw.h.p, 1, 1.0e-35, gw.V.p, c->nsm, c->st);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(gw.hh, gw.h.p, sizeof(double) * (O1 + hn), cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            const double* H1 = gw.hh + O1;
+            std::vector<int> next;
+            for (int s : cur) {
+                C* col = colR(s, j);
+                double cn = 0.0;
+                for (int i = 0; i <= j; i++) {
+                    const size_t o = 2 * ((size_t)i * S + s);
+                    col[i] = C(H1[o], H1[o + 1]);
+                    cn += std::norm(col[i]);
+                }
+                const double hsub = std::sqrt(std::max(gw.hh[s], 0.0));
+                for (int i = 0; i < j; i++) {   // the earlier rotations
+                    const double ci = gw.cs[rot(s) + i];
+                    const C si = gw.sn[rot(s) + i];
+                    const C t = ci * col[i] + si * col[i + 1];
+                    col[i + 1] = -std::conj(si) * col[i] + ci * col[i + 1];
+                    col[i] = t;
+                }
+                const double aa = std::abs(col[j]), rho = std::sqrt(aa * aa + hsub * hsub);
+                if (rho == 0.0) {   // A v_j = 0: the operator is singular
+                    status[s] = 2;
+                    continue;
+                }
+                const C ph = aa > 0.0 ? col[j] / aa : C(1.0);
+                gw.cs[rot(s) + j] = aa / rho;
+                gw.sn[rot(s) + j] = ph * hsub / rho;
+                col[j] = ph * rho;
+                C* gs = &gw.g[(size_t)s * m1];
+                gs[j + 1] = -std::conj(gw.sn[rot(s) + j]) * gs[j];
+                gs[j] = gw.cs[rot(s) + j] * gs[j];
+                gw.kk[s] = j + 1;
+                // leave: estimate below target, or the Krylov space is invariant
+                if (std::norm(gs[j + 1]) >= gw.target[s] && hsub > 1.0e-13 * std::sqrt(cn + hsub * hsub)) next.push_back(s);
+            }
+            if (next.size() != cur.size()) {
+                cur = next;
+                if (!cur.empty()) CK(cudaMemcpyAsync(gw.act.p, cur.data(), sizeof(int) * cur.size(), cudaMemcpyHostToDevice, c->st));
+            }
+        }
+        // least-squares solutions (zero-padded to the longest), summed into X
+        int kmax = 0;
+        for (int s : act) kmax = std::max(kmax, gw.kk[s]);
+        if (kmax > 0) {
+            std::fill(gw.ybuf.begin(), gw.ybuf.begin() + (size_t)kmax * S * 2, 0.0);
+            std::vector<C> y(kmax);
+            for (int s : act) {
+                const int ks = gw.kk[s];
+                const C* gs = &gw.g[(size_t)s * m1];
+                for (int i = ks - 1; i >= 0; i--) {
+                    C t = gs[i];
+                    for (int l = i + 1; l < ks; l++) t -= colR(s, l)[i] * y[l];
+                    y[i] = t / colR(s, i)[i];
+                    gw.ybuf[2 * ((size_t)i * S + s)] = y[i].real();
+                    gw.ybuf[2 * ((size_t)i * S + s) + 1] = y[i].imag();
+                }
+                steps[s] += ks;
+            }
+            CK(cudaMemcpyAsync(gw.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(h2, gw.ybuf.data(), sizeof(double) * 2 * (size_t)kmax * S, cudaMemcpyHostToDevice, c->st));
+            launch_gm_combine(ne, S, m1, kmax, a, gw.act.p, gw.V.p, h2, X, c->nsm, c->st);
+            CK(cudaGetLastError());
+        }
+    }
+    for (int s = 0; s < S; s++) {
+        iters[s] = (int)((steps[s] + 1) / 2);
+        if (errs[s] >= eps && steps[s] >= cap) iters[s] = niter + 1;   // the cap was reached
+    }
+    return check_kernel_err(c);
+}
+
 extern "C" int mstmg_t_matrix_order(mstmg_ctx* c, double trans_eps, int max_t_order, int* t_matrix_order)
 {
     if (!c || max_t_order < 1 || !t_matrix_order) {
@@ -2042,6 +2291,15 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     MultiWork<double> w64;
     MultiWork<float> w32;
     if ((rc = w64.init(Smax, ne, c->nsm, !mixed))) return rc;
+    GmresWork gw;
+    if (mixed && c->opts.mixed_solver == 2) {
+        const int m = GmresWork::pick_m(Smax, ne, 200);
+        if (m < 8) {
+            set_err("mstmg_tmatrix: no device memory for the GMRES basis");
+            return MSTMG_ERR_CUDA;
+        }
+        if ((rc = gw.init(Smax, ne, m))) return rc;
+    }
     if (mixed) {
         if ((rc = w32.init(Smax, ne, c->nsm, true))) return rc;
         CK(X64.alloc((size_t)ne * Smax));
@@ -2084,6 +2342,8 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
             int oc = 0;
             if (c->opts.mixed_solver == 1)
                 rc = solve_multi_mixed(c, w64, w32, B32, rr, idx, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
+            else if (c->opts.mixed_solver == 2)
+                rc = solve_multi_gmres(c, w64, gw, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
             else
                 rc = solve_multi_rr(c, w64, w32, rr, idx, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
             outer_total += oc;

@@ -58,6 +58,113 @@ __device__ __forceinline__ SlotPos slot_pos(const SlotMaps& sm, int e)
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Restarted GMRES for many systems: Arnoldi with classical Gram-Schmidt
+// applied twice, FP32 vectors with FP64 sums.  Basis vector i of system s is
+// V + (s m1 + i) ld; a launch works on the a systems act[0..a) (packed work
+// columns W, XP, Y by position k, basis and norms by system s = act[k]).
+// ---------------------------------------------------------------------------
+// XP[:, k] = V_{act[k], j} for k < a, zero for a <= k < apad
+__global__ void __launch_bounds__(MB) gm_gather_kernel(int ld, int m1, int j, int a, const int* act, const zf* V, zf* XP)
+{
+    const int k = blockIdx.y;
+    const zf* v = k < a ? V + ((size_t)act[k] * m1 + j) * ld : nullptr;
+    zf* o = XP + (size_t)k * ld;
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) o[e] = v ? v[e] : mk(0.0f, 0.0f);
+}
+
+// W[:, k] = XP[:, k] - M Y[:, k]   (A v = v - M H v with Y = H v)
+__global__ void __launch_bounds__(MB) gm_apply_kernel(SlotMaps sm, const zf* an, int ld, const zf* XP, const zf* Y, zf* W)
+{
+    const size_t o = (size_t)blockIdx.y * ld;
+    for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
+        SlotPos q = slot_pos(sm, e);
+        const zf* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        const zf u0 = Y[o + q.b0], u1 = Y[o + q.b1];
+        W[o + q.b0] = XP[o + q.b0] - (A[0] * u0 + A[2] * u1);
+        W[o + q.b1] = XP[o + q.b1] - (A[1] * u0 + A[3] * u1);
+    }
+}
+
+// h[i S + s] += V_{s,i}^H W[:, k] (and hacc likewise when given), i = blockIdx.y
+__global__ void __launch_bounds__(MB) gm_dots_kernel(int ld, int S, int m1, const int* act, const zf* V, const zf* W, double* h, double* hacc)
+{
+    const int i = blockIdx.y, k = blockIdx.z, s = act[k];
+    const zf* v = V + ((size_t)s * m1 + i) * ld;
+    const zf* w = W + (size_t)k * ld;
+    double acc[2] = {0.0, 0.0};
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+        const cpx<double> x = upd_(v[e]), y = upd_(w[e]);
+        acc[0] += x.x * y.x + x.y * y.y;
+        acc[1] += x.x * y.y - x.y * y.x;
+    }
+    double out[2];
+    mblock_store<2>(acc, out);
+    if (threadIdx.x == 0) {
+        const size_t o = 2 * ((size_t)i * S + s);
+        atomicAdd(&h[o], out[0]);
+        atomicAdd(&h[o + 1], out[1]);
+        if (hacc) {
+            atomicAdd(&hacc[o], out[0]);
+            atomicAdd(&hacc[o + 1], out[1]);
+        }
+    }
+}
+
+// W[:, k] -= sum_{i < kp1} V_{s,i} h[i S + s] (FP64 accumulation per
+// element); nrm[s] += |W[:, k]|^2 of the result when nrm is given
+__global__ void __launch_bounds__(MB) gm_update_kernel(int ld, int S, int m1, int kp1, const int* act, const zf* V, const double* h, zf* W,
+                                                      double* nrm)
+{
+    const int k = blockIdx.y, s = act[k];
+    const zf* vs = V + (size_t)s * m1 * ld;
+    zf* w = W + (size_t)k * ld;
+    double n2[1] = {0.0};
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+        cpx<double> x = upd_(w[e]);
+        for (int i = 0; i < kp1; i++) {
+            const cpx<double> t = upd_(vs[(size_t)i * ld + e]) * mk(h[2 * ((size_t)i * S + s)], h[2 * ((size_t)i * S + s) + 1]);
+            x.x -= t.x;
+            x.y -= t.y;
+        }
+        const zf r = mk((float)x.x, (float)x.y);
+        w[e] = r;
+        n2[0] += (double)r.x * r.x + (double)r.y * r.y;
+    }
+    if (nrm) {
+        double out[1];
+        mblock_store<1>(n2, out);
+        if (threadIdx.x == 0) atomicAdd(&nrm[s], out[0]);
+    }
+}
+
+// V_{s,jd} = src / sqrt(nrm[s stride]) with src = Wsrc[:, s] (by_sys) or
+// Wsrc[:, k]; zero where the norm is below tiny
+__global__ void __launch_bounds__(MB) gm_scale_kernel(int ld, int m1, int jd, const int* act, int by_sys, const zf* Wsrc, const double* nrm,
+                                                     int stride, double tiny, zf* V)
+{
+    const int k = blockIdx.y, s = act[k];
+    const double n2 = nrm[(size_t)s * stride];
+    const float f = (n2 > tiny * tiny) ? (float)(1.0 / sqrt(n2)) : 0.0f;
+    const zf* w = Wsrc + (size_t)(by_sys ? s : k) * ld;
+    zf* d = V + ((size_t)s * m1 + jd) * ld;
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) d[e] = f * w[e];
+}
+
+// X[:, s] += sum_{i < kp1} y[i S + s] V_{s,i} (FP64)
+__global__ void __launch_bounds__(MB) gm_combine_kernel(int ld, int S, int m1, int kp1, const int* act, const zf* V, const double* y, zd* X)
+{
+    const int k = blockIdx.y, s = act[k];
+    const zf* vs = V + (size_t)s * m1 * ld;
+    zd* x = X + (size_t)s * ld;
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+        cpx<double> a = x[e];
+        for (int i = 0; i < kp1; i++)
+            a = a + upd_(vs[(size_t)i * ld + e]) * mk(y[2 * ((size_t)i * S + s)], y[2 * ((size_t)i * S + s) + 1]);
+        x[e] = a;
+    }
+}
+
 int multi_grid(int nslots, int a, int nsm)
 {
     int want = (4 * nsm + a - 1) / (a > 0 ? a : 1);
@@ -728,3 +835,38 @@ template void launch_m_resid<float>(const SlotMaps&, const zd*, int, int, const 
                                     int, cudaStream_t, int);
 template void launch_m_addcorr<float>(int, int, const int*, const int*, zd*, const zf*, cudaStream_t);
 template void launch_m_addcorr<double>(int, int, const int*, const int*, zd*, const zd*, cudaStream_t);
+
+// ---- GMRES launchers ----
+void launch_gm_gather(int ld, int m1, int j, int a, int apad, const int* act, const zf* V, zf* XP, int nsm, cudaStream_t st)
+{
+    gm_gather_kernel<<<dim3(multi_grid(ld, apad, nsm), apad), MB, 0, st>>>(ld, m1, j, a, act, V, XP);
+    launch_counter() += 1;
+}
+void launch_gm_apply(const SlotMaps& sm, const zf* an, int ld, int a, const zf* XP, const zf* Y, zf* W, int nsm, cudaStream_t st)
+{
+    gm_apply_kernel<<<dim3(multi_grid(sm.nslots, a, nsm), a), MB, 0, st>>>(sm, an, ld, XP, Y, W);
+    launch_counter() += 1;
+}
+void launch_gm_dots(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const zf* W, double* h, double* hacc, int nsm,
+                    cudaStream_t st)
+{
+    gm_dots_kernel<<<dim3(multi_grid(ld, kp1 * a, nsm), kp1, a), MB, 0, st>>>(ld, S, m1, act, V, W, h, hacc);
+    launch_counter() += 1;
+}
+void launch_gm_update(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* h, zf* W, double* nrm, int nsm,
+                      cudaStream_t st)
+{
+    gm_update_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, h, W, nrm);
+    launch_counter() += 1;
+}
+void launch_gm_scale(int ld, int m1, int jd, int a, const int* act, int by_sys, const zf* Wsrc, const double* nrm, int stride, double tiny,
+                     zf* V, int nsm, cudaStream_t st)
+{
+    gm_scale_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, m1, jd, act, by_sys, Wsrc, nrm, stride, tiny, V);
+    launch_counter() += 1;
+}
+void launch_gm_combine(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* y, zd* X, int nsm, cudaStream_t st)
+{
+    gm_combine_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, y, X);
+    launch_counter() += 1;
+}

@@ -46,6 +46,26 @@ template <typename TL> void launch_m_addcorr(int ld, int a, const int* dst, cons
 // Y[:, k] = M X[:, k] for k < ncols (Mie multiply, idir = 1)
 void launch_m_mie(const SlotMaps& sm, const zd* an, int ld, int ncols, const zd* X, zd* Y, cudaStream_t st);
 
+// ---- restarted GMRES for many systems (FP32 vectors, FP64 sums).  Basis
+//      vector i of system s at V + (s m1 + i) ld; a launch works on the a
+//      systems act[0..a) (device), packed work columns by position k, basis,
+//      h and norms by system s = act[k]; complex h, y as 2 doubles ----
+// XP[:, k] = V_{act[k], j}, k < a; zero columns a .. apad-1
+void launch_gm_gather(int ld, int m1, int j, int a, int apad, const int* act, const zf* V, zf* XP, int nsm, cudaStream_t st);
+// W[:, k] = XP[:, k] - M Y[:, k]
+void launch_gm_apply(const SlotMaps& sm, const zf* an, int ld, int a, const zf* XP, const zf* Y, zf* W, int nsm, cudaStream_t st);
+// h[i S + s] += V_{s,i}^H W[:, k] for i < kp1 (hacc too when given; both zeroed by the caller)
+void launch_gm_dots(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const zf* W, double* h, double* hacc, int nsm,
+                    cudaStream_t st);
+// W[:, k] -= sum_{i < kp1} V_{s,i} h[i S + s]; nrm[s] += |W[:, k]|^2 after it when nrm is given
+void launch_gm_update(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* h, zf* W, double* nrm, int nsm,
+                      cudaStream_t st);
+// V_{s,jd} = Wsrc[:, by_sys ? s : k] / sqrt(nrm[s stride]), zero when the norm is below tiny
+void launch_gm_scale(int ld, int m1, int jd, int a, const int* act, int by_sys, const zf* Wsrc, const double* nrm, int stride, double tiny,
+                     zf* V, int nsm, cudaStream_t st);
+// X[:, s] += sum_{i < kp1} y[i S + s] V_{s,i} in FP64
+void launch_gm_combine(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* y, zd* X, int nsm, cudaStream_t st);
+
 // ---- T matrix (tmatrix_solution, mstm-solver-8.f90:22-332) ----
 // columns of order l: unit TE (q=1) / TM (q=2) field of degree k in the LR basis
 void launch_tm_rhs(int l, zd* P0, cudaStream_t st);

@@ -158,6 +158,24 @@ def test_zero_rhs_and_iteration_cap(api, oracle_mod):
     assert abs(rg["maxerr"] / ro["maxerr"] - 1) < 1e-6
 
 
+def test_mixed_gmres_iteration_cap(api, oracle_mod):
+    """The mixed GMRES under an iteration cap below what the solve needs: 2
+    niter Arnoldi steps at most, solution status 1, the cap reported as niter + 1
+    (the Fortran DO-loop exit value), and the FP64 true residual of what it
+    returns as its error."""
+    pos, rad, ri, em = _cluster("fractal60")
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed")
+    r = g.fixedorsoln(eps=1e-12, niter=2)
+    assert r["istat"] == 1 and r["maxiter"] == 3 and r["maxerr"] > 1e-12
+    assert r["passes32"] <= 4
+    f = g.sphereplanewavecoef()
+    x = r["amnp"]
+    bm = _mie_times(g, f)
+    res = bm - x + g.sphereinteraction(x, initial_run=True)
+    rel = np.vdot(res[:, 1], res[:, 1]).real / np.vdot(bm[:, 1], bm[:, 1]).real
+    assert abs(rel / r["maxerr"] - 1) < 1e-6
+
+
 def test_bounded_wait_gives_up_and_device_stays_usable(api, oracle_mod):
     """The translation kernels' bounded mbarrier wait, run on a barrier that no
     copy completes, gives up and records MSTMG_ERR_CUDA instead of hanging; the
@@ -200,10 +218,16 @@ def test_fixedorsoln_fp64(api, oracle_mod, name, eps):
     assert np.abs(rg["amnp"] - ro["amnp"]).max() <= 1e-8 * np.abs(ro["amnp"]).max()
 
 
+@pytest.mark.parametrize("solver", [2, 0])
 @pytest.mark.parametrize("name", ["cluster20", "fractal60"])
-def test_fixedorsoln_mixed(api, oracle_mod, name):
+def test_fixedorsoln_mixed(api, oracle_mod, name, solver):
+    """Mixed fixed-orientation solve (solver 2: restarted GMRES, 0: BiCG with
+    residual replacement) to the FP64 true residual eps, efficiencies within
+    RTOL_MIXED of the FP64 oracle."""
     pos, rad, ri, em = _cluster(name)
     g, o = _pair(api, oracle_mod, pos, rad, ri, em, precision="mixed")
+    g.close()
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", mixed_solver=solver)
     eps = 1e-12   # ||r||/||b|| < 1e-6
     rg = g.fixedorsoln(eps=eps, niter=4000)
     ro = o.fixedorsoln(eps=eps, niter=4000)
@@ -341,12 +365,14 @@ def test_tmatrix_fp64(api, oracle_mod, name):
     assert abs(qe / rg["qtot"][0] - 1) < 1e-6 and abs(qs / rg["qtot"][2] - 1) < 1e-6
 
 
-@pytest.mark.parametrize("solver", [0, 1])
+@pytest.mark.parametrize("solver", [0, 1, 2])
 def test_tmatrix_mixed(api, oracle_mod, solver):
     """FP32 column solves with FP64 true residuals, all columns together
-    (solver 0: residual replacement, 1: restarts inside FP64 refinement): the
-    orientation-averaged efficiencies within 1e-6 of the FP64 oracle; residual
-    replacement needs at most 10 % more iterations than the FP64 column solves."""
+    (solver 0: residual replacement, 1: restarts inside FP64 refinement, 2:
+    restarted GMRES): the orientation-averaged efficiencies within 1e-6 of the
+    FP64 oracle; residual replacement needs at most 10 % more iterations than
+    the FP64 column solves, GMRES no more Arnoldi-step pairs than those have
+    iterations."""
     pos, rad, ri, em = _cluster("cluster20")
     g, o = _pair(api, oracle_mod, pos, rad, ri, em, precision="mixed")
     g.close()
@@ -359,6 +385,8 @@ def test_tmatrix_mixed(api, oracle_mod, solver):
         g64 = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="fp64")
         r64 = g64.tmatrix_solution(g64.t_matrix_order(), solution_eps=1e-14, convergence_eps=1e-6)
         assert rg["maxiter"] <= 1.1 * r64["maxiter"] + 2
+    if solver == 2:
+        assert rg["maxiter"] <= ro["maxiter"]
     assert np.allclose(rg["qtot"], ro["qtot"], rtol=RTOL_MIXED)
     assert np.abs(rg["tmat"] - ro["tmat"]).max() <= 1e-6 * np.abs(ro["tmat"]).max()
 
