@@ -185,6 +185,7 @@ struct GmresWork {
     int init(int S_, int ne_, int m_)
     {
         if (S_ == S && ne_ == ne && m_ == m && hh) return MSTMG_OK;
+        V.release();
         S = S_;
         ne = ne_;
         m = m_;
@@ -243,6 +244,7 @@ struct mstmg_ctx {
     bool fo_ready = false;
     GmresWork fo_gm;   // mixed_solver 2
     bool fo_gm_ready = false;
+    GmresWork tm_gm;   // mixed_solver 2, T-matrix columns: kept across calls (sized for the largest order)
     int chunk32 = 0;   // FP32 columns per tiled chunk chosen by timing (0: not yet)
     DevBuf<double> vcc, fnm1, fnc, fnp1, fnr, bcofd;
     int vn = 0;
@@ -2291,8 +2293,9 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     MultiWork<double> w64;
     MultiWork<float> w32;
     if ((rc = w64.init(Smax, ne, c->nsm, !mixed))) return rc;
-    GmresWork gw;
-    if (mixed && c->opts.mixed_solver == 2) {
+    GmresWork& gw = c->tm_gm;
+    if (mixed && c->opts.mixed_solver == 2 && !(gw.hh && gw.ne == ne && gw.S >= Smax)) {
+        gw.V.release();   // the old basis does not count against the new one's memory
         const int m = GmresWork::pick_m(Smax, ne, 200);
         if (m < 8) {
             set_err("mstmg_tmatrix: no device memory for the GMRES basis");
@@ -2301,11 +2304,13 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
         if ((rc = gw.init(Smax, ne, m))) return rc;
     }
     if (mixed) {
-        if ((rc = w32.init(Smax, ne, c->nsm, true))) return rc;
         CK(X64.alloc((size_t)ne * Smax));
-        CK(B32.alloc((size_t)ne * Smax));
-        CK(rr.alloc(2 * (size_t)Smax));
-        CK(idx.alloc(2 * (size_t)Smax));
+        if (c->opts.mixed_solver != 2) {   // FP32 BiCG work
+            if ((rc = w32.init(Smax, ne, c->nsm, true))) return rc;
+            CK(B32.alloc((size_t)ne * Smax));
+            CK(rr.alloc(2 * (size_t)Smax));
+            CK(idx.alloc(2 * (size_t)Smax));
+        }
     }
     zd* X = mixed ? X64.p : w64.v(ne).X;
     SlotMaps sm = c->sm();
