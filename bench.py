@@ -336,12 +336,20 @@ def run_extras(args, dev, stream):
     rng = np.random.default_rng(11)
     small = [C.rsa_sphere(int(rng.integers(15, 41)), 1.0, 0.10, seed=300 + k)[0] for k in range(48)]
     EN.solve_fixed_ensemble(small[:4], 1.0, 1.5 + 0.01j, workers=1)
-    f1 = EN.solve_fixed_ensemble(small, 1.0, 1.5 + 0.01j, workers=1)
-    f4 = EN.solve_fixed_ensemble(small, 1.0, 1.5 + 0.01j, workers=4)
+
+    def median_run(workers):
+        # wall-clock rate of a sub-second run: the median of three runs (host
+        # scheduling alone moves single runs by 2x here)
+        runs = sorted((EN.solve_fixed_ensemble(small, 1.0, 1.5 + 0.01j, workers=workers) for _ in range(3)),
+                      key=lambda f: f["solves_per_s"])
+        return runs[1]
+
+    f1 = median_run(1)
+    f4 = median_run(4)
     out["ensemble_fixed_small"] = {
         "workload": "48 configurations, 15-40 spheres (seeded), x=1.0, m=1.5+0.01i, RSA at fv 0.10: fixed orientation, "
                     "both polarisations to residual 1e-6 (mixed precision)",
-        "metric": "solves/s", "one_at_a_time": round(f1["solves_per_s"], 1), "four_streams": round(f4["solves_per_s"], 1),
+        "metric": "solves/s (median of 3 runs)", "one_at_a_time": round(f1["solves_per_s"], 1), "four_streams": round(f4["solves_per_s"], 1),
         "qext_rel_diff": abs(f4["qext_mean"] / f1["qext_mean"] - 1)}
     out["ensemble_tmatrix"] = {
         "workload": "6 configurations, 50-150 spheres (seeded), x=1.5, m=1.6+0.005i, RSA at fv 0.20: cluster T matrices, "

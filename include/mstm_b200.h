@@ -53,7 +53,8 @@ typedef struct {
     double inner_eps;              /* mixed mode: squared residual reduction per inner solve (default 1e-8) */
     int max_outer;                 /* mixed mode: refinement steps cap (default 30) */
     int generic_kernel;            /* 1: always use the order-generic translation kernel (default 0) */
-    int tile_ctas_per_sm;          /* tiled kernel CTAs per SM, 1 or 2 (0: as many as shared memory allows, at most 2) */
+    int tile_ctas_per_sm;          /* tiled kernel CTAs per SM, 1..3 caps it (0: as many as shared memory and the
+                                      kernel's register budget allow: 3 for FP32 passes of 1 or 2 columns, else 2) */
     int fp32_chunk;                /* columns per chunk of FP32 tiled passes, 2 or 4 (0: chosen per context by
                                       timing one pass of each on the first pass of 4 or more columns) */
     int mixed_solver;              /* MSTMG_PRECISION_MIXED solver of the fixed-orientation and T-matrix

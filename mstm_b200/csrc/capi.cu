@@ -246,7 +246,7 @@ struct mstmg_ctx {
     bool fo_gm_ready = false;
     GmresWork tm_gm;   // mixed_solver 2, T-matrix columns: kept across calls (sized for the largest order)
     int chunk32 = 0;   // FP32 columns per tiled chunk chosen by timing (0: not yet)
-    DevBuf<double> vcc, fnm1, fnc, fnp1, fnr, bcofd;
+    DevBuf<double> vcc, fnr, rfnr, bcofd;
     int vn = 0;
     DevBuf<int> err;
     DevBuf<zd> X64, Y64, pmnp, amnp, pw0, drot, vec64, bvec64;
@@ -550,17 +550,15 @@ static int setup_layout(mstmg_ctx* c)
     c->vn = lm;
     std::vector<double> bd(lm + 2, 0.0);
     for (int k = 0; k <= lm + 1; k++) bd[k] = tb.bc(k, k);
+    std::vector<double> rf(tb.fnr.size(), 0.0);
+    for (size_t k = 1; k < rf.size(); k++) rf[k] = 1.0 / tb.fnr[k];
     CK(c->vcc.alloc(vcc.size()));
-    CK(c->fnm1.alloc(f1.size()));
-    CK(c->fnc.alloc(f2.size()));
-    CK(c->fnp1.alloc(f3.size()));
     CK(c->fnr.alloc(tb.fnr.size()));
+    CK(c->rfnr.alloc(rf.size()));
     CK(c->bcofd.alloc(bd.size()));
     CK(cudaMemcpyAsync(c->vcc.p, vcc.data(), sizeof(double) * vcc.size(), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->fnm1.p, f1.data(), sizeof(double) * f1.size(), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->fnc.p, f2.data(), sizeof(double) * f2.size(), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->fnp1.p, f3.data(), sizeof(double) * f3.size(), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->fnr.p, tb.fnr.data(), sizeof(double) * tb.fnr.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->rfnr.p, rf.data(), sizeof(double) * rf.size(), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->bcofd.p, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice, c->st));
     // work buffers
     CK(c->X64.alloc(4LL * ne));
@@ -678,7 +676,7 @@ extern "C" int mstmg_ctx_create(mstmg_ctx** out, int nsphere, const double* pos,
 extern "C" void mstmg_ctx_destroy(mstmg_ctx* c)
 {
     if (!c) return;
-    DevBuf<double>* d[] = {&c->pos, &c->rad, &c->ri, &c->qext, &c->qabs, &c->op64, &c->vcc, &c->fnm1, &c->fnc, &c->fnp1, &c->fnr,
+    DevBuf<double>* d[] = {&c->pos, &c->rad, &c->ri, &c->qext, &c->qabs, &c->op64, &c->vcc, &c->fnr, &c->rfnr,
                            &c->bcofd, &c->part, &c->qeff, &c->qtot, &c->small};
     for (auto* b : d) b->release();
     DevBuf<int>* ib[] = {&c->d_order, &c->d_offset, &c->d_mie_offset, &c->slot, &c->slot_full, &c->err};
@@ -807,10 +805,8 @@ static int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
     a.op32 = need32 ? c->op32.p : nullptr;
     a.vcc = c->vcc.p;
     a.vnmax = c->vn;
-    a.fnm1 = c->fnm1.p;
-    a.fnc = c->fnc.p;
-    a.fnp1 = c->fnp1.p;
     a.fnr = c->fnr.p;
+    a.rfnr = c->rfnr.p;
     a.bcofd = c->bcofd.p;
     a.rimed_re = c->opts.medium_re;
     a.rimed_im = c->opts.medium_im;

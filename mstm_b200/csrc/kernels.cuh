@@ -12,10 +12,8 @@ struct OpGenArgs {
     float* op32;             // may be null
     const double* vcc;       // vcc_const(vn, vn(vn+2), 0:2vn)
     int vnmax;
-    const double* fnm1;      // (-vn:vn, 1:vn)
-    const double* fnc;
-    const double* fnp1;
-    const double* fnr;       // sqrt table
+    const double* fnr;       // fnr[k] = sqrt(k)
+    const double* rfnr;      // 1 / sqrt(k) (k >= 1)
     const double* bcofd;     // bcof(n,n)
     double rimed_re, rimed_im;
     int* err;

@@ -82,8 +82,14 @@ template <int L> __host__ __device__ constexpr int hidx(int m, int n) { return m
 
 }  // namespace
 
+// CTAs per SM the register budget is sized for: 3 for FP32 with one or two
+// columns (80 registers; the extra resident warps hide the pass's latencies:
+// fractal500 FP32, 2 columns, 2.27 -> 1.88 ms), 2 otherwise (FP64 and four
+// FP32 columns slow down at the smaller budget: FP64 2 columns 2.9 -> 4.1 ms).
+template <typename T, int NR> __host__ __device__ constexpr int tiled_minb() { return (sizeof(T) == 4 && NR <= 2) ? 3 : 2; }
+
 template <typename T, int L, int NR, int B>
-__global__ void __launch_bounds__(256, 2) translate_tiled_kernel(TiledArgs<T> a)
+__global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kernel(TiledArgs<T> a)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR;            // columns: ((dir*NR)+r)*2+p
@@ -452,7 +458,7 @@ template <typename T, int L, int NR, int B> static int launch_one(const TiledArg
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = (int)((228 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
-    if (per_sm > 2) per_sm = 2;
+    if (per_sm > tiled_minb<T, NR>()) per_sm = tiled_minb<T, NR>();
     if (a.ctas_per_sm >= 1 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
     int blocks = nsm * per_sm;
     if (blocks > a.ntiles * a.nchunk) blocks = a.ntiles * a.nchunk;

@@ -45,7 +45,7 @@ class Autotuner:
     (tiled or order-generic), chosen by timing a translation pass over the
     column count of the largest T-matrix order's batch."""
 
-    CANDIDATES = [dict(tile_ctas_per_sm=c, fp32_chunk=k, generic_kernel=0) for c in (1, 2) for k in (2, 4)] + \
+    CANDIDATES = [dict(tile_ctas_per_sm=c, fp32_chunk=k, generic_kernel=0) for c in (0, 2) for k in (2, 4)] + \
                  [dict(tile_ctas_per_sm=0, fp32_chunk=0, generic_kernel=1)]
 
     def __init__(self, reps=3):
