@@ -247,6 +247,7 @@ struct mstmg_ctx {
     GmresWork tm_gm;   // mixed_solver 2, T-matrix columns: kept across calls (sized for the largest order)
     int chunk32 = 0;   // FP32 columns per tiled chunk chosen by timing (0: not yet)
     DevBuf<double> vcc, fnr, rfnr, bcofd;
+    DevBuf<zd> opgen_xi;   // Hankel functions of every pair while the operators are generated
     int vn = 0;
     DevBuf<int> err;
     DevBuf<zd> X64, Y64, pmnp, amnp, pw0, drot, vec64, bvec64;
@@ -811,6 +812,8 @@ static int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
     a.rimed_re = c->opts.medium_re;
     a.rimed_im = c->opts.medium_im;
     a.err = c->err.p;
+    CK(c->opgen_xi.alloc(opgen_xi_scratch(c->npairs)));
+    a.xi = c->opgen_xi.p;
     launch_opgen(a, c->nsm, c->st);
     CK(cudaGetLastError());
     if (need64) c->ops64_ready = true;

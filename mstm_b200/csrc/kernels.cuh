@@ -17,9 +17,11 @@ struct OpGenArgs {
     const double* bcofd;     // bcof(n,n)
     double rimed_re, rimed_im;
     int* err;
+    zd* xi;                  // scratch, opgen_xi_scratch(npairs) complex: Hankel functions per pair
 };
 
 #include "oplayout.cuh"
+size_t opgen_xi_scratch(int npairs);
 void launch_opgen(const OpGenArgs& a, int nsm, cudaStream_t st);
 
 template <typename T> struct TransArgs {
