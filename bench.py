@@ -42,9 +42,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 EPS = 1.0e-12          # squared-norm criterion: ||r||/||b|| < 1e-6
-# DRAM bytes per algorithmic byte of the FP32 tiled translation pass, from the
-# ncu capture of the 200-sphere aggregate (163.95 MB of 158.9 MB)
-TRAFFIC_PER_ALG_BYTE = 163.95 / 158.9
+# DRAM bytes per algorithmic byte of the FP32 tiled translation pass of 2
+# columns, from the ncu capture of the 200-sphere aggregate (163.45 MB of
+# 158.56 MB)
+TRAFFIC_PER_ALG_BYTE = 163.45 / 158.56
 NITER = 10000
 WORKLOAD = "fractal500"
 METRIC = "solves/s at 1e-6 residual (fractal aggregate N=500, x=2, both polarisations)"
