@@ -41,7 +41,7 @@ extern "C" {
 #define MSTMG_ERR_BREAKDOWN (-4)
 
 #define MSTMG_PRECISION_FP64 0    /* drop-in: FP64 operators and BiCG, the reference's iteration */
-#define MSTMG_PRECISION_MIXED 1   /* FP32 inner BiCG + FP64 iterative refinement, polarisations batched */
+#define MSTMG_PRECISION_MIXED 1   /* FP32 Krylov passes from FP64 true residuals (mixed_solver), systems batched */
 
 typedef struct mstmg_ctx mstmg_ctx;
 
@@ -62,6 +62,8 @@ typedef struct {
                                       residuals (default; iterations then count Arnoldi steps in pairs);
                                       0 FP32 BiCG with FP64 residual replacement; 1 restarted FP32 BiCG
                                       inside FP64 refinement */
+    int gmres_restart;             /* mixed_solver 2: Arnoldi steps per cycle at most (0: up to 200, fewer
+                                      when a quarter of the free device memory cannot hold the basis) */
 } mstmg_opts;
 
 /* Fill opts with the defaults above. */

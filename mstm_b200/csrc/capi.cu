@@ -172,10 +172,11 @@ struct GmresWork {
     }
     size_t off1() const { return (size_t)(S + (S & 1)); }
     size_t hpass() const { return (size_t)(m + 1) * S * 2; }
-    // basis length from the free device memory: at most mmax vectors a system,
-    // the basis within a quarter of the free memory
-    static int pick_m(int S, int ne, int mmax)
+    // basis length from the free device memory: at most `cap` vectors a
+    // system (200 when cap is 0), the basis within a quarter of the free memory
+    static int pick_m(int S, int ne, int cap)
     {
+        const int mmax = cap > 0 ? cap : 200;
         size_t fr = 0, tot = 0;
         if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
         const size_t per = sizeof(zf) * (size_t)S * ne;
@@ -314,6 +315,7 @@ extern "C" void mstmg_default_opts(mstmg_opts* o)
     o->tile_ctas_per_sm = 0;
     o->fp32_chunk = 0;
     o->mixed_solver = 2;
+    o->gmres_restart = 0;
 }
 
 extern "C" const char* mstmg_last_error(void) { return g_err.c_str(); }
@@ -605,6 +607,10 @@ extern "C" int mstmg_ctx_create(mstmg_ctx** out, int nsphere, const double* pos,
                 return MSTMG_ERR_ARG;
             }
         }
+    }
+    if (opts && (opts->gmres_restart < 0 || opts->mixed_solver < 0 || opts->mixed_solver > 2)) {
+        set_err("mstmg_ctx_create: gmres_restart must be >= 0 and mixed_solver 0, 1 or 2");
+        return MSTMG_ERR_ARG;
     }
     mstmg_ctx* c = new mstmg_ctx();
     if (opts) c->opts = *opts;
@@ -1409,8 +1415,8 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
         } else if (c->opts.mixed_solver == 2) {
             // both polarisations as two systems of the restarted GMRES
             if (!c->fo_gm_ready) {
-                const int m = GmresWork::pick_m(2, ne, 200);
-                if (m < 8) {
+                const int m = GmresWork::pick_m(2, ne, c->opts.gmres_restart);
+                if (m < (c->opts.gmres_restart > 0 ? std::min(c->opts.gmres_restart, 8) : 8)) {
                     set_err("mixed GMRES: no device memory for the basis");
                     return MSTMG_ERR_CUDA;
                 }
@@ -2295,8 +2301,8 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     GmresWork& gw = c->tm_gm;
     if (mixed && c->opts.mixed_solver == 2 && !(gw.hh && gw.ne == ne && gw.S >= Smax)) {
         gw.V.release();   // the old basis does not count against the new one's memory
-        const int m = GmresWork::pick_m(Smax, ne, 200);
-        if (m < 8) {
+        const int m = GmresWork::pick_m(Smax, ne, c->opts.gmres_restart);
+        if (m < (c->opts.gmres_restart > 0 ? std::min(c->opts.gmres_restart, 8) : 8)) {
             set_err("mstmg_tmatrix: no device memory for the GMRES basis");
             return MSTMG_ERR_CUDA;
         }

@@ -73,3 +73,30 @@ def test_ctx_create_rejects_invalid_host_inputs(bad):
     assert rc == -1 and not ctx.value
     msg = L.mstmg_last_error().decode()
     assert ("sphere 2" if bad != "inf_index" else "sphere 1") in msg
+
+
+@pytest.mark.parametrize("field,value", [("gmres_restart", -1), ("mixed_solver", 3)])
+def test_ctx_create_rejects_invalid_solver_options(field, value):
+    """Out-of-range solver options are rejected with MSTMG_ERR_ARG before any
+    device call (runs on a machine without a GPU)."""
+    import ctypes
+
+    import numpy as np
+
+    from mstm_b200 import _lib
+    from mstm_b200 import build as B
+    if not os.path.exists(_lib.LIB_PATH):
+        B.build()
+    L = _lib.lib()
+    opts = _lib.MstmgOpts()
+    L.mstmg_default_opts(ctypes.byref(opts))
+    assert opts.mixed_solver == 2 and opts.gmres_restart == 0
+    setattr(opts, field, value)
+    pos = np.array([[0.0, 0.0, 0.0], [3.0, 0.0, 0.0]])
+    rad = np.array([1.0, 1.0])
+    ri = np.array([[1.5, 0.01], [1.5, 0.01]])
+    ctx = ctypes.c_void_p()
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = L.mstmg_ctx_create(ctypes.byref(ctx), 2, p(pos), p(rad), p(ri), -3.0, ctypes.byref(opts))
+    assert rc == -1 and not ctx.value
+    assert "gmres_restart" in L.mstmg_last_error().decode()

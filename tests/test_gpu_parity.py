@@ -176,6 +176,31 @@ def test_mixed_gmres_iteration_cap(api, oracle_mod):
     assert abs(rel / r["maxerr"] - 1) < 1e-6
 
 
+def test_mixed_gmres_short_cycles(api, oracle_mod):
+    """GMRES cycles capped at a few Arnoldi steps (gmres_restart), so the solve
+    restarts many times from FP64 true residuals: the fixed-orientation solve
+    and the T-matrix columns still meet the criterion and agree with the FP64
+    oracle within RTOL_MIXED."""
+    pos, rad, ri, em = _cluster("fractal60")
+    g, o = _pair(api, oracle_mod, pos, rad, ri, em, precision="mixed")
+    g.close()
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", gmres_restart=10)
+    rg = g.fixedorsoln(eps=1e-12, niter=4000)
+    ro = o.fixedorsoln(eps=1e-12, niter=4000)
+    assert rg["istat"] == 0 and rg["maxerr"] < 1e-12
+    assert rg["outer"] >= 4
+    assert np.allclose(rg["qtot"], ro["qtot"], rtol=RTOL_MIXED, atol=0)
+    pos, rad, ri, em = _cluster("cluster20")
+    g2, o2 = _pair(api, oracle_mod, pos, rad, ri, em, precision="mixed")
+    g2.close()
+    g2 = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", gmres_restart=6)
+    T = g2.t_matrix_order()
+    r2 = g2.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6)
+    ro2 = o2.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-12)
+    assert r2["istat"] == 0 and r2["order"] == ro2["order"]
+    assert np.allclose(r2["qtot"], ro2["qtot"], rtol=RTOL_MIXED)
+
+
 def test_bounded_wait_gives_up_and_device_stays_usable(api, oracle_mod):
     """The translation kernels' bounded mbarrier wait, run on a barrier that no
     copy completes, gives up and records MSTMG_ERR_CUDA instead of hanging; the
