@@ -347,11 +347,15 @@ def run_extras(args, dev, stream):
 
     f1 = median_run(1)
     f4 = median_run(4)
+    EN.solve_fixed_ensemble_batched(small[:4], 1.0, 1.5 + 0.01j)
+    fb = EN.solve_fixed_ensemble_batched(small, 1.0, 1.5 + 0.01j, reps=3)
     out["ensemble_fixed_small"] = {
         "workload": "48 configurations, 15-40 spheres (seeded), x=1.0, m=1.5+0.01i, RSA at fv 0.10: fixed orientation, "
                     "both polarisations to residual 1e-6 (mixed precision)",
         "metric": "solves/s (median of 3 runs)", "one_at_a_time": round(f1["solves_per_s"], 1), "four_streams": round(f4["solves_per_s"], 1),
-        "qext_rel_diff": abs(f4["qext_mean"] / f1["qext_mean"] - 1)}
+        "one_ensemble_context": round(fb["solves_per_s"], 1),
+        "qext_rel_diff": abs(f4["qext_mean"] / f1["qext_mean"] - 1),
+        "qext_rel_diff_one_context": abs(fb["qext_mean"] / f1["qext_mean"] - 1)}
     out["ensemble_tmatrix"] = {
         "workload": "6 configurations, 50-150 spheres (seeded), x=1.5, m=1.6+0.005i, RSA at fv 0.20: cluster T matrices, "
                     "orientation-averaged Qext/Qsca and scattering matrix, ensemble means",

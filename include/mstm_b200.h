@@ -241,6 +241,33 @@ int mstmg_fixed_orientation_guess(mstmg_ctx *ctx, double alpha, double sinc, int
                                   double fallback_residual, int *used_guess, double *guess_residual, double *amnp, double *qeff,
                                   double *qtot, double *maxerr, int *maxiter);
 
+/* Ensembles of independent configurations in one context; no counterpart in
+ * MSTM, which solves one configuration per run (its configuration_average_*
+ * drivers, input:1789, 2185, loop over configurations).  Configuration c holds
+ * spheres config_start[c] .. config_start[c+1]-1 (config_start[0] = 0,
+ * config_start[nconfig] = nsphere, every configuration non-empty); the
+ * context has no pairs between configurations, so its interaction matrix is
+ * block-diagonal.  Other arguments as mstmg_ctx_create.  Entry points that
+ * treat a context as one cluster (mstmg_bicg, mstmg_fixed_orientation*,
+ * mstmg_scattering, mstmg_t_matrix_order, mstmg_tmatrix, mstmg_fft_setup)
+ * return MSTMG_ERR_UNSUPPORTED on it; mstmg_interaction applies the
+ * block-diagonal operator. */
+int mstmg_ensemble_create(mstmg_ctx **ctx, int nconfig, const int *config_start, int nsphere, const double *pos, const double *radius,
+                          const double *ref_index, double mie_epsilon, const mstmg_opts *opts);
+/* fixedorsoln (solver:350-569) of every configuration at once: per
+ * configuration and polarisation the mixed GMRES (precision mixed,
+ * mixed_solver 2; MSTMG_ERR_UNSUPPORTED otherwise) from x0 = Mie f to the
+ * reference's criterion ||r||^2 / ||b||^2 < eps on that configuration's own
+ * system, all systems advancing together (one translation pass a step for
+ * the whole ensemble).  amnp: neqns x 2; qeff: 3 x 3 x nsphere (may be NULL);
+ * qtot: 3 x 3 per configuration, as qtotcalc forms it with the
+ * configuration's own volume radius (may be NULL); iterations, errors:
+ * 2 per configuration (polarisation fastest; may be NULL), iterations in
+ * Arnoldi-step pairs.  Returns 0, or 1 when any system missed the criterion
+ * within niter. */
+int mstmg_ensemble_fixed_orientation(mstmg_ctx *ctx, double alpha, double sinc, int dir, double eps, int niter, double *amnp,
+                                     double *qeff, double *qtot, int *iterations, double *errors);
+
 /* Learned warm start network primitives (warmstart.cu), all on device memory
  * and the given stream; no counterpart in MSTM.
  *   gemm: C[M x N] (+)= op(A)[M x K] op(B)[K x N]; A FP32 (lda), B BF16

@@ -27,6 +27,9 @@ SIGNATURES = {
     "mstmg_interaction": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "mstmg_bicg": (c_int, [c_void_p, c_int, c_double, c_void_p, c_void_p, c_int, P(c_int), P(c_double)]),
     "mstmg_planewave": (c_int, [c_void_p, c_double, c_double, c_int, c_void_p]),
+    "mstmg_ensemble_create": (c_int, [P(c_void_p), c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
+    "mstmg_ensemble_fixed_orientation": (c_int, [c_void_p, c_double, c_double, c_int, c_double, c_int, c_void_p, c_void_p, c_void_p,
+                                                 c_void_p, c_void_p]),
     "mstmg_fixed_orientation": (c_int, [c_void_p, c_double, c_double, c_int, c_double, c_int, c_void_p, c_void_p, c_void_p,
                                         P(c_double), P(c_int)]),
     "mstmg_scattering": (c_int, [c_void_p, c_void_p, c_double, c_int, c_int, c_void_p, P(c_double), P(c_int), c_void_p,

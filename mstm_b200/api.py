@@ -32,48 +32,9 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
-class SphereCluster:
-    """One cluster of external spheres in a medium (free space by default).
-
-    positions: (N,3); radii: (N,) size parameters; ref_index: (N,) complex or scalar.
-    mie_epsilon: MSTM's mie_epsilon (negative -L forces order L).
-    precision: "fp64" (drop-in) or "mixed" (FP32 inner BiCG, FP64 refinement).
-    """
-
-    def __init__(self, positions, radii, ref_index, mie_epsilon=1.0e-6, precision="fp64", device=0,
-                 medium_index=1.0, inner_eps=1.0e-8, max_outer=30, generic_kernel=False, tile_ctas_per_sm=0, fp32_chunk=0,
-                 mixed_solver=2, gmres_restart=0):
-        self._L = _lib.lib()
-        pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
-        rad = np.ascontiguousarray(np.asarray(radii, np.float64).reshape(-1))
-        n = len(rad)
-        ri = np.asarray(ref_index, np.complex128)
-        if ri.ndim == 0:
-            ri = np.full(n, ri)
-        ri2 = np.ascontiguousarray(np.stack([ri.real, ri.imag], axis=1))
-        opts = _lib.MstmgOpts()
-        self._L.mstmg_default_opts(ctypes.byref(opts))
-        opts.precision = PRECISIONS[precision]
-        opts.device = device
-        opts.medium_re = float(np.real(medium_index))
-        opts.medium_im = float(np.imag(medium_index))
-        opts.inner_eps = inner_eps
-        opts.max_outer = max_outer
-        opts.generic_kernel = int(generic_kernel)
-        opts.tile_ctas_per_sm = int(tile_ctas_per_sm)
-        opts.fp32_chunk = int(fp32_chunk)
-        opts.mixed_solver = int(mixed_solver)
-        opts.gmres_restart = int(gmres_restart)
-        self.ctx = ctypes.c_void_p()
-        check(self._L.mstmg_ctx_create(ctypes.byref(self.ctx), n, _ptr(pos), _ptr(rad), _ptr(ri2), float(mie_epsilon),
-                                       ctypes.byref(opts)), "mstmg_ctx_create")
-        self.number_spheres = n
-        self.positions, self.radii = pos, rad
-        self.number_eqns = self._L.mstmg_neqns(self.ctx)
-        self.sphere_order = np.zeros(n, np.int32)
-        self.sphere_offset = np.zeros(n + 1, np.int32)
-        check(self._L.mstmg_sphere_orders(self.ctx, _ptr(self.sphere_order), _ptr(self.sphere_offset)), "orders")
-        self.precision = precision
+class _Context:
+    """What a cluster context and an ensemble context share: lifetime, the
+    Mie coefficients, positions, the interaction matvec and solve statistics."""
 
     def close(self):
         if self.ctx:
@@ -118,6 +79,58 @@ class SphereCluster:
         check(self._L.mstmg_interaction(self.ctx, nrhs, _ptr(ain), _ptr(out), _ptr(ct), _ptr(mm), int(initial_run)),
               "sphereinteraction")
         return out
+
+
+    def last_stats(self):
+        it = np.zeros(2, np.int32)
+        outer, p64, p32 = c_int(0), c_int(0), c_int(0)
+        check(self._L.mstmg_last_stats(self.ctx, _ptr(it), ctypes.byref(outer), ctypes.byref(p64), ctypes.byref(p32)),
+              "stats")
+        return dict(iterations=it.tolist(), outer=outer.value, passes64=p64.value, passes32=p32.value)
+
+class SphereCluster(_Context):
+    """One cluster of external spheres in a medium (free space by default).
+
+    positions: (N,3); radii: (N,) size parameters; ref_index: (N,) complex or scalar.
+    mie_epsilon: MSTM's mie_epsilon (negative -L forces order L).
+    precision: "fp64" (drop-in) or "mixed" (FP32 Krylov passes from FP64 true
+    residuals; mixed_solver 2 = restarted GMRES, the default).
+    """
+
+    def __init__(self, positions, radii, ref_index, mie_epsilon=1.0e-6, precision="fp64", device=0,
+                 medium_index=1.0, inner_eps=1.0e-8, max_outer=30, generic_kernel=False, tile_ctas_per_sm=0, fp32_chunk=0,
+                 mixed_solver=2, gmres_restart=0):
+        self._L = _lib.lib()
+        pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
+        rad = np.ascontiguousarray(np.asarray(radii, np.float64).reshape(-1))
+        n = len(rad)
+        ri = np.asarray(ref_index, np.complex128)
+        if ri.ndim == 0:
+            ri = np.full(n, ri)
+        ri2 = np.ascontiguousarray(np.stack([ri.real, ri.imag], axis=1))
+        opts = _lib.MstmgOpts()
+        self._L.mstmg_default_opts(ctypes.byref(opts))
+        opts.precision = PRECISIONS[precision]
+        opts.device = device
+        opts.medium_re = float(np.real(medium_index))
+        opts.medium_im = float(np.imag(medium_index))
+        opts.inner_eps = inner_eps
+        opts.max_outer = max_outer
+        opts.generic_kernel = int(generic_kernel)
+        opts.tile_ctas_per_sm = int(tile_ctas_per_sm)
+        opts.fp32_chunk = int(fp32_chunk)
+        opts.mixed_solver = int(mixed_solver)
+        opts.gmres_restart = int(gmres_restart)
+        self.ctx = ctypes.c_void_p()
+        check(self._L.mstmg_ctx_create(ctypes.byref(self.ctx), n, _ptr(pos), _ptr(rad), _ptr(ri2), float(mie_epsilon),
+                                       ctypes.byref(opts)), "mstmg_ctx_create")
+        self.number_spheres = n
+        self.positions, self.radii = pos, rad
+        self.number_eqns = self._L.mstmg_neqns(self.ctx)
+        self.sphere_order = np.zeros(n, np.int32)
+        self.sphere_offset = np.zeros(n + 1, np.int32)
+        check(self._L.mstmg_sphere_orders(self.ctx, _ptr(self.sphere_order), _ptr(self.sphere_offset)), "orders")
+        self.precision = precision
 
     def sphereinteraction_ex(self, ain, con_tran=None, mie_mult=None, initial_run=False, rhs_list=None, fft_option=-1,
                              store_matrix_option=True, skip_external_translation=False):
@@ -292,13 +305,6 @@ class SphereCluster:
             out["smat"] = smat.reshape(nangles, 4, 4).transpose(0, 2, 1).copy()
         return out
 
-    def last_stats(self):
-        it = np.zeros(2, np.int32)
-        outer, p64, p32 = c_int(0), c_int(0), c_int(0)
-        check(self._L.mstmg_last_stats(self.ctx, _ptr(it), ctypes.byref(outer), ctypes.byref(p64), ctypes.byref(p32)),
-              "stats")
-        return dict(iterations=it.tolist(), outer=outer.value, passes64=p64.value, passes32=p32.value)
-
     def operator_bytes(self, precision="fp64"):
         s, c = c_double(0.0), c_double(0.0)
         check(self._L.mstmg_operator_bytes(self.ctx, PRECISIONS[precision], ctypes.byref(s), ctypes.byref(c)), "bytes")
@@ -308,6 +314,72 @@ class SphereCluster:
         ms = c_double(0.0)
         check(self._L.mstmg_time_translation(self.ctx, PRECISIONS[precision], nrhs, reps, ctypes.byref(ms)), "time")
         return ms.value
+
+
+class SphereEnsemble(_Context):
+    """Independent configurations solved together (mstmg_ensemble_create; no
+    counterpart in MSTM, which solves one configuration per run).
+
+    configs: list of (positions (N_c, 3), radii (N_c,), ref_index (N_c,) or
+    scalar).  The context holds no pairs between configurations, and
+    fixedorsoln() runs every configuration's two polarisations through the
+    mixed GMRES together, one translation pass a step for the whole ensemble,
+    each system to the reference's criterion on its own configuration.
+    """
+
+    def __init__(self, configs, mie_epsilon=1.0e-6, device=0, medium_index=1.0, gmres_restart=0, max_outer=30, inner_eps=1.0e-8,
+                 tile_ctas_per_sm=0):
+        self._L = _lib.lib()
+        pos, rad, ri, start = [], [], [], [0]
+        for p_, r_, m_ in configs:
+            p_ = np.asarray(p_, np.float64).reshape(-1, 3)
+            r_ = np.asarray(r_, np.float64).reshape(-1)
+            m_ = np.asarray(m_, np.complex128)
+            pos.append(p_)
+            rad.append(r_)
+            ri.append(np.full(len(r_), m_) if m_.ndim == 0 else m_.reshape(-1))
+            start.append(start[-1] + len(r_))
+        pos = np.ascontiguousarray(np.concatenate(pos))
+        rad = np.ascontiguousarray(np.concatenate(rad))
+        ri = np.concatenate(ri)
+        ri2 = np.ascontiguousarray(np.stack([ri.real, ri.imag], axis=1))
+        self.config_start = np.ascontiguousarray(start, np.int32)
+        self.number_configs = len(configs)
+        opts = _lib.MstmgOpts()
+        self._L.mstmg_default_opts(ctypes.byref(opts))
+        opts.precision = PRECISIONS["mixed"]
+        opts.device = device
+        opts.medium_re = float(np.real(medium_index))
+        opts.medium_im = float(np.imag(medium_index))
+        opts.gmres_restart = int(gmres_restart)
+        opts.max_outer = max_outer
+        opts.inner_eps = inner_eps
+        opts.tile_ctas_per_sm = int(tile_ctas_per_sm)
+        self.ctx = ctypes.c_void_p()
+        check(self._L.mstmg_ensemble_create(ctypes.byref(self.ctx), self.number_configs, _ptr(self.config_start), len(rad), _ptr(pos),
+                                            _ptr(rad), _ptr(ri2), float(mie_epsilon), ctypes.byref(opts)), "mstmg_ensemble_create")
+        self.number_spheres = len(rad)
+        self.number_eqns = self._L.mstmg_neqns(self.ctx)
+        self.sphere_order = np.zeros(len(rad), np.int32)
+        self.sphere_offset = np.zeros(len(rad) + 1, np.int32)
+        check(self._L.mstmg_sphere_orders(self.ctx, _ptr(self.sphere_order), _ptr(self.sphere_offset)), "orders")
+
+    def fixedorsoln(self, eps=1.0e-6, niter=10000, alpha=0.0, sinc=0.0, direction=1):
+        """Returns dict(amnp (neqns, 2), qeff (3, 3, N), qtot (nconfig, 3, 3),
+        iterations (nconfig, 2) in Arnoldi-step pairs, errors (nconfig, 2),
+        istat, and amnp_of(c): configuration c's rows of amnp)."""
+        nc = self.number_configs
+        amnp = np.zeros((self.number_eqns, 2), np.complex128, order="F")
+        qeff = np.zeros((3, 3, self.number_spheres), np.float64, order="F")
+        qtot = np.zeros((3, 3, nc), np.float64, order="F")
+        its = np.zeros(2 * nc, np.int32)
+        errs = np.zeros(2 * nc, np.float64)
+        st = check(self._L.mstmg_ensemble_fixed_orientation(self.ctx, alpha, sinc, direction, eps, niter, _ptr(amnp), _ptr(qeff), _ptr(qtot),
+                                                            _ptr(its), _ptr(errs)), "ensemble fixedorsoln")
+        off = self.sphere_offset
+        start = self.config_start
+        return dict(amnp=amnp, qeff=qeff, qtot=np.moveaxis(qtot, 2, 0).copy(), iterations=its.reshape(nc, 2), errors=errs.reshape(nc, 2),
+                    istat=st, amnp_of=lambda c: amnp[off[start[c]]:off[start[c + 1]]])
 
 
 def qtotcalc(qeff, radii, vol_radius):

@@ -246,6 +246,14 @@ struct mstmg_ctx {
     GmresWork fo_gm;   // mixed_solver 2
     bool fo_gm_ready = false;
     GmresWork tm_gm;   // mixed_solver 2, T-matrix columns: kept across calls (sized for the largest order)
+    // ensembles (mstmg_ensemble_create): configuration c holds spheres
+    // cfg_start[c] .. cfg_start[c+1]-1; no pairs between configurations
+    std::vector<int> cfg_start, cfg_of;
+    std::vector<double> cfg_xg;   // volume-equivalent radius of each configuration
+    DevBuf<int> d_cfg_start, ens_off, ens_len;
+    DevBuf<double> d_cfg_xg, cfg_qtot;
+    GmresWork ens_gm;
+    int ens_ldv = 0;
     int chunk32 = 0;   // FP32 columns per tiled chunk chosen by timing (0: not yet)
     DevBuf<double> vcc, fnr, rfnr, bcofd;
     DevBuf<zd> opgen_xi;   // Hankel functions of every pair while the operators are generated
@@ -337,6 +345,16 @@ static void resolve_timing(mstmg_ctx* c)
         }
     }
     c->pending.swap(keep);
+}
+
+// entry points that treat the context as one cluster refuse an ensemble
+static int reject_ensemble(const mstmg_ctx* c, const char* fn)
+{
+    if (c && !c->cfg_start.empty()) {
+        set_err(std::string(fn) + ": not available on an ensemble context (mstmg_ensemble_fixed_orientation solves ensembles)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    return MSTMG_OK;
 }
 
 static int check_kernel_err(mstmg_ctx* c)
@@ -444,13 +462,15 @@ static int setup_layout(mstmg_ctx* c)
     // reference's dense path (coefficient_translation, rot_op false)
     const int tso = c->opts.translation_switch_order;
     auto dense_pair = [&](int i, int j) { return std::min(c->order[i], c->order[j]) < tso; };
+    // an ensemble has no pairs between its configurations
+    auto same_cfg = [&](int i, int j) { return c->cfg_of.empty() || c->cfg_of[i] == c->cfg_of[j]; };
     {
         std::vector<int2> dp;
         std::vector<long long> doff;
         long long du = 0;
         for (int i = 0; i < n; i++)
             for (int j = i + 1; j < n; j++)
-                if (dense_pair(i, j)) {
+                if (same_cfg(i, j) && dense_pair(i, j)) {
                     dp.push_back(make_int2(i, j));
                     doff.push_back(du);
                     du += 2LL * c->order[i] * (c->order[i] + 2) * c->order[j] * (c->order[j] + 2);
@@ -478,6 +498,13 @@ static int setup_layout(mstmg_ctx* c)
     }
     // pair list (i < j, the reference's loop order) and operator offsets
     long long np = (long long)n * (n - 1) / 2 - c->ndense;
+    if (!c->cfg_of.empty()) {
+        np = -c->ndense;
+        for (size_t k = 0; k + 1 < c->cfg_start.size(); k++) {
+            const long long m = c->cfg_start[k + 1] - c->cfg_start[k];
+            np += m * (m - 1) / 2;
+        }
+    }
     if (np > 2000000000LL) {
         set_err("too many sphere pairs for the direct translation path");
         return MSTMG_ERR_UNSUPPORTED;
@@ -528,7 +555,7 @@ static int setup_layout(mstmg_ctx* c)
             int start = (int)t;
             for (int i = i0; i < std::min(n, i0 + B); i++)
                 for (int j = j0; j < std::min(n, j0 + B); j++)
-                    if (i < j) add_pair(i, j);
+                    if (i < j && same_cfg(i, j)) add_pair(i, j);
             int cnt = (int)t - start;
             if (cnt > 0) tl.push_back(make_int4(start, cnt, (i0 << 16) | j0, I == J ? 1 : 0));
         }
@@ -536,7 +563,7 @@ static int setup_layout(mstmg_ctx* c)
         std::vector<std::pair<int, int>> pp;
         tournament(n, pp);
         for (auto& ij : pp)
-            if (!dense_pair(ij.first, ij.second)) add_pair(ij.first, ij.second);
+            if (same_cfg(ij.first, ij.second) && !dense_pair(ij.first, ij.second)) add_pair(ij.first, ij.second);
     }
     if (t != np) {
         set_err("internal error: pair schedule incomplete");
@@ -585,12 +612,62 @@ static int setup_layout(mstmg_ctx* c)
     double v = 0.0;
     for (int i = 0; i < n; i++) v = v + c->radius[i] * c->radius[i] * c->radius[i];
     c->xg = std::pow(v, (double)0.333333f);
+    if (!c->cfg_start.empty()) {
+        const int nc = (int)c->cfg_start.size() - 1;
+        c->cfg_xg.assign(nc, 0.0);
+        std::vector<int> off(2 * nc), len(2 * nc);
+        c->ens_ldv = 0;
+        for (int k = 0; k < nc; k++) {
+            double vk = 0.0;
+            for (int i = c->cfg_start[k]; i < c->cfg_start[k + 1]; i++) vk = vk + c->radius[i] * c->radius[i] * c->radius[i];
+            c->cfg_xg[k] = std::pow(vk, (double)0.333333f);
+            const int o = c->offset[c->cfg_start[k]], l = c->offset[c->cfg_start[k + 1]] - o;
+            off[2 * k] = off[2 * k + 1] = o;
+            len[2 * k] = len[2 * k + 1] = l;
+            c->ens_ldv = std::max(c->ens_ldv, l);
+        }
+        c->ens_ldv = ((c->ens_ldv + 3) / 4) * 4;
+        CK(c->d_cfg_start.alloc(nc + 1));
+        CK(c->d_cfg_xg.alloc(nc));
+        CK(c->cfg_qtot.alloc(9LL * nc));
+        CK(c->ens_off.alloc(2 * nc));
+        CK(c->ens_len.alloc(2 * nc));
+        CK(cudaMemcpyAsync(c->d_cfg_start.p, c->cfg_start.data(), sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->d_cfg_xg.p, c->cfg_xg.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->ens_off.p, off.data(), sizeof(int) * 2 * nc, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->ens_len.p, len.data(), sizeof(int) * 2 * nc, cudaMemcpyHostToDevice, c->st));
+    }
     CK(cudaStreamSynchronize(c->st));
     return MSTMG_OK;
 }
 
+static int create_impl(mstmg_ctx** out, int nsphere, const double* pos, const double* radius, const double* ref_index, double mie_epsilon,
+                       const mstmg_opts* opts, int nconfig, const int* config_start);
+
 extern "C" int mstmg_ctx_create(mstmg_ctx** out, int nsphere, const double* pos, const double* radius, const double* ref_index,
                                 double mie_epsilon, const mstmg_opts* opts)
+{
+    return create_impl(out, nsphere, pos, radius, ref_index, mie_epsilon, opts, 0, nullptr);
+}
+
+extern "C" int mstmg_ensemble_create(mstmg_ctx** out, int nconfig, const int* config_start, int nsphere, const double* pos,
+                                     const double* radius, const double* ref_index, double mie_epsilon, const mstmg_opts* opts)
+{
+    if (out) *out = nullptr;
+    if (nconfig < 1 || !config_start || config_start[0] != 0 || config_start[nconfig] != nsphere) {
+        set_err("mstmg_ensemble_create: config_start must run from 0 to nsphere over nconfig >= 1 configurations");
+        return MSTMG_ERR_ARG;
+    }
+    for (int k = 0; k < nconfig; k++)
+        if (config_start[k + 1] <= config_start[k]) {
+            set_err("mstmg_ensemble_create: configuration " + std::to_string(k + 1) + " has no spheres");
+            return MSTMG_ERR_ARG;
+        }
+    return create_impl(out, nsphere, pos, radius, ref_index, mie_epsilon, opts, nconfig, config_start);
+}
+
+static int create_impl(mstmg_ctx** out, int nsphere, const double* pos, const double* radius, const double* ref_index, double mie_epsilon,
+                       const mstmg_opts* opts, int nconfig, const int* config_start)
 {
     if (!out || nsphere < 1 || !pos || !radius || !ref_index) {
         set_err("mstmg_ctx_create: bad arguments");
@@ -674,6 +751,12 @@ extern "C" int mstmg_ctx_create(mstmg_ctx** out, int nsphere, const double* pos,
         return fail(MSTMG_ERR_CUDA);
     }
     ord.release();
+    if (nconfig > 0) {
+        c->cfg_start.assign(config_start, config_start + nconfig + 1);
+        c->cfg_of.assign(nsphere, 0);
+        for (int k = 0; k < nconfig; k++)
+            for (int i = config_start[k]; i < config_start[k + 1]; i++) c->cfg_of[i] = k;
+    }
     rc = setup_layout(c);
     if (rc != MSTMG_OK) return fail(rc);
     *out = c;
@@ -1191,6 +1274,7 @@ extern "C" int mstmg_bicg(mstmg_ctx* c, int niter, double eps, const double* pnp
 {
     NvtxRange nvtx_("mstmg_bicg");
     if (!c || !pnp || !anp) return MSTMG_ERR_ARG;
+    if (int rc0 = reject_ensemble(c, "mstmg_bicg")) return rc0;
     int rc = ensure_ops(c, 0, initialize != 0);
     if (rc) return rc;
     const int ne = c->neqns;
@@ -1321,8 +1405,16 @@ static int solve_mixed(mstmg_ctx* c, zd* const* b, zd* const* x, double eps, int
 static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>& w32, DevBuf<double>& rr, DevBuf<int>& idx, int S,
                           const zd* B, zd* X, double eps, int niter, std::vector<int>& iters, std::vector<double>& errs,
                           std::vector<int>& status, int* outer_count);
+// systems of an ensemble: segment offsets and lengths per system (device),
+// vectors of ldv elements in the GMRES work
+struct EnsSeg {
+    const int* off;
+    const int* len;
+    int ldv;
+};
 static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S, const zd* B, zd* X, double eps, int niter,
-                             std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count);
+                             std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count,
+                             const EnsSeg* seg = nullptr);
 
 
 static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, const double* x0, double fallback,
@@ -1351,6 +1443,7 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
                                   int* used_guess, double* guess_res, double* amnp, double* qeff, double* qtot, double* maxerr, int* maxiter)
 {
     if (!c || !amnp) return MSTMG_ERR_ARG;
+    if (int rc0 = reject_ensemble(c, "mstmg_fixed_orientation")) return rc0;
     const int ne = c->neqns;
     SlotMaps sm = c->sm();
     c->passes64 = c->passes32 = 0;
@@ -1480,6 +1573,77 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
     CK(cudaStreamSynchronize(c->st));
     if (maxerr) *maxerr = me;
     if (maxiter) *maxiter = mi;
+    rc = check_kernel_err(c);
+    if (rc) return rc;
+    return istat;
+}
+
+// Fixed-orientation solves of every configuration of an ensemble at once:
+// per configuration and polarisation the mixed GMRES of fixedorsoln's system
+// (solver:350-569; x0 = Mie f, the reference's criterion per system), all
+// systems advancing together so that one translation pass a step serves the
+// whole ensemble.
+extern "C" int mstmg_ensemble_fixed_orientation(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, double* amnp,
+                                                double* qeff, double* qtot, int* iterations, double* errors)
+{
+    NvtxRange nvtx_("mstmg_ensemble_fixed_orientation");
+    if (!c || c->cfg_start.empty()) {
+        set_err("mstmg_ensemble_fixed_orientation: not an ensemble context (mstmg_ensemble_create)");
+        return MSTMG_ERR_ARG;
+    }
+    if (!amnp || niter < 1 || !(eps > 0.0)) {
+        set_err("mstmg_ensemble_fixed_orientation: bad arguments (amnp required, niter >= 1, eps > 0)");
+        return MSTMG_ERR_ARG;
+    }
+    if (c->opts.precision != MSTMG_PRECISION_MIXED || c->opts.mixed_solver != 2) {
+        set_err("mstmg_ensemble_fixed_orientation: ensembles are solved by the mixed GMRES (precision mixed, mixed_solver 2)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    const int ne = c->neqns, nc = (int)c->cfg_start.size() - 1, S = 2 * nc;
+    SlotMaps sm = c->sm();
+    c->passes64 = c->passes32 = 0;
+    c->outer = 0;
+    int rc = ensure_ops_both(c, true, true, true);
+    if (rc) return rc;
+    launch_planewave(alpha, sinc, dir, c->lmax, ne, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p, c->pmnp.p,
+                     c->st);
+    zd* bvec = c->bvec64.p;
+    for (int p = 0; p < 2; p++)
+        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, 1, 0, c->pmnp.p + (size_t)p * ne,
+                           bvec + (size_t)p * ne, c->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->amnp.p, bvec, sizeof(zd) * 2 * (size_t)ne, cudaMemcpyDeviceToDevice, c->st));
+    if (!c->ens_gm.hh) {
+        const int m = GmresWork::pick_m(S, c->ens_ldv, c->opts.gmres_restart);
+        if (m < (c->opts.gmres_restart > 0 ? std::min(c->opts.gmres_restart, 8) : 8)) {
+            set_err("mstmg_ensemble_fixed_orientation: no device memory for the GMRES basis");
+            return MSTMG_ERR_CUDA;
+        }
+        if ((rc = c->ens_gm.init(S, c->ens_ldv, m))) return rc;
+    }
+    const EnsSeg seg{c->ens_off.p, c->ens_len.p, c->ens_ldv};
+    std::vector<int> its, sts;
+    std::vector<double> ers;
+    int oc = 0;
+    rc = solve_multi_gmres(c, c->fo64, c->ens_gm, S, bvec, c->amnp.p, eps, niter, its, ers, sts, &oc, &seg);
+    if (rc) return rc;
+    c->outer = oc;
+    launch_qeff(c->n, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, mk(c->opts.medium_re, c->opts.medium_im), c->an_inv.p,
+                c->amnp.p, c->pmnp.p, ne, c->qeff.p, c->xg, c->qtot.p, c->st);
+    launch_qtot_configs(nc, c->d_cfg_start.p, c->rad.p, c->qeff.p, c->d_cfg_xg.p, c->cfg_qtot.p, c->st);
+    CK(cudaGetLastError());
+    CK(copy_out(amnp, c->amnp.p, sizeof(zd) * 2 * (size_t)ne, c->st));
+    if (qeff) CK(copy_out(qeff, c->qeff.p, sizeof(double) * 9 * (size_t)c->n, c->st));
+    if (qtot) CK(copy_out(qtot, c->cfg_qtot.p, sizeof(double) * 9 * (size_t)nc, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int istat = 0;
+    for (int s = 0; s < S; s++) {
+        if (iterations) iterations[s] = its[s];
+        if (errors) errors[s] = ers[s];
+        if (its[s] > niter || ers[s] > eps || sts[s] == 2) istat = 1;
+    }
+    c->iters[0] = its[0];
+    c->iters[1] = its[1];
     rc = check_kernel_err(c);
     if (rc) return rc;
     return istat;
@@ -1667,6 +1831,7 @@ static MergeArgs merge_args(mstmg_ctx* c, const RegTables& rt, const BigTablesDe
 extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_eps, int max_t_order, int nangles, double* smat,
                                 double* g, int* t_matrix_order, double* amnp0, int amnp0_cap)
 {
+    if (int rc0 = reject_ensemble(c, "mstmg_scattering")) return rc0;
     NvtxRange nvtx_("mstmg_scattering");
     if (!c || !amnp || nangles < 2 || max_t_order < 1) {
         set_err("mstmg_scattering: bad arguments");
@@ -2084,12 +2249,20 @@ static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>
 // of the reference.  iters counts Arnoldi steps in pairs (a BiCG iteration
 // is two matvecs), so the cap niter allows 2 niter steps.  X holds the
 // initial guesses on entry.
+// With seg (an ensemble), system s = 2 c + p is the segment of configuration c
+// in column p of the ne x 2 blocks B and X: every pass translates the two
+// columns with the active systems' basis vectors in their segments (the
+// operator has no pairs between configurations), and each system keeps its
+// own basis, Hessenberg matrix and stopping test.
 static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S, const zd* B, zd* X, double eps, int niter,
-                             std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count)
+                             std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count,
+                             const EnsSeg* seg)
 {
     using C = std::complex<double>;
     NvtxRange nvtx_("mixed GMRES");
     const int ne = c->neqns, m = gw.m, m1 = gw.m + 1;
+    const int ldv = seg ? seg->ldv : ne;             // elements a basis vector is stored in
+    const int* slen = seg ? seg->len : nullptr;      // elements a system's vectors hold
     SlotMaps sm = c->sm();
     const zf* an32 = (const zf*)c->an32.p;
     const size_t O1 = gw.off1(), HP = gw.hpass();
@@ -2108,13 +2281,21 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
     auto rot = [&](int s) { return (size_t)s * m; };
     auto colR = [&](int s, int j) { return &gw.Rm[((size_t)s * m + j) * m1]; };
     for (int cyc = 0; cyc <= c->opts.max_outer && !act.empty(); cyc++) {
-        // FP64 true residuals of the cycle's systems into R (FP32, by system)
+        // FP64 true residuals of the cycle's systems into R (FP32, by system,
+        // or the two columns of an ensemble)
         int a = (int)act.size();
-        const int apad = a == 1 ? 1 : ((a + 1) / 2) * 2;
-        CK(cudaMemcpyAsync(w64.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
-        launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
-        if ((rc = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u))) return rc;
-        launch_m_resid<float>(sm, c->an.p, ne, a, w64.act.p, B, X, w64.YP.p, gw.R.p, w64.part.p, gw.rr.p, c->nsm, c->st, 1);
+        if (seg) {
+            CK(cudaMemcpyAsync(gw.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+            if ((rc = translate_many<double>(c, X, c->Y64.p, 2, 0u))) return rc;
+            CK(cudaMemsetAsync(gw.rr.p, 0, sizeof(double) * 2 * S, c->st));
+            launch_eg_resid(sm, c->an.p, ne, ldv, a, gw.act.p, seg->off, seg->len, B, X, c->Y64.p, gw.R.p, gw.rr.p, c->nsm, c->st);
+        } else {
+            const int apad = a == 1 ? 1 : ((a + 1) / 2) * 2;
+            CK(cudaMemcpyAsync(w64.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+            launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
+            if ((rc = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u))) return rc;
+            launch_m_resid<float>(sm, c->an.p, ne, a, w64.act.p, B, X, w64.YP.p, gw.R.p, w64.part.p, gw.rr.p, c->nsm, c->st, 1);
+        }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(hrr.data(), gw.rr.p, sizeof(double) * 2 * S, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
@@ -2130,7 +2311,8 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
         if (a == 0 || cyc == c->opts.max_outer) break;
         CK(cudaMemcpyAsync(gw.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
         // v_0 = r / |r|
-        launch_gm_scale(ne, m1, 0, a, gw.act.p, 1, gw.R.p, gw.rr.p, 2, 1.0e-35, gw.V.p, c->nsm, c->st);
+        if (seg) launch_eg_start(ne, ldv, m1, a, gw.act.p, seg->off, seg->len, gw.R.p, gw.rr.p, 1.0e-35, gw.V.p, c->nsm, c->st);
+        else launch_gm_scale(ne, m1, 0, a, gw.act.p, 1, gw.R.p, gw.rr.p, 2, 1.0e-35, gw.V.p, c->nsm, c->st);
         long long room = cap;
         for (int s : act) {
             const double beta2 = hrr[2 * s];
@@ -2145,18 +2327,25 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
         const int jmax = (int)std::min<long long>(m, room);
         for (int j = 0; j < jmax && !cur.empty(); j++) {
             const int na = (int)cur.size();
-            const int npad = na <= 2 ? na : ((na + 3) / 4) * 4;   // whole FP32 chunks
-            launch_gm_gather(ne, m1, j, na, npad, gw.act.p, gw.V.p, gw.XP.p, c->nsm, c->st);
-            if ((rc = translate_many<float>(c, gw.XP.p, gw.Y.p, npad, 0u))) return rc;
-            launch_gm_apply(sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+            if (seg) {
+                CK(cudaMemsetAsync(gw.XP.p, 0, sizeof(zf) * 2 * (size_t)ne, c->st));
+                launch_eg_gather(ne, ldv, m1, j, na, gw.act.p, seg->off, seg->len, gw.V.p, gw.XP.p, c->nsm, c->st);
+                if ((rc = translate_many<float>(c, gw.XP.p, gw.Y.p, 2, 0u))) return rc;
+                launch_eg_apply(sm, an32, ne, ldv, na, gw.act.p, seg->off, seg->len, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+            } else {
+                const int npad = na <= 2 ? na : ((na + 3) / 4) * 4;   // whole FP32 chunks
+                launch_gm_gather(ne, m1, j, na, npad, gw.act.p, gw.V.p, gw.XP.p, c->nsm, c->st);
+                if ((rc = translate_many<float>(c, gw.XP.p, gw.Y.p, npad, 0u))) return rc;
+                launch_gm_apply(sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+            }
             const size_t hn = (size_t)(j + 1) * S * 2;
             CK(cudaMemsetAsync(gw.h.p, 0, sizeof(double) * (O1 + hn), c->st));
             CK(cudaMemsetAsync(h2, 0, sizeof(double) * hn, c->st));
-            launch_gm_dots(ne, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h1, nullptr, c->nsm, c->st);
-            launch_gm_update(ne, S, m1, j + 1, na, gw.act.p, gw.V.p, h1, gw.W.p, nullptr, c->nsm, c->st);
-            launch_gm_dots(ne, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h2, h1, c->nsm, c->st);
-            launch_gm_update(ne, S, m1, j + 1, na, gw.act.p, gw.V.p, h2, gw.W.p, gw.h.p, c->nsm, c->st);
-            launch_gm_scale(ne, m1, j + 1, na, gw.act.p, 0, gw.W.p, gw.h.p, 1, 1.0e-35, gw.V.p, c->nsm, c->st);
+            launch_gm_dots(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h1, nullptr, c->nsm, c->st, slen);
+            launch_gm_update(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, h1, gw.W.p, nullptr, c->nsm, c->st, slen);
+            launch_gm_dots(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h2, h1, c->nsm, c->st, slen);
+            launch_gm_update(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, h2, gw.W.p, gw.h.p, c->nsm, c->st, slen);
+            launch_gm_scale(ldv, m1, j + 1, na, gw.act.p, 0, gw.W.p, gw.h.p, 1, 1.0e-35, gw.V.p, c->nsm, c->st, slen);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(gw.hh, gw.h.p, sizeof(double) * (O1 + hn), cudaMemcpyDeviceToHost, c->st));
             CK(cudaStreamSynchronize(c->st));
@@ -2219,7 +2408,8 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
             }
             CK(cudaMemcpyAsync(gw.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
             CK(cudaMemcpyAsync(h2, gw.ybuf.data(), sizeof(double) * 2 * (size_t)kmax * S, cudaMemcpyHostToDevice, c->st));
-            launch_gm_combine(ne, S, m1, kmax, a, gw.act.p, gw.V.p, h2, X, c->nsm, c->st);
+            if (seg) launch_eg_combine(ne, ldv, S, m1, kmax, a, gw.act.p, seg->off, seg->len, gw.V.p, h2, X, c->nsm, c->st);
+            else launch_gm_combine(ne, S, m1, kmax, a, gw.act.p, gw.V.p, h2, X, c->nsm, c->st);
             CK(cudaGetLastError());
         }
     }
@@ -2232,6 +2422,7 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
 
 extern "C" int mstmg_t_matrix_order(mstmg_ctx* c, double trans_eps, int max_t_order, int* t_matrix_order)
 {
+    if (int rc0 = reject_ensemble(c, "mstmg_t_matrix_order")) return rc0;
     if (!c || max_t_order < 1 || !t_matrix_order) {
         set_err("mstmg_t_matrix_order: bad arguments");
         return MSTMG_ERR_ARG;
@@ -2253,6 +2444,7 @@ extern "C" int mstmg_t_matrix_order(mstmg_ctx* c, double trans_eps, int max_t_or
 extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_eps, double convergence_eps, int max_iterations,
                              double* tmat, double* sphere_qeff, double* qtot, int* order_used, int* maxiter, double* maxerr)
 {
+    if (int rc0 = reject_ensemble(c, "mstmg_tmatrix")) return rc0;
     NvtxRange nvtx_("mstmg_tmatrix");
     if (!c || t_matrix_order < 1 || t_matrix_order > 200 || !tmat || max_iterations < 1) {
         set_err("mstmg_tmatrix: bad arguments (1 <= t_matrix_order <= 200, max_iterations >= 1, tmat required)");
@@ -2766,6 +2958,7 @@ static int fft_build(mstmg_ctx* c)
 extern "C" int mstmg_fft_setup(mstmg_ctx* c, double cell_volume_fraction, double d_cell, int node_order, int neighbor_node_model,
                                int* cell_dim, double* d_cell_out, int* node_order_out, int* near_pairs)
 {
+    if (int rc0 = reject_ensemble(c, "mstmg_fft_setup")) return rc0;
     NvtxRange nvtx_("mstmg_fft_setup");
     if (!c || c->n < 2 || neighbor_node_model < 0 || neighbor_node_model > 2) {
         set_err("mstmg_fft_setup: bad arguments (two or more spheres, neighbor_node_model 0..2)");

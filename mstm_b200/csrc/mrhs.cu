@@ -87,13 +87,15 @@ __global__ void __launch_bounds__(MB) gm_apply_kernel(SlotMaps sm, const zf* an,
 }
 
 // h[i S + s] += V_{s,i}^H W[:, k] (and hacc likewise when given), i = blockIdx.y
-__global__ void __launch_bounds__(MB) gm_dots_kernel(int ld, int S, int m1, const int* act, const zf* V, const zf* W, double* h, double* hacc)
+__global__ void __launch_bounds__(MB) gm_dots_kernel(int ld, int S, int m1, const int* act, const zf* V, const zf* W, double* h, double* hacc,
+                                                     const int* len)
 {
     const int i = blockIdx.y, k = blockIdx.z, s = act[k];
     const zf* v = V + ((size_t)s * m1 + i) * ld;
     const zf* w = W + (size_t)k * ld;
+    const int ne = len ? len[s] : ld;
     double acc[2] = {0.0, 0.0};
-    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ne; e += gridDim.x * MB) {
         const cpx<double> x = upd_(v[e]), y = upd_(w[e]);
         acc[0] += x.x * y.x + x.y * y.y;
         acc[1] += x.x * y.y - x.y * y.x;
@@ -114,13 +116,14 @@ __global__ void __launch_bounds__(MB) gm_dots_kernel(int ld, int S, int m1, cons
 // W[:, k] -= sum_{i < kp1} V_{s,i} h[i S + s] (FP64 accumulation per
 // element); nrm[s] += |W[:, k]|^2 of the result when nrm is given
 __global__ void __launch_bounds__(MB) gm_update_kernel(int ld, int S, int m1, int kp1, const int* act, const zf* V, const double* h, zf* W,
-                                                      double* nrm)
+                                                      double* nrm, const int* len)
 {
     const int k = blockIdx.y, s = act[k];
     const zf* vs = V + (size_t)s * m1 * ld;
     zf* w = W + (size_t)k * ld;
+    const int ne = len ? len[s] : ld;
     double n2[1] = {0.0};
-    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ne; e += gridDim.x * MB) {
         cpx<double> x = upd_(w[e]);
         for (int i = 0; i < kp1; i++) {
             const cpx<double> t = upd_(vs[(size_t)i * ld + e]) * mk(h[2 * ((size_t)i * S + s)], h[2 * ((size_t)i * S + s) + 1]);
@@ -141,14 +144,15 @@ __global__ void __launch_bounds__(MB) gm_update_kernel(int ld, int S, int m1, in
 // V_{s,jd} = src / sqrt(nrm[s stride]) with src = Wsrc[:, s] (by_sys) or
 // Wsrc[:, k]; zero where the norm is below tiny
 __global__ void __launch_bounds__(MB) gm_scale_kernel(int ld, int m1, int jd, const int* act, int by_sys, const zf* Wsrc, const double* nrm,
-                                                     int stride, double tiny, zf* V)
+                                                     int stride, double tiny, zf* V, const int* len)
 {
     const int k = blockIdx.y, s = act[k];
     const double n2 = nrm[(size_t)s * stride];
     const float f = (n2 > tiny * tiny) ? (float)(1.0 / sqrt(n2)) : 0.0f;
     const zf* w = Wsrc + (size_t)(by_sys ? s : k) * ld;
     zf* d = V + ((size_t)s * m1 + jd) * ld;
-    for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) d[e] = f * w[e];
+    const int ne = len ? len[s] : ld;
+    for (int e = blockIdx.x * MB + threadIdx.x; e < ne; e += gridDim.x * MB) d[e] = f * w[e];
 }
 
 // X[:, s] += sum_{i < kp1} y[i S + s] V_{s,i} (FP64)
@@ -161,6 +165,98 @@ __global__ void __launch_bounds__(MB) gm_combine_kernel(int ld, int S, int m1, i
         cpx<double> a = x[e];
         for (int i = 0; i < kp1; i++)
             a = a + upd_(vs[(size_t)i * ld + e]) * mk(y[2 * ((size_t)i * S + s)], y[2 * ((size_t)i * S + s) + 1]);
+        x[e] = a;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Ensembles: independent configurations in one index space (no pairs between
+// them).  System s = 2 c + p is polarisation p of configuration c: column p
+// of the ne x 2 blocks, elements [off[s], off[s] + len[s]) (slots
+// [off[s]/2, (off[s] + len[s])/2)).  Basis vector i of system s at
+// V + (s m1 + i) ldv, work column k at W + k ldv.
+// ---------------------------------------------------------------------------
+// R[p] = B - X + M YP over the segment of system act[k] (rounded to FP32);
+// rr[2 s] += |r|^2, rr[2 s + 1] += |b|^2 over it (zeroed by the caller)
+__global__ void __launch_bounds__(MB) eg_resid_kernel(SlotMaps sm, const zd* an, int ne, const int* act, const int* off, const int* len,
+                                                     const zd* B, const zd* X, const zd* YP, zf* R, double* rr)
+{
+    const int s = act[blockIdx.y], p = s & 1;
+    const size_t o = (size_t)p * ne;
+    const int e0 = off[s] / 2, e1 = (off[s] + len[s]) / 2;
+    double acc[2] = {0.0, 0.0};
+    for (int e = e0 + blockIdx.x * MB + threadIdx.x; e < e1; e += gridDim.x * MB) {
+        SlotPos q = slot_pos(sm, e);
+        const zd* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        const zd u0 = YP[o + q.b0], u1 = YP[o + q.b1];
+        const zd m[2] = {A[0] * u0 + A[2] * u1, A[1] * u0 + A[3] * u1};
+        const int bb[2] = {q.b0, q.b1};
+        for (int h = 0; h < 2; h++) {
+            const zd bv = B[o + bb[h]];
+            const zd rv = (bv - X[o + bb[h]]) + m[h];
+            R[o + bb[h]] = mk((float)rv.x, (float)rv.y);
+            acc[0] += rv.x * rv.x + rv.y * rv.y;
+            acc[1] += bv.x * bv.x + bv.y * bv.y;
+        }
+    }
+    double out[2];
+    mblock_store<2>(acc, out);
+    if (threadIdx.x == 0) {
+        atomicAdd(&rr[2 * s], out[0]);
+        atomicAdd(&rr[2 * s + 1], out[1]);
+    }
+}
+
+// V_{s,0} = R[p, segment] / sqrt(rr[2 s]) (zero where the norm is below tiny)
+__global__ void __launch_bounds__(MB) eg_start_kernel(int ne, int ldv, int m1, const int* act, const int* off, const int* len, const zf* R,
+                                                     const double* rr, double tiny, zf* V)
+{
+    const int s = act[blockIdx.y], p = s & 1;
+    const double n2 = rr[2 * s];
+    const float f = (n2 > tiny * tiny) ? (float)(1.0 / sqrt(n2)) : 0.0f;
+    const zf* r = R + (size_t)p * ne + off[s];
+    zf* v = V + (size_t)s * m1 * ldv;
+    for (int e = blockIdx.x * MB + threadIdx.x; e < len[s]; e += gridDim.x * MB) v[e] = f * r[e];
+}
+
+// XP[p, segment of s] = V_{s,j} (XP zeroed by the caller)
+__global__ void __launch_bounds__(MB) eg_gather_kernel(int ne, int ldv, int m1, int j, const int* act, const int* off, const int* len,
+                                                      const zf* V, zf* XP)
+{
+    const int s = act[blockIdx.y], p = s & 1;
+    const zf* v = V + ((size_t)s * m1 + j) * ldv;
+    zf* x = XP + (size_t)p * ne + off[s];
+    for (int e = blockIdx.x * MB + threadIdx.x; e < len[s]; e += gridDim.x * MB) x[e] = v[e];
+}
+
+// W[:, k] = (XP - M Y)[p, segment of s], local indices
+__global__ void __launch_bounds__(MB) eg_apply_kernel(SlotMaps sm, const zf* an, int ne, int ldv, const int* act, const int* off, const int* len,
+                                                     const zf* XP, const zf* Y, zf* W)
+{
+    const int k = blockIdx.y, s = act[k], p = s & 1;
+    const size_t o = (size_t)p * ne;
+    const int e0 = off[s] / 2, e1 = (off[s] + len[s]) / 2;
+    zf* w = W + (size_t)k * ldv - off[s];
+    for (int e = e0 + blockIdx.x * MB + threadIdx.x; e < e1; e += gridDim.x * MB) {
+        SlotPos q = slot_pos(sm, e);
+        const zf* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        const zf u0 = Y[o + q.b0], u1 = Y[o + q.b1];
+        w[q.b0] = XP[o + q.b0] - (A[0] * u0 + A[2] * u1);
+        w[q.b1] = XP[o + q.b1] - (A[1] * u0 + A[3] * u1);
+    }
+}
+
+// X[p, segment of s] += sum_{i < kp1} y[i S + s] V_{s,i} (FP64)
+__global__ void __launch_bounds__(MB) eg_combine_kernel(int ne, int ldv, int S, int m1, int kp1, const int* act, const int* off, const int* len,
+                                                       const zf* V, const double* y, zd* X)
+{
+    const int s = act[blockIdx.y], p = s & 1;
+    const zf* vs = V + (size_t)s * m1 * ldv;
+    zd* x = X + (size_t)p * ne + off[s];
+    for (int e = blockIdx.x * MB + threadIdx.x; e < len[s]; e += gridDim.x * MB) {
+        cpx<double> a = x[e];
+        for (int i = 0; i < kp1; i++)
+            a = a + upd_(vs[(size_t)i * ldv + e]) * mk(y[2 * ((size_t)i * S + s)], y[2 * ((size_t)i * S + s) + 1]);
         x[e] = a;
     }
 }
@@ -848,25 +944,56 @@ void launch_gm_apply(const SlotMaps& sm, const zf* an, int ld, int a, const zf* 
     launch_counter() += 1;
 }
 void launch_gm_dots(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const zf* W, double* h, double* hacc, int nsm,
-                    cudaStream_t st)
+                    cudaStream_t st, const int* len)
 {
-    gm_dots_kernel<<<dim3(multi_grid(ld, kp1 * a, nsm), kp1, a), MB, 0, st>>>(ld, S, m1, act, V, W, h, hacc);
+    gm_dots_kernel<<<dim3(multi_grid(ld, kp1 * a, nsm), kp1, a), MB, 0, st>>>(ld, S, m1, act, V, W, h, hacc, len);
     launch_counter() += 1;
 }
 void launch_gm_update(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* h, zf* W, double* nrm, int nsm,
-                      cudaStream_t st)
+                      cudaStream_t st, const int* len)
 {
-    gm_update_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, h, W, nrm);
+    gm_update_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, h, W, nrm, len);
     launch_counter() += 1;
 }
 void launch_gm_scale(int ld, int m1, int jd, int a, const int* act, int by_sys, const zf* Wsrc, const double* nrm, int stride, double tiny,
-                     zf* V, int nsm, cudaStream_t st)
+                     zf* V, int nsm, cudaStream_t st, const int* len)
 {
-    gm_scale_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, m1, jd, act, by_sys, Wsrc, nrm, stride, tiny, V);
+    gm_scale_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, m1, jd, act, by_sys, Wsrc, nrm, stride, tiny, V, len);
     launch_counter() += 1;
 }
 void launch_gm_combine(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* y, zd* X, int nsm, cudaStream_t st)
 {
     gm_combine_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, y, X);
+    launch_counter() += 1;
+}
+// ---- ensemble launchers (grid rows = active systems) ----
+void launch_eg_resid(const SlotMaps& sm, const zd* an, int ne, int ldv, int a, const int* act, const int* off, const int* len, const zd* B,
+                     const zd* X, const zd* YP, zf* R, double* rr, int nsm, cudaStream_t st)
+{
+    eg_resid_kernel<<<dim3(multi_grid(ldv / 2, a, nsm), a), MB, 0, st>>>(sm, an, ne, act, off, len, B, X, YP, R, rr);
+    launch_counter() += 1;
+}
+void launch_eg_start(int ne, int ldv, int m1, int a, const int* act, const int* off, const int* len, const zf* R, const double* rr, double tiny,
+                     zf* V, int nsm, cudaStream_t st)
+{
+    eg_start_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, m1, act, off, len, R, rr, tiny, V);
+    launch_counter() += 1;
+}
+void launch_eg_gather(int ne, int ldv, int m1, int j, int a, const int* act, const int* off, const int* len, const zf* V, zf* XP, int nsm,
+                      cudaStream_t st)
+{
+    eg_gather_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, m1, j, act, off, len, V, XP);
+    launch_counter() += 1;
+}
+void launch_eg_apply(const SlotMaps& sm, const zf* an, int ne, int ldv, int a, const int* act, const int* off, const int* len, const zf* XP,
+                     const zf* Y, zf* W, int nsm, cudaStream_t st)
+{
+    eg_apply_kernel<<<dim3(multi_grid(ldv / 2, a, nsm), a), MB, 0, st>>>(sm, an, ne, ldv, act, off, len, XP, Y, W);
+    launch_counter() += 1;
+}
+void launch_eg_combine(int ne, int ldv, int S, int m1, int kp1, int a, const int* act, const int* off, const int* len, const zf* V,
+                       const double* y, zd* X, int nsm, cudaStream_t st)
+{
+    eg_combine_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, S, m1, kp1, act, off, len, V, y, X);
     launch_counter() += 1;
 }

@@ -54,17 +54,38 @@ void launch_m_mie(const SlotMaps& sm, const zd* an, int ld, int ncols, const zd*
 void launch_gm_gather(int ld, int m1, int j, int a, int apad, const int* act, const zf* V, zf* XP, int nsm, cudaStream_t st);
 // W[:, k] = XP[:, k] - M Y[:, k]
 void launch_gm_apply(const SlotMaps& sm, const zf* an, int ld, int a, const zf* XP, const zf* Y, zf* W, int nsm, cudaStream_t st);
+// (len, when given: system s's vectors hold len[s] <= ld elements)
 // h[i S + s] += V_{s,i}^H W[:, k] for i < kp1 (hacc too when given; both zeroed by the caller)
 void launch_gm_dots(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const zf* W, double* h, double* hacc, int nsm,
-                    cudaStream_t st);
+                    cudaStream_t st, const int* len = nullptr);
 // W[:, k] -= sum_{i < kp1} V_{s,i} h[i S + s]; nrm[s] += |W[:, k]|^2 after it when nrm is given
 void launch_gm_update(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* h, zf* W, double* nrm, int nsm,
-                      cudaStream_t st);
+                      cudaStream_t st, const int* len = nullptr);
 // V_{s,jd} = Wsrc[:, by_sys ? s : k] / sqrt(nrm[s stride]), zero when the norm is below tiny
 void launch_gm_scale(int ld, int m1, int jd, int a, const int* act, int by_sys, const zf* Wsrc, const double* nrm, int stride, double tiny,
-                     zf* V, int nsm, cudaStream_t st);
+                     zf* V, int nsm, cudaStream_t st, const int* len = nullptr);
 // X[:, s] += sum_{i < kp1} y[i S + s] V_{s,i} in FP64
 void launch_gm_combine(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* y, zd* X, int nsm, cudaStream_t st);
+
+// ---- ensembles of independent configurations in one index space: system
+//      s = 2 c + p is polarisation p (column p of ne x 2 blocks) over the
+//      elements [off[s], off[s] + len[s]) of configuration c; basis vector i
+//      of s at V + (s m1 + i) ldv, work column k at W + k ldv (ldv >= len) ----
+// R[p, seg] = B - X + M YP (FP32); rr[2s] += |r|^2, rr[2s+1] += |b|^2 (rr zeroed by the caller)
+void launch_eg_resid(const SlotMaps& sm, const zd* an, int ne, int ldv, int a, const int* act, const int* off, const int* len, const zd* B,
+                     const zd* X, const zd* YP, zf* R, double* rr, int nsm, cudaStream_t st);
+// V_{s,0} = R[p, seg] / sqrt(rr[2s])
+void launch_eg_start(int ne, int ldv, int m1, int a, const int* act, const int* off, const int* len, const zf* R, const double* rr, double tiny,
+                     zf* V, int nsm, cudaStream_t st);
+// XP[p, seg] = V_{s,j} (XP zeroed by the caller)
+void launch_eg_gather(int ne, int ldv, int m1, int j, int a, const int* act, const int* off, const int* len, const zf* V, zf* XP, int nsm,
+                      cudaStream_t st);
+// W[:, k] = (XP - M Y)[p, seg]
+void launch_eg_apply(const SlotMaps& sm, const zf* an, int ne, int ldv, int a, const int* act, const int* off, const int* len, const zf* XP,
+                     const zf* Y, zf* W, int nsm, cudaStream_t st);
+// X[p, seg] += sum_{i < kp1} y[i S + s] V_{s,i} (FP64)
+void launch_eg_combine(int ne, int ldv, int S, int m1, int kp1, int a, const int* act, const int* off, const int* len, const zf* V,
+                       const double* y, zd* X, int nsm, cudaStream_t st);
 
 // ---- T matrix (tmatrix_solution, mstm-solver-8.f90:22-332) ----
 // columns of order l: unit TE (q=1) / TM (q=2) field of degree k in the LR basis

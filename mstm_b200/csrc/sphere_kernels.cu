@@ -408,6 +408,25 @@ __global__ void qtot_kernel(int nsph, const double* radius, const double* qeff, 
     for (int k = 0; k < 9; k++) qtot[k] = s[k];
 }
 
+// qtot_kernel over the spheres of each configuration of an ensemble (one
+// thread a configuration, the same sums in the same order)
+__global__ void qtot_configs_kernel(int nc, const int* cfg_start, const double* radius, const double* qeff, const double* xg, double* qtot)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nc) return;
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = cfg_start[k]; i < cfg_start[k + 1]; i++)
+        for (int q = 0; q < 9; q++) s[q] = s[q] + qeff[q + 9 * i] * radius[i] * radius[i] / (xg[k] * xg[k]);
+    for (int pol = 0; pol < 3; pol++) s[2 + 3 * pol] = s[0 + 3 * pol] + s[2 + 3 * pol] - s[1 + 3 * pol];
+    for (int q = 0; q < 9; q++) qtot[q + 9 * k] = s[q];
+}
+
+void launch_qtot_configs(int nc, const int* cfg_start, const double* radius, const double* qeff, const double* xg, double* qtot, cudaStream_t st)
+{
+    qtot_configs_kernel<<<(nc + 63) / 64, 64, 0, st>>>(nc, cfg_start, radius, qeff, xg, qtot);
+    launch_counter() += 1;
+}
+
 void launch_qeff(int nsph, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed, const zd* an_inv,
                  const zd* amnp, const zd* pmnp0, int ld, double* qeff, double xg, double* qtot, cudaStream_t st)
 {

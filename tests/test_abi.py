@@ -100,3 +100,27 @@ def test_ctx_create_rejects_invalid_solver_options(field, value):
     rc = L.mstmg_ctx_create(ctypes.byref(ctx), 2, p(pos), p(rad), p(ri), -3.0, ctypes.byref(opts))
     assert rc == -1 and not ctx.value
     assert "gmres_restart" in L.mstmg_last_error().decode()
+
+
+@pytest.mark.parametrize("starts", [[1, 2, 4], [0, 2, 3], [0, 2, 2, 4]])
+def test_ensemble_create_rejects_bad_config_start(starts):
+    """config_start must run from 0 to nsphere with every configuration
+    non-empty; checked before any device call."""
+    import ctypes
+
+    import numpy as np
+
+    from mstm_b200 import _lib
+    from mstm_b200 import build as B
+    if not os.path.exists(_lib.LIB_PATH):
+        B.build()
+    L = _lib.lib()
+    pos = np.array([[0.0, 0.0, 0.0], [3.0, 0.0, 0.0], [0.0, 3.0, 0.0], [0.0, 0.0, 3.0]])
+    rad = np.ones(4)
+    ri = np.tile([1.5, 0.01], (4, 1))
+    cs = np.array(starts, np.int32)
+    ctx = ctypes.c_void_p()
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = L.mstmg_ensemble_create(ctypes.byref(ctx), len(starts) - 1, p(cs), 4, p(pos), p(rad), p(ri), -3.0, None)
+    assert rc == -1 and not ctx.value
+    assert "mstmg_ensemble_create" in L.mstmg_last_error().decode()

@@ -41,3 +41,88 @@ def test_fixed_ensemble_concurrent_matches_fp64():
     for a, b in zip(ens["per_config"], seq["per_config"]):
         assert a["istat"] == 0 and b["istat"] == 0
         assert np.allclose(a["qtot"], b["qtot"], rtol=1e-6)
+
+
+def _mie_times(an, order, f):
+    """Mie multiply (LR-basis 2x2 per degree) of MSTM-layout columns f."""
+    out = np.zeros_like(f)
+    off, moff = 0, 0
+    for L in order:
+        hb = L * (L + 2)
+        loc = np.arange(hb)
+        row, col = loc % (L + 2), loc // (L + 2) + 1
+        n = np.where(row <= col, col, row - 1)
+        a = [an[moff + 4 * (n - 1) + k][:, None] for k in range(4)]
+        u0, u1 = f[off:off + hb], f[off + hb:off + 2 * hb]
+        out[off:off + hb] = a[0] * u0 + a[2] * u1
+        out[off + hb:off + 2 * hb] = a[1] * u0 + a[3] * u1
+        off += 2 * hb
+        moff += 4 * L
+    return out
+
+
+@pytest.mark.parametrize("mixed_orders", [False, True])
+def test_one_context_ensemble_matches_separate_solves(oracle_mod, mixed_orders):
+    """An ensemble context (no pairs between configurations; one translation
+    pass a step for all of them) gives every configuration the efficiencies
+    of its own mixed-precision solve and of the FP64 oracle within 1e-6, each
+    system meets the criterion on its own configuration, and the returned
+    coefficients satisfy each configuration's FP64 system.  With mixed_orders
+    the configurations have two sphere orders (the non-tiled pair path)."""
+    from mstm_b200 import api
+    from mstm_b200 import configs as C
+    sizes = (12, 18, 25, 31, 16, 22)
+    xs = [1.0 if (not mixed_orders or k % 2 == 0) else 1.4 for k in range(len(sizes))]
+    cfgs = [(C.rsa_sphere(n, x, 0.10, seed=500 + n)[0], np.full(n, x), 1.5 + 0.01j) for n, x in zip(sizes, xs)]
+    em = 1e-6 if mixed_orders else -C.truncation_order(1.0)
+    ens = api.SphereEnsemble(cfgs, mie_epsilon=em)
+    r = ens.fixedorsoln(eps=1e-12, niter=4000)
+    assert r["istat"] == 0 and (r["errors"] < 1e-12).all()
+    an, _, _ = ens.miecoefcalc()
+    f = np.zeros((ens.number_eqns, 2), complex)
+    for k, (pos, rad, m) in enumerate(cfgs):
+        g = api.SphereCluster(pos, rad, np.full(len(rad), m), mie_epsilon=em, precision="mixed")
+        rs = g.fixedorsoln(eps=1e-12, niter=4000)
+        assert np.allclose(r["qtot"][k], rs["qtot"], rtol=1e-6), k
+        assert abs(int(r["iterations"][k].max()) - int(rs["maxiter"])) <= 2
+        # this configuration's FP64 system (I - M H) x = M f, checked on its own context
+        x = r["amnp_of"](k)
+        fk = g.sphereplanewavecoef()
+        ank, _, _ = g.miecoefcalc()
+        bm = _mie_times(ank, g.sphere_order, fk)
+        res = bm - x + g.sphereinteraction(x, initial_run=True)
+        for p in range(2):
+            rel = np.vdot(res[:, p], res[:, p]).real / np.vdot(bm[:, p], bm[:, p]).real
+            assert rel < 1e-11, (k, p, rel)
+        if k == 0:
+            o = oracle_mod.Oracle(pos, rad, np.full(len(rad), m), mie_eps=em)
+            ro = o.fixedorsoln(eps=1e-12, niter=4000)
+            assert np.allclose(r["qtot"][k], ro["qtot"], rtol=1e-6)
+        g.close()
+
+
+def test_ensemble_context_refuses_single_cluster_entry_points():
+    """Entry points that treat a context as one cluster return
+    MSTMG_ERR_UNSUPPORTED on an ensemble; the block-diagonal matvec is the
+    configurations' own matvecs side by side."""
+    import ctypes
+    from mstm_b200 import _lib, api
+    from mstm_b200 import configs as C
+    cfgs = [(C.rsa_sphere(n, 1.0, 0.10, seed=700 + n)[0], np.full(n, 1.0), 1.5 + 0.01j) for n in (9, 14)]
+    ens = api.SphereEnsemble(cfgs, mie_epsilon=-C.truncation_order(1.0))
+    L = _lib.lib()
+    amnp = np.zeros((ens.number_eqns, 2), np.complex128)
+    me, mi = ctypes.c_double(0.0), ctypes.c_int(0)
+    rc = L.mstmg_fixed_orientation(ens.ctx, 0.0, 0.0, 1, 1e-12, 100, amnp.ctypes.data_as(ctypes.c_void_p), None, None,
+                                   ctypes.byref(me), ctypes.byref(mi))
+    assert rc == -3 and "ensemble" in L.mstmg_last_error().decode()
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=(ens.number_eqns, 2)) + 1j * rng.normal(size=(ens.number_eqns, 2))
+    y = ens.sphereinteraction(x, initial_run=True)
+    off = ens.sphere_offset
+    for k, (pos, rad, m) in enumerate(cfgs):
+        g = api.SphereCluster(pos, rad, np.full(len(rad), m), mie_epsilon=-C.truncation_order(1.0), precision="fp64")
+        a, b = off[ens.config_start[k]], off[ens.config_start[k + 1]]
+        yk = g.sphereinteraction(x[a:b], initial_run=True)
+        assert np.abs(y[a:b] - yk).max() <= 1e-12 * np.abs(yk).max()
+        g.close()
