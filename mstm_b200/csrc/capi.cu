@@ -23,7 +23,6 @@
 #include <nvtx3/nvToolsExt.h>
 #include <cufft.h>
 #include <memory>
-#include <algorithm>
 #include <type_traits>
 
 static thread_local std::string g_err;
@@ -232,6 +231,10 @@ struct mstmg_ctx {
     DevBuf<long long> opoff;
     DevBuf<int4> tiles;
     int ntiles = 0;
+    // grouped tiles (the FFT path's near pairs): spheres of each tile by slot
+    // and the slots of each pair; empty for block tiles
+    DevBuf<int> tsph;
+    DevBuf<short2> pslot;
     bool tiled = false;   // monodisperse cluster: pairs stored in tile order for the fast kernel
     DevBuf<double> op64;
     DevBuf<float> op32;
@@ -569,6 +572,8 @@ static int setup_layout(mstmg_ctx* c)
         set_err("internal error: pair schedule incomplete");
         return MSTMG_ERR_ARG;
     }
+    c->tsph.release();   // block tiles
+    c->pslot.release();
     (void)off;
     (void)maxrec;
     int rc_ = upload_pairs(c, pr, (int)np, tl);
@@ -960,6 +965,8 @@ template <typename T> static int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>
         ta.contran = contran;
         ta.err = c->err.p;
         ta.ctas_per_sm = c->opts.tile_ctas_per_sm;
+        ta.tsph = c->tsph.p;
+        ta.pslot = c->pslot.p;
     }
     if (nchunk > 1 && !use_tiled) return MSTMG_ERR_UNSUPPORTED;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -2855,8 +2862,67 @@ static int fft_build(mstmg_ctx* c)
             for (int j : members[(size_t)(sx - 1) + (size_t)F.cd[0] * ((sy - 1) + (size_t)F.cd[1] * (sz - 1))])
                 if (j > i) pr.push_back(make_int2(i, j));
         }
-    c->tiled = false;
-    int rc = upload_pairs(c, pr, (int)pr.size(), std::vector<int4>());
+    // Grouped tiles for the tiled kernel (one sphere order it supports): the
+    // spheres, taken cell by cell, form groups of TILE_B; a tile holds the
+    // near pairs between two groups (or inside one), its spheres listed by
+    // slot, so the near pairs of nearby spheres share the tiles' output
+    // accumulation as the block tiles of a whole cluster do.
+    c->tsph.release();
+    c->pslot.release();
+    std::vector<int4> tl;
+    {
+        const int B = TILE_B, NS2 = 2 * TILE_B;
+        const int lmin = *std::min_element(c->order.begin(), c->order.end());
+        c->tiled = !c->opts.generic_kernel && lmin == c->lmax && lmin >= c->opts.translation_switch_order && tiled_supported(c->lmax, 1) &&
+                   !pr.empty();
+        if (c->tiled) {
+            std::vector<int> grp(n), gs(n);
+            int k = 0;
+            for (const auto& cm : members)
+                for (int i : cm) {
+                    grp[i] = k / B;
+                    gs[i] = k % B;
+                    k++;
+                }
+            const long long ng = (n + B - 1) / B;
+            std::vector<int> gmem((size_t)ng * B, -1);
+            for (int i = 0; i < n; i++) gmem[(size_t)grp[i] * B + gs[i]] = i;
+            std::vector<long long> key(pr.size());
+            std::vector<int> idx(pr.size());
+            for (size_t q = 0; q < pr.size(); q++) {
+                const long long ga = std::min(grp[pr[q].x], grp[pr[q].y]), gb = std::max(grp[pr[q].x], grp[pr[q].y]);
+                key[q] = ga * ng + gb;
+                idx[q] = (int)q;
+            }
+            std::stable_sort(idx.begin(), idx.end(), [&](int u, int v) { return key[u] < key[v]; });
+            std::vector<int2> pr2(pr.size());
+            std::vector<int> ts;
+            std::vector<short2> ps(pr.size());
+            size_t q = 0;
+            while (q < idx.size()) {
+                const long long kk = key[idx[q]];
+                const int ga = (int)(kk / ng), gb = (int)(kk % ng);
+                const size_t start = q;
+                for (int s = 0; s < B; s++) ts.push_back(gmem[(size_t)ga * B + s]);
+                for (int s = 0; s < B; s++) ts.push_back(ga == gb ? -1 : gmem[(size_t)gb * B + s]);
+                for (; q < idx.size() && key[idx[q]] == kk; q++) {
+                    const int2 p2 = pr[idx[q]];
+                    pr2[q] = p2;
+                    const short si = (short)(grp[p2.x] == ga ? gs[p2.x] : B + gs[p2.x]);
+                    const short sj = (short)(grp[p2.y] == ga ? gs[p2.y] : B + gs[p2.y]);
+                    ps[q] = make_short2(si, sj);
+                }
+                tl.push_back(make_int4((int)start, (int)(q - start), 0, ga == gb ? 1 : 0));
+            }
+            pr.swap(pr2);
+            CK(c->tsph.alloc(ts.size()));
+            CK(c->pslot.alloc(ps.size()));
+            CK(cudaMemcpyAsync(c->tsph.p, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(c->pslot.p, ps.data(), sizeof(short2) * ps.size(), cudaMemcpyHostToDevice, c->st));
+            (void)NS2;
+        }
+    }
+    int rc = upload_pairs(c, pr, (int)pr.size(), tl);   // synchronises: the host vectors above are done with
     if (rc) return rc;
     // node translations
     std::vector<long long> joff(n + 1);

@@ -195,9 +195,16 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
             return;
         }
         const T* rec = opb + b * REC;
-        const int2 pr = a.pairs[q];
-        const int si = pr.x - i0;
-        const int sj = diag ? (pr.y - i0) : (B + pr.y - j0);
+        int si, sj;
+        if (a.pslot) {
+            const short2 ps = a.pslot[q];
+            si = ps.x;
+            sj = ps.y;
+        } else {
+            const int2 pr = a.pairs[q];
+            si = pr.x - i0;
+            sj = diag ? (pr.y - i0) : (B + pr.y - j0);
+        }
         if (tid == 0) {
             cpx<T> ep = mk(rec[0], rec[1]);
             cpx<T>* e = ephm + L;
@@ -419,8 +426,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int r = rem / NB, el = rem - r * NB;
-                const int sph = (slot < B) ? (i0 + slot) : (j0 + slot - B);
-                if (!(diag && slot >= B) && sph < a.nsph) {
+                const int sph = a.tsph ? a.tsph[(size_t)tile_of(tcur) * NSLOT + slot] : ((slot < B) ? (i0 + slot) : (j0 + slot - B));
+                if (a.tsph ? sph >= 0 : (!(diag && slot >= B) && sph < a.nsph)) {
                     cpx<T> v = ACC[idx];
                     red_add<T>(yc + (size_t)r * a.ld + (size_t)sph * NB + el, v);
                 }

@@ -14,8 +14,12 @@ template <typename T> struct TiledArgs {
     int ld, nrhs, nsph;      // nrhs: columns per chunk (the kernel's NR)
     int nchunk;              // chunks of nrhs columns: x and y hold nrhs * nchunk columns
     unsigned contran;        // bit r: column r of every chunk is a conjugate-transpose product
-    int ctas_per_sm;         // 0: as many as shared memory allows (at most 2)
+    int ctas_per_sm;         // 0: as many as shared memory and the register budget allow
     int* err;
+    // grouped tiles (null for block tiles): tile t's spheres by slot,
+    // tsph[t * 2B + slot] (-1: none), and each pair's (slot of i, slot of j)
+    const int* tsph = nullptr;
+    const short2* pslot = nullptr;
 };
 
 bool tiled_supported(int L, int nrhs);
