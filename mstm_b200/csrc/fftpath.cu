@@ -220,22 +220,24 @@ __global__ void __launch_bounds__(FFT_NT) fft_s2n_kernel(FftMArgs a, const cpx<T
     }
 }
 
-// per frequency f: G[col][p][l][f] = sum_n H[p][l][n][f] A[col][p][n][f]
+// per frequency f: G[col][p][l][f] = sum_n H[p][l][n][f] A[col][p][n][f].
+// Row (p, l) = blockIdx.y, frequencies over threads: every H element is read
+// once, coalesced along f, and the A rows are shared through the caches by
+// the 2 nbN rows of a frequency block.
 template <typename T>
 __global__ void __launch_bounds__(FFT_NT) fft_mul_kernel(int nbN, size_t N8, int ncol, const float2* H, const cpx<T>* A, cpx<T>* G)
 {
+    const int pl = blockIdx.y, p = pl / nbN, l = pl - p * nbN;
+    const float2* h = H + (size_t)pl * nbN * N8;
     for (size_t f = blockIdx.x * (size_t)FFT_NT + threadIdx.x; f < N8; f += (size_t)gridDim.x * FFT_NT) {
-        for (int p = 0; p < 2; p++)
-            for (int l = 0; l < nbN; l++) {
-                cpx<T> acc[4];
-                for (int c = 0; c < ncol; c++) acc[c] = mk((T)0, (T)0);
-                for (int n = 0; n < nbN; n++) {
-                    float2 h = H[((size_t)(p * nbN + l) * nbN + n) * N8 + f];
-                    cpx<T> hv = mk((T)h.x, (T)h.y);
-                    for (int c = 0; c < ncol; c++) acc[c] = acc[c] + hv * A[((size_t)(c * 2 + p) * nbN + n) * N8 + f];
-                }
-                for (int c = 0; c < ncol; c++) G[((size_t)(c * 2 + p) * nbN + l) * N8 + f] = acc[c];
-            }
+        cpx<T> acc[4];
+        for (int c = 0; c < ncol; c++) acc[c] = mk((T)0, (T)0);
+        for (int n = 0; n < nbN; n++) {
+            const float2 hh = h[(size_t)n * N8 + f];
+            const cpx<T> hv = mk((T)hh.x, (T)hh.y);
+            for (int c = 0; c < ncol; c++) acc[c] = acc[c] + hv * A[((size_t)(c * 2 + p) * nbN + n) * N8 + f];
+        }
+        for (int c = 0; c < ncol; c++) G[((size_t)(c * 2 + p) * nbN + l) * N8 + f] = acc[c];
     }
 }
 
@@ -314,8 +316,10 @@ void launch_fft_s2n(const FftMArgs& a, const cpx<T>* J, const cpx<T>* x, int ld,
 }
 template <typename T> void launch_fft_mul(int nbN, size_t N8, int ncol, const float2* H, const cpx<T>* A, cpx<T>* G, int nsm, cudaStream_t st)
 {
-    int g = (int)std::min<size_t>((N8 + FFT_NT - 1) / FFT_NT, (size_t)nsm * 8);
-    fft_mul_kernel<T><<<g, FFT_NT, 0, st>>>(nbN, N8, ncol, H, A, G);
+    const int rows = 2 * nbN;
+    const int want = std::max(1, nsm * 16 / rows);   // about 16 CTAs per SM over all rows
+    int g = (int)std::min<size_t>((N8 + FFT_NT - 1) / FFT_NT, (size_t)want);
+    fft_mul_kernel<T><<<dim3(g, rows), FFT_NT, 0, st>>>(nbN, N8, ncol, H, A, G);
     launch_counter() += 1;
 }
 template <typename T>

@@ -398,18 +398,33 @@ __global__ void qeff_kernel(int nsph, const int* order, const int* offset, const
 }
 
 // qtotcalc (scatprops:872-912), no host spheres, one block, fixed summation order.
-__global__ void qtot_kernel(int nsph, const double* radius, const double* qeff, double xg, double* qtot)
+// qtotcalc (scatprops:872-912): one block of QTOT_NT threads, strided partial
+// sums of the area-weighted efficiencies reduced in shared memory (the
+// reference sums the spheres in order; only the summation order differs)
+#define QTOT_NT 256
+__global__ void __launch_bounds__(QTOT_NT) qtot_kernel(int nsph, const double* radius, const double* qeff, double xg, double* qtot)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double red[9][QTOT_NT];
     double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = 0; i < nsph; i++)
+    for (int i = threadIdx.x; i < nsph; i += QTOT_NT)
         for (int k = 0; k < 9; k++) s[k] = s[k] + qeff[k + 9 * i] * radius[i] * radius[i] / (xg * xg);
-    for (int pol = 0; pol < 3; pol++) s[2 + 3 * pol] = s[0 + 3 * pol] + s[2 + 3 * pol] - s[1 + 3 * pol];
-    for (int k = 0; k < 9; k++) qtot[k] = s[k];
+    for (int k = 0; k < 9; k++) red[k][threadIdx.x] = s[k];
+    __syncthreads();
+    for (int w = QTOT_NT / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 9; k++) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double t[9];
+        for (int k = 0; k < 9; k++) t[k] = red[k][0];
+        for (int pol = 0; pol < 3; pol++) t[2 + 3 * pol] = t[0 + 3 * pol] + t[2 + 3 * pol] - t[1 + 3 * pol];
+        for (int k = 0; k < 9; k++) qtot[k] = t[k];
+    }
 }
 
-// qtot_kernel over the spheres of each configuration of an ensemble (one
-// thread a configuration, the same sums in the same order)
+// totals over the spheres of each configuration of an ensemble (one thread
+// a configuration, the spheres summed in order as qtotcalc does)
 __global__ void qtot_configs_kernel(int nc, const int* cfg_start, const double* radius, const double* qeff, const double* xg, double* qtot)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -431,6 +446,6 @@ void launch_qeff(int nsph, const int* order, const int* offset, const int* mie_o
                  const zd* amnp, const zd* pmnp0, int ld, double* qeff, double xg, double* qtot, cudaStream_t st)
 {
     qeff_kernel<<<(nsph + 63) / 64, 64, 0, st>>>(nsph, order, offset, mie_offset, radius, rimed, an_inv, amnp, pmnp0, ld, qeff);
-    qtot_kernel<<<1, 32, 0, st>>>(nsph, radius, qeff, xg, qtot);
+    qtot_kernel<<<1, QTOT_NT, 0, st>>>(nsph, radius, qeff, xg, qtot);
     launch_counter() += 2;
 }
