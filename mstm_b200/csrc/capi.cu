@@ -2871,7 +2871,7 @@ static int fft_build(mstmg_ctx* c)
     c->pslot.release();
     std::vector<int4> tl;
     {
-        const int B = TILE_B, NS2 = 2 * TILE_B;
+        const int B = TILE_B;
         const int lmin = *std::min_element(c->order.begin(), c->order.end());
         c->tiled = !c->opts.generic_kernel && lmin == c->lmax && lmin >= c->opts.translation_switch_order && tiled_supported(c->lmax, 1) &&
                    !pr.empty();
@@ -2919,7 +2919,6 @@ static int fft_build(mstmg_ctx* c)
             CK(c->pslot.alloc(ps.size()));
             CK(cudaMemcpyAsync(c->tsph.p, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice, c->st));
             CK(cudaMemcpyAsync(c->pslot.p, ps.data(), sizeof(short2) * ps.size(), cudaMemcpyHostToDevice, c->st));
-            (void)NS2;
         }
     }
     int rc = upload_pairs(c, pr, (int)pr.size(), tl);   // synchronises: the host vectors above are done with
