@@ -182,9 +182,21 @@ struct GmresWork {
         const size_t fit = fr / 4 / (per ? per : 1);
         return (int)std::min<size_t>(mmax, fit > 1 ? fit - 1 : 0);
     }
+    // allocate for S systems of ne elements with the basis length pick_m
+    // allows (an error when it is below 8 steps, or below the cap when smaller)
+    int setup(int S_, int ne_, int cap, const char* who)
+    {
+        V.release();   // the old basis does not count against the new one's memory
+        const int m_ = pick_m(S_, ne_, cap);
+        if (m_ < (cap > 0 ? std::min(cap, 8) : 8)) {
+            set_err(std::string(who) + ": no device memory for the GMRES basis");
+            return MSTMG_ERR_CUDA;
+        }
+        return init(S_, ne_, m_);
+    }
     int init(int S_, int ne_, int m_)
     {
-        if (S_ == S && ne_ == ne && m_ == m && hh) return MSTMG_OK;
+        if (S_ == S && ne_ == ne && m_ == m && hh && V.p) return MSTMG_OK;
         V.release();
         S = S_;
         ne = ne_;
@@ -1515,12 +1527,8 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
         } else if (c->opts.mixed_solver == 2) {
             // both polarisations as two systems of the restarted GMRES
             if (!c->fo_gm_ready) {
-                const int m = GmresWork::pick_m(2, ne, c->opts.gmres_restart);
-                if (m < (c->opts.gmres_restart > 0 ? std::min(c->opts.gmres_restart, 8) : 8)) {
-                    set_err("mixed GMRES: no device memory for the basis");
-                    return MSTMG_ERR_CUDA;
-                }
-                if ((rc = c->fo64.init(2, ne, c->nsm, false)) || (rc = c->fo_gm.init(2, ne, m))) return rc;
+                if ((rc = c->fo64.init(2, ne, c->nsm, false)) || (rc = c->fo_gm.setup(2, ne, c->opts.gmres_restart, "mstmg_fixed_orientation")))
+                    return rc;
                 c->fo_gm_ready = true;
             }
             std::vector<int> its, sts;
@@ -1620,14 +1628,7 @@ extern "C" int mstmg_ensemble_fixed_orientation(mstmg_ctx* c, double alpha, doub
                            bvec + (size_t)p * ne, c->st);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->amnp.p, bvec, sizeof(zd) * 2 * (size_t)ne, cudaMemcpyDeviceToDevice, c->st));
-    if (!c->ens_gm.hh) {
-        const int m = GmresWork::pick_m(S, c->ens_ldv, c->opts.gmres_restart);
-        if (m < (c->opts.gmres_restart > 0 ? std::min(c->opts.gmres_restart, 8) : 8)) {
-            set_err("mstmg_ensemble_fixed_orientation: no device memory for the GMRES basis");
-            return MSTMG_ERR_CUDA;
-        }
-        if ((rc = c->ens_gm.init(S, c->ens_ldv, m))) return rc;
-    }
+    if (!c->ens_gm.hh && (rc = c->ens_gm.setup(S, c->ens_ldv, c->opts.gmres_restart, "mstmg_ensemble_fixed_orientation"))) return rc;
     const EnsSeg seg{c->ens_off.p, c->ens_len.p, c->ens_ldv};
     std::vector<int> its, sts;
     std::vector<double> ers;
@@ -2498,15 +2499,9 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     MultiWork<float> w32;
     if ((rc = w64.init(Smax, ne, c->nsm, !mixed))) return rc;
     GmresWork& gw = c->tm_gm;
-    if (mixed && c->opts.mixed_solver == 2 && !(gw.hh && gw.ne == ne && gw.S >= Smax)) {
-        gw.V.release();   // the old basis does not count against the new one's memory
-        const int m = GmresWork::pick_m(Smax, ne, c->opts.gmres_restart);
-        if (m < (c->opts.gmres_restart > 0 ? std::min(c->opts.gmres_restart, 8) : 8)) {
-            set_err("mstmg_tmatrix: no device memory for the GMRES basis");
-            return MSTMG_ERR_CUDA;
-        }
-        if ((rc = gw.init(Smax, ne, m))) return rc;
-    }
+    if (mixed && c->opts.mixed_solver == 2 && !(gw.hh && gw.ne == ne && gw.S >= Smax) &&
+        (rc = gw.setup(Smax, ne, c->opts.gmres_restart, "mstmg_tmatrix")))
+        return rc;
     if (mixed) {
         CK(X64.alloc((size_t)ne * Smax));
         if (c->opts.mixed_solver != 2) {   // FP32 BiCG work
