@@ -218,3 +218,47 @@ def solve_fixed_ensemble_batched(positions, x, m, solution_eps=1e-12, max_iterat
     results = [dict(qtot=r["qtot"][k], iterations=r["iterations"][k].tolist(), istat=int(r["istat"])) for k in range(len(positions))]
     q = np.array([rk["qtot"][0, 0] for rk in results])
     return dict(per_config=results, qext_mean=float(q.mean()), wall_s=wall, solves_per_s=len(positions) / wall)
+
+
+def shard_configs(sizes, world):
+    """Split configurations over `world` ranks with balanced work: largest
+    first, each to the rank with the least work so far (a solve's pass work
+    grows as N^2 pairs).  Returns one sorted index list per rank."""
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for k in sorted(range(len(sizes)), key=lambda k: (-sizes[k], k)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        parts[r].append(k)
+        load[r] += float(sizes[k]) ** 2
+    return [sorted(p) for p in parts]
+
+
+def reduce_means(qtots, dist=None, device="cpu"):
+    """Ensemble means of Qext, Qabs, Qsca (unpolarised) over all ranks: each
+    rank's sums and count, one all-reduce (SUM) when a process group is
+    given.  qtots: this rank's (3, 3) efficiency arrays."""
+    import torch
+    s = np.zeros(4)
+    for q in qtots:
+        s[:3] += [q[0, 0], q[1, 0], q[2, 0]]
+        s[3] += 1.0
+    t = torch.tensor(s, dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t)
+    s = t.cpu().numpy()
+    n = max(s[3], 1.0)
+    return dict(qext_mean=s[0] / n, qabs_mean=s[1] / n, qsca_mean=s[2] / n, count=int(s[3]))
+
+
+def solve_fixed_ensemble_sharded(positions, x, m, rank=0, world=1, dist=None, device="cpu", solve=None, **kw):
+    """An ensemble split over ranks (one GPU each, no exchange during the
+    solves): this rank solves its share (shard_configs) with `solve`
+    (default solve_fixed_ensemble_batched: one ensemble context), then one
+    all-reduce gives every rank the ensemble means.  Returns dict(indices,
+    per_config of this rank, and the means of reduce_means)."""
+    solve = solve_fixed_ensemble_batched if solve is None else solve
+    idx = shard_configs([len(p) for p in positions], world)[rank]
+    local = solve([positions[k] for k in idx], x, m, **kw) if idx else dict(per_config=[])
+    out = reduce_means([r["qtot"] for r in local["per_config"]], dist, device)
+    out.update(indices=idx, per_config=local["per_config"])
+    return out
