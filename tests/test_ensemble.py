@@ -126,3 +126,25 @@ def test_ensemble_context_refuses_single_cluster_entry_points():
         yk = g.sphereinteraction(x[a:b], initial_run=True)
         assert np.abs(y[a:b] - yk).max() <= 1e-12 * np.abs(yk).max()
         g.close()
+
+
+def test_ensemble_edge_configurations(oracle_mod):
+    """Configurations of one and two spheres beside larger ones, and GMRES
+    cycles of 4 steps: every system meets the criterion and the single sphere
+    gives its Mie efficiency (no pairs: the Mie start is the solution)."""
+    from mstm_b200 import api
+    from mstm_b200 import configs as C
+    L = C.truncation_order(1.0)
+    cfgs = [(np.zeros((1, 3)), np.full(1, 1.0), 1.5 + 0.01j),
+            (np.array([[0.0, 0.0, 0.0], [2.5, 0.0, 0.0]]), np.full(2, 1.0), 1.5 + 0.01j),
+            (C.rsa_sphere(15, 1.0, 0.10, seed=801)[0], np.full(15, 1.0), 1.5 + 0.01j)]
+    ens = api.SphereEnsemble(cfgs, mie_epsilon=-L, gmres_restart=4)
+    r = ens.fixedorsoln(eps=1e-12, niter=4000)
+    assert r["istat"] == 0 and (r["errors"] < 1e-12).all()
+    _, qe, _ = ens.miecoefcalc()
+    assert abs(r["qtot"][0][0, 0] / qe[0] - 1) < 1e-12
+    for k in (1, 2):
+        pos, rad, m = cfgs[k]
+        o = oracle_mod.Oracle(pos, rad, np.full(len(rad), m), mie_eps=-L)
+        ro = o.fixedorsoln(eps=1e-12, niter=4000)
+        assert np.allclose(r["qtot"][k], ro["qtot"], rtol=1e-6), k
