@@ -2,8 +2,9 @@
 
 Tolerances: the FP64 drop-in path follows the reference's iteration step for
 step, so efficiencies agree within 1e-9 relative; the mixed-precision path
-(FP32 inner BiCG + FP64 refinement) is compared with the oracle solved to the
-same strict residual and agrees within 1e-6 relative on efficiencies.
+(FP32 Krylov passes from FP64 true residuals: restarted GMRES by default, the
+BiCG forms as options) is compared with the oracle solved to the same strict
+residual and agrees within 1e-6 relative on efficiencies.
 """
 import numpy as np
 import pytest
