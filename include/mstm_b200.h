@@ -50,8 +50,10 @@ typedef struct {
     int device;                    /* CUDA device ordinal */
     double medium_re, medium_im;   /* host medium refractive index (MSTM layer_ref_index(0)); 1 in free space */
     int translation_switch_order;  /* MSTM translation_switch_order (mstm-modules-33.f90:5126), default 3 */
-    double inner_eps;              /* mixed mode: squared residual reduction per inner solve (default 1e-8) */
-    int max_outer;                 /* mixed mode: refinement steps cap (default 30) */
+    double inner_eps;              /* mixed mode: squared residual reduction a GMRES cycle (or inner BiCG solve)
+                                      aims at, at most (default 1e-8) */
+    int max_outer;                 /* mixed mode: GMRES cycles (mixed_solver 2) or refinement steps
+                                      (mixed_solver 1) at most (default 30) */
     int generic_kernel;            /* 1: always use the order-generic translation kernel (default 0) */
     int tile_ctas_per_sm;          /* tiled kernel CTAs per SM, 1..3 caps it (0: as many as shared memory and the
                                       kernel's register budget allow: 3 for FP32 passes of 1 or 2 columns, else 2) */
