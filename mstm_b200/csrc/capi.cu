@@ -22,6 +22,7 @@
 #include "densepair.cuh"
 #include <nvtx3/nvToolsExt.h>
 #include <cufft.h>
+#include <map>
 #include <memory>
 #include <type_traits>
 
@@ -162,11 +163,27 @@ struct GmresWork {
     std::vector<double> cs, target, ybuf;
     std::vector<int> kk;
     std::vector<char> frozen;
+    // Arnoldi steps captured as CUDA graphs, keyed by (step j, active
+    // systems): kernel launches and passes they hold, replayed with them
+    struct StepGraph {
+        cudaGraphExec_t exec;
+        long long launches;
+        int passes32;
+    };
+    std::map<long long, StepGraph> graphs;
+    unsigned long long graph_gen = ~0ull;   // the context's layout generation the graphs were captured at
+    bool graphs_ok = true;                  // false once a capture failed: plain launches from then on
+    void drop_graphs()
+    {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+        graphs.clear();
+    }
     GmresWork() = default;
     GmresWork(const GmresWork&) = delete;
     GmresWork& operator=(const GmresWork&) = delete;
     ~GmresWork()
     {
+        drop_graphs();
         if (hh) cudaFreeHost(hh);
     }
     size_t off1() const { return (size_t)(S + (S & 1)); }
@@ -197,6 +214,7 @@ struct GmresWork {
     int init(int S_, int ne_, int m_)
     {
         if (S_ == S && ne_ == ne && m_ == m && hh && V.p) return MSTMG_OK;
+        drop_graphs();   // they hold this work's buffers
         V.release();
         S = S_;
         ne = ne_;
@@ -229,6 +247,9 @@ struct mstmg_ctx {
     int dev = 0, nsm = 148;
     cudaStream_t st = nullptr;
     mstmg_opts opts;
+    // bumped whenever the pair lists, tiles or operator buffers may move:
+    // CUDA graphs captured before hold the old pointers
+    unsigned long long layout_gen = 0;
     int n = 0, neqns = 0, lmax = 0, npairs = 0, maxrec = 0;
     long long op_units = 0;
     double xg = 1.0;
@@ -408,6 +429,7 @@ static int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const
     }
     c->op_units = u;
     c->maxrec = maxrec;
+    c->layout_gen++;
     if (np > 0) {
         CK(c->pairs.alloc(np));
         CK(c->opoff.alloc(np));
@@ -883,6 +905,7 @@ static int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
     if (!need64 && !need32) return MSTMG_OK;
     if (c->ndense > 0) {
         DenseArgs d = dense_args(c);
+        const void* was[2] = {c->dop64.p, c->dop32.p};
         if (need64) {
             CK(c->dop64.alloc(c->dense_units));
             d.rec64 = c->dop64.p;
@@ -891,6 +914,7 @@ static int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
             CK(c->dop32.alloc(c->dense_units));
             d.rec32 = c->dop32.p;
         }
+        if (was[0] != c->dop64.p || was[1] != c->dop32.p) c->layout_gen++;
         launch_dense_gen(d, c->st);
         CK(cudaGetLastError());
     }
@@ -899,8 +923,12 @@ static int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
         if (need32) c->ops32_ready = true;
         return MSTMG_OK;
     }
-    if (need64) CK(c->op64.alloc(c->op_units));
-    if (need32) CK(c->op32.alloc(c->op_units));
+    {
+        const void* was[2] = {c->op64.p, c->op32.p};
+        if (need64) CK(c->op64.alloc(c->op_units));
+        if (need32) CK(c->op32.alloc(c->op_units));
+        if (was[0] != c->op64.p || was[1] != c->op32.p) c->layout_gen++;
+    }
     NvtxRange nvtx_("pair operator generation");
     OpGenArgs a;
     a.npairs = c->npairs;
@@ -2271,6 +2299,14 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
     const int ne = c->neqns, m = gw.m, m1 = gw.m + 1;
     const int ldv = seg ? seg->ldv : ne;             // elements a basis vector is stored in
     const int* slen = seg ? seg->len : nullptr;      // elements a system's vectors hold
+    // Arnoldi steps as CUDA graphs for the two-column solves (a fixed
+    // orientation, an ensemble), whose steps are launch-bound on small
+    // clusters: not with kernel timing (events) or the FFT path (cuFFT plans)
+    bool graphs = gw.graphs_ok && (seg || S <= 2) && !c->timing && !(c->fft && c->fft->on);
+    if (graphs && gw.graph_gen != c->layout_gen) {
+        gw.drop_graphs();
+        gw.graph_gen = c->layout_gen;
+    }
     SlotMaps sm = c->sm();
     const zf* an32 = (const zf*)c->an32.p;
     const size_t O1 = gw.off1(), HP = gw.hpass();
@@ -2335,27 +2371,70 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
         const int jmax = (int)std::min<long long>(m, room);
         for (int j = 0; j < jmax && !cur.empty(); j++) {
             const int na = (int)cur.size();
-            if (seg) {
-                CK(cudaMemsetAsync(gw.XP.p, 0, sizeof(zf) * 2 * (size_t)ne, c->st));
-                launch_eg_gather(ne, ldv, m1, j, na, gw.act.p, seg->off, seg->len, gw.V.p, gw.XP.p, c->nsm, c->st);
-                if ((rc = translate_many<float>(c, gw.XP.p, gw.Y.p, 2, 0u))) return rc;
-                launch_eg_apply(sm, an32, ne, ldv, na, gw.act.p, seg->off, seg->len, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
-            } else {
-                const int npad = na <= 2 ? na : ((na + 3) / 4) * 4;   // whole FP32 chunks
-                launch_gm_gather(ne, m1, j, na, npad, gw.act.p, gw.V.p, gw.XP.p, c->nsm, c->st);
-                if ((rc = translate_many<float>(c, gw.XP.p, gw.Y.p, npad, 0u))) return rc;
-                launch_gm_apply(sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
-            }
             const size_t hn = (size_t)(j + 1) * S * 2;
-            CK(cudaMemsetAsync(gw.h.p, 0, sizeof(double) * (O1 + hn), c->st));
-            CK(cudaMemsetAsync(h2, 0, sizeof(double) * hn, c->st));
-            launch_gm_dots(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h1, nullptr, c->nsm, c->st, slen);
-            launch_gm_update(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, h1, gw.W.p, nullptr, c->nsm, c->st, slen);
-            launch_gm_dots(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h2, h1, c->nsm, c->st, slen);
-            launch_gm_update(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, h2, gw.W.p, gw.h.p, c->nsm, c->st, slen);
-            launch_gm_scale(ldv, m1, j + 1, na, gw.act.p, 0, gw.W.p, gw.h.p, 1, 1.0e-35, gw.V.p, c->nsm, c->st, slen);
-            CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(gw.hh, gw.h.p, sizeof(double) * (O1 + hn), cudaMemcpyDeviceToHost, c->st));
+            // one Arnoldi step on the device: the pass, the Mie multiply, two
+            // Gram-Schmidt passes, the new basis vector, the Hessenberg column home
+            auto step = [&]() -> int {
+                int r2;
+                if (seg) {
+                    CK(cudaMemsetAsync(gw.XP.p, 0, sizeof(zf) * 2 * (size_t)ne, c->st));
+                    launch_eg_gather(ne, ldv, m1, j, na, gw.act.p, seg->off, seg->len, gw.V.p, gw.XP.p, c->nsm, c->st);
+                    if ((r2 = translate_many<float>(c, gw.XP.p, gw.Y.p, 2, 0u))) return r2;
+                    launch_eg_apply(sm, an32, ne, ldv, na, gw.act.p, seg->off, seg->len, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+                } else {
+                    const int npad = na <= 2 ? na : ((na + 3) / 4) * 4;   // whole FP32 chunks
+                    launch_gm_gather(ne, m1, j, na, npad, gw.act.p, gw.V.p, gw.XP.p, c->nsm, c->st);
+                    if ((r2 = translate_many<float>(c, gw.XP.p, gw.Y.p, npad, 0u))) return r2;
+                    launch_gm_apply(sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+                }
+                CK(cudaMemsetAsync(gw.h.p, 0, sizeof(double) * (O1 + hn), c->st));
+                CK(cudaMemsetAsync(h2, 0, sizeof(double) * hn, c->st));
+                launch_gm_dots(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h1, nullptr, c->nsm, c->st, slen);
+                launch_gm_update(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, h1, gw.W.p, nullptr, c->nsm, c->st, slen);
+                launch_gm_dots(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, gw.W.p, h2, h1, c->nsm, c->st, slen);
+                launch_gm_update(ldv, S, m1, j + 1, na, gw.act.p, gw.V.p, h2, gw.W.p, gw.h.p, c->nsm, c->st, slen);
+                launch_gm_scale(ldv, m1, j + 1, na, gw.act.p, 0, gw.W.p, gw.h.p, 1, 1.0e-35, gw.V.p, c->nsm, c->st, slen);
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(gw.hh, gw.h.p, sizeof(double) * (O1 + hn), cudaMemcpyDeviceToHost, c->st));
+                return MSTMG_OK;
+            };
+            if (graphs) {
+                // replayed as a CUDA graph, captured the first time this (step,
+                // active systems) shape comes up; plain launches if capture fails
+                const long long key = ((long long)j << 32) | (long long)(unsigned)na;
+                auto it = gw.graphs.find(key);
+                if (it == gw.graphs.end()) {
+                    const long long l0 = launch_counter().load();
+                    const int p0 = c->passes32;
+                    cudaGraph_t gr = nullptr;
+                    cudaGraphExec_t ex = nullptr;
+                    bool ok = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                    const int src = ok ? step() : MSTMG_ERR_CUDA;
+                    if (ok) ok = cudaStreamEndCapture(c->st, &gr) == cudaSuccess && src == MSTMG_OK && gr != nullptr;
+                    if (ok) ok = cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess;
+                    if (gr) cudaGraphDestroy(gr);
+                    const long long dl = launch_counter().load() - l0;
+                    launch_counter() -= dl;   // counted when the graph runs
+                    const int dp = c->passes32 - p0;
+                    c->passes32 = p0;
+                    if (!ok) {
+                        if (ex) cudaGraphExecDestroy(ex);
+                        (void)cudaGetLastError();   // the failed capture's error
+                        gw.graphs_ok = false;
+                        graphs = false;
+                        if ((rc = step())) return rc;
+                    } else {
+                        it = gw.graphs.emplace(key, GmresWork::StepGraph{ex, dl, dp}).first;
+                    }
+                }
+                if (graphs) {
+                    CK(cudaGraphLaunch(it->second.exec, c->st));
+                    launch_counter() += it->second.launches;
+                    c->passes32 += it->second.passes32;
+                }
+            } else if ((rc = step())) {
+                return rc;
+            }
             CK(cudaStreamSynchronize(c->st));
             const double* H1 = gw.hh + O1;
             std::vector<int> next;
