@@ -148,3 +148,22 @@ def test_ensemble_edge_configurations(oracle_mod):
         o = oracle_mod.Oracle(pos, rad, np.full(len(rad), m), mie_eps=-L)
         ro = o.fixedorsoln(eps=1e-12, niter=4000)
         assert np.allclose(r["qtot"][k], ro["qtot"], rtol=1e-6), k
+
+
+def test_sharded_ensemble_single_rank_matches_batched():
+    """solve_fixed_ensemble_sharded on one rank (no process group) solves the
+    whole ensemble in one context: its means are those of its own
+    per-configuration results, and agree with a separate batched solve to far
+    below the solution criterion (two solves differ only in the FP32 passes'
+    summation order)."""
+    from mstm_b200 import ensemble as E
+    from mstm_b200 import configs as C
+    pos = [C.rsa_sphere(n, 1.0, 0.10, seed=600 + n)[0] for n in (10, 17, 24)]
+    sh = E.solve_fixed_ensemble_sharded(pos, 1.0, 1.5 + 0.01j, rank=0, world=1)
+    assert sh["indices"] == [0, 1, 2] and sh["count"] == 3
+    own = np.array([r["qtot"] for r in sh["per_config"]])
+    assert abs(sh["qext_mean"] / own[:, 0, 0].mean() - 1) < 1e-14
+    assert abs(sh["qsca_mean"] / own[:, 2, 0].mean() - 1) < 1e-14
+    b = E.solve_fixed_ensemble_batched(pos, 1.0, 1.5 + 0.01j)
+    q = np.array([r["qtot"] for r in b["per_config"]])
+    assert abs(sh["qext_mean"] / q[:, 0, 0].mean() - 1) < 1e-8
