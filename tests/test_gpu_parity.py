@@ -479,6 +479,26 @@ def test_fft_translation_solve(api, oracle_mod):
     assert abs(rg["qtot"][0, 0] / rd["qtot"][0, 0] - 1) < 0.02
 
 
+def test_graph_replayed_solves_across_a_layout_change(api):
+    """Mixed solves replay their Arnoldi steps as CUDA graphs; a context that
+    solved directly (graphs captured), then switched to the FFT path (new pair
+    list and tiles), solves as a context set up for the FFT path from the
+    start, and repeated direct solves agree with the first."""
+    pos, rad, ri, em = _cylinder()
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed")
+    r1 = g.fixedorsoln(eps=1e-12)
+    r2 = g.fixedorsoln(eps=1e-12)   # replayed steps
+    assert r1["istat"] == r2["istat"] == 0
+    assert np.allclose(r2["qtot"], r1["qtot"], rtol=1e-8)
+    g.fft_setup(d_cell=4.0)
+    rf = g.fixedorsoln(eps=1e-12)
+    h = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed")
+    h.fft_setup(d_cell=4.0)
+    rh = h.fixedorsoln(eps=1e-12)
+    assert rf["istat"] == rh["istat"] == 0
+    assert np.allclose(rf["qtot"], rh["qtot"], rtol=1e-8)
+
+
 def test_dense_pairs_below_switch_order(api, oracle_mod):
     """Spheres of order 2 among order-4 spheres: their pairs use the dense
     gentranmatrix records on the device; matvec (both product orientations)
