@@ -120,7 +120,9 @@ int mstmg_planewave(mstmg_ctx *ctx, double alpha, double sinc, int dir, double *
 
 /* fixedorsoln (mstm-solver-8.f90:350-569) and qtotcalc.  amnp: neqns x 2 (out);
  * qeff: 3 x 3 x nsphere (out, may be NULL); qtot: 3 x 3 (out, may be NULL):
- * [ext, abs, sca] x [unpolarised, par, perp].  maxerr/maxiter as fixedorsoln's. */
+ * [ext, abs, sca] x [unpolarised, par, perp].  maxerr/maxiter as fixedorsoln's
+ * (FP64: BiCG iterations, the reference's count; mixed with mixed_solver 2:
+ * Arnoldi steps in pairs, maxerr the FP64 true residual). */
 int mstmg_fixed_orientation(mstmg_ctx *ctx, double alpha, double sinc, int dir, double eps, int niter, double *amnp,
                             double *qeff, double *qtot, double *maxerr, int *maxiter);
 
