@@ -4,7 +4,7 @@
  * Drop-in boundary for MSTM's solver path (dmckwski/MSTM, december2023 tree).
  * The reference has no FFI; its boundary is the Fortran subroutine interface.
  * Each entry point below replaces one Fortran routine, called from Fortran
- * through an ISO_C_BINDING interface module (INTEGRATION.md shows it):
+ * through an ISO_C_BINDING interface module that declares them bind(c):
  *
  *   mstmg_ctx_create         replaces the spheredata/mie module set-up:
  *                            miecoefcalc (mstm-modules-33.f90:5301-5407) and
@@ -339,21 +339,25 @@ int mstmg_kernel_time(mstmg_ctx *ctx, double *ms64, int *n64, double *ms32, int 
 /* Number of kernels this library has launched in the process so far. */
 long long mstmg_kernel_launches(void);
 
-/* Incident plane-wave coefficients (as mstmg_planewave) for callers that
- * cannot allocate device memory: no context and no cudaMalloc.  This entry
- * point has no counterpart in the reference.  It is meant for callers that
- * own all device memory themselves (e.g. a host code with its own memory
- * manager or a fixed device-memory budget).
- *   nsphere spheres, all of order `order` (1..16); pos: device array 3*nsphere;
- *   pmnp: device array, neqns x 2 complex (neqns = nsphere*2*order*(order+2)),
- *   written in MSTM's layout; stream: a cudaStream_t or NULL.
+/* Incident plane-wave coefficients for callers that cannot allocate device
+ * memory: no context and no cudaMalloc.  This entry point has no counterpart
+ * in the reference.  It is meant for callers that own all device memory
+ * themselves (e.g. a host code with its own memory manager or a fixed
+ * device-memory budget).  The same values as mstmg_planewave on a context in
+ * free space: the medium's refractive index is 1 here.
+ *   nsphere spheres, all of order `order` (1..16); pos: device array 3*nsphere
+ *   of the current device; pmnp: device array of the current device, neqns x 2
+ *   complex (neqns = nsphere*2*order*(order+2)), written in MSTM's layout;
+ *   dir 1 or 2 as mstmg_planewave's; stream: a cudaStream_t or NULL.
  * Intermediate tables live in a fixed ~32 KB device array inside the library
- * (held by every GPU that loads it until the process exits).  The first call
- * on each device looks that array up (cudaGetSymbolAddress), so make that
- * first call before any stream capture.  All calls share the array: calls
- * that overlap on the GPU race and must be serialised by the caller.  Orders
- * above 16 are rejected with MSTMG_ERR_UNSUPPORTED; host pointers with
- * MSTMG_ERR_ARG. */
+ * (held by every GPU that loads it until the process exits).  Every call made
+ * outside stream capture looks up that array's address in the current
+ * context (cudaGetSymbolAddress); a call on a stream being captured reuses
+ * the last address found on its device, so make the first call on each
+ * device before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  Orders
+ * above 16 are rejected with MSTMG_ERR_UNSUPPORTED; host pointers, or memory
+ * of another device, with MSTMG_ERR_ARG. */
 int mstmg_planewave_noalloc(int nsphere, int order, const double *pos, double alpha, double sinc, int dir, double *pmnp,
                             void *stream);
 

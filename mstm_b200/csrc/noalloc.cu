@@ -11,11 +11,16 @@
 //
 // The array is a fixed, modest size (enough for sphere order MSTMG_LMAX = 16,
 // about 32 KB) and every GPU that loads the library holds it until the
-// process exits.  Its address is looked up with cudaGetSymbolAddress on the
-// first call made on each device (that call must therefore come before any
-// stream capture).  All calls share it: each call rewrites every entry it
+// process exits.  Its device address is looked up with cudaGetSymbolAddress
+// on every call made outside stream capture, with the calling thread's
+// current device and context (a context that was destroyed and made again
+// may load the module at another address); a call made while its stream is
+// being captured reuses the address the last uncaptured call on that device
+// found, so the first call on each device must come before any stream
+// capture.  All calls share the array: each call rewrites every entry it
 // reads, but calls that overlap on the GPU (different streams, or host
 // threads on one device) race on it and must be serialised by the caller.
+// The incident field is the free-space one (medium refractive index 1).
 #include <mutex>
 #include <string>
 #include "../../include/mstm_b200.h"
@@ -55,14 +60,17 @@ __global__ void planewave_phase_uniform_kernel(int nsph, int L, const double* po
     for (int k = 0; k < 2; k++) pmnp[(size_t)k * ne + e] = (pw0[(size_t)k * nb + src] * phz) * phl;
 }
 
-static bool dev_ptr(const void* p)
+// Memory the kernels on device `dev` can use directly: device memory of
+// that device, or managed memory.
+static bool dev_ptr(const void* p, int dev)
 {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 extern "C" int mstmg_planewave_noalloc(int nsphere, int order, const double* pos, double alpha, double sinc, int dir,
@@ -77,20 +85,29 @@ extern "C" int mstmg_planewave_noalloc(int nsphere, int order, const double* pos
                         std::to_string(MSTMG_LMAX));
         return MSTMG_ERR_UNSUPPORTED;
     }
-    if (!dev_ptr(pos) || !dev_ptr(pmnp)) {
-        mstmg_internal_set_error("mstmg_planewave_noalloc: pos and pmnp must be device memory");
-        return MSTMG_ERR_ARG;
-    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 64) {
         mstmg_internal_set_error("mstmg_planewave_noalloc: no usable CUDA device");
         return MSTMG_ERR_CUDA;
     }
+    if (!dev_ptr(pos, dev) || !dev_ptr(pmnp, dev)) {
+        mstmg_internal_set_error("mstmg_planewave_noalloc: pos and pmnp must be device memory of the current device");
+        return MSTMG_ERR_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) {
+        mstmg_internal_set_error(std::string("mstmg_planewave_noalloc: cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+        return MSTMG_ERR_CUDA;
+    }
     zd* scratch;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_scratch_ptr[dev]) {
+        if (cap == cudaStreamCaptureStatusNone) {
+            // the address in the current context (looked up every time: the
+            // context may have been destroyed and created again since)
             zd* ptr = nullptr;
             e = cudaGetSymbolAddress((void**)&ptr, g_pw_scratch);
             if (e != cudaSuccess || !ptr) {
@@ -98,10 +115,12 @@ extern "C" int mstmg_planewave_noalloc(int nsphere, int order, const double* pos
                 return MSTMG_ERR_CUDA;
             }
             g_scratch_ptr[dev] = ptr;
+        } else if (!g_scratch_ptr[dev]) {
+            mstmg_internal_set_error("mstmg_planewave_noalloc: the first call on a device must come before stream capture");
+            return MSTMG_ERR_ARG;
         }
         scratch = g_scratch_ptr[dev];
     }
-    cudaStream_t st = (cudaStream_t)stream;
     zd riinc = mk(1.0, 0.0);
     zd a = cdiv(mk(sinc, 0.0), riinc);
     zd cbinc = csqrtd((mk(1.0, 0.0) - a) * (mk(1.0, 0.0) + a)) * (double)(3 - 2 * dir);

@@ -988,6 +988,7 @@ struct orc_ctx {
     cplx *Jsn, *Jns;       /* per sphere: dense J(node - pos) (nbN x nb_i x 2) and J(pos - node) (nb_i x nbN x 2) */
     size_t *joff;
     cplx *Hc;              /* dense H at every node offset (2cd-1)^3 x nbN x nbN x 2, zero inside the hole */
+    int last_iter[2];      /* cbicg iterations of each polarisation in the last orc_fixedorsoln */
 };
 
 orc_ctx *orc_create(int nsphere, const double *pos, const double *radius, const double *ri,
@@ -1843,6 +1844,7 @@ int orc_fixedorsoln(orc_ctx *c, double alpha, double sinc, int dir, double eps, 
             else orc_cbicg(c, niter, eps, pmnpan, amnp + (size_t)neq * p, initialize, &iter, &serr);
         }
         initialize = 0;
+        c->last_iter[p] = iter;
         *maxiter = imax(iter, *maxiter);
         *maxerr = serr > *maxerr ? serr : *maxerr;
         if (iter > niter || serr > eps) istat = 1;
@@ -1851,6 +1853,10 @@ int orc_fixedorsoln(orc_ctx *c, double alpha, double sinc, int dir, double eps, 
     free(pmnp0); free(pmnpan);
     return istat;
 }
+
+/* Iteration counts of both polarisations of the last orc_fixedorsoln (the
+ * reference reports only the second one, solver:524-531). */
+void orc_last_iterations(const orc_ctx *c, int *iters2) { iters2[0] = c->last_iter[0]; iters2[1] = c->last_iter[1]; }
 
 /* ---- low-level exports used by the unit tests ---- */
 void orc_x_rotcoef(double cbe, int kmax, int nmax, double *dc) { tables_init(); rotcoef(cbe, kmax, nmax, dc); }

@@ -47,6 +47,7 @@ void orc_planewave(const orc_ctx *c, double alpha, double sinc, int dir, ocplx *
 int orc_fixedorsoln(orc_ctx *c, double alpha, double sinc, int dir, double eps, int niter,
                     ocplx *amnp, double *qeff, double *maxerr, int *maxiter, int direct);
 void orc_qtotcalc(const orc_ctx *c, double *qeff, double *qtot);
+void orc_last_iterations(const orc_ctx *c, int *iters2);
 double orc_vol_radius(const orc_ctx *c);
 
 #endif

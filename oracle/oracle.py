@@ -47,6 +47,7 @@ def lib():
                                       P(c_double), P(c_int), c_int]
         L.orc_fixedorsoln.restype = c_int
         L.orc_qtotcalc.argtypes = [c_void_p, c_void_p, c_void_p]
+        L.orc_last_iterations.argtypes = [c_void_p, c_void_p]
         L.orc_vol_radius.argtypes = [c_void_p]
         L.orc_vol_radius.restype = c_double
         L.orc_x_rotcoef.argtypes = [c_double, c_int, c_int, c_void_p]
@@ -172,7 +173,10 @@ class Oracle:
                                     ctypes.byref(maxerr), ctypes.byref(maxiter), int(direct))
         qtot = np.zeros((3, 3), np.float64, order="F")
         self.L.orc_qtotcalc(self.ctx, _p(qeff), _p(qtot))
-        return dict(amnp=amnp, qeff=qeff, qtot=qtot, status=st, maxerr=maxerr.value, maxiter=maxiter.value)
+        iters = np.zeros(2, np.int32)
+        self.L.orc_last_iterations(self.ctx, _p(iters))
+        return dict(amnp=amnp, qeff=qeff, qtot=qtot, status=st, maxerr=maxerr.value, maxiter=maxiter.value,
+                    iterations=iters.tolist())
 
     def direct_solve(self, pnp):
         pnp = np.ascontiguousarray(pnp, np.complex128)
