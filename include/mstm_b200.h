@@ -66,6 +66,10 @@ typedef struct {
                                       inside FP64 refinement */
     int gmres_restart;             /* mixed_solver 2: Arnoldi steps per cycle at most (0: up to 200, fewer
                                       when a quarter of the free device memory cannot hold the basis) */
+    int tensor_core;               /* FP32 passes of 12 or more plain columns (the T-matrix GMRES) on the
+                                      tensor cores with dense TF32 hi/lo pair operators: 0 when the context
+                                      qualifies (one sphere order 5..10, direct pairs) and the operators fit
+                                      in a third of the free device memory (default), -1 never */
 } mstmg_opts;
 
 /* Fill opts with the defaults above. */
@@ -310,7 +314,10 @@ int mstmg_operator_bytes(const mstmg_ctx *ctx, int prec, double *stored_bytes, d
  * mstm-modules-33.f90:6390-6525, no Mie multiply): ncols columns (<= 256) of
  * neqns complex values, column k a conjugate-transpose product when
  * con_tran[k] != 0 (NULL: none), with the FP64 (prec 0) or FP32 (prec 1)
- * operators and kernels the solvers use; FP32 results are returned widened. */
+ * operators and kernels the solvers use, or (prec 2) the tensor-core pass
+ * with dense TF32 hi/lo operators, which takes no conjugate-transpose columns
+ * and returns MSTMG_ERR_UNSUPPORTED where the context does not qualify (see
+ * mstmg_opts.tensor_core); FP32 results are returned widened. */
 int mstmg_translation_pass(mstmg_ctx *ctx, int prec, int ncols, const int *con_tran, const double *x, double *y);
 
 /* Diagnostic, no counterpart in the reference: runs the bounded mbarrier
@@ -335,6 +342,9 @@ int mstmg_set_stream(mstmg_ctx *ctx, void *stream);
  * of the FP64 and FP32 translation kernels since the last reset. */
 int mstmg_set_timing(mstmg_ctx *ctx, int enable);
 int mstmg_kernel_time(mstmg_ctx *ctx, double *ms64, int *n64, double *ms32, int *n32);
+/* The same for the tensor-core passes (mstmg_opts.tensor_core): summed
+ * milliseconds and count since the last call. */
+int mstmg_kernel_time_tc(mstmg_ctx *ctx, double *ms, int *n);
 
 /* Number of kernels this library has launched in the process so far. */
 long long mstmg_kernel_launches(void);

@@ -68,6 +68,7 @@ SIGNATURES = {
     "mstmg_set_stream": (c_int, [c_void_p, c_void_p]),
     "mstmg_set_timing": (c_int, [c_void_p, c_int]),
     "mstmg_kernel_time": (c_int, [c_void_p, P(c_double), P(c_int), P(c_double), P(c_int)]),
+    "mstmg_kernel_time_tc": (c_int, [c_void_p, P(c_double), P(c_int)]),
     "mstmg_kernel_launches": (ctypes.c_longlong, []),
     "mstmg_planewave_noalloc": (c_int, [c_int, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p]),
     "mstmg_last_error": (ctypes.c_char_p, []),
@@ -78,7 +79,7 @@ class MstmgOpts(ctypes.Structure):
     _fields_ = [("precision", c_int), ("device", c_int), ("medium_re", c_double), ("medium_im", c_double),
                 ("translation_switch_order", c_int), ("inner_eps", c_double), ("max_outer", c_int),
                 ("generic_kernel", c_int), ("tile_ctas_per_sm", c_int), ("fp32_chunk", c_int),
-                ("mixed_solver", c_int), ("gmres_restart", c_int)]
+                ("mixed_solver", c_int), ("gmres_restart", c_int), ("tensor_core", c_int)]
 
 
 class MstmgError(RuntimeError):

@@ -99,7 +99,7 @@ class SphereCluster(_Context):
 
     def __init__(self, positions, radii, ref_index, mie_epsilon=1.0e-6, precision="fp64", device=0,
                  medium_index=1.0, inner_eps=1.0e-8, max_outer=30, generic_kernel=False, tile_ctas_per_sm=0, fp32_chunk=0,
-                 mixed_solver=2, gmres_restart=0):
+                 mixed_solver=2, gmres_restart=0, tensor_core=0):
         self._L = _lib.lib()
         pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
         rad = np.ascontiguousarray(np.asarray(radii, np.float64).reshape(-1))
@@ -121,6 +121,7 @@ class SphereCluster(_Context):
         opts.fp32_chunk = int(fp32_chunk)
         opts.mixed_solver = int(mixed_solver)
         opts.gmres_restart = int(gmres_restart)
+        opts.tensor_core = int(tensor_core)
         self.ctx = ctypes.c_void_p()
         check(self._L.mstmg_ctx_create(ctypes.byref(self.ctx), n, _ptr(pos), _ptr(rad), _ptr(ri2), float(mie_epsilon),
                                        ctypes.byref(opts)), "mstmg_ctx_create")
@@ -192,12 +193,15 @@ class SphereCluster(_Context):
 
     def translation_pass(self, x, con_tran=None, precision="fp64"):
         """y = H x, the pair translation pass alone (external_to_external_expansion,
-        mstm-modules-33.f90:6390-6525) with the FP64 or FP32 ("fp32") operators."""
+        mstm-modules-33.f90:6390-6525) with the FP64 ("fp64") or FP32 ("fp32")
+        operators, or ("tc") the tensor-core pass (dense TF32 hi/lo operators,
+        plain columns only)."""
         x = np.asfortranarray(np.asarray(x, np.complex128).reshape(self.number_eqns, -1))
         ncols = x.shape[1]
         y = np.zeros_like(x, order="F")
         ct = None if con_tran is None else np.ascontiguousarray(np.asarray(con_tran, np.int32))
-        check(self._L.mstmg_translation_pass(self.ctx, 0 if precision == "fp64" else 1, ncols, None if ct is None else _ptr(ct),
+        prec = {"fp64": 0, "fp32": 1, "mixed": 1, "tc": 2}[precision]
+        check(self._L.mstmg_translation_pass(self.ctx, prec, ncols, None if ct is None else _ptr(ct),
                                              _ptr(x), _ptr(y)), "translation_pass")
         return y
 

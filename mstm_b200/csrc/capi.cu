@@ -20,6 +20,7 @@
 #include "ranorient.cuh"
 #include "fftpath.cuh"
 #include "densepair.cuh"
+#include "tcpass.cuh"
 #include <nvtx3/nvToolsExt.h>
 #include <cufft.h>
 #include <map>
@@ -313,13 +314,21 @@ struct mstmg_ctx {
     DevBuf<zf> dop32;
     DevBuf<double> gt_tc, gt_bcd, gt_fnr;
     int gt_nmax = 0;
+    // dense operators of every ordered pair for the tensor-core pass of many
+    // FP32 columns (tcpass.cu): images, ordered pairs by target, column images
+    int tc_state = 0;   // 0 not built, 1 built, -1 not available for this context
+    DevBuf<float> tc_h, tc_a;
+    DevBuf<int> tc_rstart, tc_rsrc;
+    DevBuf<int2> tc_ent;
+    int tc_nent = 0;
+    int tc_passes = 0;
     cudaStream_t own_st = nullptr;
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
     struct Pending { cudaEvent_t a, b; int prec; };
     std::vector<Pending> pending;
-    double kt_ms[2] = {0.0, 0.0};
-    int kt_n[2] = {0, 0};
+    double kt_ms[3] = {0.0, 0.0, 0.0};   // FP64, FP32 rotation passes; FP32 tensor-core passes
+    int kt_n[3] = {0, 0, 0};
     SlotMaps sm() const { return SlotMaps{neqns / 2, slot.p, d_order.p, d_offset.p, d_mie_offset.p}; }
 };
 
@@ -360,6 +369,7 @@ extern "C" void mstmg_default_opts(mstmg_opts* o)
     o->fp32_chunk = 0;
     o->mixed_solver = 2;
     o->gmres_restart = 0;
+    o->tensor_core = 0;
 }
 
 extern "C" const char* mstmg_last_error(void) { return g_err.c_str(); }
@@ -438,6 +448,27 @@ static int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const
         CK(cudaStreamSynchronize(c->st));   // host vectors are freed on return
     }
     c->ops64_ready = c->ops32_ready = false;
+    if (c->tc_state == 1) c->tc_state = 0;
+    return MSTMG_OK;
+}
+
+// tran_coef constants of gentranmatrix (and the tables its Legendre
+// recurrence uses) for orders up to lm, on the device
+static int ensure_gentran(mstmg_ctx* c, int lm)
+{
+    if (c->gt_nmax >= lm) return MSTMG_OK;
+    std::vector<double> tcv, bd(GT_WMAX + 2);
+    gentran_constants(lm, tcv);
+    mstmg::Tables tb(6 * GT_WMAX + 6);
+    for (int k = 0; k < (int)bd.size(); k++) bd[k] = tb.bc(k, k);
+    CK(c->gt_tc.alloc(tcv.size()));
+    CK(c->gt_bcd.alloc(bd.size()));
+    CK(c->gt_fnr.alloc(tb.fnr.size()));
+    CK(cudaMemcpyAsync(c->gt_tc.p, tcv.data(), sizeof(double) * tcv.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->gt_bcd.p, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->gt_fnr.p, tb.fnr.data(), sizeof(double) * tb.fnr.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->gt_nmax = lm;
     return MSTMG_OK;
 }
 
@@ -519,18 +550,7 @@ static int setup_layout(mstmg_ctx* c)
             CK(c->doff.alloc(doff.size()));
             CK(cudaMemcpyAsync(c->dpairs.p, dp.data(), sizeof(int2) * dp.size(), cudaMemcpyHostToDevice, c->st));
             CK(cudaMemcpyAsync(c->doff.p, doff.data(), sizeof(long long) * doff.size(), cudaMemcpyHostToDevice, c->st));
-            std::vector<double> tcv, bd(GT_WMAX + 2);
-            gentran_constants(lm, tcv);
-            mstmg::Tables tb(6 * GT_WMAX + 6);
-            for (int k = 0; k < (int)bd.size(); k++) bd[k] = tb.bc(k, k);
-            CK(c->gt_tc.alloc(tcv.size()));
-            CK(c->gt_bcd.alloc(bd.size()));
-            CK(c->gt_fnr.alloc(tb.fnr.size()));
-            CK(cudaMemcpyAsync(c->gt_tc.p, tcv.data(), sizeof(double) * tcv.size(), cudaMemcpyHostToDevice, c->st));
-            CK(cudaMemcpyAsync(c->gt_bcd.p, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice, c->st));
-            CK(cudaMemcpyAsync(c->gt_fnr.p, tb.fnr.data(), sizeof(double) * tb.fnr.size(), cudaMemcpyHostToDevice, c->st));
-            CK(cudaStreamSynchronize(c->st));
-            c->gt_nmax = lm;
+            if (int rg = ensure_gentran(c, lm)) return rg;
         }
     }
     // pair list (i < j, the reference's loop order) and operator offsets
@@ -724,8 +744,9 @@ static int create_impl(mstmg_ctx** out, int nsphere, const double* pos, const do
             }
         }
     }
-    if (opts && (opts->gmres_restart < 0 || opts->mixed_solver < 0 || opts->mixed_solver > 2)) {
-        set_err("mstmg_ctx_create: gmres_restart must be >= 0 and mixed_solver 0, 1 or 2");
+    if (opts && (opts->gmres_restart < 0 || opts->mixed_solver < 0 || opts->mixed_solver > 2 || opts->tensor_core < -1 ||
+                 opts->tensor_core > 1)) {
+        set_err("mstmg_ctx_create: gmres_restart must be >= 0, mixed_solver 0, 1 or 2 and tensor_core -1, 0 or 1");
         return MSTMG_ERR_ARG;
     }
     mstmg_ctx* c = new mstmg_ctx();
@@ -841,6 +862,7 @@ extern "C" int mstmg_ctx_set_positions(mstmg_ctx* c, const double* pos)
     if (is_dev(pos)) CK(cudaMemcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n, cudaMemcpyDeviceToHost));
     else memcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n);
     c->ops64_ready = c->ops32_ready = false;
+    if (c->tc_state == 1) c->tc_state = 0;
     if (c->fft && c->fft->on) {
         c->fft->drop_plans();
         c->fft->on = false;
@@ -1080,6 +1102,143 @@ static int fp32_chunk(mstmg_ctx* c, const zf* x, zf* y, int ncols, unsigned patt
     return c->chunk32;
 }
 
+// ---------------------------------------------------------------------------
+// the tensor-core pass of many FP32 columns (tcpass.cu)
+// ---------------------------------------------------------------------------
+// Columns from which a plain (no conjugate-transpose column) FP32 pass goes to
+// the tensor cores: one M tile costs the same for 1 or 128 columns, and at 12
+// columns it already beats the rotation kernel.
+#define TC_MIN_COLS 12
+
+// One sphere order (5..10), pairs translated directly (no FFT, no dense
+// pairs): the cases the dense TF32 images serve.
+static bool tc_eligible(const mstmg_ctx* c)
+{
+    if (c->opts.tensor_core < 0 || c->tc_state < 0) return false;
+    if (!c->tiled || c->ndense > 0 || (c->fft && c->fft->on) || c->npairs == 0) return false;
+    return c->lmax >= 5 && tc_geom(c->lmax).NP <= 128;
+}
+
+// Build the dense operator images of every ordered pair (both directions of
+// each pair of the context's list), unless they would take more than a third
+// of the free device memory (the context then keeps the rotation kernels).
+static int ensure_tc(mstmg_ctx* c)
+{
+    if (c->tc_state == 1) return MSTMG_OK;
+    if (!tc_eligible(c)) return MSTMG_ERR_UNSUPPORTED;
+    NvtxRange nvtx_("tensor-core operator images");
+    const TcGeom g = tc_geom(c->lmax);
+    std::vector<int2> pr(c->npairs);
+    CK(cudaMemcpyAsync(pr.data(), c->pairs.p, sizeof(int2) * c->npairs, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    std::vector<std::vector<int>> nbr(c->n);
+    for (const int2& q : pr) {
+        nbr[q.x].push_back(q.y);
+        nbr[q.y].push_back(q.x);
+    }
+    std::vector<int> rstart(c->n + 1, 0), rsrc;
+    std::vector<int2> ent;
+    rsrc.reserve(2 * (size_t)c->npairs);
+    ent.reserve(2 * (size_t)c->npairs);
+    for (int i = 0; i < c->n; i++) {
+        std::sort(nbr[i].begin(), nbr[i].end());
+        rstart[i] = (int)rsrc.size();
+        for (int j : nbr[i]) {
+            rsrc.push_back(j);
+            ent.push_back(make_int2(i, j));
+        }
+    }
+    rstart[c->n] = (int)rsrc.size();
+    const size_t need = ent.size() * tc_himg_floats(g) * sizeof(float);
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    if (need > fr / 3) {
+        c->tc_state = -1;
+        set_err("tensor-core operator images (" + std::to_string(need >> 20) + " MiB) exceed a third of the free device memory");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    if (int rg = ensure_gentran(c, c->lmax)) return rg;
+    const void* was = c->tc_h.p;
+    CK(c->tc_h.alloc(ent.size() * tc_himg_floats(g)));
+    CK(c->tc_ent.alloc(ent.size()));
+    CK(c->tc_rstart.alloc(rstart.size()));
+    CK(c->tc_rsrc.alloc(rsrc.size()));
+    if (was != c->tc_h.p) c->layout_gen++;
+    CK(cudaMemcpyAsync(c->tc_ent.p, ent.data(), sizeof(int2) * ent.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->tc_rstart.p, rstart.data(), sizeof(int) * rstart.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->tc_rsrc.p, rsrc.data(), sizeof(int) * rsrc.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(c->tc_h.p, 0, need, c->st));   // the padded rows and sources stay zero
+    TcGenArgs a;
+    a.nent = (int)ent.size();
+    a.ent = c->tc_ent.p;
+    a.pos = c->pos.p;
+    a.geo = g;
+    a.rimed_re = c->opts.medium_re;
+    a.rimed_im = c->opts.medium_im;
+    a.g.tc = c->gt_tc.p;
+    a.g.nmax = c->gt_nmax;
+    a.g.nd = c->gt_nmax * (c->gt_nmax + 2);
+    a.g.fnr = c->gt_fnr.p;
+    a.g.bcd = c->gt_bcd.p;
+    a.himg = c->tc_h.p;
+    launch_tc_gen(a, c->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->st));   // the host vectors above are freed on return
+    c->tc_nent = (int)ent.size();
+    c->tc_state = 1;
+    return MSTMG_OK;
+}
+
+// y[:, 0:ncols] = H x[:, 0:ncols] (no conjugate-transpose columns) on the
+// tensor cores; y zeroed here
+static int tc_translate(mstmg_ctx* c, const zf* x, zf* y, int ncols)
+{
+    NvtxRange nvtx_("translation pass FP32 tensor cores");
+    if (int rc = ensure_tc(c)) return rc;
+    const TcGeom g = tc_geom(c->lmax);
+    const int nmt = (ncols + TC_M - 1) / TC_M;
+    const void* was = c->tc_a.p;
+    CK(c->tc_a.alloc((size_t)nmt * c->n * tc_aimg_floats(g)));
+    if (was != c->tc_a.p) c->layout_gen++;
+    CK(cudaMemsetAsync(y, 0, sizeof(zf) * (size_t)c->neqns * ncols, c->st));
+    TcPassArgs a;
+    a.nsph = c->n;
+    a.geo = g;
+    a.ld = c->neqns;
+    a.ncols = ncols;
+    a.nmt = nmt;
+    a.rstart = c->tc_rstart.p;
+    a.rsrc = c->tc_rsrc.p;
+    a.nent = c->tc_nent;
+    a.himg = c->tc_h.p;
+    a.aimg = c->tc_a.p;
+    a.x = x;
+    a.y = y;
+    a.err = c->err.p;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c->timing) {
+        for (cudaEvent_t* ev : {&e0, &e1}) {
+            if (!c->ev_pool.empty()) { *ev = c->ev_pool.back(); c->ev_pool.pop_back(); }
+            else CK(cudaEventCreate(ev));
+        }
+        CK(cudaEventRecord(e0, c->st));
+    }
+    if (launch_tc_pass(a, c->nsm, c->st) != 0) {
+        if (e0) c->ev_pool.push_back(e0);
+        if (e1) c->ev_pool.push_back(e1);
+        set_err("tensor-core pass: unsupported geometry");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    CK(cudaGetLastError());
+    if (c->timing) {
+        CK(cudaEventRecord(e1, c->st));
+        c->pending.push_back({e0, e1, 2});
+    }
+    c->passes32++;
+    c->tc_passes++;
+    return MSTMG_OK;
+}
+
 // Many columns: y[:, 0:ncols] = H x[:, 0:ncols], where column k is a
 // conjugate-transpose product when bit (k & 1) of pattern2 is set (BiCG packs
 // [p_1, w_1, p_2, w_2, ...]: pattern2 = 2).  On the tiled path the columns go
@@ -1094,7 +1253,15 @@ template <typename T> static int translate_many(mstmg_ctx* c, const cpx<T>* x, c
         return m;
     };
     int NR = 2;
-    if constexpr (sizeof(T) == 4) NR = fp32_chunk(c, x, y, ncols, pattern2);
+    if constexpr (sizeof(T) == 4) {
+        // many plain columns: the tensor-core pass when the context has (or can
+        // build) its dense operator images
+        if (pattern2 == 0 && ncols >= TC_MIN_COLS && tc_eligible(c)) {
+            int rc = tc_translate(c, x, y, ncols);
+            if (rc != MSTMG_ERR_UNSUPPORTED) return rc;
+        }
+        NR = fp32_chunk(c, x, y, ncols, pattern2);
+    }
     if (c->tiled && ncols > NR && ncols % NR == 0 && tiled_supported(c->lmax, NR)) {
         int rc = translate<T>(c, x, y, NR, expand(NR), ncols / NR);
         if (rc != MSTMG_ERR_UNSUPPORTED) return rc;
@@ -3135,8 +3302,10 @@ extern "C" int mstmg_set_timing(mstmg_ctx* c, int enable)
     CK(cudaStreamSynchronize(c->st));
     resolve_timing(c);
     c->timing = enable != 0;
-    c->kt_ms[0] = c->kt_ms[1] = 0.0;
-    c->kt_n[0] = c->kt_n[1] = 0;
+    for (int k = 0; k < 3; k++) {
+        c->kt_ms[k] = 0.0;
+        c->kt_n[k] = 0;
+    }
     return MSTMG_OK;
 }
 
@@ -3149,8 +3318,22 @@ extern "C" int mstmg_kernel_time(mstmg_ctx* c, double* ms64, int* n64, double* m
     if (n64) *n64 = c->kt_n[0];
     if (ms32) *ms32 = c->kt_ms[1];
     if (n32) *n32 = c->kt_n[1];
-    c->kt_ms[0] = c->kt_ms[1] = 0.0;
-    c->kt_n[0] = c->kt_n[1] = 0;
+    for (int k = 0; k < 2; k++) {
+        c->kt_ms[k] = 0.0;
+        c->kt_n[k] = 0;
+    }
+    return MSTMG_OK;
+}
+
+extern "C" int mstmg_kernel_time_tc(mstmg_ctx* c, double* ms, int* n)
+{
+    if (!c) return MSTMG_ERR_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    resolve_timing(c);
+    if (ms) *ms = c->kt_ms[2];
+    if (n) *n = c->kt_n[2];
+    c->kt_ms[2] = 0.0;
+    c->kt_n[2] = 0;
     return MSTMG_OK;
 }
 
@@ -3185,11 +3368,22 @@ extern "C" int mstmg_selftest_bounded_wait(int device, int limit, int* status)
 extern "C" int mstmg_translation_pass(mstmg_ctx* c, int prec, int ncols, const int* con_tran, const double* x, double* y)
 {
     NvtxRange nvtx_("mstmg_translation_pass");
-    if (!c || ncols < 1 || ncols > 256 || !x || !y || (prec != 0 && prec != 1)) {
+    if (!c || ncols < 1 || ncols > 256 || !x || !y || prec < 0 || prec > 2) {
         set_err("mstmg_translation_pass: bad arguments");
         return MSTMG_ERR_ARG;
     }
-    int rc = ensure_ops(c, prec, false);
+    if (prec == 2) {   // the tensor-core pass, required
+        for (int k = 0; con_tran && k < ncols; k++)
+            if (con_tran[k]) {
+                set_err("mstmg_translation_pass: the tensor-core pass takes no conjugate-transpose columns");
+                return MSTMG_ERR_UNSUPPORTED;
+            }
+        if (!tc_eligible(c)) {
+            set_err("mstmg_translation_pass: no tensor-core pass for this context (one sphere order 5..10, direct pairs)");
+            return MSTMG_ERR_UNSUPPORTED;
+        }
+    }
+    int rc = prec == 2 ? MSTMG_OK : ensure_ops(c, prec, false);
     if (rc) return rc;
     const size_t ne = (size_t)c->neqns, cols = ne * ncols;
     // a period-2 con_tran pattern goes through the many-column path; anything
@@ -3224,7 +3418,9 @@ extern "C" int mstmg_translation_pass(mstmg_ctx* c, int prec, int ncols, const i
         CK(x32.alloc(cols));
         CK(y32.alloc(cols));
         launch_d2f((int)cols, x64.p, x32.p, c->st);
-        if ((rc = groups(x32.p, y32.p))) return rc;
+        if (prec == 2) rc = tc_translate(c, x32.p, y32.p, ncols);
+        else rc = groups(x32.p, y32.p);
+        if (rc) return rc;
         CK(cudaMemsetAsync(y64.p, 0, sizeof(zd) * cols, c->st));
         launch_add_correction_f((int)cols, y64.p, y32.p, c->st);
         CK(cudaGetLastError());
