@@ -17,8 +17,10 @@ Arms:
                      true residuals, both polarisations in each pass), with
                      the plain FP64 drop-in path (the reference's BiCG step for
                      step) measured beside it;
-  --impl reference   the CPU restatement of the reference (oracle/), on the host
-                     cores, over a bounded sample scaled to a full solve.
+  --impl reference   the CPU restatement of the reference (oracle/) on all host
+                     cores: one complete FP64 solve of the same configuration
+                     per timed step (its own BiCG iterations to the same
+                     criterion).
 
 Timing: CUDA events on the stream the library launches on, W untimed warm-up
 solves, K timed solves; operators (2 GB FP64 + 1 GB FP32) exceed the 126 MB L2,
@@ -80,6 +82,41 @@ def max_over_ranks(dist, x, device):
 def job_value(ws, steps, ms_total_max):
     """Whole-job throughput: the solves of all ranks over the slowest rank's time."""
     return ws * steps * 1000.0 / ms_total_max
+
+
+def bench_config(ws):
+    """The workload both arms time (the same dict in both lines)."""
+    return {"workload": "fractal aggregate, 500 touching monomers, x=2.0, m=1.6+0.05i, Df=1.8, kf=1.3, "
+                        "L=9, +z incidence, both polarisations",
+            "neqns": 99000, "pairs": 124750, "residual": "||r||/||b|| < 1e-6 (squared-norm eps 1e-12)",
+            "parallelism": "replicas" if ws > 1 else "single GPU",
+            "l2": "operators (2 GB FP64 / 1 GB FP32) exceed the 126 MB L2; no flush needed"}
+
+
+def oracle_fixture(name):
+    """The oracle's frozen FP64 results for a workload (tests/golden, made by
+    tests/golden/make_oracle_fixtures.py), or None."""
+    path = os.path.join(ROOT, "tests", "golden", "oracle_%s.npz" % name)
+    if not os.path.exists(path):
+        return None
+    return dict(np.load(path))
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def errors_vs_oracle(qtot, smat, g, f):
+    """Relative errors of a fixed-orientation result against the oracle's:
+    each efficiency (unpolarised) and the 3 x 3 table, the 181-angle
+    scattering matrix (of S11's largest value) and the asymmetry parameter."""
+    out = {"qext": abs(qtot[0, 0] / f["qtot"][0, 0] - 1), "qabs": abs(qtot[1, 0] / f["qtot"][1, 0] - 1),
+           "qsca": abs(qtot[2, 0] / f["qtot"][2, 0] - 1), "qtot_3x3": rel_err(qtot, f["qtot"])}
+    if smat is not None:
+        out["smat_of_s11max"] = float(np.abs(smat - f["smat"]).max() / np.abs(f["smat"][:, 0, 0]).max())
+        out["g"] = abs(g / f["g"] - 1)
+    return {k: float("%.3g" % v) for k, v in out.items()}
 
 
 def workload_for_rank(rank):
@@ -204,9 +241,16 @@ def run_gpu(args):
         stats = g.last_stats()
         ms_max = max_over_ranks(dist, ms, dev)
         q = qtot.cpu().numpy().reshape(3, 3, order="F")
+        vs_oracle = None
+        fx = oracle_fixture(WORKLOAD) if rank == 0 else None
+        if fx is not None:
+            sol = amnp.cpu().numpy().view(np.complex128).reshape(2, ne).T
+            sc = g.scattering(np.asfortranarray(sol))
+            vs_oracle = errors_vs_oracle(q, sc["smat"], sc["g"], fx)
         results[prec] = dict(ms_total=ms_max, ms_per_step=ms_max / args.steps, istat=st, maxerr=me.value, stats=stats,
                              qtot=q, launches=launches, k64=(k64.value, n64.value), k32=(k32.value, n32.value), clocks=ck,
-                             bytes64=g.operator_bytes("fp64"), bytes32=g.operator_bytes("mixed"), nrhs_hint=None)
+                             bytes64=g.operator_bytes("fp64"), bytes32=g.operator_bytes("mixed"), nrhs_hint=None,
+                             vs_oracle=vs_oracle)
         if prec == "mixed":
             # end to end through the public C ABI with host buffers: new
             # positions copied in from pinned host memory, results read back
@@ -242,7 +286,7 @@ def run_gpu(args):
             line["other_workloads"] = extras
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline_sample(results["fp64"]["stats"]["iterations"], threads=os.cpu_count() or 1)
+            cpu = cpu_baseline_sample(threads=os.cpu_count() or 1)
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -288,11 +332,33 @@ def run_extras(args, dev, stream):
     pos = pos[0] if isinstance(pos, tuple) else pos
     row = {"workload": "5000 spheres, x=1.0, m=1.31, RSA in a cylinder (aspect 1) at fv 0.25, FFT translation, d_cell 4",
            "metric": "solves/s at 1e-6 residual (both polarisations)"}
+    fx = oracle_fixture("cylinder_fft")
     for prec in ("mixed", "fp64"):
         g = cluster(pos, 1.0, 1.31 + 0j, prec)
         grid = g.fft_setup(d_cell=4.0)
         ms, r = timed(lambda: g.fixedorsoln(eps=EPS, niter=NITER), 2)
         row[prec] = {"solves_per_s": round(1000.0 / ms, 3), "ms": round(ms, 2), "qext": r["qtot"][0, 0], "iterations": r["iterations"]}
+        if fx is not None:
+            sc = g.scattering(r["amnp"])
+            row[prec]["vs_oracle"] = errors_vs_oracle(r["qtot"], sc["smat"], sc["g"], fx)
+        if prec == "mixed":
+            # the matvec against the FFT path's algorithmic bytes: near-pair
+            # operators (FP32) + the kernel spectra (complex64, read once) +
+            # the node grids (written and read by the forward and inverse
+            # transforms) + x read and y written, for the two columns of an
+            # Arnoldi pass
+            ms_pass = g.time_translation("mixed", 2, 10)
+            near = g.operator_bytes("mixed")[0]
+            cdim, no = grid["cell_dim"], grid["node_order"]
+            nodes = (2 * cdim[0]) * (2 * cdim[1]) * (2 * cdim[2])
+            nbn = no * (no + 2)
+            spectra = nodes * nbn * nbn * 2 * 8
+            grids = 2 * 2 * nodes * nbn * 2 * 2 * 8
+            vecs = 2 * g.number_eqns * 8 * 2
+            alg = near + spectra + grids + vecs
+            row["matvec"] = {"ms_per_pass_2_columns": round(ms_pass, 4), "algorithmic_bytes": alg,
+                             "bytes": {"near_pair_operators": near, "kernel_spectra": spectra, "node_grids": grids, "vectors": vecs},
+                             "achieved_gbs": round(alg / ms_pass / 1e6, 1), "frac_of_measured_hbm": round(alg / ms_pass / 1e6 / hbm_peak(), 4)}
         row["grid"] = grid
         g.close()
     row["qext_rel_diff"] = abs(row["mixed"]["qext"] / row["fp64"]["qext"] - 1)
@@ -302,14 +368,40 @@ def run_extras(args, dev, stream):
     row = {"workload": "100 spheres, x=1.5, m=1.6+0.005i, RSA in a sphere at fv 0.20: cluster T matrix, "
                        "all 2Lc(Lc+2) columns to residual 1e-6 (solution_eps 1e-12), t_matrix_convergence 1e-6",
            "metric": "T matrices/s"}
-    for prec in ("mixed", "fp64"):
-        g = cluster(pos, 1.5, 1.6 + 0.005j, prec)
+    fx = oracle_fixture("tmatrix100")
+    for prec, tcore in (("mixed", 0), ("mixed", -1), ("fp64", 0)):
+        key = prec if (prec == "fp64" or tcore == 0) else "mixed_rotation_kernels"
+        n = len(pos)
+        g = api.SphereCluster(pos, np.full(n, 1.5), np.full(n, 1.6 + 0.005j), mie_epsilon=-C.truncation_order(1.5),
+                              precision=prec, tensor_core=tcore)
+        _lib.check(L.mstmg_set_stream(g.ctx, ctypes.c_void_p(stream.cuda_stream)), "set_stream")
         T = g.t_matrix_order()
         ms, r = timed(lambda: g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6), 3)
-        row[prec] = {"tmatrices_per_s": round(1000.0 / ms, 4), "ms": round(ms, 1), "order": r["order"], "t_matrix_order": T,
-                     "columns": 2 * r["order"] * (r["order"] + 2), "qext": r["qtot"][0], "maxiter": r["maxiter"]}
+        row[key] = {"tmatrices_per_s": round(1000.0 / ms, 4), "ms": round(ms, 1), "order": r["order"], "t_matrix_order": T,
+                    "columns": 2 * r["order"] * (r["order"] + 2), "qext": r["qtot"][0], "maxiter": r["maxiter"]}
+        if fx is not None:
+            u = r["order"]
+            nb = 2 * u * (u + 2)
+            tm = np.asfortranarray(r["tmat"][:nb, :nb])
+            ro = g.ranorientscatmatrix(tm, u)
+            row[key]["vs_oracle"] = {
+                "qext": float("%.3g" % abs(r["qtot"][0] / fx["qtot"][0] - 1)),
+                "qsca": float("%.3g" % abs(r["qtot"][2] / fx["qtot"][2] - 1)),
+                "tmat_col_norms": float("%.3g" % rel_err(np.linalg.norm(tm, axis=0), fx["col_norms"])),
+                "ranorient_smat_of_s11max": float("%.3g" % (np.abs(ro["smat"] - fx["smat"]).max() / np.abs(fx["smat"][:, 0, 0]).max())),
+                "order_used_equal": bool(u == int(fx["order_used"]))}
+        if key == "mixed":
+            # the tensor-core pass alone: its launches timed with CUDA events in one more solve
+            _lib.check(L.mstmg_set_timing(g.ctx, 1), "timing")
+            g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6)
+            tms, tn = ctypes.c_double(0), ctypes.c_int(0)
+            _lib.check(L.mstmg_kernel_time_tc(g.ctx, ctypes.byref(tms), ctypes.byref(tn)), "kernel_time_tc")
+            _lib.check(L.mstmg_set_timing(g.ctx, 0), "timing")
+            row[key]["tensor_core_passes"] = {"launches": tn.value, "ms_total": round(tms.value, 2),
+                                              "ms_per_pass": round(tms.value / max(1, tn.value), 4)}
         g.close()
     row["qext_rel_diff"] = abs(row["mixed"]["qext"] / row["fp64"]["qext"] - 1)
+    row["speedup_tensor_cores"] = round(row["mixed_rotation_kernels"]["ms"] / row["mixed"]["ms"], 2)
     out["tmatrix_cluster100"] = row
     # the 20-sphere cluster (the reference's CPU-sized case)
     w = C.workload("cluster20")
@@ -367,6 +459,13 @@ def run_extras(args, dev, stream):
     return out
 
 
+def hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
 def report_line(args, ws, R, ne):
     peaks = {}
     try:
@@ -381,7 +480,7 @@ def report_line(args, ws, R, ne):
     plain = job_value(ws, args.steps, p["ms_total"])
     # dominant kernel: the FP32 translation pass of the tuned path
     ms32, n32 = m["k32"]
-    stored32, canon64 = m["bytes32"]
+    stored32, canon32 = m["bytes32"]   # FP32 folded bytes, and the reference layout's bytes at 4 B per real
     # algorithmic bytes per launch: folded operator read once + x read + y written
     # (one column per active polarisation: the tuned path's Arnoldi passes carry
     # 2 columns while both polarisations are active; iterations count Arnoldi
@@ -411,11 +510,7 @@ def report_line(args, ws, R, ne):
         "vs_baseline": None,
         "dtype": "c64 GMRES cycles + c128 true residuals (tuned); c128 BiCG (plain)",
         "data": "synthetic: seeded PCA fractal aggregate (no dataset)",
-        "config": {"workload": "fractal aggregate, 500 touching monomers, x=2.0, m=1.6+0.05i, Df=1.8, kf=1.3, "
-                               "L=9, +z incidence, both polarisations",
-                   "neqns": ne, "pairs": 124750, "residual": "||r||/||b|| < 1e-6 (squared-norm eps 1e-12)",
-                   "parallelism": "replicas" if ws > 1 else "single GPU",
-                   "l2": "operators (2 GB FP64 / 1 GB FP32) exceed the 126 MB L2; no flush needed"},
+        "config": bench_config(ws),
         "plain_fp64": {"value": round(plain, 4), "ms_per_step": round(p["ms_per_step"], 3),
                        "iterations": p["stats"]["iterations"], "translation_gbs": round(ach64, 1) if ach64 else None,
                        "translation_frac": round(ach64 / hbm, 4) if ach64 else None},
@@ -431,11 +526,15 @@ def report_line(args, ws, R, ne):
                                        "(profiles/translate_tiled_fp32_fractal200.md), scaled by algorithmic bytes",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": alg, "launch_ms": round(dur, 4), "launches": n32,
-                     "canonical_equiv_gbs": round((canon64 / 2 + vec_bytes) / (dur * 1e-3) / 1e9, 1) if n32 else None},
+                     "canonical_equiv_gbs": round((canon32 + vec_bytes) / (dur * 1e-3) / 1e9, 1) if n32 else None},
         "e2e": {"value": round(ws * 1000.0 * args.steps / e2e["ms"], 4), "unit": "solves/s",
                 "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
         "gpu_launches": int(m["launches"]),
     }
+    if m.get("vs_oracle") or p.get("vs_oracle"):
+        line["vs_oracle"] = {"workload": WORKLOAD + " (oracle FP64, same seeded configuration, tests/golden)",
+                             "tuned": m.get("vs_oracle"), "plain_fp64": p.get("vs_oracle"),
+                             "tolerance": "plain 1e-9 relative; tuned 1e-6 on efficiencies, 1e-4 on the scattering matrix"}
     if m["clocks"]:
         line["clocks"] = m["clocks"]
     return line
@@ -444,81 +543,117 @@ def report_line(args, ws, R, ne):
 # ---------------------------------------------------------------------------
 # CPU: the oracle (restatement of the reference) on the host cores
 # ---------------------------------------------------------------------------
-def cpu_sample_solve_time(threads, iters_per_pol, sample_iters=3):
-    """Time operator generation + `sample_iters` BiCG iterations of one
-    polarisation with the oracle, and scale to the full solve (both
-    polarisations, iterations as the FP64 solve takes)."""
+def _oracle_for(name, threads, store=True):
     from mstm_b200 import configs as C
     from oracle import oracle as O
-    w = C.workload(WORKLOAD)
-    o = O.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-w["order"], store_matrix=True, nthreads=threads)
+    w = C.workload(name)
+    return O.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-w["order"], store_matrix=store, nthreads=threads)
+
+
+def cpu_full_solve(name, threads):
+    """One complete FP64 oracle solve (operator generation, both
+    polarisations to the reference's criterion, efficiencies), as the
+    reference's fixedorsoln runs it: seconds, and the iteration counts."""
+    o = _oracle_for(name, threads)
+    t0 = time.perf_counter()
+    r = o.fixedorsoln(eps=EPS, niter=NITER)
+    dt = time.perf_counter() - t0
+    o.close()
+    return dt, r["iterations"], r["status"]
+
+
+def cpu_sample_solve_time(threads, iters_total, sample_iters=3):
+    """Operator generation + `sample_iters` BiCG iterations of one
+    polarisation with the oracle, scaled to a full solve of `iters_total`
+    iterations (both polarisations)."""
+    o = _oracle_for(WORKLOAD, threads)
     f = o.planewave()
     pnp = o.multmie(np.ascontiguousarray(f[:, 0]))
     t0 = time.perf_counter()
     o.sphereinteraction(pnp, initial_run=True)   # generates and stores the operators, + one pass
     t1 = time.perf_counter()
-    x, it, err, _ = o.cbicg(pnp, pnp, niter=sample_iters, eps=0.0, initialize=False)
+    o.cbicg(pnp, pnp, niter=sample_iters, eps=0.0, initialize=False)
     t2 = time.perf_counter()
     setup = t1 - t0
     per_iter = (t2 - t1) / (sample_iters + 1.0 / 2.0)   # cbicg's initial residual is one half-width pass
-    total_iters = sum(iters_per_pol) if iters_per_pol else 2 * 60
-    total = setup + per_iter * total_iters
     o.close()
-    return total, setup, per_iter, total_iters
+    return setup + per_iter * iters_total, setup, per_iter
 
 
-def cpu_baseline_sample(iters_per_pol, threads):
+def cpu_baseline_sample(threads):
+    """The GPU arm's CPU baseline, a bounded sample: on fractal500, operator
+    generation + 3 BiCG iterations on all host threads (and + 1 iteration on
+    one thread), scaled by the iteration count of the oracle's own solve of
+    this configuration (tests/golden); beside it, complete oracle solves of
+    the 20-sphere cluster (the reference's CPU-sized case) on all threads and
+    on one."""
+    fx = oracle_fixture(WORKLOAD)
+    iters = [int(v) for v in fx["iterations"]] if fx is not None else [79, 78]
     try:
-        total, setup, per_iter, n = cpu_sample_solve_time(threads, iters_per_pol)
+        tot, setup, per_iter = cpu_sample_solve_time(threads, sum(iters))
+        tot1, setup1, per_iter1 = cpu_sample_solve_time(1, sum(iters), sample_iters=1)
+        c20, it20, _ = cpu_full_solve("cluster20", threads)
+        c20_1, _, _ = cpu_full_solve("cluster20", 1)
     except Exception as e:  # the baseline never blocks the GPU line
         return {"value": None, "unit": "solves/s", "cores": threads, "kind": "port", "sample": "failed: %s" % e}
-    return {"value": round(1.0 / total, 6), "unit": "solves/s", "cores": threads, "kind": "port",
+    return {"value": round(1.0 / tot, 6), "unit": "solves/s", "cores": threads, "kind": "port",
             "sample": "oracle (C restatement of MSTM, OpenMP over pairs, stored operators) on fractal500: operator "
-                      "generation + 3 BiCG iterations timed (%.2f s + %.2f s/iter), scaled to the %d iterations "
-                      "the FP64 solve takes" % (setup, per_iter, n)}
+                      "generation + 3 BiCG iterations timed (%.2f s + %.3f s/iteration), scaled to the %d iterations "
+                      "of the oracle's own solve (%s)" % (setup, per_iter, sum(iters), iters),
+            "one_core": {"value": round(1.0 / tot1, 7), "setup_s": round(setup1, 2), "s_per_iteration": round(per_iter1, 3)},
+            "cluster20_full_solve": {"solves_per_s": round(1.0 / c20, 3), "solves_per_s_one_core": round(1.0 / c20_1, 3),
+                                     "iterations": it20, "note": "20 spheres, x=1, both polarisations to 1e-6, complete"}}
 
 
 def run_reference(args):
+    """The reference arm: complete FP64 solves of the benchmark configuration
+    by the oracle (the C restatement of MSTM's fixedorsoln: stored operators
+    as store_translation_matrix = .true., the reference's BiCG to its own
+    criterion and its own iteration count, efficiencies) on all host
+    threads, one solve per timed step.  The warm-up steps are bounded
+    samples (operator generation + one BiCG iteration), which bring the
+    threads, pages and caches to the state the timed solves run in."""
     ws, rank, local = dist_env()
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    # iteration count of the reference's FP64 solve on this workload, from the
-    # FP64 GPU run (same iteration as cbicg), else a recorded value
-    iters = [int(v) for v in os.environ.get("MSTM_REF_ITERS", "0,0").split(",")]
-    if sum(iters) == 0:
-        iters = REF_ITERS
-    times = []
-    for k in range(args.warmup + args.steps):
-        total, setup, per_iter, n = cpu_sample_solve_time(threads, iters, sample_iters=1)
-        if k >= args.warmup:
-            times.append(total)
+    for _ in range(args.warmup):
+        cpu_sample_solve_time(threads, 0, sample_iters=1)
+    times, its = [], None
+    for _ in range(args.steps):
+        dt, its, st = cpu_full_solve(WORKLOAD, threads)
+        times.append(dt)
     mean = sum(times) / len(times)
     v = 1.0 / mean
-    line = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "solves/s", "n_gpus": 1,
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "solves/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean * 1000, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic: seeded PCA fractal aggregate",
-            "config": {"workload": "fractal aggregate, 500 touching monomers, x=2.0, m=1.6+0.05i, Df=1.8, kf=1.3, L=9",
-                       "residual": "||r||/||b|| < 1e-6"},
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic: seeded PCA fractal aggregate (no dataset)",
+            "config": bench_config(ws),
             "cpu_baseline": {"value": round(v, 6), "unit": "solves/s", "cores": threads, "kind": "port",
-                             "sample": "per step: oracle operator generation + 1 BiCG iteration on fractal500, scaled "
-                                       "to %d iterations (reference Fortran cannot be built: no Fortran compiler)" % sum(iters)},
+                             "sample": "per timed step one complete oracle solve of fractal500 (operator generation, both "
+                                       "polarisations to ||r||^2/||b||^2 < 1e-12: %s BiCG iterations, efficiencies); "
+                                       "warm-up steps: operator generation + 1 iteration; the Fortran reference cannot be "
+                                       "built here (no Fortran compiler)" % its,
+                             "solve_s": [round(t, 2) for t in times]},
             "e2e": {"value": round(v, 6), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-REF_ITERS = [79, 78]
 
 
 def run_translation_case(args):
     """Operator generation + `--translation-passes` translation passes of one
     workload, timed with CUDA events (the case the ncu captures use)."""
     from mstm_b200 import api, configs as C
-    w = C.workload(args.workload)
-    g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=-w["order"], precision=args.precision,
+    if args.workload.startswith("tmcluster"):   # the T-matrix clusters: x = 1.5, RSA at fv 0.20, seed 4
+        n = int(args.workload[len("tmcluster"):])
+        pos, _ = C.rsa_sphere(n, 1.5, 0.20, seed=4)
+        w = dict(pos=pos, radius=np.full(n, 1.5), ref_index=np.full(n, 1.6 + 0.005j), order=C.truncation_order(1.5))
+    else:
+        w = C.workload(args.workload)
+    prec = "mixed" if args.precision == "tc" else args.precision
+    g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=-w["order"], precision=prec,
                           fp32_chunk=args.fp32_chunk, tile_ctas_per_sm=args.ctas_per_sm)
     ms = g.time_translation(args.precision, args.nrhs, args.translation_passes)
-    sb, cb = g.operator_bytes(args.precision)
+    sb, cb = g.operator_bytes(prec)
     print(json.dumps({"workload": args.workload, "precision": args.precision, "nrhs": args.nrhs, "fp32_chunk": args.fp32_chunk,
                       "ctas_per_sm": args.ctas_per_sm, "ms_per_pass": ms, "operator_bytes": sb, "operator_gbs": sb / ms / 1e6}))
     g.close()
@@ -533,7 +668,7 @@ def run_tmatrix_case(args):
     n = args.tmatrix_case
     pos, _ = C.rsa_sphere(n, 1.5, 0.20, seed=4)
     g = api.SphereCluster(pos, np.full(n, 1.5), np.full(n, 1.6 + 0.005j), mie_epsilon=-C.truncation_order(1.5),
-                          precision=args.precision)
+                          precision=args.precision, tensor_core=args.tensor_core)
     T = g.t_matrix_order()
     g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6)
     L = _lib.lib()
@@ -541,8 +676,9 @@ def run_tmatrix_case(args):
     t0 = time.perf_counter()
     r = g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6)
     dt = time.perf_counter() - t0
-    print(json.dumps({"spheres": n, "precision": args.precision, "t_matrix_order": T, "order": r["order"], "s": dt,
-                      "launches": L.mstmg_kernel_launches() - l0, "maxiter": r["maxiter"], "outer": r["outer"]}))
+    print(json.dumps({"spheres": n, "precision": args.precision, "tensor_core": args.tensor_core, "t_matrix_order": T,
+                      "order": r["order"], "s": dt, "launches": L.mstmg_kernel_launches() - l0, "maxiter": r["maxiter"],
+                      "outer": r["outer"], "qext": r["qtot"][0]}))
     g.close()
 
 
@@ -557,11 +693,12 @@ def main():
     ap.add_argument("--translation-passes", type=int, default=0,
                     help="profiling case: only run this many translation passes (no solve)")
     ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "tc"])
     ap.add_argument("--fp32-chunk", type=int, default=0, help="profiling case: FP32 column chunk (2 or 4; 0 default)")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="profiling case: tiled kernel CTAs per SM (0 default)")
     ap.add_argument("--nrhs", type=int, default=4)
     ap.add_argument("--tmatrix-case", type=int, default=0, help="profiling case: one T matrix of this many spheres")
+    ap.add_argument("--tensor-core", type=int, default=0, help="profiling case: 0 tensor-core passes where they apply, -1 never")
     args = ap.parse_args()
     if args.translation_passes:
         run_translation_case(args)

@@ -328,8 +328,10 @@ int mstmg_translation_pass(mstmg_ctx *ctx, int prec, int ncols, const int *con_t
  * usable afterwards. */
 int mstmg_selftest_bounded_wait(int device, int limit, int *status);
 
-/* Time `reps` translation passes (nrhs right-hand sides, FP64 or FP32) with CUDA
- * events on the context stream; returns the average milliseconds per pass. */
+/* Time `reps` translation passes (nrhs right-hand sides, FP64 (prec 0) or
+ * FP32 (prec 1) with every second column a conjugate-transpose product, or
+ * (prec 2) plain FP32 columns on the tensor cores) with CUDA events on the
+ * context stream; returns the average milliseconds per pass. */
 int mstmg_time_translation(mstmg_ctx *ctx, int prec, int nrhs, int reps, double *ms_per_pass);
 
 /* Run this context's work on the caller's CUDA stream (a cudaStream_t; NULL

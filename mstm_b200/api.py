@@ -315,8 +315,11 @@ class SphereCluster(_Context):
         return s.value, c.value
 
     def time_translation(self, precision="fp64", nrhs=2, reps=10):
+        """Milliseconds per translation pass: "fp64", "mixed" (FP32 rotation
+        kernels) or "tc" (plain columns on the tensor cores)."""
         ms = c_double(0.0)
-        check(self._L.mstmg_time_translation(self.ctx, PRECISIONS[precision], nrhs, reps, ctypes.byref(ms)), "time")
+        prec = {"fp64": 0, "mixed": 1, "fp32": 1, "tc": 2}[precision]
+        check(self._L.mstmg_time_translation(self.ctx, prec, nrhs, reps, ctypes.byref(ms)), "time")
         return ms.value
 
 

@@ -1197,8 +1197,9 @@ static int tc_translate(mstmg_ctx* c, const zf* x, zf* y, int ncols)
     if (int rc = ensure_tc(c)) return rc;
     const TcGeom g = tc_geom(c->lmax);
     const int nmt = (ncols + TC_M - 1) / TC_M;
+    const int mtn = tc_tiles_per_cta(g, nmt);
     const void* was = c->tc_a.p;
-    CK(c->tc_a.alloc((size_t)nmt * c->n * tc_aimg_floats(g)));
+    CK(c->tc_a.alloc((size_t)((nmt + mtn - 1) / mtn * mtn) * c->n * tc_aimg_floats(g)));
     if (was != c->tc_a.p) c->layout_gen++;
     CK(cudaMemsetAsync(y, 0, sizeof(zf) * (size_t)c->neqns * ncols, c->st));
     TcPassArgs a;
@@ -2712,7 +2713,16 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     int rc = ensure_ops_both(c, true, mixed, false);
     if (rc) return rc;
     const int n = c->n, L = c->lmax, ne = c->neqns, TM = t_matrix_order;
-    const int nblkt = 2 * TM * (TM + 2), Smax = 2 * (2 * TM + 1);
+    // With the tensor-core pass serving the mixed GMRES, the columns of
+    // several consecutive orders are solved together (up to TM_GROUP columns)
+    // so that the pass's 128-column tiles fill; the orders of a group are then
+    // post-processed one by one as the reference's loop over l does
+    // (solver:141-318), and the order at which the extinction converges ends
+    // the loop there (later orders of its group are dropped unused).
+    const bool grouped = mixed && c->opts.mixed_solver == 2 && tc_eligible(c);
+    const int TM_GROUP = 256;
+    auto cols_of = [](int q) { return 2 * (2 * q + 1); };
+    const int nblkt = 2 * TM * (TM + 2), Sord = cols_of(TM), Smax = grouped ? std::max(Sord, TM_GROUP) : Sord;
     BigTablesDev bt;
     if ((rc = upload_big(c, bt))) return rc;
     double r0[3] = {0.0, 0.0, 0.0};
@@ -2731,13 +2741,13 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     DevBuf<zf> B32;
     DevBuf<int> idx;
     CK(mscr.alloc((size_t)grid * std::max(strm, strd)));
-    CK(P0.alloc((size_t)2 * TM * (TM + 2) * Smax));
-    CK(A0.alloc((size_t)2 * TM * (TM + 2) * Smax));
+    CK(P0.alloc((size_t)2 * TM * (TM + 2) * Sord));
+    CK(A0.alloc((size_t)2 * TM * (TM + 2) * Sord));
     CK(PK.alloc((size_t)ne * Smax));
     CK(B64.alloc((size_t)ne * Smax));
     CK(dT.alloc((size_t)nblkt * nblkt));
     CK(cudaMemsetAsync(dT.p, 0, sizeof(zd) * (size_t)nblkt * nblkt, c->st));
-    CK(qcol.alloc((size_t)3 * n * Smax));
+    CK(qcol.alloc((size_t)3 * n * Sord));
     CK(dsq.alloc((size_t)3 * n));
     CK(cudaMemsetAsync(dsq.p, 0, sizeof(double) * 3 * n, c->st));
     CK(qsum.alloc(3));
@@ -2762,28 +2772,32 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     const zd rimed = mk(c->opts.medium_re, c->opts.medium_im);
     int istat = 0, mit = 0, used = TM, outer_total = 0;
     double merr = 0.0, qold = 0.0, hq[3] = {0.0, 0.0, 0.0};
-    int l;
-    for (l = 1; l <= TM; l++) {
-        const int S = 2 * (2 * l + 1), nb = 2 * l * (l + 2);
-        // right-hand sides: unit TE/TM fields of order l at the origin, distributed to the spheres
-        launch_tm_rhs(l, P0.p, c->st);
-        CK(cudaMemsetAsync(PK.p, 0, sizeof(zd) * (size_t)ne * S, c->st));
-        MergeArgs md = merge_args(c, rtd, bt, r0, dtord.p);
-        md.mode = 1;
-        md.out = PK.p;
-        md.ldo = ne;
-        md.T = l;
-        md.amnp = P0.p;
-        md.ld = nb;
-        md.npol = S;
-        md.amnp0 = nullptr;
-        md.ld0 = 0;
-        md.scratch = mscr.p;
-        md.scratch_stride = strd;
-        launch_merge(md, grid, c->st);
+    bool done = false;
+    for (int la = 1; la <= TM && !done;) {
+        int lb = la, Sg = cols_of(la);
+        while (grouped && lb < TM && Sg + cols_of(lb + 1) <= TM_GROUP) Sg += cols_of(++lb);
+        // right-hand sides: unit TE/TM fields of orders la..lb at the origin,
+        // distributed to the spheres, one order after the other in the columns
+        CK(cudaMemsetAsync(PK.p, 0, sizeof(zd) * (size_t)ne * Sg, c->st));
+        for (int q = la, col0 = 0; q <= lb; col0 += cols_of(q), q++) {
+            launch_tm_rhs(q, P0.p, c->st);
+            MergeArgs md = merge_args(c, rtd, bt, r0, dtord.p);
+            md.mode = 1;
+            md.out = PK.p + (size_t)col0 * ne;
+            md.ldo = ne;
+            md.T = q;
+            md.amnp = P0.p;
+            md.ld = 2 * q * (q + 2);
+            md.npol = cols_of(q);
+            md.amnp0 = nullptr;
+            md.ld0 = 0;
+            md.scratch = mscr.p;
+            md.scratch_stride = strd;
+            launch_merge(md, grid, c->st);
+        }
         // b = Mie f, initial guess b (solver:185-187)
-        launch_m_mie(sm, c->an.p, ne, S, PK.p, B64.p, c->st);
-        CK(cudaMemcpyAsync(X, B64.p, sizeof(zd) * (size_t)ne * S, cudaMemcpyDeviceToDevice, c->st));
+        launch_m_mie(sm, c->an.p, ne, Sg, PK.p, B64.p, c->st);
+        CK(cudaMemcpyAsync(X, B64.p, sizeof(zd) * (size_t)ne * Sg, cudaMemcpyDeviceToDevice, c->st));
         CK(cudaGetLastError());
         std::vector<int> its;
         std::vector<double> errs;
@@ -2791,49 +2805,58 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
         if (mixed) {
             int oc = 0;
             if (c->opts.mixed_solver == 1)
-                rc = solve_multi_mixed(c, w64, w32, B32, rr, idx, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
+                rc = solve_multi_mixed(c, w64, w32, B32, rr, idx, Sg, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
             else if (c->opts.mixed_solver == 2)
-                rc = solve_multi_gmres(c, w64, gw, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
+                rc = solve_multi_gmres(c, w64, gw, Sg, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
             else
-                rc = solve_multi_rr(c, w64, w32, rr, idx, S, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
+                rc = solve_multi_rr(c, w64, w32, rr, idx, Sg, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
             outer_total += oc;
         } else {
-            std::vector<int> sys(S);
-            for (int s = 0; s < S; s++) sys[s] = s;
+            std::vector<int> sys(Sg);
+            for (int k = 0; k < Sg; k++) sys[k] = k;
             std::vector<double> ev(Smax, solution_eps);
             w64.S = Smax;
             rc = bicg_multi<double>(c, w64, B64.p, sys, true, max_iterations, ev, its, errs, sts);
         }
         if (rc) return rc;
-        for (int s = 0; s < S; s++) {
-            mit = std::max(mit, its[s]);
-            merr = std::max(merr, errs[s]);
-            if (its[s] > max_iterations || errs[s] > solution_eps || sts[s] == 2) istat = 1;
+        for (int q = la, col0 = 0; q <= lb; col0 += cols_of(q), q++) {
+            const int S = cols_of(q), nb = 2 * q * (q + 2);
+            for (int k = col0; k < col0 + S; k++) {
+                mit = std::max(mit, its[k]);
+                merr = std::max(merr, errs[k]);
+                if (its[k] > max_iterations || errs[k] > solution_eps || sts[k] == 2) istat = 1;
+            }
+            zd* Xq = X + (size_t)col0 * ne;
+            // per-sphere efficiencies of every column, summed
+            launch_tm_qeff(n, S, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, rimed, c->an_inv.p, Xq, PK.p + (size_t)col0 * ne,
+                           ne, qcol.p, c->st);
+            launch_tm_qsum(n, S, qcol.p, c->rad.p, c->xg, dsq.p, qsum.p, c->st);
+            // merge the solutions to the origin: T-matrix columns of order q
+            CK(cudaMemsetAsync(A0.p, 0, sizeof(zd) * (size_t)nb * S, c->st));
+            MergeArgs mm = merge_args(c, rtm, bt, r0, dtord.p);
+            mm.T = q;
+            mm.amnp = Xq;
+            mm.ld = ne;
+            mm.npol = S;
+            mm.amnp0 = A0.p;
+            mm.ld0 = nb;
+            mm.scratch = mscr.p;
+            mm.scratch_stride = strm;
+            launch_merge(mm, grid, c->st);
+            launch_tm_store(q, TM, A0.p, dT.p, c->st);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(hq, qsum.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            double converr = hq[0] - qold;
+            qold = hq[0];
+            if (convergence_eps > 0.0 && converr < convergence_eps) {
+                used = q;
+                done = true;
+                break;
+            }
         }
-        // per-sphere efficiencies of every column, summed
-        launch_tm_qeff(n, S, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, rimed, c->an_inv.p, X, PK.p, ne, qcol.p, c->st);
-        launch_tm_qsum(n, S, qcol.p, c->rad.p, c->xg, dsq.p, qsum.p, c->st);
-        // merge the solutions to the origin: T-matrix columns of order l
-        CK(cudaMemsetAsync(A0.p, 0, sizeof(zd) * (size_t)nb * S, c->st));
-        MergeArgs mm = merge_args(c, rtm, bt, r0, dtord.p);
-        mm.T = l;
-        mm.amnp = X;
-        mm.ld = ne;
-        mm.npol = S;
-        mm.amnp0 = A0.p;
-        mm.ld0 = nb;
-        mm.scratch = mscr.p;
-        mm.scratch_stride = strm;
-        launch_merge(mm, grid, c->st);
-        launch_tm_store(l, TM, A0.p, dT.p, c->st);
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(hq, qsum.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-        double converr = hq[0] - qold;
-        qold = hq[0];
-        if (convergence_eps > 0.0 && converr < convergence_eps) break;
+        la = lb + 1;
     }
-    used = l < TM ? l : TM;
     c->outer = outer_total;
     CK(copy_out(tmat, dT.p, sizeof(zd) * (size_t)nblkt * nblkt, c->st));
     if (sphere_qeff) CK(copy_out(sphere_qeff, dsq.p, sizeof(double) * 3 * n, c->st));
@@ -3435,8 +3458,12 @@ extern "C" int mstmg_translation_pass(mstmg_ctx* c, int prec, int ncols, const i
 
 extern "C" int mstmg_time_translation(mstmg_ctx* c, int prec, int nrhs, int reps, double* ms)
 {
-    if (!c || nrhs < 1 || nrhs > 256 || reps < 1) return MSTMG_ERR_ARG;
-    int rc = ensure_ops(c, prec, false);
+    if (!c || nrhs < 1 || nrhs > 256 || reps < 1 || prec < 0 || prec > 2) return MSTMG_ERR_ARG;
+    if (prec == 2 && !tc_eligible(c)) {
+        set_err("mstmg_time_translation: no tensor-core pass for this context");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    int rc = prec == 2 ? ensure_tc(c) : ensure_ops(c, prec, false);
     if (rc) return rc;
     DevBuf<zd> x64, y64;
     DevBuf<zf> x32, y32;
@@ -3452,6 +3479,7 @@ extern "C" int mstmg_time_translation(mstmg_ctx* c, int prec, int nrhs, int reps
     }
     auto pass = [&]() -> int {
         if (prec == 0) return translate_many<double>(c, x64.p, y64.p, nrhs, nrhs >= 2 ? 2u : 0u);
+        if (prec == 2) return tc_translate(c, x32.p, y32.p, nrhs);   // plain columns on the tensor cores
         return translate_many<float>(c, x32.p, y32.p, nrhs, nrhs >= 2 ? 2u : 0u);
     };
     if ((rc = pass())) return rc;

@@ -19,24 +19,24 @@
 //
 // Data layout: both operands are stored in HBM as images of the shared-memory
 // tiles the MMA reads (K-major, no swizzle: core matrices of 8 rows x 16 bytes),
-// chunk by chunk of 16 sources, so one bulk copy (cp.async.bulk) moves a
-// chunk into a pipeline stage:
+// chunk by chunk of 8 sources (one MMA K step), so one bulk copy
+// (cp.async.bulk) moves a chunk into a pipeline stage:
 //   * operator images (built once per cluster by tc_gen_kernel): per ordered
 //     pair (i <- j), mode p, chunk kc: [Hr; Hi] hi plane and lo plane, 2NP rows
-//     (targets) x 16 sources;
+//     (targets) x 8 sources;
 //   * column images (built every pass by tc_pack_kernel): per M tile, source
 //     sphere j, mode p, chunk kc: Xr hi, Xr lo, Xi hi, Xi lo, 128 rows (columns)
-//     x 16 sources.
+//     x 8 sources.
 //
 // The pass is a persistent kernel, one CTA per SM: the work is the list of
-// (target, mode, source) units, cut into equal ranges, one range per CTA
-// group (the CTAs of one group take the M tiles, so they read the same
-// operator chunks at the same time and share them through L2).  Inside a CTA,
-// warp 4 streams the chunks into a ring of stages (bulk copies + mbarriers),
-// warp 5 issues the MMAs (one thread) into one of two tensor-memory
-// accumulators, and warps 0-3 read a finished accumulator out (tcgen05.ld)
-// and add it into y with vector atomics while the next target accumulates
-// in the other.  Every wait is bounded: a wait that gives up records
+// (target, mode, source) units, cut into equal ranges, one range per CTA.  A
+// CTA carries up to two M tiles (256 columns), so every operator chunk is
+// read from HBM once per pass.  Inside a CTA, warp 4 streams the chunks into
+// a ring of stages (bulk copies + mbarriers), warp 5 issues the MMAs (one
+// thread) into the tensor-memory accumulators, and warps 0-3 read a finished
+// accumulator out (tcgen05.ld) and add it into y with vector atomics; with
+// one M tile there are two accumulators, so the next target accumulates
+// while the last one is read out.  Every wait is bounded: a wait that gives up records
 // MSTMG_ERR_CUDA and ends the CTA's work.
 #include "common.cuh"
 #include "tcpass.cuh"
@@ -136,8 +136,12 @@ __device__ __forceinline__ float tf32_rna(float v)
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
     return __uint_as_float(r);
 }
-// float offset of element (row r, source k) inside a K-major plane of 16 sources
-__host__ __device__ __forceinline__ int img_off(int r, int k) { return (r >> 3) * 128 + (k >> 2) * 32 + (r & 7) * 4 + (k & 3); }
+// float offset of element (row r, source k) inside a K-major plane of 8
+// sources: core matrices of 8 rows x 4 sources (128 bytes), the two of a row
+// group adjacent (LBO 128 bytes), row groups 256 bytes apart (SBO)
+__host__ __device__ __forceinline__ int img_off(int r, int k) { return (r >> 3) * 64 + (k >> 2) * 32 + (r & 7) * 4 + (k & 3); }
+#define TC_LBO 128u
+#define TC_SBO 256u
 
 // unit u of the flat list (target i, mode p, entry e): i-major, then p, then e
 struct UnitIt {
@@ -188,7 +192,7 @@ __global__ void __launch_bounds__(128) tc_gen_kernel(TcGenArgs a)
     double xp[3] = {a.pos[3 * i] - a.pos[3 * j], a.pos[3 * i + 1] - a.pos[3 * j + 1], a.pos[3 * i + 2] - a.pos[3 * j + 2]};
     gt_prepare(gs, a.g, xp, 3, mk(a.rimed_re, a.rimed_im), 2 * G.L);
     float* base = a.himg + (size_t)q * tc_himg_floats(G);
-    const int plane = 2 * G.NP * 16;
+    const int plane = 2 * G.NP * TC_KC;
     for (int el = threadIdx.x; el < G.nb * G.nb; el += blockDim.x) {
         const int t = el / G.nb, s = el - t * G.nb;   // target row, source column
         int m, n, k, l;
@@ -196,7 +200,7 @@ __global__ void __launch_bounds__(128) tc_gen_kernel(TcGenArgs a)
         gt_mn(t, G.L, k, l);
         zd e[2];
         gt_element(gs, a.g, 3, 2 * G.L, n, m, l, k, e[0], e[1]);
-        const int kc = s >> 4, kk = s & 15;
+        const int kc = s / TC_KC, kk = s % TC_KC;
 #pragma unroll
         for (int p = 0; p < 2; p++) {
             float* img = base + ((size_t)p * G.NKC + kc) * 2 * plane;
@@ -224,7 +228,7 @@ void launch_tc_gen(const TcGenArgs& a, cudaStream_t st)
 // column images: one CTA per (M tile, sphere, mode, chunk), a thread per
 // (row, group of 4 sources)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) tc_pack_kernel(TcPassArgs a)
+__global__ void __launch_bounds__(256) tc_pack_kernel(TcPassArgs a)
 {
     const TcGeom G = a.geo;
     int b = blockIdx.x;
@@ -233,13 +237,13 @@ __global__ void __launch_bounds__(512) tc_pack_kernel(TcPassArgs a)
     const int p = b & 1;
     b >>= 1;
     const int j = b % a.nsph, mt = b / a.nsph;
-    const int r = threadIdx.x >> 2, k4 = threadIdx.x & 3;
+    const int r = threadIdx.x >> 1, k4 = threadIdx.x & 1;
     const int c = mt * TC_M + r;
     float4 v[4];
     float* pv = reinterpret_cast<float*>(v);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        const int s = kc * 16 + k4 * 4 + q;
+        const int s = kc * TC_KC + k4 * 4 + q;
         zf x = mk(0.f, 0.f);
         if (c < a.ncols && s < G.nb) x = a.x[(size_t)c * a.ld + (size_t)j * 2 * G.nb + (size_t)p * G.nb + s];
         const float rh = tf32_rna(x.x), ih = tf32_rna(x.y);
@@ -248,25 +252,31 @@ __global__ void __launch_bounds__(512) tc_pack_kernel(TcPassArgs a)
         pv[2 * 4 + q] = ih;
         pv[3 * 4 + q] = tf32_rna(x.y - ih);
     }
-    float* base = a.aimg + ((((size_t)mt * a.nsph + j) * 2 + p) * G.NKC + kc) * (4 * TC_M * 16);
+    float* base = a.aimg + ((((size_t)mt * a.nsph + j) * 2 + p) * G.NKC + kc) * (4 * TC_M * TC_KC);
     const int o = img_off(r, k4 * 4);
 #pragma unroll
-    for (int pl = 0; pl < 4; pl++) *reinterpret_cast<float4*>(base + pl * (TC_M * 16) + o) = v[pl];
+    for (int pl = 0; pl < 4; pl++) *reinterpret_cast<float4*>(base + pl * (TC_M * TC_KC) + o) = v[pl];
 }
 
 // ---------------------------------------------------------------------------
 // the pass
 // ---------------------------------------------------------------------------
-#define TC_SA (4 * TC_M * 16 * 4)   // bytes of a stage's column images
-#define TC_MAXST 6
+#define TC_SA (4 * TC_M * TC_KC * 4)   // bytes of one M tile's column images in a stage
+#define TC_MAXST 8
 
+template <int MTN>
 __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstage, long long nunit, int ngroup)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     const TcGeom G = a.geo;
     const int NP = G.NP, NKC = G.NKC;
-    const uint32_t SB = 2u * 2u * NP * 16u * 4u;   // bytes of a stage's operator images (hi, lo)
-    const uint32_t STG = TC_SA + SB;
+    const uint32_t SB = 2u * 2u * NP * TC_KC * 4u;   // bytes of a stage's operator images (hi, lo)
+    const uint32_t SA = MTN * TC_SA;
+    const uint32_t STG = SA + SB;
+    // tensor memory: per segment MTN accumulators of 2NP columns ([Yr | Yi]);
+    // two segments' worth (double buffering) when they fit in 256 columns
+    const int RS = MTN * 2 * NP;
+    const int nbuf = RS <= 256 ? 2 : 1;
     const uint32_t sbase = su32(sm);
     auto bar_full = [&](int s) { return sbase + 8u * s; };
     auto bar_empty = [&](int s) { return sbase + 8u * (TC_MAXST + s); };
@@ -300,7 +310,9 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
     tc_fence_after();
     const uint32_t tbase = *tmem_holder;
 
-    const int mt = blockIdx.x % a.nmt, grp = blockIdx.x / a.nmt;
+    const int ntp = (a.nmt + MTN - 1) / MTN;
+    const int tp = blockIdx.x % ntp, grp = blockIdx.x / ntp;
+    const int mt0 = tp * MTN;
     const long long u0 = nunit * grp / ngroup, u1 = nunit * (grp + 1) / ngroup;
 
     if (u0 < u1) {
@@ -322,8 +334,12 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
                         }
                         const uint32_t dst = stage0 + (uint32_t)s * STG;
                         mb_expect(bar_full(s), STG);
-                        bulk_g2s(dst, a.aimg + ((((size_t)mt * a.nsph + j) * 2 + it.p) * NKC + kc) * (4 * TC_M * 16), TC_SA, bar_full(s));
-                        bulk_g2s(dst + TC_SA, a.himg + (((size_t)it.e * 2 + it.p) * NKC + kc) * (2 * 2 * NP * 16), SB, bar_full(s));
+#pragma unroll
+                        for (int t = 0; t < MTN; t++)
+                            bulk_g2s(dst + t * TC_SA,
+                                     a.aimg + ((((size_t)(mt0 + t) * a.nsph + j) * 2 + it.p) * NKC + kc) * (4 * TC_M * TC_KC), TC_SA,
+                                     bar_full(s));
+                        bulk_g2s(dst + SA, a.himg + (((size_t)it.e * 2 + it.p) * NKC + kc) * (2 * 2 * NP * TC_KC), SB, bar_full(s));
                     }
                     if (u + 1 < u1) unit_next(a.rstart, it);
                 }
@@ -332,21 +348,21 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
             // ---- MMA issuer ----
             if (lane == 0) {
                 const uint32_t id2 = idesc_tf32(2 * NP, 0), id1 = idesc_tf32(NP, 0), id1n = idesc_tf32(NP, 1);
-                const uint32_t hoff = (uint32_t)NP * 64u;   // the Hi half of an operator plane
+                const uint32_t hoff = (uint32_t)(NP / 8) * TC_SBO;   // the Hi half of an operator plane
                 UnitIt it = unit_at(a.rstart, a.nsph, u0);
                 long long q = 0;
                 int seg = 0;
                 bool first = true, ok = true;
                 for (long long u = u0; u < u1 && ok; u++) {
-                    const int b = seg & 1;
+                    const int b = seg % nbuf;
                     if (first) {
-                        if (!mb_wait(bar_tempty(b), (uint32_t)(((seg >> 1) & 1) ^ 1), abort)) {
+                        if (!mb_wait(bar_tempty(b), (uint32_t)(((seg / nbuf) & 1) ^ 1), abort)) {
                             ok = false;
                             break;
                         }
                         tc_fence_after();
                     }
-                    const uint32_t d0 = tbase + (uint32_t)b * 256u, dy = d0 + (uint32_t)NP;
+                    const uint32_t dbuf = tbase + (uint32_t)b * 256u;
                     for (int kc = 0; kc < NKC; kc++, q++) {
                         const int s = (int)(q % nstage);
                         if (!mb_wait(bar_full(s), (uint32_t)((q / nstage) & 1), abort)) {
@@ -355,21 +371,23 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
                         }
                         tc_fence_after();
                         const uint32_t st = stage0 + (uint32_t)s * STG;
-                        const uint32_t arh = st, arl = st + 8192u, aih = st + 16384u, ail = st + 24576u;
-                        const uint32_t bh = st + TC_SA, bl = bh + SB / 2u;
+                        const uint32_t bh = st + SA, bl = bh + SB / 2u;
+                        const uint32_t acc = (first && kc == 0) ? 0u : 1u;
 #pragma unroll
-                        for (int ks = 0; ks < 2; ks++) {
-                            const uint32_t ko = 256u * ks;
-                            const uint32_t acc = (first && kc == 0 && ks == 0) ? 0u : 1u;
-                            mma_tf32(d0, sdesc(arh + ko, 128, 512), sdesc(bh + ko, 128, 512), id2, acc);
-                            mma_tf32(d0, sdesc(arh + ko, 128, 512), sdesc(bl + ko, 128, 512), id2, 1u);
-                            mma_tf32(d0, sdesc(arl + ko, 128, 512), sdesc(bh + ko, 128, 512), id2, 1u);
-                            mma_tf32(d0, sdesc(aih + ko, 128, 512), sdesc(bh + hoff + ko, 128, 512), id1n, 1u);
-                            mma_tf32(d0, sdesc(aih + ko, 128, 512), sdesc(bl + hoff + ko, 128, 512), id1n, 1u);
-                            mma_tf32(d0, sdesc(ail + ko, 128, 512), sdesc(bh + hoff + ko, 128, 512), id1n, 1u);
-                            mma_tf32(dy, sdesc(aih + ko, 128, 512), sdesc(bh + ko, 128, 512), id1, 1u);
-                            mma_tf32(dy, sdesc(aih + ko, 128, 512), sdesc(bl + ko, 128, 512), id1, 1u);
-                            mma_tf32(dy, sdesc(ail + ko, 128, 512), sdesc(bh + ko, 128, 512), id1, 1u);
+                        for (int t = 0; t < MTN; t++) {
+                            const uint32_t d0 = dbuf + (uint32_t)(t * 2 * NP), dy = d0 + (uint32_t)NP;
+                            const uint32_t at = st + t * TC_SA;
+                            const uint32_t arh = at, arl = at + 1u * TC_M * TC_KC * 4u, aih = at + 2u * TC_M * TC_KC * 4u,
+                                           ail = at + 3u * TC_M * TC_KC * 4u;
+                            mma_tf32(d0, sdesc(arh, TC_LBO, TC_SBO), sdesc(bh, TC_LBO, TC_SBO), id2, acc);
+                            mma_tf32(d0, sdesc(arh, TC_LBO, TC_SBO), sdesc(bl, TC_LBO, TC_SBO), id2, 1u);
+                            mma_tf32(d0, sdesc(arl, TC_LBO, TC_SBO), sdesc(bh, TC_LBO, TC_SBO), id2, 1u);
+                            mma_tf32(d0, sdesc(aih, TC_LBO, TC_SBO), sdesc(bh + hoff, TC_LBO, TC_SBO), id1n, 1u);
+                            mma_tf32(d0, sdesc(aih, TC_LBO, TC_SBO), sdesc(bl + hoff, TC_LBO, TC_SBO), id1n, 1u);
+                            mma_tf32(d0, sdesc(ail, TC_LBO, TC_SBO), sdesc(bh + hoff, TC_LBO, TC_SBO), id1n, 1u);
+                            mma_tf32(dy, sdesc(aih, TC_LBO, TC_SBO), sdesc(bh, TC_LBO, TC_SBO), id1, 1u);
+                            mma_tf32(dy, sdesc(aih, TC_LBO, TC_SBO), sdesc(bl, TC_LBO, TC_SBO), id1, 1u);
+                            mma_tf32(dy, sdesc(ail, TC_LBO, TC_SBO), sdesc(bh, TC_LBO, TC_SBO), id1, 1u);
                         }
                         mma_commit(bar_empty(s));   // the stage is free once these MMAs are done
                     }
@@ -399,7 +417,6 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
         } else {
             // ---- epilogue: warps 0-3, accumulator rows 32 w .. 32 w + 31 ----
             const int row = warp * 32 + lane;
-            const int c = mt * TC_M + row;
             UnitIt it = unit_at(a.rstart, a.nsph, u0);
             int seg = 0;
             for (long long u = u0; u < u1; u++) {
@@ -410,23 +427,27 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
                     last = (nx.i != it.i || nx.p != it.p);
                 }
                 if (last) {
-                    const int b = seg & 1;
-                    if (!mb_wait(bar_tfull(b), (uint32_t)((seg >> 1) & 1), abort)) {
+                    const int b = seg % nbuf;
+                    if (!mb_wait(bar_tfull(b), (uint32_t)((seg / nbuf) & 1), abort)) {
                         atomicExch(a.err, MSTMG_ERR_CUDA);
                         *abort = 1;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t tr = tbase + (uint32_t)b * 256u + ((uint32_t)(warp * 32) << 16);
-                    zf* yo = a.y + (size_t)c * a.ld + (size_t)it.i * 2 * G.nb + (size_t)it.p * G.nb;
-                    for (int t0 = 0; t0 < NP; t0 += 16) {
-                        float vr[16], vi[16];
-                        tmem_ld16(tr + (uint32_t)t0, vr);
-                        tmem_ld16(tr + (uint32_t)(NP + t0), vi);
-                        if (c < a.ncols) {
 #pragma unroll
-                            for (int k = 0; k < 16; k++)
-                                if (t0 + k < G.nb) atomicAdd(reinterpret_cast<float2*>(yo + t0 + k), make_float2(vr[k], vi[k]));
+                    for (int t = 0; t < MTN; t++) {
+                        const int c = (mt0 + t) * TC_M + row;
+                        const uint32_t tr = tbase + (uint32_t)b * 256u + (uint32_t)(t * 2 * NP) + ((uint32_t)(warp * 32) << 16);
+                        zf* yo = a.y + (size_t)c * a.ld + (size_t)it.i * 2 * G.nb + (size_t)it.p * G.nb;
+                        for (int t0 = 0; t0 < NP; t0 += 16) {
+                            float vr[16], vi[16];
+                            tmem_ld16(tr + (uint32_t)t0, vr);
+                            tmem_ld16(tr + (uint32_t)(NP + t0), vi);
+                            if (c < a.ncols) {
+#pragma unroll
+                                for (int k = 0; k < 16; k++)
+                                    if (t0 + k < G.nb) atomicAdd(reinterpret_cast<float2*>(yo + t0 + k), make_float2(vr[k], vi[k]));
+                            }
                         }
                     }
                     tc_fence_before();
@@ -444,24 +465,32 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
     if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(512));
 }
 
-int launch_tc_pass(const TcPassArgs& a, int nsm, cudaStream_t st)
+template <int MTN> static int launch_pass(const TcPassArgs& a, int nsm, cudaStream_t st)
 {
     const TcGeom& G = a.geo;
-    if (G.NP > 128 || G.NP < 16 || a.nmt < 1 || a.nent < 1) return -1;
-    // column images of this pass
-    tc_pack_kernel<<<(unsigned)(a.nmt * a.nsph * 2 * G.NKC), 512, 0, st>>>(a);
-    launch_counter() += 1;
-    const size_t stg = TC_SA + (size_t)2 * 2 * G.NP * 16 * 4;
+    const size_t stg = (size_t)MTN * TC_SA + (size_t)2 * 2 * G.NP * TC_KC * 4;
     int nstage = (int)((220 * 1024 - 1024) / stg);
     if (nstage > TC_MAXST) nstage = TC_MAXST;
     if (nstage < 2) return -1;
     const size_t smem = 1024 + (size_t)nstage * stg;
-    cudaFuncSetAttribute(tc_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(tc_pass_kernel<MTN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const long long nunit = 2LL * a.nent;
-    int ngroup = nsm / a.nmt;
+    const int ntp = (a.nmt + MTN - 1) / MTN;
+    int ngroup = nsm / ntp;
     if (ngroup < 1) ngroup = 1;
     if (ngroup > nunit) ngroup = (int)nunit;
-    tc_pass_kernel<<<(unsigned)(ngroup * a.nmt), 192, smem, st>>>(a, nstage, nunit, ngroup);
+    tc_pass_kernel<MTN><<<(unsigned)(ngroup * ntp), 192, smem, st>>>(a, nstage, nunit, ngroup);
     launch_counter() += 1;
     return 0;
+}
+
+int launch_tc_pass(const TcPassArgs& a, int nsm, cudaStream_t st)
+{
+    const TcGeom& G = a.geo;
+    if (G.NP > 128 || G.NP < 16 || a.nmt < 1 || a.nent < 1) return -1;
+    const int mtn = tc_tiles_per_cta(G, a.nmt);
+    const int ntile = (a.nmt + mtn - 1) / mtn * mtn;   // column images of every tile the CTAs read
+    tc_pack_kernel<<<(unsigned)(ntile * a.nsph * 2 * G.NKC), 256, 0, st>>>(a);
+    launch_counter() += 1;
+    return mtn == 2 ? launch_pass<2>(a, nsm, st) : launch_pass<1>(a, nsm, st);
 }
