@@ -376,7 +376,7 @@ def run_extras(args, dev, stream):
                               precision=prec, tensor_core=tcore)
         _lib.check(L.mstmg_set_stream(g.ctx, ctypes.c_void_p(stream.cuda_stream)), "set_stream")
         T = g.t_matrix_order()
-        ms, r = timed(lambda: g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6), 3)
+        ms, r = timed(lambda: g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6), 1 if prec == "fp64" else 3)
         row[key] = {"tmatrices_per_s": round(1000.0 / ms, 4), "ms": round(ms, 1), "order": r["order"], "t_matrix_order": T,
                     "columns": 2 * r["order"] * (r["order"] + 2), "qext": r["qtot"][0], "maxiter": r["maxiter"]}
         if fx is not None:
@@ -419,12 +419,40 @@ def run_extras(args, dev, stream):
     ws["workload"] = ("held-out configurations of 100-300 spheres, x in [0.5, 2], m random, fv in [0.05, 0.3], "
                       "+z incidence, mixed precision to 1e-6 residual; network trained here on solver outputs")
     out["warm_start"] = ws
-    # batched ensemble of T matrices (uneven sizes), concurrent and autotuned, against one at a time
+    # the orientation-averaged ensemble: configurations of 50-400 spheres
+    # (x = 1.5, seed 4), each a cluster T matrix (tensor-core passes) and its
+    # random-orientation averages; 8 of the 256 configurations, every 32nd by
+    # size, so the sample spans the size range
     from mstm_b200 import ensemble as EN
-    cfgs = EN.ensemble_configs(6, seed=4, nmin=50, nmax=150)
-    seq = EN.solve_ensemble(cfgs, precision="mixed", workers=1, solution_eps=1e-12)
+    cfgs = EN.ensemble_configs(256, seed=4, nmin=50, nmax=400)
+    by_size = sorted(range(len(cfgs)), key=lambda k: (cfgs[k]["n"], k))
+    subset = [cfgs[k] for k in by_size[16::32]]
+    EN.solve_one(cfgs[by_size[0]], "mixed", solution_eps=1e-12)   # warm-up (module load, first allocations)
+    torch.cuda.synchronize(dev)
     tuner = EN.Autotuner(reps=2)
-    bat = EN.solve_ensemble(cfgs, precision="mixed", workers=4, tuner=tuner, solution_eps=1e-12)
+    ens = EN.solve_ensemble(subset, precision="mixed", workers=1, tuner=tuner, solution_eps=1e-12)
+    s11 = ens["smat"][:, 0, 0]
+    row = {"workload": "orientation-averaged ensemble: 256 seeded configurations of 50-400 spheres (uniform), x=1.5, "
+                       "m=1.6+0.005i, RSA in a sphere at fv 0.20; timed here: 8 of them, every 32nd by size (%s spheres); "
+                       "per configuration the cluster T matrix to residual 1e-6 (tensor-core passes) and its random-orientation "
+                       "Qext/Qsca and scattering matrix" % [c["n"] for c in subset],
+           "metric": "T matrices/s (wall clock, one after the other)",
+           "tmatrices_per_s": round(ens["tmatrices_per_s"], 4), "wall_s": round(ens["wall_s"], 2),
+           "orders": [r["order"] for r in ens["per_config"]], "qext_mean": ens["qext"], "qsca_mean": ens["qsca"],
+           "s11_mean_every_10deg": [float("%.6g" % v) for v in s11[::10]], "tuning_s": round(ens["tune_s"], 2),
+           "autotuner_chose": [dict(size=l["key"][0], best=l["best"], ms=round(l["best_ms"], 3)) for l in tuner.log]}
+    errs = {}
+    for k in by_size[:2]:   # the two smallest configurations against the oracle's frozen T matrices
+        fx = oracle_fixture("ensemble_tmatrix_c%d" % k)
+        if fx is None:
+            continue
+        r = EN.solve_one(cfgs[k], "mixed", solution_eps=1e-12)
+        errs["c%d" % k] = {"n": cfgs[k]["n"], "qext": float("%.3g" % abs(r["qtot"][0] / fx["qtot"][0] - 1)),
+                           "qsca": float("%.3g" % abs(r["qtot"][2] / fx["qtot"][2] - 1)),
+                           "smat_of_s11max": float("%.3g" % (np.abs(r["smat"] - fx["smat"]).max() / np.abs(fx["smat"][:, 0, 0]).max())),
+                           "order_used_equal": bool(r["order"] == int(fx["order_used"]))}
+    row["vs_oracle"] = errs
+    out["ensemble_tmatrix_cfg4"] = row
     # many small fixed-orientation configurations: one at a time against four streams
     rng = np.random.default_rng(11)
     small = [C.rsa_sphere(int(rng.integers(15, 41)), 1.0, 0.10, seed=300 + k)[0] for k in range(48)]
@@ -448,14 +476,6 @@ def run_extras(args, dev, stream):
         "one_ensemble_context": round(fb["solves_per_s"], 1),
         "qext_rel_diff": abs(f4["qext_mean"] / f1["qext_mean"] - 1),
         "qext_rel_diff_one_context": abs(fb["qext_mean"] / f1["qext_mean"] - 1)}
-    out["ensemble_tmatrix"] = {
-        "workload": "6 configurations, 50-150 spheres (seeded), x=1.5, m=1.6+0.005i, RSA at fv 0.20: cluster T matrices, "
-                    "orientation-averaged Qext/Qsca and scattering matrix, ensemble means",
-        "metric": "T matrices/s (mixed precision)",
-        "one_at_a_time": round(seq["tmatrices_per_s"], 4), "batched_autotuned": round(bat["tmatrices_per_s"], 4),
-        "tuning_s": round(bat["tune_s"], 2), "qext_mean": bat["qext"], "qsca_mean": bat["qsca"],
-        "chosen": [dict(size=l["key"][0], order=l["key"][1], best=l["best"], ms=round(l["best_ms"], 3)) for l in tuner.log],
-    }
     return out
 
 

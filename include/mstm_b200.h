@@ -306,6 +306,13 @@ int mstmg_nn_knn(int n, int k, const int *cfg_start, const int *sphere_cfg, cons
  * FP64 and FP32 operator passes. */
 int mstmg_last_stats(const mstmg_ctx *ctx, int *iters2, int *outer, int *passes64, int *passes32);
 
+/* Host synchronisations of the last mixed GMRES solve on the context.  The
+ * two-column solves (a fixed orientation, an ensemble) run each restart
+ * cycle as one CUDA graph whose Arnoldi step repeats on the device under a
+ * conditional WHILE node, so they synchronise once per cycle (the FP64 true
+ * residual that starts it) and once at the end. */
+int mstmg_last_host_syncs(const mstmg_ctx *ctx);
+
 /* Bytes of one FP64 (prec=0) or FP32 (prec=1) operator pass, and the
  * reference's canonical per-pass operator bytes (translation_data layout). */
 int mstmg_operator_bytes(const mstmg_ctx *ctx, int prec, double *stored_bytes, double *canonical_bytes);

@@ -86,7 +86,8 @@ class _Context:
         outer, p64, p32 = c_int(0), c_int(0), c_int(0)
         check(self._L.mstmg_last_stats(self.ctx, _ptr(it), ctypes.byref(outer), ctypes.byref(p64), ctypes.byref(p32)),
               "stats")
-        return dict(iterations=it.tolist(), outer=outer.value, passes64=p64.value, passes32=p32.value)
+        return dict(iterations=it.tolist(), outer=outer.value, passes64=p64.value, passes32=p32.value,
+                    host_syncs=self._L.mstmg_last_host_syncs(self.ctx))
 
 class SphereCluster(_Context):
     """One cluster of external spheres in a medium (free space by default).

@@ -174,10 +174,26 @@ struct GmresWork {
     std::map<long long, StepGraph> graphs;
     unsigned long long graph_gen = ~0ull;   // the context's layout generation the graphs were captured at
     bool graphs_ok = true;                  // false once a capture failed: plain launches from then on
+    // Arnoldi cycles driven on the device (two-column solves): the state of
+    // the rotations in device memory and one graph per active-system count,
+    // the step under a conditional WHILE node (mrhs.cu, gm_givens_kernel)
+    DevBuf<int> dj, djmax, dalive, dkk, dstatus, dkmax;
+    DevBuf<double> dtarget, dcs;
+    DevBuf<double2> dsn, dg, dRm;
+    int* hkk = nullptr;   // pinned: kk, status of every system and the steps of the last device cycle
+    struct CycleGraph {
+        cudaGraphExec_t exec;
+        long long launches_per_step;
+        int passes32_per_step;
+    };
+    std::map<int, CycleGraph> cycles;
+    GmDevState dev() { return GmDevState{dj.p, djmax.p, dalive.p, dkk.p, dstatus.p, dtarget.p, dcs.p, dsn.p, dg.p, dRm.p}; }
     void drop_graphs()
     {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
         graphs.clear();
+        for (auto& kv : cycles) cudaGraphExecDestroy(kv.second.exec);
+        cycles.clear();
     }
     GmresWork() = default;
     GmresWork(const GmresWork&) = delete;
@@ -186,6 +202,7 @@ struct GmresWork {
     {
         drop_graphs();
         if (hh) cudaFreeHost(hh);
+        if (hkk) cudaFreeHost(hkk);
     }
     size_t off1() const { return (size_t)(S + (S & 1)); }
     size_t hpass() const { return (size_t)(m + 1) * S * 2; }
@@ -232,6 +249,21 @@ struct GmresWork {
         if (hh) cudaFreeHost(hh);
         hh = nullptr;
         CK(cudaMallocHost((void**)&hh, sizeof(double) * (off1() + hpass())));
+        dRm.release();
+        CK(dj.alloc(1));
+        CK(djmax.alloc(1));
+        CK(dkmax.alloc(1));
+        CK(dalive.alloc(S));
+        CK(dkk.alloc(S));
+        CK(dstatus.alloc(S));
+        CK(dtarget.alloc(S));
+        CK(dcs.alloc((size_t)S * m));
+        CK(dsn.alloc((size_t)S * m));
+        CK(dg.alloc((size_t)S * (m + 1)));
+        CK(dRm.alloc((size_t)S * m * (m + 1)));
+        if (hkk) cudaFreeHost(hkk);
+        hkk = nullptr;
+        CK(cudaMallocHost((void**)&hkk, sizeof(int) * (2 * (size_t)S + 1)));
         Rm.assign((size_t)S * m * (m + 1), 0.0);
         g.assign((size_t)S * (m + 1), 0.0);
         sn.assign((size_t)S * m, 0.0);
@@ -303,6 +335,7 @@ struct mstmg_ctx {
     BicgScalars* h_sc = nullptr;
     double* h_small = nullptr;
     int iters[2] = {0, 0}, outer = 0, passes64 = 0, passes32 = 0;
+    int host_syncs = 0;   // host synchronisations of the last mixed GMRES solve
     std::vector<int> tord;   // translation order of each sphere to the cluster origin (mstmg_t_matrix_order)
     std::unique_ptr<FftState> fft;   // set by mstmg_fft_setup
     // pairs below translation_switch_order: dense gentranmatrix records (densepair.cu)
@@ -1629,7 +1662,7 @@ struct EnsSeg {
 };
 static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S, const zd* B, zd* X, double eps, int niter,
                              std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count,
-                             const EnsSeg* seg = nullptr);
+                             const EnsSeg* seg = nullptr, bool x_zero = false);
 
 
 static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int dir, double eps, int niter, const double* x0, double fallback,
@@ -1852,6 +1885,8 @@ extern "C" int mstmg_ensemble_fixed_orientation(mstmg_ctx* c, double alpha, doub
     if (rc) return rc;
     return istat;
 }
+
+extern "C" int mstmg_last_host_syncs(const mstmg_ctx* c) { return c ? c->host_syncs : -1; }
 
 extern "C" int mstmg_last_stats(const mstmg_ctx* c, int* iters2, int* outer, int* passes64, int* passes32)
 {
@@ -2458,12 +2493,15 @@ static int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>
 // columns with the active systems' basis vectors in their segments (the
 // operator has no pairs between configurations), and each system keeps its
 // own basis, Hessenberg matrix and stopping test.
+// x_zero: X holds zeros on entry, so the first cycle's true residual is B
+// itself and needs no FP64 pass.
 static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S, const zd* B, zd* X, double eps, int niter,
                              std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count,
-                             const EnsSeg* seg)
+                             const EnsSeg* seg, bool x_zero)
 {
     using C = std::complex<double>;
     NvtxRange nvtx_("mixed GMRES");
+    c->host_syncs = 0;
     const int ne = c->neqns, m = gw.m, m1 = gw.m + 1;
     const int ldv = seg ? seg->ldv : ne;             // elements a basis vector is stored in
     const int* slen = seg ? seg->len : nullptr;      // elements a system's vectors hold
@@ -2492,6 +2530,22 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
     int rc;
     auto rot = [&](int s) { return (size_t)s * m; };
     auto colR = [&](int s, int j) { return &gw.Rm[((size_t)s * m + j) * m1]; };
+    // a device-driven cycle leaves its step counts in gw.hkk (pinned), read
+    // after the next synchronisation
+    std::vector<int> dev_act;
+    long long dev_per_step = 0;
+    int dev_passes_per_step = 0;
+    auto fold_device_cycle = [&]() {
+        if (dev_act.empty()) return;
+        for (int s : dev_act) {
+            steps[s] += gw.hkk[s];
+            if (gw.hkk[S + s] == 2) status[s] = 2;
+        }
+        const int nstep = gw.hkk[2 * S];
+        launch_counter() += (long long)nstep * dev_per_step;
+        c->passes32 += nstep * dev_passes_per_step;
+        dev_act.clear();
+    };
     for (int cyc = 0; cyc <= c->opts.max_outer && !act.empty(); cyc++) {
         // FP64 true residuals of the cycle's systems into R (FP32, by system,
         // or the two columns of an ensemble)
@@ -2504,14 +2558,21 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
         } else {
             const int apad = a == 1 ? 1 : ((a + 1) / 2) * 2;
             CK(cudaMemcpyAsync(w64.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
-            launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
-            if ((rc = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u))) return rc;
+            if (x_zero && cyc == 0) {
+                // H 0 = 0: the residual is B
+                CK(cudaMemsetAsync(w64.YP.p, 0, sizeof(zd) * (size_t)ne * apad, c->st));
+            } else {
+                launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
+                if ((rc = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u))) return rc;
+            }
             launch_m_resid<float>(sm, c->an.p, ne, a, w64.act.p, B, X, w64.YP.p, gw.R.p, w64.part.p, gw.rr.p, c->nsm, c->st, 1);
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(hrr.data(), gw.rr.p, sizeof(double) * 2 * S, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
+        c->host_syncs++;
         (*outer_count)++;
+        fold_device_cycle();
         std::vector<int> keep;
         for (int s : act) {
             const double bb = hrr[2 * s + 1];
@@ -2537,6 +2598,110 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
         }
         cur = act;
         const int jmax = (int)std::min<long long>(m, room);
+        if (graphs && jmax > 0) {
+            // the whole cycle on the device: one graph launch, its Arnoldi
+            // step repeated under a conditional WHILE node until every system
+            // has left or jmax steps are done; then the least-squares
+            // solutions and the corrections, with no synchronisation
+            const int na = a;
+            std::vector<int> alive(S, 0);
+            std::vector<double2> g0((size_t)S * m1, make_double2(0.0, 0.0));
+            for (int s : act) {
+                alive[s] = 1;
+                g0[(size_t)s * m1] = make_double2(std::sqrt(hrr[2 * s]), 0.0);
+            }
+            const int zero = 0;
+            CK(cudaMemcpyAsync(gw.dalive.p, alive.data(), sizeof(int) * S, cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(gw.dg.p, g0.data(), sizeof(double2) * g0.size(), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(gw.dtarget.p, gw.target.data(), sizeof(double) * S, cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(gw.dj.p, &zero, sizeof(int), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(gw.djmax.p, &jmax, sizeof(int), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemsetAsync(gw.dkk.p, 0, sizeof(int) * S, c->st));
+            CK(cudaMemsetAsync(gw.dstatus.p, 0, sizeof(int) * S, c->st));
+            auto it = gw.cycles.find(na);
+            if (it == gw.cycles.end()) {
+                cudaGraph_t gr = nullptr, body = nullptr;
+                cudaGraphExec_t ex = nullptr;
+                cudaGraphConditionalHandle hc;
+                bool ok = cudaGraphCreate(&gr, 0) == cudaSuccess && cudaGraphConditionalHandleCreate(&hc, gr, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+                cudaGraphNodeParams np = {};
+                cudaGraphNode_t node;
+                if (ok) {
+                    np.type = cudaGraphNodeTypeConditional;
+                    np.conditional.handle = hc;
+                    np.conditional.type = cudaGraphCondTypeWhile;
+                    np.conditional.size = 1;
+                    ok = cudaGraphAddNode(&node, gr, nullptr, 0, &np) == cudaSuccess;
+                }
+                if (ok) body = np.conditional.phGraph_out[0];
+                const long long l0 = launch_counter().load();
+                const int p0 = c->passes32;
+                int src = MSTMG_ERR_CUDA;
+                if (ok) ok = cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    src = [&]() -> int {
+                        GmDevState d = gw.dev();
+                        if (seg) {
+                            CK(cudaMemsetAsync(gw.XP.p, 0, sizeof(zf) * 2 * (size_t)ne, c->st));
+                            launch_eg_gather_dev(ne, ldv, m1, na, gw.act.p, seg->off, seg->len, d.j, d.alive, gw.V.p, gw.XP.p, c->nsm, c->st);
+                            int r2 = translate_many<float>(c, gw.XP.p, gw.Y.p, 2, 0u);
+                            if (r2) return r2;
+                            launch_eg_apply(sm, an32, ne, ldv, na, gw.act.p, seg->off, seg->len, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+                        } else {
+                            launch_gm_gather_dev(ne, m1, na, na, gw.act.p, d.j, d.alive, gw.V.p, gw.XP.p, c->nsm, c->st);
+                            int r2 = translate_many<float>(c, gw.XP.p, gw.Y.p, na, 0u);
+                            if (r2) return r2;
+                            launch_gm_apply(sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+                        }
+                        CK(cudaMemsetAsync(gw.h.p, 0, sizeof(double) * (O1 + 2 * HP), c->st));
+                        launch_gm_dots_dev(ldv, S, m1, na, gw.act.p, d.j, gw.V.p, gw.W.p, h1, nullptr, c->nsm, c->st, slen);
+                        launch_gm_update_dev(ldv, S, m1, na, gw.act.p, d.j, gw.V.p, h1, gw.W.p, nullptr, c->nsm, c->st, slen);
+                        launch_gm_dots_dev(ldv, S, m1, na, gw.act.p, d.j, gw.V.p, gw.W.p, h2, h1, c->nsm, c->st, slen);
+                        launch_gm_update_dev(ldv, S, m1, na, gw.act.p, d.j, gw.V.p, h2, gw.W.p, gw.h.p, c->nsm, c->st, slen);
+                        launch_gm_scale_dev(ldv, m1, na, gw.act.p, d.j, gw.W.p, gw.h.p, 1.0e-35, gw.V.p, c->nsm, c->st, slen);
+                        launch_gm_givens(S, m, na, gw.act.p, gw.h.p, h1, d, hc, c->st);
+                        CK(cudaGetLastError());
+                        return MSTMG_OK;
+                    }();
+                    cudaGraph_t cap = nullptr;
+                    ok = cudaStreamEndCapture(c->st, &cap) == cudaSuccess && src == MSTMG_OK;
+                }
+                if (ok) ok = cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess;
+                if (gr) cudaGraphDestroy(gr);
+                const long long dl = launch_counter().load() - l0;
+                launch_counter() -= dl;   // counted per step when the graph runs
+                const int dp = c->passes32 - p0;
+                c->passes32 = p0;
+                if (!ok) {
+                    if (ex) cudaGraphExecDestroy(ex);
+                    (void)cudaGetLastError();   // the failed capture's error
+                    gw.graphs_ok = false;
+                    graphs = false;
+                } else {
+                    it = gw.cycles.emplace(na, GmresWork::CycleGraph{ex, dl, dp}).first;
+                }
+            }
+            if (graphs) {
+                CK(cudaGraphLaunch(it->second.exec, c->st));
+                dev_per_step = it->second.launches_per_step;
+                dev_passes_per_step = it->second.passes32_per_step;
+                // least-squares solutions on the device, summed into X
+                GmDevState d = gw.dev();
+                CK(cudaMemsetAsync(h2, 0, sizeof(double) * HP, c->st));
+                CK(cudaMemsetAsync(gw.dkmax.p, 0, sizeof(int), c->st));
+                launch_gm_backsolve(S, m, na, gw.act.p, d, h2, gw.dkmax.p, c->st);
+                if (seg) launch_eg_combine_dev(ne, ldv, S, m1, na, gw.act.p, seg->off, seg->len, gw.V.p, h2, gw.dkmax.p, X, c->nsm, c->st);
+                else launch_gm_combine_dev(ne, S, m1, na, gw.act.p, gw.V.p, h2, gw.dkmax.p, X, c->nsm, c->st);
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(gw.hkk, gw.dkk.p, sizeof(int) * S, cudaMemcpyDeviceToHost, c->st));
+                CK(cudaMemcpyAsync(gw.hkk + S, gw.dstatus.p, sizeof(int) * S, cudaMemcpyDeviceToHost, c->st));
+                CK(cudaMemcpyAsync(gw.hkk + 2 * S, gw.dj.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+                dev_act = act;
+                continue;
+            }
+            // capture failed: the host-driven steps below
+            CK(cudaMemcpyAsync(gw.act.p, act.data(), sizeof(int) * a, cudaMemcpyHostToDevice, c->st));
+        }
         for (int j = 0; j < jmax && !cur.empty(); j++) {
             const int na = (int)cur.size();
             const size_t hn = (size_t)(j + 1) * S * 2;
@@ -2604,6 +2769,7 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
                 return rc;
             }
             CK(cudaStreamSynchronize(c->st));
+        c->host_syncs++;
             const double* H1 = gw.hh + O1;
             std::vector<int> next;
             for (int s : cur) {
@@ -2667,6 +2833,11 @@ static int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw
             else launch_gm_combine(ne, S, m1, kmax, a, gw.act.p, gw.V.p, h2, X, c->nsm, c->st);
             CK(cudaGetLastError());
         }
+    }
+    if (!dev_act.empty()) {
+        CK(cudaStreamSynchronize(c->st));
+        c->host_syncs++;
+        fold_device_cycle();
     }
     for (int s = 0; s < S; s++) {
         iters[s] = (int)((steps[s] + 1) / 2);
@@ -2795,9 +2966,12 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
             md.scratch_stride = strd;
             launch_merge(md, grid, c->st);
         }
-        // b = Mie f, initial guess b (solver:185-187)
+        // b = Mie f, initial guess b (solver:185-187); the grouped mixed
+        // GMRES starts from zero instead, whose residual b needs no FP64 pass
+        // (the Krylov space holds b after the first step)
         launch_m_mie(sm, c->an.p, ne, Sg, PK.p, B64.p, c->st);
-        CK(cudaMemcpyAsync(X, B64.p, sizeof(zd) * (size_t)ne * Sg, cudaMemcpyDeviceToDevice, c->st));
+        if (grouped) CK(cudaMemsetAsync(X, 0, sizeof(zd) * (size_t)ne * Sg, c->st));
+        else CK(cudaMemcpyAsync(X, B64.p, sizeof(zd) * (size_t)ne * Sg, cudaMemcpyDeviceToDevice, c->st));
         CK(cudaGetLastError());
         std::vector<int> its;
         std::vector<double> errs;
@@ -2807,7 +2981,7 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
             if (c->opts.mixed_solver == 1)
                 rc = solve_multi_mixed(c, w64, w32, B32, rr, idx, Sg, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
             else if (c->opts.mixed_solver == 2)
-                rc = solve_multi_gmres(c, w64, gw, Sg, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
+                rc = solve_multi_gmres(c, w64, gw, Sg, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc, nullptr, grouped);
             else
                 rc = solve_multi_rr(c, w64, w32, rr, idx, Sg, B64.p, X, solution_eps, max_iterations, its, errs, sts, &oc);
             outer_total += oc;

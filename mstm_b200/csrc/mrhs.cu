@@ -64,11 +64,14 @@ __device__ __forceinline__ SlotPos slot_pos(const SlotMaps& sm, int e)
 // V + (s m1 + i) ld; a launch works on the a systems act[0..a) (packed work
 // columns W, XP, Y by position k, basis and norms by system s = act[k]).
 // ---------------------------------------------------------------------------
-// XP[:, k] = V_{act[k], j} for k < a, zero for a <= k < apad
-__global__ void __launch_bounds__(MB) gm_gather_kernel(int ld, int m1, int j, int a, const int* act, const zf* V, zf* XP)
+// XP[:, k] = V_{act[k], j} for k < a, zero for a <= k < apad; with jp, j =
+// *jp and systems whose alive flag is 0 give zero columns
+__global__ void __launch_bounds__(MB) gm_gather_kernel(int ld, int m1, int j, int a, const int* act, const zf* V, zf* XP, const int* jp,
+                                                      const int* alive)
 {
     const int k = blockIdx.y;
-    const zf* v = k < a ? V + ((size_t)act[k] * m1 + j) * ld : nullptr;
+    if (jp) j = *jp;
+    const zf* v = (k < a && (!alive || alive[act[k]])) ? V + ((size_t)act[k] * m1 + j) * ld : nullptr;
     zf* o = XP + (size_t)k * ld;
     for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) o[e] = v ? v[e] : mk(0.0f, 0.0f);
 }
@@ -114,11 +117,13 @@ __global__ void __launch_bounds__(MB) gm_dots_kernel(int ld, int S, int m1, cons
 }
 
 // W[:, k] -= sum_{i < kp1} V_{s,i} h[i S + s] (FP64 accumulation per
-// element); nrm[s] += |W[:, k]|^2 of the result when nrm is given
+// element); nrm[s] += |W[:, k]|^2 of the result when nrm is given; with
+// jp, kp1 = *jp + 1
 __global__ void __launch_bounds__(MB) gm_update_kernel(int ld, int S, int m1, int kp1, const int* act, const zf* V, const double* h, zf* W,
-                                                      double* nrm, const int* len)
+                                                      double* nrm, const int* len, const int* jp)
 {
     const int k = blockIdx.y, s = act[k];
+    if (jp) kp1 = *jp + 1;
     const zf* vs = V + (size_t)s * m1 * ld;
     zf* w = W + (size_t)k * ld;
     const int ne = len ? len[s] : ld;
@@ -144,9 +149,10 @@ __global__ void __launch_bounds__(MB) gm_update_kernel(int ld, int S, int m1, in
 // V_{s,jd} = src / sqrt(nrm[s stride]) with src = Wsrc[:, s] (by_sys) or
 // Wsrc[:, k]; zero where the norm is below tiny
 __global__ void __launch_bounds__(MB) gm_scale_kernel(int ld, int m1, int jd, const int* act, int by_sys, const zf* Wsrc, const double* nrm,
-                                                     int stride, double tiny, zf* V, const int* len)
+                                                     int stride, double tiny, zf* V, const int* len, const int* jp)
 {
     const int k = blockIdx.y, s = act[k];
+    if (jp) jd = *jp + 1;
     const double n2 = nrm[(size_t)s * stride];
     const float f = (n2 > tiny * tiny) ? (float)(1.0 / sqrt(n2)) : 0.0f;
     const zf* w = Wsrc + (size_t)(by_sys ? s : k) * ld;
@@ -155,10 +161,12 @@ __global__ void __launch_bounds__(MB) gm_scale_kernel(int ld, int m1, int jd, co
     for (int e = blockIdx.x * MB + threadIdx.x; e < ne; e += gridDim.x * MB) d[e] = f * w[e];
 }
 
-// X[:, s] += sum_{i < kp1} y[i S + s] V_{s,i} (FP64)
-__global__ void __launch_bounds__(MB) gm_combine_kernel(int ld, int S, int m1, int kp1, const int* act, const zf* V, const double* y, zd* X)
+// X[:, s] += sum_{i < kp1} y[i S + s] V_{s,i} (FP64); with kp1p, kp1 = *kp1p
+__global__ void __launch_bounds__(MB) gm_combine_kernel(int ld, int S, int m1, int kp1, const int* act, const zf* V, const double* y, zd* X,
+                                                       const int* kp1p)
 {
     const int k = blockIdx.y, s = act[k];
+    if (kp1p) kp1 = *kp1p;
     const zf* vs = V + (size_t)s * m1 * ld;
     zd* x = X + (size_t)s * ld;
     for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) {
@@ -219,11 +227,14 @@ __global__ void __launch_bounds__(MB) eg_start_kernel(int ne, int ldv, int m1, c
     for (int e = blockIdx.x * MB + threadIdx.x; e < len[s]; e += gridDim.x * MB) v[e] = f * r[e];
 }
 
-// XP[p, segment of s] = V_{s,j} (XP zeroed by the caller)
+// XP[p, segment of s] = V_{s,j} (XP zeroed by the caller); with jp, j = *jp
+// and systems whose alive flag is 0 are left out
 __global__ void __launch_bounds__(MB) eg_gather_kernel(int ne, int ldv, int m1, int j, const int* act, const int* off, const int* len,
-                                                      const zf* V, zf* XP)
+                                                      const zf* V, zf* XP, const int* jp, const int* alive)
 {
     const int s = act[blockIdx.y], p = s & 1;
+    if (jp) j = *jp;
+    if (alive && !alive[s]) return;
     const zf* v = V + ((size_t)s * m1 + j) * ldv;
     zf* x = XP + (size_t)p * ne + off[s];
     for (int e = blockIdx.x * MB + threadIdx.x; e < len[s]; e += gridDim.x * MB) x[e] = v[e];
@@ -248,9 +259,10 @@ __global__ void __launch_bounds__(MB) eg_apply_kernel(SlotMaps sm, const zf* an,
 
 // X[p, segment of s] += sum_{i < kp1} y[i S + s] V_{s,i} (FP64)
 __global__ void __launch_bounds__(MB) eg_combine_kernel(int ne, int ldv, int S, int m1, int kp1, const int* act, const int* off, const int* len,
-                                                       const zf* V, const double* y, zd* X)
+                                                       const zf* V, const double* y, zd* X, const int* kp1p)
 {
     const int s = act[blockIdx.y], p = s & 1;
+    if (kp1p) kp1 = *kp1p;
     const zf* vs = V + (size_t)s * m1 * ldv;
     zd* x = X + (size_t)p * ne + off[s];
     for (int e = blockIdx.x * MB + threadIdx.x; e < len[s]; e += gridDim.x * MB) {
@@ -935,7 +947,7 @@ template void launch_m_addcorr<double>(int, int, const int*, const int*, zd*, co
 // ---- GMRES launchers ----
 void launch_gm_gather(int ld, int m1, int j, int a, int apad, const int* act, const zf* V, zf* XP, int nsm, cudaStream_t st)
 {
-    gm_gather_kernel<<<dim3(multi_grid(ld, apad, nsm), apad), MB, 0, st>>>(ld, m1, j, a, act, V, XP);
+    gm_gather_kernel<<<dim3(multi_grid(ld, apad, nsm), apad), MB, 0, st>>>(ld, m1, j, a, act, V, XP, nullptr, nullptr);
     launch_counter() += 1;
 }
 void launch_gm_apply(const SlotMaps& sm, const zf* an, int ld, int a, const zf* XP, const zf* Y, zf* W, int nsm, cudaStream_t st)
@@ -952,18 +964,18 @@ void launch_gm_dots(int ld, int S, int m1, int kp1, int a, const int* act, const
 void launch_gm_update(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* h, zf* W, double* nrm, int nsm,
                       cudaStream_t st, const int* len)
 {
-    gm_update_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, h, W, nrm, len);
+    gm_update_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, h, W, nrm, len, nullptr);
     launch_counter() += 1;
 }
 void launch_gm_scale(int ld, int m1, int jd, int a, const int* act, int by_sys, const zf* Wsrc, const double* nrm, int stride, double tiny,
                      zf* V, int nsm, cudaStream_t st, const int* len)
 {
-    gm_scale_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, m1, jd, act, by_sys, Wsrc, nrm, stride, tiny, V, len);
+    gm_scale_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, m1, jd, act, by_sys, Wsrc, nrm, stride, tiny, V, len, nullptr);
     launch_counter() += 1;
 }
 void launch_gm_combine(int ld, int S, int m1, int kp1, int a, const int* act, const zf* V, const double* y, zd* X, int nsm, cudaStream_t st)
 {
-    gm_combine_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, y, X);
+    gm_combine_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, kp1, act, V, y, X, nullptr);
     launch_counter() += 1;
 }
 // ---- ensemble launchers (grid rows = active systems) ----
@@ -982,7 +994,7 @@ void launch_eg_start(int ne, int ldv, int m1, int a, const int* act, const int* 
 void launch_eg_gather(int ne, int ldv, int m1, int j, int a, const int* act, const int* off, const int* len, const zf* V, zf* XP, int nsm,
                       cudaStream_t st)
 {
-    eg_gather_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, m1, j, act, off, len, V, XP);
+    eg_gather_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, m1, j, act, off, len, V, XP, nullptr, nullptr);
     launch_counter() += 1;
 }
 void launch_eg_apply(const SlotMaps& sm, const zf* an, int ne, int ldv, int a, const int* act, const int* off, const int* len, const zf* XP,
@@ -994,6 +1006,197 @@ void launch_eg_apply(const SlotMaps& sm, const zf* an, int ne, int ldv, int a, c
 void launch_eg_combine(int ne, int ldv, int S, int m1, int kp1, int a, const int* act, const int* off, const int* len, const zf* V,
                        const double* y, zd* X, int nsm, cudaStream_t st)
 {
-    eg_combine_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, S, m1, kp1, act, off, len, V, y, X);
+    eg_combine_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, S, m1, kp1, act, off, len, V, y, X, nullptr);
+    launch_counter() += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Arnoldi cycles driven on the device (the two-column solves: a fixed
+// orientation, an ensemble).  The step index j, the systems still iterating
+// (alive), the Givens rotations, the rotated Hessenberg columns and the
+// least-squares right-hand sides live in device memory, so a whole cycle runs
+// as one CUDA graph whose body (one Arnoldi step) repeats under a conditional
+// WHILE node that the Givens kernel clears; the host synchronises once per
+// cycle.  Same arithmetic as the host's rotations (FP64).
+// ---------------------------------------------------------------------------
+// h[i S + s] (+ hacc) += V_{s,i}^H W[:, k] for i <= *jp: items (i, k, chunk)
+// over a fixed grid, partial dots over chunks of `chunk` elements
+__global__ void __launch_bounds__(MB) gm_dots_dev_kernel(int ld, int S, int m1, int a, const int* act, const int* jp, const zf* V, const zf* W,
+                                                        double* h, double* hacc, const int* len, int chunk)
+{
+    const int kp1 = *jp + 1;
+    const int nch = (ld + chunk - 1) / chunk;
+    const long long nitem = (long long)kp1 * a * nch;
+    for (long long it = blockIdx.x; it < nitem; it += gridDim.x) {
+        const int ch = (int)(it % nch);
+        const int k = (int)((it / nch) % a);
+        const int i = (int)(it / ((long long)nch * a));
+        const int s = act[k];
+        const int ne = len ? len[s] : ld;
+        const zf* v = V + ((size_t)s * m1 + i) * ld;
+        const zf* w = W + (size_t)k * ld;
+        double acc[2] = {0.0, 0.0};
+        const int e1 = min(ne, (ch + 1) * chunk);
+        for (int e = ch * chunk + threadIdx.x; e < e1; e += MB) {
+            const cpx<double> x = upd_(v[e]), y = upd_(w[e]);
+            acc[0] += x.x * y.x + x.y * y.y;
+            acc[1] += x.x * y.y - x.y * y.x;
+        }
+        double out[2];
+        mblock_store<2>(acc, out);
+        if (threadIdx.x == 0) {
+            const size_t o = 2 * ((size_t)i * S + s);
+            atomicAdd(&h[o], out[0]);
+            atomicAdd(&h[o + 1], out[1]);
+            if (hacc) {
+                atomicAdd(&hacc[o], out[0]);
+                atomicAdd(&hacc[o + 1], out[1]);
+            }
+        }
+        __syncthreads();   // mblock_store's shared slots are reused by the next item
+    }
+}
+
+// One block: the Givens step of every alive system (thread k for system
+// act[k]), as the host does it: the Hessenberg column of step j (h1) and
+// the norm of the new vector (h0[s]), the earlier rotations, the new one,
+// the least-squares right-hand side g; a system stops when its residual
+// estimate |g_{j+1}|^2 falls below target[s] or its Krylov space is
+// invariant (status 2 when the column is zero).  Thread 0 then advances j and
+// sets the cycle's WHILE condition: some system alive and j < jmax.
+__global__ void __launch_bounds__(256) gm_givens_kernel(int S, int m, int a, const int* act, const double* h0, const double* h1, GmDevState d,
+                                                       cudaGraphConditionalHandle cond)
+{
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    const int j = *d.j, m1 = m + 1;
+    for (int k = threadIdx.x; k < a; k += blockDim.x) {
+        const int s = act[k];
+        if (!d.alive[s]) continue;
+        double2* col = d.Rm + ((size_t)s * m + j) * m1;
+        double cn = 0.0;
+        for (int i = 0; i <= j; i++) {
+            const size_t o = 2 * ((size_t)i * S + s);
+            col[i] = make_double2(h1[o], h1[o + 1]);
+            cn += h1[o] * h1[o] + h1[o + 1] * h1[o + 1];
+        }
+        const double hsub = sqrt(fmax(h0[s], 0.0));
+        const double* cs = d.cs + (size_t)s * m;
+        const double2* sn = d.sn + (size_t)s * m;
+        for (int i = 0; i < j; i++) {   // the earlier rotations
+            const double ci = cs[i];
+            const double2 si = sn[i], a0 = col[i], a1 = col[i + 1];
+            // t = ci a0 + si a1; a1' = -conj(si) a0 + ci a1
+            const double2 t = make_double2(ci * a0.x + si.x * a1.x - si.y * a1.y, ci * a0.y + si.x * a1.y + si.y * a1.x);
+            col[i + 1] = make_double2(-(si.x * a0.x + si.y * a0.y) + ci * a1.x, -(si.x * a0.y - si.y * a0.x) + ci * a1.y);
+            col[i] = t;
+        }
+        const double aa = hypot(col[j].x, col[j].y), rho = sqrt(aa * aa + hsub * hsub);
+        if (rho == 0.0) {   // A v_j = 0: the operator is singular
+            d.status[s] = 2;
+            d.alive[s] = 0;
+            continue;
+        }
+        const double2 ph = aa > 0.0 ? make_double2(col[j].x / aa, col[j].y / aa) : make_double2(1.0, 0.0);
+        const double cj = aa / rho;
+        const double2 sj = make_double2(ph.x * hsub / rho, ph.y * hsub / rho);
+        d.cs[(size_t)s * m + j] = cj;
+        d.sn[(size_t)s * m + j] = sj;
+        col[j] = make_double2(ph.x * rho, ph.y * rho);
+        double2* g = d.g + (size_t)s * m1;
+        const double2 gj = g[j];
+        g[j + 1] = make_double2(-(sj.x * gj.x + sj.y * gj.y), -(sj.x * gj.y - sj.y * gj.x));   // -conj(sj) gj
+        g[j] = make_double2(cj * gj.x, cj * gj.y);
+        d.kk[s] = j + 1;
+        const double e2 = g[j + 1].x * g[j + 1].x + g[j + 1].y * g[j + 1].y;
+        if (e2 >= d.target[s] && hsub > 1.0e-13 * sqrt(cn + hsub * hsub)) atomicAdd(&cnt, 1);
+        else d.alive[s] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *d.j = j + 1;
+        cudaGraphSetConditional(cond, (cnt > 0 && j + 1 < *d.jmax) ? 1u : 0u);
+    }
+}
+
+// The cycle's least-squares solutions R y = g (back substitution per system,
+// thread k for system act[k]) into y[i S + s] (complex as 2 doubles, zero past
+// kk[s]; y zeroed by the caller), and *kmax = the largest kk.
+__global__ void __launch_bounds__(256) gm_backsolve_kernel(int S, int m, int a, const int* act, GmDevState d, double* y, int* kmax)
+{
+    const int m1 = m + 1;
+    for (int k = threadIdx.x + blockIdx.x * blockDim.x; k < a; k += blockDim.x * gridDim.x) {
+        const int s = act[k], ks = d.kk[s];
+        atomicMax(kmax, ks);
+        const double2* R = d.Rm + (size_t)s * m * m1;   // column l at R + l m1
+        const double2* g = d.g + (size_t)s * m1;
+        for (int i = ks - 1; i >= 0; i--) {
+            double2 t = g[i];
+            for (int l = i + 1; l < ks; l++) {
+                const double2 r = R[(size_t)l * m1 + i];
+                const double yx = y[2 * ((size_t)l * S + s)], yy = y[2 * ((size_t)l * S + s) + 1];
+                t.x -= r.x * yx - r.y * yy;
+                t.y -= r.x * yy + r.y * yx;
+            }
+            const double2 d0 = R[(size_t)i * m1 + i];
+            const double den = d0.x * d0.x + d0.y * d0.y;
+            y[2 * ((size_t)i * S + s)] = (t.x * d0.x + t.y * d0.y) / den;
+            y[2 * ((size_t)i * S + s) + 1] = (t.y * d0.x - t.x * d0.y) / den;
+        }
+    }
+}
+
+void launch_gm_gather_dev(int ld, int m1, int a, int apad, const int* act, const int* jp, const int* alive, const zf* V, zf* XP, int nsm,
+                          cudaStream_t st)
+{
+    gm_gather_kernel<<<dim3(multi_grid(ld, apad, nsm), apad), MB, 0, st>>>(ld, m1, 0, a, act, V, XP, jp, alive);
+    launch_counter() += 1;
+}
+void launch_eg_gather_dev(int ne, int ldv, int m1, int a, const int* act, const int* off, const int* len, const int* jp, const int* alive,
+                          const zf* V, zf* XP, int nsm, cudaStream_t st)
+{
+    eg_gather_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, m1, 0, act, off, len, V, XP, jp, alive);
+    launch_counter() += 1;
+}
+void launch_gm_dots_dev(int ld, int S, int m1, int a, const int* act, const int* jp, const zf* V, const zf* W, double* h, double* hacc,
+                        int nsm, cudaStream_t st, const int* len)
+{
+    gm_dots_dev_kernel<<<4 * nsm, MB, 0, st>>>(ld, S, m1, a, act, jp, V, W, h, hacc, len, 8192);
+    launch_counter() += 1;
+}
+void launch_gm_update_dev(int ld, int S, int m1, int a, const int* act, const int* jp, const zf* V, const double* h, zf* W, double* nrm,
+                          int nsm, cudaStream_t st, const int* len)
+{
+    gm_update_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, 0, act, V, h, W, nrm, len, jp);
+    launch_counter() += 1;
+}
+void launch_gm_scale_dev(int ld, int m1, int a, const int* act, const int* jp, const zf* Wsrc, const double* nrm, double tiny, zf* V,
+                         int nsm, cudaStream_t st, const int* len)
+{
+    gm_scale_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, m1, 0, act, 0, Wsrc, nrm, 1, tiny, V, len, jp);
+    launch_counter() += 1;
+}
+void launch_gm_givens(int S, int m, int a, const int* act, const double* h0, const double* h1, const GmDevState& d,
+                      cudaGraphConditionalHandle cond, cudaStream_t st)
+{
+    gm_givens_kernel<<<1, 256, 0, st>>>(S, m, a, act, h0, h1, d, cond);
+    launch_counter() += 1;
+}
+void launch_gm_backsolve(int S, int m, int a, const int* act, const GmDevState& d, double* y, int* kmax, cudaStream_t st)
+{
+    gm_backsolve_kernel<<<(a + 255) / 256, 256, 0, st>>>(S, m, a, act, d, y, kmax);
+    launch_counter() += 1;
+}
+void launch_gm_combine_dev(int ld, int S, int m1, int a, const int* act, const zf* V, const double* y, const int* kp1, zd* X, int nsm,
+                           cudaStream_t st)
+{
+    gm_combine_kernel<<<dim3(multi_grid(ld, a, nsm), a), MB, 0, st>>>(ld, S, m1, 0, act, V, y, X, kp1);
+    launch_counter() += 1;
+}
+void launch_eg_combine_dev(int ne, int ldv, int S, int m1, int a, const int* act, const int* off, const int* len, const zf* V, const double* y,
+                           const int* kp1, zd* X, int nsm, cudaStream_t st)
+{
+    eg_combine_kernel<<<dim3(multi_grid(ldv, a, nsm), a), MB, 0, st>>>(ne, ldv, S, m1, 0, act, off, len, V, y, X, kp1);
     launch_counter() += 1;
 }

@@ -87,6 +87,38 @@ void launch_eg_apply(const SlotMaps& sm, const zf* an, int ne, int ldv, int a, c
 void launch_eg_combine(int ne, int ldv, int S, int m1, int kp1, int a, const int* act, const int* off, const int* len, const zf* V,
                        const double* y, zd* X, int nsm, cudaStream_t st);
 
+// ---- Arnoldi cycles driven on the device (one CUDA graph per cycle: the
+//      step under a conditional WHILE node); state in device memory ----
+struct GmDevState {
+    int* j;          // step index of the cycle
+    int* jmax;       // steps the cycle may take
+    int* alive;      // per system: still iterating in this cycle
+    int* kk;         // per system: steps taken in this cycle
+    int* status;     // per system: 2 when the operator was found singular
+    double* target;  // per system: squared residual estimate that ends its cycle
+    double* cs;      // per system: m rotation cosines
+    double2* sn;     // per system: m rotation sines
+    double2* g;      // per system: m + 1 least-squares right-hand side
+    double2* Rm;     // per system: m rotated Hessenberg columns of m + 1
+};
+void launch_gm_gather_dev(int ld, int m1, int a, int apad, const int* act, const int* jp, const int* alive, const zf* V, zf* XP, int nsm,
+                          cudaStream_t st);
+void launch_eg_gather_dev(int ne, int ldv, int m1, int a, const int* act, const int* off, const int* len, const int* jp, const int* alive,
+                          const zf* V, zf* XP, int nsm, cudaStream_t st);
+void launch_gm_dots_dev(int ld, int S, int m1, int a, const int* act, const int* jp, const zf* V, const zf* W, double* h, double* hacc,
+                        int nsm, cudaStream_t st, const int* len = nullptr);
+void launch_gm_update_dev(int ld, int S, int m1, int a, const int* act, const int* jp, const zf* V, const double* h, zf* W, double* nrm,
+                          int nsm, cudaStream_t st, const int* len = nullptr);
+void launch_gm_scale_dev(int ld, int m1, int a, const int* act, const int* jp, const zf* Wsrc, const double* nrm, double tiny, zf* V,
+                         int nsm, cudaStream_t st, const int* len = nullptr);
+void launch_gm_givens(int S, int m, int a, const int* act, const double* h0, const double* h1, const GmDevState& d,
+                      cudaGraphConditionalHandle cond, cudaStream_t st);
+void launch_gm_backsolve(int S, int m, int a, const int* act, const GmDevState& d, double* y, int* kmax, cudaStream_t st);
+void launch_gm_combine_dev(int ld, int S, int m1, int a, const int* act, const zf* V, const double* y, const int* kp1, zd* X, int nsm,
+                           cudaStream_t st);
+void launch_eg_combine_dev(int ne, int ldv, int S, int m1, int a, const int* act, const int* off, const int* len, const zf* V, const double* y,
+                           const int* kp1, zd* X, int nsm, cudaStream_t st);
+
 // ---- T matrix (tmatrix_solution, mstm-solver-8.f90:22-332) ----
 // columns of order l: unit TE (q=1) / TM (q=2) field of degree k in the LR basis
 void launch_tm_rhs(int l, zd* P0, cudaStream_t st);

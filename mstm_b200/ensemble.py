@@ -41,12 +41,14 @@ def ensemble_configs(count, seed=4, nmin=50, nmax=400, x=1.5, m=1.6 + 0.005j, fv
 
 class Autotuner:
     """Per size class (sphere count rounded to 50, sphere order, precision), the
-    tiled kernel's CTAs per SM, the FP32 column chunk and the kernel family
-    (tiled or order-generic), chosen by timing a translation pass over the
-    column count of the largest T-matrix order's batch."""
+    pass that serves the many-column solves: the tensor-core pass (dense TF32
+    hi/lo operators), or the rotation kernels with their CTAs per SM, FP32
+    column chunk and kernel family (tiled or order-generic), chosen by timing
+    one translation pass over the column count of a T-matrix group."""
 
-    CANDIDATES = [dict(tile_ctas_per_sm=c, fp32_chunk=k, generic_kernel=0) for c in (0, 2) for k in (2, 4)] + \
-                 [dict(tile_ctas_per_sm=0, fp32_chunk=0, generic_kernel=1)]
+    CANDIDATES = [dict(tensor_core=0)] + \
+                 [dict(tensor_core=-1, tile_ctas_per_sm=c, fp32_chunk=k, generic_kernel=0) for c in (0, 2) for k in (2, 4)] + \
+                 [dict(tensor_core=-1, tile_ctas_per_sm=0, fp32_chunk=0, generic_kernel=1)]
 
     def __init__(self, reps=3):
         self.reps = reps
@@ -70,7 +72,7 @@ class Autotuner:
             g = api.SphereCluster(cfg["pos"], np.full(n, cfg["x"]), np.full(n, cfg["m"]), mie_epsilon=-cfg["order"],
                                   precision=precision, **cand)
             ms = ctypes.c_double(0.0)
-            prec = 0 if precision == "fp64" else 1
+            prec = 0 if precision == "fp64" else (2 if cand.get("tensor_core", -1) == 0 else 1)
             rc = L.mstmg_time_translation(g.ctx, prec, columns, self.reps, ctypes.byref(ms))
             err = L.mstmg_last_error().decode() if rc != 0 else ""
             g.close()
@@ -109,7 +111,7 @@ def solve_ensemble(cfgs, precision="mixed", workers=4, tuner=None, **kw):
     return per-configuration results, ensemble means and throughput."""
     order = sorted(range(len(cfgs)), key=lambda k: -len(cfgs[k]["pos"]))
     results = [None] * len(cfgs)
-    tune_cols = 2 * (2 * 25 + 1)   # column count of a large order's batch, the tuning case
+    tune_cols = 128   # columns of one tensor-core tile, about a T-matrix order group
     t_tune = time.time()
     if tuner is not None:
         # one representative per size class, timed alone before any solve runs

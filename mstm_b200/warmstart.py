@@ -476,6 +476,204 @@ def solve_with_guess(cfg, x0, eps=1e-12, precision="mixed", fallback=1.0):
     return dict(amnp=amnp, qtot=qtot.reshape(3, 3, order="F"), used=used.tolist(), guess_residual=res.tolist(), **stats)
 
 
+# ---------------------------------------------------------------------------
+# the study at scale: configurations solved in ensembles, graphs kept on the GPU
+# ---------------------------------------------------------------------------
+def _draw_params(rng, n):
+    """The parameters of n configurations as sample_config draws them (the
+    positions come later, from their own seeds)."""
+    out = []
+    for _ in range(n):
+        nn = int(rng.integers(100, 301))
+        x = float(rng.uniform(0.5, 2.0))
+        m = complex(rng.uniform(1.3, 1.7), 10.0 ** rng.uniform(-4.0, -1.0))
+        fv = float(rng.uniform(0.05, 0.30))
+        out.append(dict(n=nn, x=x, m=m, fv=fv, seed=int(rng.integers(0, 2 ** 31 - 1)), order=C.truncation_order(x)))
+    return out
+
+
+def _rsa_positions(p):
+    pos, _ = C.rsa_sphere_batched(p["n"], p["x"], p["fv"], seed=p["seed"])
+    return np.asarray(pos, np.float64)
+
+
+def draw_configs(n, seed, workers=0):
+    """n configurations of the study (100-300 spheres, x in [0.5, 2], Re m in
+    [1.3, 1.7], Im m log-uniform in [1e-4, 0.1], fv in [0.05, 0.30], RSA in a
+    bounding sphere with batched candidates), the positions made by a process
+    pool (spawned, so it can start after CUDA) when workers > 1."""
+    params = _draw_params(np.random.default_rng(seed), n)
+    if workers > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(workers) as pool:
+            pos = pool.map(_rsa_positions, params, chunksize=16)
+    else:
+        pos = [_rsa_positions(p) for p in params]
+    return [dict(pos=q, x=p["x"], m=p["m"], fv=p["fv"], order=p["order"]) for p, q in zip(params, pos)]
+
+
+def solve_samples(cfgs, eps=1e-10, batch=32):
+    """Training samples of many configurations: the solver's own solutions,
+    configurations of one sphere order solved together in ensemble contexts
+    (mstmg_ensemble_fixed_orientation), the Mie start a^0 = Mie f and the
+    targets formed as make_sample forms them."""
+    L_ = _lib.lib()
+    by_order = {}
+    for k, cfg in enumerate(cfgs):
+        by_order.setdefault(cfg["order"], []).append(k)
+    out = [None] * len(cfgs)
+    for L, idx in sorted(by_order.items()):
+        nb = 2 * L * (L + 2)
+        src, dst = block_map(L)
+        for b0 in range(0, len(idx), batch):
+            chunk = idx[b0:b0 + batch]
+            ens = api.SphereEnsemble([(cfgs[k]["pos"], np.full(len(cfgs[k]["pos"]), cfgs[k]["x"]), cfgs[k]["m"]) for k in chunk],
+                                     mie_epsilon=-L)
+            r = ens.fixedorsoln(eps=eps)
+            an_all = ens.miecoefcalc()[0]
+            pw = np.zeros((ens.number_eqns, 2), np.complex128, order="F")
+            _lib.check(L_.mstmg_planewave(ens.ctx, 0.0, 0.0, 1, api._ptr(pw)), "planewave")
+            off, start = ens.sphere_offset, ens.config_start
+            for c, k in enumerate(chunk):
+                cfg = cfgs[k]
+                n = len(cfg["pos"])
+                i0 = start[c]
+                an = np.asarray(an_all[4 * L * i0:4 * L * (i0 + 1)])
+                A, Ainv = _mie_blocks(an, L)
+                rows = slice(off[start[c]], off[start[c + 1]])
+                a = r["amnp"][rows]
+                f = pw[rows]
+                a0 = np.zeros_like(a)
+                for pol in range(2):
+                    a0[:, pol] = _apply_blocks(A, f[:, pol].reshape(n, nb), L).reshape(-1)
+                phase = np.exp(-1j * cfg["pos"][:, 2])
+                t = np.zeros((n, NOUT), np.float32)
+                mask = np.zeros((n, NOUT), np.float32)
+                for pol in range(2):
+                    e = _apply_blocks(Ainv, (a[:, pol] - a0[:, pol]).reshape(n, nb) * phase[:, None], L)
+                    for c_ in range(2):
+                        cols = pol * 4 * NBH + 2 * dst + c_
+                        t[:, cols] = (e.real if c_ == 0 else e.imag)[:, src]
+                        mask[:, cols] = 1.0
+                out[k] = dict(cfg=cfg, X=node_features(cfg, an), target=t, mask=mask, a0=np.asfortranarray(a0), an=an)
+            ens.close()
+    return out
+
+
+def save_net(net, path, meta=None):
+    """The trained weights (FP32 masters), the target scale and a description."""
+    import json
+    np.savez_compressed(path, params=net.state(), scale=net.scale, hidden=net.H, layers=net.layers,
+                        meta=json.dumps(meta or {}))
+
+
+def load_net(path, device):
+    import json
+    d = np.load(path)
+    net = WarmStartNet(device, seed=0, hidden=int(d["hidden"]), layers=int(d["layers"]))
+    net.load(d["params"])
+    net.scale = d["scale"]
+    return net, json.loads(str(d["meta"]))
+
+
+def evaluate(net, held, fallbacks=(1.0, 0.1), eps=1e-12, precision="mixed"):
+    """Held-out configurations: solver iterations and wall time (the guess's
+    network inference included) to ||r||/||b|| < 1e-6 from the network's guess
+    under each fallback threshold, against the reference's Mie start."""
+    import time
+    import torch
+    res = {}
+    t_mie, it_mie, r_mie = 0.0, 0, []
+    guesses = []
+    for s in held:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x0 = predict_guess(net, s)
+        torch.cuda.synchronize()
+        guesses.append((x0, time.perf_counter() - t0))
+        t0 = time.perf_counter()
+        rp = solve_with_guess(s["cfg"], s["a0"], eps=eps, precision=precision, fallback=10.0)
+        t_mie += time.perf_counter() - t0
+        it_mie += sum(rp["iterations"])
+        r_mie += rp["guess_residual"]
+    for fb in fallbacks:
+        t_w, it_w, nfb, r_w = 0.0, 0, 0, []
+        for s, (x0, t_inf) in zip(held, guesses):
+            t0 = time.perf_counter()
+            rw = solve_with_guess(s["cfg"], x0, eps=eps, precision=precision, fallback=fb)
+            t_w += time.perf_counter() - t0 + t_inf
+            it_w += sum(rw["iterations"])
+            nfb += 2 - sum(rw["used"])
+            r_w += rw["guess_residual"]
+        res["fallback_%g" % fb] = dict(fallback=fb, iterations_warm=it_w, iterations_mie_start=it_mie,
+                                      iteration_ratio=round(it_w / max(1, it_mie), 4), wall_s_warm=round(t_w, 2),
+                                      wall_s_mie_start=round(t_mie, 2), wall_ratio=round(t_w / max(1e-9, t_mie), 4),
+                                      mean_initial_residual_warm=float(np.mean(r_w)),
+                                      mean_initial_residual_mie=float(np.mean(r_mie)), fallbacks=nfb,
+                                      polarisations=2 * len(held))
+    return res
+
+
+def study_at_scale(n_train=20000, n_eval=1000, epochs=20, batch=16, lr=2e-3, train_seed=5, eval_seed=6, workers=16, device=None,
+                   save=None, log=print):
+    """The warm-start study as specified: n_train configurations drawn with
+    seed 5 and solved by the library (ensembles of one sphere order), the
+    network trained on them on the GPU with the library's kernels, n_eval
+    held-out configurations drawn with seed 6 evaluated against the Mie start
+    with the 1.0 and 0.1 fallback thresholds."""
+    import time
+    import torch
+    dev = device or torch.device("cuda", 0)
+    t0 = time.time()
+    tr_cfgs = draw_configs(n_train, train_seed, workers)
+    ev_cfgs = draw_configs(n_eval, eval_seed, workers)
+    t_draw = time.time() - t0
+    t0 = time.time()
+    graphs, scale_src, ntr = [], [], 0
+    net = WarmStartNet(dev, seed=0)
+    for b0 in range(0, n_train, 512):
+        samples = solve_samples(tr_cfgs[b0:b0 + 512])
+        if net.scale is None:
+            net.scale = fit_scale(samples)
+        for i in range(0, len(samples), batch):
+            part = [dict(s, target=(s["target"] / net.scale).astype(np.float32)) for s in samples[i:i + batch]]
+            graphs.append(batch_graph(part, dev))
+        ntr += len(samples)
+        if log:
+            log("solved %d / %d training configurations (%.0f s)" % (ntr, n_train, time.time() - t0))
+    held = solve_samples(ev_cfgs)
+    torch.cuda.synchronize(dev)
+    t_gen = time.time() - t0
+    rng = np.random.default_rng(0)
+    t0 = time.time()
+    hist = []
+    for ep in range(epochs):
+        tot = 0.0
+        for b in rng.permutation(len(graphs)):
+            gr = graphs[b]
+            y, cache = net.forward(gr)
+            loss, dy = net.loss_grad(y, gr["target"], gr["mask"], gr["msum"])
+            net.backward(gr, cache, dy)
+            net.adam(lr=lr * (0.5 if ep >= epochs // 2 else 1.0))
+            tot += float(loss.item())
+        hist.append(tot / len(graphs))
+        if log:
+            log("epoch %d loss %.4e" % (ep, hist[-1]))
+    torch.cuda.synchronize(dev)
+    t_train = time.time() - t0
+    del graphs
+    t0 = time.time()
+    ev = evaluate(net, held)
+    t_eval = time.time() - t0
+    out = dict(n_train=n_train, n_eval=n_eval, epochs=epochs, batch=batch, draw_s=round(t_draw, 1), gen_s=round(t_gen, 1),
+               train_s=round(t_train, 1), eval_s=round(t_eval, 1), loss_first=hist[0], loss_last=hist[-1], **ev)
+    if save:
+        save_net(net, save, meta=out)
+    if log:
+        log(out)
+    return out
+
+
 def study(n_train=200, n_eval=16, epochs=60, seed=5, device=None, fallback=1.0, log=print):
     """Generate, train, evaluate: the warm-start study on configurations drawn
     as sample_config draws them.  Returns a summary dict (iterations and
@@ -519,9 +717,11 @@ if __name__ == "__main__":
     import argparse
     import json
     ap = argparse.ArgumentParser(description="train and evaluate the learned warm start")
-    ap.add_argument("--train", type=int, default=500)
-    ap.add_argument("--eval", type=int, default=16)
-    ap.add_argument("--epochs", type=int, default=150)
-    ap.add_argument("--fallback", type=float, default=1.0)
+    ap.add_argument("--train", type=int, default=20000)
+    ap.add_argument("--eval", type=int, default=1000)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--save", default=None, help="write the trained network here (.npz)")
     a = ap.parse_args()
-    print(json.dumps(study(a.train, a.eval, a.epochs, fallback=a.fallback, log=None)))
+    print(json.dumps(study_at_scale(a.train, a.eval, a.epochs, workers=a.workers, save=a.save,
+                                    log=lambda m: print(m, flush=True))))

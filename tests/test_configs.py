@@ -85,3 +85,15 @@ def test_position_file_round_trip(tmp_path):
     assert rows.shape == (40, 6) and np.allclose(rows[:, 4], 1.6) and np.allclose(rows[:, 5], 0.05)
     pos3, _ = C.read_position_file(str(p))
     assert np.allclose(pos3, pos, rtol=1e-10, atol=1e-10)
+
+
+@pytest.mark.parametrize("n,x,fv,seed", [(300, 1.0, 0.30, 3), (120, 2.0, 0.05, 8)])
+def test_rsa_sphere_batched(n, x, fv, seed):
+    """The batched sampler of the warm-start study: n spheres, inside the
+    bounding sphere of rsa_sphere's radius, no overlaps, seeded."""
+    pos, R = C.rsa_sphere_batched(n, x, fv, seed=seed)
+    assert pos.shape == (n, 3)
+    assert abs(n * x ** 3 / R ** 3 - fv) < 1e-12
+    assert np.sqrt((pos ** 2).sum(1)).max() <= R - x + 1e-12
+    assert _pair_dist(pos).min() >= 2.0 * x
+    assert np.array_equal(pos, C.rsa_sphere_batched(n, x, fv, seed=seed)[0])

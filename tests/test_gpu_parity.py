@@ -536,3 +536,34 @@ def test_order_of_scattering_mode(api, oracle_mod):
     fg = g.fixedorsoln(eps=1e-10, niter=-100)
     assert fg["iterations"][1] == fo["maxiter"]
     assert np.allclose(fg["qtot"], fo["qtot"], rtol=RTOL_FP64)
+
+
+@pytest.mark.parametrize("name", ["cluster20", "fractal60"])
+def test_device_driven_cycles_sync_once_per_cycle(api, oracle_mod, name):
+    """Two-column mixed solves run each GMRES restart cycle as one CUDA graph
+    (the Arnoldi step under a conditional WHILE node, Givens rotations on
+    the device): one host synchronisation per cycle plus one at the end,
+    the same iterations (to one step: the device sums its dot products in
+    another order) and efficiencies as the host-driven steps (kernel timing
+    turns the graphs off), and the oracle's efficiencies."""
+    from mstm_b200 import _lib
+    pos, rad, ri, em = _cluster(name)
+    o = oracle_mod.Oracle(pos, rad, ri, mie_eps=em, store_matrix=True, nthreads=8)
+    ro = o.fixedorsoln(eps=1e-12, niter=4000)
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed")
+    rd = g.fixedorsoln(eps=1e-12, niter=4000)
+    st = g.last_stats()
+    assert rd["istat"] == 0 and rd["maxerr"] < 1e-12
+    assert st["host_syncs"] <= st["outer"] + 1, st
+    assert np.allclose(rd["qtot"], ro["qtot"], rtol=RTOL_MIXED)
+    h = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed")
+    L = _lib.lib()
+    L.mstmg_set_timing(h.ctx, 1)   # kernel timing: host-driven steps
+    rh = h.fixedorsoln(eps=1e-12, niter=4000)
+    sh = h.last_stats()
+    L.mstmg_set_timing(h.ctx, 0)
+    assert sh["host_syncs"] > st["host_syncs"]
+    assert all(abs(a - b) <= 1 for a, b in zip(rh["iterations"], rd["iterations"]))
+    assert np.allclose(rh["qtot"], rd["qtot"], rtol=RTOL_MIXED)
+    g.close()
+    h.close()

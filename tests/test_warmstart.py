@@ -127,3 +127,21 @@ def test_fallback_to_mie_start(ws):
     assert rw["used"] == [0, 0] and min(rw["guess_residual"]) > 0.1
     assert rw["iterations"] == rp["iterations"]
     assert np.allclose(rw["qtot"], rp["qtot"], rtol=1e-12)
+
+
+def test_ensemble_samples_match_single_solves(ws):
+    """The study's training samples from ensemble solves (configurations of
+    one order together) carry the same Mie start and, to the solution
+    tolerance, the same targets as one-at-a-time solves."""
+    from mstm_b200 import configs as C
+    W, _ = ws
+    cfgs = W.draw_configs(4, 17)
+    cfgs[1] = dict(cfgs[1], order=cfgs[0]["order"], x=cfgs[0]["x"])   # two of one order share an ensemble
+    cfgs[1]["pos"] = C.rsa_sphere_batched(len(cfgs[1]["pos"]), cfgs[1]["x"], cfgs[1]["fv"], seed=3)[0]
+    batched = W.solve_samples(cfgs, eps=1e-12)
+    for cfg, b in zip(cfgs, batched):
+        s = W.make_sample(cfg, eps=1e-12)
+        assert np.abs(b["a0"] - s["a0"]).max() <= 1e-12 * np.abs(s["a0"]).max()
+        assert np.array_equal(b["mask"], s["mask"]) and np.allclose(b["X"], s["X"])
+        scale = np.abs(s["target"]).max()
+        assert np.abs(b["target"] - s["target"]).max() <= 1e-4 * scale
