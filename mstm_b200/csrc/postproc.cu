@@ -16,85 +16,12 @@
 #include "common.cuh"
 #include "special.cuh"
 #include "postproc.cuh"
+#include "vcoupling.cuh"
 #include <algorithm>
 
 #define PP_NT 128
 
-// ---------------------------------------------------------------------------
-// vector-coupling coefficients on the device (vcfunc / vcfuncuprec,
-// modules:950-1056), from a bcof/fnr table of side nbc+1
-// ---------------------------------------------------------------------------
-struct VCTab {
-    const double* bcof;  // (nbc+1)^2
-    const double* fnr;   // 0..2*nbc
-    int nbc;
-    __device__ double bc(int n, int l) const { return bcof[(size_t)n * (nbc + 1) + l]; }
-    __device__ double fr(int n) const { return fnr[n]; }
-};
-
-__device__ void vc_uprec(const VCTab& t, int m, int n, int k, int l, int wmax, double* vcn)
-{
-    int mk = abs(m + k), nl = abs(n - l), w, m1, l1, k1;
-    double vc1;
-    if (nl >= mk) {
-        w = nl;
-        if (n >= l) { m1 = m; l1 = l; k1 = k; }
-        else { m1 = k; k1 = m; l1 = n; }
-        vc1 = pm1(k1 + l1) * t.bc(l1 + k1, w - m1 - k1) * t.bc(l1 - k1, w + m1 + k1) / t.bc(l1 + l1, w + w + 1);
-    } else {
-        w = mk;
-        if (m + k >= 0) vc1 = pm1(n + m) * t.bc(n - l + w, l - k) * t.bc(l - n + w, n - m) / t.bc(w + w + 1, n + l - w);
-        else vc1 = pm1(l + k) * t.bc(n - l + w, l + k) * t.bc(l - n + w, n + m) / t.bc(w + w + 1, n + l - w);
-    }
-    int w1 = w;
-    vcn[w] = vc1;
-    w = w1 + 1;
-    mk = m + k;
-    int w2 = min(wmax, n + l);
-    if (w2 > w1) {
-        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
-                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
-        double t2 = (w1 == 0) ? 0.5 * (double)(m - k)
-                              : (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
-        vcn[w] = t1 * t2 * vcn[w1];
-    }
-    for (w = w1 + 2; w <= w2; w++) {
-        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
-                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
-        double t2 = (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
-        double t3 = t.fr(w - mk - 1) * t.fr(w + mk - 1) * t.fr(l - n + w - 1) * t.fr(n - l + w - 1) * t.fr(n + l - w + 2) * t.fr(n + l + w) /
-                    ((double)(2 * (w - 1)) * t.fr(2 * w - 3) * t.fr(2 * w - 1));
-        vcn[w] = t1 * (t2 * vcn[w - 1] - t3 * vcn[w - 2]);
-    }
-}
-
-__device__ void vc_func(const VCTab& t, int m, int n, int k, int l, double* vcn)
-{
-    for (int w = 0; w <= n + l; w++) vcn[w] = 0.0;
-    int wmax = n + l;
-    int wmin = max(abs(n - l), abs(m + k));
-    vcn[wmax] = t.bc(n + m, l + k) * t.bc(n - m, l - k) / t.bc(n + n, l + l);
-    if (wmin == wmax) return;
-    vcn[wmax - 1] = vcn[wmax] * (l * m - k * n) * t.fr(2 * (l + n) - 1) / t.fr(l) / t.fr(n) / t.fr(n + l + m + k) / t.fr(n + l - m - k);
-    if (wmin == wmax - 1) return;
-    int mk = m + k;
-    double vcmax = fabs(vcn[wmax]) + fabs(vcn[wmax - 1]);
-    int w;
-    for (w = wmax; w >= wmin + 2; w--) {
-        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
-                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
-        double t2 = (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
-        double t3 = t.fr(w - mk - 1) * t.fr(w + mk - 1) * t.fr(l - n + w - 1) * t.fr(n - l + w - 1) * t.fr(n + l - w + 2) * t.fr(n + l + w) /
-                    ((double)(2 * (w - 1)) * t.fr(2 * w - 3) * t.fr(2 * w - 1));
-        vcn[w - 2] = (t2 * vcn[w - 1] - vcn[w] / t1) / t3;
-        if ((wmax - w) % 2 == 1) {
-            double vctest = fabs(vcn[w - 2]) + fabs(vcn[w - 1]);
-            vcmax = vcmax > vctest ? vcmax : vctest;
-            if (vctest / vcmax < 0.01) break;
-        }
-    }
-    if (w - 2 > wmin) vc_uprec(t, m, n, k, l, w - 3, vcn);
-}
+// vector-coupling coefficients: vc_func / vc_uprec of vcoupling.cuh
 
 __device__ __forceinline__ zd ipow_z(int k)
 {

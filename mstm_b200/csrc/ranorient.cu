@@ -14,80 +14,9 @@
 //                    by the rotcoef recurrence (kmax = 2) and the 16 elements
 #include "common.cuh"
 #include "ranorient.cuh"
+#include "vcoupling.cuh"
 
 namespace {
-
-struct VT {
-    const double* bcof;
-    const double* fnr;
-    int nbc;
-    __device__ double bc(int n, int l) const { return bcof[(size_t)n * (nbc + 1) + l]; }
-    __device__ double fr(int n) const { return fnr[n]; }
-};
-
-// vcfunc / vcfuncuprec (mstm-modules-33.f90:950-1056), one thread
-__device__ void ro_vcup(const VT& t, int m, int n, int k, int l, int wmax, double* vcn)
-{
-    int mk = abs(m + k), nl = abs(n - l), w, m1, l1, k1;
-    double vc1;
-    if (nl >= mk) {
-        w = nl;
-        if (n >= l) { m1 = m; l1 = l; k1 = k; }
-        else { m1 = k; k1 = m; l1 = n; }
-        vc1 = pm1(k1 + l1) * t.bc(l1 + k1, w - m1 - k1) * t.bc(l1 - k1, w + m1 + k1) / t.bc(l1 + l1, w + w + 1);
-    } else {
-        w = mk;
-        if (m + k >= 0) vc1 = pm1(n + m) * t.bc(n - l + w, l - k) * t.bc(l - n + w, n - m) / t.bc(w + w + 1, n + l - w);
-        else vc1 = pm1(l + k) * t.bc(n - l + w, l + k) * t.bc(l - n + w, n + m) / t.bc(w + w + 1, n + l - w);
-    }
-    int w1 = w;
-    vcn[w] = vc1;
-    w = w1 + 1;
-    mk = m + k;
-    int w2 = min(wmax, n + l);
-    if (w2 > w1) {
-        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
-                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
-        double t2 = (w1 == 0) ? 0.5 * (double)(m - k)
-                              : (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
-        vcn[w] = t1 * t2 * vcn[w1];
-    }
-    for (w = w1 + 2; w <= w2; w++) {
-        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
-                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
-        double t2 = (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
-        double t3 = t.fr(w - mk - 1) * t.fr(w + mk - 1) * t.fr(l - n + w - 1) * t.fr(n - l + w - 1) * t.fr(n + l - w + 2) * t.fr(n + l + w) /
-                    ((double)(2 * (w - 1)) * t.fr(2 * w - 3) * t.fr(2 * w - 1));
-        vcn[w] = t1 * (t2 * vcn[w - 1] - t3 * vcn[w - 2]);
-    }
-}
-__device__ void ro_vc(const VT& t, int m, int n, int k, int l, double* vcn)
-{
-    for (int w = 0; w <= n + l; w++) vcn[w] = 0.0;
-    int wmax = n + l;
-    int wmin = max(abs(n - l), abs(m + k));
-    vcn[wmax] = t.bc(n + m, l + k) * t.bc(n - m, l - k) / t.bc(n + n, l + l);
-    if (wmin == wmax) return;
-    vcn[wmax - 1] = vcn[wmax] * (l * m - k * n) * t.fr(2 * (l + n) - 1) / t.fr(l) / t.fr(n) / t.fr(n + l + m + k) / t.fr(n + l - m - k);
-    if (wmin == wmax - 1) return;
-    int mk = m + k;
-    double vcmax = fabs(vcn[wmax]) + fabs(vcn[wmax - 1]);
-    int w;
-    for (w = wmax; w >= wmin + 2; w--) {
-        double t1 = 2 * w * t.fr(w + w + 1) * t.fr(w + w - 1) /
-                    (t.fr(w + mk) * t.fr(w - mk) * t.fr(n - l + w) * t.fr(l - n + w) * t.fr(n + l - w + 1) * t.fr(n + l + w + 1));
-        double t2 = (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
-        double t3 = t.fr(w - mk - 1) * t.fr(w + mk - 1) * t.fr(l - n + w - 1) * t.fr(n - l + w - 1) * t.fr(n + l - w + 2) * t.fr(n + l + w) /
-                    ((double)(2 * (w - 1)) * t.fr(2 * w - 3) * t.fr(2 * w - 1));
-        vcn[w - 2] = (t2 * vcn[w - 1] - vcn[w] / t1) / t3;
-        if ((wmax - w) % 2 == 1) {
-            double vctest = fabs(vcn[w - 2]) + fabs(vcn[w - 1]);
-            vcmax = vcmax > vctest ? vcmax : vctest;
-            if (vctest / vcmax < 0.01) break;
-        }
-    }
-    if (w - 2 > wmin) ro_vcup(t, m, n, k, l, w - 3, vcn);
-}
 
 __device__ __forceinline__ zd ipw(int k)
 {
@@ -166,7 +95,7 @@ __global__ void __launch_bounds__(RO_NT) ro_dm_kernel(RoArgs a)
     extern __shared__ __align__(16) unsigned char smraw[];
     const int nodr = a.nodr, nodr2 = 2 * nodr, nodrw = nodr2, nblk = nodr * (nodr + 2), nblkt = 2 * nblk;
     const int tid = threadIdx.x;
-    const VT vt{a.bcof, a.fnr, a.nbc};
+    const VCTab vt{a.bcof, a.fnr, a.nbc};
     zd* bm = reinterpret_cast<zd*>(smraw);                 // bm(k,mn,p): 2 x nblk x 2
     zd* bmcf = bm + 4 * nblk;
     zd* am = bmcf + 4 * nblk;                              // am(k,l,p): 2 x (nodr+1) x 2
@@ -189,7 +118,7 @@ __global__ void __launch_bounds__(RO_NT) ro_dm_kernel(RoArgs a)
             const int nn1 = n * (n + 1), lmax = min(nodr, W + n);
             for (int e = tid; e < 8 * (nodr + 1); e += RO_NT) am[e] = mk(0.0, 0.0);
             // vcfunc(v, w, -t, n) for t = -n..n
-            for (int t = -n + tid; t <= n; t += RO_NT) ro_vc(vt, v, W, -t, n, vct + (size_t)(t + n) * VL);
+            for (int t = -n + tid; t <= n; t += RO_NT) vc_func(vt, v, W, -t, n, vct + (size_t)(t + n) * VL);
             __syncthreads();
             // am(k,l,p) = sum_t vc(l) tc(p, n(n+1)+t, k, l(l+1)+t-v)
             for (int e = tid; e < 4 * lmax; e += RO_NT) {
@@ -213,7 +142,7 @@ __global__ void __launch_bounds__(RO_NT) ro_dm_kernel(RoArgs a)
                 int m = e / 2 - n, k = e % 2 + 1;
                 int u = m - (-3 + 2 * k);
                 if (abs(u) > W) continue;
-                ro_vc(vt, -u, W, m, n, vthr);
+                vc_func(vt, -u, W, m, n, vthr);
                 int mn = nn1 + m;
                 for (int l = max(1, abs(W - n)); l <= lmax; l++) {
                     double fl = -pm1(l) * vthr[l] / (double)(l + l + 1);
@@ -259,7 +188,7 @@ __global__ void __launch_bounds__(RO_NT) ro_dm_kernel(RoArgs a)
 __global__ void __launch_bounds__(RO_NT) ro_coef_kernel(RoArgs a)
 {
     const int nodr = a.nodr, w = blockIdx.x, tid = threadIdx.x;
-    const VT vt{a.bcof, a.fnr, a.nbc};
+    const VCTab vt{a.bcof, a.fnr, a.nbc};
     const int VL = 3 * nodr + 2;
     double* vthr = a.vscr + ((size_t)blockIdx.x * RO_NT + tid) * VL;
     zd* fm = a.fm + (size_t)w * 2 * (3 * nodr * 2 * nodr * 2);
@@ -279,13 +208,13 @@ __global__ void __launch_bounds__(RO_NT) ro_coef_kernel(RoArgs a)
                     m = u + k;
                     mlim = max(1, abs(m));
                     if (n < mlim || n1 < mlim) continue;
-                    ro_vc(vt, m, n, 0, w, vthr);
+                    vc_func(vt, m, n, 0, w, vthr);
                 } else {
                     if (w < 2) break;
                     m = u + 1;
                     int m1 = u - 1;
                     if (n < max(1, abs(m)) || n1 < max(1, abs(m1))) continue;
-                    ro_vc(vt, m, n, -2, w, vthr);
+                    vc_func(vt, m, n, -2, w, vthr);
                 }
                 double fl = -pm1(n) * vthr[n1] * a.fnr[w + w + 1] / a.fnr[n1 + n1 + 1];
                 for (int p = 1; p <= 2; p++)
@@ -314,7 +243,7 @@ __global__ void __launch_bounds__(RO_NT) ro_coef_kernel(RoArgs a)
     for (int n = 1; n <= nodr; n++) {
         int n1s = max(1, abs(n - w)), n1e = min(nodr, n + w);
         double in = pm1(n);
-        ro_vc(vt, 1, n, 0, w, vthr);
+        vc_func(vt, 1, n, 0, w, vthr);
         for (int n1 = n1s; n1 <= n1e; n1++) {
             double fl = 2.0 * in * vthr[n1] * a.fnr[w + w + 1] / a.fnr[n1 + n1 + 1];
             int i = (n + n1 - w) % 2 + 1;
@@ -333,7 +262,7 @@ __global__ void __launch_bounds__(RO_NT) ro_coef_kernel(RoArgs a)
             }
         }
         if (w < 2) continue;
-        ro_vc(vt, 1, n, -2, w, vthr);
+        vc_func(vt, 1, n, -2, w, vthr);
         for (int n1 = n1s; n1 <= n1e; n1++) {
             double fl = 2.0 * in * vthr[n1] * a.fnr[w + w + 1] / a.fnr[n1 + n1 + 1];
             int i = (n + n1 - w) % 2 + 1;

@@ -5,6 +5,7 @@
 // translation constants vcc_const, fnm1_const, fn_const, fnp1_const
 // (axialtrancoefinit, modules:1680-1722).
 #include "tables.h"
+#include "vcoupling.cuh"
 #include <cmath>
 #include <cstdlib>
 
@@ -30,66 +31,12 @@ Tables::Tables(int nbc_) : nbc(nbc_)
 
 void Tables::vcfuncuprec(int m, int n, int k, int l, int wmax, double* vcn) const
 {
-    int mk = std::abs(m + k), nl = std::abs(n - l), w, m1, l1, k1;
-    double vc1;
-    if (nl >= mk) {
-        w = nl;
-        if (n >= l) { m1 = m; l1 = l; k1 = k; }
-        else { m1 = k; k1 = m; l1 = n; }
-        vc1 = pm1(k1 + l1) * bc(l1 + k1, w - m1 - k1) * bc(l1 - k1, w + m1 + k1) / bc(l1 + l1, w + w + 1);
-    } else {
-        w = mk;
-        if (m + k >= 0) vc1 = pm1(n + m) * bc(n - l + w, l - k) * bc(l - n + w, n - m) / bc(w + w + 1, n + l - w);
-        else vc1 = pm1(l + k) * bc(n - l + w, l + k) * bc(l - n + w, n + m) / bc(w + w + 1, n + l - w);
-    }
-    int w1 = w;
-    vcn[w] = vc1;
-    w = w1 + 1;
-    mk = m + k;
-    int w2 = wmax < n + l ? wmax : n + l;
-    auto t1f = [&](int w) {
-        return 2 * w * fnr[w + w + 1] * fnr[w + w - 1] /
-               (fnr[w + mk] * fnr[w - mk] * fnr[n - l + w] * fnr[l - n + w] * fnr[n + l - w + 1] * fnr[n + l + w + 1]);
-    };
-    auto t2f = [&](int w) { return (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1)); };
-    auto t3f = [&](int w) {
-        return fnr[w - mk - 1] * fnr[w + mk - 1] * fnr[l - n + w - 1] * fnr[n - l + w - 1] * fnr[n + l - w + 2] * fnr[n + l + w] /
-               ((double)(2 * (w - 1)) * fnr[2 * w - 3] * fnr[2 * w - 1]);
-    };
-    if (w2 > w1) {
-        double t1 = t1f(w);
-        double t2 = (w1 == 0) ? 0.5 * (double)(m - k) : t2f(w);
-        vcn[w] = t1 * t2 * vcn[w1];
-    }
-    for (w = w1 + 2; w <= w2; w++) vcn[w] = t1f(w) * (t2f(w) * vcn[w - 1] - t3f(w) * vcn[w - 2]);
+    vc_uprec(VCTab{bcof.data(), fnr.data(), nbc}, m, n, k, l, wmax, vcn);
 }
 
 void Tables::vcfunc(int m, int n, int k, int l, double* vcn) const
 {
-    for (int w = 0; w <= n + l; w++) vcn[w] = 0.0;
-    int wmax = n + l;
-    int wmin = std::max(std::abs(n - l), std::abs(m + k));
-    vcn[wmax] = bc(n + m, l + k) * bc(n - m, l - k) / bc(n + n, l + l);
-    if (wmin == wmax) return;
-    vcn[wmax - 1] = vcn[wmax] * (l * m - k * n) * fnr[2 * (l + n) - 1] / fnr[l] / fnr[n] / fnr[n + l + m + k] / fnr[n + l - m - k];
-    if (wmin == wmax - 1) return;
-    int mk = m + k;
-    double vcmax = std::fabs(vcn[wmax]) + std::fabs(vcn[wmax - 1]);
-    int w;
-    for (w = wmax; w >= wmin + 2; w--) {
-        double t1 = 2 * w * fnr[w + w + 1] * fnr[w + w - 1] /
-                    (fnr[w + mk] * fnr[w - mk] * fnr[n - l + w] * fnr[l - n + w] * fnr[n + l - w + 1] * fnr[n + l + w + 1]);
-        double t2 = (double)((m - k) * w * (w - 1) - mk * n * (n + 1) + mk * l * (l + 1)) / (double)(2 * w * (w - 1));
-        double t3 = fnr[w - mk - 1] * fnr[w + mk - 1] * fnr[l - n + w - 1] * fnr[n - l + w - 1] * fnr[n + l - w + 2] * fnr[n + l + w] /
-                    ((double)(2 * (w - 1)) * fnr[2 * w - 3] * fnr[2 * w - 1]);
-        vcn[w - 2] = (t2 * vcn[w - 1] - vcn[w] / t1) / t3;
-        if ((wmax - w) % 2 == 1) {
-            double vctest = std::fabs(vcn[w - 2]) + std::fabs(vcn[w - 1]);
-            vcmax = vcmax > vctest ? vcmax : vctest;
-            if (vctest / vcmax < 0.01) break;
-        }
-    }
-    if (w - 2 > wmin) vcfuncuprec(m, n, k, l, w - 3, vcn);
+    vc_func(VCTab{bcof.data(), fnr.data(), nbc}, m, n, k, l, vcn);
 }
 
 void Tables::axial_constants(int nmax, std::vector<double>& vcc, std::vector<double>& fnm1, std::vector<double>& fnc,

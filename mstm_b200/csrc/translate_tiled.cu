@@ -74,6 +74,30 @@ template <> __device__ __forceinline__ void red_add<double>(cpx<double>* p, cpx<
     atomicAdd(&p->y, v.y);
 }
 
+// Multiply-accumulates of the passes: acc + r v (real r) and acc + z v
+// (complex z).  FP32 values go through the packed two-lane FMA of sm_100
+// (one instruction for both halves of a complex number); FP64 through
+// scalar FMAs.
+template <typename T> __device__ __forceinline__ cpx<T> mac_r(cpx<T> acc, T r, cpx<T> v)
+{
+    return mk(fma(r, v.x, acc.x), fma(r, v.y, acc.y));
+}
+template <> __device__ __forceinline__ cpx<float> mac_r<float>(cpx<float> acc, float r, cpx<float> v)
+{
+    const float2 o = __ffma2_rn(make_float2(r, r), make_float2(v.x, v.y), make_float2(acc.x, acc.y));
+    return mk(o.x, o.y);
+}
+template <typename T> __device__ __forceinline__ cpx<T> mac_c(cpx<T> acc, cpx<T> z, cpx<T> v)
+{
+    return mk(fma(z.x, v.x, fma(-z.y, v.y, acc.x)), fma(z.x, v.y, fma(z.y, v.x, acc.y)));
+}
+template <> __device__ __forceinline__ cpx<float> mac_c<float>(cpx<float> acc, cpx<float> z, cpx<float> v)
+{
+    float2 o = __ffma2_rn(make_float2(-z.y, z.y), make_float2(v.y, v.x), make_float2(acc.x, acc.y));
+    o = __ffma2_rn(make_float2(z.x, z.x), make_float2(v.x, v.y), o);
+    return mk(o.x, o.y);
+}
+
 // degree offsets in the packed per-column arrays
 __host__ __device__ constexpr int sofs(int n) { return (n - 1) * (n + 2) / 2; }   // S/P: m = 0..n
 __host__ __device__ constexpr int tofs(int n) { return (n - 1) * n / 2; }         // T/Q: m = 1..n
@@ -285,10 +309,10 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
                 cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
 #pragma unroll
                 for (int mm = 0; mm <= L; mm++)
-                    if (mm <= n) P = P + er[mm] * sv[mm];
+                    if (mm <= n) P = mac_r(P, er[mm], sv[mm]);
 #pragma unroll
                 for (int mm = 0; mm < L; mm++)
-                    if (mm < n) Q = Q + orr[mm] * tv[mm];
+                    if (mm < n) Q = mac_r(Q, orr[mm], tv[mm]);
                 cpx<T>* ap = W2 + c * NB2;
                 if (k == 0) {
                     ap[hidx<L>(0, n)] = P;
@@ -325,8 +349,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
                 for (int u = 0; u < dim; u++) {
                     const cpx<T> z = mk(z0[u * zst], z0[u * zst + 1]);
                     const int h = (L + 2) * u;   // hidx(0, 1+u)
-                    g0 = g0 + z * a0[h];
-                    g1 = g1 + z * a1[h];
+                    g0 = mac_c(g0, z, a0[h]);
+                    g1 = mac_c(g1, z, a1[h]);
                 }
                 o0[sofs(line)] = g0;
                 o1[sofs(line)] = g1;
@@ -337,10 +361,10 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
                     const cpx<T> za = mk(z0[u * zst], z0[u * zst + 1]);
                     const cpx<T> zb = mk(z1[u * zst], z1[u * zst + 1]);
                     const int hp = hp0 + (L + 2) * u, hm = hm0 + u;
-                    gp0 = gp0 + za * a0[hp];   // mode 0, +m: Z_m[0]
-                    gm0 = gm0 + zb * a0[hm];   // mode 0, -m: Z_m[1]
-                    gp1 = gp1 + zb * a1[hp];   // mode 1, +m: Z_m[1]
-                    gm1 = gm1 + za * a1[hm];   // mode 1, -m: Z_m[0]
+                    gp0 = mac_c(gp0, za, a0[hp]);   // mode 0, +m: Z_m[0]
+                    gm0 = mac_c(gm0, zb, a0[hm]);   // mode 0, -m: Z_m[1]
+                    gp1 = mac_c(gp1, zb, a1[hp]);   // mode 1, +m: Z_m[1]
+                    gm1 = mac_c(gm1, za, a1[hm]);   // mode 1, -m: Z_m[0]
                 }
                 const T sg = (m & 1) ? (T)-1 : (T)1;
                 const int so = sofs(line) + m, to = NS + tofs(line) + m - 1;
@@ -389,10 +413,10 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
                 cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
 #pragma unroll
                 for (int mm = 0; mm <= L; mm++)
-                    if (mm <= n) P = P + ec[mm] * sv[mm];
+                    if (mm <= n) P = mac_r(P, ec[mm], sv[mm]);
 #pragma unroll
                 for (int mm = 0; mm < L; mm++)
-                    if (mm < n) Q = Q + oc[mm] * tv[mm];
+                    if (mm < n) Q = mac_r(Q, oc[mm], tv[mm]);
                 const int slot = dir ? sj : si;
                 cpx<T>* acc = ACC + (slot * NR + r) * NB + p * NB2;
                 if (k == 0) {

@@ -6,7 +6,10 @@
 //
 // Forward and backward passes are composed on the host from these primitives:
 //   nn_gemm        C (+)= op(A) op(B), FP32 activations, weights in BF16 (or
-//                  FP32 for the gradient check), FP32 accumulation; 64x64
+//                  FP32 for the gradient check), FP32 accumulation: the
+//                  activation products with BF16 weights on the tensor cores
+//                  (tcgen05 kind::f16, activations as BF16 hi + lo), the
+//                  rest (weight gradients, FP32 weights) in 64x64 CUDA-core
 //                  tiles, split-K with FP32 atomics for the weight gradients
 //   nn_bias_act    Y = act(Z + b) (identity or SiLU), keeps Z for backward
 //   nn_act_back    dZ = dY * act'(Z)
@@ -92,6 +95,151 @@ __global__ void __launch_bounds__(256) nn_gemm_kernel(int M, int N, int K, const
                 else *c = acc[p][q];
             }
         }
+}
+
+// ---------------------------------------------------------------------------
+// The network's activation products on the tensor cores: C[M x N] (+)= A op(B)
+// with A FP32 activations (row-major) split into BF16 hi + lo parts, B the
+// BF16 weights, FP32 accumulation in tensor memory (tcgen05.mma kind::f16).
+// One CTA per 128-row tile and up to 256 output columns (one accumulator in
+// 256 tensor-memory columns); K in chunks of 16 staged by the CTA's threads into shared
+// memory in the MMA's K-major layout (core matrices of 8 rows x 16 bytes),
+// double-buffered: the next chunk is written while the MMAs of the current
+// one run.  Every wait is bounded.
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ uint32_t nn_su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool nn_mb_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool nn_mb_wait(uint32_t bar, uint32_t parity)
+{
+    for (int it = 0; it < (1 << 22); ++it)
+        if (nn_mb_try(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ uint64_t nn_sdesc(uint32_t saddr)
+{
+    // K-major, no swizzle: LBO 128 bytes (the two core matrices of a K step), SBO 256 bytes (8-row groups)
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(256u >> 4) << 32) | (1ull << 46);
+}
+// kind::f16 with BF16 A and B, FP32 D, both K-major, M = 128
+__device__ __forceinline__ uint32_t nn_idesc(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ int nn_off(int r, int k) { return (r >> 3) * 256 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2; }
+}  // namespace
+
+#define NN_TC_MAXN 256
+template <bool TB>
+__global__ void __launch_bounds__(128) nn_gemm_tc_kernel(int M, int N, int K, const float* A, int lda, const __nv_bfloat16* B, int ldb,
+                                                         float* C, int ldc, int accumulate, int* err)
+{
+    // per buffer: A hi, A lo (128 x 16 BF16 = 4 KB each), B (up to 256 x 16 BF16 = 8 KB)
+    __shared__ __align__(1024) unsigned char sbuf[2][8192 + 8192];
+    __shared__ __align__(8) uint64_t bars[3];
+    __shared__ uint32_t tmem_holder;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * NN_TC_MAXN;
+    const int ncols = min(NN_TC_MAXN, N - n0);
+    const int npad = (ncols + 15) / 16 * 16;
+    const int nseg = (npad + 255) / 256;
+    if (tid == 0) {
+        for (int b = 0; b < 3; b++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(nn_su32(&bars[b])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(nn_su32(&tmem_holder)), "r"(256));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tbase = tmem_holder;
+    const int nk = (K + 15) / 16;
+    bool ok = true;
+    for (int kc = 0; kc < nk; kc++) {
+        const int b = kc & 1;
+        // the MMAs that read this buffer two chunks ago are done
+        if (kc >= 2 && !nn_mb_wait(nn_su32(&bars[b]), (uint32_t)(((kc - 2) >> 1) & 1))) ok = false;
+        unsigned char* ah = sbuf[b];
+        unsigned char* al = sbuf[b] + 4096;
+        unsigned char* bs = sbuf[b] + 8192;
+        const int k0 = kc * 16;
+        for (int e = tid; e < 128 * 16; e += 128) {
+            const int r = e >> 4, k = e & 15;
+            float v = 0.0f;
+            if (m0 + r < M && k0 + k < K) v = A[(size_t)(m0 + r) * lda + k0 + k];
+            const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+            const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+            *reinterpret_cast<__nv_bfloat16*>(ah + nn_off(r, k)) = hi;
+            *reinterpret_cast<__nv_bfloat16*>(al + nn_off(r, k)) = lo;
+        }
+        for (int e = tid; e < npad * 16; e += 128) {
+            const int nn = e >> 4, k = e & 15;
+            __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+            const int j = n0 + nn, kk = k0 + k;
+            if (nn < ncols && kk < K) v = TB ? B[(size_t)j * ldb + kk] : B[(size_t)kk * ldb + j];
+            *reinterpret_cast<__nv_bfloat16*>(bs + nn_off(nn, k)) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic writes -> the tensor cores' reads
+        __syncthreads();
+        if (tid == 0 && ok) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int sg = 0; sg < nseg; sg++) {
+                const int nw = min(256, npad - sg * 256);
+                const uint32_t d = tbase + (uint32_t)(sg * 256);
+                const uint64_t bd = nn_sdesc(nn_su32(bs) + (uint32_t)(sg * 256 / 8) * 256u);
+                const uint32_t idesc = nn_idesc(nw), acc0 = kc > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d),
+                    "l"(nn_sdesc(nn_su32(ah))), "l"(bd), "r"(idesc), "r"(acc0), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d),
+                    "l"(nn_sdesc(nn_su32(al))), "l"(bd), "r"(idesc), "r"(1u), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(nn_su32(&bars[b])) : "memory");
+        }
+    }
+    // all MMAs done: the last commit covers every earlier one of this thread
+    if (tid == 0 && ok) asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(nn_su32(&bars[2])) : "memory");
+    if (!(ok && nn_mb_wait(nn_su32(&bars[2]), 0u))) ok = false;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        const int r = warp * 32 + lane;
+        for (int c0 = 0; c0 < npad; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t ta = tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)((c0 / 256) * 256 + c0 % 256);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]),
+                  "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(ta));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m0 + r < M) {
+                float* c = C + (size_t)(m0 + r) * ldc + n0;
+#pragma unroll
+                for (int q = 0; q < 16; q++)
+                    if (c0 + q < ncols) c[c0 + q] = (accumulate ? c[c0 + q] : 0.0f) + __uint_as_float(v[q]);
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, MSTMG_ERR_CUDA);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(256));
 }
 
 __global__ void nn_bias_act_kernel(int M, int N, const float* Z, const float* b, float* Y, int act)
@@ -229,11 +377,27 @@ __global__ void nn_knn_kernel(int n, int k, const int* cfg_start, const int* sph
 // ---------------------------------------------------------------------------
 static int grid1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 32); }
 
+static int* nn_err_flag()
+{
+    static int* p = nullptr;   // device status word of the tensor-core products (set on a wait that gave up)
+    if (!p && cudaMalloc((void**)&p, sizeof(int)) == cudaSuccess) cudaMemset(p, 0, sizeof(int));
+    return p;
+}
+
 extern "C" int mstmg_nn_gemm(int M, int N, int K, const float* A, int lda, int transA, const void* B, int ldb, int transB, int b_bf16,
                              float* C, int ldc, int accumulate, void* stream)
 {
     if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C) return MSTMG_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
+    // activation products with BF16 weights: the tensor cores
+    if (b_bf16 && !transA && nn_err_flag()) {
+        dim3 grid((M + 127) / 128, (N + NN_TC_MAXN - 1) / NN_TC_MAXN);
+        const __nv_bfloat16* Bw = (const __nv_bfloat16*)B;
+        if (transB) nn_gemm_tc_kernel<true><<<grid, 128, 0, st>>>(M, N, K, A, lda, Bw, ldb, C, ldc, accumulate, nn_err_flag());
+        else nn_gemm_tc_kernel<false><<<grid, 128, 0, st>>>(M, N, K, A, lda, Bw, ldb, C, ldc, accumulate, nn_err_flag());
+        launch_counter() += 1;
+        return cudaGetLastError() == cudaSuccess ? MSTMG_OK : MSTMG_ERR_CUDA;
+    }
     dim3 grid((N + NN_TN - 1) / NN_TN, (M + NN_TM - 1) / NN_TM, 1);
     int tiles = grid.x * grid.y;
     int splits = 1;
