@@ -671,11 +671,11 @@ def run_translation_case(args):
         w = C.workload(args.workload)
     prec = "mixed" if args.precision == "tc" else args.precision
     g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=-w["order"], precision=prec,
-                          fp32_chunk=args.fp32_chunk, tile_ctas_per_sm=args.ctas_per_sm)
+                          fp32_chunk=args.fp32_chunk, tile_ctas_per_sm=args.ctas_per_sm, tile_pairs=args.tile_pairs)
     ms = g.time_translation(args.precision, args.nrhs, args.translation_passes)
     sb, cb = g.operator_bytes(prec)
     print(json.dumps({"workload": args.workload, "precision": args.precision, "nrhs": args.nrhs, "fp32_chunk": args.fp32_chunk,
-                      "ctas_per_sm": args.ctas_per_sm, "ms_per_pass": ms, "operator_bytes": sb, "operator_gbs": sb / ms / 1e6}))
+                      "ctas_per_sm": args.ctas_per_sm, "tile_pairs": args.tile_pairs, "ms_per_pass": ms, "operator_bytes": sb, "operator_gbs": sb / ms / 1e6}))
     g.close()
 
 
@@ -716,6 +716,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "tc"])
     ap.add_argument("--fp32-chunk", type=int, default=0, help="profiling case: FP32 column chunk (2 or 4; 0 default)")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="profiling case: tiled kernel CTAs per SM (0 default)")
+    ap.add_argument("--tile-pairs", type=int, default=0, help="profiling case: pairs per step of the tiled kernel (0 default)")
     ap.add_argument("--nrhs", type=int, default=4)
     ap.add_argument("--tmatrix-case", type=int, default=0, help="profiling case: one T matrix of this many spheres")
     ap.add_argument("--tensor-core", type=int, default=0, help="profiling case: 0 tensor-core passes where they apply, -1 never")

@@ -66,6 +66,9 @@ typedef struct {
                                       inside FP64 refinement */
     int gmres_restart;             /* mixed_solver 2: Arnoldi steps per cycle at most (0: up to 200, fewer
                                       when a quarter of the free device memory cannot hold the basis) */
+    int tile_pairs;                /* pairs of a tile the tiled kernel handles per step, its four phases and
+                                      barriers shared: 2 for FP32 passes of one or two columns when set to 2,
+                                      otherwise 1 (the default: faster at three CTAs per SM) */
     int tensor_core;               /* FP32 passes of 12 or more plain columns (the T-matrix GMRES) on the
                                       tensor cores with dense TF32 hi/lo pair operators: 0 when the context
                                       qualifies (one sphere order 5..10, direct pairs) and the operators fit

@@ -80,7 +80,7 @@ class MstmgOpts(ctypes.Structure):
     _fields_ = [("precision", c_int), ("device", c_int), ("medium_re", c_double), ("medium_im", c_double),
                 ("translation_switch_order", c_int), ("inner_eps", c_double), ("max_outer", c_int),
                 ("generic_kernel", c_int), ("tile_ctas_per_sm", c_int), ("fp32_chunk", c_int),
-                ("mixed_solver", c_int), ("gmres_restart", c_int), ("tensor_core", c_int)]
+                ("mixed_solver", c_int), ("gmres_restart", c_int), ("tile_pairs", c_int), ("tensor_core", c_int)]
 
 
 class MstmgError(RuntimeError):

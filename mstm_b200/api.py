@@ -100,7 +100,7 @@ class SphereCluster(_Context):
 
     def __init__(self, positions, radii, ref_index, mie_epsilon=1.0e-6, precision="fp64", device=0,
                  medium_index=1.0, inner_eps=1.0e-8, max_outer=30, generic_kernel=False, tile_ctas_per_sm=0, fp32_chunk=0,
-                 mixed_solver=2, gmres_restart=0, tensor_core=0):
+                 mixed_solver=2, gmres_restart=0, tensor_core=0, tile_pairs=0):
         self._L = _lib.lib()
         pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
         rad = np.ascontiguousarray(np.asarray(radii, np.float64).reshape(-1))
@@ -123,6 +123,7 @@ class SphereCluster(_Context):
         opts.mixed_solver = int(mixed_solver)
         opts.gmres_restart = int(gmres_restart)
         opts.tensor_core = int(tensor_core)
+        opts.tile_pairs = int(tile_pairs)
         self.ctx = ctypes.c_void_p()
         check(self._L.mstmg_ctx_create(ctypes.byref(self.ctx), n, _ptr(pos), _ptr(rad), _ptr(ri2), float(mie_epsilon),
                                        ctypes.byref(opts)), "mstmg_ctx_create")

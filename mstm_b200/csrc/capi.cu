@@ -22,6 +22,7 @@ extern "C" void mstmg_default_opts(mstmg_opts* o)
     o->fp32_chunk = 0;
     o->mixed_solver = 2;
     o->gmres_restart = 0;
+    o->tile_pairs = 0;
     o->tensor_core = 0;
 }
 
@@ -398,8 +399,8 @@ static int create_impl(mstmg_ctx** out, int nsphere, const double* pos, const do
         }
     }
     if (opts && (opts->gmres_restart < 0 || opts->mixed_solver < 0 || opts->mixed_solver > 2 || opts->tensor_core < -1 ||
-                 opts->tensor_core > 1)) {
-        set_err("mstmg_ctx_create: gmres_restart must be >= 0, mixed_solver 0, 1 or 2 and tensor_core -1, 0 or 1");
+                 opts->tensor_core > 1 || opts->tile_pairs < 0 || opts->tile_pairs > 2)) {
+        set_err("mstmg_ctx_create: gmres_restart must be >= 0, mixed_solver 0, 1 or 2, tensor_core -1, 0 or 1, tile_pairs 0, 1 or 2");
         return MSTMG_ERR_ARG;
     }
     mstmg_ctx* c = new mstmg_ctx();

@@ -141,6 +141,7 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
         ta.ctas_per_sm = c->opts.tile_ctas_per_sm;
         ta.tsph = c->tsph.p;
         ta.pslot = c->pslot.p;
+        ta.pairs_per_step = c->opts.tile_pairs;
     }
     if (nchunk > 1 && !use_tiled) return MSTMG_ERR_UNSUPPORTED;
     cudaEvent_t e0 = nullptr, e1 = nullptr;

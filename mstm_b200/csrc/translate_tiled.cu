@@ -110,13 +110,19 @@ template <int L> __host__ __device__ constexpr int hidx(int m, int n) { return m
 // columns (80 registers; the extra resident warps hide the pass's latencies:
 // fractal500 FP32, 2 columns, 2.27 -> 1.88 ms), 2 otherwise (FP64 and four
 // FP32 columns slow down at the smaller budget: FP64 2 columns 2.9 -> 4.1 ms).
-template <typename T, int NR> __host__ __device__ constexpr int tiled_minb() { return (sizeof(T) == 4 && NR <= 2) ? 3 : 2; }
+// With two pairs a step the shared memory holds two CTAs per SM, which get
+// the 128-register budget.
+template <typename T, int NR, int PP> __host__ __device__ constexpr int tiled_minb() { return (sizeof(T) == 4 && NR <= 2 && PP == 1) ? 3 : 2; }
 
-template <typename T, int L, int NR, int B>
-__global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kernel(TiledArgs<T> a)
+// One CTA works through whole tiles, PP pairs of a tile at a time (a step):
+// consecutive pairs whose output slots are disjoint share one step, so the
+// four phases and their barriers serve both (PP = 2), which fills the
+// threads of the rotation phases and halves the barriers per pair.
+template <typename T, int L, int NR, int B, int PP>
+__global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_kernel(TiledArgs<T> a)
 {
     constexpr int NT = 256;
-    constexpr int C = 4 * NR;            // columns: ((dir*NR)+r)*2+p
+    constexpr int C = 4 * NR;            // columns of a pair: ((dir*NR)+r)*2+p
     constexpr int CB = 4;                // columns per item in the rotations
     constexpr int NG = C / CB;
     constexpr int NS = L * (L + 3) / 2;  // (n, k>=0) rows
@@ -128,6 +134,7 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
     constexpr int NSLOT = 2 * B;
     constexpr uint32_t RECB = (uint32_t)(REC * sizeof(T));
     constexpr uint32_t XB = (uint32_t)(NB * sizeof(cpx<T>));   // one sphere block of one rhs
+    constexpr int WP = C * NB2;          // one pair's share of W1 / W2
 
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm);          // [0],[1] operators, [2] sources
@@ -136,15 +143,15 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
     short2* tabC = tabQ + NQ;                                  // NS entries (m, line), m = 0..L, line = max(1,m)..L
     size_t off = 64 + sizeof(short2) * (NS + NQ + NS);
     off = (off + 127) & ~(size_t)127;
-    cpx<T>* ephm = reinterpret_cast<cpx<T>*>(sm + off);       // 2L+1
-    off += sizeof(cpx<T>) * (2 * L + 1);
+    cpx<T>* ephm = reinterpret_cast<cpx<T>*>(sm + off);       // PP x (2L+1)
+    off += sizeof(cpx<T>) * PP * (2 * L + 1);
     off = (off + 127) & ~(size_t)127;
-    T* opb = reinterpret_cast<T*>(sm + off);                  // 2 x REC
-    off += sizeof(T) * 2 * REC;
+    T* opb = reinterpret_cast<T*>(sm + off);                  // 2 buffers x PP records
+    off += sizeof(T) * 2 * PP * REC;
     off = (off + 127) & ~(size_t)127;
-    cpx<T>* W1 = reinterpret_cast<cpx<T>*>(sm + off);         // C x NB2: S/T, then g
-    cpx<T>* W2 = W1 + C * NB2;                                // C x NB2: sources x (2 spheres x NR x NB), then a'
-    cpx<T>* ACC = W2 + C * NB2;                               // NSLOT x NR x NB
+    cpx<T>* W1 = reinterpret_cast<cpx<T>*>(sm + off);         // PP x C x NB2: S/T, then g
+    cpx<T>* W2 = W1 + PP * WP;                                // PP x C x NB2: sources (2 spheres x NR x NB), then a'
+    cpx<T>* ACC = W2 + PP * WP;                               // NSLOT x NR x NB
 
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -176,11 +183,35 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
     if (tcur >= NI) return;
     auto tile_of = [&](int it) { return it / a.nchunk; };
     auto col0 = [&](int it) { return (size_t)(it % a.nchunk) * NR * (size_t)a.ld; };
-    // thread 0's iterators: operators two pairs ahead, sources one pair ahead
+    // output slots of pair qq of work item it
+    auto slots_of = [&](int qq, int it, int& s_i, int& s_j) {
+        if (a.pslot) {
+            const short2 ps = a.pslot[qq];
+            s_i = ps.x;
+            s_j = ps.y;
+        } else {
+            const int4 ti = a.tiles[tile_of(it)];
+            const int2 pr = a.pairs[qq];
+            s_i = pr.x - (ti.z >> 16);
+            s_j = ti.w ? (pr.y - (ti.z >> 16)) : (B + pr.y - (ti.z & 0xffff));
+        }
+    };
+    // pairs of the step that starts at pair qq: two when the next pair of the
+    // tile writes other slots
+    auto step_np = [&](int qq, int it) -> int {
+        if (PP == 1) return 1;
+        const int4 ti = a.tiles[tile_of(it)];
+        if (qq + 1 >= ti.x + ti.y) return 1;
+        int a1, b1, a2, b2;
+        slots_of(qq, it, a1, b1);
+        slots_of(qq + 1, it, a2, b2);
+        return (a1 != a2 && a1 != b2 && b1 != a2 && b1 != b2) ? 2 : 1;
+    };
+    // thread 0's iterators: operators two steps ahead, sources one step ahead
     int pf_t = tcur, pf_q = a.tiles[tile_of(tcur)].x;
     bool pf_ok = true;
     auto pf_adv = [&]() {
-        pf_q++;
+        pf_q += step_np(pf_q, pf_t);
         const int4 ti = a.tiles[tile_of(pf_t)];
         if (pf_q >= ti.x + ti.y) {
             pf_t += G;
@@ -188,22 +219,28 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
             pf_q = a.tiles[tile_of(pf_t)].x;
         }
     };
+    auto load_ops = [&](int bb) {
+        const int np_ = step_np(pf_q, pf_t);
+        mb_expect(&bar[bb], (uint32_t)np_ * RECB);
+        bulk_copy(opb + (size_t)bb * PP * REC, a.ops + (size_t)pf_q * REC, (uint32_t)np_ * RECB, &bar[bb]);   // consecutive records
+        pf_adv();
+    };
     auto load_sources = [&](int qq, int it) {
-        const int2 pr = a.pairs[qq];
+        const int np_ = step_np(qq, it);
         const cpx<T>* xs = a.x + col0(it);
-        mb_expect(&bar[2], 2u * NR * XB);
-        for (int r = 0; r < NR; r++) {
-            bulk_copy(W2 + (size_t)(0 * NR + r) * NB, xs + (size_t)r * a.ld + (size_t)pr.y * NB, XB, &bar[2]);   // source of j -> i
-            bulk_copy(W2 + (size_t)(1 * NR + r) * NB, xs + (size_t)r * a.ld + (size_t)pr.x * NB, XB, &bar[2]);   // source of i -> j
+        mb_expect(&bar[2], (uint32_t)np_ * 2u * NR * XB);
+        for (int u = 0; u < np_; u++) {
+            const int2 pr = a.pairs[qq + u];
+            cpx<T>* w = W2 + (size_t)u * WP;
+            for (int r = 0; r < NR; r++) {
+                bulk_copy(w + (size_t)(0 * NR + r) * NB, xs + (size_t)r * a.ld + (size_t)pr.y * NB, XB, &bar[2]);   // source of j -> i
+                bulk_copy(w + (size_t)(1 * NR + r) * NB, xs + (size_t)r * a.ld + (size_t)pr.x * NB, XB, &bar[2]);   // source of i -> j
+            }
         }
     };
     if (tid == 0) {
         load_sources(pf_q, tcur);
-        for (int b = 0; b < 2 && pf_ok; b++) {
-            mb_expect(&bar[b], RECB);
-            bulk_copy(opb + b * REC, a.ops + (size_t)pf_q * REC, RECB, &bar[b]);
-            pf_adv();
-        }
+        for (int bb = 0; bb < 2 && pf_ok; bb++) load_ops(bb);
     }
     int q = a.tiles[tile_of(tcur)].x;
     int t = 0;
@@ -212,26 +249,24 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
         const int i0 = tinfo.z >> 16, j0 = tinfo.z & 0xffff;   // block starts
         const int diag = tinfo.w;
         const int b = t & 1;
+        const int np = step_np(q, tcur);
         if (!mb_wait(&bar[b], (t >> 1) & 1) || !mb_wait(&bar[2], t & 1)) {
             if (tid == 0) atomicExch(a.err, MSTMG_ERR_CUDA);
             mb_wait(&bar[b ^ 1], ((t + 1) >> 1) & 1);
             mb_wait(&bar[2], t & 1);
             return;
         }
-        const T* rec = opb + b * REC;
-        int si, sj;
-        if (a.pslot) {
-            const short2 ps = a.pslot[q];
-            si = ps.x;
-            sj = ps.y;
-        } else {
-            const int2 pr = a.pairs[q];
-            si = pr.x - i0;
-            sj = diag ? (pr.y - i0) : (B + pr.y - j0);
+        int si[PP], sj[PP];
+#pragma unroll
+        for (int u = 0; u < PP; u++) {
+            si[u] = 0;
+            sj[u] = 0;
+            if (u < np) slots_of(q + u, tcur, si[u], sj[u]);
         }
-        if (tid == 0) {
+        if (tid < np) {
+            const T* rec = opb + ((size_t)b * PP + tid) * REC;
             cpx<T> ep = mk(rec[0], rec[1]);
-            cpx<T>* e = ephm + L;
+            cpx<T>* e = ephm + (size_t)tid * (2 * L + 1) + L;
             e[0] = mk((T)1, (T)0);
 #pragma unroll
             for (int m = 1; m <= L; m++) {
@@ -240,33 +275,34 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
             }
         }
         __syncthreads();
-        const cpx<T>* e = ephm + L;
 
         // ---- A: shift, phase, even/odd split of the staged sources.  Each
         //      thread takes IA items; all their loads are issued before any
         //      arithmetic, so the shared-memory latencies overlap ----
         {
-            constexpr int NA = C * NS, IA = (NA + NT - 1) / NT;
+            constexpr int NA1 = C * NS, NA = PP * NA1, IA = (NA + NT - 1) / NT;
             cpx<T> U[IA], V[IA], EU[IA];
             int sdst[IA], tdst[IA], mm[IA];   // S and T slots; m, with the shift flag as -m-1
 #pragma unroll
             for (int k = 0; k < IA; k++) {
                 const int idx = tid + k * NT;
                 sdst[k] = -1;
-                if (idx < NA) {
-                    const int c = idx / NS, jj = idx - c * NS;
+                const int u = idx / NA1, li = idx - u * NA1;
+                if (idx < NA && u < np) {
+                    const int c = li / NS, jj = li - c * NS;
                     const short2 nm = tabS[jj];
                     const int n = nm.x, m = nm.y;
                     const int r = (c >> 1) % NR, dir = (c >> 1) / NR;
                     const bool swp = (dir != (int)((a.contran >> r) & 1u));
-                    const cpx<T>* xs = W2 + (size_t)c * NB2;
+                    const cpx<T>* xs = W2 + (size_t)u * WP + (size_t)c * NB2;
+                    const cpx<T>* e = ephm + (size_t)u * (2 * L + 1) + L;
                     const int hp = hidx<L>(m, n), hm = m ? hidx<L>(-m, n) : hp;
                     // with the shift the +m and -m sources trade places (and take the sign (-1)^m)
                     U[k] = xs[swp ? hm : hp];
                     V[k] = xs[swp ? hp : hm];
                     EU[k] = e[dir ? -m : m];
-                    sdst[k] = c * NB2 + sofs(n) + m;
-                    tdst[k] = c * NB2 + NS + tofs(n) + m - 1;
+                    sdst[k] = u * WP + c * NB2 + sofs(n) + m;
+                    tdst[k] = u * WP + c * NB2 + NS + tofs(n) + m - 1;
                     mm[k] = swp ? -m - 1 : m;
                 }
             }
@@ -290,10 +326,12 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
 
         // ---- B: forward rotation: a'(k) = P+Q, a'(-k) = (-1)^k (P-Q),
         //      P = E_n[k][:] s, Q = O_n[k][:] t ----
-        for (int idx = tid; idx < NS * NG; idx += NT) {
-            const int jj = idx / NG, g = idx - jj * NG;
+        for (int idx = tid; idx < np * NS * NG; idx += NT) {
+            const int u = idx / (NS * NG), li = idx - u * (NS * NG);
+            const int jj = li / NG, g = li - jj * NG;
             const short2 nk = tabS[jj];
             const int n = nk.x, k = nk.y;
+            const T* rec = opb + ((size_t)b * PP + u) * REC;
             const T* Er = rec + 2 + op_rot_offset(n, L) + k * (n + 1);
             const T* Or = rec + 2 + op_rot_offset(n, L) + (n + 1) * (n + 1) + (k - 1) * n;
             T er[L + 1], orr[L];
@@ -304,8 +342,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
 #pragma unroll
             for (int cc = 0; cc < CB; cc++) {
                 const int c = g * CB + cc;
-                const cpx<T>* sv = W1 + c * NB2 + sofs(n);
-                const cpx<T>* tv = W1 + c * NB2 + NS + tofs(n);
+                const cpx<T>* sv = W1 + u * WP + c * NB2 + sofs(n);
+                const cpx<T>* tv = W1 + u * WP + c * NB2 + NS + tofs(n);
                 cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
 #pragma unroll
                 for (int mm = 0; mm <= L; mm++)
@@ -313,7 +351,7 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
 #pragma unroll
                 for (int mm = 0; mm < L; mm++)
                     if (mm < n) Q = mac_r(Q, orr[mm], tv[mm]);
-                cpx<T>* ap = W2 + c * NB2;
+                cpx<T>* ap = W2 + u * WP + c * NB2;
                 if (k == 0) {
                     ap[hidx<L>(0, n)] = P;
                 } else {
@@ -330,25 +368,27 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
         //      Z_m[1] applied to both modes, written as the back rotation's
         //      inputs s'(m) = g(m) + (-1)^m g(-m), t'(m) = g(m) - (-1)^m g(-m)
         //      (s'(0) = g(0)) in the packed S/T layout of W1 ----
-        for (int idx = tid; idx < NS * 2 * NR; idx += NT) {
-            const int zr = idx / (2 * NR), dr = idx - zr * (2 * NR);
+        for (int idx = tid; idx < np * NS * 2 * NR; idx += NT) {
+            const int u = idx / (NS * 2 * NR), li = idx - u * (NS * 2 * NR);
+            const int zr = li / (2 * NR), dr = li - zr * (2 * NR);
             const int dir = dr / NR, r = dr - dir * NR;
             const short2 ml = tabC[zr];
             const int m = ml.x, line = ml.y;
             const int m1 = m < 1 ? 1 : m;
             const int dim = L - m1 + 1;
+            const T* rec = opb + ((size_t)b * PP + u) * REC;
             const T* z0 = rec + 2 + RS + 2 * op_z_offset(m, L, L) + (dir ? 2 * (line - m1) : 2 * (line - m1) * dim);
             const T* z1 = z0 + 2 * dim * dim;
             const int zst = dir ? 2 * dim : 2;
-            const cpx<T>* a0 = W2 + (((dir * NR) + r) * 2 + 0) * NB2;
-            const cpx<T>* a1 = W2 + (((dir * NR) + r) * 2 + 1) * NB2;
-            cpx<T>* o0 = W1 + (((dir * NR) + r) * 2 + 0) * NB2;
-            cpx<T>* o1 = W1 + (((dir * NR) + r) * 2 + 1) * NB2;
+            const cpx<T>* a0 = W2 + u * WP + (((dir * NR) + r) * 2 + 0) * NB2;
+            const cpx<T>* a1 = W2 + u * WP + (((dir * NR) + r) * 2 + 1) * NB2;
+            cpx<T>* o0 = W1 + u * WP + (((dir * NR) + r) * 2 + 0) * NB2;
+            cpx<T>* o1 = W1 + u * WP + (((dir * NR) + r) * 2 + 1) * NB2;
             if (m == 0) {
                 cpx<T> g0 = mk((T)0, (T)0), g1 = mk((T)0, (T)0);
-                for (int u = 0; u < dim; u++) {
-                    const cpx<T> z = mk(z0[u * zst], z0[u * zst + 1]);
-                    const int h = (L + 2) * u;   // hidx(0, 1+u)
+                for (int v = 0; v < dim; v++) {
+                    const cpx<T> z = mk(z0[v * zst], z0[v * zst + 1]);
+                    const int h = (L + 2) * v;   // hidx(0, 1+v)
                     g0 = mac_c(g0, z, a0[h]);
                     g1 = mac_c(g1, z, a1[h]);
                 }
@@ -357,10 +397,10 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
             } else {
                 cpx<T> gp0 = mk((T)0, (T)0), gm0 = gp0, gp1 = gp0, gm1 = gp0;
                 const int hp0 = hidx<L>(m, m1), hm0 = hidx<L>(-m, m1);
-                for (int u = 0; u < dim; u++) {
-                    const cpx<T> za = mk(z0[u * zst], z0[u * zst + 1]);
-                    const cpx<T> zb = mk(z1[u * zst], z1[u * zst + 1]);
-                    const int hp = hp0 + (L + 2) * u, hm = hm0 + u;
+                for (int v = 0; v < dim; v++) {
+                    const cpx<T> za = mk(z0[v * zst], z0[v * zst + 1]);
+                    const cpx<T> zb = mk(z1[v * zst], z1[v * zst + 1]);
+                    const int hp = hp0 + (L + 2) * v, hm = hm0 + v;
                     gp0 = mac_c(gp0, za, a0[hp]);   // mode 0, +m: Z_m[0]
                     gm0 = mac_c(gm0, zb, a0[hm]);   // mode 0, -m: Z_m[1]
                     gp1 = mac_c(gp1, zb, a1[hp]);   // mode 1, +m: Z_m[1]
@@ -376,9 +416,9 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
         }
         __syncthreads();
 
-        // ---- the next pair's sources stream into W2 while D runs ----
+        // ---- the next step's sources stream into W2 while D runs ----
         if (tid == 0) {
-            int nq = q + 1, nit = tcur;
+            int nq = q + np, nit = tcur;
             bool have = true;
             if (nq >= tinfo.x + tinfo.y) {
                 nit = tcur + G;
@@ -392,13 +432,17 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
         }
 
         // ---- D: back rotation g'(k) = sum_m s'(m) E_n[m][k] +/- sum_m t'(m) O_n[m][k],
-        //      phase, shift, accumulate into the tile's smem outputs ----
-        for (int idx = tid; idx < NS * NG; idx += NT) {
-            const int jj = idx / NG, g = idx - jj * NG;
+        //      phase, shift, accumulate into the tile's smem outputs (the
+        //      pairs of a step write disjoint slots) ----
+        for (int idx = tid; idx < np * NS * NG; idx += NT) {
+            const int u = idx / (NS * NG), li = idx - u * (NS * NG);
+            const int jj = li / NG, g = li - jj * NG;
             const short2 nk = tabS[jj];
             const int n = nk.x, k = nk.y;
+            const T* rec = opb + ((size_t)b * PP + u) * REC;
             const T* E = rec + 2 + op_rot_offset(n, L);
             const T* O = E + (n + 1) * (n + 1);
+            const cpx<T>* e = ephm + (size_t)u * (2 * L + 1) + L;
             T ec[L + 1], oc[L];
 #pragma unroll
             for (int mm = 0; mm <= L; mm++) ec[mm] = (mm <= n) ? E[mm * (n + 1) + k] : (T)0;
@@ -408,8 +452,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
             for (int cc = 0; cc < CB; cc++) {
                 const int c = g * CB + cc;
                 const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
-                const cpx<T>* sv = W1 + c * NB2 + sofs(n);
-                const cpx<T>* tv = W1 + c * NB2 + NS + tofs(n);
+                const cpx<T>* sv = W1 + u * WP + c * NB2 + sofs(n);
+                const cpx<T>* tv = W1 + u * WP + c * NB2 + NS + tofs(n);
                 cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
 #pragma unroll
                 for (int mm = 0; mm <= L; mm++)
@@ -417,7 +461,7 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
 #pragma unroll
                 for (int mm = 0; mm < L; mm++)
                     if (mm < n) Q = mac_r(Q, oc[mm], tv[mm]);
-                const int slot = dir ? sj : si;
+                const int slot = dir ? (u == 0 ? sj[0] : sj[PP - 1]) : (u == 0 ? si[0] : si[PP - 1]);
                 cpx<T>* acc = ACC + (slot * NR + r) * NB + p * NB2;
                 if (k == 0) {
                     acc[hidx<L>(0, n)] = acc[hidx<L>(0, n)] + (T)2 * P;
@@ -435,15 +479,13 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
         }
         __syncthreads();
 
-        // ---- refill this operator buffer with the pair after next ----
+        // ---- refill this operator buffer with the step after next ----
         if (tid == 0 && pf_ok) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mb_expect(&bar[b], RECB);
-            bulk_copy(opb + b * REC, a.ops + (size_t)pf_q * REC, RECB, &bar[b]);
-            pf_adv();
+            load_ops(b);
         }
         // ---- end of tile: flush the tile's outputs with coalesced atomics ----
-        const bool last = (q + 1 == tinfo.x + tinfo.y);
+        const bool last = (q + np == tinfo.x + tinfo.y);
         if (last) {
             cpx<T>* yc = a.y + col0(tcur);
             for (int idx = tid; idx < NSLOT * NR * NB; idx += NT) {
@@ -462,34 +504,34 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR>()) translate_tiled_kern
             if (tcur >= NI) break;
             q = a.tiles[tile_of(tcur)].x;
         } else {
-            q++;
+            q += np;
         }
         t++;
     }
 }
 
-template <typename T, int L, int NR, int B> static size_t tiled_smem()
+template <typename T, int L, int NR, int B, int PP> static size_t tiled_smem()
 {
     constexpr int NS = L * (L + 3) / 2, NQ = L * (L + 1) / 2, NB2 = L * (L + 2), NB = 2 * NB2, C = 4 * NR;
     size_t off = 64 + sizeof(short2) * (NS + NQ + NS);
     off = (off + 127) & ~(size_t)127;
-    off += sizeof(cpx<T>) * (2 * L + 1);
+    off += sizeof(cpx<T>) * PP * (2 * L + 1);
     off = (off + 127) & ~(size_t)127;
-    off += sizeof(T) * 2 * op_record_units(L, L);
+    off += sizeof(T) * 2 * PP * op_record_units(L, L);
     off = (off + 127) & ~(size_t)127;
-    off += sizeof(cpx<T>) * ((size_t)2 * C * NB2 + (size_t)2 * B * NR * NB);
+    off += sizeof(cpx<T>) * ((size_t)2 * PP * C * NB2 + (size_t)2 * B * NR * NB);
     return off;
 }
 
-template <typename T, int L, int NR, int B> static int launch_one(const TiledArgs<T>& a, int nsm, cudaStream_t st)
+template <typename T, int L, int NR, int B, int PP> static int launch_pp(const TiledArgs<T>& a, int nsm, cudaStream_t st)
 {
-    size_t smem = tiled_smem<T, L, NR, B>();
+    size_t smem = tiled_smem<T, L, NR, B, PP>();
     if (smem > 227 * 1024) return -1;
-    auto kern = translate_tiled_kernel<T, L, NR, B>;
+    auto kern = translate_tiled_kernel<T, L, NR, B, PP>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = (int)((228 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
-    if (per_sm > tiled_minb<T, NR>()) per_sm = tiled_minb<T, NR>();
+    if (per_sm > tiled_minb<T, NR, PP>()) per_sm = tiled_minb<T, NR, PP>();
     if (a.ctas_per_sm >= 1 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
     int blocks = nsm * per_sm;
     if (blocks > a.ntiles * a.nchunk) blocks = a.ntiles * a.nchunk;
@@ -497,6 +539,19 @@ template <typename T, int L, int NR, int B> static int launch_one(const TiledArg
     kern<<<blocks, 256, smem, st>>>(a);
     launch_counter() += 1;
     return 0;
+}
+
+// Two pairs a step only when asked for (FP32 passes of one or two columns):
+// it fills the rotation phases and halves the barriers per pair, but its
+// shared memory leaves two CTAs per SM instead of three, and measured on the
+// 500-sphere aggregate it is slower (FP32, 2 columns: 2.28 against 1.86 ms;
+// 1 column: 1.82 against 1.40 ms).
+template <typename T, int L, int NR, int B> static int launch_one(const TiledArgs<T>& a, int nsm, cudaStream_t st)
+{
+    if constexpr (sizeof(T) == 4 && NR <= 2) {
+        if (a.pairs_per_step == 2) return launch_pp<T, L, NR, B, 2>(a, nsm, st);
+    }
+    return launch_pp<T, L, NR, B, 1>(a, nsm, st);
 }
 
 template <typename T, int L> static int launch_L(const TiledArgs<T>& a, int nsm, cudaStream_t st)

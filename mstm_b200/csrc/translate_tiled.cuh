@@ -20,6 +20,7 @@ template <typename T> struct TiledArgs {
     // tsph[t * 2B + slot] (-1: none), and each pair's (slot of i, slot of j)
     const int* tsph = nullptr;
     const short2* pslot = nullptr;
+    int pairs_per_step = 0;  // 2: two slot-disjoint pairs a step (FP32, one or two columns); otherwise one
 };
 
 bool tiled_supported(int L, int nrhs);

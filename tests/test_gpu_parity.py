@@ -567,3 +567,25 @@ def test_device_driven_cycles_sync_once_per_cycle(api, oracle_mod, name):
     assert np.allclose(rh["qtot"], rd["qtot"], rtol=RTOL_MIXED)
     g.close()
     h.close()
+
+
+@pytest.mark.parametrize("name", ["fractal60", "cluster20"])
+def test_two_pairs_per_step_match_one(api, name):
+    """The tiled kernel with two slot-disjoint pairs of a tile per step (the
+    default for FP32 passes of one or two columns) gives the FP32 pass of
+    one pair per step, and the FP64 pass, to FP32 rounding, for plain and
+    conjugate-transpose columns."""
+    pos, rad, ri, em = _cluster(name)
+    two = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", tile_pairs=2)
+    one = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", tile_pairs=1)
+    rng = np.random.default_rng(9)
+    for ct in ([0], [1], [0, 1], [1, 1]):
+        x = rng.normal(size=(two.number_eqns, len(ct))) + 1j * rng.normal(size=(two.number_eqns, len(ct)))
+        y64 = one.translation_pass(x, ct, "fp64")
+        s = np.abs(y64).max()
+        y2 = two.translation_pass(x, ct, "fp32")
+        y1 = one.translation_pass(x, ct, "fp32")
+        assert np.abs(y2 - y1).max() <= 2e-6 * s, ct
+        assert np.abs(y2 - y64).max() <= 2e-6 * s, ct
+    two.close()
+    one.close()
