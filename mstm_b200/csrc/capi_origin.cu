@@ -351,7 +351,7 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     DevBuf<double> qcol, dsq, qsum, rr;
     DevBuf<zf> B32;
     DevBuf<int> idx;
-    CK(mscr.alloc((size_t)grid * std::max(strm, strd)));
+    CK(mscr.alloc((size_t)grid * merge_chunks(Sord) * std::max(strm, strd)));
     CK(P0.alloc((size_t)2 * TM * (TM + 2) * Sord));
     CK(A0.alloc((size_t)2 * TM * (TM + 2) * Sord));
     CK(PK.alloc((size_t)ne * Smax));

@@ -76,20 +76,30 @@ __global__ void tranorder_kernel(int nsph, const double* pos, const int* order, 
 }
 
 // ---------------------------------------------------------------------------
-// merge to the common origin: one CTA per sphere (grid-stride), scratch per CTA
+// merge to / distribute from the common origin: CTAs over (sphere, chunk of
+// MERGE_PC columns), spheres grid-strided, scratch per CTA.  Per sphere the
+// translation's tables are made once -- e^{i m phi} powers, the regular
+// radial functions, the Wigner-d rows (rotcoef recurrence) and the axial
+// blocks of every degree m (first row and last column by the
+// vector-coupling sums, the interior by the three-term recurrence, as
+// axialtrancoefrecurrence fills them) -- and then applied to the chunk's
+// columns together: forward rotation, axial translation, back rotation,
+// each phase one barrier for all the columns.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
 {
-    extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x;
     const int T = a.T;
-    zd* base = a.scratch + (size_t)blockIdx.x * a.scratch_stride;
+    zd* base = a.scratch + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * a.scratch_stride;
     const bool dist = (a.mode == 1);
+    const int p0 = blockIdx.y * MERGE_PC, np = min(MERGE_PC, a.npol - p0);
+    if (np <= 0) return;
     for (int i = blockIdx.x; i < a.nsph; i += gridDim.x) {
         const int Li = a.order[i];
         const int L = dist ? T : Li;                       // source order
         const int nt = dist ? Li : min(T, a.tord[i]);      // target order
         const int nmin = min(L, nt), nmax = max(L, nt);
+        const int W = 2 * nmin + 1;
         const double sv = dist ? -1.0 : 1.0;               // translation vector: target - source
         const double rv0 = sv * (a.r0[0] - a.pos[3 * i]), rv1 = sv * (a.r0[1] - a.pos[3 * i + 1]), rv2 = sv * (a.r0[2] - a.pos[3 * i + 2]);
         const size_t soff = dist ? 0 : (size_t)a.offset[i];
@@ -97,49 +107,68 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
         // scratch layout
         zd* xi = base;                                        // nt+L+2
         zd* hs = xi + (nmax + L + 4);                         // Bessel scratch 2*(nt+L+2)
-        double* D = (double*)(hs + 2 * (nmax + L + 4));       // Wigner rows: per degree n, (2nmin+1) x (2n+1), restricted index first
+        zd* eph = hs + 2 * (nmax + L + 4);                    // e^{i m phi}, m = -nmax..nmax
+        double* D = (double*)(eph + (2 * nmax + 1));          // Wigner rows: per degree n, W x (2n+1), restricted index first
         size_t dsz = 0;
-        for (int n = 0; n <= nmax; n++) dsz += (size_t)(2 * nmin + 1) * (2 * n + 1);
-        zd* Z = (zd*)(D + dsz + 1);                           // one axial block: 2 x nt x L
-        zd* G = Z + 2 * (size_t)nt * L;                       // g(m, n, p): 2 x nt x (2nmin+1)
-        zd* AP = G + 2 * (size_t)nt * (2 * nmin + 1);         // a'(k, l, p): 2 x L x (2nmin+1)
-        double* dk0 = (double*)(AP + 2 * (size_t)L * (2 * nmin + 1)) + (nmax + 1);
+        for (int n = 0; n <= nmax; n++) dsz += (size_t)W * (2 * n + 1);
+        double* dk0 = D + dsz + 1 + (nmax + 1);
         double* dk01 = dk0 + (2 * nmax + 3);
+        int* dofs = (int*)(dk01 + (nmax + 2));                // offsets of D per degree, nmax + 2 ints
+        zd* Zall = (zd*)(dofs + ((nmax + 3 + 3) & ~3));       // axial blocks, per degree ma: 2 x nt x L
+        zd* AP = Zall + (size_t)(nmin + 1) * 2 * nt * L;      // a'(k, l, q) per column: PC x 2 x L x W
+        zd* G = AP + (size_t)MERGE_PC * 2 * L * W;            // g(m, n, q) per column: PC x 2 x nt x W
         const zd* src = a.amnp;
         __syncthreads();
         if (rr < 1.0e-12) {
             // zero translation of regular functions: copy the overlapping orders (mtransfer)
             int nc = min(L, nt);
-            for (int p = 0; p < a.npol; p++)
-                for (int e = tid; e < nc * (nc + 2); e += PP_NT) {
-                    int n = 1;
-                    while (n * (n + 2) <= e) n++;
-                    int m = e - (n * n - 1) - n;   // e = n(n+1)-1+m ... -> m in -n..n
-                    zd v1 = src[(size_t)p * a.ld + soff + aidx(m, n, 0, L)];
-                    zd v2 = src[(size_t)p * a.ld + soff + aidx(m, n, 1, L)];
-                    if (dist) {
-                        zd* o = a.out + (size_t)p * a.ldo + a.offset[i];
-                        o[aidx(m, n, 0, nt)] = v1;
-                        o[aidx(m, n, 1, nt)] = v2;
-                        continue;
-                    }
-                    int s = aidx(m, n, 0, T);
-                    atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s].x, v1.x + v2.x);
-                    atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s].y, v1.y + v2.y);
-                    atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s + T * (T + 2)].x, v1.x - v2.x);
-                    atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s + T * (T + 2)].y, v1.y - v2.y);
+            for (int e = tid; e < np * nc * (nc + 2); e += PP_NT) {
+                const int pc = e / (nc * (nc + 2)), ee = e - pc * (nc * (nc + 2));
+                const int p = p0 + pc;
+                int n = 1;
+                while (n * (n + 2) <= ee) n++;
+                int m = ee - (n * n - 1) - n;   // ee = n(n+1)-1+m ... -> m in -n..n
+                zd v1 = src[(size_t)p * a.ld + soff + aidx(m, n, 0, L)];
+                zd v2 = src[(size_t)p * a.ld + soff + aidx(m, n, 1, L)];
+                if (dist) {
+                    zd* o = a.out + (size_t)p * a.ldo + a.offset[i];
+                    o[aidx(m, n, 0, nt)] = v1;
+                    o[aidx(m, n, 1, nt)] = v2;
+                    continue;
                 }
+                int s_ = aidx(m, n, 0, T);
+                atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s_].x, v1.x + v2.x);
+                atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s_].y, v1.y + v2.y);
+                atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s_ + T * (T + 2)].x, v1.x - v2.x);
+                atomicAdd(&a.amnp0[(size_t)p * a.ld0 + s_ + T * (T + 2)].y, v1.y - v2.y);
+            }
             __syncthreads();
             continue;
         }
         const double r = sqrt(rr);
         const double ct = rv2 / r;
-        zd ephi = (rv0 == 0.0 && rv1 == 0.0) ? mk(1.0, 0.0) : mk(rv0 / sqrt(rv0 * rv0 + rv1 * rv1), rv1 / sqrt(rv0 * rv0 + rv1 * rv1));
-        // Bessel functions psi_n(r)/r (cricbessel), n = 0..nt+L
+        const zd ephi = (rv0 == 0.0 && rv1 == 0.0) ? mk(1.0, 0.0) : mk(rv0 / sqrt(rv0 * rv0 + rv1 * rv1), rv1 / sqrt(rv0 * rv0 + rv1 * rv1));
+        // Bessel functions psi_n(r)/r (cricbessel), n = 0..nt+L; e^{i m phi}; degree offsets of D
         if (tid == 0) {
             zd z = mk(r * a.rimed_re, r * a.rimed_im);
             mstm_cricbessel(nt + L, z, xi, hs);
             for (int k = 0; k <= nt + L; k++) xi[k] = cdiv(xi[k], z);
+        }
+        if (tid == 32) {
+            zd* e = eph + nmax;
+            e[0] = mk(1.0, 0.0);
+            for (int m = 1; m <= nmax; m++) {
+                e[m] = ephi * e[m - 1];
+                e[-m] = cj(e[m]);
+            }
+        }
+        if (tid == 64) {
+            int o = W;   // degree 0 occupies W x 1 but only its centre matters
+            dofs[0] = 0;
+            for (int n = 1; n <= nmax; n++) {
+                dofs[n] = o;
+                o += W * (2 * n + 1);
+            }
         }
         // Wigner-d rows by the rotcoef recurrence (kmax = nmin, nmax)
         {
@@ -151,8 +180,7 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
             __syncthreads();
             int sgn = 1;
             double sben = 1.0;
-            size_t doff = 1;   // degree 0 occupies (2nmin+1) x 1 but only its centre matters
-            doff = (size_t)(2 * nmin + 1);
+            size_t doff = (size_t)W;
             for (int n = 1; n <= nmax; n++) {
                 int kk = min(n, nmin);
                 int ld = 2 * n + 1;
@@ -194,127 +222,125 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
                     }
                     __syncthreads();
                 }
-                doff += (size_t)(2 * nmin + 1) * ld;
+                doff += (size_t)W * ld;
             }
         }
         __syncthreads();
-        // degree offsets of D
-        auto dofs = [&](int n) -> size_t {
-            size_t o = (size_t)(2 * nmin + 1);
-            for (int q = 1; q < n; q++) o += (size_t)(2 * nmin + 1) * (2 * q + 1);
-            return o;
-        };
-        for (int p = 0; p < a.npol; p++) {
-            const zd* x = src + (size_t)p * a.ld + soff;
-            // phase (shift_op = F: e^{+i m phi} on the source) and forward rotation of degrees l <= L
-            for (int e = tid; e < 2 * L * (2 * nmin + 1); e += PP_NT) {
-                int q = e / (L * (2 * nmin + 1));
-                int rem = e - q * L * (2 * nmin + 1);
-                int l = rem / (2 * nmin + 1) + 1;
-                int k = rem % (2 * nmin + 1) - nmin;
-                int n1 = min(l, nt);
-                zd acc = mk(0.0, 0.0);
-                if (abs(k) <= n1) {
-                    const double* Dl = D + dofs(l);
-                    zd ep = mk(1.0, 0.0);
-                    // a_tt(m) = a(m) e^{i m phi}; sum over m = -l..l
-                    for (int m = -l; m <= l; m++) {
-                        zd em = mk(1.0, 0.0);
-                        int am = m < 0 ? -m : m;
-                        for (int s = 0; s < am; s++) em = ephi * em;
-                        if (m < 0) em = cj(em);
-                        zd v = x[aidx(m, l, q, L)] * em;
-                        acc = acc + Dl[(k + nmin) * (2 * l + 1) + (m + l)] * v;
-                    }
-                    (void)ep;
-                }
-                AP[(q * L + (l - 1)) * (2 * nmin + 1) + (k + nmin)] = acc;
+        // axial blocks of every degree ma (regular functions), kept for all columns
+        for (int ma = 0; ma <= nmin; ma++) {
+            zd* Z = Zall + (size_t)ma * 2 * nt * L;
+            int m1 = max(1, ma);
+            int rows = nt - m1 + 1, cols = L - m1 + 1;
+            // first row n = m1 and last column l = L
+            for (int e = tid; e < cols + (rows - 1); e += PP_NT) {
+                int n, l;
+                if (e < cols) { n = m1; l = m1 + e; }
+                else { n = m1 + 1 + (e - cols); l = L; }
+                int wmin = abs(n - l), wmax = n + l, ml = l * (l + 1) + ma;
+                zd s1 = mk(0.0, 0.0), s2 = mk(0.0, 0.0);
+                for (int w = wmin; w <= wmax; w += 2) s1 = s1 + a.vcc[(n - 1) + (size_t)a.vcT * ((ml - 1) + (size_t)a.vcML * w)] * xi[w];
+                for (int w = wmin + 1; w <= wmax - 1; w += 2) s2 = s2 + a.vcc[(n - 1) + (size_t)a.vcT * ((ml - 1) + (size_t)a.vcML * w)] * xi[w];
+                s2 = imul(s2);
+                Z[(0 * nt + (n - 1)) * L + (l - 1)] = s1 + s2;
+                Z[(1 * nt + (n - 1)) * L + (l - 1)] = s1 - s2;
             }
             __syncthreads();
-            // axial translation per degree m (regular functions), both signs of m
-            for (int ma = 0; ma <= nmin; ma++) {
-                int m1 = max(1, ma);
-                int rows = nt - m1 + 1, cols = L - m1 + 1;
-                // first row n = m1 and last column l = L
-                for (int e = tid; e < cols + (rows - 1); e += PP_NT) {
-                    int n, l;
-                    if (e < cols) { n = m1; l = m1 + e; }
-                    else { n = m1 + 1 + (e - cols); l = L; }
-                    int wmin = abs(n - l), wmax = n + l, ml = l * (l + 1) + ma;
-                    zd s1 = mk(0.0, 0.0), s2 = mk(0.0, 0.0);
-                    for (int w = wmin; w <= wmax; w += 2) s1 = s1 + a.vcc[(n - 1) + (size_t)a.vcT * ((ml - 1) + (size_t)a.vcML * w)] * xi[w];
-                    for (int w = wmin + 1; w <= wmax - 1; w += 2) s2 = s2 + a.vcc[(n - 1) + (size_t)a.vcT * ((ml - 1) + (size_t)a.vcML * w)] * xi[w];
-                    s2 = imul(s2);
-                    Z[(0 * nt + (n - 1)) * L + (l - 1)] = s1 + s2;
-                    Z[(1 * nt + (n - 1)) * L + (l - 1)] = s1 - s2;
-                }
-                __syncthreads();
-                if (m1 < min(nt, L)) {
-                    for (int n = m1; n <= nt - 1; n++) {
-                        for (int e = tid; e < 2 * (L - m1); e += PP_NT) {
-                            int pp = e / (L - m1), l = m1 + e % (L - m1);
-                            double sp = (pp == 0) ? 1.0 : -1.0;
+            if (m1 < min(nt, L)) {
+                for (int n = m1; n <= nt - 1; n++) {
+                    for (int e = tid; e < 2 * (L - m1); e += PP_NT) {
+                        int pp = e / (L - m1), l = m1 + e % (L - m1);
+                        double sp = (pp == 0) ? 1.0 : -1.0;
 #define ZA(nn, ll) Z[(pp * nt + ((nn) - 1)) * L + ((ll) - 1)]
 #define FC(arr, mm, ll) arr[((mm) + a.fcN) + (2 * a.fcN + 1) * ((ll) - 1)]
-                            zd v = -(ZA(n, l + 1) * FC(a.fnp1, ma, l)) + imul(sp * (FC(a.fnc, ma, l) - FC(a.fnc, ma, n)) * ZA(n, l));
-                            if (l >= m1 + 1) v = v + ZA(n, l - 1) * FC(a.fnm1, ma, l);
-                            if (n > m1) v = v + ZA(n - 1, l) * FC(a.fnm1, ma, n);
-                            double dd = FC(a.fnp1, ma, n);
-                            ZA(n + 1, l) = mk(v.x / dd, v.y / dd);
+                        zd v = -(ZA(n, l + 1) * FC(a.fnp1, ma, l)) + imul(sp * (FC(a.fnc, ma, l) - FC(a.fnc, ma, n)) * ZA(n, l));
+                        if (l >= m1 + 1) v = v + ZA(n, l - 1) * FC(a.fnm1, ma, l);
+                        if (n > m1) v = v + ZA(n - 1, l) * FC(a.fnm1, ma, n);
+                        double dd = FC(a.fnp1, ma, n);
+                        ZA(n + 1, l) = mk(v.x / dd, v.y / dd);
 #undef ZA
 #undef FC
-                        }
-                        __syncthreads();
                     }
+                    __syncthreads();
                 }
-                // g(+ma, n, p) = Z[mode p] a'(+ma) ; g(-ma, n, p) = Z[mode 1-p] a'(-ma)
-                for (int e = tid; e < 2 * 2 * rows; e += PP_NT) {
-                    int sg = e / (2 * rows);
-                    int rem = e - sg * 2 * rows;
-                    int pm = rem / rows, n = m1 + rem % rows;
-                    if (ma == 0 && sg == 1) continue;
-                    int mm = sg ? -ma : ma;
-                    int pz = (ma == 0) ? 0 : (sg == 0 ? pm : 1 - pm);
-                    zd acc = mk(0.0, 0.0);
-                    for (int l = m1; l <= L; l++)
-                        acc = acc + Z[(pz * nt + (n - 1)) * L + (l - 1)] * AP[(pm * L + (l - 1)) * (2 * nmin + 1) + (mm + nmin)];
-                    G[(pm * nt + (n - 1)) * (2 * nmin + 1) + (mm + nmin)] = acc;
-                }
-                __syncthreads();
             }
-            // back rotation per target degree n, phase back, LR -> TE/TM, accumulate
-            for (int e = tid; e < nt * (nt + 2); e += PP_NT) {
-                int n = 1;
-                while (n * (n + 2) <= e) n++;
-                int k = e - (n * n - 1) - n;   // -n..n
-                int n1 = min(n, L);
-                const double* Dn = D + dofs(n);
-                zd gq[2];
-                for (int pm = 0; pm < 2; pm++) {
-                    zd acc = mk(0.0, 0.0);
-                    for (int m = -n1; m <= n1; m++) acc = acc + Dn[(m + nmin) * (2 * n + 1) + (k + n)] * G[(pm * nt + (n - 1)) * (2 * nmin + 1) + (m + nmin)];
-                    // phase back: e^{-i k phi}
-                    zd em = mk(1.0, 0.0);
-                    int ak = k < 0 ? -k : k;
-                    for (int s = 0; s < ak; s++) em = ephi * em;
-                    if (k > 0) em = cj(em);
-                    gq[pm] = acc * em;
-                }
-                if (dist) {
-                    zd* od = a.out + (size_t)p * a.ldo + a.offset[i];
-                    od[aidx(k, n, 0, nt)] = gq[0];
-                    od[aidx(k, n, 1, nt)] = gq[1];
-                    continue;
-                }
-                int s = aidx(k, n, 0, T);
-                zd* o = a.amnp0 + (size_t)p * a.ld0;
-                atomicAdd(&o[s].x, gq[0].x + gq[1].x);
-                atomicAdd(&o[s].y, gq[0].y + gq[1].y);
-                atomicAdd(&o[s + T * (T + 2)].x, gq[0].x - gq[1].x);
-                atomicAdd(&o[s + T * (T + 2)].y, gq[0].y - gq[1].y);
-            }
-            __syncthreads();
         }
+        __syncthreads();
+        const zd* e = eph + nmax;
+        // phase (shift_op = F: e^{+i m phi} on the source) and forward rotation of degrees l <= L, every column
+        for (int it = tid; it < np * 2 * L * W; it += PP_NT) {
+            const int pc = it / (2 * L * W), ee = it - pc * (2 * L * W);
+            int q = ee / (L * W);
+            int rem = ee - q * L * W;
+            int l = rem / W + 1;
+            int k = rem % W - nmin;
+            int n1 = min(l, nt);
+            zd acc = mk(0.0, 0.0);
+            if (abs(k) <= n1) {
+                const double* Dl = D + dofs[l];
+                const zd* x = src + (size_t)(p0 + pc) * a.ld + soff;
+                for (int m = -l; m <= l; m++) acc = acc + Dl[(k + nmin) * (2 * l + 1) + (m + l)] * (x[aidx(m, l, q, L)] * e[m]);
+            }
+            AP[(((size_t)pc * 2 + q) * L + (l - 1)) * W + (k + nmin)] = acc;
+        }
+        __syncthreads();
+        // g(+ma, n, p) = Z[mode p] a'(+ma) ; g(-ma, n, p) = Z[mode 1-p] a'(-ma), every degree ma and column
+        {
+            // items (column, ma, sign, mode, n) with n = max(1, ma) .. nt
+            const int per_col = 2 * 2 * (nt + nt * nmin - (nmin * (nmin - 1)) / 2);   // 4 x sum over ma of the rows
+            for (int it = tid; it < np * per_col; it += PP_NT) {
+                const int pc = it / per_col;
+                int rem = it - pc * per_col;
+                int ma = 0;
+                for (;; ma++) {
+                    const int rows = nt - max(1, ma) + 1;
+                    if (rem < 4 * rows) break;
+                    rem -= 4 * rows;
+                }
+                const int m1 = max(1, ma), rows = nt - m1 + 1;
+                const int sg = rem / (2 * rows);
+                rem -= sg * 2 * rows;
+                const int pm = rem / rows, n = m1 + rem % rows;
+                if (ma == 0 && sg == 1) continue;
+                const int mm = sg ? -ma : ma;
+                const int pz = (ma == 0) ? 0 : (sg == 0 ? pm : 1 - pm);
+                const zd* Z = Zall + (size_t)ma * 2 * nt * L;
+                const zd* ap = AP + ((size_t)pc * 2 + pm) * L * W;
+                zd acc = mk(0.0, 0.0);
+                for (int l = m1; l <= L; l++) acc = acc + Z[(pz * nt + (n - 1)) * L + (l - 1)] * ap[(l - 1) * W + (mm + nmin)];
+                G[(((size_t)pc * 2 + pm) * nt + (n - 1)) * W + (mm + nmin)] = acc;
+            }
+        }
+        __syncthreads();
+        // back rotation per target degree n, phase back, LR -> TE/TM, accumulate
+        for (int it = tid; it < np * nt * (nt + 2); it += PP_NT) {
+            const int pc = it / (nt * (nt + 2)), ee = it - pc * (nt * (nt + 2));
+            const int p = p0 + pc;
+            int n = 1;
+            while (n * (n + 2) <= ee) n++;
+            int k = ee - (n * n - 1) - n;   // -n..n
+            int n1 = min(n, L);
+            const double* Dn = D + dofs[n];
+            zd gq[2];
+            for (int pm = 0; pm < 2; pm++) {
+                const zd* g = G + ((size_t)pc * 2 + pm) * nt * W;
+                zd acc = mk(0.0, 0.0);
+                for (int m = -n1; m <= n1; m++) acc = acc + Dn[(m + nmin) * (2 * n + 1) + (k + n)] * g[(n - 1) * W + (m + nmin)];
+                gq[pm] = acc * e[-k];   // phase back: e^{-i k phi}
+            }
+            if (dist) {
+                zd* od = a.out + (size_t)p * a.ldo + a.offset[i];
+                od[aidx(k, n, 0, nt)] = gq[0];
+                od[aidx(k, n, 1, nt)] = gq[1];
+                continue;
+            }
+            int s_ = aidx(k, n, 0, T);
+            zd* o = a.amnp0 + (size_t)p * a.ld0;
+            atomicAdd(&o[s_].x, gq[0].x + gq[1].x);
+            atomicAdd(&o[s_].y, gq[0].y + gq[1].y);
+            atomicAdd(&o[s_ + T * (T + 2)].x, gq[0].x - gq[1].x);
+            atomicAdd(&o[s_ + T * (T + 2)].y, gq[0].y - gq[1].y);
+        }
+        __syncthreads();
     }
 }
 
@@ -656,18 +682,19 @@ void launch_tranorder(int nsph, const double* pos, const int* order, const doubl
 
 size_t merge_scratch_per_cta(int T, int L)
 {
-    int nmin = std::min(T, L), nmax = std::max(T, L);
+    int nmin = std::min(T, L), nmax = std::max(T, L), W = 2 * nmin + 1;
     size_t dsz = 0;
-    for (int n = 0; n <= nmax; n++) dsz += (size_t)(2 * nmin + 1) * (2 * n + 1);
-    size_t z = (size_t)(nmax + L + 4) * 3;                       // xi + Bessel scratch
-    size_t dbl = dsz + 1 + 2 * (2 * nmax + 3) + 8;                // D + dk arrays
-    size_t zz = 2 * (size_t)T * L + 2 * (size_t)T * (2 * nmin + 1) + 2 * (size_t)L * (2 * nmin + 1);
-    return z + (dbl + 1) / 2 + zz + 8;                            // in zd units
+    for (int n = 0; n <= nmax; n++) dsz += (size_t)W * (2 * n + 1);
+    size_t z = (size_t)(nmax + L + 4) * 3 + (2 * nmax + 1);             // xi + Bessel scratch + e^{i m phi}
+    size_t dbl = dsz + 1 + 2 * (2 * nmax + 3) + 8 + (nmax + 8) / 2 + 2;  // D + dk arrays + degree offsets
+    size_t zz = (size_t)(nmin + 1) * 2 * T * L + (size_t)MERGE_PC * (2 * (size_t)L * W + 2 * (size_t)T * W);
+    return z + (dbl + 1) / 2 + zz + 8;                                  // in zd units
 }
+int merge_chunks(int npol) { return (npol + MERGE_PC - 1) / MERGE_PC; }
 
 void launch_merge(const MergeArgs& a, int grid, cudaStream_t st)
 {
-    merge_kernel<<<grid, PP_NT, 0, st>>>(a);
+    merge_kernel<<<dim3(grid, merge_chunks(a.npol)), PP_NT, 0, st>>>(a);
     launch_counter() += 1;
 }
 

@@ -38,7 +38,12 @@ struct MergeArgs {
 
 void launch_tranorder(int nsph, const double* pos, const int* order, const double* origin, double rire, double eps, int maxt,
                       const double* bcof, const double* fnr, int nbc, zd* scratch, int sstride, int* tord, cudaStream_t st);
+#define MERGE_PC 16   // columns a CTA of the merge kernel translates together
+// zd units of merge-kernel scratch per CTA; a launch of `grid` CTAs per chunk
+// of MERGE_PC columns needs grid * merge_chunks(npol) of them
 size_t merge_scratch_per_cta(int T, int L);
+int merge_chunks(int npol);
+// grid CTAs over the spheres times merge_chunks(npol) column chunks
 void launch_merge(const MergeArgs& a, int grid, cudaStream_t st);
 int fosm_grid(int ntot);
 size_t fosm_scratch_doubles(int ntot);
