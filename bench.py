@@ -413,11 +413,25 @@ def run_extras(args, dev, stream):
         row[prec] = {"solves_per_s": round(1000.0 / ms, 2), "ms": round(ms, 3), "qext": r["qtot"][0, 0]}
         g.close()
     out["cluster20"] = row
-    # learned warm start: a short study (training set generated by the solver)
+    # learned warm start: the network trained on the solver's own solutions of
+    # 20,000 seeded configurations (mstm_b200/data/warmstart_net.npz, made by
+    # `python -m mstm_b200.warmstart --train 20000 --eval 1000`, whose held-out
+    # results it carries), evaluated here live on the first 100 configurations
+    # of the same held-out stream (seed 6)
     from mstm_b200 import warmstart as WS
-    ws = WS.study(n_train=120, n_eval=8, epochs=60, device=dev, log=None)
+    wpath = os.path.join(ROOT, "mstm_b200", "data", "warmstart_net.npz")
+    if os.path.exists(wpath):
+        net, meta = WS.load_net(wpath, dev)
+        held = WS.solve_samples(WS.draw_configs(100, 6, workers=8))
+        live = WS.evaluate(net, held)
+        ws = {"n_train": meta.get("n_train"), "n_eval": meta.get("n_eval"), "epochs": meta.get("epochs"),
+              "study": {k: meta[k] for k in meta if k.startswith("fallback_")},
+              "live_n_eval": len(held), "live": live}
+    else:
+        ws = WS.study(n_train=120, n_eval=8, epochs=60, device=dev, log=None)
     ws["workload"] = ("held-out configurations of 100-300 spheres, x in [0.5, 2], m random, fv in [0.05, 0.3], "
-                      "+z incidence, mixed precision to 1e-6 residual; network trained here on solver outputs")
+                      "+z incidence, mixed precision to 1e-6 residual; network trained on the solver's own solutions; "
+                      "iterations in GMRES step pairs over both polarisations, wall time including the network's inference")
     out["warm_start"] = ws
     # the orientation-averaged ensemble: configurations of 50-400 spheres
     # (x = 1.5, seed 4), each a cluster T matrix (tensor-core passes) and its
