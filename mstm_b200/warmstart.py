@@ -579,37 +579,49 @@ def load_net(path, device):
 def evaluate(net, held, fallbacks=(1.0, 0.1), eps=1e-12, precision="mixed"):
     """Held-out configurations: solver iterations and wall time (the guess's
     network inference included) to ||r||/||b|| < 1e-6 from the network's guess
-    under each fallback threshold, against the reference's Mie start."""
+    under each fallback threshold, against the reference's Mie start.  The
+    variants of one configuration run back to back in an order that rotates
+    from one configuration to the next, after an untimed run of each, so that
+    warm-up and clock drift fall on all of them alike."""
     import time
     import torch
     res = {}
-    t_mie, it_mie, r_mie = 0.0, 0, []
-    guesses = []
-    for s in held:
+    variants = ["mie"] + list(fallbacks)
+    t = {v: 0.0 for v in variants}
+    it = {v: 0 for v in variants}
+    nfb = {v: 0 for v in variants}
+    r0 = {v: [] for v in variants}
+
+    def run(s, v, x0, t_inf):
+        t0 = time.perf_counter()
+        if v == "mie":
+            rp = solve_with_guess(s["cfg"], s["a0"], eps=eps, precision=precision, fallback=10.0)
+        else:
+            rp = solve_with_guess(s["cfg"], x0, eps=eps, precision=precision, fallback=v)
+        return rp, time.perf_counter() - t0 + (0.0 if v == "mie" else t_inf)
+
+    for k, s in enumerate(held):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         x0 = predict_guess(net, s)
         torch.cuda.synchronize()
-        guesses.append((x0, time.perf_counter() - t0))
-        t0 = time.perf_counter()
-        rp = solve_with_guess(s["cfg"], s["a0"], eps=eps, precision=precision, fallback=10.0)
-        t_mie += time.perf_counter() - t0
-        it_mie += sum(rp["iterations"])
-        r_mie += rp["guess_residual"]
+        t_inf = time.perf_counter() - t0
+        if k == 0:
+            for v in variants:
+                run(s, v, x0, t_inf)   # untimed
+        for v in variants[k % len(variants):] + variants[:k % len(variants)]:
+            rp, dt = run(s, v, x0, t_inf)
+            t[v] += dt
+            it[v] += sum(rp["iterations"])
+            r0[v] += rp["guess_residual"]
+            if v != "mie":
+                nfb[v] += 2 - sum(rp["used"])
     for fb in fallbacks:
-        t_w, it_w, nfb, r_w = 0.0, 0, 0, []
-        for s, (x0, t_inf) in zip(held, guesses):
-            t0 = time.perf_counter()
-            rw = solve_with_guess(s["cfg"], x0, eps=eps, precision=precision, fallback=fb)
-            t_w += time.perf_counter() - t0 + t_inf
-            it_w += sum(rw["iterations"])
-            nfb += 2 - sum(rw["used"])
-            r_w += rw["guess_residual"]
-        res["fallback_%g" % fb] = dict(fallback=fb, iterations_warm=it_w, iterations_mie_start=it_mie,
-                                      iteration_ratio=round(it_w / max(1, it_mie), 4), wall_s_warm=round(t_w, 2),
-                                      wall_s_mie_start=round(t_mie, 2), wall_ratio=round(t_w / max(1e-9, t_mie), 4),
-                                      mean_initial_residual_warm=float(np.mean(r_w)),
-                                      mean_initial_residual_mie=float(np.mean(r_mie)), fallbacks=nfb,
+        res["fallback_%g" % fb] = dict(fallback=fb, iterations_warm=it[fb], iterations_mie_start=it["mie"],
+                                      iteration_ratio=round(it[fb] / max(1, it["mie"]), 4), wall_s_warm=round(t[fb], 2),
+                                      wall_s_mie_start=round(t["mie"], 2), wall_ratio=round(t[fb] / max(1e-9, t["mie"]), 4),
+                                      mean_initial_residual_warm=float(np.mean(r0[fb])),
+                                      mean_initial_residual_mie=float(np.mean(r0["mie"])), fallbacks=nfb[fb],
                                       polarisations=2 * len(held))
     return res
 

@@ -9,6 +9,8 @@
   fraction, every sphere inside the boundary, no overlaps.
 * Position files in the `x y z r` format read_sphere_data_input_file reads
   (mstm-input-37.f90:2886-2923) round-trip.
+* The warm-start network file the benchmark loads was trained on the
+  solver's solutions of 20,000 configurations drawn by these generators.
 """
 import math
 
@@ -97,3 +99,18 @@ def test_rsa_sphere_batched(n, x, fv, seed):
     assert np.sqrt((pos ** 2).sum(1)).max() <= R - x + 1e-12
     assert _pair_dist(pos).min() >= 2.0 * x
     assert np.array_equal(pos, C.rsa_sphere_batched(n, x, fv, seed=seed)[0])
+
+
+def test_committed_warm_start_network_file():
+    """The weights the benchmark's warm-start row loads: the network trained on
+    the solver's solutions of 20,000 seeded configurations, with its held-out
+    study (1,000 configurations) in the file's description."""
+    import json
+    import os
+    from mstm_b200 import warmstart as W
+    d = np.load(os.path.join(os.path.dirname(W.__file__), "data", "warmstart_net.npz"))
+    meta = json.loads(str(d["meta"]))
+    assert meta["n_train"] == 20000 and meta["n_eval"] == 1000 and meta["epochs"] == 20
+    r = meta["fallback_1"]
+    assert r["polarisations"] == 2000 and r["iterations_warm"] < r["iterations_mie_start"]
+    assert int(d["hidden"]) > 0 and int(d["layers"]) > 0 and d["params"].dtype == np.float32

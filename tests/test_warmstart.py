@@ -145,3 +145,21 @@ def test_ensemble_samples_match_single_solves(ws):
         assert np.array_equal(b["mask"], s["mask"]) and np.allclose(b["X"], s["X"])
         scale = np.abs(s["target"]).max()
         assert np.abs(b["target"] - s["target"]).max() <= 1e-4 * scale
+
+
+def test_saved_network_reloads_and_evaluates(ws, tmp_path):
+    """The network trained at scale (mstm_b200/data/warmstart_net.npz) loads,
+    its guesses on held-out configurations start below the Mie start's
+    residual, and a save / load round trip keeps the weights."""
+    import os
+    W, dev = ws
+    path = os.path.join(os.path.dirname(W.__file__), "data", "warmstart_net.npz")
+    net, meta = W.load_net(path, dev)
+    assert meta["n_train"] == 20000 and meta["n_eval"] == 1000
+    held = W.solve_samples(W.draw_configs(4, 6, workers=0))
+    ev = W.evaluate(net, held, fallbacks=(1.0,))
+    r = ev["fallback_1"]
+    assert r["polarisations"] == 8 and r["mean_initial_residual_warm"] < r["mean_initial_residual_mie"]
+    W.save_net(net, str(tmp_path / "n.npz"), meta=meta)
+    net2, meta2 = W.load_net(str(tmp_path / "n.npz"), dev)
+    assert np.array_equal(net2.state(), net.state()) and meta2 == meta
