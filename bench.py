@@ -730,7 +730,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "tc"])
     ap.add_argument("--fp32-chunk", type=int, default=0, help="profiling case: FP32 column chunk (2 or 4; 0 default)")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="profiling case: tiled kernel CTAs per SM (0 default)")
-    ap.add_argument("--tile-pairs", type=int, default=0, help="profiling case: pairs per step of the tiled kernel (0 default)")
+    ap.add_argument("--tile-pairs", type=int, default=0, help="profiling case: 0 the FP32 row kernel (default), 1 or 2 the rotation-tiled kernel with that many pairs per step")
     ap.add_argument("--nrhs", type=int, default=4)
     ap.add_argument("--tmatrix-case", type=int, default=0, help="profiling case: one T matrix of this many spheres")
     ap.add_argument("--tensor-core", type=int, default=0, help="profiling case: 0 tensor-core passes where they apply, -1 never")

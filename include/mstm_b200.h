@@ -55,8 +55,9 @@ typedef struct {
     int max_outer;                 /* mixed mode: GMRES cycles (mixed_solver 2) or refinement steps
                                       (mixed_solver 1) at most (default 30) */
     int generic_kernel;            /* 1: always use the order-generic translation kernel (default 0) */
-    int tile_ctas_per_sm;          /* tiled kernel CTAs per SM, 1..3 caps it (0: as many as shared memory and the
-                                      kernel's register budget allow: 3 for FP32 passes of 1 or 2 columns, else 2) */
+    int tile_ctas_per_sm;          /* tiled kernels' CTAs per SM, 1..3 caps it (0: as many as shared memory and
+                                      the kernel's register budget allow: 2 for the row kernel and FP64 passes,
+                                      3 for the rotation-tiled kernel's FP32 passes of 1 or 2 columns) */
     int fp32_chunk;                /* columns per chunk of FP32 tiled passes, 2 or 4 (0: chosen per context by
                                       timing one pass of each on the first pass of 4 or more columns) */
     int mixed_solver;              /* MSTMG_PRECISION_MIXED solver of the fixed-orientation and T-matrix
@@ -66,9 +67,10 @@ typedef struct {
                                       inside FP64 refinement */
     int gmres_restart;             /* mixed_solver 2: Arnoldi steps per cycle at most (0: up to 200, fewer
                                       when a quarter of the free device memory cannot hold the basis) */
-    int tile_pairs;                /* pairs of a tile the tiled kernel handles per step, its four phases and
-                                      barriers shared: 2 for FP32 passes of one or two columns when set to 2,
-                                      otherwise 1 (the default: faster at three CTAs per SM) */
+    int tile_pairs;                /* FP32 passes of clusters of one sphere order: 0 (default) the row kernel
+                                      (operator rows broadcast from shared memory to the columns of up to two
+                                      pairs a step, FP32 operators in row records); 1 or 2 the rotation-tiled
+                                      kernel with that many pairs a step (FP32 operators in the FP64 layout) */
     int tensor_core;               /* FP32 passes of 12 or more plain columns (the T-matrix GMRES) on the
                                       tensor cores with dense TF32 hi/lo pair operators: 0 when the context
                                       qualifies (one sphere order 5..10, direct pairs) and the operators fit

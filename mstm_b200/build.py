@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmstm_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
-SOURCES = ["tcpass.cu", "opgen.cu", "translate.cu", "translate_tiled.cu", "sphere_kernels.cu", "bicg.cu", "mrhs.cu", "ranorient.cu", "fftpath.cu", "warmstart.cu", "densepair.cu", "postproc.cu", "capi.cu", "capi_pass.cu", "capi_solve.cu", "capi_origin.cu", "noalloc.cu", "tables.cpp"]
+SOURCES = ["tcpass.cu", "opgen.cu", "translate.cu", "translate_tiled.cu", "translate_rows.cu", "sphere_kernels.cu", "bicg.cu", "mrhs.cu", "ranorient.cu", "fftpath.cu", "warmstart.cu", "densepair.cu", "postproc.cu", "capi.cu", "capi_pass.cu", "capi_solve.cu", "capi_origin.cu", "noalloc.cu", "tables.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

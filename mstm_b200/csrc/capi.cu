@@ -93,6 +93,9 @@ int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const std::v
     }
     c->op_units = u;
     c->maxrec = maxrec;
+    // FP32 passes of the tiled path run the row kernel on row records unless
+    // the rotation-tiled kernel is asked for (tile_pairs 1 or 2)
+    c->row32 = (c->tiled && c->opts.tile_pairs == 0 && rows_supported(c->lmax, 1)) ? row_record_units(c->lmax) : 0;
     c->layout_gen++;
     if (np > 0) {
         CK(c->pairs.alloc(np));
@@ -264,9 +267,22 @@ int setup_layout(mstmg_ctx* c)
             int I = IJ.first, J = IJ.second;
             int i0 = I * B, j0 = J * B;
             int start = (int)t;
-            for (int i = i0; i < std::min(n, i0 + B); i++)
-                for (int j = j0; j < std::min(n, j0 + B); j++)
-                    if (i < j && same_cfg(i, j)) add_pair(i, j);
+            // inside a tile, consecutive pairs (0,1), (2,3), ... share no
+            // sphere wherever the tile is whole: an off-diagonal tile runs the
+            // diagonals (a, a+s mod B) of its block pair, a diagonal tile the
+            // matchings {01, 23}, {02, 13}, {03, 12}; the row kernel takes two
+            // such pairs a step
+            static_assert(TILE_B == 4, "the diagonal-tile order below is for blocks of 4 spheres");
+            static const int dg[6][2] = {{0, 1}, {2, 3}, {0, 2}, {1, 3}, {0, 3}, {1, 2}};
+            auto try_add = [&](int i, int j) {
+                if (i < n && j < n && i < j && same_cfg(i, j)) add_pair(i, j);
+            };
+            if (I == J) {
+                for (const auto& d : dg) try_add(i0 + d[0], i0 + d[1]);
+            } else {
+                for (int sft = 0; sft < B; sft++)
+                    for (int a_ = 0; a_ < B; a_++) try_add(i0 + a_, j0 + (a_ + sft) % B);
+            }
             int cnt = (int)t - start;
             if (cnt > 0) tl.push_back(make_int4(start, cnt, (i0 << 16) | j0, I == J ? 1 : 0));
         }

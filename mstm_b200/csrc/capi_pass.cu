@@ -60,8 +60,10 @@ int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
     {
         const void* was[2] = {c->op64.p, c->op32.p};
         if (need64) CK(c->op64.alloc(c->op_units));
-        if (need32) CK(c->op32.alloc(c->op_units));
+        if (need32) CK(c->op32.alloc(c->row32 ? (long long)c->npairs * c->row32 : c->op_units));
         if (was[0] != c->op64.p || was[1] != c->op32.p) c->layout_gen++;
+        // row records: the padding of every row reads as zero
+        if (need32 && c->row32) CK(cudaMemsetAsync(c->op32.p, 0, sizeof(float) * (size_t)c->npairs * c->row32, c->st));
     }
     NvtxRange nvtx_("pair operator generation");
     OpGenArgs a;
@@ -72,6 +74,7 @@ int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
     a.opoff = c->opoff.p;
     a.op64 = need64 ? c->op64.p : nullptr;
     a.op32 = need32 ? c->op32.p : nullptr;
+    a.row32 = c->row32;
     a.vcc = c->vcc.p;
     a.vnmax = c->vn;
     a.fnr = c->fnr.p;
@@ -94,6 +97,27 @@ template <typename T> static const T* ops_ptr(mstmg_ctx* c);
 template <> const double* ops_ptr<double>(mstmg_ctx* c) { return c->op64.p; }
 template <> const float* ops_ptr<float>(mstmg_ctx* c) { return c->op32.p; }
 
+
+// FP32 passes on row records: the row kernel, in groups of 4, 2 or 1 columns
+// when the pass has another column count (the records fit no other kernel)
+template <typename T> static int rows_pass(mstmg_ctx*, const TiledArgs<T>&, int, int, unsigned) { return -1; }
+template <> int rows_pass<float>(mstmg_ctx* c, const TiledArgs<float>& tf, int nrhs, int nchunk, unsigned contran)
+{
+    if (rows_supported(c->lmax, nrhs)) return launch_translate_rows(tf, c->lmax, c->nsm, c->st);
+    if (nchunk != 1) return -1;
+    int rc = 0;
+    for (int c0 = 0; c0 < nrhs && rc == 0;) {
+        const int w = nrhs - c0 >= 4 ? 4 : (nrhs - c0 >= 2 ? 2 : 1);
+        TiledArgs<float> tw = tf;
+        tw.x = tf.x + (size_t)c0 * c->neqns;
+        tw.y = tf.y + (size_t)c0 * c->neqns;
+        tw.nrhs = w;
+        tw.contran = (contran >> c0) & ((1u << w) - 1u);
+        rc = launch_translate_rows(tw, c->lmax, c->nsm, c->st);
+        c0 += w;
+    }
+    return rc;
+}
 
 // y[:, 0:nrhs*nchunk] = H x[:, 0:nrhs*nchunk]  (y zeroed here).  nchunk > 1
 // only on the tiled path: contran then applies to column r of every chunk.
@@ -124,7 +148,7 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
     a.maxrec = c->maxrec;
     a.err = c->err.p;
     TiledArgs<T> ta;
-    bool use_tiled = c->tiled && tiled_supported(c->lmax, nrhs);
+    bool use_tiled = c->tiled && (tiled_supported(c->lmax, nrhs) || (sizeof(T) == 4 && c->row32));
     if (use_tiled) {
         ta.ntiles = c->ntiles;
         ta.tiles = c->tiles.p;
@@ -152,7 +176,15 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
         }
         CK(cudaEventRecord(e0, c->st));
     }
-    if (!use_tiled || launch_translate_tiled<T>(ta, c->lmax, c->nsm, c->st) != 0) {
+    if (use_tiled && sizeof(T) == 4 && c->row32) {
+        const int rc = rows_pass(c, ta, nrhs, nchunk, contran);
+        if (rc != 0) {
+            if (e0) c->ev_pool.push_back(e0);
+            if (e1) c->ev_pool.push_back(e1);
+            set_err("FP32 translation pass: no row-kernel configuration for this order and column count");
+            return MSTMG_ERR_UNSUPPORTED;
+        }
+    } else if (!use_tiled || launch_translate_tiled<T>(ta, c->lmax, c->nsm, c->st) != 0) {
         if (nchunk > 1) {
             if (e0) c->ev_pool.push_back(e0);
             if (e1) c->ev_pool.push_back(e1);

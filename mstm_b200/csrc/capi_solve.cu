@@ -518,7 +518,7 @@ extern "C" int mstmg_operator_bytes(const mstmg_ctx* c, int prec, double* stored
 {
     if (!c) return MSTMG_ERR_ARG;
     double es = prec == 0 ? 8.0 : 4.0;
-    if (stored) *stored = (double)c->op_units * es;
+    if (stored) *stored = (prec != 0 && c->row32) ? (double)c->npairs * c->row32 * es : (double)c->op_units * es;
     if (canonical) {
         double s = 0.0;
         for (int i = 0; i < c->n - 1; i++)

@@ -23,6 +23,7 @@
 #include "sphere_kernels.cuh"
 #include "tables.h"
 #include "translate_tiled.cuh"
+#include "translate_rows.cuh"
 #include "postproc.cuh"
 #include "mrhs.cuh"
 #include "ranorient.cuh"
@@ -309,6 +310,7 @@ struct mstmg_ctx {
     DevBuf<int> tsph;
     DevBuf<short2> pslot;
     bool tiled = false;   // monodisperse cluster: pairs stored in tile order for the fast kernel
+    int row32 = 0;        // tiled: floats per FP32 row record (translate_rows.cuh); 0: FP32 records as FP64
     DevBuf<double> op64;
     DevBuf<float> op32;
     bool ops64_ready = false, ops32_ready = false;

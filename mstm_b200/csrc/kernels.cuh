@@ -10,6 +10,7 @@ struct OpGenArgs {
     const long long* opoff;  // per pair, in storage units
     double* op64;            // may be null
     float* op32;             // may be null
+    int row32;               // > 0: op32 holds row records (translate_rows.cuh) of one order, row32 floats each
     const double* vcc;       // vcc_const(vn, vn(vn+2), 0:2vn)
     int vnmax;
     const double* fnr;       // fnr[k] = sqrt(k)

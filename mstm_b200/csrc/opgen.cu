@@ -27,9 +27,12 @@
 //   [2, 2+R)         E_1, O_1, E_2, O_2, ...   (row-major, restricted index first)
 //   [2+R, 2+R+2Z)    Z_0[p=0], Z_1[p=0], Z_1[p=1], Z_2[p=0], ... complex, [row n][col l]
 //   padding to a multiple of 4 units.
+// FP32 records of clusters of one sphere order (the tiled passes) use the row
+// layout of translate_rows.cuh instead: the same values, rows 16-byte aligned.
 #include "common.cuh"
 #include "special.cuh"
 #include "kernels.cuh"
+#include "translate_rows.cuh"
 
 #define DW (2 * MSTMG_LMAX + 1)
 #define XIW (2 * MSTMG_LMAX + 1)   // Hankel orders w = 0 .. nt + ns <= 2 LMAX per pair
@@ -89,7 +92,16 @@ __global__ void __launch_bounds__(128) opgen_pair_kernel(OpGenArgs a)
             a.op64[off] = g.ephi.x;
             a.op64[off + 1] = g.ephi.y;
         }
-        if (a.op32) {
+        if (a.op32 && a.row32) {
+            // row records: the powers e^{i m phi}, m = 0..nt, by the recurrence in FP64
+            float* h = a.op32 + (long long)q * a.row32;
+            zd e = mk(1.0, 0.0);
+            for (int m = 0; m <= g.nt; m++) {
+                h[2 * m] = (float)e.x;
+                h[2 * m + 1] = (float)e.y;
+                e = e * g.ephi;
+            }
+        } else if (a.op32) {
             a.op32[off] = (float)g.ephi.x;
             a.op32[off + 1] = (float)g.ephi.y;
         }
@@ -123,7 +135,8 @@ __global__ void __launch_bounds__(128) opgen_rot_kernel(OpGenArgs a)
         const double ct = g.ct;
         const long long off = a.opoff[q];
         double* rec64 = a.op64 ? a.op64 + off : nullptr;
-        float* rec32 = a.op32 ? a.op32 + off : nullptr;
+        float* rec32 = (a.op32 && !a.row32) ? a.op32 + off : nullptr;
+        float* row32 = (a.op32 && a.row32) ? a.op32 + (size_t)q * a.row32 : nullptr;
         const double sbe = (fabs(ct) >= 1.0) ? 0.0 : sqrt(fabs((1.0 + ct) * (1.0 - ct)));
         const double cbe2 = 0.5 * (1.0 + ct), sbe2 = 0.5 * (1.0 - ct);
         for (int k = lane; k < 2 * MSTMG_LMAX + 3; k += 32) {
@@ -201,6 +214,19 @@ __global__ void __launch_bounds__(128) opgen_rot_kernel(OpGenArgs a)
                 }
                 if (rec64) rec64[roff + e] = v;
                 if (rec32) rec32[roff + e] = (float)v;
+                if (row32) {
+                    // row layout: row k of degree n is [E(k,0), 0, E(k,1), O(k,1), ..., E(k,n), O(k,n)]
+                    int k, slot;
+                    if (e < ne) {
+                        k = (int)(((float)e + 0.5f) * rn1);
+                        slot = 2 * (e - k * (n + 1));
+                    } else {
+                        const int qq = (int)(((float)(e - ne) + 0.5f) * rn);
+                        k = 1 + qq;
+                        slot = 2 * (1 + (e - ne) - qq * n) + 1;
+                    }
+                    row32[rr_rot_off(n, nmax) + k * rr_rw(n) + slot] = (float)v;
+                }
             }
             __syncwarp();
         }
@@ -223,7 +249,8 @@ __global__ void __launch_bounds__(128) opgen_axial_kernel(OpGenArgs a)
         __syncthreads();
         const long long off = a.opoff[q];
         double* rec64 = a.op64 ? a.op64 + off : nullptr;
-        float* rec32 = a.op32 ? a.op32 + off : nullptr;
+        float* rec32 = (a.op32 && !a.row32) ? a.op32 + off : nullptr;
+        float* row32 = (a.op32 && a.row32) ? a.op32 + (size_t)q * a.row32 : nullptr;
         const int zbase = 2 + op_rot_size(g.nmax, nmin);
         // walk the blocks forward: block m holds rc(m) elements, mode-1 copies
         // after the mode-0 ones for m > 0 (op_z_offset)
@@ -254,6 +281,20 @@ __global__ void __launch_bounds__(128) opgen_axial_kernel(OpGenArgs a)
                 if (m > 0) {
                     rec64[zo + 2 * rc] = v1.x;
                     rec64[zo + 2 * rc + 1] = v1.y;
+                }
+            }
+            if (row32) {
+                // row layout: m = 0 rows of Z_0(n, .); m > 0 rows of (Z_m^0, Z_m^1)(n, l) pairs
+                if (m == 0) {
+                    float* z = row32 + rr_z_off(0, nt) + (n - 1) * rr_zw0(nt) + 2 * (l - 1);
+                    z[0] = (float)v0.x;
+                    z[1] = (float)v0.y;
+                } else {
+                    float* z = row32 + rr_z_off(m, nt) + (n - m1) * 4 * cols + 4 * (l - m1);
+                    z[0] = (float)v0.x;
+                    z[1] = (float)v0.y;
+                    z[2] = (float)v1.x;
+                    z[3] = (float)v1.y;
                 }
             }
             if (rec32) {

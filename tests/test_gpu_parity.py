@@ -571,10 +571,9 @@ def test_device_driven_cycles_sync_once_per_cycle(api, oracle_mod, name):
 
 @pytest.mark.parametrize("name", ["fractal60", "cluster20"])
 def test_two_pairs_per_step_match_one(api, name):
-    """The tiled kernel with two slot-disjoint pairs of a tile per step (the
-    default for FP32 passes of one or two columns) gives the FP32 pass of
-    one pair per step, and the FP64 pass, to FP32 rounding, for plain and
-    conjugate-transpose columns."""
+    """The rotation-tiled kernel with two slot-disjoint pairs of a tile per
+    step gives the FP32 pass of one pair per step, and the FP64 pass, to FP32
+    rounding, for plain and conjugate-transpose columns."""
     pos, rad, ri, em = _cluster(name)
     two = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", tile_pairs=2)
     one = api.SphereCluster(pos, rad, ri, mie_epsilon=em, precision="mixed", tile_pairs=1)
