@@ -64,14 +64,19 @@ __host__ __device__ constexpr size_t al128(size_t v) { return (v + 127) & ~(size
 // packed-S offset of degree n: entries (n, m = 0..n) of all degrees in one array
 __host__ __device__ constexpr int sofs(int n) { return (n - 1) * (n + 2) / 2; }
 
+// strides padded for the shared-memory banks: (s', t') columns an odd number
+// of 16-byte units apart, tile-output slots an odd number of complex values
+__host__ __device__ constexpr int rows_gs(int L) { return (L * (L + 3) / 2) | 1; }
+__host__ __device__ constexpr int rows_ss(int L, int NR) { return NR * 2 * L * (L + 2) + 1; }
+
 template <int L, int NR, int PP> __host__ __device__ constexpr size_t rows_smem_pp()
 {
-    constexpr int NB2 = L * (L + 2), NS = L * (L + 3) / 2, C = 4 * NR;
-    size_t off = 64;                                                    // mbarriers
+    constexpr int NB2 = L * (L + 2), C = 4 * NR;
+    size_t off = 128;                                                   // mbarriers, step descriptors
     off = al128(off + sizeof(float) * 2 * PP * row_record_units(L));    // records, two steps
     off += sizeof(zf) * 3 * (size_t)PP * C * NB2;                      // sources (two steps), a'
-    off += sizeof(float4) * (size_t)PP * C * NS;                       // (s', t') of the axial products
-    off += sizeof(zf) * (size_t)2 * TILE_B * NR * 2 * NB2;             // tile outputs
+    off += sizeof(float4) * (size_t)PP * C * rows_gs(L);               // (s', t') of the axial products
+    off += sizeof(zf) * (size_t)2 * TILE_B * rows_ss(L, NR);           // tile outputs
     return off;
 }
 // pairs per step: two while two CTAs of that size fit an SM
@@ -331,13 +336,23 @@ template <int L, int H, int N = 1> __device__ __forceinline__ void d_any(int n, 
     }
 }
 
+// A step's descriptor, written by the thread that streams the step in.
+struct StepMeta {
+    int q;      // first pair
+    int np;     // pairs (1..PP)
+    int item;   // work item (tile, chunk)
+    int last;   // last step of the tile
+    int slots;  // output slots: pair u's (i, j) slots in bytes 2u, 2u + 1
+    int i0, j0, diag;   // the tile's block starts and diagonal flag
+};
+
 template <int L, int NR>
 __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float> a, RowSched sc)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR, PP = rows_pp<L, NR>(), H = 32 / (PP * C);
     static_assert(PP * C * H == 32, "a warp holds PP pairs x C columns x H row sets");
-    constexpr int NB2 = L * (L + 2), NB = 2 * NB2, NS = L * (L + 3) / 2;
+    constexpr int NB2 = L * (L + 2), NB = 2 * NB2, GS = rows_gs(L), SS = rows_ss(L, NR);
     constexpr int REC = row_record_units(L);
     constexpr int NSLOT = 2 * TILE_B;
     constexpr uint32_t RECB = (uint32_t)(REC * sizeof(float));
@@ -346,13 +361,14 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
 
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm);   // [0],[1] records, [2],[3] sources of steps t, t + 1
-    size_t off = 64;
+    StepMeta* meta = reinterpret_cast<StepMeta*>(sm + 64);   // descriptors of steps t, t + 1
+    size_t off = 128;
     float* recs = reinterpret_cast<float*>(sm + off);
     off = al128(off + sizeof(float) * 2 * PP * REC);
     zf* SRC = reinterpret_cast<zf*>(sm + off);   // two buffers
     zf* AP = SRC + 2 * CW;
     float4* GB = reinterpret_cast<float4*>(AP + CW);
-    zf* ACC = reinterpret_cast<zf*>(GB + PP * C * NS);
+    zf* ACC = reinterpret_cast<zf*>(GB + PP * C * GS);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int c = lane % C, qq = (lane / C) % PP;
@@ -365,9 +381,9 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
     ln.dsg = ln.dir ? -1.f : 1.f;
     ln.sig = ln.swp ? -1.f : 1.f;
     ln.ap = AP + (size_t)(qq * C + c) * NB2;
-    ln.g = GB + (size_t)(qq * C + c) * NS;
+    ln.g = GB + (size_t)(qq * C + c) * GS;
 
-    for (int e = tid; e < NSLOT * NR * NB; e += NT) ACC[e] = mk(0.f, 0.f);
+    for (int e = tid; e < NSLOT * SS; e += NT) ACC[e] = mk(0.f, 0.f);
     if (tid == 0) {
         mb_init(&bar[0], 1);
         mb_init(&bar[1], 1);
@@ -379,59 +395,77 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
 
     const int G = gridDim.x;
     const int NI = a.ntiles * a.nchunk;   // work items (tile, chunk), chunk fastest
-    int tcur = blockIdx.x;
-    if (tcur >= NI) return;
+    if ((int)blockIdx.x >= NI) return;
     auto tile_of = [&](int it) { return it / a.nchunk; };
     auto col0 = [&](int it) { return (size_t)(it % a.nchunk) * NR * (size_t)a.ld; };
-    auto slots_of = [&](int q_, int it, int& s_i, int& s_j) {
-        if (a.pslot) {
-            const short2 ps = a.pslot[q_];
-            s_i = ps.x;
-            s_j = ps.y;
-        } else {
-            const int4 ti = a.tiles[tile_of(it)];
-            const int2 pr = a.pairs[q_];
-            s_i = pr.x - (ti.z >> 16);
-            s_j = ti.w ? (pr.y - (ti.z >> 16)) : (TILE_B + pr.y - (ti.z & 0xffff));
-        }
-    };
-    // pairs of the step that starts at pair q_: up to PP consecutive pairs of
-    // the tile whose output slots are all different
-    auto step_np = [&](int q_, int it) -> int {
-        if (PP == 1) return 1;
-        const int4 ti = a.tiles[tile_of(it)];
-        if (q_ + 1 >= ti.x + ti.y) return 1;
-        int a1, b1, a2, b2;
-        slots_of(q_, it, a1, b1);
-        slots_of(q_ + 1, it, a2, b2);
-        return (a1 != a2 && a1 != b2 && b1 != a2 && b1 != b2) ? 2 : 1;
-    };
-    // thread 0's iterator: the step two ahead, whose sources are issued when
-    // this step's AB phase is done with its buffer and whose records when the
-    // step is done
-    int pf_t = tcur, pf_q = a.tiles[tile_of(tcur)].x;
+
+    // Thread 0 streams the step two ahead.  Its tile entry and first two
+    // pairs are loaded when the previous step has been issued, a phase
+    // before they are used, so their latency stays off the barriers.
+    int pf_t = blockIdx.x, pf_q = 0;
+    int4 pf_ti = make_int4(0, 0, 0, 0);
+    int2 pf_p0 = make_int2(0, 0), pf_p1 = pf_p0;
+    short2 pf_s0 = make_short2(0, 0), pf_s1 = pf_s0;
     bool pf_ok = true;
-    auto pf_adv = [&]() {
-        pf_q += step_np(pf_q, pf_t);
-        const int4 ti = a.tiles[tile_of(pf_t)];
-        if (pf_q >= ti.x + ti.y) {
-            pf_t += G;
-            if (pf_t >= NI) { pf_ok = false; return; }
-            pf_q = a.tiles[tile_of(pf_t)].x;
+    auto pf_fetch = [&]() {
+        pf_p0 = a.pairs[pf_q];
+        if (PP == 2 && pf_q + 1 < pf_ti.x + pf_ti.y) pf_p1 = a.pairs[pf_q + 1];
+        if (a.pslot) {
+            pf_s0 = a.pslot[pf_q];
+            if (PP == 2 && pf_q + 1 < pf_ti.x + pf_ti.y) pf_s1 = a.pslot[pf_q + 1];
         }
     };
-    auto load_ops = [&](int bb) {
-        const int np_ = step_np(pf_q, pf_t);
-        mb_expect(&bar[bb], (uint32_t)np_ * RECB);
-        bulk_copy(recs + (size_t)bb * PP * REC, a.ops + (size_t)pf_q * REC, (uint32_t)np_ * RECB, &bar[bb]);   // consecutive records
-        pf_adv();
+    // the prefetch step's descriptor: pairs, output slots, end of tile
+    auto pf_meta = [&]() {
+        auto slots = [&](int2 pr, short2 ps, int& s_i, int& s_j) {
+            if (a.pslot) {
+                s_i = ps.x;
+                s_j = ps.y;
+            } else {
+                s_i = pr.x - (pf_ti.z >> 16);
+                s_j = pf_ti.w ? (pr.y - (pf_ti.z >> 16)) : (TILE_B + pr.y - (pf_ti.z & 0xffff));
+            }
+        };
+        int si0, sj0, si1 = 0, sj1 = 0, np = 1;
+        slots(pf_p0, pf_s0, si0, sj0);
+        if (PP == 2 && pf_q + 1 < pf_ti.x + pf_ti.y) {
+            slots(pf_p1, pf_s1, si1, sj1);
+            if (si0 != si1 && si0 != sj1 && sj0 != si1 && sj0 != sj1) np = 2;
+        }
+        StepMeta m;
+        m.q = pf_q;
+        m.np = np;
+        m.item = pf_t;
+        m.last = (pf_q + np == pf_ti.x + pf_ti.y) ? 1 : 0;
+        m.slots = si0 | (sj0 << 8) | (si1 << 16) | (sj1 << 24);
+        m.i0 = pf_ti.z >> 16;
+        m.j0 = pf_ti.z & 0xffff;
+        m.diag = pf_ti.w;
+        return m;
     };
-    auto load_sources = [&](int bb) {
-        const int np_ = step_np(pf_q, pf_t);
-        const zf* xs = a.x + col0(pf_t);
-        mb_expect(&bar[2 + bb], (uint32_t)np_ * 2u * NR * XB);
-        for (int u = 0; u < np_; u++) {
-            const int2 pr = a.pairs[pf_q + u];
+    auto pf_start = [&]() {
+        pf_ti = a.tiles[tile_of(pf_t)];
+        pf_q = pf_ti.x;
+        pf_fetch();
+    };
+    auto pf_adv = [&](int np) {
+        pf_q += np;
+        if (pf_q >= pf_ti.x + pf_ti.y) {
+            pf_t += G;
+            if (pf_t >= NI) {
+                pf_ok = false;
+                return;
+            }
+            pf_start();
+        } else {
+            pf_fetch();
+        }
+    };
+    auto load_sources = [&](int bb, const StepMeta& m) {
+        const zf* xs = a.x + col0(m.item);
+        mb_expect(&bar[2 + bb], (uint32_t)m.np * 2u * NR * XB);
+        for (int u = 0; u < m.np; u++) {
+            const int2 pr = u ? pf_p1 : pf_p0;
             zf* w = SRC + (size_t)bb * CW + (size_t)u * C * NB2;
             for (int rr = 0; rr < NR; rr++) {
                 bulk_copy(w + (size_t)(0 * NR + rr) * NB, xs + (size_t)rr * a.ld + (size_t)pr.y * NB, XB, &bar[2 + bb]);   // source of j -> i
@@ -439,20 +473,24 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
             }
         }
     };
+    // records of the prefetch step; its descriptor goes to the ring slot
+    // the step uses (read there after the records' mbarrier completes)
+    auto load_ops = [&](int bb, const StepMeta& m) {
+        meta[bb] = m;
+        mb_expect(&bar[bb], (uint32_t)m.np * RECB);
+        bulk_copy(recs + (size_t)bb * PP * REC, a.ops + (size_t)m.q * REC, (uint32_t)m.np * RECB, &bar[bb]);   // consecutive records
+    };
     if (tid == 0) {
+        pf_start();
         for (int bb = 0; bb < 2 && pf_ok; bb++) {
-            load_sources(bb);
-            load_ops(bb);
+            const StepMeta m = pf_meta();
+            load_sources(bb, m);
+            load_ops(bb, m);
+            pf_adv(m.np);
         }
     }
-    int q = a.tiles[tile_of(tcur)].x;
-    int t = 0;
-    while (true) {
-        const int4 tinfo = a.tiles[tile_of(tcur)];
-        const int i0 = tinfo.z >> 16, j0b = tinfo.z & 0xffff;   // block starts
-        const int diag = tinfo.w;
+    for (int t = 0;; t++) {
         const int b = t & 1;
-        const int np = step_np(q, tcur);
         if (!mb_wait(&bar[b], (t >> 1) & 1) || !mb_wait(&bar[2 + b], (t >> 1) & 1)) {
             // give up; first let the copies in flight land (bounded waits)
             if (tid == 0) atomicExch(a.err, MSTMG_ERR_CUDA);
@@ -462,15 +500,17 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
             mb_wait(&bar[2 + (b ^ 1)], ((t + 1) >> 1) & 1);
             return;
         }
-        ln.act = qq < np;
+        const StepMeta cm = meta[b];
+        ln.act = qq < cm.np;
         {
-            int si = 0, sj = 0;
-            if (ln.act) slots_of(q + qq, tcur, si, sj);
-            const int slot = ln.dir ? sj : si;
-            ln.acc = ACC + (size_t)(slot * NR + r) * NB + (size_t)ln.p * NB2;
+            const int sl = (cm.slots >> (16 * qq + (ln.dir ? 8 : 0))) & 255;
+            ln.acc = ACC + (size_t)(ln.act ? sl : 0) * SS + (size_t)r * NB + (size_t)ln.p * NB2;
         }
         ln.rec = recs + ((size_t)b * PP + qq) * REC;
         ln.src = SRC + (size_t)b * CW + (size_t)(qq * C + c) * NB2;
+        // the prefetch step's descriptor (thread 0; its loads were issued a phase ago)
+        StepMeta pm;
+        if (tid == 0 && pf_ok) pm = pf_meta();
 
         for (int u = sc.first[0][warp]; u < sc.first[0][warp + 1]; u++) {
             const unsigned un = sc.unit[0][u];
@@ -481,7 +521,7 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
         // the sources of the step after next stream into this step's buffer
         if (tid == 0 && pf_ok) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            load_sources(b);
+            load_sources(b, pm);
         }
 
         for (int u = sc.first[1][warp]; u < sc.first[1][warp + 1]; u++) {
@@ -496,31 +536,28 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
         }
         __syncthreads();
 
-        // ---- refill this record buffer with the step after next ----
+        // ---- refill this record buffer with the step after next, then
+        //      start the loads of the descriptor of the one after it ----
         if (tid == 0 && pf_ok) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            load_ops(b);
+            load_ops(b, pm);
+            pf_adv(pm.np);
         }
         // ---- end of tile: flush the tile's outputs with coalesced atomics
         //      (the next writes to ACC come two barriers later) ----
-        const bool last = (q + np == tinfo.x + tinfo.y);
-        if (last) {
-            zf* yc = a.y + col0(tcur);
+        if (cm.last) {
+            zf* yc = a.y + col0(cm.item);
             for (int idx = tid; idx < NSLOT * NR * NB; idx += NT) {
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int rr = rem / NB, el = rem - rr * NB;
-                const int sph = a.tsph ? a.tsph[(size_t)tile_of(tcur) * NSLOT + slot] : ((slot < TILE_B) ? (i0 + slot) : (j0b + slot - TILE_B));
-                if (a.tsph ? sph >= 0 : (!(diag && slot >= TILE_B) && sph < a.nsph)) red_add<float>(yc + (size_t)rr * a.ld + (size_t)sph * NB + el, ACC[idx]);
-                ACC[idx] = mk(0.f, 0.f);
+                const int sph = a.tsph ? a.tsph[(size_t)tile_of(cm.item) * NSLOT + slot] : ((slot < TILE_B) ? (cm.i0 + slot) : (cm.j0 + slot - TILE_B));
+                zf* av = ACC + (size_t)slot * SS + rem;
+                if (a.tsph ? sph >= 0 : (!(cm.diag && slot >= TILE_B) && sph < a.nsph)) red_add<float>(yc + (size_t)rr * a.ld + (size_t)sph * NB + el, *av);
+                *av = mk(0.f, 0.f);
             }
-            tcur += G;
-            if (tcur >= NI) break;
-            q = a.tiles[tile_of(tcur)].x;
-        } else {
-            q += np;
+            if (cm.item + G >= NI) break;
         }
-        t++;
     }
 }
 
