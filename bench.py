@@ -44,10 +44,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 EPS = 1.0e-12          # squared-norm criterion: ||r||/||b|| < 1e-6
-# DRAM bytes per algorithmic byte of the FP32 tiled translation pass of 2
-# columns, from the ncu capture of the 200-sphere aggregate (163.45 MB of
-# 158.56 MB)
-TRAFFIC_PER_ALG_BYTE = 163.45 / 158.56
+# DRAM bytes per algorithmic byte of the FP32 row-kernel translation pass of
+# 2 columns, from the ncu capture of the 200-sphere aggregate (179.01 MB of
+# 172.2 MB)
+TRAFFIC_PER_ALG_BYTE = 179.01 / 172.2
 NITER = 10000
 WORKLOAD = "fractal500"
 METRIC = "solves/s at 1e-6 residual (fractal aggregate N=500, x=2, both polarisations)"
@@ -552,12 +552,12 @@ def report_line(args, ws, R, ne):
         "tuned": {"iterations": it, "outer": m["stats"]["outer"], "passes64": m["stats"]["passes64"],
                   "passes32": m["stats"]["passes32"], "qext": m["qtot"][0, 0], "qext_plain": p["qtot"][0, 0],
                   "qext_rel_diff": abs(m["qtot"][0, 0] / p["qtot"][0, 0] - 1)},
-        "roofline": {"kernel": "translate_tiled_kernel<float> (pair translation pass)", "bound": "hbm",
+        "roofline": {"kernel": "translate_rows_kernel<9, 2> (FP32 pair translation pass, row kernel)", "bound": "hbm",
                      "achieved": round(achieved, 1) if achieved else None, "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4) if achieved else None,
                      "traffic": round(TRAFFIC_PER_ALG_BYTE * alg),
                      "traffic_source": "ncu dram__bytes_read+write of this kernel on the 200-sphere aggregate "
-                                       "(profiles/translate_tiled_fp32_fractal200.md), scaled by algorithmic bytes",
+                                       "(profiles/translate_rows_fp32_fractal200.md), scaled by algorithmic bytes",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": alg, "launch_ms": round(dur, 4), "launches": n32,
                      "canonical_equiv_gbs": round((canon32 + vec_bytes) / (dur * 1e-3) / 1e9, 1) if n32 else None},
