@@ -110,8 +110,10 @@ def rel_err(a, b):
 def errors_vs_oracle(qtot, smat, g, f):
     """Relative errors of a fixed-orientation result against the oracle's:
     each efficiency (unpolarised) and the 3 x 3 table, the 181-angle
-    scattering matrix (of S11's largest value) and the asymmetry parameter."""
-    out = {"qext": abs(qtot[0, 0] / f["qtot"][0, 0] - 1), "qabs": abs(qtot[1, 0] / f["qtot"][1, 0] - 1),
+    scattering matrix (of S11's largest value) and the asymmetry parameter.
+    Qabs is compared relative to Qext (non-absorbing spheres have Qabs at
+    rounding level, where a relative error means nothing)."""
+    out = {"qext": abs(qtot[0, 0] / f["qtot"][0, 0] - 1), "qabs_of_qext": abs(qtot[1, 0] - f["qtot"][1, 0]) / abs(f["qtot"][0, 0]),
            "qsca": abs(qtot[2, 0] / f["qtot"][2, 0] - 1), "qtot_3x3": rel_err(qtot, f["qtot"])}
     if smat is not None:
         out["smat_of_s11max"] = float(np.abs(smat - f["smat"]).max() / np.abs(f["smat"][:, 0, 0]).max())
