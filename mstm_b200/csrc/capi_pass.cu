@@ -712,6 +712,22 @@ int fft_build(mstmg_ctx* c)
                     const short sj = (short)(grp[p2.y] == ga ? gs[p2.y] : B + gs[p2.y]);
                     ps[q] = make_short2(si, sj);
                 }
+                // couples of consecutive pairs with four different output
+                // slots where the tile has them (the row kernel runs such a
+                // couple as one step)
+                for (size_t u = start; u + 1 < q;) {
+                    const short2 a0 = ps[u];
+                    bool found = false;
+                    for (size_t v = u + 1; v < q && !found; v++) {
+                        const short2 b0 = ps[v];
+                        if (a0.x != b0.x && a0.x != b0.y && a0.y != b0.x && a0.y != b0.y) {
+                            std::swap(ps[u + 1], ps[v]);
+                            std::swap(pr2[u + 1], pr2[v]);
+                            found = true;
+                        }
+                    }
+                    u += found ? 2 : 1;
+                }
                 tl.push_back(make_int4((int)start, (int)(q - start), 0, ga == gb ? 1 : 0));
             }
             pr.swap(pr2);
