@@ -385,6 +385,30 @@ long long mstmg_kernel_launches(void);
 int mstmg_planewave_noalloc(int nsphere, int order, const double *pos, double alpha, double sinc, int dir, double *pmnp,
                             void *stream);
 
+/* Single-cluster sharding over ranks (the reference's MPI partition of the
+ * pair translations: pairs dealt round-robin to the ranks of the group,
+ * mstm-modules-33.f90:6466-6474, and an allreduce of the results,
+ * mstm-scatprops-26.f90:152-156).  After mstmg_set_pair_shard(ctx, s, n) the
+ * context translates the tiles t of its pair list with t % n == s, so
+ * mstmg_interaction(_ex) and mstmg_translation_pass (prec 0, 1) return this
+ * shard's part of H x (times the Mie coefficients where asked; the Mie
+ * multiply is linear, so the parts still sum to the whole).  The caller sums
+ * the parts over its ranks and drives the iteration (mstm_b200.shard does
+ * both with torch.distributed); the solver entry points (mstmg_bicg,
+ * mstmg_fixed_orientation(_guess), mstmg_tmatrix) and the tensor-core pass
+ * refuse a sharded context.  Contexts of one sphere order with direct pairs
+ * only (MSTMG_ERR_UNSUPPORTED otherwise); n = 1 restores the whole pair set.
+ * Replaces the reference's MPI task loop inside external_to_external_expansion. */
+int mstmg_set_pair_shard(mstmg_ctx *ctx, int shard, int nshards);
+
+/* Right-hand sides of the fixed-orientation system (Mie x plane wave, both
+ * polarisations: neqns x 2, fixedorsoln's pmnpan, mstm-solver-8.f90:465-483)
+ * and the efficiencies of a given solution amnp (neqns x 2; qeff 3 x 3 x N,
+ * qtot 3 x 3, either may be NULL; qefficiencyfactors / qtotcalc): the two
+ * ends of mstmg_fixed_orientation for a caller that iterates itself. */
+int mstmg_fixed_orientation_rhs(mstmg_ctx *ctx, double alpha, double sinc, int dir, double *pmnpan);
+int mstmg_efficiencies(mstmg_ctx *ctx, double alpha, double sinc, int dir, const double *amnp, double *qeff, double *qtot);
+
 /* Message of the last error on this thread. */
 const char *mstmg_last_error(void);
 

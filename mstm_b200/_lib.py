@@ -70,6 +70,9 @@ SIGNATURES = {
     "mstmg_kernel_time": (c_int, [c_void_p, P(c_double), P(c_int), P(c_double), P(c_int)]),
     "mstmg_kernel_time_tc": (c_int, [c_void_p, P(c_double), P(c_int)]),
     "mstmg_last_host_syncs": (c_int, [c_void_p]),
+    "mstmg_set_pair_shard": (c_int, [c_void_p, c_int, c_int]),
+    "mstmg_fixed_orientation_rhs": (c_int, [c_void_p, c_double, c_double, c_int, c_void_p]),
+    "mstmg_efficiencies": (c_int, [c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p]),
     "mstmg_kernel_launches": (ctypes.c_longlong, []),
     "mstmg_planewave_noalloc": (c_int, [c_int, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p]),
     "mstmg_last_error": (ctypes.c_char_p, []),

@@ -176,6 +176,25 @@ class SphereCluster(_Context):
         stats = self.last_stats()
         return dict(amnp=amnp, qeff=qeff, qtot=qtot, maxerr=me.value, maxiter=mi.value, istat=st, **stats)
 
+    def set_pair_shard(self, shard, nshards):
+        """Translate only the tiles t with t % nshards == shard (the pairs of one
+        rank of a group; see mstm_b200.shard).  nshards = 1 restores all pairs."""
+        check(self._L.mstmg_set_pair_shard(self.ctx, int(shard), int(nshards)), "set_pair_shard")
+
+    def fixed_orientation_rhs(self, alpha=0.0, sinc=0.0, direction=1):
+        """Right-hand sides Mie x plane wave of both polarisations (neqns x 2)."""
+        out = np.zeros((self.number_eqns, 2), np.complex128, order="F")
+        check(self._L.mstmg_fixed_orientation_rhs(self.ctx, alpha, sinc, direction, _ptr(out)), "fixed_orientation_rhs")
+        return out
+
+    def efficiencies(self, amnp, alpha=0.0, sinc=0.0, direction=1):
+        """Efficiencies of a solution amnp (neqns x 2): dict(qeff (3,3,N), qtot (3,3))."""
+        a = np.asfortranarray(amnp, np.complex128)
+        qeff = np.zeros((3, 3, self.number_spheres), np.float64, order="F")
+        qtot = np.zeros((3, 3), np.float64, order="F")
+        check(self._L.mstmg_efficiencies(self.ctx, alpha, sinc, direction, _ptr(a), _ptr(qeff), _ptr(qtot)), "efficiencies")
+        return dict(qeff=qeff, qtot=qtot)
+
     def scattering(self, amnp, trans_eps=1.0e-5, max_t_order=100, nangles=181):
         """Azimuth-averaged scattering matrix (nangles, 4, 4), asymmetry parameter
         g, t_matrix_order and the common-origin expansion amnp0 (2T(T+2), 2;

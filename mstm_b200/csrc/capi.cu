@@ -57,6 +57,35 @@ int reject_ensemble(const mstmg_ctx* c, const char* fn)
     return MSTMG_OK;
 }
 
+// Solvers need the whole H x inside every iteration: a context holding one
+// shard of the pairs leaves the iteration to the caller (who sums the parts).
+int reject_sharded(const mstmg_ctx* c, const char* fn)
+{
+    if (c && c->nshards > 1) {
+        set_err(std::string(fn) + ": the context translates one shard of the pairs (mstmg_set_pair_shard); iterate over the "
+                                  "summed interactions instead");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    return MSTMG_OK;
+}
+
+// Upload the tiles of this context's shard (all tiles when nshards == 1).
+int apply_shard(mstmg_ctx* c)
+{
+    std::vector<int4> sub;
+    sub.reserve(c->tiles_host.size() / (size_t)c->nshards + 1);
+    for (size_t t = 0; t < c->tiles_host.size(); t++)
+        if ((int)(t % (size_t)c->nshards) == c->shard) sub.push_back(c->tiles_host[t]);
+    c->ntiles = (int)sub.size();
+    if (!sub.empty()) {
+        CK(c->tiles.alloc(sub.size()));
+        CK(cudaMemcpyAsync(c->tiles.p, sub.data(), sizeof(int4) * sub.size(), cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
+    c->layout_gen++;
+    return MSTMG_OK;
+}
+
 int check_kernel_err(mstmg_ctx* c)
 {
     int herr = 0;
@@ -86,11 +115,12 @@ int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const std::v
         u += rec;
     }
     c->npairs = np;
-    c->ntiles = (int)tl.size();
-    if (c->ntiles > 0) {
-        CK(c->tiles.alloc(tl.size()));
-        CK(cudaMemcpyAsync(c->tiles.p, tl.data(), sizeof(int4) * tl.size(), cudaMemcpyHostToDevice, c->st));
+    c->tiles_host = tl;
+    if (!c->tiled) {   // shards need tiles; a re-layout without them drops the shard
+        c->shard = 0;
+        c->nshards = 1;
     }
+    if (int rs = apply_shard(c)) return rs;
     c->op_units = u;
     c->maxrec = maxrec;
     // FP32 passes of the tiled path run the row kernel on row records unless
@@ -539,6 +569,20 @@ extern "C" int mstmg_ctx_set_positions(mstmg_ctx* c, const double* pos)
         return fft_build(c);
     }
     return MSTMG_OK;
+}
+
+extern "C" int mstmg_set_pair_shard(mstmg_ctx* c, int shard, int nshards)
+{
+    if (!c || nshards < 1 || shard < 0 || shard >= nshards) return MSTMG_ERR_ARG;
+    if (int rc0 = reject_ensemble(c, "mstmg_set_pair_shard")) return rc0;
+    if (nshards > 1 && (!c->tiled || (c->fft && c->fft->on) || c->ndense > 0)) {
+        set_err("mstmg_set_pair_shard: shards are tiles of direct pairs of one sphere order (no FFT grid, no dense pairs)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    c->shard = shard;
+    c->nshards = nshards;
+    if (c->tc_state == 1) c->tc_state = 0;   // the tensor-core images cover every pair
+    return apply_shard(c);
 }
 
 extern "C" int mstmg_neqns(const mstmg_ctx* c) { return c ? c->neqns : 0; }

@@ -311,6 +311,7 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
                              double* tmat, double* sphere_qeff, double* qtot, int* order_used, int* maxiter, double* maxerr)
 {
     if (int rc0 = reject_ensemble(c, "mstmg_tmatrix")) return rc0;
+    if (int rc1 = reject_sharded(c, "mstmg_tmatrix")) return rc1;
     NvtxRange nvtx_("mstmg_tmatrix");
     if (!c || t_matrix_order < 1 || t_matrix_order > 200 || !tmat || max_iterations < 1) {
         set_err("mstmg_tmatrix: bad arguments (1 <= t_matrix_order <= 200, max_iterations >= 1, tmat required)");

@@ -259,7 +259,7 @@ int fp32_chunk(mstmg_ctx* c, const zf* x, zf* y, int ncols, unsigned pattern2)
 // pairs): the cases the dense TF32 images serve.
 bool tc_eligible(const mstmg_ctx* c)
 {
-    if (c->opts.tensor_core < 0 || c->tc_state < 0) return false;
+    if (c->opts.tensor_core < 0 || c->tc_state < 0 || c->nshards > 1) return false;
     if (!c->tiled || c->ndense > 0 || (c->fft && c->fft->on) || c->npairs == 0) return false;
     return c->lmax >= 5 && tc_geom(c->lmax).NP <= 128;
 }

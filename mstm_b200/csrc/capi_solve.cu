@@ -144,6 +144,7 @@ extern "C" int mstmg_bicg(mstmg_ctx* c, int niter, double eps, const double* pnp
     NvtxRange nvtx_("mstmg_bicg");
     if (!c || !pnp || !anp) return MSTMG_ERR_ARG;
     if (int rc0 = reject_ensemble(c, "mstmg_bicg")) return rc0;
+    if (int rc1 = reject_sharded(c, "mstmg_bicg")) return rc1;
     int rc = ensure_ops(c, 0, initialize != 0);
     if (rc) return rc;
     const int ne = c->neqns;
@@ -302,6 +303,7 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
 {
     if (!c || !amnp) return MSTMG_ERR_ARG;
     if (int rc0 = reject_ensemble(c, "mstmg_fixed_orientation")) return rc0;
+    if (int rc1 = reject_sharded(c, "mstmg_fixed_orientation")) return rc1;
     const int ne = c->neqns;
     SlotMaps sm = c->sm();
     c->passes64 = c->passes32 = 0;
@@ -494,6 +496,45 @@ extern "C" int mstmg_ensemble_fixed_orientation(mstmg_ctx* c, double alpha, doub
     rc = check_kernel_err(c);
     if (rc) return rc;
     return istat;
+}
+
+// The fixed-orientation system's right-hand sides, Mie x plane wave of both
+// polarisations (fixedorsoln's pmnpan, mstm-solver-8.f90:465-483), for a
+// caller that drives the iteration itself.
+extern "C" int mstmg_fixed_orientation_rhs(mstmg_ctx* c, double alpha, double sinc, int dir, double* pmnpan)
+{
+    if (!c || !pmnpan) return MSTMG_ERR_ARG;
+    if (int rc0 = reject_ensemble(c, "mstmg_fixed_orientation_rhs")) return rc0;
+    const int ne = c->neqns;
+    SlotMaps sm = c->sm();
+    launch_planewave(alpha, sinc, dir, c->lmax, ne, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p,
+                     c->pmnp.p, c->st);
+    for (int p = 0; p < 2; p++)
+        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, 1, 0, c->pmnp.p + (size_t)p * ne,
+                           c->bvec64.p + (size_t)p * ne, c->st);
+    CK(cudaGetLastError());
+    CK(copy_out(pmnpan, c->bvec64.p, sizeof(zd) * 2 * (size_t)ne, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return check_kernel_err(c);
+}
+
+// Efficiencies of a given fixed-orientation solution (qefficiencyfactors and
+// qtotcalc, as mstmg_fixed_orientation reports them).
+extern "C" int mstmg_efficiencies(mstmg_ctx* c, double alpha, double sinc, int dir, const double* amnp, double* qeff, double* qtot)
+{
+    if (!c || !amnp) return MSTMG_ERR_ARG;
+    if (int rc0 = reject_ensemble(c, "mstmg_efficiencies")) return rc0;
+    const int ne = c->neqns;
+    launch_planewave(alpha, sinc, dir, c->lmax, ne, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p,
+                     c->pmnp.p, c->st);
+    CK(copy_in(c->amnp.p, amnp, sizeof(zd) * 2 * (size_t)ne, c->st));
+    launch_qeff(c->n, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, mk(c->opts.medium_re, c->opts.medium_im), c->an_inv.p,
+                c->amnp.p, c->pmnp.p, ne, c->qeff.p, c->xg, c->qtot.p, c->st);
+    CK(cudaGetLastError());
+    if (qeff) CK(copy_out(qeff, c->qeff.p, sizeof(double) * 9 * (size_t)c->n, c->st));
+    if (qtot) CK(copy_out(qtot, c->qtot.p, sizeof(double) * 9, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return check_kernel_err(c);
 }
 
 extern "C" int mstmg_last_host_syncs(const mstmg_ctx* c) { return c ? c->host_syncs : -1; }

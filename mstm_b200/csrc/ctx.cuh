@@ -311,6 +311,10 @@ struct mstmg_ctx {
     DevBuf<short2> pslot;
     bool tiled = false;   // monodisperse cluster: pairs stored in tile order for the fast kernel
     int row32 = 0;        // tiled: floats per FP32 row record (translate_rows.cuh); 0: FP32 records as FP64
+    // pair shard (mstmg_set_pair_shard): this context translates the tiles
+    // t with t % nshards == shard; all tiles kept on the host
+    int shard = 0, nshards = 1;
+    std::vector<int4> tiles_host;
     DevBuf<double> op64;
     DevBuf<float> op32;
     bool ops64_ready = false, ops32_ready = false;
@@ -403,6 +407,8 @@ struct EnsSeg {
 // capi.cu
 void resolve_timing(mstmg_ctx* c);
 int reject_ensemble(const mstmg_ctx* c, const char* fn);
+int reject_sharded(const mstmg_ctx* c, const char* fn);
+int apply_shard(mstmg_ctx* c);
 int check_kernel_err(mstmg_ctx* c);
 int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const std::vector<int4>& tl);
 int ensure_gentran(mstmg_ctx* c, int lm);
