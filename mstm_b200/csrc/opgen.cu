@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(128) opgen_axial_kernel(OpGenArgs a)
                     z[0] = (float)v0.x;
                     z[1] = (float)v0.y;
                 } else {
-                    float* z = row32 + rr_z_off(m, nt) + (n - m1) * 4 * cols + 4 * (l - m1);
+                    float* z = row32 + rr_z_off(m, nt) + (n - m1) * 4 * rr_zq(cols) + 4 * (l - m1);
                     z[0] = (float)v0.x;
                     z[1] = (float)v0.y;
                     z[2] = (float)v1.x;

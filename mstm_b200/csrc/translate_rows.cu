@@ -61,8 +61,10 @@ struct RowSched {
 
 __host__ __device__ constexpr size_t al128(size_t v) { return (v + 127) & ~(size_t)127; }
 
-// packed-S offset of degree n: entries (n, m = 0..n) of all degrees in one array
-__host__ __device__ constexpr int sofs(int n) { return (n - 1) * (n + 2) / 2; }
+// the axial products' (s', t') by degree m: entries n = max(1, m)..L of m
+// after those of 0..m-1, so the rows of one m are consecutive
+template <int L> __host__ __device__ constexpr int goff(int m) { return m == 0 ? 0 : L + (m - 1) * (L + 1) - (m - 1) * m / 2; }
+template <int L> __host__ __device__ constexpr int gidx(int m, int n) { return goff<L>(m) + n - (m < 1 ? 1 : m); }
 
 // strides padded for the shared-memory banks: (s', t') columns an odd number
 // of 16-byte units apart, tile-output slots an odd number of complex values
@@ -197,7 +199,10 @@ template <int L, int M, int H, int STRIDE> __device__ __forceinline__ void c_uni
 {
     constexpr int m1 = M < 1 ? 1 : M, dim = L - m1 + 1;
     if constexpr (M == 0) {
-        constexpr int QN = (dim + 1) / 2, QH = (QN + H - 1) / H;   // quads (2 complex) per row, per lane
+        // quads (2 complex) per row in the record and per lane; with H = 2 the
+        // even row length splits exactly and no lane needs a bounds test
+        constexpr int Q0 = rr_zw0(L) / 4, QH = (Q0 + H - 1) / H;
+        constexpr bool PRED = QH * H > Q0;
         CIn in[2 * QH];
 #pragma unroll
         for (int t = 0; t < 2 * QH; t++) {
@@ -209,7 +214,7 @@ template <int L, int M, int H, int STRIDE> __device__ __forceinline__ void c_uni
             float2 a0 = f2(0.f, 0.f), b0 = a0, a1 = a0, b1 = a0;
 #pragma unroll
             for (int t = 0; t < QH; t++) {
-                if (QH * ln.h + t < QN) {
+                if (!PRED || QH * ln.h + t < Q0) {
                     const float4 z = rw[t];
                     a0 = __ffma2_rn(f2(z.x, z.y), in[2 * t].a, a0);
                     b0 = __ffma2_rn(f2(z.x, z.y), in[2 * t].b, b0);
@@ -219,10 +224,11 @@ template <int L, int M, int H, int STRIDE> __device__ __forceinline__ void c_uni
             }
             const zf g = hsum<H, STRIDE>(mk(a0.x + b0.y + a1.x + b1.y, a0.y + b0.x + a1.y + b1.x));
             // m = 0: s'(0) = g, t'(0) = 0
-            if (ln.act && ln.h == 0) ln.g[sofs(line)] = make_float4(g.x, 0.f, g.y, 0.f);
+            if (ln.act && ln.h == 0) ln.g[gidx<L>(0, line)] = make_float4(g.x, 0.f, g.y, 0.f);
         }
     } else {
-        constexpr int QN = dim, QH = (QN + H - 1) / H;   // quads (Z0, Z1 of one l) per row, per lane
+        constexpr int ZQ = rr_zq(dim), QH = (ZQ + H - 1) / H;   // quads (Z0, Z1 of one l) per row, per lane
+        constexpr bool PRED = QH * H > ZQ;
         CIn in0[QH], in1[QH];
 #pragma unroll
         for (int t = 0; t < QH; t++) {
@@ -236,12 +242,13 @@ template <int L, int M, int H, int STRIDE> __device__ __forceinline__ void c_uni
             in0[t] = cin(ln.p ? am : ap);
             in1[t] = cin(ln.p ? ap : am);
         }
+        const float sg = (M & 1) ? -1.f : 1.f;
         for (int line = l0; line < l1; line++) {
-            const float4* rw = reinterpret_cast<const float4*>(ln.rec + rr_z_off(M, L) + (line - m1) * 4 * dim) + QH * ln.h;
+            const float4* rw = reinterpret_cast<const float4*>(ln.rec + rr_z_off(M, L) + (line - m1) * 4 * ZQ) + QH * ln.h;
             float2 a0 = f2(0.f, 0.f), b0 = a0, a1 = a0, b1 = a0;
 #pragma unroll
             for (int t = 0; t < QH; t++) {
-                if (QH * ln.h + t < QN) {
+                if (!PRED || QH * ln.h + t < ZQ) {
                     const float4 z = rw[t];
                     a0 = __ffma2_rn(f2(z.x, z.y), in0[t].a, a0);
                     b0 = __ffma2_rn(f2(z.x, z.y), in0[t].b, b0);
@@ -252,9 +259,8 @@ template <int L, int M, int H, int STRIDE> __device__ __forceinline__ void c_uni
             const zf o0 = hsum<H, STRIDE>(mk(a0.x + b0.y, a0.y + b0.x));
             const zf o1 = hsum<H, STRIDE>(mk(a1.x + b1.y, a1.y + b1.x));
             const zf gp = ln.p ? o1 : o0, gm = ln.p ? o0 : o1;
-            const float sg = (M & 1) ? -1.f : 1.f;
             // s'(m) = g(m) + (-1)^m g(-m), t'(m) = g(m) - (-1)^m g(-m), stored as (s'.x, t'.x, s'.y, t'.y)
-            float* gs = reinterpret_cast<float*>(ln.g + sofs(line) + M);
+            float* gs = reinterpret_cast<float*>(ln.g + gidx<L>(M, line));
             if (ln.act && ln.h == 0) {
                 const zf sv = gp + cpos(gm, sg);
                 gs[0] = sv.x;
@@ -277,7 +283,7 @@ template <int L, int N, int H> __device__ __forceinline__ void d_unit(const Lane
     float2 X[N + 1], Y[N + 1];
 #pragma unroll
     for (int m = 0; m <= N; m++) {
-        const float4 g = ln.g[sofs(N) + m];
+        const float4 g = ln.g[gidx<L>(m, N)];
         X[m] = m ? f2(g.x, g.y) : f2(2.f * g.x, 0.f);
         Y[m] = m ? f2(g.z, g.w) : f2(2.f * g.z, 0.f);
     }

@@ -12,8 +12,10 @@
 //       [E_n(k,0), 0, E_n(k,1), O_n(k,1), ..., E_n(k,n), O_n(k,n), 0...]
 //       (O_n(0, .) = 0)
 //   axial, m = 0: rows n = 1..L of rr_zw0(L) floats, Z_0(n, l) complex for l = 1..L (0-padded)
-//   axial, m = 1..L: rows n = m..L of 4 (L - m + 1) floats,
-//       [Z_m^0(n, l), Z_m^1(n, l)] for l = m..L (the two modes' blocks interleaved)
+//   axial, m = 1..L: rows n = m..L of 4 rr_zq(L - m + 1) floats,
+//       [Z_m^0(n, l), Z_m^1(n, l)] for l = m..L (the two modes' blocks interleaved, 0-padded)
+//   (the axial rows hold an even number of 16-byte units, so that two lanes
+//   split every row without a bounds test)
 //   padding to row_record_units(L) = 4 (mod 32) floats, so that the records of
 //   consecutive pairs fall on different shared-memory banks.
 __host__ __device__ constexpr int rr_hdr(int L) { return (2 * (L + 1) + 3) & ~3; }
@@ -24,12 +26,13 @@ __host__ __device__ constexpr int rr_rot_off(int n, int L)
     for (int q = 1; q < n; q++) s += (q + 1) * rr_rw(q);
     return s;
 }
-__host__ __device__ constexpr int rr_zw0(int L) { return 2 * ((L + 1) & ~1); }
+__host__ __device__ constexpr int rr_zq(int dim) { return (dim + 1) & ~1; }   // 16-byte units of an m > 0 row
+__host__ __device__ constexpr int rr_zw0(int L) { return 4 * rr_zq((L + 1) / 2); }   // floats of an m = 0 row
 __host__ __device__ constexpr int rr_z_off(int m, int L)
 {
     int s = rr_rot_off(L + 1, L);
     if (m > 0) s += L * rr_zw0(L);
-    for (int q = 1; q < m; q++) s += 4 * (L - q + 1) * (L - q + 1);
+    for (int q = 1; q < m; q++) s += 4 * (L - q + 1) * rr_zq(L - q + 1);
     return s;
 }
 __host__ __device__ constexpr int row_record_units(int L)
