@@ -396,8 +396,10 @@ int mstmg_planewave_noalloc(int nsphere, int order, const double *pos, double al
  * the parts over its ranks and drives the iteration (mstm_b200.shard does
  * both with torch.distributed); the solver entry points (mstmg_bicg,
  * mstmg_fixed_orientation(_guess), mstmg_tmatrix) and the tensor-core pass
- * refuse a sharded context.  Contexts of one sphere order with direct pairs
- * only (MSTMG_ERR_UNSUPPORTED otherwise); n = 1 restores the whole pair set.
+ * refuse a sharded context.  Contexts of one sphere order without dense
+ * pairs (MSTMG_ERR_UNSUPPORTED otherwise); on the FFT path the near-pair
+ * tiles are dealt and shard 0 adds the far field.  n = 1 restores the whole
+ * pair set.
  * Replaces the reference's MPI task loop inside external_to_external_expansion. */
 int mstmg_set_pair_shard(mstmg_ctx *ctx, int shard, int nshards);
 

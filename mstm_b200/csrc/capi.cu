@@ -575,8 +575,8 @@ extern "C" int mstmg_set_pair_shard(mstmg_ctx* c, int shard, int nshards)
 {
     if (!c || nshards < 1 || shard < 0 || shard >= nshards) return MSTMG_ERR_ARG;
     if (int rc0 = reject_ensemble(c, "mstmg_set_pair_shard")) return rc0;
-    if (nshards > 1 && (!c->tiled || (c->fft && c->fft->on) || c->ndense > 0)) {
-        set_err("mstmg_set_pair_shard: shards are tiles of direct pairs of one sphere order (no FFT grid, no dense pairs)");
+    if (nshards > 1 && (!c->tiled || c->ndense > 0)) {
+        set_err("mstmg_set_pair_shard: shards are tiles of pairs of one sphere order (no dense pairs)");
         return MSTMG_ERR_UNSUPPORTED;
     }
     c->shard = shard;

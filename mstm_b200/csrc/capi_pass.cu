@@ -131,7 +131,9 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
         launch_dense_apply<T>(dense_args(c), drec, x, y, c->neqns, nrhs, contran, c->st);
         CK(cudaGetLastError());
     }
-    if (c->npairs == 0) return (c->fft && c->fft->on) ? fft_far<T>(c, x, y, nrhs * nchunk, contran) : MSTMG_OK;
+    // a sharded context: shard 0 adds the FFT path's far field, every shard its near-pair tiles
+    const bool far = c->fft && c->fft->on && c->shard == 0;
+    if (c->npairs == 0) return far ? fft_far<T>(c, x, y, nrhs * nchunk, contran) : MSTMG_OK;
     TransArgs<T> a;
     a.npairs = c->npairs;
     a.pairs = c->pairs.p;
@@ -199,7 +201,7 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
     }
     if (sizeof(T) == 8) c->passes64++;
     else c->passes32++;
-    if (c->fft && c->fft->on) return fft_far<T>(c, x, y, nrhs * nchunk, contran);
+    if (far) return fft_far<T>(c, x, y, nrhs * nchunk, contran);
     return MSTMG_OK;
 }
 
@@ -728,7 +730,8 @@ int fft_build(mstmg_ctx* c)
                     }
                     u += found ? 2 : 1;
                 }
-                tl.push_back(make_int4((int)start, (int)(q - start), 0, ga == gb ? 1 : 0));
+                // z: the tile's row of the sphere lists (tiles may be dealt to shards)
+                tl.push_back(make_int4((int)start, (int)(q - start), (int)tl.size(), ga == gb ? 1 : 0));
             }
             pr.swap(pr2);
             CK(c->tsph.alloc(ts.size()));

@@ -557,7 +557,8 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int rr = rem / NB, el = rem - rr * NB;
-                const int sph = a.tsph ? a.tsph[(size_t)tile_of(cm.item) * NSLOT + slot] : ((slot < TILE_B) ? (cm.i0 + slot) : (cm.j0 + slot - TILE_B));
+                // grouped tiles carry their sphere-list row in z (i0 << 16 | j0 here)
+                const int sph = a.tsph ? a.tsph[(size_t)((cm.i0 << 16) | cm.j0) * NSLOT + slot] : ((slot < TILE_B) ? (cm.i0 + slot) : (cm.j0 + slot - TILE_B));
                 zf* av = ACC + (size_t)slot * SS + rem;
                 if (a.tsph ? sph >= 0 : (!(cm.diag && slot >= TILE_B) && sph < a.nsph)) red_add<float>(yc + (size_t)rr * a.ld + (size_t)sph * NB + el, *av);
                 *av = mk(0.f, 0.f);

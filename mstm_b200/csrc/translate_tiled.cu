@@ -425,7 +425,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int r = rem / NB, el = rem - r * NB;
-                const int sph = a.tsph ? a.tsph[(size_t)tile_of(tcur) * NSLOT + slot] : ((slot < B) ? (i0 + slot) : (j0 + slot - B));
+                // grouped tiles carry their sphere-list row in z
+                const int sph = a.tsph ? a.tsph[(size_t)tinfo.z * NSLOT + slot] : ((slot < B) ? (i0 + slot) : (j0 + slot - B));
                 if (a.tsph ? sph >= 0 : (!(diag && slot >= B) && sph < a.nsph)) {
                     cpx<T> v = ACC[idx];
                     red_add<T>(yc + (size_t)r * a.ld + (size_t)sph * NB + el, v);

@@ -6,7 +6,7 @@
 
 template <typename T> struct TiledArgs {
     int ntiles;
-    const int4* tiles;       // (pair start, pair count, (i0<<16)|j0, diagonal)
+    const int4* tiles;       // (pair start, pair count, (i0<<16)|j0 -- grouped tiles: the row of tsph --, diagonal)
     const int2* pairs;       // tile-ordered pairs, i < j
     const T* ops;            // records in pair order, op_record_units(L,L) each
     const cpx<T>* x;         // ld x nrhs

@@ -4,8 +4,9 @@ CPU (gloo, world size 2): the reference's BiCG driven on interactions summed
 over the ranks, each rank holding one part of a dense operator, reaches the
 dense solution and the single-rank iterates.  GPU: the shards of a cluster's
 tiles sum to the whole translation pass (FP64 to 1e-12 and FP32 to 2e-6 of
-the largest output) and to the whole Mie-multiplied interaction, plain and
-conjugate-transpose columns; a BiCG on two shard contexts summed in one
+the largest output; on the FFT path too, shard 0 adding the far field) and
+to the whole Mie-multiplied interaction, plain and conjugate-transpose
+columns; a BiCG on two shard contexts summed in one
 process gives the library's FP64 fixed-orientation solve (its iterations,
 efficiencies to 1e-9); the solvers refuse a sharded context.
 """
@@ -171,9 +172,29 @@ def test_sharded_context_refuses_the_solvers():
     with pytest.raises(MstmgError):
         g.set_pair_shard(2, 2)
     g.close()
+
+
+@pytest.mark.gpu
+def test_fft_shards_sum_to_the_whole_pass():
+    """On the FFT path the near-pair tiles are dealt to the shards and shard 0
+    adds the far field: the shards still sum to the whole pass."""
+    from mstm_b200 import api
     cyl, _ = C.rsa_cylinder(300, 1.0, 0.25, 1.0, seed=3)
-    f = api.SphereCluster(cyl, np.full(len(cyl), 1.0), np.full(len(cyl), 1.31 + 0j), mie_epsilon=-7, precision="mixed")
-    f.fft_setup(d_cell=4.0)
-    with pytest.raises(MstmgError):
-        f.set_pair_shard(0, 2)
-    f.close()
+    n = len(cyl)
+    mk = lambda: api.SphereCluster(cyl, np.full(n, 1.0), np.full(n, 1.31 + 0j), mie_epsilon=-7, precision="mixed")
+    whole = mk()
+    whole.fft_setup(d_cell=4.0)
+    parts = []
+    for s in range(2):
+        g = mk()
+        g.fft_setup(d_cell=4.0)
+        g.set_pair_shard(s, 2)
+        parts.append(g)
+    rng = np.random.default_rng(11)
+    x = rng.normal(size=(whole.number_eqns, 2)) + 1j * rng.normal(size=(whole.number_eqns, 2))
+    for prec, tol in (("fp64", 1e-12), ("fp32", 2e-6)):
+        y = whole.translation_pass(x, [0, 1], prec)
+        ys = parts[0].translation_pass(x, [0, 1], prec) + parts[1].translation_pass(x, [0, 1], prec)
+        assert np.abs(ys - y).max() <= tol * np.abs(y).max(), prec
+    for g in parts + [whole]:
+        g.close()
