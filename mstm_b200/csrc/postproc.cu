@@ -347,17 +347,8 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
 // ---------------------------------------------------------------------------
 // fosmexpansion: one CTA per (n, l); threads over m; atomics into s arrays
 // ---------------------------------------------------------------------------
-// The CTA's sums go to shared memory first (the eight elements of the four
-// 4 x 4 tables this expansion fills, per Hankel order w) and to the global
-// tables once, at the end: the atomics into a few hundred global addresses
-// from every (n, l, m, p, q, w) were the kernel's cost.
-#define FOSM_NE 8
 __global__ void fosm_kernel(int ntot, const zd* a0, VCTab tab, double* s00, double* s02, double* sp22, double* sm22, double* vscr)
 {
-  extern __shared__ double facc[];   // FOSM_NE x (2 ntot + 1)
-  const int W = 2 * ntot + 1;
-  for (int k = threadIdx.x; k < FOSM_NE * W; k += blockDim.x) facc[k] = 0.0;
-  __syncthreads();
   double* base = vscr + ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 5 * (2 * ntot + 2);
   for (int nl = blockIdx.x; nl < ntot * ntot; nl += gridDim.x) {
     int n = nl / ntot + 1, l = nl % ntot + 1;
@@ -398,46 +389,27 @@ __global__ void fosm_kernel(int ntot, const zd* a0, VCTab tab, double* s00, doub
                 for (int w = wmin; w <= wmax; w++) {
                     double m1w = pm1(w);
                     bool ev = ((n + l + w + p + q) % 2 == 0);
-#define SA(e) (&facc[(e) * W + w])
-                    if (ev) atomicAdd(SA(0), -((m1m * fnl) * a1122 * (cm1p1[w] * cmmpm[w])).x / 2.0);                   // s00(1,1)
-                    else atomicAdd(SA(1), (imul(mk(0.5, 0.0)) * (m1m * fnl) * a2112 * (cm1p1[w] * cmmpm[w])).x);         // s00(4,4)
+#define SS(arr, i, j) (&arr[((i) - 1) + 4 * ((j) - 1) + 16 * w])
+                    if (ev) atomicAdd(SS(s00, 1, 1), -((m1m * fnl) * a1122 * (cm1p1[w] * cmmpm[w])).x / 2.0);
+                    else atomicAdd(SS(s00, 4, 4), (imul(mk(0.5, 0.0)) * (m1m * fnl) * a2112 * (cm1p1[w] * cmmpm[w])).x);
                     if (w < 2) continue;
                     if (ev) {
-                        atomicAdd(SA(2), -((m1mq * a1122) * fnl * (cm1m1[w] * cmmpm[w])).x / 2.0);                   // s02(2,1)
-                        atomicAdd(SA(3), -((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).x / 4.0);                   // s02(1,2)
-                        atomicAdd(SA(3), -((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).x / 4.0);
+                        atomicAdd(SS(s02, 2, 1), -((m1mq * a1122) * fnl * (cm1m1[w] * cmmpm[w])).x / 2.0);
+                        atomicAdd(SS(s02, 1, 2), -((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).x / 4.0);
+                        atomicAdd(SS(s02, 1, 2), -((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).x / 4.0);
                     } else {
-                        atomicAdd(SA(4), (imul(mk(-0.5, 0.0)) * (m1mq * a2112) * fnl * (cm1m1[w] * cmmpm[w])).y);    // s02(3,4)
-                        atomicAdd(SA(5), ((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).y / 4.0);                    // s02(4,3)
-                        atomicAdd(SA(5), -((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).y / 4.0);
+                        atomicAdd(SS(s02, 3, 4), (imul(mk(-0.5, 0.0)) * (m1mq * a2112) * fnl * (cm1m1[w] * cmmpm[w])).y);
+                        atomicAdd(SS(s02, 4, 3), ((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).y / 4.0);
+                        atomicAdd(SS(s02, 4, 3), -((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).y / 4.0);
                     }
-                    atomicAdd(SA(6), -((m1mnpl * m1w * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0);             // sm22(2,2)
-                    atomicAdd(SA(7), -((m1mq * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0);                     // sp22(2,2)
-                    atomicAdd(SA(6), -((m1mq * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0);
-                    atomicAdd(SA(7), -((m1mnpl * m1w * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0);
-#undef SA
+                    atomicAdd(SS(sm22, 2, 2), -((m1mnpl * m1w * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0);
+                    atomicAdd(SS(sp22, 2, 2), -((m1mq * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0);
+                    atomicAdd(SS(sm22, 2, 2), -((m1mq * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0);
+                    atomicAdd(SS(sp22, 2, 2), -((m1mnpl * m1w * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0);
+#undef SS
                 }
             }
     }
-  }
-  __syncthreads();
-  // the CTA's sums into the global tables, element (i, j) of order w at (i-1) + 4 (j-1) + 16 w
-  for (int k = threadIdx.x; k < FOSM_NE * W; k += blockDim.x) {
-    const double v = facc[k];
-    if (v == 0.0) continue;
-    const int e = k / W, w = k - e * W;
-    double* dst;
-    switch (e) {
-    case 0: dst = s00 + 0 + 4 * 0; break;
-    case 1: dst = s00 + 3 + 4 * 3; break;
-    case 2: dst = s02 + 1 + 4 * 0; break;
-    case 3: dst = s02 + 0 + 4 * 1; break;
-    case 4: dst = s02 + 2 + 4 * 3; break;
-    case 5: dst = s02 + 3 + 4 * 2; break;
-    case 6: dst = sm22 + 1 + 4 * 1; break;
-    default: dst = sp22 + 1 + 4 * 1; break;
-    }
-    atomicAdd(dst + 16 * w, v);
   }
 }
 
@@ -734,7 +706,7 @@ void launch_fosm(int ntot, const zd* a0, const double* bcof, const double* fnr, 
                  double* sm22, double* vscr, cudaStream_t st)
 {
     VCTab t{bcof, fnr, nbc};
-    fosm_kernel<<<fosm_grid(ntot), 32, sizeof(double) * FOSM_NE * (2 * ntot + 1), st>>>(ntot, a0, t, s00, s02, sp22, sm22, vscr);
+    fosm_kernel<<<fosm_grid(ntot), 32, 0, st>>>(ntot, a0, t, s00, s02, sp22, sm22, vscr);
     fosm_patch_kernel<<<(2 * ntot + 1 + 63) / 64, 64, 0, st>>>(ntot, s00, s02, sp22, sm22, 1.0);
     launch_counter() += 2;
 }
