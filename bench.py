@@ -46,8 +46,8 @@ sys.path.insert(0, ROOT)
 EPS = 1.0e-12          # squared-norm criterion: ||r||/||b|| < 1e-6
 # DRAM bytes per byte of row records and vectors of the FP32 row-kernel
 # translation pass of 2 columns, from the ncu capture of the 200-sphere
-# aggregate (179.01 MB of 172.2 MB)
-TRAFFIC_PER_ALG_BYTE = 179.01 / 172.2
+# aggregate (189.06 MB of 185.0 MB)
+TRAFFIC_PER_ALG_BYTE = 189.06 / 185.0
 NITER = 10000
 WORKLOAD = "fractal500"
 METRIC = "solves/s at 1e-6 residual (fractal aggregate N=500, x=2, both polarisations)"
@@ -562,7 +562,7 @@ def report_line(args, ws, R, ne):
                      "traffic": round(TRAFFIC_PER_ALG_BYTE * (stored32 + vec_bytes)),
                      "row_record_bytes": stored32,
                      "traffic_source": "ncu dram__bytes_read+write of this kernel on the 200-sphere aggregate "
-                                       "(profiles/translate_rows_fp32_fractal200.md: 1.04x the row records and vectors "
+                                       "(profiles/translate_rows_fp32_fractal200.md: 1.02x the row records and vectors "
                                        "read and written), scaled to this workload's row records",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": alg, "launch_ms": round(dur, 4), "launches": n32,
