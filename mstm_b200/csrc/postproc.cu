@@ -345,11 +345,27 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// fosmexpansion: one CTA per (n, l); threads over m; atomics into s arrays
+// fosmexpansion: one warp per (n, l); lanes over m, 32 at a time.  For each
+// (p, q, w) the lanes' contributions go to the same few table elements, so
+// the warp adds them up first (a butterfly over the lanes) and one lane
+// issues the atomics into the global tables.
 // ---------------------------------------------------------------------------
-__global__ void fosm_kernel(int ntot, const zd* a0, VCTab tab, double* s00, double* s02, double* sp22, double* sm22, double* vscr)
+__device__ __forceinline__ double warp_allsum(double v)
 {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(32) fosm_kernel(int ntot, const zd* a0, VCTab tab, double* s00, double* s02, double* sp22, double* sm22, double* vscr)
+{
+  const int lane = threadIdx.x;
   double* base = vscr + ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 5 * (2 * ntot + 2);
+  double* cm1p1 = base;
+  double* cm1m1 = cm1p1 + (2 * ntot + 2);
+  double* cmmpm = cm1m1 + (2 * ntot + 2);
+  double* cmmm2pm = cmmpm + (2 * ntot + 2);
+  double* cmmp2pm = cmmm2pm + (2 * ntot + 2);
   for (int nl = blockIdx.x; nl < ntot * ntot; nl += gridDim.x) {
     int n = nl / ntot + 1, l = nl % ntot + 1;
     const int nb = 2 * ntot * (ntot + 2);
@@ -357,23 +373,21 @@ __global__ void fosm_kernel(int ntot, const zd* a0, VCTab tab, double* s00, doub
     int wmin = abs(n - l), wmax = n + l;
     zd fnl = sqrt((double)((n + n + 1) * (l + l + 1))) * ipow_z(l - n);
     int mm = min(n, l + 2);
-    for (int m = -mm + (int)threadIdx.x; m <= mm; m += blockDim.x) {
-        double* cm1p1 = base;
-        double* cm1m1 = cm1p1 + (2 * ntot + 2);
-        double* cmmpm = cm1m1 + (2 * ntot + 2);
-        double* cmmm2pm = cmmpm + (2 * ntot + 2);
-        double* cmmp2pm = cmmm2pm + (2 * ntot + 2);
-        vc_func(tab, -1, n, 1, l, cm1p1);
-        vc_func(tab, -1, n, -1, l, cm1m1);
-        if (abs(m) <= l) vc_func(tab, -m, n, m, l, cmmpm);
+    // the m-independent couplings, once per (n, l)
+    vc_func(tab, -1, n, 1, l, cm1p1);
+    vc_func(tab, -1, n, -1, l, cm1m1);
+    for (int m0 = -mm; m0 <= mm; m0 += 32) {
+        const int m = m0 + lane;
+        const bool act = m <= mm;
+        if (act && abs(m) <= l) vc_func(tab, -m, n, m, l, cmmpm);
         else for (int w = 0; w <= n + l; w++) cmmpm[w] = 0.0;
-        if (abs(-2 + m) <= l) vc_func(tab, -m, n, -2 + m, l, cmmm2pm);
+        if (act && abs(-2 + m) <= l) vc_func(tab, -m, n, -2 + m, l, cmmm2pm);
         else for (int w = 0; w <= n + l; w++) cmmm2pm[w] = 0.0;
-        if (abs(2 + m) <= l) vc_func(tab, -m, n, 2 + m, l, cmmp2pm);
+        if (act && abs(2 + m) <= l) vc_func(tab, -m, n, 2 + m, l, cmmp2pm);
         else for (int w = 0; w <= n + l; w++) cmmp2pm[w] = 0.0;
         double m1m = pm1(m);
         auto A = [&](int pol, int mq, int nq, int p) -> zd {
-            if (mq < -nq || mq > nq) return mk(0.0, 0.0);
+            if (!act || mq < -nq || mq > nq) return mk(0.0, 0.0);
             return a0[(size_t)pol * nb + aidx(mq, nq, 0, ntot) + (size_t)half * p];
         };
         for (int p = 1; p <= 2; p++)
@@ -388,24 +402,43 @@ __global__ void fosm_kernel(int ntot, const zd* a0, VCTab tab, double* s00, doub
                 zd a1m2 = (a1n - imul(a2n)) * cj(A(0, m + 2, l, q - 1) + imul(A(1, m + 2, l, q - 1)));
                 for (int w = wmin; w <= wmax; w++) {
                     double m1w = pm1(w);
-                    bool ev = ((n + l + w + p + q) % 2 == 0);
+                    bool ev = ((n + l + w + p + q) % 2 == 0);   // one parity for the whole warp
 #define SS(arr, i, j) (&arr[((i) - 1) + 4 * ((j) - 1) + 16 * w])
-                    if (ev) atomicAdd(SS(s00, 1, 1), -((m1m * fnl) * a1122 * (cm1p1[w] * cmmpm[w])).x / 2.0);
-                    else atomicAdd(SS(s00, 4, 4), (imul(mk(0.5, 0.0)) * (m1m * fnl) * a2112 * (cm1p1[w] * cmmpm[w])).x);
-                    if (w < 2) continue;
-                    if (ev) {
-                        atomicAdd(SS(s02, 2, 1), -((m1mq * a1122) * fnl * (cm1m1[w] * cmmpm[w])).x / 2.0);
-                        atomicAdd(SS(s02, 1, 2), -((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).x / 4.0);
-                        atomicAdd(SS(s02, 1, 2), -((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).x / 4.0);
-                    } else {
-                        atomicAdd(SS(s02, 3, 4), (imul(mk(-0.5, 0.0)) * (m1mq * a2112) * fnl * (cm1m1[w] * cmmpm[w])).y);
-                        atomicAdd(SS(s02, 4, 3), ((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).y / 4.0);
-                        atomicAdd(SS(s02, 4, 3), -((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).y / 4.0);
+                    // this lane's terms of the five elements (n, l, w, p, q) feeds
+                    double v0, v1 = 0.0, v2 = 0.0, v3 = 0.0, v4 = 0.0;
+                    if (ev) v0 = -((m1m * fnl) * a1122 * (cm1p1[w] * cmmpm[w])).x / 2.0;
+                    else v0 = (imul(mk(0.5, 0.0)) * (m1m * fnl) * a2112 * (cm1p1[w] * cmmpm[w])).x;
+                    if (w >= 2) {
+                        if (ev) {
+                            v1 = -((m1mq * a1122) * fnl * (cm1m1[w] * cmmpm[w])).x / 2.0;
+                            v2 = -((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).x / 4.0
+                                 - ((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).x / 4.0;
+                        } else {
+                            v1 = (imul(mk(-0.5, 0.0)) * (m1mq * a2112) * fnl * (cm1m1[w] * cmmpm[w])).y;
+                            v2 = ((m1m * a1p2) * fnl * (cm1p1[w] * cmmm2pm[w])).y / 4.0
+                                 - ((m1m * a1m2) * fnl * (cm1p1[w] * cmmp2pm[w])).y / 4.0;
+                        }
+                        v3 = -((m1mnpl * m1w * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0
+                             - ((m1mq * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0;
+                        v4 = -((m1mq * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0
+                             - ((m1mnpl * m1w * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0;
                     }
-                    atomicAdd(SS(sm22, 2, 2), -((m1mnpl * m1w * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0);
-                    atomicAdd(SS(sp22, 2, 2), -((m1mq * a1p2) * fnl * (cm1m1[w] * cmmm2pm[w])).x / 8.0);
-                    atomicAdd(SS(sm22, 2, 2), -((m1mq * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0);
-                    atomicAdd(SS(sp22, 2, 2), -((m1mnpl * m1w * a1m2) * fnl * (cm1m1[w] * cmmp2pm[w])).x / 8.0);
+                    v0 = warp_allsum(v0);
+                    if (w >= 2) {
+                        v1 = warp_allsum(v1);
+                        v2 = warp_allsum(v2);
+                        v3 = warp_allsum(v3);
+                        v4 = warp_allsum(v4);
+                    }
+                    if (lane == 0) {
+                        atomicAdd(ev ? SS(s00, 1, 1) : SS(s00, 4, 4), v0);
+                        if (w >= 2) {
+                            atomicAdd(ev ? SS(s02, 2, 1) : SS(s02, 3, 4), v1);
+                            atomicAdd(ev ? SS(s02, 1, 2) : SS(s02, 4, 3), v2);
+                            atomicAdd(SS(sm22, 2, 2), v3);
+                            atomicAdd(SS(sp22, 2, 2), v4);
+                        }
+                    }
 #undef SS
                 }
             }
