@@ -51,7 +51,7 @@ static int origin_orders(mstmg_ctx* c, const BigTablesDev& bt, double trans_eps,
     DevBuf<zd> tscr;
     const int sstride = 3 * (200 + MSTMG_LMAX + 4);
     CK(dtord.alloc(n));
-    CK(tscr.alloc((size_t)n * sstride));
+    CK(tscr.alloc(tranorder_scratch(n, sstride)));
     launch_tranorder(n, c->pos.p, c->d_order.p, r0, c->opts.medium_re, trans_eps, max_t_order, bt.bc.p, bt.fnr.p, bt.nbc, tscr.p, sstride,
                      dtord.p, c->st);
     tord.resize(n);

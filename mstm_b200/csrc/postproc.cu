@@ -30,49 +30,70 @@ __device__ __forceinline__ zd ipow_z(int k)
 }
 
 // ---------------------------------------------------------------------------
-// tranordertest per sphere
+// tranordertest per sphere: a warp per sphere, its lanes evaluating the
+// terms of 32 consecutive orders n at a time; one lane adds them in order of
+// n, exactly as the reference's loop does, and stops at the first order whose
+// partial sum meets the criterion.
 // ---------------------------------------------------------------------------
-__global__ void tranorder_kernel(int nsph, const double* pos, const int* order, double ox, double oy, double oz, double rire, double eps,
-                                 int maxt, VCTab tab, zd* scratch, int sstride, int* tord)
+#define TRANORDER_WPB 4
+__global__ void __launch_bounds__(32 * TRANORDER_WPB) tranorder_kernel(int nsph, const double* pos, const int* order, double ox,
+                                                                       double oy, double oz, double rire, double eps, int maxt,
+                                                                       VCTab tab, zd* scratch, int sstride, int* tord)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nsph) return;
+    __shared__ double terms[TRANORDER_WPB][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gw = blockIdx.x * TRANORDER_WPB + wib, nw = gridDim.x * TRANORDER_WPB;
     const int nlim = 200;
-    int lmax = order[i];
-    double dx = pos[3 * i] - ox, dy = pos[3 * i + 1] - oy, dz = pos[3 * i + 2] - oz;
-    double r = sqrt(dx * dx + dy * dy + dz * dz);
-    int nmax;
-    if (r == 0.0) {
-        nmax = lmax;
-    } else {
-        zd* xi = scratch + (size_t)i * sstride;
-        zd* scr = xi + (nlim + lmax + 2);
-        double* vc1 = (double*)(scr + (nlim + lmax + 2));
-        zd z = mk(r * rire, 0.0);
-        double sum = 0.0;
-        int n;
-        for (n = 1; n <= nlim; n++) {
-            mstm_cricbessel(n + lmax, z, xi, scr);
-            for (int l = 0; l <= n + lmax; l++) xi[l] = cdiv(xi[l], z) * ipow_z(l);
-            int l = lmax;
-            zd c = (tab.fr(n + n + 1) * tab.fr(l + l + 1)) * ipow_z(n - l);
-            vc_func(tab, -1, n, 1, l, vc1);
-            int wmin = abs(n - l), wmax = n + l;
-            zd a = mk(0.0, 0.0), b = mk(0.0, 0.0);
-            for (int w = wmin; w <= wmax; w++) {
-                double alnw = vc1[w] * vc1[w];
-                if ((n + l + w) % 2 == 0) a = a + alnw * xi[w];
-                else b = b + alnw * xi[w];
+    zd* xi = scratch + ((size_t)gw * 32 + lane) * sstride;
+    zd* scr = xi + (nlim + MSTMG_LMAX + 2);
+    double* vc1 = (double*)(scr + (nlim + MSTMG_LMAX + 2));
+    for (int i = gw; i < nsph; i += nw) {
+        const int lmax = order[i];
+        const double dx = pos[3 * i] - ox, dy = pos[3 * i + 1] - oy, dz = pos[3 * i + 2] - oz;
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        int nmax = lmax;
+        if (r != 0.0) {
+            const zd z = mk(r * rire, 0.0);
+            double sum = 0.0;
+            int found = 0;
+            for (int n0 = 1; n0 <= nlim && !found; n0 += 32) {
+                const int n = n0 + lane;
+                double term = 0.0;
+                if (n <= nlim) {
+                    mstm_cricbessel(n + lmax, z, xi, scr);
+                    for (int l = 0; l <= n + lmax; l++) xi[l] = cdiv(xi[l], z) * ipow_z(l);
+                    const int l = lmax;
+                    const zd c = (tab.fr(n + n + 1) * tab.fr(l + l + 1)) * ipow_z(n - l);
+                    vc_func(tab, -1, n, 1, l, vc1);
+                    const int wmin = abs(n - l), wmax = n + l;
+                    zd a = mk(0.0, 0.0), b = mk(0.0, 0.0);
+                    for (int w = wmin; w <= wmax; w++) {
+                        const double alnw = vc1[w] * vc1[w];
+                        if ((n + l + w) % 2 == 0) a = a + alnw * xi[w];
+                        else b = b + alnw * xi[w];
+                    }
+                    a = c * a;
+                    b = c * b;
+                    term = (a * cj(a) + b * cj(b)).x;
+                }
+                terms[wib][lane] = term;
+                __syncwarp();
+                if (lane == 0)
+                    for (int k = 0; k < 32 && n0 + k <= nlim; k++) {
+                        sum = sum + terms[wib][k];
+                        if (fabs(1.0 - sum) < eps) {
+                            found = n0 + k;
+                            break;
+                        }
+                    }
+                found = __shfl_sync(0xffffffffu, found, 0);
+                __syncwarp();
             }
-            a = c * a;
-            b = c * b;
-            sum = sum + (a * cj(a) + b * cj(b)).x;
-            if (fabs(1.0 - sum) < eps) break;
+            nmax = found ? found : nlim;
+            nmax = max(nmax, lmax);
         }
-        nmax = min(n, nlim);
-        nmax = max(nmax, lmax);
+        if (lane == 0) tord[i] = min(nmax, maxt);
     }
-    tord[i] = min(nmax, maxt);
 }
 
 // ---------------------------------------------------------------------------
@@ -704,12 +725,16 @@ __global__ void __launch_bounds__(PS_NT) planesm_kernel(PlaneSmArgs a)
     }
 }
 
+// blocks of TRANORDER_WPB warps, at most one warp per SM's worth (148) in all
+int tranorder_blocks(int nsph) { return std::max(1, (std::min(nsph, 148) + TRANORDER_WPB - 1) / TRANORDER_WPB); }
+size_t tranorder_scratch(int nsph, int sstride) { return (size_t)tranorder_blocks(nsph) * TRANORDER_WPB * 32 * (size_t)sstride; }
+
 void launch_tranorder(int nsph, const double* pos, const int* order, const double* origin, double rire, double eps, int maxt,
                       const double* bcof, const double* fnr, int nbc, zd* scratch, int sstride, int* tord, cudaStream_t st)
 {
     VCTab t{bcof, fnr, nbc};
-    tranorder_kernel<<<(nsph + 63) / 64, 64, 0, st>>>(nsph, pos, order, origin[0], origin[1], origin[2], rire, eps, maxt, t, scratch,
-                                                      sstride, tord);
+    tranorder_kernel<<<tranorder_blocks(nsph), 32 * TRANORDER_WPB, 0, st>>>(nsph, pos, order, origin[0], origin[1], origin[2], rire,
+                                                                            eps, maxt, t, scratch, sstride, tord);
     launch_counter() += 1;
 }
 

@@ -36,6 +36,7 @@ struct MergeArgs {
     size_t scratch_stride;  // zd units per CTA
 };
 
+size_t tranorder_scratch(int nsph, int sstride);   // complex values of scratch launch_tranorder needs
 void launch_tranorder(int nsph, const double* pos, const int* order, const double* origin, double rire, double eps, int maxt,
                       const double* bcof, const double* fnr, int nbc, zd* scratch, int sstride, int* tord, cudaStream_t st);
 #define MERGE_PC 16   // columns a CTA of the merge kernel translates together
