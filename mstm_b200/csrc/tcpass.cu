@@ -84,11 +84,24 @@ __device__ __forceinline__ bool mb_wait_all(uint32_t bar, uint32_t parity)
         if (mb_try(bar, parity)) return true;
     return false;
 }
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+// bulk copy global -> shared with an L2 eviction-priority hint for the lines it reads
+__device__ __forceinline__ void bulk_g2s_hint(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar, uint64_t policy)
 {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst), "l"(src),
-                 "r"(bytes), "r"(bar)
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar), "l"(policy)
                  : "memory");
+}
+__device__ __forceinline__ uint64_t l2_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
 }
 // shared-memory matrix descriptor: K-major, no swizzle (core matrices of 8
 // rows x 16 bytes), lbo = byte distance of the two core matrices along K of
@@ -319,6 +332,9 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
         if (warp == 4) {
             // ---- producer: column and operator chunks into the stages ----
             if (lane == 0) {
+                // the column images are read by every CTA and should stay in
+                // L2; the operator images stream through once
+                const uint64_t keep = l2_evict_last(), stream = l2_evict_first();
                 UnitIt it = unit_at(a.rstart, a.nsph, u0);
                 long long q = 0;
                 for (long long u = u0; u < u1; u++) {
@@ -336,10 +352,11 @@ __global__ void __launch_bounds__(192, 1) tc_pass_kernel(TcPassArgs a, int nstag
                         mb_expect(bar_full(s), STG);
 #pragma unroll
                         for (int t = 0; t < MTN; t++)
-                            bulk_g2s(dst + t * TC_SA,
-                                     a.aimg + ((((size_t)(mt0 + t) * a.nsph + j) * 2 + it.p) * NKC + kc) * (4 * TC_M * TC_KC), TC_SA,
-                                     bar_full(s));
-                        bulk_g2s(dst + SA, a.himg + (((size_t)it.e * 2 + it.p) * NKC + kc) * (2 * 2 * NP * TC_KC), SB, bar_full(s));
+                            bulk_g2s_hint(dst + t * TC_SA,
+                                          a.aimg + ((((size_t)(mt0 + t) * a.nsph + j) * 2 + it.p) * NKC + kc) * (4 * TC_M * TC_KC),
+                                          TC_SA, bar_full(s), keep);
+                        bulk_g2s_hint(dst + SA, a.himg + (((size_t)it.e * 2 + it.p) * NKC + kc) * (2 * 2 * NP * TC_KC), SB, bar_full(s),
+                                      stream);
                     }
                     if (u + 1 < u1) unit_next(a.rstart, it);
                 }
