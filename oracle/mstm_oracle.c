@@ -301,6 +301,66 @@ static void mieoa(double x, cplx ri, cplx rimed, int *nodr0, double qeps, double
     free(psi); free(xi); free(qext1);
 }
 
+/* The generalized Mie coefficients of a host sphere (mieoa's dnp_mie,
+ * unp_mie, vnp_mie, modules:5495-5528) for orders 1..nodr: with the
+ * sphere's scattered coefficients a and the regular coefficients f of the
+ * field inside it, (a, f) = [[A, U], [D, V]] (g, b) for the exciting field g
+ * outside and b inside (multmiecoeffmult, modules:5690-5747).  Each (2,2,nodr)
+ * column-major; non-optically-active sphere. */
+static void mieoa_host(double x, cplx ri, cplx rimed, int nodr, cplx *dnp, cplx *unp, cplx *vnp)
+{
+    cplx rii[2] = {rimed, ri};   /* region 0 outside, 1 inside; both helicities equal */
+    cplx rb[2], xri[2];
+    for (int i = 0; i < 2; i++) {
+        rb[i] = 2.0 / (1.0 / rii[i] + 1.0 / rii[i]);
+        xri[i] = x * rii[i];
+    }
+    int nb = nodr + 1;
+    cplx *psi = (cplx *)malloc(sizeof(cplx) * (nb + 1) * 2);
+    cplx *xi = (cplx *)malloc(sizeof(cplx) * (nb + 1) * 2);
+    for (int i = 0; i < 2; i++) {
+        cricbessel(nb, xri[i], psi + (nb + 1) * i);
+        crichankel(nb, xri[i], xi + (nb + 1) * i);
+    }
+#define PS(n, i) psi[(n) + (nb + 1) * (i)]
+#define XS(n, i) xi[(n) + (nb + 1) * (i)]
+    for (int n = 1; n <= nodr; n++) {
+        cplx psip[2], xip[2], psipn[2], xipn[2];
+        for (int i = 0; i < 2; i++) {
+            psip[i] = PS(n - 1, i) - (double)n * PS(n, i) / xri[i];
+            xip[i] = XS(n - 1, i) - (double)n * XS(n, i) / xri[i];
+            psipn[i] = PS(n - 1, i) / PS(n, i) - (double)n / xri[i];
+            xipn[i] = XS(n - 1, i) / XS(n, i) - (double)n / xri[i];
+        }
+        cplx g[4], b[4], u[4], d[4], v[4];
+        for (int s = 1; s <= 2; s++) {
+            double ss = pm1(s);
+            for (int t = 1; t <= 2; t++) {
+                double st = pm1(t);
+                M2(g, s, t) = (ss * rb[0] + st * rb[1]) / (rii[1] * rii[0]) * (psipn[1] * XS(n, 0) - ss * st * xip[0]);
+                M2(u, s, t) = (ss * rb[1] + st * rb[1]) / (rii[1] * rii[1]) * CI / PS(n, 1);
+                M2(b, s, t) = (ss * rb[1] + st * rb[0]) / (rii[0] * rii[1]) * (xipn[0] * PS(n, 1) - ss * st * psip[1]);
+                M2(d, s, t) = -(ss * rb[0] + st * rb[0]) / (rii[0] * rii[0]) * CI / XS(n, 0);
+                M2(v, s, t) = (ss * rb[1] + st * rb[0]) / (rii[0] * rii[1]) * (xipn[0] * XS(n, 1) - ss * st * xip[1]);
+            }
+        }
+        cplx gi[4], bi[4];
+        twobytwoinverse(g, gi);
+        twobytwoinverse(b, bi);
+        matmul22(gi, u, u);
+        matmul22(bi, d, d);
+        matmul22(bi, v, v);
+        for (int k = 0; k < 4; k++) {
+            unp[4 * (n - 1) + k] = -u[k];
+            dnp[4 * (n - 1) + k] = -d[k];
+            vnp[4 * (n - 1) + k] = -v[k];
+        }
+    }
+#undef PS
+#undef XS
+    free(psi); free(xi);
+}
+
 /* ------------------------------------------------------------------------ */
 /* vector coupling coefficients (modules:950-1056)                          */
 /* vcn indexed 0..n+l                                                        */
@@ -989,7 +1049,48 @@ struct orc_ctx {
     size_t *joff;
     cplx *Hc;              /* dense H at every node offset (2cd-1)^3 x nbN x nbN x 2, zero inside the hole */
     int last_iter[2];      /* cbicg iterations of each polarisation in the last orc_fixedorsoln */
+    /* host spheres (spheredata, modules:5088-5278): spheres inside others */
+    int *host;             /* findhostspheres: the host of each sphere, -1 outside every sphere */
+    int *nfe;              /* number_field_expansions: 2 for a sphere holding others, else 1 */
+    int nhosted;           /* number_host_spheres: spheres that have a host */
+    cplx *rext;            /* exteriorrefindex: the index around each sphere */
+    cplx *dn, *un, *vn;    /* the host spheres' D, U, V Mie coefficients (mie_offset) */
+    int nhp;               /* external_to_internal pairs: (host, sphere it holds) */
+    int *hpi, *hpj;
+    pairop_t *hops;        /* their regular translation operators */
 };
+
+/* findhostspheres (modules:5230-5276): the host of sphere i is the smallest
+ * larger sphere whose surface encloses i's centre (the first in order among
+ * equal radii); sphere_order then raised so that every host has at least the
+ * order of the spheres inside it (miecoefcalc, modules:5331-5342). */
+static void find_hosts(orc_ctx *c)
+{
+    int n = c->n;
+    c->nhosted = 0;
+    for (int i = 0; i < n; i++) {
+        c->host[i] = -1;
+        c->nfe[i] = 1;
+    }
+    for (int i = 0; i < n; i++) {
+        double xspmin = 1.0e6;
+        for (int j = 0; j < n; j++) {
+            if (!(c->rad[j] > c->rad[i])) continue;
+            double d0 = c->pos[3 * j] - c->pos[3 * i], d1 = c->pos[3 * j + 1] - c->pos[3 * i + 1], d2 = c->pos[3 * j + 2] - c->pos[3 * i + 2];
+            double rij = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+            if (rij <= c->rad[j] && c->rad[j] < xspmin) {
+                c->host[i] = j;
+                xspmin = c->rad[j];
+            }
+        }
+    }
+    for (int i = 0; i < n; i++)
+        if (c->host[i] >= 0) {
+            c->nfe[c->host[i]] = 2;
+            c->nhosted++;
+        }
+    for (int i = 0; i < n; i++) c->rext[i] = c->host[i] >= 0 ? c->ri[c->host[i]] : c->rimed;
+}
 
 orc_ctx *orc_create(int nsphere, const double *pos, const double *radius, const double *ri,
                     double mie_eps, int store_matrix, int nthreads)
@@ -1004,46 +1105,73 @@ orc_ctx *orc_create(int nsphere, const double *pos, const double *radius, const 
     memcpy(c->rad, radius, sizeof(double) * nsphere);
     for (int i = 0; i < nsphere; i++) c->ri[i] = ri[2 * i] + CI * ri[2 * i + 1];
     c->rimed = 1.0;
+    c->host = (int *)malloc(sizeof(int) * (nsphere + 1));
+    c->nfe = (int *)malloc(sizeof(int) * (nsphere + 1));
+    c->rext = (cplx *)malloc(sizeof(cplx) * (nsphere + 1));
+    find_hosts(c);
     c->order = (int *)malloc(sizeof(int) * nsphere);
     c->offset = (int *)malloc(sizeof(int) * (nsphere + 1));
     c->mie_offset = (int *)malloc(sizeof(int) * (nsphere + 1));
     c->qext_mie = (double *)malloc(sizeof(double) * nsphere);
     c->qabs_mie = (double *)malloc(sizeof(double) * nsphere);
-    /* miecoefcalc (modules:5301-5407) for external spheres, medium index 1 */
+    /* miecoefcalc (modules:5301-5407): each sphere in the medium around it */
     int nterms = 0, nblk = 0, maxo = 0;
     for (int i = 0; i < nsphere; i++) {
         int nodrn = 0;
         double qe, qs, qa;
-        mieoa(c->rad[i], c->ri[i], c->rimed, &nodrn, mie_eps, &qe, &qs, &qa, NULL, NULL);
+        mieoa(c->rad[i], c->ri[i], c->rext[i], &nodrn, mie_eps, &qe, &qs, &qa, NULL, NULL);
         c->order[i] = nodrn;
     }
+    for (int i = 0; i < nsphere; i++)
+        for (int j = c->host[i]; j >= 0; j = c->host[j]) c->order[j] = imax(c->order[j], c->order[i]);
     for (int i = 0; i < nsphere; i++) {
         c->mie_offset[i] = nterms;
         nterms += 4 * c->order[i];
         c->offset[i] = nblk;
-        nblk += 2 * c->order[i] * (c->order[i] + 2);
+        nblk += 2 * c->order[i] * (c->order[i] + 2) * c->nfe[i];
         maxo = imax(maxo, c->order[i]);
     }
     c->mie_offset[nsphere] = nterms;
     c->offset[nsphere] = nblk;
     c->neqns = nblk;
     c->max_order = maxo;
-    c->an = (cplx *)malloc(sizeof(cplx) * nterms);
-    c->an_inv = (cplx *)malloc(sizeof(cplx) * nterms);
+    c->an = (cplx *)malloc(sizeof(cplx) * (nterms + 1));
+    c->an_inv = (cplx *)malloc(sizeof(cplx) * (nterms + 1));
+    c->dn = (cplx *)calloc(nterms + 1, sizeof(cplx));
+    c->un = (cplx *)calloc(nterms + 1, sizeof(cplx));
+    c->vn = (cplx *)calloc(nterms + 1, sizeof(cplx));
     for (int i = 0; i < nsphere; i++) {
         int nodrn = c->order[i];
-        mieoa(c->rad[i], c->ri[i], c->rimed, &nodrn, 0.0, &c->qext_mie[i], NULL, &c->qabs_mie[i],
+        mieoa(c->rad[i], c->ri[i], c->rext[i], &nodrn, 0.0, &c->qext_mie[i], NULL, &c->qabs_mie[i],
               c->an + c->mie_offset[i], c->an_inv + c->mie_offset[i]);
+        if (c->nfe[i] == 2)
+            mieoa_host(c->rad[i], c->ri[i], c->rext[i], nodrn, c->dn + c->mie_offset[i], c->un + c->mie_offset[i],
+                       c->vn + c->mie_offset[i]);
     }
     axialtrancoefinit(maxo);
     c->store = store_matrix;
     c->nthreads = nthreads > 0 ? nthreads : 1;
-    c->npairs = nsphere * (nsphere - 1) / 2;
+    /* external_to_external_expansion's pairs: i < j in the same host
+     * (modules:6466-6469); external_to_internal_expansion's: a host and a
+     * sphere it holds (modules:6569-6571) */
+    c->npairs = 0;
+    c->nhp = 0;
+    for (int i = 0; i < nsphere - 1; i++)
+        for (int j = i + 1; j < nsphere; j++) {
+            if (c->host[i] == c->host[j]) c->npairs++;
+            if (c->host[j] == i || c->host[i] == j) c->nhp++;
+        }
     c->pi_ = (int *)malloc(sizeof(int) * (c->npairs + 1));
     c->pj_ = (int *)malloc(sizeof(int) * (c->npairs + 1));
-    int t = 0;
+    c->hpi = (int *)malloc(sizeof(int) * (c->nhp + 1));
+    c->hpj = (int *)malloc(sizeof(int) * (c->nhp + 1));
+    int t = 0, h = 0;
     for (int i = 0; i < nsphere - 1; i++)
-        for (int j = i + 1; j < nsphere; j++) { c->pi_[t] = i; c->pj_[t] = j; t++; }
+        for (int j = i + 1; j < nsphere; j++) {
+            if (c->host[i] == c->host[j]) { c->pi_[t] = i; c->pj_[t] = j; t++; }
+            if (c->host[j] == i) { c->hpi[h] = i; c->hpj[h] = j; h++; }
+            else if (c->host[i] == j) { c->hpi[h] = j; c->hpj[h] = i; h++; }
+        }
     return c;
 }
 
@@ -1054,10 +1182,25 @@ void orc_destroy(orc_ctx *c)
     free(c->pos); free(c->rad); free(c->ri); free(c->order); free(c->offset); free(c->mie_offset);
     free(c->an); free(c->an_inv); free(c->qext_mie); free(c->qabs_mie); free(c->pi_); free(c->pj_);
     free(c->snode); free(c->Jsn); free(c->Jns); free(c->joff); free(c->Hc);
+    if (c->hops) { for (int k = 0; k < c->nhp; k++) pairop_free(&c->hops[k]); free(c->hops); }
+    free(c->host); free(c->nfe); free(c->rext); free(c->dn); free(c->un); free(c->vn); free(c->hpi); free(c->hpj);
     free(c);
 }
 
 int orc_neqns(const orc_ctx *c) { return c->neqns; }
+/* host[i]: the sphere holding sphere i (-1: none); returns number_host_spheres */
+int orc_hosts(const orc_ctx *c, int *host)
+{
+    if (host) memcpy(host, c->host, sizeof(int) * c->n);
+    return c->nhosted;
+}
+void orc_host_mie_coefs(const orc_ctx *c, cplx *dn, cplx *un, cplx *vn)
+{
+    int nt = c->mie_offset[c->n];
+    if (dn) memcpy(dn, c->dn, sizeof(cplx) * nt);
+    if (un) memcpy(un, c->un, sizeof(cplx) * nt);
+    if (vn) memcpy(vn, c->vn, sizeof(cplx) * nt);
+}
 void orc_orders(const orc_ctx *c, int *order, int *offset, int *mie_offset)
 {
     if (order) memcpy(order, c->order, sizeof(int) * c->n);
@@ -1073,14 +1216,10 @@ void orc_mie_coefs(const orc_ctx *c, cplx *an, cplx *an_inv, double *qext, doubl
     if (qabs) memcpy(qabs, c->qabs_mie, sizeof(double) * c->n);
 }
 
-/* onemiecoeffmult / multmiecoeffmult, external spheres only (modules:5585-5688).
+/* onemiecoeffmult / multmiecoeffmult (modules:5585-5688).
  * idir==1: y = A x ; otherwise y = A^T x.  In-place allowed. */
-static void mie_mult_sphere(const cplx *an1, int nodr, int idir, const cplx *x, cplx *y)
+static void mie_acc(const cplx *an1, int nodr, int idir, const cplx *t, cplx *y)
 {
-    int nb = 2 * nodr * (nodr + 2);
-    cplx *t = (cplx *)malloc(sizeof(cplx) * nb);
-    memcpy(t, x, sizeof(cplx) * nb);
-    for (int k = 0; k < nb; k++) y[k] = 0;
     for (int n = 1; n <= nodr; n++)
         for (int p = 1; p <= 2; p++)
             for (int q = 1; q <= 2; q++) {
@@ -1088,12 +1227,41 @@ static void mie_mult_sphere(const cplx *an1, int nodr, int idir, const cplx *x, 
                 for (int m = 1; m <= n; m++) y[AIDX(n + 1, m, p - 1, nodr)] += a * t[AIDX(n + 1, m, q - 1, nodr)];
                 for (int m = 0; m <= n; m++) y[AIDX(m, n, p - 1, nodr)] += a * t[AIDX(m, n, q - 1, nodr)];
             }
+}
+static void mie_mult_sphere(const cplx *an1, int nodr, int idir, const cplx *x, cplx *y)
+{
+    int nb = 2 * nodr * (nodr + 2);
+    cplx *t = (cplx *)malloc(sizeof(cplx) * nb);
+    memcpy(t, x, sizeof(cplx) * nb);
+    for (int k = 0; k < nb; k++) y[k] = 0;
+    mie_acc(an1, nodr, idir, t, y);
     free(t);
+}
+/* The host branch of multmiecoeffmult (modules:5690-5747): the sphere's
+ * block (g) and the block of the field inside it (b) give
+ * idir==1: a = A g + U b, f = D g + V b; otherwise the transpose,
+ * a = A^T g + D^T b, f = U^T g + V^T b. */
+static void mie_mult_host(const orc_ctx *c, int i, int idir, const cplx *ain, cplx *aout)
+{
+    int nodr = c->order[i], nb = 2 * nodr * (nodr + 2), mo = c->mie_offset[i];
+    const cplx *g = ain + c->offset[i], *b = g + nb;
+    cplx *a = aout + c->offset[i], *f = a + nb;
+    cplx *tg = (cplx *)malloc(sizeof(cplx) * 2 * nb), *tb = tg + nb;
+    memcpy(tg, g, sizeof(cplx) * nb);
+    memcpy(tb, b, sizeof(cplx) * nb);
+    for (int k = 0; k < nb; k++) { a[k] = 0; f[k] = 0; }
+    mie_acc(c->an + mo, nodr, idir, tg, a);
+    mie_acc((idir == 1 ? c->un : c->dn) + mo, nodr, idir, tb, a);
+    mie_acc((idir == 1 ? c->dn : c->un) + mo, nodr, idir, tg, f);
+    mie_acc(c->vn + mo, nodr, idir, tb, f);
+    free(tg);
 }
 static void multmiecoeffmult(const orc_ctx *c, int idir, const cplx *ain, cplx *aout, const cplx *coef)
 {
-    for (int i = 0; i < c->n; i++)
-        mie_mult_sphere(coef + c->mie_offset[i], c->order[i], idir, ain + c->offset[i], aout + c->offset[i]);
+    for (int i = 0; i < c->n; i++) {
+        if (c->nfe[i] == 2 && coef == c->an) mie_mult_host(c, i, idir, ain, aout);
+        else mie_mult_sphere(coef + c->mie_offset[i], c->order[i], idir, ain + c->offset[i], aout + c->offset[i]);
+    }
 }
 
 /* external_to_external_expansion (modules:6390-6525).  The pair loop is
@@ -1331,7 +1499,7 @@ static void dense_pair_apply(const orc_ctx *c, int i, int j, int nrhs, const cpl
     int Li = c->order[i], Lj = c->order[j], nbi = Li * (Li + 2), nbj = Lj * (Lj + 2), neq = c->neqns;
     cplx *H = (cplx *)malloc(sizeof(cplx) * (size_t)nbi * nbj * 2);
     double rv[3] = {c->pos[3 * i] - c->pos[3 * j], c->pos[3 * i + 1] - c->pos[3 * j + 1], c->pos[3 * i + 2] - c->pos[3 * j + 2]};
-    gentranmatrix(Lj, Li, rv, c->rimed, 3, H);
+    gentranmatrix(Lj, Li, rv, c->rext[i], 3, H);
     cplx *a = (cplx *)malloc(sizeof(cplx) * 2 * (nbi > nbj ? nbi : nbj));
     cplx *o = (cplx *)malloc(sizeof(cplx) * 2 * (nbi > nbj ? nbi : nbj));
     for (int r = 0; r < nrhs; r++) {
@@ -1373,7 +1541,7 @@ static void external_to_external(orc_ctx *c, int nrhs, const cplx *ain, cplx *go
         for (int t = 0; t < c->npairs; t++) {
             int i = c->pi_[t], j = c->pj_[t];
             double rv[3] = {c->pos[3 * i] - c->pos[3 * j], c->pos[3 * i + 1] - c->pos[3 * j + 1], c->pos[3 * i + 2] - c->pos[3 * j + 2]};
-            pairop_compute(&c->ops[t], c->order[i], c->order[j], rv, 3, c->rimed);
+            pairop_compute(&c->ops[t], c->order[i], c->order[j], rv, 3, c->rext[i]);
         }
         c->ops_ready = 1;
     }
@@ -1395,7 +1563,7 @@ static void external_to_external(orc_ctx *c, int nrhs, const cplx *ain, cplx *go
             if (c->store) op = &c->ops[t];
             else {
                 double rv[3] = {c->pos[3 * i] - c->pos[3 * j], c->pos[3 * i + 1] - c->pos[3 * j + 1], c->pos[3 * i + 2] - c->pos[3 * j + 2]};
-                pairop_compute(&local, noi, noj, rv, 3, c->rimed);
+                pairop_compute(&local, noi, noj, rv, 3, c->rext[i]);
                 op = &local;
             }
             if (imin(noi, noj) < 3) {
@@ -1417,9 +1585,38 @@ static void external_to_external(orc_ctx *c, int nrhs, const cplx *ain, cplx *go
     if (c->fft) fft_far_field(c, nrhs, ain, gout, contran);
 }
 
-/* sphereinteraction (scatprops:25-180), free-space external spheres */
-void orc_sphereinteraction(orc_ctx *c, int nrhs, const cplx *ain, cplx *aout, const int *con_tran,
-                           const int *mie_mult, int initial_run)
+/* external_to_internal_expansion (modules:6533-6608): for each host and a
+ * sphere it holds, the regular translation (vswf_type 1, in the host's
+ * index) of the sphere's scattered coefficients into the host's internal
+ * block, and of the host's internal block back onto the sphere (shift_op);
+ * coincident centres copy the common orders (mtransfer).  bout is zeroed. */
+static void external_to_internal(orc_ctx *c, int nrhs, const cplx *ain, cplx *bout, const int *contran)
+{
+    int neq = c->neqns;
+    for (size_t k = 0; k < (size_t)neq * nrhs; k++) bout[k] = 0;
+    if (!c->hops) {
+        c->hops = (pairop_t *)calloc(c->nhp > 0 ? c->nhp : 1, sizeof(pairop_t));
+        for (int t = 0; t < c->nhp; t++) {
+            int hi = c->hpi[t], e = c->hpj[t];
+            double rv[3] = {c->pos[3 * hi] - c->pos[3 * e], c->pos[3 * hi + 1] - c->pos[3 * e + 1], c->pos[3 * hi + 2] - c->pos[3 * e + 2]};
+            pairop_compute(&c->hops[t], c->order[hi], c->order[e], rv, 1, c->ri[hi]);
+        }
+    }
+    for (int t = 0; t < c->nhp; t++) {
+        int hi = c->hpi[t], e = c->hpj[t];
+        int noint = c->order[hi], noext = c->order[e];
+        int ext1 = c->offset[e], int1 = c->offset[hi] + noint * (noint + 2) * 2;
+        for (int r = 0; r < nrhs; r++) {
+            coefficient_translation(noext, noint, ain + (size_t)neq * r + ext1, bout + (size_t)neq * r + int1, &c->hops[t], 0, contran[r]);
+            coefficient_translation(noint, noext, ain + (size_t)neq * r + int1, bout + (size_t)neq * r + ext1, &c->hops[t], 1, contran[r]);
+        }
+    }
+}
+
+/* sphereinteraction (scatprops:25-180) without plane boundaries or periodic
+ * lattices; skip_external leaves out external_to_external_expansion */
+static void sphereinteraction_ex(orc_ctx *c, int nrhs, const cplx *ain, cplx *aout, const int *con_tran,
+                                 const int *mie_mult, int initial_run, int skip_external)
 {
     int neq = c->neqns;
     cplx *ain_t = (cplx *)malloc(sizeof(cplx) * neq * nrhs);
@@ -1438,7 +1635,17 @@ void orc_sphereinteraction(orc_ctx *c, int nrhs, const cplx *ain, cplx *aout, co
             memcpy(t, x, sizeof(cplx) * neq);
         }
     }
-    external_to_external(c, nrhs, ain_t, aout_t, ct, initial_run);
+    if (skip_external) {
+        for (size_t k = 0; k < (size_t)neq * nrhs; k++) aout_t[k] = 0;
+    } else {
+        external_to_external(c, nrhs, ain_t, aout_t, ct, initial_run);
+    }
+    if (c->nhosted > 0) {
+        cplx *t2 = (cplx *)malloc(sizeof(cplx) * neq * nrhs);
+        external_to_internal(c, nrhs, ain_t, t2, ct);
+        for (size_t k = 0; k < (size_t)neq * nrhs; k++) aout_t[k] += t2[k];
+        free(t2);
+    }
     for (int r = 0; r < nrhs; r++) {
         int mm = mie_mult ? mie_mult[r] : 1;
         cplx *o = aout + (size_t)neq * r;
@@ -1451,6 +1658,16 @@ void orc_sphereinteraction(orc_ctx *c, int nrhs, const cplx *ain, cplx *aout, co
         }
     }
     free(ain_t); free(aout_t); free(ct);
+}
+void orc_sphereinteraction(orc_ctx *c, int nrhs, const cplx *ain, cplx *aout, const int *con_tran,
+                           const int *mie_mult, int initial_run)
+{
+    sphereinteraction_ex(c, nrhs, ain, aout, con_tran, mie_mult, initial_run, 0);
+}
+void orc_sphereinteraction_ex(orc_ctx *c, int nrhs, const cplx *ain, cplx *aout, const int *con_tran,
+                              const int *mie_mult, int initial_run, int skip_external)
+{
+    sphereinteraction_ex(c, nrhs, ain, aout, con_tran, mie_mult, initial_run, skip_external);
 }
 
 /* Fortran dot_product for complex: sum(conj(a)*b) */
@@ -1592,6 +1809,7 @@ void orc_planewave(const orc_ctx *c, double alpha, double sinc, int dir, cplx *p
     cplx s = sinc;
     for (size_t k = 0; k < (size_t)neq * 2; k++) pmnp[k] = 0;
     for (int i = 0; i < c->n; i++) {
+        if (c->host[i] >= 0) continue;   /* spheres inside others see no incident wave (scatprops:268) */
         int L = c->order[i], nb = 2 * L * (L + 2);
         cplx *pw = (cplx *)malloc(sizeof(cplx) * nb * 2);
         genplanewavecoef(alpha, cbinc, L, pw);
@@ -1669,20 +1887,30 @@ static void lrsphereqeff(cplx ri0, int nodr, double xsp, const cplx *anp /*(nb,2
     free(psi); free(xi);
 }
 
-/* qefficiencyfactors (scatprops:782-870), npol=2, no host spheres.
- * qeff(3,3,N) column-major: qeff[q + 3*(pol + 3*i)], q: ext,abs,sca(inc). */
-static void qefficiencyfactors(const orc_ctx *c, const cplx *amnp, const cplx *gmnp0, double *qeff)
+/* qefficiencyfactors (scatprops:782-870), npol=2.
+ * qeff(3,3,N) column-major: qeff[q + 3*(pol + 3*i)], q: ext,abs,sca(inc).
+ * Without host spheres the exciting field is A^{-1} a; with them it is the
+ * interaction without the Mie multiply plus the incident field. */
+static void qefficiencyfactors(orc_ctx *c, const cplx *amnp, const cplx *gmnp0, double *qeff)
 {
     int neq = c->neqns;
     cplx *gmnp = (cplx *)calloc((size_t)neq * 2, sizeof(cplx));
-    for (int p = 0; p < 2; p++)
-        for (int i = 0; i < c->n; i++)
-            mie_mult_sphere(c->an_inv + c->mie_offset[i], c->order[i], 1, amnp + (size_t)neq * p + c->offset[i],
-                            gmnp + (size_t)neq * p + c->offset[i]);
+    if (c->nhosted == 0) {
+        for (int p = 0; p < 2; p++)
+            for (int i = 0; i < c->n; i++)
+                mie_mult_sphere(c->an_inv + c->mie_offset[i], c->order[i], 1, amnp + (size_t)neq * p + c->offset[i],
+                                gmnp + (size_t)neq * p + c->offset[i]);
+    } else {
+        int zero = 0;
+        for (int p = 0; p < 2; p++) {
+            sphereinteraction_ex(c, 1, amnp + (size_t)neq * p, gmnp + (size_t)neq * p, &zero, &zero, 0, 0);
+            for (int k = 0; k < neq; k++) gmnp[(size_t)neq * p + k] += gmnp0[(size_t)neq * p + k];
+        }
+    }
     for (int i = 0; i < c->n; i++) {
         double qe[3], qs[3], qa[3];
         int off = c->offset[i];
-        lrsphereqeff(c->rimed, c->order[i], c->rad[i], amnp + off, neq, gmnp0 + off, gmnp + off, qe, qs, qa);
+        lrsphereqeff(c->rext[i], c->order[i], c->rad[i], amnp + off, neq, gmnp0 + off, gmnp + off, qe, qs, qa);
         double qeffi[3][3];  /* [q][k] */
         for (int k = 0; k < 3; k++) { qeffi[0][k] = qe[k]; qeffi[2][k] = qs[k]; qeffi[1][k] = qa[k]; }
         for (int q = 0; q < 3; q++) {
@@ -1694,22 +1922,47 @@ static void qefficiencyfactors(const orc_ctx *c, const cplx *amnp, const cplx *g
     free(gmnp);
 }
 
-/* vol_radius as main_calling_program forms it: (sum r^3)**.333333 where
- * .333333 is a default-real (single precision) literal (input:1219-1225). */
+/* vol_radius as main_calling_program forms it, over the spheres outside
+ * every other: (sum r^3)**.333333 where .333333 is a default-real (single
+ * precision) literal (input:1218-1225). */
 double orc_vol_radius(const orc_ctx *c)
 {
     double v = 0.0;
-    for (int i = 0; i < c->n; i++) v = v + c->rad[i] * c->rad[i] * c->rad[i];
+    for (int i = 0; i < c->n; i++)
+        if (c->host[i] < 0) v = v + c->rad[i] * c->rad[i] * c->rad[i];
     return pow(v, (double)0.333333f);
 }
 
-/* qtotcalc (scatprops:872-912), no host spheres; qtot(3,3) column-major. */
+/* qtotcalc (scatprops:872-912); qtot(3,3) column-major.  A host's absorption
+ * net of the spheres it holds (qabsvol), then the holds' added back, each
+ * scaled by the area ratio; qeff's absorption rows are rewritten as the
+ * reference does.  The totals sum the spheres outside every other. */
 void orc_qtotcalc(const orc_ctx *c, double *qeff, double *qtot)
 {
+    int n = c->n;
     double xg = orc_vol_radius(c);
+    if (c->nhosted > 0) {
+        double *qv = (double *)malloc(sizeof(double) * 3 * n);
+        for (int i = 0; i < n; i++)
+            for (int p = 0; p < 3; p++) {
+                double v = qeff[1 + 3 * (p + 3 * i)];
+                for (int j = 0; j < n; j++)
+                    if (c->host[j] == i) v = v - qeff[1 + 3 * (p + 3 * j)] * c->rad[j] * c->rad[j] / (c->rad[i] * c->rad[i]);
+                qv[p + 3 * i] = v;
+            }
+        for (int i = 0; i < n; i++)
+            for (int p = 0; p < 3; p++) {
+                double v = qv[p + 3 * i];
+                for (int j = 0; j < n; j++)
+                    if (c->host[j] == i) v = v + qv[p + 3 * j] * c->rad[j] * c->rad[j] / (c->rad[i] * c->rad[i]);
+                qeff[1 + 3 * (p + 3 * i)] = v;
+            }
+        free(qv);
+    }
     for (int k = 0; k < 9; k++) qtot[k] = 0.0;
-    for (int i = 0; i < c->n; i++)
-        for (int k = 0; k < 9; k++) qtot[k] = qtot[k] + qeff[k + 9 * i] * c->rad[i] * c->rad[i] / (xg * xg);
+    for (int i = 0; i < n; i++)
+        if (c->host[i] < 0)
+            for (int k = 0; k < 9; k++) qtot[k] = qtot[k] + qeff[k + 9 * i] * c->rad[i] * c->rad[i] / (xg * xg);
     for (int pol = 0; pol < 3; pol++) qtot[2 + 3 * pol] = qtot[0 + 3 * pol] + qtot[2 + 3 * pol] - qtot[1 + 3 * pol];
 }
 
@@ -1777,6 +2030,23 @@ static void direct_solve(orc_ctx *c, const cplx *pnp, cplx *anp)
 {
     int neq = c->neqns;
     cplx *amat = (cplx *)calloc((size_t)neq * neq, sizeof(cplx));
+    cplx *col = NULL;
+    if (c->nhosted > 0) {
+        /* with host spheres: column k of I - M H is e_k minus the interaction
+         * of e_k (the same linear map general_interaction_matrix assembles
+         * block by block, modules:5854-5985) */
+        cplx *e = (cplx *)calloc(neq, sizeof(cplx));
+        int zero = 0;
+        for (int k = 0; k < neq; k++) {
+            e[k] = 1.0;
+            sphereinteraction_ex(c, 1, e, amat + (size_t)neq * k, &zero, NULL, 0, 0);
+            e[k] = 0.0;
+            for (int r = 0; r < neq; r++) amat[(size_t)neq * k + r] = -amat[(size_t)neq * k + r];
+            amat[(size_t)neq * k + k] += 1.0;
+        }
+        free(e);
+        goto factor;
+    }
     for (int i = 0; i < c->n; i++) {
         int nbi = c->order[i] * (c->order[i] + 2);
         for (int j = 0; j < c->n; j++) {
@@ -1791,7 +2061,7 @@ static void direct_solve(orc_ctx *c, const cplx *pnp, cplx *anp)
             free(fs);
         }
     }
-    cplx *col = (cplx *)malloc(sizeof(cplx) * neq);
+    col = (cplx *)malloc(sizeof(cplx) * neq);
     for (int j = 0; j < neq; j++) {
         cplx *mj = amat + (size_t)neq * j;
         int nz = 0;
@@ -1802,6 +2072,7 @@ static void direct_solve(orc_ctx *c, const cplx *pnp, cplx *anp)
         }
         mj[j] += 1.0;
     }
+factor:;
     cplx *lu = (cplx *)malloc(sizeof(cplx) * (size_t)neq * neq);
     memcpy(lu, amat, sizeof(cplx) * (size_t)neq * neq);
     int *indx = (int *)malloc(sizeof(int) * neq);
@@ -1842,6 +2113,14 @@ int orc_fixedorsoln(orc_ctx *c, double alpha, double sinc, int dir, double eps, 
         if (niter != 0) {
             if (direct) direct_solve(c, pmnpan, amnp + (size_t)neq * p);
             else orc_cbicg(c, niter, eps, pmnpan, amnp + (size_t)neq * p, initialize, &iter, &serr);
+        } else if (c->nhosted > 0) {
+            /* the coupling of the spheres inside hosts alone (solver:509-518) */
+            int zero = 0;
+            cplx *t = (cplx *)calloc(neq, sizeof(cplx));
+            sphereinteraction_ex(c, 1, amnp + (size_t)neq * p, t, &zero, NULL, initialize, 1);
+            sphereinteraction_ex(c, 1, t, t, &zero, NULL, 0, 1);
+            for (int k = 0; k < neq; k++) amnp[(size_t)neq * p + k] += t[k];
+            free(t);
         }
         initialize = 0;
         c->last_iter[p] = iter;

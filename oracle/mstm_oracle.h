@@ -41,6 +41,17 @@ void orc_mie_coefs(const orc_ctx *c, ocplx *an, ocplx *an_inv, double *qext, dou
 
 void orc_sphereinteraction(orc_ctx *c, int nrhs, const ocplx *ain, ocplx *aout,
                            const int *con_tran, const int *mie_mult, int initial_run);
+/* skip_external != 0: without external_to_external_expansion (the host
+ * coupling alone, sphereinteraction's skip_external_translation) */
+void orc_sphereinteraction_ex(orc_ctx *c, int nrhs, const ocplx *ain, ocplx *aout,
+                              const int *con_tran, const int *mie_mult, int initial_run,
+                              int skip_external);
+/* Host spheres (findhostspheres, modules:5230-5276): host[i] is the sphere
+ * holding sphere i, -1 for none; returns the number of spheres with a host.
+ * A host's equations hold its scattered block and then the block of the
+ * regular field inside it. */
+int orc_hosts(const orc_ctx *c, int *host);
+void orc_host_mie_coefs(const orc_ctx *c, ocplx *dn, ocplx *un, ocplx *vn);
 int orc_cbicg(orc_ctx *c, int niter, double eps, const ocplx *pnp, ocplx *anp,
               int initialize, int *iter, double *err);
 void orc_planewave(const orc_ctx *c, double alpha, double sinc, int dir, ocplx *pmnp);

@@ -40,6 +40,10 @@ def lib():
         L.orc_orders.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
         L.orc_mie_coefs.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
         L.orc_sphereinteraction.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int]
+        L.orc_sphereinteraction_ex.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int]
+        L.orc_hosts.argtypes = [c_void_p, c_void_p]
+        L.orc_hosts.restype = c_int
+        L.orc_host_mie_coefs.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
         L.orc_cbicg.argtypes = [c_void_p, c_int, c_double, c_void_p, c_void_p, c_int, P(c_int), P(c_double)]
         L.orc_cbicg.restype = c_int
         L.orc_planewave.argtypes = [c_void_p, c_double, c_double, c_int, c_void_p]
@@ -97,7 +101,8 @@ def _p(a):
 
 
 class Oracle:
-    """FP64 CPU restatement of one MSTM sphere cluster (free space, medium index 1).
+    """FP64 CPU restatement of one MSTM sphere cluster (free space, medium index 1;
+    spheres may lie inside others, as the reference's host spheres).
 
     positions (N,3), radii (N,), ref_index (N,) complex; mie_eps as the
     reference's ``mie_epsilon`` (negative -L forces order L).
@@ -141,14 +146,28 @@ class Oracle:
         self.L.orc_mie_coefs(self.ctx, _p(an), _p(ai), _p(qe), _p(qa))
         return an, ai, qe, qa
 
-    def sphereinteraction(self, ain, con_tran=None, mie_mult=None, initial_run=False):
+    def sphereinteraction(self, ain, con_tran=None, mie_mult=None, initial_run=False, skip_external=False):
         ain = np.asfortranarray(np.asarray(ain, np.complex128).reshape(self.neqns, -1, order="F"))
         nrhs = ain.shape[1]
         out = np.zeros((self.neqns, nrhs), np.complex128, order="F")
         ct = np.array(con_tran if con_tran is not None else [0] * nrhs, np.int32)
         mm = np.array(mie_mult if mie_mult is not None else [1] * nrhs, np.int32)
-        self.L.orc_sphereinteraction(self.ctx, nrhs, _p(ain), _p(out), _p(ct), _p(mm), int(initial_run))
+        self.L.orc_sphereinteraction_ex(self.ctx, nrhs, _p(ain), _p(out), _p(ct), _p(mm), int(initial_run),
+                                        int(skip_external))
         return out
+
+    def hosts(self):
+        """(host of each sphere, -1 for none; number of spheres with a host)"""
+        h = np.zeros(self.n, np.int32)
+        nh = self.L.orc_hosts(self.ctx, _p(h))
+        return h, nh
+
+    def host_mie(self):
+        """The D, U, V coefficients of the host spheres (zero for the others)."""
+        nt = int(self.mie_offset[-1])
+        d, u, v = (np.zeros(nt, np.complex128) for _ in range(3))
+        self.L.orc_host_mie_coefs(self.ctx, _p(d), _p(u), _p(v))
+        return d, u, v
 
     def cbicg(self, pnp, x0, niter=10000, eps=1e-6, initialize=True):
         pnp = np.ascontiguousarray(pnp, np.complex128)
