@@ -98,8 +98,29 @@ int mstmg_npairs(const mstmg_ctx *ctx);
 int mstmg_sphere_orders(const mstmg_ctx *ctx, int *order, int *offset);
 /* an: 2 * 4*sum(L) doubles (MSTM an_mie layout); qext, qabs: nsphere (may be NULL). */
 int mstmg_mie_coefficients(const mstmg_ctx *ctx, double *an, double *qext, double *qabs);
-/* (sum r^3)^.333333 as MSTM forms vol_radius (mstm-input-37.f90:1219-1225). */
+/* (sum r^3)^.333333 as MSTM forms vol_radius (mstm-input-37.f90:1218-1225),
+ * over the spheres outside every other sphere. */
 double mstmg_vol_radius(const mstmg_ctx *ctx);
+
+/* Host spheres (MSTM spheredata findhostspheres, mstm-modules-33.f90:5230-5276):
+ * a sphere whose centre lies inside a larger sphere is held by the smallest
+ * such sphere, sits in that sphere's refractive index, and couples to the
+ * other spheres of the same host directly and to its host through the
+ * regular field inside the host (external_to_internal_expansion,
+ * mstm-modules-33.f90:6533-6608).  A host's equations are its own block
+ * followed by the block of the field inside it (number_field_expansions 2),
+ * as sphere_offset lays them out.  mstmg_ctx_create detects hosts always.
+ * host (may be NULL): nsphere entries, the holding sphere (0-based) or -1.
+ * Returns the number of spheres that have a host (number_host_spheres).
+ * With hosts, the FP64 solvers (mstmg_bicg, mstmg_fixed_orientation with
+ * precision FP64), mstmg_interaction(_ex), mstmg_planewave,
+ * mstmg_fixed_orientation_rhs, mstmg_efficiencies and FP64 translation passes
+ * are available; the other entry points return MSTMG_ERR_UNSUPPORTED. */
+int mstmg_host_spheres(const mstmg_ctx *ctx, int *host);
+/* The D, U, V Mie coefficients of the host spheres (mieoa's dnp_mie, unp_mie,
+ * vnp_mie, mstm-modules-33.f90:5495-5528), laid out as an (zero for spheres
+ * holding no others). */
+int mstmg_host_mie_coefficients(const mstmg_ctx *ctx, double *dn, double *un, double *vn);
 
 /* sphereinteraction (mstm-scatprops-26.f90:25-180).  ain, aout: neqns x nrhs complex.
  * con_tran[r] != 0: column r gets conj((Mie*H)^T conj(x)); mie_mult[r] == 0 skips the

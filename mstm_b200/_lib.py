@@ -24,6 +24,8 @@ SIGNATURES = {
     "mstmg_sphere_orders": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mstmg_mie_coefficients": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mstmg_vol_radius": (c_double, [c_void_p]),
+    "mstmg_host_spheres": (c_int, [c_void_p, c_void_p]),
+    "mstmg_host_mie_coefficients": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mstmg_interaction": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "mstmg_bicg": (c_int, [c_void_p, c_int, c_double, c_void_p, c_void_p, c_int, P(c_int), P(c_double)]),
     "mstmg_planewave": (c_int, [c_void_p, c_double, c_double, c_int, c_void_p]),

@@ -62,6 +62,23 @@ class _Context:
         check(self._L.mstmg_ctx_set_positions(self.ctx, _ptr(pos)), "set_positions")
         self.positions = pos
 
+    def host_spheres(self):
+        """findhostspheres: (the sphere holding each sphere, -1 for none;
+        the number of spheres with a host)."""
+        h = np.zeros(self.number_spheres, np.int32)
+        nh = self._L.mstmg_host_spheres(self.ctx, _ptr(h))
+        if nh < 0:
+            check(nh, "host_spheres")
+        return h, nh
+
+    def host_mie_coefficients(self):
+        """The D, U, V Mie coefficients of the host spheres (an_mie layout,
+        zero for spheres holding no others)."""
+        nt = int(4 * self.sphere_order.sum())
+        d, u, v = (np.zeros(nt, np.complex128) for _ in range(3))
+        check(self._L.mstmg_host_mie_coefficients(self.ctx, _ptr(d), _ptr(u), _ptr(v)), "host_mie")
+        return d, u, v
+
     def miecoefcalc(self):
         nt = int(4 * self.sphere_order.sum())
         an = np.zeros(nt, np.complex128)

@@ -40,7 +40,8 @@ template <int K> __device__ __forceinline__ void block_reduce_store(double (&v)[
 
 template <typename T> __device__ __forceinline__ cpx<double> up(cpx<T> a) { return mk((double)a.x, (double)a.y); }
 
-// cap = p - M*y0 (Mie multiply, idir=1), caw = w - conj(y1); partial sum conj(w)*cap
+// cap = p - M*y0 (Mie multiply, idir=1), caw = w - conj(y1); partial sum conj(w)*cap.
+// an == null: y0 already holds M*y0 (the host-sphere Mie multiply runs apart)
 template <typename T>
 __global__ void __launch_bounds__(RB) post_kernel(int nslots, const int* slot_sphere, const int* order, const int* offset,
                                                   const int* mie_offset, const cpx<T>* an, const cpx<T>* p, const cpx<T>* w,
@@ -54,10 +55,13 @@ __global__ void __launch_bounds__(RB) post_kernel(int nslots, const int* slot_sp
         int row = loc % (L + 2), col = loc / (L + 2) + 1;
         int n = (row <= col) ? col : row - 1;
         int b0 = offset[i] + loc, b1 = b0 + hb;
-        const cpx<T>* A = an + mie_offset[i] + 4 * (n - 1);
         cpx<T> u0 = y0[b0], u1 = y0[b1];
-        cpx<T> m0 = A[0] * u0 + A[2] * u1;
-        cpx<T> m1 = A[1] * u0 + A[3] * u1;
+        cpx<T> m0 = u0, m1 = u1;
+        if (an) {
+            const cpx<T>* A = an + mie_offset[i] + 4 * (n - 1);
+            m0 = A[0] * u0 + A[2] * u1;
+            m1 = A[1] * u0 + A[3] * u1;
+        }
         cpx<T> c0 = p[b0] - m0, c1 = p[b1] - m1;
         cap[b0] = c0;
         cap[b1] = c1;
@@ -71,7 +75,8 @@ __global__ void __launch_bounds__(RB) post_kernel(int nslots, const int* slot_sp
 }
 
 // Initial residual: cr = b - x + M*y0 ; cq = conj(cr) ; cw = cq ; cp = cr.
-// Partials: sum cr*cr (complex, no conjugate) and sum |b|^2.
+// Partials: sum cr*cr (complex, no conjugate) and sum |b|^2.  an == null:
+// y0 already holds M*y0.
 template <typename T>
 __global__ void __launch_bounds__(RB) init_kernel(int nslots, const int* slot_sphere, const int* order, const int* offset,
                                                   const int* mie_offset, const cpx<T>* an, const cpx<T>* b, const cpx<T>* x,
@@ -88,10 +93,14 @@ __global__ void __launch_bounds__(RB) init_kernel(int nslots, const int* slot_sp
         int bb[2] = {offset[i] + loc, offset[i] + loc + hb};
         cpx<T> m[2] = {mk((T)0, (T)0), mk((T)0, (T)0)};
         if (have_y) {
-            const cpx<T>* A = an + mie_offset[i] + 4 * (n - 1);
             cpx<T> u0 = y0[bb[0]], u1 = y0[bb[1]];
-            m[0] = A[0] * u0 + A[2] * u1;
-            m[1] = A[1] * u0 + A[3] * u1;
+            m[0] = u0;
+            m[1] = u1;
+            if (an) {
+                const cpx<T>* A = an + mie_offset[i] + 4 * (n - 1);
+                m[0] = A[0] * u0 + A[2] * u1;
+                m[1] = A[1] * u0 + A[3] * u1;
+            }
         }
         for (int h = 0; h < 2; h++) {
             int k = bb[h];

@@ -69,6 +69,56 @@ int reject_sharded(const mstmg_ctx* c, const char* fn)
     return MSTMG_OK;
 }
 
+// Entry points built for clusters of spheres that all sit in the medium
+// refuse a context with spheres inside others.
+int reject_hosts(const mstmg_ctx* c, const char* fn)
+{
+    if (c && c->hs.on()) {
+        set_err(std::string(fn) + ": not available for a cluster with spheres inside other spheres (host spheres)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
+    return MSTMG_OK;
+}
+
+// findhostspheres (modules:5230-5276): the holder of sphere i is the
+// smallest larger sphere whose surface encloses i's centre (the first in
+// order among equal radii); exteriorrefindex (modules:5408-5419) gives the
+// index around each sphere.
+static void find_hosts(mstmg_ctx* c, const std::vector<double>& ri)
+{
+    const int n = c->n;
+    HostSpheres& h = c->hs;
+    h.host.assign(n, -1);
+    h.vid.assign(n, -1);
+    h.rext.assign(2 * (size_t)n, 0.0);
+    h.nhosted = h.nv = 0;
+    for (int i = 0; i < n; i++) {
+        double xspmin = 1.0e6;
+        for (int j = 0; j < n; j++) {
+            if (!(c->radius[j] > c->radius[i])) continue;
+            if (!c->cfg_of.empty() && c->cfg_of[j] != c->cfg_of[i]) continue;   // an ensemble's configurations do not meet
+            const double d0 = c->hpos[3 * (size_t)j] - c->hpos[3 * (size_t)i], d1 = c->hpos[3 * (size_t)j + 1] - c->hpos[3 * (size_t)i + 1],
+                         d2 = c->hpos[3 * (size_t)j + 2] - c->hpos[3 * (size_t)i + 2];
+            const double rij = std::sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+            if (rij <= c->radius[j] && c->radius[j] < xspmin) {
+                h.host[i] = j;
+                xspmin = c->radius[j];
+            }
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        const int j = h.host[i];
+        if (j >= 0) {
+            h.nhosted++;
+            if (h.vid[j] < 0) h.vid[j] = 0;
+        }
+        h.rext[2 * (size_t)i] = j >= 0 ? ri[2 * (size_t)j] : c->opts.medium_re;
+        h.rext[2 * (size_t)i + 1] = j >= 0 ? ri[2 * (size_t)j + 1] : c->opts.medium_im;
+    }
+    for (int i = 0; i < n; i++)
+        if (h.vid[i] >= 0) h.vid[i] = n + 1 + h.nv++;
+}
+
 // Upload the tiles of this context's shard (all tiles when nshards == 1).
 int apply_shard(mstmg_ctx* c)
 {
@@ -159,6 +209,87 @@ int ensure_gentran(mstmg_ctx* c, int lm)
     return MSTMG_OK;
 }
 
+// The host-sphere pieces of the pair lists: the medium index of every
+// same-host pair (rotation and dense), and the regular translations between
+// each host's internal block and the spheres it holds
+// (external_to_internal_expansion, modules:6533-6608), with their operator
+// record offsets; coincident centres go to the copy list.
+static int setup_host_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np)
+{
+    HostSpheres& h = c->hs;
+    const int n = c->n;
+    std::vector<double> pm(2 * (size_t)std::max(np, 1)), dm(2 * (size_t)std::max(c->ndense, 1));
+    for (int t = 0; t < np; t++) {
+        pm[2 * (size_t)t] = h.rext[2 * (size_t)pr[t].x];
+        pm[2 * (size_t)t + 1] = h.rext[2 * (size_t)pr[t].x + 1];
+    }
+    if (c->ndense > 0) {
+        std::vector<int2> dp(c->ndense);
+        CK(cudaMemcpy(dp.data(), c->dpairs.p, sizeof(int2) * c->ndense, cudaMemcpyDeviceToHost));
+        for (int t = 0; t < c->ndense; t++) {
+            dm[2 * (size_t)t] = h.rext[2 * (size_t)dp[t].x];
+            dm[2 * (size_t)t + 1] = h.rext[2 * (size_t)dp[t].x + 1];
+        }
+    }
+    CK(h.pmed.alloc(pm.size()));
+    CK(h.dmed.alloc(dm.size()));
+    CK(cudaMemcpy(h.pmed.p, pm.data(), sizeof(double) * pm.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h.dmed.p, dm.data(), sizeof(double) * dm.size(), cudaMemcpyHostToDevice));
+    // positions of the device sphere arrays (the internal blocks at their host's centre)
+    std::vector<double> xp(3 * (size_t)(n + 1 + h.nv), 0.0);
+    std::copy(c->hpos.begin(), c->hpos.end(), xp.begin());
+    for (int i = 0; i < n; i++)
+        if (h.vid[i] >= 0)
+            for (int k = 0; k < 3; k++) xp[3 * (size_t)h.vid[i] + k] = c->hpos[3 * (size_t)i + k];
+    std::vector<int2> hp, zp;
+    std::vector<long long> off;
+    std::vector<double> hm;
+    long long u = 0;
+    int maxrec = 4, hl = 0;
+    for (int j = 0; j < n; j++) {
+        const int i = h.host[j];
+        if (i < 0) continue;
+        double d2 = 0.0;
+        for (int k = 0; k < 3; k++) {
+            const double d = c->hpos[3 * (size_t)i + k] - c->hpos[3 * (size_t)j + k];
+            d2 += d * d;
+        }
+        if (d2 < 1.0e-12) {   // zero_translation (modules:6645-6650)
+            zp.push_back(make_int2(h.vid[i], j));
+            continue;
+        }
+        hp.push_back(make_int2(h.vid[i], j));
+        off.push_back(u);
+        const int rec = op_record_units(c->order[i], c->order[j]);
+        maxrec = std::max(maxrec, rec);
+        hl = std::max(hl, std::max(c->order[i], c->order[j]));
+        u += rec;
+        hm.push_back(c->ri_host[2 * (size_t)i]);
+        hm.push_back(c->ri_host[2 * (size_t)i + 1]);
+    }
+    h.nhp = (int)hp.size();
+    h.nzp = (int)zp.size();
+    h.hunits = u;
+    h.hmaxrec = maxrec;
+    h.hlmax = hl;
+    h.hops_ready = false;
+    if (h.nhp > 0) {
+        CK(h.hpairs.alloc(h.nhp));
+        CK(h.hopoff.alloc(h.nhp));
+        CK(h.hmed.alloc(hm.size()));
+        CK(h.xpos.alloc(xp.size()));
+        CK(cudaMemcpy(h.hpairs.p, hp.data(), sizeof(int2) * hp.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h.hopoff.p, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h.hmed.p, hm.data(), sizeof(double) * hm.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h.xpos.p, xp.data(), sizeof(double) * xp.size(), cudaMemcpyHostToDevice));
+    }
+    if (h.nzp > 0) {
+        CK(h.zpairs.alloc(h.nzp));
+        CK(cudaMemcpy(h.zpairs.p, zp.data(), sizeof(int2) * zp.size(), cudaMemcpyHostToDevice));
+    }
+    return MSTMG_OK;
+}
+
 int setup_layout(mstmg_ctx* c)
 {
     const int n = c->n;
@@ -166,11 +297,13 @@ int setup_layout(mstmg_ctx* c)
     c->mie_offset.assign(n + 1, 0);
     int lm = 0, lmin = 1 << 30;
     long long ne = 0, nt = 0;
+    const HostSpheres& hs = c->hs;
     for (int i = 0; i < n; i++) {
         int L = c->order[i];
         c->offset[i] = (int)ne;
         c->mie_offset[i] = (int)nt;
-        ne += 2LL * L * (L + 2);
+        // a sphere holding others: its block, then the field inside it (number_field_expansions 2)
+        ne += 2LL * L * (L + 2) * (hs.on() && hs.vid[i] >= 0 ? 2 : 1);
         nt += 4LL * L;
         lm = std::max(lm, L);
         lmin = std::min(lmin, L);
@@ -187,18 +320,38 @@ int setup_layout(mstmg_ctx* c)
     }
     c->neqns = (int)ne;
     c->lmax = lm;
-    CK(c->d_order.alloc(n));
-    CK(c->d_offset.alloc(n + 1));
-    CK(c->d_mie_offset.alloc(n + 1));
-    CK(cudaMemcpyAsync(c->d_order.p, c->order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d_offset.p, c->offset.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d_mie_offset.p, c->mie_offset.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c->st));
+    // device sphere arrays: the spheres, the offset sentinel at n, then the
+    // internal blocks of the spheres holding others (index n + 1 + v)
+    const int next = n + 1 + hs.nv;
+    std::vector<int> xord(next, 0), xoff(next, 0), xmie(next, 0), hoff(hs.on() ? n : 0, -1);
+    for (int i = 0; i < n; i++) {
+        xord[i] = c->order[i];
+        xoff[i] = c->offset[i];
+        xmie[i] = c->mie_offset[i];
+    }
+    xoff[n] = c->offset[n];
+    xmie[n] = c->mie_offset[n];
+    if (hs.on())
+        for (int i = 0; i < n; i++)
+            if (hs.vid[i] >= 0) {
+                const int v = hs.vid[i], L = c->order[i];
+                xord[v] = L;
+                xoff[v] = hoff[i] = c->offset[i] + 2 * L * (L + 2);
+                xmie[v] = c->mie_offset[i];
+            }
+    CK(c->d_order.alloc(next));
+    CK(c->d_offset.alloc(next));
+    CK(c->d_mie_offset.alloc(next));
+    CK(cudaMemcpyAsync(c->d_order.p, xord.data(), sizeof(int) * next, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_offset.p, xoff.data(), sizeof(int) * next, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_mie_offset.p, xmie.data(), sizeof(int) * next, cudaMemcpyHostToDevice, c->st));
     // slot maps
     std::vector<int> slot(ne / 2), slotf(ne);
-    for (int i = 0; i < n; i++) {
-        int L = c->order[i], hb = L * (L + 2);
-        for (int k = 0; k < hb; k++) slot[c->offset[i] / 2 + k] = i;
-        for (int k = 0; k < 2 * hb; k++) slotf[c->offset[i] + k] = i;
+    for (int i = 0; i < next; i++) {
+        if (i == n) continue;
+        int L = xord[i], hb = L * (L + 2);
+        for (int k = 0; k < hb; k++) slot[xoff[i] / 2 + k] = i;
+        for (int k = 0; k < 2 * hb; k++) slotf[xoff[i] + k] = i;
     }
     CK(c->slot.alloc(ne / 2));
     CK(c->slot_full.alloc(ne));
@@ -210,15 +363,34 @@ int setup_layout(mstmg_ctx* c)
     CK(c->an32.alloc(2 * nt));
     CK(c->qext.alloc(n));
     CK(c->qabs.alloc(n));
-    launch_mie_coefs(n, c->rad.p, c->ri.p, c->opts.medium_re, c->opts.medium_im, c->d_order.p, c->d_mie_offset.p, c->an.p,
-                     c->an_inv.p, c->an32.p, c->qext.p, c->qabs.p, c->st);
+    if (hs.on()) {
+        HostSpheres& h = c->hs;
+        std::vector<int> outside(n);
+        for (int i = 0; i < n; i++) outside[i] = h.host[i] < 0 ? 1 : 0;
+        CK(h.d_hoff.alloc(n));
+        CK(h.d_outside.alloc(n));
+        CK(h.d_host.alloc(n));
+        CK(h.qv.alloc(3LL * n));
+        CK(h.dn.alloc(nt));
+        CK(h.un.alloc(nt));
+        CK(h.vn.alloc(nt));
+        CK(cudaMemcpyAsync(h.d_hoff.p, hoff.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(h.d_outside.p, outside.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(h.d_host.p, h.host.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+    }
+    launch_mie_coefs(n, c->rad.p, c->ri.p, c->opts.medium_re, c->opts.medium_im, hs.on() ? hs.d_rext.p : nullptr, c->d_order.p,
+                     c->d_mie_offset.p, hs.on() ? hs.d_hoff.p : nullptr, c->an.p, c->an_inv.p, c->an32.p, c->hs.dn.p, c->hs.un.p,
+                     c->hs.vn.p, c->qext.p, c->qabs.p, c->st);
     CK(cudaGetLastError());
     // pairs whose smaller order is below translation_switch_order take the
     // reference's dense path (coefficient_translation, rot_op false)
     const int tso = c->opts.translation_switch_order;
     auto dense_pair = [&](int i, int j) { return std::min(c->order[i], c->order[j]) < tso; };
-    // an ensemble has no pairs between its configurations
-    auto same_cfg = [&](int i, int j) { return c->cfg_of.empty() || c->cfg_of[i] == c->cfg_of[j]; };
+    // an ensemble has no pairs between its configurations; spheres interact
+    // directly only inside the same host (modules:6466-6469)
+    auto same_cfg = [&](int i, int j) {
+        return (c->cfg_of.empty() || c->cfg_of[i] == c->cfg_of[j]) && (!hs.on() || hs.host[i] == hs.host[j]);
+    };
     {
         std::vector<int2> dp;
         std::vector<long long> doff;
@@ -242,7 +414,11 @@ int setup_layout(mstmg_ctx* c)
     }
     // pair list (i < j, the reference's loop order) and operator offsets
     long long np = (long long)n * (n - 1) / 2 - c->ndense;
-    if (!c->cfg_of.empty()) {
+    if (hs.on()) {
+        np = -c->ndense;
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++) np += same_cfg(i, j) ? 1 : 0;
+    } else if (!c->cfg_of.empty()) {
         np = -c->ndense;
         for (size_t k = 0; k + 1 < c->cfg_start.size(); k++) {
             const long long m = c->cfg_start[k + 1] - c->cfg_start[k];
@@ -285,7 +461,7 @@ int setup_layout(mstmg_ctx* c)
                 out.push_back({std::min(a_, b_), std::max(a_, b_)});
             }
     };
-    c->tiled = !c->opts.generic_kernel && (lm == lmin) && lmin >= tso && tiled_supported(lm, 1) && n > 1 && n < 65536;
+    c->tiled = !c->opts.generic_kernel && !hs.on() && (lm == lmin) && lmin >= tso && tiled_supported(lm, 1) && n > 1 && n < 65536;
     std::vector<int4> tl;
     if (c->tiled) {
         const int B = TILE_B;
@@ -332,6 +508,10 @@ int setup_layout(mstmg_ctx* c)
     (void)maxrec;
     int rc_ = upload_pairs(c, pr, (int)np, tl);
     if (rc_) return rc_;
+    if (hs.on()) {
+        rc_ = setup_host_pairs(c, pr, (int)np);
+        if (rc_) return rc_;
+    }
     // constant tables
     mstmg::Tables tb(6 * lm + 6);
     std::vector<double> vcc, f1, f2, f3;
@@ -367,9 +547,11 @@ int setup_layout(mstmg_ctx* c)
     CK(c->qtot.alloc(9));
     CK(c->small.alloc(16));
     CK(c->sc.alloc(4));
-    // vol_radius as main_calling_program forms it: (sum r^3)**.333333 (single-precision literal)
+    // vol_radius as main_calling_program forms it: (sum r^3)**.333333 (single-precision
+    // literal) over the spheres outside every other (input:1218-1225)
     double v = 0.0;
-    for (int i = 0; i < n; i++) v = v + c->radius[i] * c->radius[i] * c->radius[i];
+    for (int i = 0; i < n; i++)
+        if (!hs.on() || hs.host[i] < 0) v = v + c->radius[i] * c->radius[i] * c->radius[i];
     c->xg = std::pow(v, (double)0.333333f);
     if (!c->cfg_start.empty()) {
         const int nc = (int)c->cfg_start.size() - 1;
@@ -499,10 +681,36 @@ static int create_impl(mstmg_ctx** out, int nsphere, const double* pos, const do
     if (is_dev(radius)) {
         if (cudaMemcpy(c->radius.data(), radius, sizeof(double) * nsphere, cudaMemcpyDeviceToHost)) return fail(MSTMG_ERR_CUDA);
     }
-    // sphere orders on the device (mieoa order test), read back for the layout
+    c->ri_host.assign(2 * (size_t)nsphere, 0.0);
+    if (is_dev(ref_index)) {
+        if (cudaMemcpy(c->ri_host.data(), ref_index, sizeof(double) * 2 * nsphere, cudaMemcpyDeviceToHost)) return fail(MSTMG_ERR_CUDA);
+    } else {
+        memcpy(c->ri_host.data(), ref_index, sizeof(double) * 2 * nsphere);
+    }
+    if (nconfig > 0) {
+        c->cfg_start.assign(config_start, config_start + nconfig + 1);
+        c->cfg_of.assign(nsphere, 0);
+        for (int k = 0; k < nconfig; k++)
+            for (int i = config_start[k]; i < config_start[k + 1]; i++) c->cfg_of[i] = k;
+    }
+    find_hosts(c, c->ri_host);
+    if (c->hs.on()) {
+        if (nconfig > 0) {
+            set_err("mstmg_ensemble_create: configurations with spheres inside other spheres are not supported in ensembles");
+            return fail(MSTMG_ERR_UNSUPPORTED);
+        }
+        if (c->hs.d_rext.alloc(2LL * nsphere) ||
+            cudaMemcpyAsync(c->hs.d_rext.p, c->hs.rext.data(), sizeof(double) * 2 * nsphere, cudaMemcpyHostToDevice, c->st)) {
+            set_err("copy of the exterior indices failed");
+            return fail(MSTMG_ERR_CUDA);
+        }
+    }
+    // sphere orders on the device (mieoa order test, each sphere in the index
+    // around it), read back for the layout
     DevBuf<int> ord;
     if (ord.alloc(nsphere)) return fail(MSTMG_ERR_CUDA);
-    launch_mie_orders(nsphere, c->rad.p, c->ri.p, c->opts.medium_re, c->opts.medium_im, mie_epsilon, ord.p, c->st);
+    launch_mie_orders(nsphere, c->rad.p, c->ri.p, c->opts.medium_re, c->opts.medium_im, c->hs.on() ? c->hs.d_rext.p : nullptr, mie_epsilon,
+                      ord.p, c->st);
     c->order.assign(nsphere, 0);
     if (cudaMemcpyAsync(c->order.data(), ord.p, sizeof(int) * nsphere, cudaMemcpyDeviceToHost, c->st) ||
         cudaStreamSynchronize(c->st)) {
@@ -511,12 +719,10 @@ static int create_impl(mstmg_ctx** out, int nsphere, const double* pos, const do
         return fail(MSTMG_ERR_CUDA);
     }
     ord.release();
-    if (nconfig > 0) {
-        c->cfg_start.assign(config_start, config_start + nconfig + 1);
-        c->cfg_of.assign(nsphere, 0);
-        for (int k = 0; k < nconfig; k++)
-            for (int i = config_start[k]; i < config_start[k + 1]; i++) c->cfg_of[i] = k;
-    }
+    // a host has at least the order of every sphere inside it (modules:5331-5342)
+    if (c->hs.on())
+        for (int i = 0; i < nsphere; i++)
+            for (int j = c->hs.host[i]; j >= 0; j = c->hs.host[j]) c->order[j] = std::max(c->order[j], c->order[i]);
     rc = setup_layout(c);
     if (rc != MSTMG_OK) return fail(rc);
     *out = c;
@@ -552,6 +758,7 @@ extern "C" void mstmg_ctx_destroy(mstmg_ctx* c)
 extern "C" int mstmg_ctx_set_positions(mstmg_ctx* c, const double* pos)
 {
     if (!c || !pos) return MSTMG_ERR_ARG;
+    if (int rh = reject_hosts(c, "mstmg_ctx_set_positions")) return rh;
     if (!is_dev(pos))
         for (int k = 0; k < 3 * c->n; k++)
             if (!std::isfinite(pos[k])) {
@@ -575,6 +782,8 @@ extern "C" int mstmg_set_pair_shard(mstmg_ctx* c, int shard, int nshards)
 {
     if (!c || nshards < 1 || shard < 0 || shard >= nshards) return MSTMG_ERR_ARG;
     if (int rc0 = reject_ensemble(c, "mstmg_set_pair_shard")) return rc0;
+    if (nshards > 1)
+        if (int rh = reject_hosts(c, "mstmg_set_pair_shard")) return rh;
     if (nshards > 1 && (!c->tiled || c->ndense > 0)) {
         set_err("mstmg_set_pair_shard: shards are tiles of pairs of one sphere order (no dense pairs)");
         return MSTMG_ERR_UNSUPPORTED;
@@ -603,6 +812,29 @@ extern "C" int mstmg_mie_coefficients(const mstmg_ctx* c, double* an, double* qe
     if (an) CK(copy_out(an, c->an.p, sizeof(zd) * c->mie_offset[c->n], c->st));
     if (qext) CK(copy_out(qext, c->qext.p, sizeof(double) * c->n, c->st));
     if (qabs) CK(copy_out(qabs, c->qabs.p, sizeof(double) * c->n, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return MSTMG_OK;
+}
+
+extern "C" int mstmg_host_spheres(const mstmg_ctx* c, int* host)
+{
+    if (!c) return MSTMG_ERR_ARG;
+    if (host)
+        for (int i = 0; i < c->n; i++) host[i] = c->hs.on() ? c->hs.host[i] : -1;
+    return c->hs.nhosted;
+}
+
+extern "C" int mstmg_host_mie_coefficients(const mstmg_ctx* c, double* dn, double* un, double* vn)
+{
+    if (!c) return MSTMG_ERR_ARG;
+    const size_t nt = (size_t)c->mie_offset[c->n];
+    double* out[3] = {dn, un, vn};
+    const zd* src[3] = {c->hs.dn.p, c->hs.un.p, c->hs.vn.p};
+    for (int k = 0; k < 3; k++) {
+        if (!out[k]) continue;
+        if (c->hs.on()) CK(copy_out(out[k], src[k], sizeof(zd) * nt, c->st));
+        else memset(out[k], 0, sizeof(zd) * nt);
+    }
     CK(cudaStreamSynchronize(c->st));
     return MSTMG_OK;
 }

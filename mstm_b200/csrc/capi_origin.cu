@@ -155,6 +155,7 @@ extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_e
                                 double* g, int* t_matrix_order, double* amnp0, int amnp0_cap)
 {
     if (int rc0 = reject_ensemble(c, "mstmg_scattering")) return rc0;
+    if (int rh = reject_hosts(c, "mstmg_scattering")) return rh;
     NvtxRange nvtx_("mstmg_scattering");
     if (!c || !amnp || nangles < 2 || max_t_order < 1) {
         set_err("mstmg_scattering: bad arguments");
@@ -289,6 +290,7 @@ extern "C" int mstmg_scattering_plane(mstmg_ctx* c, int t_matrix_order, const do
 extern "C" int mstmg_t_matrix_order(mstmg_ctx* c, double trans_eps, int max_t_order, int* t_matrix_order)
 {
     if (int rc0 = reject_ensemble(c, "mstmg_t_matrix_order")) return rc0;
+    if (int rh = reject_hosts(c, "mstmg_t_matrix_order")) return rh;
     if (!c || max_t_order < 1 || !t_matrix_order) {
         set_err("mstmg_t_matrix_order: bad arguments");
         return MSTMG_ERR_ARG;
@@ -311,6 +313,7 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
                              double* tmat, double* sphere_qeff, double* qtot, int* order_used, int* maxiter, double* maxerr)
 {
     if (int rc0 = reject_ensemble(c, "mstmg_tmatrix")) return rc0;
+    if (int rh = reject_hosts(c, "mstmg_tmatrix")) return rh;
     if (int rc1 = reject_sharded(c, "mstmg_tmatrix")) return rc1;
     NvtxRange nvtx_("mstmg_tmatrix");
     if (!c || t_matrix_order < 1 || t_matrix_order > 200 || !tmat || max_iterations < 1) {

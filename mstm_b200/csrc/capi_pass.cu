@@ -23,6 +23,7 @@ DenseArgs dense_args(mstmg_ctx* c)
     d.rec32 = nullptr;
     d.rimed_re = c->opts.medium_re;
     d.rimed_im = c->opts.medium_im;
+    d.pmed = c->hs.on() ? c->hs.dmed.p : nullptr;
     d.g.tc = c->gt_tc.p;
     d.g.nmax = c->gt_nmax;
     d.g.nd = c->gt_nmax * (c->gt_nmax + 2);
@@ -82,14 +83,76 @@ int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
     a.bcofd = c->bcofd.p;
     a.rimed_re = c->opts.medium_re;
     a.rimed_im = c->opts.medium_im;
+    a.pmed = c->hs.on() ? c->hs.pmed.p : nullptr;
     a.err = c->err.p;
-    CK(c->opgen_xi.alloc(opgen_xi_scratch(c->npairs)));
+    CK(c->opgen_xi.alloc(opgen_xi_scratch(std::max(c->npairs, c->hs.nhp))));
     a.xi = c->opgen_xi.p;
     launch_opgen(a, c->nsm, c->st);
     CK(cudaGetLastError());
+    if (need64 && c->hs.nhp > 0) {
+        // regular translations between hosts and the spheres they hold, in
+        // the host's index (external_to_internal_expansion, modules:6579-6592)
+        HostSpheres& h = c->hs;
+        CK(h.hop64.alloc(h.hunits));
+        OpGenArgs b = a;
+        b.npairs = h.nhp;
+        b.pairs = h.hpairs.p;
+        b.pos = h.xpos.p;
+        b.opoff = h.hopoff.p;
+        b.op64 = h.hop64.p;
+        b.op32 = nullptr;
+        b.row32 = 0;
+        b.pmed = h.hmed.p;
+        b.regular = 1;
+        launch_opgen(b, c->nsm, c->st);
+        CK(cudaGetLastError());
+        h.hops_ready = true;
+    }
     if (need64) c->ops64_ready = true;
     if (need32) c->ops32_ready = true;
     return MSTMG_OK;
+}
+
+// y[:, 0:nrhs] += the host-sphere couplings of x (external_to_internal_expansion)
+int translate_hosts(mstmg_ctx* c, const zd* x, zd* y, int nrhs, unsigned contran)
+{
+    HostSpheres& h = c->hs;
+    if (!h.on()) return MSTMG_OK;
+    if (h.nhp > 0) {
+        if (!h.hops_ready) {
+            set_err("internal error: host-sphere operators not generated");
+            return MSTMG_ERR_ARG;
+        }
+        TransArgs<double> a;
+        a.npairs = h.nhp;
+        a.pairs = h.hpairs.p;
+        a.order = c->d_order.p;
+        a.offset = c->d_offset.p;
+        a.ops = h.hop64.p;
+        a.opoff = h.hopoff.p;
+        a.x = x;
+        a.y = y;
+        a.ld = c->neqns;
+        a.nrhs = nrhs;
+        a.contran = contran;
+        a.lmax = h.hlmax;
+        a.maxrec = h.hmaxrec;
+        a.err = c->err.p;
+        launch_translate<double>(a, c->nsm, c->st);
+    }
+    launch_mtransfer(h.nzp, h.zpairs.p, c->d_order.p, c->d_offset.p, x, y, c->neqns, nrhs, c->st);
+    CK(cudaGetLastError());
+    return MSTMG_OK;
+}
+
+void mie_all(mstmg_ctx* c, int idir, int conj_in, const zd* x, zd* y)
+{
+    SlotMaps sm = c->sm();
+    if (c->hs.on())
+        launch_hmie(sm.nslots, c->n, sm.slot, sm.order, sm.offset, sm.mie_offset, c->hs.d_hoff.p, c->an.p, c->hs.dn.p, c->hs.un.p,
+                    c->hs.vn.p, idir, conj_in, x, y, c->st);
+    else
+        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, idir, conj_in, x, y, c->st);
 }
 int ensure_ops(mstmg_ctx* c, int prec, bool force) { return ensure_ops_both(c, prec == 0, prec == 1, force); }
 
@@ -124,7 +187,16 @@ template <> int rows_pass<float>(mstmg_ctx* c, const TiledArgs<float>& tf, int n
 template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran, int nchunk)
 {
     NvtxRange nvtx_(sizeof(T) == 8 ? "translation pass FP64" : "translation pass FP32");
+    if (sizeof(T) == 4 && c->hs.on()) {
+        set_err("FP32 translation passes are not available for clusters with spheres inside other spheres");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
     CK(cudaMemsetAsync(y, 0, sizeof(cpx<T>) * (size_t)c->neqns * nrhs * nchunk, c->st));
+    if (c->hs.on()) {
+        if (nchunk > 1) return MSTMG_ERR_UNSUPPORTED;
+        int rh = translate_hosts(c, (const zd*)x, (zd*)y, nrhs, contran);
+        if (rh) return rh;
+    }
     if (c->ndense > 0) {
         if (nchunk > 1) return MSTMG_ERR_UNSUPPORTED;
         const T* drec = sizeof(T) == 8 ? (const T*)c->dop64.p : (const T*)c->dop32.p;
@@ -434,7 +506,6 @@ int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, co
     int rc = skip_external ? MSTMG_OK : ensure_ops(c, 0, initial_run != 0);
     if (rc) return rc;
     const int ne = c->neqns;
-    SlotMaps sm = c->sm();
     unsigned mask = 0;
     CK(copy_in(c->X64.p, ain, sizeof(zd) * (size_t)ne * nrhs, c->st));
     // columns left out of rhs_list are not translated: their output is zero
@@ -447,14 +518,20 @@ int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, co
         zd* col = c->X64.p + (size_t)r * ne;
         if (ct) {
             mask |= 1u << r;
-            if (mm) launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, -1, 1, col, col, c->st);
+            if (mm) mie_all(c, -1, 1, col, col);
             else launch_conj_copy<double>(ne, col, col, c->st);
         }
     }
     if (skip_external) {
-        // no pair translation (and, on this path, no host spheres or plane
-        // boundaries): the interaction is zero
+        // no pair translation: only the host-sphere couplings (none without
+        // host spheres; no plane boundaries on this path)
         CK(cudaMemsetAsync(c->Y64.p, 0, sizeof(zd) * (size_t)ne * nrhs, c->st));
+        if (c->hs.on()) {
+            rc = ensure_ops(c, 0, initial_run != 0);
+            if (rc) return rc;
+            rc = translate_hosts(c, c->X64.p, c->Y64.p, nrhs, mask);
+            if (rc) return rc;
+        }
     } else {
         rc = translate<double>(c, c->X64.p, c->Y64.p, nrhs, mask);
         if (rc) return rc;
@@ -464,7 +541,7 @@ int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, co
         int mm = mie_mult ? mie_mult[r] : 1;
         zd* col = c->Y64.p + (size_t)r * ne;
         if (!ct) {
-            if (mm) launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, 1, 0, col, col, c->st);
+            if (mm) mie_all(c, 1, 0, col, col);
         } else {
             launch_conj_copy<double>(ne, col, col, c->st);
         }
@@ -843,6 +920,7 @@ extern "C" int mstmg_fft_setup(mstmg_ctx* c, double cell_volume_fraction, double
                                int* cell_dim, double* d_cell_out, int* node_order_out, int* near_pairs)
 {
     if (int rc0 = reject_ensemble(c, "mstmg_fft_setup")) return rc0;
+    if (int rh = reject_hosts(c, "mstmg_fft_setup")) return rh;
     NvtxRange nvtx_("mstmg_fft_setup");
     if (!c || c->n < 2 || neighbor_node_model < 0 || neighbor_node_model > 2) {
         set_err("mstmg_fft_setup: bad arguments (two or more spheres, neighbor_node_model 0..2)");

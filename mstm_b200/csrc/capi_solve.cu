@@ -4,6 +4,37 @@
 // FP64 refinement, restarted GMRES with FP64 true residuals).
 #include "ctx.cuh"
 
+// The incident plane wave at every sphere the wave reaches (sphereplanewavecoef,
+// scatprops:262-281): all spheres, or those outside every other sphere
+static void planewave_ctx(mstmg_ctx* c, double alpha, double sinc, int dir)
+{
+    launch_planewave(alpha, sinc, dir, c->lmax, c->neqns, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p,
+                     c->pmnp.p, c->st, c->n, c->hs.on() ? c->hs.d_outside.p : nullptr);
+}
+
+// qefficiencyfactors + qtotcalc of the solution amnp (device, 2 columns) for
+// the incident field in c->pmnp (scatprops:782-912).  With host spheres the
+// exciting fields are the interaction without the Mie multiply plus the
+// incident field, in Y64's first two columns.
+static int qeff_ctx(mstmg_ctx* c, const zd* amnp)
+{
+    const int ne = c->neqns;
+    const zd* g = nullptr;
+    if (c->hs.on()) {
+        int rc = ensure_ops(c, 0, false);
+        if (rc) return rc;
+        rc = translate<double>(c, amnp, c->Y64.p, 2, 0u);
+        if (rc) return rc;
+        launch_add_correction_d(2 * ne, c->Y64.p, c->pmnp.p, c->st);
+        g = c->Y64.p;
+    }
+    launch_qeff(c->n, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, mk(c->opts.medium_re, c->opts.medium_im), c->an_inv.p,
+                amnp, c->pmnp.p, ne, c->qeff.p, c->xg, c->qtot.p, c->st, c->hs.on() ? c->hs.d_rext.p : nullptr, g,
+                c->hs.on() ? c->hs.d_host.p : nullptr, c->hs.on() ? c->hs.qv.p : nullptr);
+    CK(cudaGetLastError());
+    return MSTMG_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Batched BiCG: S independent systems advance in lockstep, sharing one
 // translation pass per iteration ([p_1, w_1, p_2, w_2, ...], the w columns as
@@ -33,9 +64,13 @@ int bicg_batched(mstmg_ctx* c, int S, const cpx<T>* const* b, BicgVecs<T>* v, bo
         rc = translate<T>(c, X, Y, S, 0u);
         if (rc) return rc;
     }
+    // host spheres: the Mie multiply runs apart (mie_all), the fused kernels take y as M y
+    const bool hosts = sizeof(T) == 8 && c->hs.on();
+    const cpx<T>* anf = hosts ? nullptr : an;
     for (int s = 0; s < S; s++) {
         if (!have_x0) CK(cudaMemsetAsync(v[s].x, 0, sizeof(cpx<T>) * ne, c->st));
-        launch_init<T>(sm, an, b[s], v[s].x, Y + (size_t)s * ne, have_x0 ? 1 : 0, v[s].r, v[s].p, v[s].w, v[s].q, part, c->sc.p + s, 1,
+        if (hosts && have_x0) mie_all(c, 1, 0, (const zd*)(Y + (size_t)s * ne), (zd*)(Y + (size_t)s * ne));
+        launch_init<T>(sm, anf, b[s], v[s].x, Y + (size_t)s * ne, have_x0 ? 1 : 0, v[s].r, v[s].p, v[s].w, v[s].q, part, c->sc.p + s, 1,
                        c->nsm, c->st);
     }
     CK(cudaMemcpyAsync(c->h_sc, c->sc.p, sizeof(BicgScalars) * S, cudaMemcpyDeviceToHost, c->st));
@@ -56,14 +91,16 @@ int bicg_batched(mstmg_ctx* c, int S, const cpx<T>* const* b, BicgVecs<T>* v, bo
         for (int k = 0; k < a; k++) {
             int s = slots[k];
             CK(cudaMemcpyAsync(X + (size_t)(2 * k) * ne, v[s].p, sizeof(cpx<T>) * ne, cudaMemcpyDeviceToDevice, c->st));
-            launch_mie<T>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, an, -1, 1, v[s].w, X + (size_t)(2 * k + 1) * ne, c->st);
+            if (hosts) mie_all(c, -1, 1, (const zd*)v[s].w, (zd*)(X + (size_t)(2 * k + 1) * ne));
+            else launch_mie<T>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, an, -1, 1, v[s].w, X + (size_t)(2 * k + 1) * ne, c->st);
             mask |= 2u << (2 * k);
         }
         rc = translate<T>(c, X, Y, 2 * a, mask);
         if (rc) return rc;
         for (int k = 0; k < a; k++) {
             int s = slots[k];
-            launch_post<T>(sm, an, v[s].p, v[s].w, Y + (size_t)(2 * k) * ne, Y + (size_t)(2 * k + 1) * ne, v[s].cap, v[s].caw, part,
+            if (hosts) mie_all(c, 1, 0, (const zd*)(Y + (size_t)(2 * k) * ne), (zd*)(Y + (size_t)(2 * k) * ne));
+            launch_post<T>(sm, anf, v[s].p, v[s].w, Y + (size_t)(2 * k) * ne, Y + (size_t)(2 * k + 1) * ne, v[s].cap, v[s].caw, part,
                            c->sc.p + s, c->nsm, c->st);
             launch_upd<T>(ne, v[s].x, v[s].r, v[s].q, v[s].p, v[s].w, v[s].cap, v[s].caw, part, c->sc.p + s, eps[s], c->nsm, c->st);
         }
@@ -122,7 +159,7 @@ int oos_solve(mstmg_ctx* c, const zd* b, zd* x, int niter, double eps, int* iter
     for (it = 1; it <= -niter; it++) {
         int rc = translate<double>(c, cp, c->Y64.p, 1, 0u);
         if (rc) return rc;
-        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, 1, 0, c->Y64.p, cr, c->st);
+        mie_all(c, 1, 0, c->Y64.p, cr);
         launch_add_correction_d(ne, x, cr, c->st);
         CK(cudaMemcpyAsync(cp, cr, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
         launch_rr_dot_norm(ne, cr, c->part.p, c->small.p, c->nsm, c->st);
@@ -181,8 +218,7 @@ extern "C" int mstmg_bicg(mstmg_ctx* c, int niter, double eps, const double* pnp
 extern "C" int mstmg_planewave(mstmg_ctx* c, double alpha, double sinc, int dir, double* pmnp)
 {
     if (!c || !pmnp) return MSTMG_ERR_ARG;
-    launch_planewave(alpha, sinc, dir, c->lmax, c->neqns, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p,
-                     c->pmnp.p, c->st);
+    planewave_ctx(c, alpha, sinc, dir);
     CK(cudaGetLastError());
     CK(copy_out(pmnp, c->pmnp.p, sizeof(zd) * 2 * (size_t)c->neqns, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -304,6 +340,10 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
     if (!c || !amnp) return MSTMG_ERR_ARG;
     if (int rc0 = reject_ensemble(c, "mstmg_fixed_orientation")) return rc0;
     if (int rc1 = reject_sharded(c, "mstmg_fixed_orientation")) return rc1;
+    if (c->hs.on() && (x0 || (niter > 0 && c->opts.precision == MSTMG_PRECISION_MIXED))) {
+        set_err("mstmg_fixed_orientation: with spheres inside other spheres the solve is the FP64 BiCG (precision FP64, no initial guess)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
     const int ne = c->neqns;
     SlotMaps sm = c->sm();
     c->passes64 = c->passes32 = 0;
@@ -311,12 +351,10 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
     // operators are (re)generated for this configuration: the reference's initial_run
     int rc = ensure_ops_both(c, true, c->opts.precision == MSTMG_PRECISION_MIXED, true);
     if (rc) return rc;
-    launch_planewave(alpha, sinc, dir, c->lmax, ne, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p,
-                     c->pmnp.p, c->st);
+    planewave_ctx(c, alpha, sinc, dir);
     zd* bvec = c->bvec64.p;   // pmnpan for both polarisations: 2 x ne
     for (int p = 0; p < 2; p++)
-        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, 1, 0, c->pmnp.p + (size_t)p * ne,
-                           bvec + (size_t)p * ne, c->st);
+        mie_all(c, 1, 0, c->pmnp.p + (size_t)p * ne, bvec + (size_t)p * ne);
     CK(cudaGetLastError());
     int istat = 0;
     int it[2] = {0, 0}, st[2] = {0, 0};
@@ -358,6 +396,19 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
         if (xinit != c->amnp.p)
             for (int p = 0; p < 2; p++)
                 CK(cudaMemcpyAsync(c->amnp.p + (size_t)p * ne, bvec + (size_t)p * ne, sizeof(zd) * ne, cudaMemcpyDeviceToDevice, c->st));
+        if (c->hs.on()) {
+            // the couplings through the host spheres alone, applied twice
+            // (solver:509-518): x += (M H_host) x + (M H_host)^2 x
+            CK(cudaMemcpyAsync(c->X64.p, c->amnp.p, sizeof(zd) * 2 * (size_t)ne, cudaMemcpyDeviceToDevice, c->st));
+            for (int k = 0; k < 2; k++) {
+                CK(cudaMemsetAsync(c->Y64.p, 0, sizeof(zd) * 2 * (size_t)ne, c->st));
+                rc = translate_hosts(c, c->X64.p, c->Y64.p, 2, 0u);
+                if (rc) return rc;
+                mie_all(c, 1, 0, c->Y64.p, c->X64.p);
+                mie_all(c, 1, 0, c->Y64.p + ne, c->X64.p + ne);
+            }
+            launch_add_correction_d(2 * ne, c->amnp.p, c->X64.p, c->st);
+        }
     } else if (c->opts.precision == MSTMG_PRECISION_MIXED) {
         zd* xs[2] = {c->amnp.p, c->amnp.p + ne};
         zd* bs[2] = {bvec, bvec + ne};
@@ -420,9 +471,8 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
     if (st[0] == 2 || st[1] == 2) istat = 1;
     c->iters[0] = it[0];
     c->iters[1] = it[1];
-    launch_qeff(c->n, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, mk(c->opts.medium_re, c->opts.medium_im), c->an_inv.p,
-                c->amnp.p, c->pmnp.p, ne, c->qeff.p, c->xg, c->qtot.p, c->st);
-    CK(cudaGetLastError());
+    rc = qeff_ctx(c, c->amnp.p);
+    if (rc) return rc;
     CK(copy_out(amnp, c->amnp.p, sizeof(zd) * 2 * (size_t)ne, c->st));
     if (qeff) CK(copy_out(qeff, c->qeff.p, sizeof(double) * 9 * (size_t)c->n, c->st));
     if (qtot) CK(copy_out(qtot, c->qtot.p, sizeof(double) * 9, c->st));
@@ -461,12 +511,10 @@ extern "C" int mstmg_ensemble_fixed_orientation(mstmg_ctx* c, double alpha, doub
     c->outer = 0;
     int rc = ensure_ops_both(c, true, true, true);
     if (rc) return rc;
-    launch_planewave(alpha, sinc, dir, c->lmax, ne, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p, c->pmnp.p,
-                     c->st);
+    planewave_ctx(c, alpha, sinc, dir);
     zd* bvec = c->bvec64.p;
     for (int p = 0; p < 2; p++)
-        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, 1, 0, c->pmnp.p + (size_t)p * ne,
-                           bvec + (size_t)p * ne, c->st);
+        mie_all(c, 1, 0, c->pmnp.p + (size_t)p * ne, bvec + (size_t)p * ne);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->amnp.p, bvec, sizeof(zd) * 2 * (size_t)ne, cudaMemcpyDeviceToDevice, c->st));
     if (!c->ens_gm.hh && (rc = c->ens_gm.setup(S, c->ens_ldv, c->opts.gmres_restart, "mstmg_ensemble_fixed_orientation"))) return rc;
@@ -507,11 +555,9 @@ extern "C" int mstmg_fixed_orientation_rhs(mstmg_ctx* c, double alpha, double si
     if (int rc0 = reject_ensemble(c, "mstmg_fixed_orientation_rhs")) return rc0;
     const int ne = c->neqns;
     SlotMaps sm = c->sm();
-    launch_planewave(alpha, sinc, dir, c->lmax, ne, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p,
-                     c->pmnp.p, c->st);
+    planewave_ctx(c, alpha, sinc, dir);
     for (int p = 0; p < 2; p++)
-        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, 1, 0, c->pmnp.p + (size_t)p * ne,
-                           c->bvec64.p + (size_t)p * ne, c->st);
+        mie_all(c, 1, 0, c->pmnp.p + (size_t)p * ne, c->bvec64.p + (size_t)p * ne);
     CK(cudaGetLastError());
     CK(copy_out(pmnpan, c->bvec64.p, sizeof(zd) * 2 * (size_t)ne, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -525,12 +571,9 @@ extern "C" int mstmg_efficiencies(mstmg_ctx* c, double alpha, double sinc, int d
     if (!c || !amnp) return MSTMG_ERR_ARG;
     if (int rc0 = reject_ensemble(c, "mstmg_efficiencies")) return rc0;
     const int ne = c->neqns;
-    launch_planewave(alpha, sinc, dir, c->lmax, ne, c->slot_full.p, c->d_order.p, c->d_offset.p, c->pos.p, c->pw0.p, c->drot.p,
-                     c->pmnp.p, c->st);
+    planewave_ctx(c, alpha, sinc, dir);
     CK(copy_in(c->amnp.p, amnp, sizeof(zd) * 2 * (size_t)ne, c->st));
-    launch_qeff(c->n, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, mk(c->opts.medium_re, c->opts.medium_im), c->an_inv.p,
-                c->amnp.p, c->pmnp.p, ne, c->qeff.p, c->xg, c->qtot.p, c->st);
-    CK(cudaGetLastError());
+    if (int rq = qeff_ctx(c, c->amnp.p)) return rq;
     if (qeff) CK(copy_out(qeff, c->qeff.p, sizeof(double) * 9 * (size_t)c->n, c->st));
     if (qtot) CK(copy_out(qtot, c->qtot.p, sizeof(double) * 9, c->st));
     CK(cudaStreamSynchronize(c->st));

@@ -284,6 +284,35 @@ struct GmresWork {
     }
 };
 
+// Spheres inside other spheres (MSTM's host spheres, spheredata
+// findhostspheres, december2023/mstm-modules-33.f90:5230-5276).  A sphere
+// that holds others has a second block of equations right after its own,
+// the regular field inside it; the kernels see that block as a sphere of
+// its own at index n + 1 + v (after the offset sentinel at n), with the
+// host's order, so that slot maps and pair lists address it like any other.
+struct HostSpheres {
+    int nhosted = 0;             // spheres with a host (number_host_spheres)
+    int nv = 0;                  // spheres holding others
+    std::vector<int> host;       // per sphere: the sphere holding it, -1 none
+    std::vector<int> vid;        // per sphere: the index of its internal block, -1 none
+    std::vector<double> rext;    // per sphere: re, im of the index around it (exteriorrefindex)
+    DevBuf<double> d_rext, qv, xpos;   // xpos: positions of the device sphere arrays (internal blocks at their host's centre)
+    DevBuf<int> d_host, d_hoff, d_outside;   // holding sphere; offset of the internal block (-1 none); 1 outside every sphere
+    DevBuf<zd> dn, un, vn;       // the holding spheres' D, U, V Mie coefficients (mie_offset)
+    DevBuf<double> pmed, dmed;   // the index of each same-host pair's medium: rotation pairs, dense pairs
+    // external_to_internal_expansion: (internal block, held sphere) pairs
+    // translated by regular operators in the host's index; coincident
+    // centres copy the common orders instead
+    int nhp = 0, hmaxrec = 4, hlmax = 0;
+    long long hunits = 0;
+    DevBuf<int2> hpairs, zpairs;
+    int nzp = 0;
+    DevBuf<long long> hopoff;
+    DevBuf<double> hop64, hmed;
+    bool hops_ready = false;
+    bool on() const { return nhosted > 0; }
+};
+
 struct mstmg_ctx {
     int dev = 0, nsm = 148;
     cudaStream_t st = nullptr;
@@ -297,6 +326,7 @@ struct mstmg_ctx {
     std::vector<int> order, offset, mie_offset;
     std::vector<double> radius;
     std::vector<double> hpos;   // host copy of the positions (cluster origin)
+    std::vector<double> ri_host;   // host copy of the refractive indices (re, im)
     DevBuf<double> pos, rad, ri, qext, qabs;
     DevBuf<int> d_order, d_offset, d_mie_offset, slot, slot_full;
     DevBuf<zd> an, an_inv;
@@ -351,6 +381,7 @@ struct mstmg_ctx {
     int host_syncs = 0;   // host synchronisations of the last mixed GMRES solve
     std::vector<int> tord;   // translation order of each sphere to the cluster origin (mstmg_t_matrix_order)
     std::unique_ptr<FftState> fft;   // set by mstmg_fft_setup
+    HostSpheres hs;                  // spheres inside others (empty when none)
     // pairs below translation_switch_order: dense gentranmatrix records (densepair.cu)
     int ndense = 0;
     long long dense_units = 0;
@@ -408,6 +439,7 @@ struct EnsSeg {
 void resolve_timing(mstmg_ctx* c);
 int reject_ensemble(const mstmg_ctx* c, const char* fn);
 int reject_sharded(const mstmg_ctx* c, const char* fn);
+int reject_hosts(const mstmg_ctx* c, const char* fn);
 int apply_shard(mstmg_ctx* c);
 int check_kernel_err(mstmg_ctx* c);
 int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const std::vector<int4>& tl);
@@ -425,6 +457,11 @@ int tc_translate(mstmg_ctx* c, const zf* x, zf* y, int ncols);
 template <typename T> int translate_many(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int ncols, unsigned pattern2);
 int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, const int* con_tran, const int* mie_mult, int initial_run,
                      const int* rhs_list, int skip_external);
+// host spheres: y[:, 0:nrhs] += the regular translations between hosts and
+// the spheres they hold (external_to_internal_expansion)
+int translate_hosts(mstmg_ctx* c, const zd* x, zd* y, int nrhs, unsigned contran);
+// the Mie multiply of every sphere (host spheres' blocks included), FP64
+void mie_all(mstmg_ctx* c, int idir, int conj_in, const zd* x, zd* y);
 template <typename T> int fft_far(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int ncols, unsigned contran);
 int fft_build(mstmg_ctx* c);
 // capi_origin.cu

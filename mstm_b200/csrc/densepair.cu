@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(128) dense_gen_kernel(DenseArgs a)
     const int Li = a.order[i], Lj = a.order[j];
     const int nbi = Li * (Li + 2), nbj = Lj * (Lj + 2);
     double xp[3] = {a.pos[3 * i] - a.pos[3 * j], a.pos[3 * i + 1] - a.pos[3 * j + 1], a.pos[3 * i + 2] - a.pos[3 * j + 2]};
-    gt_prepare(gs, a.g, xp, 3, mk(a.rimed_re, a.rimed_im), Li + Lj);
+    gt_prepare(gs, a.g, xp, 3, a.pmed ? mk(a.pmed[2 * q], a.pmed[2 * q + 1]) : mk(a.rimed_re, a.rimed_im), Li + Lj);
     zd* rec64 = a.rec64 ? a.rec64 + a.off[q] : nullptr;
     zf* rec32 = a.rec32 ? a.rec32 + a.off[q] : nullptr;
     for (int e = threadIdx.x; e < nbi * nbj; e += blockDim.x) {

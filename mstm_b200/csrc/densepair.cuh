@@ -13,6 +13,7 @@ struct DenseArgs {
     zd* rec64;               // generation targets (either may be null)
     zf* rec32;
     double rimed_re, rimed_im;
+    const double* pmed = nullptr;   // per pair re, im: the index the pair sits in (null: rimed)
     GtConst g;
 };
 

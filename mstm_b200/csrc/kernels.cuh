@@ -17,8 +17,10 @@ struct OpGenArgs {
     const double* rfnr;      // 1 / sqrt(k) (k >= 1)
     const double* bcofd;     // bcof(n,n)
     double rimed_re, rimed_im;
+    const double* pmed = nullptr;   // per pair re, im: the index the pair sits in (null: rimed)
+    int regular = 0;         // 1: regular translations (vswf_type 1, Bessel j) instead of outgoing
     int* err;
-    zd* xi;                  // scratch, opgen_xi_scratch(npairs) complex: Hankel functions per pair
+    zd* xi;                  // scratch, opgen_xi_scratch(npairs) complex: Hankel (or Bessel) functions per pair
 };
 
 #include "oplayout.cuh"
@@ -43,6 +45,9 @@ template <typename T> struct TransArgs {
 };
 template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cudaStream_t st);
 template <typename T> size_t translate_smem_bytes(int lmax, int nrhs, int maxrec);
+// y(:, r) += the order-truncated copies between the blocks of each pair
+// (i, j) and back: coincident centres of a host and a sphere it holds
+void launch_mtransfer(int npairs, const int2* pairs, const int* order, const int* offset, const zd* x, zd* y, int ld, int nrhs, cudaStream_t st);
 
 // Mie multiply over all spheres: y(:,r) = A x(:,r) (idir=1) or A^T x(:,r);
 // optional conjugation of the input.  slot_sphere maps each (row, column)

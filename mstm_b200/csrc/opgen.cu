@@ -77,7 +77,7 @@ __device__ __forceinline__ PairGeom pair_geom(const OpGenArgs& a, int q)
 }
 
 // e^{i phi} into the record and xi_w(z) / z, z = r m_medium, w = 0 .. nt + ns
-// into the scratch: one thread per pair
+// into the scratch (psi_w(z) / z for regular translations): one thread per pair
 __global__ void __launch_bounds__(128) opgen_pair_kernel(OpGenArgs a)
 {
     zd hs[2 * (XIW + 1)];   // spherical Bessel scratch of the complex-argument branch
@@ -107,8 +107,9 @@ __global__ void __launch_bounds__(128) opgen_pair_kernel(OpGenArgs a)
         }
         zd* xi = a.xi + (size_t)q * XIW;
         const int nl = g.nt + g.ns;
-        const zd z = mk(g.r * a.rimed_re, g.r * a.rimed_im);
-        mstm_crichankel(nl, z, xi, hs);
+        const zd z = a.pmed ? mk(g.r * a.pmed[2 * q], g.r * a.pmed[2 * q + 1]) : mk(g.r * a.rimed_re, g.r * a.rimed_im);
+        if (a.regular) mstm_cricbessel(nl, z, xi, hs);
+        else mstm_crichankel(nl, z, xi, hs);
         for (int k = 0; k <= nl; k++) xi[k] = cdiv(xi[k], z);
     }
 }
@@ -233,7 +234,8 @@ __global__ void __launch_bounds__(128) opgen_rot_kernel(OpGenArgs a)
     }
 }
 
-// axial translation blocks (itype 3, outgoing), one CTA per pair: the
+// axial translation blocks (itype 3, outgoing; itype 1, regular, with the
+// Bessel functions in the scratch), one CTA per pair: the
 // pair's xi_w / z staged in shared memory, thread t takes the mode-0
 // elements t, t + 128, ... of the concatenated blocks Z_0, Z_1, ...
 __global__ void __launch_bounds__(128) opgen_axial_kernel(OpGenArgs a)

@@ -14,8 +14,12 @@
 // (qeps>0 convergence test; qeps<0 forces ceiling(-qeps)); mode 1: write the
 // 2x2 LR-basis matrices anp(2,2,n) and their inverses for the given order.
 // ---------------------------------------------------------------------------
+// With dnp (mode 1) also the coefficients of a host sphere: D, U, V of
+// (a, f) = [[A, U], [D, V]] (g, b), b the exciting field inside the sphere and
+// f the regular field there (mieoa's dnp_mie, unp_mie, vnp_mie,
+// modules:5495-5528).
 __device__ void mie_one(double x, zd ri, zd rimed, double qeps, int mode, int* nodr_io, zd* anp, zd* anpinv,
-                        double* qext_o, double* qabs_o)
+                        double* qext_o, double* qabs_o, zd* dnp = nullptr, zd* unp = nullptr, zd* vnp = nullptr)
 {
     int nstop;
     if (mode == 0) {
@@ -64,6 +68,31 @@ __device__ void mie_one(double x, zd ri, zd rimed, double qeps, int mode, int* n
             for (int k = 0; k < 4; k++) anp[4 * (n - 1) + k] = am[k];
             mstm_inv22(am, anpinv + 4 * (n - 1));
         }
+        if (mode == 1 && dnp) {
+            const zd xipn0 = cdiv(xi[0][n - 1], xi[0][n]) - cdivr((double)n, xri[0]);
+            zd bm[4], um[4], dm[4], vm[4];
+            for (int s = 1; s <= 2; s++) {
+                double ss = pm1(s);
+                for (int t = 1; t <= 2; t++) {
+                    double st = pm1(t);
+                    const int k = (s - 1) + 2 * (t - 1);
+                    const zd pb = cdiv(ss * ribulk[1] + st * ribulk[0], rii[0] * rii[1]);
+                    um[k] = cdiv((ss + st) * ribulk[1], rii[1] * rii[1]) * cdiv(mk(0.0, 1.0), psi[1][n]);
+                    dm[k] = -(cdiv((ss + st) * ribulk[0], rii[0] * rii[0]) * cdiv(mk(0.0, 1.0), xi[0][n]));
+                    bm[k] = pb * (xipn0 * psi[1][n] - (ss * st) * psip[1]);
+                    vm[k] = pb * (xipn0 * xi[1][n] - (ss * st) * xip[1]);
+                }
+            }
+            zd binv[4];
+            mstm_inv22(bm, binv);
+            for (int r = 0; r < 2; r++)
+                for (int c = 0; c < 2; c++) {
+                    const int k = r + 2 * c;
+                    unp[4 * (n - 1) + k] = -(ginv[r] * um[2 * c] + ginv[r + 2] * um[1 + 2 * c]);
+                    dnp[4 * (n - 1) + k] = -(binv[r] * dm[2 * c] + binv[r + 2] * dm[1 + 2 * c]);
+                    vnp[4 * (n - 1) + k] = -(binv[r] * vm[2 * c] + binv[r + 2] * vm[1 + 2 * c]);
+                }
+        }
         qext1[n] = 0.0;
         double fn1 = n + n + 1;
         for (int p = 1; p <= 2; p++) {
@@ -95,40 +124,54 @@ __device__ void mie_one(double x, zd ri, zd rimed, double qeps, int mode, int* n
     if (qabs_o) *qabs_o = qext - qsca;
 }
 
-__global__ void mie_order_kernel(int n, const double* radius, const double* ri, double rimed_re, double rimed_im, double qeps,
-                                 int* order)
+// rext (per sphere re, im; may be null): the index around each sphere, else
+// the medium's
+__device__ __forceinline__ zd exterior(const double* rext, int i, double mre, double mim)
+{
+    return rext ? mk(rext[2 * i], rext[2 * i + 1]) : mk(mre, mim);
+}
+
+__global__ void mie_order_kernel(int n, const double* radius, const double* ri, double rimed_re, double rimed_im, const double* rext,
+                                 double qeps, int* order)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int nodr = 0;
-    mie_one(radius[i], mk(ri[2 * i], ri[2 * i + 1]), mk(rimed_re, rimed_im), qeps, 0, &nodr, nullptr, nullptr, nullptr, nullptr);
+    mie_one(radius[i], mk(ri[2 * i], ri[2 * i + 1]), exterior(rext, i, rimed_re, rimed_im), qeps, 0, &nodr, nullptr, nullptr, nullptr,
+            nullptr);
     order[i] = nodr;
 }
 
-__global__ void mie_coef_kernel(int n, const double* radius, const double* ri, double rimed_re, double rimed_im, const int* order,
-                                const int* mie_offset, zd* an, zd* an_inv, float* an32, double* qext, double* qabs)
+// hoff (may be null): spheres with hoff[i] >= 0 hold others and also get D, U, V
+__global__ void mie_coef_kernel(int n, const double* radius, const double* ri, double rimed_re, double rimed_im, const double* rext,
+                                const int* order, const int* mie_offset, const int* hoff, zd* an, zd* an_inv, float* an32, zd* dn,
+                                zd* un, zd* vn, double* qext, double* qabs)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int nodr = order[i];
-    mie_one(radius[i], mk(ri[2 * i], ri[2 * i + 1]), mk(rimed_re, rimed_im), 0.0, 1, &nodr, an + mie_offset[i],
-            an_inv + mie_offset[i], &qext[i], &qabs[i]);
+    const int mo = mie_offset[i];
+    const bool h = hoff && hoff[i] >= 0;
+    mie_one(radius[i], mk(ri[2 * i], ri[2 * i + 1]), exterior(rext, i, rimed_re, rimed_im), 0.0, 1, &nodr, an + mo, an_inv + mo, &qext[i],
+            &qabs[i], h ? dn + mo : nullptr, h ? un + mo : nullptr, h ? vn + mo : nullptr);
     for (int k = 0; k < 4 * order[i]; k++) {
-        an32[2 * (mie_offset[i] + k)] = (float)an[mie_offset[i] + k].x;
-        an32[2 * (mie_offset[i] + k) + 1] = (float)an[mie_offset[i] + k].y;
+        an32[2 * (mo + k)] = (float)an[mo + k].x;
+        an32[2 * (mo + k) + 1] = (float)an[mo + k].y;
     }
 }
 
-void launch_mie_orders(int n, const double* radius, const double* ri, double mre, double mim, double qeps, int* order,
+void launch_mie_orders(int n, const double* radius, const double* ri, double mre, double mim, const double* rext, double qeps, int* order,
                        cudaStream_t st)
 {
-    mie_order_kernel<<<(n + 63) / 64, 64, 0, st>>>(n, radius, ri, mre, mim, qeps, order);
+    mie_order_kernel<<<(n + 63) / 64, 64, 0, st>>>(n, radius, ri, mre, mim, rext, qeps, order);
     launch_counter() += 1;
 }
-void launch_mie_coefs(int n, const double* radius, const double* ri, double mre, double mim, const int* order,
-                      const int* mie_offset, zd* an, zd* an_inv, float* an32, double* qext, double* qabs, cudaStream_t st)
+void launch_mie_coefs(int n, const double* radius, const double* ri, double mre, double mim, const double* rext, const int* order,
+                      const int* mie_offset, const int* hoff, zd* an, zd* an_inv, float* an32, zd* dn, zd* un, zd* vn, double* qext,
+                      double* qabs, cudaStream_t st)
 {
-    mie_coef_kernel<<<(n + 63) / 64, 64, 0, st>>>(n, radius, ri, mre, mim, order, mie_offset, an, an_inv, an32, qext, qabs);
+    mie_coef_kernel<<<(n + 63) / 64, 64, 0, st>>>(n, radius, ri, mre, mim, rext, order, mie_offset, hoff, an, an_inv, an32, dn, un, vn,
+                                                  qext, qabs);
     launch_counter() += 1;
 }
 
@@ -233,8 +276,12 @@ __global__ void planewave_common_kernel(double alpha, zd cb, int nodr, zd* pw0, 
 #undef DC
 }
 
+// outside (may be null): 1 for the spheres outside every other; the others,
+// and the blocks of the fields inside host spheres (sphere indices >= nreal),
+// get no incident wave (sphereplanewavecoef, scatprops:268)
 __global__ void planewave_phase_kernel(int nslots2, const int* slot_sphere, const int* order, const int* offset, const double* pos,
-                                       int lmax, const zd* pw0, zd cbinc, zd riinc, double sinc, double alpha, zd* pmnp, int ld)
+                                       int lmax, const zd* pw0, zd cbinc, zd riinc, double sinc, double alpha, zd* pmnp, int ld,
+                                       int nreal, const int* outside)
 {
     // nslots2 = neqns: every coefficient of every sphere block (both modes)
     int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -242,6 +289,10 @@ __global__ void planewave_phase_kernel(int nslots2, const int* slot_sphere, cons
     int half = e;  // index in the full vector
     // locate sphere via slot_sphere over the first-mode half of each block
     int i = slot_sphere[e];
+    if (outside && (i >= nreal || !outside[i])) {
+        for (int k = 0; k < 2; k++) pmnp[(size_t)k * ld + e] = mk(0.0, 0.0);
+        return;
+    }
     int L = order[i], off = offset[i];
     int loc = half - off;
     int hb = L * (L + 2);
@@ -257,14 +308,14 @@ __global__ void planewave_phase_kernel(int nslots2, const int* slot_sphere, cons
 }
 
 void launch_planewave(double alpha, double sinc, int dir, int lmax, int neqns, const int* slot_full, const int* order,
-                      const int* offset, const double* pos, zd* pw0, zd* drot, zd* pmnp, cudaStream_t st)
+                      const int* offset, const double* pos, zd* pw0, zd* drot, zd* pmnp, cudaStream_t st, int nreal, const int* outside)
 {
     zd riinc = mk(1.0, 0.0);
     zd a = cdiv(mk(sinc, 0.0), riinc);
     zd cbinc = csqrtd((mk(1.0, 0.0) - a) * (mk(1.0, 0.0) + a)) * (double)(3 - 2 * dir);
     planewave_common_kernel<<<1, 32, 0, st>>>(alpha, cbinc, lmax, pw0, drot);
     planewave_phase_kernel<<<(neqns + 255) / 256, 256, 0, st>>>(neqns, slot_full, order, offset, pos, lmax, pw0, cbinc, riinc,
-                                                                 sinc, alpha, pmnp, neqns);
+                                                                 sinc, alpha, pmnp, neqns, nreal, outside);
     launch_counter() += 2;
 }
 
@@ -312,18 +363,87 @@ template void launch_mie<double>(int, const int*, const int*, const int*, const 
 template void launch_mie<float>(int, const int*, const int*, const int*, const int*, const zf*, int, int, const zf*, zf*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
+// Mie multiply with host spheres (multmiecoeffmult with its host branch,
+// modules:5633-5751).  A sphere that holds others has a second block at
+// hoff[i], the regular field inside it; with g its exciting field outside
+// and b inside:  idir=1  a = A g + U b,  f = D g + V b;
+//               idir!=1 a = A^T g + D^T b,  f = U^T g + V^T b.
+// One thread per (m,n) slot of a sphere's first mode half; the slots of the
+// internal blocks (slot sphere >= nreal) are done by their host's thread.
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ void m22(const cpx<T>* X, bool tr, cpx<T> v0, cpx<T> v1, cpx<T>& o0, cpx<T>& o1)
+{
+    if (!tr) {
+        o0 = o0 + X[0] * v0 + X[2] * v1;
+        o1 = o1 + X[1] * v0 + X[3] * v1;
+    } else {
+        o0 = o0 + X[0] * v0 + X[1] * v1;
+        o1 = o1 + X[2] * v0 + X[3] * v1;
+    }
+}
+
+__global__ void hmie_kernel(int nslots, int nreal, const int* slot_sphere, const int* order, const int* offset, const int* mie_offset,
+                            const int* hoff, const zd* an, const zd* dn, const zd* un, const zd* vn, int idir, int conj_in, const zd* x,
+                            zd* y)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nslots) return;
+    int i = slot_sphere[e];
+    if (i >= nreal) return;
+    int L = order[i];
+    int hb = L * (L + 2);
+    int loc = e - offset[i] / 2;
+    int row = loc % (L + 2), col = loc / (L + 2) + 1;
+    int n = (row <= col) ? col : row - 1;
+    int base = offset[i] + loc;
+    zd g0 = x[base], g1 = x[base + hb];
+    if (conj_in) { g0 = cj(g0); g1 = cj(g1); }
+    const int q = mie_offset[i] + 4 * (n - 1);
+    const bool tr = idir != 1;
+    zd a0 = mk(0.0, 0.0), a1 = mk(0.0, 0.0);
+    m22<double>(an + q, tr, g0, g1, a0, a1);
+    if (hoff[i] < 0) {
+        y[base] = a0;
+        y[base + hb] = a1;
+        return;
+    }
+    const int bb = hoff[i] + loc;
+    zd b0 = x[bb], b1 = x[bb + hb];
+    if (conj_in) { b0 = cj(b0); b1 = cj(b1); }
+    zd f0 = mk(0.0, 0.0), f1 = mk(0.0, 0.0);
+    m22<double>((tr ? dn : un) + q, tr, b0, b1, a0, a1);
+    m22<double>((tr ? un : dn) + q, tr, g0, g1, f0, f1);
+    m22<double>(vn + q, tr, b0, b1, f0, f1);
+    y[base] = a0;
+    y[base + hb] = a1;
+    y[bb] = f0;
+    y[bb + hb] = f1;
+}
+
+void launch_hmie(int nslots, int nreal, const int* slot_sphere, const int* order, const int* offset, const int* mie_offset, const int* hoff,
+                 const zd* an, const zd* dn, const zd* un, const zd* vn, int idir, int conj_in, const zd* x, zd* y, cudaStream_t st)
+{
+    hmie_kernel<<<(nslots + 255) / 256, 256, 0, st>>>(nslots, nreal, slot_sphere, order, offset, mie_offset, hoff, an, dn, un, vn, idir,
+                                                      conj_in, x, y);
+    launch_counter() += 1;
+}
+
+// ---------------------------------------------------------------------------
 // Efficiencies: lrsphereqeff (scatprops:676-776) per sphere, npol=2, with
 // g = A^{-1} a (qefficiencyfactors, scatprops:782-870, no host spheres).
 // qeff(3,3,N): qeff[q + 3*(pol + 3*i)].
 // ---------------------------------------------------------------------------
+// With host spheres (gmnp given) the exciting field is the interaction
+// without the Mie multiply plus the incident field, and each sphere sits in
+// the index rext around it (qefficiencyfactors, scatprops:807-840).
 __global__ void qeff_kernel(int nsph, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed,
-                            const zd* an_inv, const zd* amnp, const zd* pmnp0, int ld, double* qeff)
+                            const zd* an_inv, const zd* amnp, const zd* pmnp0, int ld, double* qeff, const double* rext, const zd* gmnp)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nsph) return;
     int L = order[i], off = offset[i];
     double xsp = radius[i];
-    zd ri0 = rimed;
+    zd ri0 = rext ? mk(rext[2 * i], rext[2 * i + 1]) : rimed;
     zd xri = xsp * ri0;
     zd rib = cdivr(2.0, cdivr(1.0, ri0) + cdivr(1.0, ri0));
     zd psi[MIE_NMAX], xi[MIE_NMAX], scr[2 * MIE_NMAX];
@@ -355,9 +475,14 @@ __global__ void qeff_kernel(int nsph, const int* order, const int* offset, const
                 zd x0 = amnp[(size_t)pol * ld + off + a0], x1 = amnp[(size_t)pol * ld + off + a0 + hb];
                 av[pol][0] = x0;
                 av[pol][1] = x1;
-                // onemiecoeffmult with the inverse: g(p) = sum_q Ainv(p,q) a(q)
-                gv[pol][0] = Ain[0] * x0 + Ain[2] * x1;
-                gv[pol][1] = Ain[1] * x0 + Ain[3] * x1;
+                if (gmnp) {
+                    gv[pol][0] = gmnp[(size_t)pol * ld + off + a0];
+                    gv[pol][1] = gmnp[(size_t)pol * ld + off + a0 + hb];
+                } else {
+                    // onemiecoeffmult with the inverse: g(p) = sum_q Ainv(p,q) a(q)
+                    gv[pol][0] = Ain[0] * x0 + Ain[2] * x1;
+                    gv[pol][1] = Ain[1] * x0 + Ain[3] * x1;
+                }
                 fv[pol][0] = pmnp0[(size_t)pol * ld + off + a0];
                 fv[pol][1] = pmnp0[(size_t)pol * ld + off + a0 + hb];
             }
@@ -442,10 +567,56 @@ void launch_qtot_configs(int nc, const int* cfg_start, const double* radius, con
     launch_counter() += 1;
 }
 
-void launch_qeff(int nsph, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed, const zd* an_inv,
-                 const zd* amnp, const zd* pmnp0, int ld, double* qeff, double xg, double* qtot, cudaStream_t st)
+// qtotcalc (scatprops:872-912) with host spheres, one block: each host's
+// absorption net of the spheres it holds (qabsvol), then theirs added back,
+// both scaled by the area ratio, written into qeff's absorption rows as the
+// reference does; the totals over the spheres outside every other.
+// qv: scratch of 3 nsph doubles.
+__global__ void __launch_bounds__(QTOT_NT) qtot_hosts_kernel(int nsph, const double* radius, const int* host, double* qeff, double* qv,
+                                                             double xg, double* qtot)
 {
-    qeff_kernel<<<(nsph + 63) / 64, 64, 0, st>>>(nsph, order, offset, mie_offset, radius, rimed, an_inv, amnp, pmnp0, ld, qeff);
-    qtot_kernel<<<1, QTOT_NT, 0, st>>>(nsph, radius, qeff, xg, qtot);
+    __shared__ double red[9][QTOT_NT];
+    for (int i = threadIdx.x; i < nsph; i += QTOT_NT)
+        for (int p = 0; p < 3; p++) {
+            double v = qeff[1 + 3 * (p + 3 * i)];
+            for (int j = 0; j < nsph; j++)
+                if (host[j] == i) v = v - qeff[1 + 3 * (p + 3 * j)] * radius[j] * radius[j] / (radius[i] * radius[i]);
+            qv[p + 3 * i] = v;
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsph; i += QTOT_NT)
+        for (int p = 0; p < 3; p++) {
+            double v = qv[p + 3 * i];
+            for (int j = 0; j < nsph; j++)
+                if (host[j] == i) v = v + qv[p + 3 * j] * radius[j] * radius[j] / (radius[i] * radius[i]);
+            qeff[1 + 3 * (p + 3 * i)] = v;
+        }
+    __syncthreads();
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < nsph; i += QTOT_NT)
+        if (host[i] < 0)
+            for (int k = 0; k < 9; k++) s[k] = s[k] + qeff[k + 9 * i] * radius[i] * radius[i] / (xg * xg);
+    for (int k = 0; k < 9; k++) red[k][threadIdx.x] = s[k];
+    __syncthreads();
+    for (int w = QTOT_NT / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 9; k++) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double t[9];
+        for (int k = 0; k < 9; k++) t[k] = red[k][0];
+        for (int pol = 0; pol < 3; pol++) t[2 + 3 * pol] = t[0 + 3 * pol] + t[2 + 3 * pol] - t[1 + 3 * pol];
+        for (int k = 0; k < 9; k++) qtot[k] = t[k];
+    }
+}
+
+void launch_qeff(int nsph, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed, const zd* an_inv,
+                 const zd* amnp, const zd* pmnp0, int ld, double* qeff, double xg, double* qtot, cudaStream_t st, const double* rext,
+                 const zd* gmnp, const int* host, double* qv)
+{
+    qeff_kernel<<<(nsph + 63) / 64, 64, 0, st>>>(nsph, order, offset, mie_offset, radius, rimed, an_inv, amnp, pmnp0, ld, qeff, rext, gmnp);
+    if (host) qtot_hosts_kernel<<<1, QTOT_NT, 0, st>>>(nsph, radius, host, qeff, qv, xg, qtot);
+    else qtot_kernel<<<1, QTOT_NT, 0, st>>>(nsph, radius, qeff, xg, qtot);
     launch_counter() += 2;
 }

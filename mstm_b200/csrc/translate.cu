@@ -300,6 +300,37 @@ template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cuda
     launch_counter() += 1;
 }
 
+// Coincident centres of a host and a sphere it holds (coefficient_translation's
+// zero_translation with vswf_type 1, mtransfer, modules:2334-2344): the
+// regular translation is the identity on the common orders, in both
+// directions and whatever the shift.  One CTA per (pair, column).
+__global__ void mtransfer_kernel(int npairs, const int2* pairs, const int* order, const int* offset, const zd* x, zd* y, int ld)
+{
+    const int q = blockIdx.x, r = blockIdx.y;
+    if (q >= npairs) return;
+    const int i = pairs[q].x, j = pairs[q].y;
+    const int Li = order[i], Lj = order[j], L = Li < Lj ? Li : Lj;
+    const int nb = L * (L + 2);
+    const zd* xr = x + (size_t)r * ld;
+    zd* yr = y + (size_t)r * ld;
+    for (int e = threadIdx.x; e < 2 * nb; e += blockDim.x) {
+        const int p = e / nb, k = e - p * nb;
+        const int n = (int)sqrt((double)(k + 1) + 0.5), m = k + 1 - n * n - n;   // k + 1 = n(n+1) + m
+        const int ai = offset[i] + aidx(m, n, p, Li), aj = offset[j] + aidx(m, n, p, Lj);
+        atomicAdd(&yr[ai].x, xr[aj].x);
+        atomicAdd(&yr[ai].y, xr[aj].y);
+        atomicAdd(&yr[aj].x, xr[ai].x);
+        atomicAdd(&yr[aj].y, xr[ai].y);
+    }
+}
+
+void launch_mtransfer(int npairs, const int2* pairs, const int* order, const int* offset, const zd* x, zd* y, int ld, int nrhs, cudaStream_t st)
+{
+    if (npairs <= 0) return;
+    mtransfer_kernel<<<dim3(npairs, nrhs), 128, 0, st>>>(npairs, pairs, order, offset, x, y, ld);
+    launch_counter() += 1;
+}
+
 template void launch_translate<double>(const TransArgs<double>&, int, cudaStream_t);
 template void launch_translate<float>(const TransArgs<float>&, int, cudaStream_t);
 template size_t translate_smem_bytes<double>(int, int, int);

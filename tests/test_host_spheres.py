@@ -1,0 +1,234 @@
+"""Host spheres: spheres inside other spheres (findhostspheres,
+december2023/mstm-modules-33.f90:5230-5276; external_to_internal_expansion,
+:6533-6608; the host branch of multmiecoeffmult, :5690-5747).
+
+CPU: the oracle's host branch is pinned by two known answers -- a core
+concentric in a shell is the coated sphere of Aden and Kerker (written here
+from the published formulas with scipy's spherical Bessel functions), and a
+host whose index matches the medium is transparent (the spheres inside it
+scatter and absorb as the same cluster in free space) -- and by its BiCG
+against its dense solve.  GPU: the device path against the oracle on a
+cluster with two host levels, coincident and offset centres, small spheres
+on the dense path and spheres outside: host map, orders, layout, Mie
+coefficients (1e-12), sphereinteraction in every argument form (1e-12), the
+FP64 solves (same iterations, efficiencies to 1e-9) and the refusals of the
+entry points built for spheres in the medium.
+"""
+import numpy as np
+import pytest
+from scipy.special import spherical_jn, spherical_yn
+
+
+def coated_sphere(x, y, m1, m2, nmax):
+    """Qext, Qsca of a sphere of size parameter x and index m1 inside a
+    concentric shell of size parameter y and index m2 (Aden-Kerker; the
+    coefficients as Bohren and Huffman write them, section 8.1)."""
+    n = np.arange(1, nmax + 1)
+
+    def psi(z):
+        return z * spherical_jn(n, z)
+
+    def dpsi(z):
+        return spherical_jn(n, z) + z * spherical_jn(n, z, derivative=True)
+
+    def chi(z):
+        return -z * spherical_yn(n, z)
+
+    def dchi(z):
+        return -spherical_yn(n, z) - z * spherical_yn(n, z, derivative=True)
+
+    def xi(z):
+        return psi(z) - 1j * chi(z)
+
+    def dxi(z):
+        return dpsi(z) - 1j * dchi(z)
+
+    A = (m2 * psi(m2 * x) * dpsi(m1 * x) - m1 * dpsi(m2 * x) * psi(m1 * x)) / \
+        (m2 * chi(m2 * x) * dpsi(m1 * x) - m1 * dchi(m2 * x) * psi(m1 * x))
+    B = (m2 * psi(m1 * x) * dpsi(m2 * x) - m1 * psi(m2 * x) * dpsi(m1 * x)) / \
+        (m2 * dchi(m2 * x) * psi(m1 * x) - m1 * dpsi(m1 * x) * chi(m2 * x))
+    u, du = psi(m2 * y) - A * chi(m2 * y), dpsi(m2 * y) - A * dchi(m2 * y)
+    v, dv = psi(m2 * y) - B * chi(m2 * y), dpsi(m2 * y) - B * dchi(m2 * y)
+    a = (psi(y) * du - m2 * dpsi(y) * u) / (xi(y) * du - m2 * dxi(y) * u)
+    b = (m2 * psi(y) * dv - dpsi(y) * v) / (m2 * xi(y) * dv - dxi(y) * v)
+    f = 2 * n + 1
+    return 2 / y ** 2 * np.sum(f * (a + b).real), 2 / y ** 2 * np.sum(f * (np.abs(a) ** 2 + np.abs(b) ** 2))
+
+
+def host_cluster():
+    """Host A (radius 2.5) holding a concentric core, sphere F and sphere B,
+    which holds the small sphere C; outside, sphere D and the small sphere E
+    (orders below 3: dense pairs)."""
+    pos = np.array([
+        [0.0, 0.0, 0.0],     # A host
+        [0.0, 0.0, 0.0],     # core, concentric in A
+        [1.55, 0.0, 0.1],    # B, in A, holds C
+        [1.62, 0.12, 0.05],  # C, in B
+        [-0.9, 1.3, -0.4],   # F, in A
+        [4.2, 0.3, 0.6],     # D, outside
+        [-3.6, 1.1, -0.2],   # E, outside, small
+    ])
+    rad = np.array([2.5, 0.7, 0.5, 0.15, 0.45, 0.7, 0.2])
+    ri = np.array([1.33 + 0.001j, 1.6 + 0.05j, 1.5 + 0.01j, 1.7 + 0.1j, 1.45 + 0.0j, 1.55 + 0.02j, 1.4 + 0.0j])
+    return pos, rad, ri
+
+
+# ---------------------------------------------------------------------------
+# CPU: the oracle's host branch against known answers
+# ---------------------------------------------------------------------------
+def test_oracle_finds_hosts_and_raises_orders(oracle_mod):
+    pos, rad, ri = host_cluster()
+    o = oracle_mod.Oracle(pos, rad, ri, mie_eps=1e-6)
+    host, nh = o.hosts()
+    assert host.tolist() == [-1, 0, 0, 2, 0, -1, -1] and nh == 4
+    # a host's order is at least that of every sphere inside it
+    assert o.order[0] >= o.order[[1, 2, 3, 4]].max() and o.order[2] >= o.order[3]
+    # layout: the hosts' blocks are followed by their internal blocks
+    nb = 2 * o.order * (o.order + 2)
+    assert np.array_equal(np.diff(o.offset), nb * np.array([2, 1, 2, 1, 1, 1, 1]))
+    assert o.order[6] < 3
+
+
+def test_oracle_coated_sphere_is_aden_kerker(oracle_mod):
+    x, y, m1, m2 = 1.2, 2.0, 1.6 + 0.05j, 1.33 + 0.01j
+    o = oracle_mod.Oracle([[0, 0, 0], [0, 0, 0]], [y, x], [m2, m1], mie_eps=-14)
+    r = o.fixedorsoln(eps=1e-20, niter=300)
+    qe, qs = coated_sphere(x, y, m1, m2, 14)
+    # the shell's efficiencies (its absorption net of the core's, then the
+    # core's added back, as qtotcalc forms them) are the coated sphere's
+    assert abs(r["qeff"][0, 0, 0] - qe) <= 1e-9 * qe
+    assert abs((r["qeff"][0, 0, 0] - r["qeff"][1, 0, 0]) - qs) <= 1e-9 * qs
+    # qtot differs only by vol_radius's single-precision exponent
+    xg = o.vol_radius()
+    assert abs(r["qtot"][0, 0] * xg ** 2 - qe * y ** 2) <= 1e-9 * qe * y ** 2
+
+
+def test_oracle_index_matched_host_is_transparent(oracle_mod):
+    inner = np.array([[0.8, 0.0, 0.1], [-0.7, 0.3, -0.2], [0.0, -0.6, 0.7]])
+    ri_in = np.array([1.5 + 0.02j, 1.45 + 0.0j, 1.6 + 0.1j])
+    rin = np.array([0.5, 0.55, 0.45])
+    L = 14
+    free = oracle_mod.Oracle(inner, rin, ri_in, mie_eps=-L)
+    rf = free.fixedorsoln(eps=1e-20, niter=300)
+    h = oracle_mod.Oracle(np.vstack([[0, 0, 0], inner]), np.r_[2.0, rin], np.r_[1.0 + 0j, ri_in], mie_eps=-L)
+    rh = h.fixedorsoln(eps=1e-20, niter=300)
+    cf = rf["qtot"][:, 0] * free.vol_radius() ** 2
+    ch = rh["qtot"][:, 0] * h.vol_radius() ** 2
+    assert np.allclose(ch, cf, rtol=1e-7, atol=0)
+    assert np.allclose(rh["qeff"][1, 0, [1, 3]], rf["qeff"][1, 0, [0, 2]], rtol=1e-8)
+
+
+def test_oracle_host_bicg_matches_dense_solve(oracle_mod):
+    pos, rad, ri = host_cluster()
+    o = oracle_mod.Oracle(pos, rad, ri, mie_eps=1e-6)
+    b = o.planewave()
+    pnp = o.multmie(b[:, 0])
+    x, it, err, rc = o.cbicg(pnp, pnp.copy(), niter=500, eps=1e-24)
+    assert rc == 0 and err < 1e-24
+    xd = o.direct_solve(pnp)
+    assert np.abs(x - xd).max() <= 1e-9 * np.abs(xd).max()
+
+
+# ---------------------------------------------------------------------------
+# GPU: the device path against the oracle
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def pair(oracle_mod):
+    from mstm_b200 import api
+    pos, rad, ri = host_cluster()
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=1e-6, precision="fp64")
+    o = oracle_mod.Oracle(pos, rad, ri, mie_eps=1e-6, store_matrix=True, nthreads=4)
+    yield g, o
+    g.close()
+    o.close()
+
+
+@pytest.mark.gpu
+def test_host_layout_and_mie_coefficients(pair):
+    g, o = pair
+    host, nh = g.host_spheres()
+    ho, nho = o.hosts()
+    assert np.array_equal(host, ho) and nh == nho == 4
+    assert np.array_equal(g.sphere_order, o.order) and np.array_equal(g.sphere_offset, o.offset)
+    assert g.number_eqns == o.neqns
+    an_g, qe_g, qa_g = g.miecoefcalc()
+    an_o, _, qe_o, qa_o = o.mie()
+    assert np.abs(an_g - an_o).max() <= 1e-12 * np.abs(an_o).max()
+    for cg, co in zip(g.host_mie_coefficients(), o.host_mie()):
+        assert np.abs(cg - co).max() <= 1e-12 * np.abs(co).max()
+    assert np.allclose(qe_g, qe_o, rtol=1e-12)
+    assert abs(g.vol_radius - o.vol_radius()) <= 1e-14 * o.vol_radius()
+
+
+@pytest.mark.gpu
+def test_host_sphereinteraction(pair):
+    g, o = pair
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((g.number_eqns, 4)) + 1j * rng.standard_normal((g.number_eqns, 4))
+    for ct, mm in (([0, 1, 0, 1], [1, 1, 0, 0]), ([1, 0, 1, 0], [1, 0, 1, 0])):
+        yg = g.sphereinteraction(x, con_tran=ct, mie_mult=mm, initial_run=True)
+        yo = o.sphereinteraction(x, con_tran=ct, mie_mult=mm, initial_run=True)
+        assert np.abs(yg - yo).max() <= 1e-12 * np.abs(yo).max()
+    # the host couplings alone (skip_external_translation)
+    yg = g.sphereinteraction_ex(x[:, :2], con_tran=[0, 1], skip_external_translation=True)
+    yo = o.sphereinteraction(x[:, :2], con_tran=[0, 1], skip_external=True)
+    assert np.abs(yo).max() > 0
+    assert np.abs(yg - yo).max() <= 1e-12 * np.abs(yo).max()
+    # the incident wave reaches the spheres outside every other only
+    pg = g.sphereplanewavecoef()
+    po = o.planewave()
+    assert np.abs(pg - po).max() <= 1e-13 * np.abs(po).max()
+    off = o.offset
+    assert np.abs(po[off[1]:off[5]]).max() == 0.0
+
+
+@pytest.mark.gpu
+def test_host_fixedorsoln(pair):
+    g, o = pair
+    ro = o.fixedorsoln(eps=1e-12, niter=500)
+    rg = g.fixedorsoln(eps=1e-12, niter=500)
+    assert rg["istat"] == ro["status"] == 0
+    assert rg["iterations"] == ro["iterations"]
+    assert np.abs(rg["amnp"] - ro["amnp"]).max() <= 1e-8 * np.abs(ro["amnp"]).max()
+    assert np.allclose(rg["qeff"], ro["qeff"], rtol=1e-9, atol=1e-12)
+    assert np.allclose(rg["qtot"], ro["qtot"], rtol=1e-9)
+    # efficiencies of a given solution, and the right-hand sides
+    q = g.efficiencies(ro["amnp"])
+    assert np.allclose(q["qtot"], ro["qtot"], rtol=1e-10)
+    b = g.fixed_orientation_rhs()
+    po = o.planewave()
+    assert np.abs(b[:, 0] - o.multmie(po[:, 0])).max() <= 1e-12 * np.abs(b).max()
+
+
+@pytest.mark.gpu
+def test_host_solver_modes(pair):
+    """niter 0 (the host couplings applied twice, solver:509-518) and the
+    order-of-scattering iteration (niter < 0)."""
+    g, o = pair
+    for niter in (0, -60):
+        ro = o.fixedorsoln(eps=1e-10, niter=niter)
+        rg = g.fixedorsoln(eps=1e-10, niter=niter)
+        assert rg["iterations"][1] == ro["maxiter"]
+        assert np.abs(rg["amnp"] - ro["amnp"]).max() <= 1e-9 * np.abs(ro["amnp"]).max()
+        assert np.allclose(rg["qtot"], ro["qtot"], rtol=1e-9)
+
+
+@pytest.mark.gpu
+def test_host_contexts_refuse_the_medium_only_paths(pair):
+    from mstm_b200 import api
+    from mstm_b200._lib import MstmgError
+    g, _ = pair
+    pos, rad, ri = host_cluster()
+    m = api.SphereCluster(pos, rad, ri, mie_epsilon=1e-6, precision="mixed")
+    with pytest.raises(MstmgError):
+        m.fixedorsoln(eps=1e-8)
+    m.close()
+    with pytest.raises(MstmgError):
+        g.tmatrix_solution(4)
+    with pytest.raises(MstmgError):
+        g.fft_setup(d_cell=2.0)
+    with pytest.raises(MstmgError):
+        g.set_positions(pos + 0.01)
+    x = np.ones((g.number_eqns, 2), np.complex128)
+    with pytest.raises(MstmgError):
+        g.translation_pass(x, [0, 1], "fp32")
