@@ -405,6 +405,38 @@ def run_extras(args, dev, stream):
     row["qext_rel_diff"] = abs(row["mixed"]["qext"] / row["fp64"]["qext"] - 1)
     row["speedup_tensor_cores"] = round(row["mixed_rotation_kernels"]["ms"] / row["mixed"]["ms"], 2)
     out["tmatrix_cluster100"] = row
+    # host spheres: one host sphere holding 1000 inclusions, the FP64 BiCG
+    # (the solver the reference runs), against the oracle's frozen solve and
+    # the oracle itself timed on this host's cores
+    w = C.host_inclusions(1000, 0.5, 0.15, seed=7)
+    row = {"workload": "a host sphere (m=1.33, radius %.3f, the RSA bounding radius) holding 1000 inclusions (x=0.5, "
+                       "m=1.6+0.05i, RSA at fv 0.15, seed 7): fixed orientation, both polarisations to residual 1e-6, "
+                       "FP64 BiCG, orders from mie_epsilon 1e-6" % w["radius"][0],
+           "metric": "solves/s"}
+    g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=1e-6, precision="fp64")
+    _lib.check(L.mstmg_set_stream(g.ctx, ctypes.c_void_p(stream.cuda_stream)), "set_stream")
+    ms, r = timed(lambda: g.fixedorsoln(eps=EPS, niter=NITER), 3)
+    hosts, nh = g.host_spheres()
+    row["fp64"] = {"solves_per_s": round(1000.0 / ms, 3), "ms": round(ms, 2), "qext": r["qtot"][0, 0], "iterations": r["iterations"],
+                   "unknowns": g.number_eqns, "pairs_same_host": L.mstmg_npairs(g.ctx), "spheres_with_a_host": nh,
+                   "ms_per_translation_pass_2_columns": round(g.time_translation("fp64", 2, 10), 4)}
+    fx = oracle_fixture("host1000")
+    if fx is not None:
+        row["fp64"]["vs_oracle"] = {"qext": float("%.3g" % abs(r["qtot"][0, 0] / fx["qtot"][0, 0] - 1)),
+                                    "qabs": float("%.3g" % abs(r["qtot"][1, 0] / fx["qtot"][1, 0] - 1)),
+                                    "qeff_all": float("%.3g" % rel_err(r["qeff"], fx["qeff"])),
+                                    "iterations_equal": bool(list(r["iterations"]) == list(fx["iterations"]))}
+    g.close()
+    import multiprocessing
+    threads = multiprocessing.cpu_count()
+    t0 = time.time()
+    o = _oracle_for_host(w, threads)
+    ro = o.fixedorsoln(eps=EPS, niter=NITER)
+    o.close()
+    row["oracle_cpu"] = {"s": round(time.time() - t0, 2), "threads": threads, "iterations": ro["iterations"],
+                         "what": "the oracle's full FP64 solve (operators, BiCG, efficiencies) on this host's cores"}
+    row["speedup_vs_oracle_cpu"] = round(row["oracle_cpu"]["s"] * 1000.0 / ms, 1)
+    out["host_spheres1000"] = row
     # the 20-sphere cluster (the reference's CPU-sized case)
     w = C.workload("cluster20")
     row = {"workload": "20 spheres, x=1.0, m=1.5+0.01i, RSA in a sphere at fv 0.10, both polarisations",
@@ -583,6 +615,11 @@ def report_line(args, ws, R, ne):
 # ---------------------------------------------------------------------------
 # CPU: the oracle (restatement of the reference) on the host cores
 # ---------------------------------------------------------------------------
+def _oracle_for_host(w, threads):
+    from oracle import oracle as O
+    return O.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=1e-6, store_matrix=True, nthreads=threads)
+
+
 def _oracle_for(name, threads, store=True):
     from mstm_b200 import configs as C
     from oracle import oracle as O

@@ -244,6 +244,18 @@ def read_position_file(path):
 # ---------------------------------------------------------------------------
 # The named workloads (sizes and seeds fixed here so tests and bench agree).
 # ---------------------------------------------------------------------------
+def host_inclusions(n, radius, volume_fraction, seed, host_index=1.33 + 0.0j, inclusion_index=1.6 + 0.05j):
+    """A host sphere holding n equal inclusions placed by random sequential
+    addition (rsa_sphere: inclusion volume fraction `volume_fraction` of the
+    host).  Returns dict(pos, radius, ref_index) with the host first, at the
+    origin, its radius the RSA bounding radius so every inclusion lies inside."""
+    inner, R = rsa_sphere(n, radius, volume_fraction, seed)
+    pos = np.vstack([np.zeros((1, 3)), inner])
+    rad = np.r_[R, np.full(n, radius)]
+    ri = np.r_[complex(host_index), np.full(n, complex(inclusion_index))]
+    return dict(pos=pos, radius=rad, ref_index=ri.astype(np.complex128))
+
+
 def workload(name):
     """Return dict(pos, radius, ref_index, order) for a named workload."""
     if name == "cluster20":

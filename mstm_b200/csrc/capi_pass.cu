@@ -218,7 +218,7 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
     a.ld = c->neqns;
     a.nrhs = nrhs;
     a.contran = contran;
-    a.lmax = c->lmax;
+    a.lmax = c->pair_lmax;
     a.maxrec = c->maxrec;
     a.err = c->err.p;
     TiledArgs<T> ta;

@@ -321,6 +321,7 @@ struct mstmg_ctx {
     // CUDA graphs captured before hold the old pointers
     unsigned long long layout_gen = 0;
     int n = 0, neqns = 0, lmax = 0, npairs = 0, maxrec = 0;
+    int pair_lmax = 0;   // largest order among the spheres of the rotation pairs (the order-generic kernel's strides)
     long long op_units = 0;
     double xg = 1.0;
     std::vector<int> order, offset, mie_offset;

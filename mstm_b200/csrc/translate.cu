@@ -290,9 +290,14 @@ template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cuda
     constexpr int NT = 256;
     size_t smem = translate_smem_bytes<T>(a.lmax, a.nrhs, a.maxrec);
     cudaFuncSetAttribute(translate_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = (int)((220 * 1024) / (smem + 1024));
+    // as many CTAs per SM as registers and shared memory allow (small orders: up to 8)
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, translate_kernel<T, NT>, NT, smem) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
     if (per_sm < 1) per_sm = 1;
-    if (per_sm > 4) per_sm = 4;
+    if (per_sm > 8) per_sm = 8;
     int blocks = nsm * per_sm;
     if (blocks > a.npairs) blocks = a.npairs;
     if (blocks < 1) return;

@@ -19,7 +19,12 @@ cbicg, mstm-solver-8.f90:763-767, 920-924):
                    t_matrix_convergence 1e-6, then ranorientscatmatrix
                    (scatprops:1963-2592);
   ensemble_tmatrix the two smallest configurations of the 256-configuration
-                   T-matrix ensemble (50-400 spheres, seed 4), as tmatrix100.
+                   T-matrix ensemble (50-400 spheres, seed 4), as tmatrix100;
+  host1000         a host sphere (m = 1.33) holding 1000 inclusions (x = 0.5,
+                   m = 1.6+0.05i, RSA at fv 0.15, seed 7; host radius the RSA
+                   bounding radius): fixedorsoln with host spheres
+                   (findhostspheres, external_to_internal_expansion,
+                   modules:5230-5276, 6533-6608), orders from mie_epsilon 1e-6.
 
 Stored per case: efficiencies (totals and per sphere), iteration counts,
 per-sphere norms of the solution and the full blocks of a few spheres,
@@ -77,6 +82,22 @@ def fixed_case(name, pos, x, m, threads, fft=None):
     print("%s: N=%d Qext %.12f iterations %d, %.0f s" % (name, n, r["qtot"][0, 0], r["maxiter"], t1 - t0), flush=True)
 
 
+def host_case(name, w, threads):
+    from oracle import oracle as O
+    t0 = time.time()
+    o = O.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=1.0e-6, store_matrix=True, nthreads=threads)
+    r = o.fixedorsoln(eps=EPS, niter=10000)
+    t1 = time.time()
+    amnp = r["amnp"]
+    out = dict(pos=np.asarray(w["pos"]), radius=w["radius"], ref_index=w["ref_index"], mie_eps=1.0e-6, eps=EPS, order=o.order,
+               offset=o.offset, qtot=r["qtot"], qeff=r["qeff"], maxiter=r["maxiter"], iterations=np.array(r["iterations"]),
+               maxerr=r["maxerr"], status=r["status"], sphere_norms=_sphere_norms(o, amnp), amnp_head=amnp[:o.offset[KEEP_SPHERES], :],
+               solve_s=t1 - t0, threads=threads)
+    o.close()
+    np.savez_compressed(os.path.join(HERE, "oracle_%s.npz" % name), **out)
+    print("%s: N=%d Qext %.12f iterations %s, %.0f s" % (name, len(w["radius"]), r["qtot"][0, 0], r["iterations"], t1 - t0), flush=True)
+
+
 def tmatrix_case(name, pos, x, m, threads):
     from oracle import oracle as O
     from mstm_b200 import configs as C
@@ -120,6 +141,8 @@ def main():
         small = sorted(range(len(cfgs)), key=lambda k: (cfgs[k]["n"], k))[:2]
         for k in small:
             tmatrix_case("ensemble_tmatrix_c%d" % k, cfgs[k]["pos"], 1.5, 1.6 + 0.005j, a.threads)
+    if want("host1000"):
+        host_case("host1000", C.host_inclusions(1000, 0.5, 0.15, seed=7), a.threads)
     if want("cylinder_fft"):
         pos, _ = C.rsa_cylinder(5000, 1.0, 0.25, 1.0, seed=3)
         fixed_case("cylinder_fft", pos, 1.0, 1.31 + 0j, a.threads, fft=dict(d_cell=4.0))

@@ -10,7 +10,8 @@ minutes of CPU time each):
   tmatrix100     100-sphere cluster T matrix (x = 1.5, 720 columns at order 18)
                  and its orientation averages;
   ensemble_tmatrix_c*  the two smallest configurations of the 256-configuration
-                 T-matrix ensemble.
+                 T-matrix ensemble;
+  host1000       a host sphere holding 1000 inclusions (host spheres, FP64).
 Tolerances (stated per output): the FP64 drop-in path follows the reference's
 iteration, so 1e-9 relative on efficiencies, solutions and the scattering
 matrix (of its largest element); the mixed path and the tensor-core T-matrix
@@ -59,6 +60,10 @@ def test_fixtures_match_the_seeded_configurations():
     for k, cfg in _ensemble_cfgs():
         e = _load("ensemble_tmatrix_c%d" % k)
         assert np.array_equal(e["pos"], cfg["pos"]) and e["status"] == 0
+    h = _load("host1000")
+    w = C.host_inclusions(1000, 0.5, 0.15, seed=7)
+    assert np.array_equal(h["pos"], w["pos"]) and np.array_equal(h["radius"], w["radius"])
+    assert h["status"] == 0 and h["maxerr"] < 1e-12 and h["order"][0] == 12
 
 
 # ---------------------------------------------------------------------------
@@ -159,3 +164,23 @@ def test_ensemble_tmatrix_configurations_against_oracle():
         g = api.SphereCluster(cfg["pos"], np.full(n, 1.5), np.full(n, 1.6 + 0.005j), mie_epsilon=-8, precision="mixed")
         _tmatrix_check(g, f, 1e-6, 1e-6)
         g.close()
+
+
+@pytest.mark.gpu
+def test_host1000_against_oracle():
+    """Host spheres at the benchmark's size: a host holding 1000 inclusions,
+    the FP64 BiCG (same iterations as the oracle; efficiencies, per-sphere
+    solution norms and the leading solution blocks to 1e-9)."""
+    from mstm_b200 import api
+    f = _load("host1000")
+    g = api.SphereCluster(f["pos"], f["radius"], f["ref_index"], mie_epsilon=float(f["mie_eps"]), precision="fp64")
+    assert np.array_equal(g.sphere_order, f["order"]) and np.array_equal(g.sphere_offset, f["offset"])
+    r = g.fixedorsoln(eps=float(f["eps"]), niter=10000)
+    assert r["istat"] == 0 and list(r["iterations"]) == list(f["iterations"])
+    assert _rel(r["qtot"], f["qtot"]) <= 1e-9
+    assert _rel(r["qeff"], f["qeff"]) <= 1e-9
+    off = f["offset"]
+    norms = np.array([[np.linalg.norm(r["amnp"][off[i]:off[i + 1], p]) for p in range(2)] for i in range(len(off) - 1)])
+    assert _rel(norms, f["sphere_norms"]) <= 1e-9
+    assert _rel(r["amnp"][:off[4]], f["amnp_head"]) <= 1e-9
+    g.close()
