@@ -44,10 +44,16 @@ static int origin_orders(mstmg_ctx* c, const BigTablesDev& bt, double trans_eps,
                          std::vector<int>& tord, int* T)
 {
     const int n = c->n;
+    // with host spheres: over the spheres outside every other (input:1166-1197)
+    auto outside = [&](int i) { return !c->hs.on() || c->hs.host[i] < 0; };
     r0[0] = r0[1] = r0[2] = 0.0;
+    int nout = 0;
     for (int i = 0; i < n; i++)
-        for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->hpos[3 * (size_t)i + k];
-    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)n;
+        if (outside(i)) {
+            nout++;
+            for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->hpos[3 * (size_t)i + k];
+        }
+    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)nout;
     DevBuf<zd> tscr;
     const int sstride = 3 * (200 + MSTMG_LMAX + 4);
     CK(dtord.alloc(n));
@@ -58,7 +64,8 @@ static int origin_orders(mstmg_ctx* c, const BigTablesDev& bt, double trans_eps,
     CK(cudaMemcpyAsync(tord.data(), dtord.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     int t = std::min(c->lmax, max_t_order);
-    for (int i = 0; i < n; i++) t = std::max(t, tord[i]);
+    for (int i = 0; i < n; i++)
+        if (outside(i)) t = std::max(t, tord[i]);
     if (t > 200) {
         set_err("t_matrix_order above 200 is not supported");
         return MSTMG_ERR_UNSUPPORTED;
@@ -148,6 +155,7 @@ static MergeArgs merge_args(mstmg_ctx* c, const RegTables& rt, const BigTablesDe
     ma.fcN = rt.FN;
     ma.fnr = bt.fnr.p;
     ma.bcofd = rt.bcd.p;
+    ma.active = c->hs.on() ? c->hs.d_outside.p : nullptr;
     return ma;
 }
 
@@ -155,7 +163,6 @@ extern "C" int mstmg_scattering(mstmg_ctx* c, const double* amnp, double trans_e
                                 double* g, int* t_matrix_order, double* amnp0, int amnp0_cap)
 {
     if (int rc0 = reject_ensemble(c, "mstmg_scattering")) return rc0;
-    if (int rh = reject_hosts(c, "mstmg_scattering")) return rh;
     NvtxRange nvtx_("mstmg_scattering");
     if (!c || !amnp || nangles < 2 || max_t_order < 1) {
         set_err("mstmg_scattering: bad arguments");

@@ -2229,12 +2229,19 @@ int orc_tranordertest(double r, double ri_re, int lmax, double eps)
  * tranordertest with translation_epsilon, capped at max_t_matrix_order. */
 int orc_t_matrix_order(const orc_ctx *c, double trans_eps, int maxt, double *origin, int *trans_order)
 {
+    /* the cluster origin and the translation orders over the spheres outside
+     * every other (input:1166-1197); a held sphere keeps its own order */
     double r0[3] = {0, 0, 0};
-    for (int i = 0; i < c->n; i++)
+    int nout = 0;
+    for (int i = 0; i < c->n; i++) {
+        if (c->host[i] >= 0) continue;
+        nout++;
         for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->pos[3 * i + k];
-    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)c->n;
+    }
+    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)nout;
     int tmo = imin(c->max_order, maxt);
     for (int i = 0; i < c->n; i++) {
+        if (c->host[i] >= 0) { trans_order[i] = c->order[i]; continue; }
         double d2 = 0.0;
         for (int k = 0; k < 3; k++) d2 += (c->pos[3 * i + k] - r0[k]) * (c->pos[3 * i + k] - r0[k]);
         int to = orc_tranordertest(sqrt(d2), creal(c->rimed), c->order[i], trans_eps);
@@ -2256,6 +2263,7 @@ void orc_merge_to_common_origin(const orc_ctx *c, int nodrt, const cplx *amnp, c
     for (int k = 0; k < nb0; k++) amnp0[k] = 0;
     axialtrancoefinit(imax(nodrt, c->max_order));
     for (int i = 0; i < c->n; i++) {
+        if (c->host[i] >= 0) continue;   /* origin_host 0: the spheres outside every other (scatprops:631) */
         int noi = c->order[i];
         int ntrani = imin(nodrt, trans_order[i]);
         int nbt = 2 * ntrani * (ntrani + 2);

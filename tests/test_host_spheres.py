@@ -6,13 +6,15 @@ CPU: the oracle's host branch is pinned by two known answers -- a core
 concentric in a shell is the coated sphere of Aden and Kerker (written here
 from the published formulas with scipy's spherical Bessel functions), and a
 host whose index matches the medium is transparent (the spheres inside it
-scatter and absorb as the same cluster in free space) -- and by its BiCG
+scatter and absorb as the same cluster in free space, with the same
+scattering matrix) -- and by its BiCG
 against its dense solve.  GPU: the device path against the oracle on a
 cluster with two host levels, coincident and offset centres, small spheres
 on the dense path and spheres outside: host map, orders, layout, Mie
 coefficients (1e-12), sphereinteraction in every argument form (1e-12), the
-FP64 solves (same iterations, efficiencies to 1e-9) and the refusals of the
-entry points built for spheres in the medium.
+FP64 solves (same iterations, efficiencies to 1e-9), the scattering matrix
+(1e-9 of S11's largest value) and the refusals of the entry points built for
+spheres in the medium.
 """
 import numpy as np
 import pytest
@@ -116,6 +118,11 @@ def test_oracle_index_matched_host_is_transparent(oracle_mod):
     ch = rh["qtot"][:, 0] * h.vol_radius() ** 2
     assert np.allclose(ch, cf, rtol=1e-7, atol=0)
     assert np.allclose(rh["qeff"][1, 0, [1, 3]], rf["qeff"][1, 0, [0, 2]], rtol=1e-8)
+    # the far field too: merged about the host's centre (the one sphere
+    # outside) against the free cluster merged about its own centroid
+    sf, sh = free.scattering(rf["amnp"]), h.scattering(rh["amnp"])
+    assert np.abs(sh["smat"] - sf["smat"]).max() <= 1e-7 * np.abs(sf["smat"][:, 0, 0]).max()
+    assert abs(sh["g"] - sf["g"]) <= 1e-7 * abs(sf["g"])
 
 
 def test_oracle_host_bicg_matches_dense_solve(oracle_mod):
@@ -198,6 +205,21 @@ def test_host_fixedorsoln(pair):
     b = g.fixed_orientation_rhs()
     po = o.planewave()
     assert np.abs(b[:, 0] - o.multmie(po[:, 0])).max() <= 1e-12 * np.abs(b).max()
+
+
+@pytest.mark.gpu
+def test_host_scattering_matrix(pair):
+    """The scattering matrix and g of a host cluster: the spheres outside
+    every other merged about their centroid (merge_to_common_origin with
+    origin_host 0, scatprops:631)."""
+    g, o = pair
+    ro = o.fixedorsoln(eps=1e-12, niter=500)
+    so = o.scattering(ro["amnp"])
+    sg = g.scattering(ro["amnp"])
+    assert sg["t_matrix_order"] == so["t_matrix_order"]
+    assert np.abs(sg["amnp0"] - so["amnp0"]).max() <= 1e-10 * np.abs(so["amnp0"]).max()
+    assert np.abs(sg["smat"] - so["smat"]).max() <= 1e-9 * np.abs(so["smat"][:, 0, 0]).max()
+    assert abs(sg["g"] - so["g"]) <= 1e-9 * abs(so["g"])
 
 
 @pytest.mark.gpu
