@@ -58,11 +58,13 @@ template <typename T> __device__ __forceinline__ void atomic_add_c(cpx<T>* p, cp
 
 template <typename T> __device__ __forceinline__ cpx<T> ldc(const cpx<T>* p) { return *p; }
 
-template <typename T, int NT> __global__ void __launch_bounds__(NT) translate_kernel(TransArgs<T> a)
+// LM: the largest order among the launch's pairs, a compile-time constant so
+// that the index decodes of every phase are multiplications, not divisions
+template <typename T, int NT, int LM> __global__ void __launch_bounds__(NT) translate_kernel(TransArgs<T> a)
 {
     extern __shared__ __align__(128) unsigned char sm[];
     const int tid = threadIdx.x;
-    const int lm = a.lmax;
+    constexpr int lm = LM;
     const int nrhs = a.nrhs;
     const int NI = 2 * nrhs;
     uint64_t* bar = (uint64_t*)sm;                              // 2 barriers
@@ -285,24 +287,49 @@ template <typename T> size_t translate_smem_bytes(int lmax, int nrhs, int maxrec
     return head + ops + bufs;
 }
 
-template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cudaStream_t st)
+template <typename T, int NT, int LM> static void launch_translate_lm(const TransArgs<T>& a, int nsm, cudaStream_t st)
 {
-    constexpr int NT = 256;
-    size_t smem = translate_smem_bytes<T>(a.lmax, a.nrhs, a.maxrec);
-    cudaFuncSetAttribute(translate_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    // as many CTAs per SM as registers and shared memory allow (small orders: up to 8)
+    size_t smem = translate_smem_bytes<T>(LM, a.nrhs, a.maxrec);
+    auto kern = translate_kernel<T, NT, LM>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // as many CTAs per SM as registers and shared memory allow
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, translate_kernel<T, NT>, NT, smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem) != cudaSuccess) {
         cudaGetLastError();
         per_sm = 1;
     }
     if (per_sm < 1) per_sm = 1;
-    if (per_sm > 8) per_sm = 8;
+    if (per_sm > 32) per_sm = 32;
     int blocks = nsm * per_sm;
     if (blocks > a.npairs) blocks = a.npairs;
     if (blocks < 1) return;
-    translate_kernel<T, NT><<<blocks, NT, smem, st>>>(a);
+    kern<<<blocks, NT, smem, st>>>(a);
     launch_counter() += 1;
+}
+
+// Pairs of small orders leave most of a 256-thread CTA idle in every phase:
+// two-warp CTAs up to order 6.  a.lmax (1 .. MSTMG_LMAX) picks the instance.
+template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cudaStream_t st)
+{
+    static_assert(MSTMG_LMAX == 16, "one instance per order up to MSTMG_LMAX");
+    switch (a.lmax) {
+    case 1: launch_translate_lm<T, 64, 1>(a, nsm, st); break;
+    case 2: launch_translate_lm<T, 64, 2>(a, nsm, st); break;
+    case 3: launch_translate_lm<T, 64, 3>(a, nsm, st); break;
+    case 4: launch_translate_lm<T, 64, 4>(a, nsm, st); break;
+    case 5: launch_translate_lm<T, 64, 5>(a, nsm, st); break;
+    case 6: launch_translate_lm<T, 64, 6>(a, nsm, st); break;
+    case 7: launch_translate_lm<T, 256, 7>(a, nsm, st); break;
+    case 8: launch_translate_lm<T, 256, 8>(a, nsm, st); break;
+    case 9: launch_translate_lm<T, 256, 9>(a, nsm, st); break;
+    case 10: launch_translate_lm<T, 256, 10>(a, nsm, st); break;
+    case 11: launch_translate_lm<T, 256, 11>(a, nsm, st); break;
+    case 12: launch_translate_lm<T, 256, 12>(a, nsm, st); break;
+    case 13: launch_translate_lm<T, 256, 13>(a, nsm, st); break;
+    case 14: launch_translate_lm<T, 256, 14>(a, nsm, st); break;
+    case 15: launch_translate_lm<T, 256, 15>(a, nsm, st); break;
+    default: launch_translate_lm<T, 256, 16>(a, nsm, st); break;
+    }
 }
 
 // Coincident centres of a host and a sphere it holds (coefficient_translation's
