@@ -80,6 +80,23 @@ int reject_hosts(const mstmg_ctx* c, const char* fn)
     return MSTMG_OK;
 }
 
+// Whether any sphere's centre lies inside a larger sphere (of the same
+// configuration), for positions pos (host memory, 3 per sphere).
+static bool any_host(const mstmg_ctx* c, const double* pos)
+{
+    const int n = c->n;
+    if (std::all_of(c->radius.begin(), c->radius.end(), [&](double r) { return r == c->radius[0]; })) return false;   // equal spheres
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+            if (!(c->radius[j] > c->radius[i])) continue;
+            if (!c->cfg_of.empty() && c->cfg_of[j] != c->cfg_of[i]) continue;
+            const double d0 = pos[3 * (size_t)j] - pos[3 * (size_t)i], d1 = pos[3 * (size_t)j + 1] - pos[3 * (size_t)i + 1],
+                         d2 = pos[3 * (size_t)j + 2] - pos[3 * (size_t)i + 2];
+            if (d0 * d0 + d1 * d1 + d2 * d2 <= c->radius[j] * c->radius[j]) return true;
+        }
+    return false;
+}
+
 // findhostspheres (modules:5230-5276): the holder of sphere i is the
 // smallest larger sphere whose surface encloses i's centre (the first in
 // order among equal radii); exteriorrefindex (modules:5408-5419) gives the
@@ -767,6 +784,20 @@ extern "C" int mstmg_ctx_set_positions(mstmg_ctx* c, const double* pos)
                 set_err("mstmg_ctx_set_positions: non-finite position of sphere " + std::to_string(k / 3 + 1));
                 return MSTMG_ERR_ARG;
             }
+    {
+        // spheres moved inside others would need the host-sphere layout: a new context
+        std::vector<double> hp;
+        const double* p = pos;
+        if (is_dev(pos)) {
+            hp.resize(3 * (size_t)c->n);
+            CK(cudaMemcpy(hp.data(), pos, sizeof(double) * 3 * c->n, cudaMemcpyDeviceToHost));
+            p = hp.data();
+        }
+        if (any_host(c, p)) {
+            set_err("mstmg_ctx_set_positions: a sphere's centre would lie inside another sphere (host spheres): create a new context");
+            return MSTMG_ERR_UNSUPPORTED;
+        }
+    }
     CK(copy_in(c->pos.p, pos, sizeof(double) * 3 * c->n, c->st));
     if (is_dev(pos)) CK(cudaMemcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n, cudaMemcpyDeviceToHost));
     else memcpy(c->hpos.data(), pos, sizeof(double) * 3 * c->n);

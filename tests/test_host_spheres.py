@@ -254,3 +254,19 @@ def test_host_contexts_refuse_the_medium_only_paths(pair):
     x = np.ones((g.number_eqns, 2), np.complex128)
     with pytest.raises(MstmgError):
         g.translation_pass(x, [0, 1], "fp32")
+
+
+@pytest.mark.gpu
+def test_moving_a_sphere_inside_another_needs_a_new_context():
+    from mstm_b200 import api
+    from mstm_b200._lib import MstmgError
+    pos = np.array([[0.0, 0.0, 0.0], [3.0, 0.0, 0.0], [0.0, 3.5, 0.0]])
+    rad = np.array([1.5, 0.5, 0.6])
+    g = api.SphereCluster(pos, rad, np.full(3, 1.5 + 0.01j), mie_epsilon=1e-6, precision="fp64")
+    assert g.host_spheres()[1] == 0
+    moved = pos.copy()
+    moved[1] = [0.5, 0.0, 0.0]     # now inside sphere 0
+    with pytest.raises(MstmgError):
+        g.set_positions(moved)
+    g.set_positions(pos + 0.25)    # still outside: accepted
+    g.close()
