@@ -420,6 +420,15 @@ def run_extras(args, dev, stream):
     row["fp64"] = {"solves_per_s": round(1000.0 / ms, 3), "ms": round(ms, 2), "qext": r["qtot"][0, 0], "iterations": r["iterations"],
                    "unknowns": g.number_eqns, "pairs_same_host": L.mstmg_npairs(g.ctx), "spheres_with_a_host": nh,
                    "ms_per_translation_pass_2_columns": round(g.time_translation("fp64", 2, 10), 4)}
+    # the pass against HBM: the stored FP64 records (same-host pairs and the
+    # host-to-inclusion regular translations) and the two columns in and out
+    rec = g.operator_bytes("fp64")[0]
+    alg = rec + 2 * 2 * g.number_eqns * 16
+    pms = row["fp64"]["ms_per_translation_pass_2_columns"]
+    row["fp64"]["pass_roofline"] = {"kernel": "translate_kernel<double, 64, 4> (order-generic, same-host pairs) + the host pairs' launch",
+                                    "algorithmic_bytes": alg, "achieved_gbs": round(alg / pms / 1e6, 1),
+                                    "frac_of_measured_hbm": round(alg / pms / 1e6 / hbm_peak(), 4),
+                                    "bound": "instruction issue (profiles/translate_generic_fp64_host300.md)"}
     fx = oracle_fixture("host1000")
     if fx is not None:
         row["fp64"]["vs_oracle"] = {"qext": float("%.3g" % abs(r["qtot"][0, 0] / fx["qtot"][0, 0] - 1)),

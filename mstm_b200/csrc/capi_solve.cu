@@ -602,14 +602,22 @@ extern "C" int mstmg_operator_bytes(const mstmg_ctx* c, int prec, double* stored
 {
     if (!c) return MSTMG_ERR_ARG;
     double es = prec == 0 ? 8.0 : 4.0;
-    if (stored) *stored = (prec != 0 && c->row32) ? (double)c->npairs * c->row32 * es : (double)c->op_units * es;
+    // with host spheres the stored records include the regular translations
+    // between hosts and the spheres they hold (FP64 only)
+    const double hb = c->hs.on() ? (double)c->hs.hunits * 8.0 : 0.0;
+    if (stored) *stored = ((prec != 0 && c->row32) ? (double)c->npairs * c->row32 * es : (double)c->op_units * es) + hb;
     if (canonical) {
+        auto canon = [&](int a, int b) {
+            int nmn = std::min(a, b), nmx = std::max(a, b);
+            return (2.0 * nmn + 1) * (nmx * (nmx + 2) + 1) * es + atcdim_h(a, b) * 2 * es + (2.0 * nmx + 1) * 2 * es;
+        };
         double s = 0.0;
         for (int i = 0; i < c->n - 1; i++)
-            for (int j = i + 1; j < c->n; j++) {
-                int a = c->order[i], b = c->order[j], nmn = std::min(a, b), nmx = std::max(a, b);
-                s += (2.0 * nmn + 1) * (nmx * (nmx + 2) + 1) * es + atcdim_h(a, b) * 2 * es + (2.0 * nmx + 1) * 2 * es;
-            }
+            for (int j = i + 1; j < c->n; j++)
+                if (!c->hs.on() || c->hs.host[i] == c->hs.host[j]) s += canon(c->order[i], c->order[j]);
+        if (c->hs.on())
+            for (int j = 0; j < c->n; j++)
+                if (c->hs.host[j] >= 0) s += canon(c->order[c->hs.host[j]], c->order[j]);
         *canonical = s;
     }
     return MSTMG_OK;
