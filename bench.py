@@ -559,18 +559,22 @@ def report_line(args, ws, R, ne):
     ms32, n32 = m["k32"]
     stored32, canon32 = m["bytes32"]   # FP32 row-record bytes (as stored), and the reference layout's bytes at 4 B per real
     folded32 = m["bytes64"][0] / 2.0   # the folded operator values at 4 B each, without the row records' padding
-    # algorithmic bytes per launch: the folded operator read once + x read + y
-    # written (one column per active polarisation: the tuned path's Arnoldi
-    # passes carry 2 columns while both polarisations are active; iterations
-    # count Arnoldi steps in pairs).  The row records the kernel reads carry
-    # row padding and a phase table on top (stored32), which counts as traffic.
+    # algorithmic bytes per launch, as the canonical matvec bytes define them
+    # (the reference layout's stored operator at 4 B per real, read once, +
+    # x read + y written; one column per active polarisation: the tuned
+    # path's Arnoldi passes carry 2 columns while both polarisations are
+    # active, iterations count Arnoldi steps in pairs).  The kernel itself
+    # reads the operator folded by the Wigner and axial symmetries, in row
+    # records (stored32: padding and a phase table on top), which is its DRAM
+    # traffic; the same pass against the folded values is reported beside.
     it = m["stats"]["iterations"]
     n32p = max(1, m["stats"]["passes32"])
     avg_cols = min(2.0, 2.0 * sum(it) / n32p) if sum(it) > 0 else 2.0
     vec_bytes = 2.0 * ne * 8 * avg_cols
-    alg = folded32 + vec_bytes
+    alg = canon32 + vec_bytes
     dur = ms32 / max(1, n32)
     achieved = alg / (dur * 1e-3) / 1e9 if n32 else None
+    folded_gbs = (folded32 + vec_bytes) / (dur * 1e-3) / 1e9 if n32 else None
     ms64, n64 = p["k64"]
     stored64, _ = p["bytes64"]
     dur64 = ms64 / max(1, n64)
@@ -606,8 +610,14 @@ def report_line(args, ws, R, ne):
                                        "(profiles/translate_rows_fp32_fractal200.md: 1.02x the row records and vectors "
                                        "read and written), scaled to this workload's row records",
                      "peak_source": peak_src,
-                     "algorithmic_bytes_per_launch": alg, "launch_ms": round(dur, 4), "launches": n32,
-                     "canonical_equiv_gbs": round((canon32 + vec_bytes) / (dur * 1e-3) / 1e9, 1) if n32 else None},
+                     "algorithmic_bytes_per_launch": alg,
+                     "algorithmic_bytes_source": "canonical matvec bytes (reference operator layout at 4 B per real, "
+                                                 "read once, + x and y): the kernel reads the symmetry-folded operator, "
+                                                 "so its traffic is below this",
+                     "launch_ms": round(dur, 4), "launches": n32,
+                     "folded_bytes_per_launch": folded32 + vec_bytes,
+                     "folded_gbs": round(folded_gbs, 1) if folded_gbs else None,
+                     "frac_of_folded_bytes": round(folded_gbs / hbm, 4) if folded_gbs else None},
         "e2e": {"value": round(ws * 1000.0 * args.steps / e2e["ms"], 4), "unit": "solves/s",
                 "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
         "gpu_launches": int(m["launches"]),
