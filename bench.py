@@ -411,7 +411,7 @@ def run_extras(args, dev, stream):
     w = C.host_inclusions(1000, 0.5, 0.15, seed=7)
     row = {"workload": "a host sphere (m=1.33, radius %.3f, the RSA bounding radius) holding 1000 inclusions (x=0.5, "
                        "m=1.6+0.05i, RSA at fv 0.15, seed 7): fixed orientation, both polarisations to residual 1e-6, "
-                       "FP64 BiCG, orders from mie_epsilon 1e-6" % w["radius"][0],
+                       "FP64 BiCG and mixed GMRES, orders from mie_epsilon 1e-6" % w["radius"][0],
            "metric": "solves/s"}
     g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=1e-6, precision="fp64")
     _lib.check(L.mstmg_set_stream(g.ctx, ctypes.c_void_p(stream.cuda_stream)), "set_stream")
@@ -436,6 +436,18 @@ def run_extras(args, dev, stream):
                                     "qeff_all": float("%.3g" % rel_err(r["qeff"], fx["qeff"])),
                                     "iterations_equal": bool(list(r["iterations"]) == list(fx["iterations"]))}
     g.close()
+    # the mixed solve (FP32 GMRES passes, the host couplings in FP32, FP64 true residuals)
+    g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=1e-6, precision="mixed")
+    _lib.check(L.mstmg_set_stream(g.ctx, ctypes.c_void_p(stream.cuda_stream)), "set_stream")
+    ms_m, rm = timed(lambda: g.fixedorsoln(eps=EPS, niter=NITER), 3)
+    row["mixed"] = {"solves_per_s": round(1000.0 / ms_m, 3), "ms": round(ms_m, 2), "qext": rm["qtot"][0, 0],
+                    "iterations_gmres_step_pairs": rm["iterations"],
+                    "ms_per_translation_pass_2_columns": round(g.time_translation("mixed", 2, 10), 4)}
+    if fx is not None:
+        row["mixed"]["vs_oracle"] = {"qext": float("%.3g" % abs(rm["qtot"][0, 0] / fx["qtot"][0, 0] - 1)),
+                                     "qabs_of_qext": float("%.3g" % abs((rm["qtot"][1, 0] - fx["qtot"][1, 0]) / fx["qtot"][0, 0])),
+                                     "qeff_all_of_max": float("%.3g" % (np.abs(rm["qeff"] - fx["qeff"]).max() / np.abs(fx["qeff"]).max()))}
+    g.close()
     import multiprocessing
     threads = multiprocessing.cpu_count()
     t0 = time.time()
@@ -444,7 +456,8 @@ def run_extras(args, dev, stream):
     o.close()
     row["oracle_cpu"] = {"s": round(time.time() - t0, 2), "threads": threads, "iterations": ro["iterations"],
                          "what": "the oracle's full FP64 solve (operators, BiCG, efficiencies) on this host's cores"}
-    row["speedup_vs_oracle_cpu"] = round(row["oracle_cpu"]["s"] * 1000.0 / ms, 1)
+    row["speedup_vs_oracle_cpu"] = {"fp64": round(row["oracle_cpu"]["s"] * 1000.0 / ms, 1),
+                                    "mixed": round(row["oracle_cpu"]["s"] * 1000.0 / ms_m, 1)}
     out["host_spheres1000"] = row
     # the 20-sphere cluster (the reference's CPU-sized case)
     w = C.workload("cluster20")

@@ -291,7 +291,7 @@ static int setup_host_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np)
     h.hunits = u;
     h.hmaxrec = maxrec;
     h.hlmax = hl;
-    h.hops_ready = false;
+    h.hops_ready = h.hops32_ready = false;
     if (h.nhp > 0) {
         CK(h.hpairs.alloc(h.nhp));
         CK(h.hopoff.alloc(h.nhp));
@@ -401,6 +401,16 @@ int setup_layout(mstmg_ctx* c)
                      c->d_mie_offset.p, hs.on() ? hs.d_hoff.p : nullptr, c->an.p, c->an_inv.p, c->an32.p, c->hs.dn.p, c->hs.un.p,
                      c->hs.vn.p, c->qext.p, c->qabs.p, c->st);
     CK(cudaGetLastError());
+    if (hs.on()) {
+        HostSpheres& h = c->hs;
+        CK(h.dn32.alloc(nt));
+        CK(h.un32.alloc(nt));
+        CK(h.vn32.alloc(nt));
+        launch_d2f((int)nt, h.dn.p, h.dn32.p, c->st);
+        launch_d2f((int)nt, h.un.p, h.un32.p, c->st);
+        launch_d2f((int)nt, h.vn.p, h.vn32.p, c->st);
+        CK(cudaGetLastError());
+    }
     // pairs whose smaller order is below translation_switch_order take the
     // reference's dense path (coefficient_translation, rot_op false)
     const int tso = c->opts.translation_switch_order;

@@ -89,24 +89,26 @@ int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
     a.xi = c->opgen_xi.p;
     launch_opgen(a, c->nsm, c->st);
     CK(cudaGetLastError());
-    if (need64 && c->hs.nhp > 0) {
+    if ((need64 || need32) && c->hs.nhp > 0) {
         // regular translations between hosts and the spheres they hold, in
         // the host's index (external_to_internal_expansion, modules:6579-6592)
         HostSpheres& h = c->hs;
-        CK(h.hop64.alloc(h.hunits));
+        if (need64) CK(h.hop64.alloc(h.hunits));
+        if (need32) CK(h.hop32.alloc(h.hunits));
         OpGenArgs b = a;
         b.npairs = h.nhp;
         b.pairs = h.hpairs.p;
         b.pos = h.xpos.p;
         b.opoff = h.hopoff.p;
-        b.op64 = h.hop64.p;
-        b.op32 = nullptr;
+        b.op64 = need64 ? h.hop64.p : nullptr;
+        b.op32 = need32 ? h.hop32.p : nullptr;
         b.row32 = 0;
         b.pmed = h.hmed.p;
         b.regular = 1;
         launch_opgen(b, c->nsm, c->st);
         CK(cudaGetLastError());
-        h.hops_ready = true;
+        if (need64) h.hops_ready = true;
+        if (need32) h.hops32_ready = true;
     }
     if (need64) c->ops64_ready = true;
     if (need32) c->ops32_ready = true;
@@ -114,21 +116,21 @@ int ensure_ops_both(mstmg_ctx* c, bool want64, bool want32, bool force)
 }
 
 // y[:, 0:nrhs] += the host-sphere couplings of x (external_to_internal_expansion)
-int translate_hosts(mstmg_ctx* c, const zd* x, zd* y, int nrhs, unsigned contran)
+template <typename T> int translate_hosts(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran)
 {
     HostSpheres& h = c->hs;
     if (!h.on()) return MSTMG_OK;
     if (h.nhp > 0) {
-        if (!h.hops_ready) {
+        if (sizeof(T) == 8 ? !h.hops_ready : !h.hops32_ready) {
             set_err("internal error: host-sphere operators not generated");
             return MSTMG_ERR_ARG;
         }
-        TransArgs<double> a;
+        TransArgs<T> a;
         a.npairs = h.nhp;
         a.pairs = h.hpairs.p;
         a.order = c->d_order.p;
         a.offset = c->d_offset.p;
-        a.ops = h.hop64.p;
+        a.ops = sizeof(T) == 8 ? (const T*)h.hop64.p : (const T*)h.hop32.p;
         a.opoff = h.hopoff.p;
         a.x = x;
         a.y = y;
@@ -138,28 +140,37 @@ int translate_hosts(mstmg_ctx* c, const zd* x, zd* y, int nrhs, unsigned contran
         a.lmax = h.hlmax;
         a.maxrec = h.hmaxrec;
         a.err = c->err.p;
-        launch_translate<double>(a, c->nsm, c->st);
+        launch_translate<T>(a, c->nsm, c->st);
     }
-    launch_mtransfer(h.nzp, h.zpairs.p, c->d_order.p, c->d_offset.p, x, y, c->neqns, nrhs, c->st);
+    launch_mtransfer<T>(h.nzp, h.zpairs.p, c->d_order.p, c->d_offset.p, x, y, c->neqns, nrhs, c->st);
     CK(cudaGetLastError());
     return MSTMG_OK;
 }
+template int translate_hosts<double>(mstmg_ctx*, const zd*, zd*, int, unsigned);
+template int translate_hosts<float>(mstmg_ctx*, const zf*, zf*, int, unsigned);
 
-void mie_all(mstmg_ctx* c, int idir, int conj_in, const zd* x, zd* y)
+template <typename T> void mie_all(mstmg_ctx* c, int idir, int conj_in, const cpx<T>* x, cpx<T>* y)
 {
     SlotMaps sm = c->sm();
-    if (c->hs.on())
-        launch_hmie(sm.nslots, c->n, sm.slot, sm.order, sm.offset, sm.mie_offset, c->hs.d_hoff.p, c->an.p, c->hs.dn.p, c->hs.un.p,
-                    c->hs.vn.p, idir, conj_in, x, y, c->st);
-    else
-        launch_mie<double>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, c->an.p, idir, conj_in, x, y, c->st);
+    const bool d = sizeof(T) == 8;
+    const cpx<T>* an = d ? (const cpx<T>*)c->an.p : (const cpx<T>*)c->an32.p;
+    if (c->hs.on()) {
+        const HostSpheres& h = c->hs;
+        launch_hmie<T>(sm.nslots, c->n, sm.slot, sm.order, sm.offset, sm.mie_offset, h.d_hoff.p, an,
+                       d ? (const cpx<T>*)h.dn.p : (const cpx<T>*)h.dn32.p, d ? (const cpx<T>*)h.un.p : (const cpx<T>*)h.un32.p,
+                       d ? (const cpx<T>*)h.vn.p : (const cpx<T>*)h.vn32.p, idir, conj_in, x, y, c->st);
+    } else {
+        launch_mie<T>(sm.nslots, sm.slot, sm.order, sm.offset, sm.mie_offset, an, idir, conj_in, x, y, c->st);
+    }
 }
+template void mie_all<double>(mstmg_ctx*, int, int, const zd*, zd*);
+template void mie_all<float>(mstmg_ctx*, int, int, const zf*, zf*);
+
 int ensure_ops(mstmg_ctx* c, int prec, bool force) { return ensure_ops_both(c, prec == 0, prec == 1, force); }
 
 template <typename T> static const T* ops_ptr(mstmg_ctx* c);
 template <> const double* ops_ptr<double>(mstmg_ctx* c) { return c->op64.p; }
 template <> const float* ops_ptr<float>(mstmg_ctx* c) { return c->op32.p; }
-
 
 // FP32 passes on row records: the row kernel, in groups of 4, 2 or 1 columns
 // when the pass has another column count (the records fit no other kernel)
@@ -187,14 +198,10 @@ template <> int rows_pass<float>(mstmg_ctx* c, const TiledArgs<float>& tf, int n
 template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran, int nchunk)
 {
     NvtxRange nvtx_(sizeof(T) == 8 ? "translation pass FP64" : "translation pass FP32");
-    if (sizeof(T) == 4 && c->hs.on()) {
-        set_err("FP32 translation passes are not available for clusters with spheres inside other spheres");
-        return MSTMG_ERR_UNSUPPORTED;
-    }
     CK(cudaMemsetAsync(y, 0, sizeof(cpx<T>) * (size_t)c->neqns * nrhs * nchunk, c->st));
     if (c->hs.on()) {
         if (nchunk > 1) return MSTMG_ERR_UNSUPPORTED;
-        int rh = translate_hosts(c, (const zd*)x, (zd*)y, nrhs, contran);
+        int rh = translate_hosts<T>(c, x, y, nrhs, contran);
         if (rh) return rh;
     }
     if (c->ndense > 0) {
@@ -518,7 +525,7 @@ int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, co
         zd* col = c->X64.p + (size_t)r * ne;
         if (ct) {
             mask |= 1u << r;
-            if (mm) mie_all(c, -1, 1, col, col);
+            if (mm) mie_all<double>(c, -1, 1, col, col);
             else launch_conj_copy<double>(ne, col, col, c->st);
         }
     }
@@ -529,7 +536,7 @@ int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, co
         if (c->hs.on()) {
             rc = ensure_ops(c, 0, initial_run != 0);
             if (rc) return rc;
-            rc = translate_hosts(c, c->X64.p, c->Y64.p, nrhs, mask);
+            rc = translate_hosts<double>(c, c->X64.p, c->Y64.p, nrhs, mask);
             if (rc) return rc;
         }
     } else {
@@ -541,7 +548,7 @@ int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, co
         int mm = mie_mult ? mie_mult[r] : 1;
         zd* col = c->Y64.p + (size_t)r * ne;
         if (!ct) {
-            if (mm) mie_all(c, 1, 0, col, col);
+            if (mm) mie_all<double>(c, 1, 0, col, col);
         } else {
             launch_conj_copy<double>(ne, col, col, c->st);
         }

@@ -340,8 +340,9 @@ static int fixed_orientation_impl(mstmg_ctx* c, double alpha, double sinc, int d
     if (!c || !amnp) return MSTMG_ERR_ARG;
     if (int rc0 = reject_ensemble(c, "mstmg_fixed_orientation")) return rc0;
     if (int rc1 = reject_sharded(c, "mstmg_fixed_orientation")) return rc1;
-    if (c->hs.on() && (x0 || (niter > 0 && c->opts.precision == MSTMG_PRECISION_MIXED))) {
-        set_err("mstmg_fixed_orientation: with spheres inside other spheres the solve is the FP64 BiCG (precision FP64, no initial guess)");
+    if (c->hs.on() && (x0 || (niter > 0 && c->opts.precision == MSTMG_PRECISION_MIXED && c->opts.mixed_solver != 2))) {
+        set_err("mstmg_fixed_orientation: with spheres inside other spheres the solve is the FP64 BiCG or the mixed GMRES "
+                "(mixed_solver 2), without an initial guess");
         return MSTMG_ERR_UNSUPPORTED;
     }
     const int ne = c->neqns;
@@ -916,6 +917,18 @@ int solve_multi_rr(mstmg_ctx* c, MultiWork<double>& w64, MultiWork<float>& w32, 
 // own basis, Hessenberg matrix and stopping test.
 // x_zero: X holds zeros on entry, so the first cycle's true residual is B
 // itself and needs no FP64 pass.
+// W = XP - M Y for na columns; with host spheres the Mie multiply runs
+// apart (on Y in place) and the kernel takes Y as M H v
+static void gm_apply_ctx(mstmg_ctx* c, const SlotMaps& sm, const zf* an32, int ne, int na, const zf* XP, zf* Y, zf* W)
+{
+    if (c->hs.on()) {
+        for (int k = 0; k < na; k++) mie_all<float>(c, 1, 0, Y + (size_t)k * ne, Y + (size_t)k * ne);
+        launch_gm_apply(sm, nullptr, ne, na, XP, Y, W, c->nsm, c->st);
+    } else {
+        launch_gm_apply(sm, an32, ne, na, XP, Y, W, c->nsm, c->st);
+    }
+}
+
 int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S, const zd* B, zd* X, double eps, int niter,
                              std::vector<int>& iters, std::vector<double>& errs, std::vector<int>& status, int* outer_count,
                              const EnsSeg* seg, bool x_zero)
@@ -986,7 +999,13 @@ int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S
                 launch_m_gather<double>(ne, a, apad, w64.act.p, X, w64.XP.p, c->nsm, c->st);
                 if ((rc = translate_many<double>(c, w64.XP.p, w64.YP.p, apad, 0u))) return rc;
             }
-            launch_m_resid<float>(sm, c->an.p, ne, a, w64.act.p, B, X, w64.YP.p, gw.R.p, w64.part.p, gw.rr.p, c->nsm, c->st, 1);
+            if (c->hs.on()) {
+                // host spheres: the Mie multiply apart, the residual kernel takes M H x
+                for (int k = 0; k < a; k++) mie_all<double>(c, 1, 0, w64.YP.p + (size_t)k * ne, w64.YP.p + (size_t)k * ne);
+                launch_m_resid<float>(sm, nullptr, ne, a, w64.act.p, B, X, w64.YP.p, gw.R.p, w64.part.p, gw.rr.p, c->nsm, c->st, 1);
+            } else {
+                launch_m_resid<float>(sm, c->an.p, ne, a, w64.act.p, B, X, w64.YP.p, gw.R.p, w64.part.p, gw.rr.p, c->nsm, c->st, 1);
+            }
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(hrr.data(), gw.rr.p, sizeof(double) * 2 * S, cudaMemcpyDeviceToHost, c->st));
@@ -1072,7 +1091,7 @@ int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S
                             launch_gm_gather_dev(ne, m1, na, na, gw.act.p, d.j, d.alive, gw.V.p, gw.XP.p, c->nsm, c->st);
                             int r2 = translate_many<float>(c, gw.XP.p, gw.Y.p, na, 0u);
                             if (r2) return r2;
-                            launch_gm_apply(sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+                            gm_apply_ctx(c, sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p);
                         }
                         CK(cudaMemsetAsync(gw.h.p, 0, sizeof(double) * (O1 + 2 * HP), c->st));
                         launch_gm_dots_dev(ldv, S, m1, na, gw.act.p, d.j, gw.V.p, gw.W.p, h1, nullptr, c->nsm, c->st, slen);
@@ -1139,7 +1158,7 @@ int solve_multi_gmres(mstmg_ctx* c, MultiWork<double>& w64, GmresWork& gw, int S
                     const int npad = na <= 2 ? na : ((na + 3) / 4) * 4;   // whole FP32 chunks
                     launch_gm_gather(ne, m1, j, na, npad, gw.act.p, gw.V.p, gw.XP.p, c->nsm, c->st);
                     if ((r2 = translate_many<float>(c, gw.XP.p, gw.Y.p, npad, 0u))) return r2;
-                    launch_gm_apply(sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p, c->nsm, c->st);
+                    gm_apply_ctx(c, sm, an32, ne, na, gw.XP.p, gw.Y.p, gw.W.p);
                 }
                 CK(cudaMemsetAsync(gw.h.p, 0, sizeof(double) * (O1 + hn), c->st));
                 CK(cudaMemsetAsync(h2, 0, sizeof(double) * hn, c->st));

@@ -299,6 +299,7 @@ struct HostSpheres {
     DevBuf<double> d_rext, qv, xpos;   // xpos: positions of the device sphere arrays (internal blocks at their host's centre)
     DevBuf<int> d_host, d_hoff, d_outside;   // holding sphere; offset of the internal block (-1 none); 1 outside every sphere
     DevBuf<zd> dn, un, vn;       // the holding spheres' D, U, V Mie coefficients (mie_offset)
+    DevBuf<zf> dn32, un32, vn32; // the same in FP32 (the mixed solver's passes)
     DevBuf<double> pmed, dmed;   // the index of each same-host pair's medium: rotation pairs, dense pairs
     // external_to_internal_expansion: (internal block, held sphere) pairs
     // translated by regular operators in the host's index; coincident
@@ -309,7 +310,8 @@ struct HostSpheres {
     int nzp = 0;
     DevBuf<long long> hopoff;
     DevBuf<double> hop64, hmed;
-    bool hops_ready = false;
+    DevBuf<float> hop32;
+    bool hops_ready = false, hops32_ready = false;
     bool on() const { return nhosted > 0; }
 };
 
@@ -460,9 +462,9 @@ int interaction_impl(mstmg_ctx* c, int nrhs, const double* ain, double* aout, co
                      const int* rhs_list, int skip_external);
 // host spheres: y[:, 0:nrhs] += the regular translations between hosts and
 // the spheres they hold (external_to_internal_expansion)
-int translate_hosts(mstmg_ctx* c, const zd* x, zd* y, int nrhs, unsigned contran);
-// the Mie multiply of every sphere (host spheres' blocks included), FP64
-void mie_all(mstmg_ctx* c, int idir, int conj_in, const zd* x, zd* y);
+template <typename T> int translate_hosts(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int nrhs, unsigned contran);
+// the Mie multiply of every sphere (host spheres' blocks included)
+template <typename T> void mie_all(mstmg_ctx* c, int idir, int conj_in, const cpx<T>* x, cpx<T>* y);
 template <typename T> int fft_far(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int ncols, unsigned contran);
 int fft_build(mstmg_ctx* c);
 // capi_origin.cu

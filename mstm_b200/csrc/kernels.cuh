@@ -47,7 +47,9 @@ template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cuda
 template <typename T> size_t translate_smem_bytes(int lmax, int nrhs, int maxrec);
 // y(:, r) += the order-truncated copies between the blocks of each pair
 // (i, j) and back: coincident centres of a host and a sphere it holds
-void launch_mtransfer(int npairs, const int2* pairs, const int* order, const int* offset, const zd* x, zd* y, int ld, int nrhs, cudaStream_t st);
+template <typename T>
+void launch_mtransfer(int npairs, const int2* pairs, const int* order, const int* offset, const cpx<T>* x, cpx<T>* y, int ld, int nrhs,
+                      cudaStream_t st);
 
 // Mie multiply over all spheres: y(:,r) = A x(:,r) (idir=1) or A^T x(:,r);
 // optional conjugation of the input.  slot_sphere maps each (row, column)

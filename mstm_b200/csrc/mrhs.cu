@@ -76,14 +76,20 @@ __global__ void __launch_bounds__(MB) gm_gather_kernel(int ld, int m1, int j, in
     for (int e = blockIdx.x * MB + threadIdx.x; e < ld; e += gridDim.x * MB) o[e] = v ? v[e] : mk(0.0f, 0.0f);
 }
 
-// W[:, k] = XP[:, k] - M Y[:, k]   (A v = v - M H v with Y = H v)
+// W[:, k] = XP[:, k] - M Y[:, k]   (A v = v - M H v with Y = H v); an == null:
+// Y already holds M H v (the host-sphere Mie multiply runs apart)
 __global__ void __launch_bounds__(MB) gm_apply_kernel(SlotMaps sm, const zf* an, int ld, const zf* XP, const zf* Y, zf* W)
 {
     const size_t o = (size_t)blockIdx.y * ld;
     for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
         SlotPos q = slot_pos(sm, e);
-        const zf* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
         const zf u0 = Y[o + q.b0], u1 = Y[o + q.b1];
+        if (!an) {
+            W[o + q.b0] = XP[o + q.b0] - u0;
+            W[o + q.b1] = XP[o + q.b1] - u1;
+            continue;
+        }
+        const zf* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
         W[o + q.b0] = XP[o + q.b0] - (A[0] * u0 + A[2] * u1);
         W[o + q.b1] = XP[o + q.b1] - (A[1] * u0 + A[3] * u1);
     }
@@ -565,9 +571,13 @@ __global__ void __launch_bounds__(MB) m_resid_kernel(SlotMaps sm, const zd* an, 
     double acc[2] = {0.0, 0.0};
     for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
         SlotPos q = slot_pos(sm, e);
-        const zd* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
         zd u0 = y[q.b0], u1 = y[q.b1];
-        zd m[2] = {A[0] * u0 + A[2] * u1, A[1] * u0 + A[3] * u1};
+        zd m[2] = {u0, u1};   // an == null: y already holds M H x
+        if (an) {
+            const zd* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+            m[0] = A[0] * u0 + A[2] * u1;
+            m[1] = A[1] * u0 + A[3] * u1;
+        }
         const int bb[2] = {q.b0, q.b1};
         for (int h = 0; h < 2; h++) {
             zd bv = B[o + bb[h]];

@@ -382,9 +382,10 @@ template <typename T> __device__ __forceinline__ void m22(const cpx<T>* X, bool 
     }
 }
 
+template <typename T>
 __global__ void hmie_kernel(int nslots, int nreal, const int* slot_sphere, const int* order, const int* offset, const int* mie_offset,
-                            const int* hoff, const zd* an, const zd* dn, const zd* un, const zd* vn, int idir, int conj_in, const zd* x,
-                            zd* y)
+                            const int* hoff, const cpx<T>* an, const cpx<T>* dn, const cpx<T>* un, const cpx<T>* vn, int idir, int conj_in,
+                            const cpx<T>* x, cpx<T>* y)
 {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nslots) return;
@@ -396,37 +397,43 @@ __global__ void hmie_kernel(int nslots, int nreal, const int* slot_sphere, const
     int row = loc % (L + 2), col = loc / (L + 2) + 1;
     int n = (row <= col) ? col : row - 1;
     int base = offset[i] + loc;
-    zd g0 = x[base], g1 = x[base + hb];
+    cpx<T> g0 = x[base], g1 = x[base + hb];
     if (conj_in) { g0 = cj(g0); g1 = cj(g1); }
     const int q = mie_offset[i] + 4 * (n - 1);
     const bool tr = idir != 1;
-    zd a0 = mk(0.0, 0.0), a1 = mk(0.0, 0.0);
-    m22<double>(an + q, tr, g0, g1, a0, a1);
+    cpx<T> a0 = mk((T)0, (T)0), a1 = mk((T)0, (T)0);
+    m22<T>(an + q, tr, g0, g1, a0, a1);
     if (hoff[i] < 0) {
         y[base] = a0;
         y[base + hb] = a1;
         return;
     }
     const int bb = hoff[i] + loc;
-    zd b0 = x[bb], b1 = x[bb + hb];
+    cpx<T> b0 = x[bb], b1 = x[bb + hb];
     if (conj_in) { b0 = cj(b0); b1 = cj(b1); }
-    zd f0 = mk(0.0, 0.0), f1 = mk(0.0, 0.0);
-    m22<double>((tr ? dn : un) + q, tr, b0, b1, a0, a1);
-    m22<double>((tr ? un : dn) + q, tr, g0, g1, f0, f1);
-    m22<double>(vn + q, tr, b0, b1, f0, f1);
+    cpx<T> f0 = mk((T)0, (T)0), f1 = mk((T)0, (T)0);
+    m22<T>((tr ? dn : un) + q, tr, b0, b1, a0, a1);
+    m22<T>((tr ? un : dn) + q, tr, g0, g1, f0, f1);
+    m22<T>(vn + q, tr, b0, b1, f0, f1);
     y[base] = a0;
     y[base + hb] = a1;
     y[bb] = f0;
     y[bb + hb] = f1;
 }
 
+template <typename T>
 void launch_hmie(int nslots, int nreal, const int* slot_sphere, const int* order, const int* offset, const int* mie_offset, const int* hoff,
-                 const zd* an, const zd* dn, const zd* un, const zd* vn, int idir, int conj_in, const zd* x, zd* y, cudaStream_t st)
+                 const cpx<T>* an, const cpx<T>* dn, const cpx<T>* un, const cpx<T>* vn, int idir, int conj_in, const cpx<T>* x, cpx<T>* y,
+                 cudaStream_t st)
 {
-    hmie_kernel<<<(nslots + 255) / 256, 256, 0, st>>>(nslots, nreal, slot_sphere, order, offset, mie_offset, hoff, an, dn, un, vn, idir,
-                                                      conj_in, x, y);
+    hmie_kernel<T><<<(nslots + 255) / 256, 256, 0, st>>>(nslots, nreal, slot_sphere, order, offset, mie_offset, hoff, an, dn, un, vn, idir,
+                                                         conj_in, x, y);
     launch_counter() += 1;
 }
+template void launch_hmie<double>(int, int, const int*, const int*, const int*, const int*, const int*, const zd*, const zd*, const zd*,
+                                  const zd*, int, int, const zd*, zd*, cudaStream_t);
+template void launch_hmie<float>(int, int, const int*, const int*, const int*, const int*, const int*, const zf*, const zf*, const zf*,
+                                 const zf*, int, int, const zf*, zf*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Efficiencies: lrsphereqeff (scatprops:676-776) per sphere, npol=2, with

@@ -14,9 +14,11 @@ void launch_mie_coefs(int n, const double* radius, const double* ri, double mre,
 void launch_planewave(double alpha, double sinc, int dir, int lmax, int neqns, const int* slot_full, const int* order,
                       const int* offset, const double* pos, zd* pw0, zd* drot, zd* pmnp, cudaStream_t st, int nreal = 0,
                       const int* outside = nullptr);
-// Mie multiply with host spheres' second blocks at hoff[i] (>= 0), FP64
+// Mie multiply with host spheres' second blocks at hoff[i] (>= 0)
+template <typename T>
 void launch_hmie(int nslots, int nreal, const int* slot_sphere, const int* order, const int* offset, const int* mie_offset, const int* hoff,
-                 const zd* an, const zd* dn, const zd* un, const zd* vn, int idir, int conj_in, const zd* x, zd* y, cudaStream_t st);
+                 const cpx<T>* an, const cpx<T>* dn, const cpx<T>* un, const cpx<T>* vn, int idir, int conj_in, const cpx<T>* x, cpx<T>* y,
+                 cudaStream_t st);
 // per-configuration totals of an ensemble: qtot[9 k ..] from the spheres
 // cfg_start[k] .. cfg_start[k+1]-1, volume radius xg[k] (device arrays)
 void launch_qtot_configs(int nc, const int* cfg_start, const double* radius, const double* qeff, const double* xg, double* qtot, cudaStream_t st);

@@ -336,15 +336,16 @@ template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cuda
 // zero_translation with vswf_type 1, mtransfer, modules:2334-2344): the
 // regular translation is the identity on the common orders, in both
 // directions and whatever the shift.  One CTA per (pair, column).
-__global__ void mtransfer_kernel(int npairs, const int2* pairs, const int* order, const int* offset, const zd* x, zd* y, int ld)
+template <typename T>
+__global__ void mtransfer_kernel(int npairs, const int2* pairs, const int* order, const int* offset, const cpx<T>* x, cpx<T>* y, int ld)
 {
     const int q = blockIdx.x, r = blockIdx.y;
     if (q >= npairs) return;
     const int i = pairs[q].x, j = pairs[q].y;
     const int Li = order[i], Lj = order[j], L = Li < Lj ? Li : Lj;
     const int nb = L * (L + 2);
-    const zd* xr = x + (size_t)r * ld;
-    zd* yr = y + (size_t)r * ld;
+    const cpx<T>* xr = x + (size_t)r * ld;
+    cpx<T>* yr = y + (size_t)r * ld;
     for (int e = threadIdx.x; e < 2 * nb; e += blockDim.x) {
         const int p = e / nb, k = e - p * nb;
         const int n = (int)sqrt((double)(k + 1) + 0.5), m = k + 1 - n * n - n;   // k + 1 = n(n+1) + m
@@ -356,12 +357,16 @@ __global__ void mtransfer_kernel(int npairs, const int2* pairs, const int* order
     }
 }
 
-void launch_mtransfer(int npairs, const int2* pairs, const int* order, const int* offset, const zd* x, zd* y, int ld, int nrhs, cudaStream_t st)
+template <typename T>
+void launch_mtransfer(int npairs, const int2* pairs, const int* order, const int* offset, const cpx<T>* x, cpx<T>* y, int ld, int nrhs,
+                      cudaStream_t st)
 {
     if (npairs <= 0) return;
-    mtransfer_kernel<<<dim3(npairs, nrhs), 128, 0, st>>>(npairs, pairs, order, offset, x, y, ld);
+    mtransfer_kernel<T><<<dim3(npairs, nrhs), 128, 0, st>>>(npairs, pairs, order, offset, x, y, ld);
     launch_counter() += 1;
 }
+template void launch_mtransfer<double>(int, const int2*, const int*, const int*, const zd*, zd*, int, int, cudaStream_t);
+template void launch_mtransfer<float>(int, const int2*, const int*, const int*, const zf*, zf*, int, int, cudaStream_t);
 
 template void launch_translate<double>(const TransArgs<double>&, int, cudaStream_t);
 template void launch_translate<float>(const TransArgs<float>&, int, cudaStream_t);

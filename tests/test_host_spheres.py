@@ -12,9 +12,9 @@ against its dense solve.  GPU: the device path against the oracle on a
 cluster with two host levels, coincident and offset centres, small spheres
 on the dense path and spheres outside: host map, orders, layout, Mie
 coefficients (1e-12), sphereinteraction in every argument form (1e-12), the
-FP64 solves (same iterations, efficiencies to 1e-9), the scattering matrix
-(1e-9 of S11's largest value) and the refusals of the entry points built for
-spheres in the medium.
+FP64 solves (same iterations, efficiencies to 1e-9), the mixed solve (1e-6),
+the scattering matrix (1e-9 of S11's largest value) and the refusals of the
+entry points built for spheres in the medium.
 """
 import numpy as np
 import pytest
@@ -236,12 +236,35 @@ def test_host_solver_modes(pair):
 
 
 @pytest.mark.gpu
+def test_host_mixed_precision(pair):
+    """The mixed solve (FP32 GMRES passes with the host couplings in FP32,
+    FP64 true residuals) against the oracle to the mixed path's 1e-6, and the
+    FP32 translation pass against the FP64 one."""
+    from mstm_b200 import api
+    g, o = pair
+    pos, rad, ri = host_cluster()
+    m = api.SphereCluster(pos, rad, ri, mie_epsilon=1e-6, precision="mixed")
+    rm = m.fixedorsoln(eps=1e-12, niter=500)
+    ro = o.fixedorsoln(eps=1e-16, niter=1000)
+    assert rm["istat"] == 0
+    # to 1e-6 of the extinction (absorption is a small difference here)
+    assert np.abs(rm["qtot"] - ro["qtot"]).max() <= 1e-6 * ro["qtot"][0, 0]
+    assert np.abs(rm["qeff"] - ro["qeff"]).max() <= 1e-6 * np.abs(ro["qeff"]).max()
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal((g.number_eqns, 2)) + 1j * rng.standard_normal((g.number_eqns, 2))
+    y64 = g.translation_pass(x, [0, 1], "fp64")
+    y32 = g.translation_pass(x, [0, 1], "fp32")
+    assert np.abs(y32 - y64).max() <= 2e-6 * np.abs(y64).max()
+    m.close()
+
+
+@pytest.mark.gpu
 def test_host_contexts_refuse_the_medium_only_paths(pair):
     from mstm_b200 import api
     from mstm_b200._lib import MstmgError
     g, _ = pair
     pos, rad, ri = host_cluster()
-    m = api.SphereCluster(pos, rad, ri, mie_epsilon=1e-6, precision="mixed")
+    m = api.SphereCluster(pos, rad, ri, mie_epsilon=1e-6, precision="mixed", mixed_solver=1)
     with pytest.raises(MstmgError):
         m.fixedorsoln(eps=1e-8)
     m.close()
@@ -251,9 +274,9 @@ def test_host_contexts_refuse_the_medium_only_paths(pair):
         g.fft_setup(d_cell=2.0)
     with pytest.raises(MstmgError):
         g.set_positions(pos + 0.01)
-    x = np.ones((g.number_eqns, 2), np.complex128)
+    x = np.ones((g.number_eqns, 16), np.complex128)
     with pytest.raises(MstmgError):
-        g.translation_pass(x, [0, 1], "fp32")
+        g.translation_pass(x, None, "tc")
 
 
 @pytest.mark.gpu
