@@ -112,12 +112,12 @@ double mstmg_vol_radius(const mstmg_ctx *ctx);
  * as sphere_offset lays them out.  mstmg_ctx_create detects hosts always.
  * host (may be NULL): nsphere entries, the holding sphere (0-based) or -1.
  * Returns the number of spheres that have a host (number_host_spheres).
- * With hosts, mstmg_bicg, mstmg_fixed_orientation (precision FP64, or mixed
- * with mixed_solver 2), mstmg_interaction(_ex), mstmg_planewave,
- * mstmg_fixed_orientation_rhs, mstmg_efficiencies, mstmg_scattering and the
- * FP64 / FP32 translation passes are available; the T matrix, the FFT path,
- * pair shards, ensembles, the tensor-core pass and mstmg_ctx_set_positions
- * return MSTMG_ERR_UNSUPPORTED. */
+ * With hosts, mstmg_bicg, mstmg_fixed_orientation and mstmg_tmatrix
+ * (precision FP64, or mixed with mixed_solver 2), mstmg_t_matrix_order,
+ * mstmg_interaction(_ex), mstmg_planewave, mstmg_fixed_orientation_rhs,
+ * mstmg_efficiencies, mstmg_scattering and the FP64 / FP32 translation
+ * passes are available; the FFT path, pair shards, ensembles, the
+ * tensor-core pass and mstmg_ctx_set_positions return MSTMG_ERR_UNSUPPORTED. */
 int mstmg_host_spheres(const mstmg_ctx *ctx, int *host);
 /* The D, U, V Mie coefficients of the host spheres (mieoa's dnp_mie, unp_mie,
  * vnp_mie, mstm-modules-33.f90:5495-5528), laid out as an (zero for spheres

@@ -297,7 +297,6 @@ extern "C" int mstmg_scattering_plane(mstmg_ctx* c, int t_matrix_order, const do
 extern "C" int mstmg_t_matrix_order(mstmg_ctx* c, double trans_eps, int max_t_order, int* t_matrix_order)
 {
     if (int rc0 = reject_ensemble(c, "mstmg_t_matrix_order")) return rc0;
-    if (int rh = reject_hosts(c, "mstmg_t_matrix_order")) return rh;
     if (!c || max_t_order < 1 || !t_matrix_order) {
         set_err("mstmg_t_matrix_order: bad arguments");
         return MSTMG_ERR_ARG;
@@ -320,7 +319,11 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
                              double* tmat, double* sphere_qeff, double* qtot, int* order_used, int* maxiter, double* maxerr)
 {
     if (int rc0 = reject_ensemble(c, "mstmg_tmatrix")) return rc0;
-    if (int rh = reject_hosts(c, "mstmg_tmatrix")) return rh;
+    if (c && c->hs.on() && c->opts.precision == MSTMG_PRECISION_MIXED && c->opts.mixed_solver != 2) {
+        set_err("mstmg_tmatrix: with spheres inside other spheres the columns are solved by the FP64 BiCG or the mixed GMRES "
+                "(mixed_solver 2)");
+        return MSTMG_ERR_UNSUPPORTED;
+    }
     if (int rc1 = reject_sharded(c, "mstmg_tmatrix")) return rc1;
     NvtxRange nvtx_("mstmg_tmatrix");
     if (!c || t_matrix_order < 1 || t_matrix_order > 200 || !tmat || max_iterations < 1) {
@@ -347,10 +350,15 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
     const int nblkt = 2 * TM * (TM + 2), Sord = cols_of(TM), Smax = grouped ? std::max(Sord, TM_GROUP) : Sord;
     BigTablesDev bt;
     if ((rc = upload_big(c, bt))) return rc;
+    // the cluster origin: the mean of the spheres outside every other (input:1166-1177)
     double r0[3] = {0.0, 0.0, 0.0};
+    int nout = 0;
     for (int i = 0; i < n; i++)
-        for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->hpos[3 * (size_t)i + k];
-    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)n;
+        if (!c->hs.on() || c->hs.host[i] < 0) {
+            nout++;
+            for (int k = 0; k < 3; k++) r0[k] = r0[k] + c->hpos[3 * (size_t)i + k];
+        }
+    for (int k = 0; k < 3; k++) r0[k] = r0[k] / (double)nout;
     DevBuf<int> dtord;
     CK(dtord.alloc(n));
     CK(cudaMemcpyAsync(dtord.p, c->tord.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
@@ -420,7 +428,10 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
         // b = Mie f, initial guess b (solver:185-187); the grouped mixed
         // GMRES starts from zero instead, whose residual b needs no FP64 pass
         // (the Krylov space holds b after the first step)
-        launch_m_mie(sm, c->an.p, ne, Sg, PK.p, B64.p, c->st);
+        if (c->hs.on())
+            for (int k = 0; k < Sg; k++) mie_all<double>(c, 1, 0, PK.p + (size_t)k * ne, B64.p + (size_t)k * ne);
+        else
+            launch_m_mie(sm, c->an.p, ne, Sg, PK.p, B64.p, c->st);
         if (grouped) CK(cudaMemsetAsync(X, 0, sizeof(zd) * (size_t)ne * Sg, c->st));
         else CK(cudaMemcpyAsync(X, B64.p, sizeof(zd) * (size_t)ne * Sg, cudaMemcpyDeviceToDevice, c->st));
         CK(cudaGetLastError());
@@ -452,9 +463,17 @@ extern "C" int mstmg_tmatrix(mstmg_ctx* c, int t_matrix_order, double solution_e
                 if (its[k] > max_iterations || errs[k] > solution_eps || sts[k] == 2) istat = 1;
             }
             zd* Xq = X + (size_t)col0 * ne;
-            // per-sphere efficiencies of every column, summed
+            // per-sphere efficiencies of every column, summed; with host
+            // spheres the exciting fields are the interaction without the Mie
+            // multiply plus the incident field (qefficiencyfactors), in B64
+            const zd* G = nullptr;
+            if (c->hs.on()) {
+                if ((rc = translate_many<double>(c, Xq, B64.p, S, 0u))) return rc;
+                launch_add_correction_d(S * ne, B64.p, PK.p + (size_t)col0 * ne, c->st);
+                G = B64.p;
+            }
             launch_tm_qeff(n, S, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, rimed, c->an_inv.p, Xq, PK.p + (size_t)col0 * ne,
-                           ne, qcol.p, c->st);
+                           ne, qcol.p, c->st, G, c->hs.on() ? c->hs.d_rext.p : nullptr);
             launch_tm_qsum(n, S, qcol.p, c->rad.p, c->xg, dsq.p, qsum.p, c->st);
             // merge the solutions to the origin: T-matrix columns of order q
             CK(cudaMemsetAsync(A0.p, 0, sizeof(zd) * (size_t)nb * S, c->st));

@@ -657,7 +657,11 @@ int bicg_multi(mstmg_ctx* c, MultiWork<T>& w, const cpx<T>* B, const std::vector
     } else {
         for (int k = 0; k < a; k++) CK(cudaMemsetAsync(v.X + (size_t)sys[k] * ne, 0, sizeof(cpx<T>) * ne, c->st));
     }
-    launch_m_init<T>(sm, an, ne, a, w.act.p, B, v, w.YP.p, have_x0 ? 1 : 0, w.part.p, w.sc.p, c->nsm, c->st);
+    // host spheres (FP64): the Mie multiply runs apart, the fused kernels take an = null
+    const bool hosts = sizeof(T) == 8 && c->hs.on();
+    if (hosts && have_x0)
+        for (int k = 0; k < a; k++) mie_all(c, 1, 0, (const zd*)(w.YP.p + (size_t)k * ne), (zd*)(w.YP.p + (size_t)k * ne));
+    launch_m_init<T>(sm, hosts ? nullptr : an, ne, a, w.act.p, B, v, w.YP.p, have_x0 ? 1 : 0, w.part.p, w.sc.p, c->nsm, c->st);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(w.hsc.data(), w.sc.p, sizeof(BicgScalars) * w.S, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -677,9 +681,14 @@ int bicg_multi(mstmg_ctx* c, MultiWork<T>& w, const cpx<T>* B, const std::vector
     if ((rc = compact())) return rc;
     for (int it = 1; it <= niter && a > 0; it++) {
         int apad = ((a + per_chunk - 1) / per_chunk) * per_chunk;
-        launch_m_pack<T>(sm, an, ne, a, apad, w.act.p, v.P, v.W, w.XP.p, c->nsm, c->st);
+        launch_m_pack<T>(sm, hosts ? nullptr : an, ne, a, apad, w.act.p, v.P, v.W, w.XP.p, c->nsm, c->st);
+        if (hosts)
+            for (int k = 0; k < a; k++)
+                mie_all(c, -1, 0, (const zd*)(w.XP.p + (size_t)(2 * k + 1) * ne), (zd*)(w.XP.p + (size_t)(2 * k + 1) * ne));
         if ((rc = translate_many<T>(c, w.XP.p, w.YP.p, 2 * apad, 2u))) return rc;
-        launch_m_post<T>(sm, an, ne, a, w.act.p, v, w.YP.p, w.part.p, w.sc.p, c->nsm, c->st, w.cnt.p);
+        if (hosts)
+            for (int k = 0; k < a; k++) mie_all(c, 1, 0, (const zd*)(w.YP.p + (size_t)(2 * k) * ne), (zd*)(w.YP.p + (size_t)(2 * k) * ne));
+        launch_m_post<T>(sm, hosts ? nullptr : an, ne, a, w.act.p, v, w.YP.p, w.part.p, w.sc.p, c->nsm, c->st, w.cnt.p);
         launch_m_upd<T>(ne, a, w.act.p, v, w.part.p, w.sc.p, w.epsv.p, c->nsm, c->st, w.cnt.p);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(w.hsc.data(), w.sc.p, sizeof(BicgScalars) * w.S, cudaMemcpyDeviceToHost, c->st));

@@ -321,9 +321,15 @@ __global__ void __launch_bounds__(MB) m_pack_kernel(SlotMaps sm, const cpx<T>* a
         SlotPos q = slot_pos(sm, e);
         xp[q.b0] = p[q.b0];
         xp[q.b1] = p[q.b1];
-        // A^T conj(w)  (multmiecoeffmult with idir /= 1 on the conjugated vector)
-        const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+        // A^T conj(w)  (multmiecoeffmult with idir /= 1 on the conjugated
+        // vector); an == null: conj(w) alone (the host-sphere multiply follows)
         cpx<T> x0 = cj(w[q.b0]), x1 = cj(w[q.b1]);
+        if (!an) {
+            xw[q.b0] = x0;
+            xw[q.b1] = x1;
+            continue;
+        }
+        const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
         xw[q.b0] = A[0] * x0 + A[1] * x1;
         xw[q.b1] = A[2] * x0 + A[3] * x1;
     }
@@ -342,10 +348,14 @@ __global__ void __launch_bounds__(MB) m_init_kernel(SlotMaps sm, const cpx<T>* a
         SlotPos q = slot_pos(sm, e);
         cpx<T> m[2] = {mk((T)0, (T)0), mk((T)0, (T)0)};
         if (have_y) {
-            const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
             cpx<T> u0 = y[q.b0], u1 = y[q.b1];
-            m[0] = A[0] * u0 + A[2] * u1;
-            m[1] = A[1] * u0 + A[3] * u1;
+            m[0] = u0;   // an == null: y already holds M H x
+            m[1] = u1;
+            if (an) {
+                const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+                m[0] = A[0] * u0 + A[2] * u1;
+                m[1] = A[1] * u0 + A[3] * u1;
+            }
         }
         const int bb[2] = {q.b0, q.b1};
         for (int h = 0; h < 2; h++) {
@@ -452,10 +462,13 @@ __global__ void __launch_bounds__(MB) m_post_kernel(SlotMaps sm, const cpx<T>* a
     double acc[2] = {0.0, 0.0};
     for (int e = blockIdx.x * MB + threadIdx.x; e < sm.nslots; e += gridDim.x * MB) {
         SlotPos q = slot_pos(sm, e);
-        const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
         cpx<T> u0 = y0[q.b0], u1 = y0[q.b1];
-        cpx<T> m0 = A[0] * u0 + A[2] * u1;
-        cpx<T> m1 = A[1] * u0 + A[3] * u1;
+        cpx<T> m0 = u0, m1 = u1;   // an == null: y0 already holds M H p
+        if (an) {
+            const cpx<T>* A = an + sm.mie_offset[q.i] + 4 * (q.n - 1);
+            m0 = A[0] * u0 + A[2] * u1;
+            m1 = A[1] * u0 + A[3] * u1;
+        }
         cpx<T> c0 = v.P[o + q.b0] - m0, c1 = v.P[o + q.b1] - m1;
         v.CAP[o + q.b0] = c0;
         v.CAP[o + q.b1] = c1;
@@ -650,15 +663,18 @@ __global__ void tm_rhs_kernel(int l, zd* P0)
 
 // lrsphereqeff (scatprops:676-776) with npol = 1 for one (sphere, column);
 // g = A^{-1} a as in qefficiencyfactors (scatprops:782-870, no host spheres).
+// G (may be null): the exciting fields of the columns (host spheres: the
+// interaction without the Mie multiply plus the incident field), else
+// A^{-1} a; rext (may be null): the index around each sphere, else rimed
 __global__ void tm_qeff_kernel(int nsph, int ncols, const int* order, const int* offset, const int* mie_offset, const double* radius,
-                               zd rimed, const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol)
+                               zd rimed, const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol, const zd* G, const double* rext)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nsph * ncols) return;
     const int c = t / nsph, i = t - c * nsph;
     const int L = order[i], off = offset[i], hb = L * (L + 2);
     const double xsp = radius[i];
-    const zd ri0 = rimed;
+    const zd ri0 = rext ? mk(rext[2 * i], rext[2 * i + 1]) : rimed;
     const zd xri = xsp * ri0;
     const zd rib = cdivr(2.0, cdivr(1.0, ri0) + cdivr(1.0, ri0));
     zd psi[MSTMG_LMAX + 2], xi[MSTMG_LMAX + 2], scr[2 * (MSTMG_LMAX + 2)];   // sphere orders are at most MSTMG_LMAX
@@ -686,6 +702,11 @@ __global__ void tm_qeff_kernel(int nsph, int ncols, const int* order, const int*
             int a0 = aidx(m, n, 0, L);
             zd av[2] = {a[a0], a[a0 + hb]};
             zd gv[2] = {Ain[0] * av[0] + Ain[2] * av[1], Ain[1] * av[0] + Ain[3] * av[1]};
+            if (G) {
+                const zd* gc = G + (size_t)c * ld + off;
+                gv[0] = gc[a0];
+                gv[1] = gc[a0 + hb];
+            }
             zd fv[2] = {f[a0], f[a0 + hb]};
             for (int s = 0; s < 2; s++)
                 for (int u = 0; u < 2; u++) {
@@ -905,10 +926,10 @@ void launch_tm_rhs(int l, zd* P0, cudaStream_t st)
     launch_counter() += 1;
 }
 void launch_tm_qeff(int nsph, int ncols, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed,
-                    const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol, cudaStream_t st)
+                    const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol, cudaStream_t st, const zd* G, const double* rext)
 {
     int tot = nsph * ncols;
-    tm_qeff_kernel<<<(tot + 63) / 64, 64, 0, st>>>(nsph, ncols, order, offset, mie_offset, radius, rimed, an_inv, A, P, ld, qcol);
+    tm_qeff_kernel<<<(tot + 63) / 64, 64, 0, st>>>(nsph, ncols, order, offset, mie_offset, radius, rimed, an_inv, A, P, ld, qcol, G, rext);
     launch_counter() += 1;
 }
 void launch_tm_qsum(int nsph, int ncols, const double* qcol, const double* radius, double xv, double* sq, double* qsum, cudaStream_t st)

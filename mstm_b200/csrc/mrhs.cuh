@@ -124,7 +124,8 @@ void launch_eg_combine_dev(int ne, int ldv, int S, int m1, int a, const int* act
 void launch_tm_rhs(int l, zd* P0, cudaStream_t st);
 // per-column, per-sphere efficiencies (qefficiencyfactors with npol = 1): qcol[3 (i + N c)]
 void launch_tm_qeff(int nsph, int ncols, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed,
-                    const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol, cudaStream_t st);
+                    const zd* an_inv, const zd* A, const zd* P, int ld, double* qcol, cudaStream_t st, const zd* G = nullptr,
+                    const double* rext = nullptr);
 // sphere_qeff(3,N) += sum over the columns (fixed order); qsum[0..2] = sum_i sphere_qeff r_i^2 / xv^2
 void launch_tm_qsum(int nsph, int ncols, const double* qcol, const double* radius, double xv, double* sphere_qeff, double* qsum,
                     cudaStream_t st);

@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(PP_NT) merge_kernel(MergeArgs a)
     const int p0 = blockIdx.y * MERGE_PC, np = min(MERGE_PC, a.npol - p0);
     if (np <= 0) return;
     for (int i = blockIdx.x; i < a.nsph; i += gridDim.x) {
-        if (!dist && a.active && !a.active[i]) continue;   // uniform over the CTA
+        if (a.active && !a.active[i]) continue;   // uniform over the CTA
         const int Li = a.order[i];
         const int L = dist ? T : Li;                       // source order
         const int nt = dist ? Li : min(T, a.tord[i]);      // target order

@@ -34,7 +34,7 @@ struct MergeArgs {
     const double* bcofd;
     zd* scratch;
     size_t scratch_stride;  // zd units per CTA
-    const int* active = nullptr;   // mode 0 with host spheres: 1 for the spheres merged (those outside every other)
+    const int* active = nullptr;   // with host spheres: 1 for the spheres merged or distributed to (those outside every other)
 };
 
 size_t tranorder_scratch(int nsph, int sstride);   // complex values of scratch launch_tranorder needs

@@ -2292,6 +2292,7 @@ void orc_distribute_from_common_origin(const orc_ctx *c, int nodrt, const cplx *
     for (int k = 0; k < c->neqns; k++) amnp[k] = 0;
     axialtrancoefinit(imax(nodrt, c->max_order));
     for (int i = 0; i < c->n; i++) {
+        if (c->host[i] >= 0) continue;   /* origin_host 0: the spheres outside every other (scatprops:631) */
         int noi = c->order[i];
         double rv[3] = {c->pos[3 * i] - r0[0], c->pos[3 * i + 1] - r0[1], c->pos[3 * i + 2] - r0[2]};
         pairop_t op;
@@ -2311,6 +2312,8 @@ void orc_distribute_from_common_origin(const orc_ctx *c, int nodrt, const cplx *
  * efficiencies of every column (qefficiencyfactors with npol=1) are summed in
  * sphere_qeff(3,N); the order loop stops after the order at which the
  * summed extinction changes by less than conveps (qeff(1) - qeffold(1), signed).
+ * With host spheres the excitation reaches the spheres outside every other
+ * only, and the sum runs over every sphere (exlist all true, solver:266-271).
  * Returns istat; *order_used = the T-matrix order kept (t_matrix_order). */
 int orc_tmatrix_solution(orc_ctx *c, int tmo, const int *trans_order, const double *r0, double solneps, double conveps,
                          int niter, cplx *tmat, double *sphere_qeff, int *order_used, int *maxiter_o, double *maxerr_o)
@@ -2343,13 +2346,21 @@ int orc_tmatrix_solution(orc_ctx *c, int tmo, const int *trans_order, const doub
                 if (iter > niter || serr > solneps) istat = 1;
             }
             initialize = 0;
-            /* qefficiencyfactors(npol=1): the first-polarisation terms of lrsphereqeff */
-            for (int i = 0; i < c->n; i++)
-                mie_mult_sphere(c->an_inv + c->mie_offset[i], c->order[i], 1, amnpkq + c->offset[i], gmnp + c->offset[i]);
+            /* qefficiencyfactors(npol=1): the first-polarisation terms of
+             * lrsphereqeff; with host spheres the exciting field is the
+             * interaction without the Mie multiply plus the incident field */
+            if (c->nhosted == 0) {
+                for (int i = 0; i < c->n; i++)
+                    mie_mult_sphere(c->an_inv + c->mie_offset[i], c->order[i], 1, amnpkq + c->offset[i], gmnp + c->offset[i]);
+            } else {
+                int zero = 0;
+                sphereinteraction_ex(c, 1, amnpkq, gmnp, &zero, &zero, 0, 0);
+                for (int e = 0; e < neq; e++) gmnp[e] += pmnpkq[e];
+            }
             for (int i = 0; i < c->n; i++) {
                 double qe[3], qs[3], qa[3];
                 int off = c->offset[i];
-                lrsphereqeff(c->rimed, c->order[i], c->rad[i], amnpkq + off, 0, pmnpkq + off, gmnp + off, qe, qs, qa);
+                lrsphereqeff(c->rext[i], c->order[i], c->rad[i], amnpkq + off, 0, pmnpkq + off, gmnp + off, qe, qs, qa);
                 sphere_qeff[3 * i] += qe[0];
                 sphere_qeff[3 * i + 1] += qa[0];
                 sphere_qeff[3 * i + 2] += qs[0];

@@ -7,14 +7,16 @@ concentric in a shell is the coated sphere of Aden and Kerker (written here
 from the published formulas with scipy's spherical Bessel functions), and a
 host whose index matches the medium is transparent (the spheres inside it
 scatter and absorb as the same cluster in free space, with the same
-scattering matrix) -- and by its BiCG
+scattering matrix), and the coated sphere's T matrix averages to its Qext and
+Qsca -- and by its BiCG
 against its dense solve.  GPU: the device path against the oracle on a
 cluster with two host levels, coincident and offset centres, small spheres
 on the dense path and spheres outside: host map, orders, layout, Mie
 coefficients (1e-12), sphereinteraction in every argument form (1e-12), the
 FP64 solves (same iterations, efficiencies to 1e-9), the mixed solve (1e-6),
-the scattering matrix (1e-9 of S11's largest value) and the refusals of the
-entry points built for spheres in the medium.
+the scattering matrix (1e-9 of S11's largest value), the cluster T matrix
+(1e-9 FP64, 1e-6 mixed) and the refusals of the entry points built for
+spheres in the medium.
 """
 import numpy as np
 import pytest
@@ -125,6 +127,21 @@ def test_oracle_index_matched_host_is_transparent(oracle_mod):
     assert abs(sh["g"] - sf["g"]) <= 1e-7 * abs(sf["g"])
 
 
+def test_oracle_coated_sphere_t_matrix(oracle_mod):
+    """The T matrix of a coated sphere (the core's excitation reaches it
+    through the shell's internal field only): its orientation-averaged Qext
+    and Qsca are the Aden-Kerker ones."""
+    x, y, m1, m2 = 1.2, 2.0, 1.6 + 0.05j, 1.33 + 0.01j
+    o = oracle_mod.Oracle([[0, 0, 0], [0, 0, 0]], [y, x], [m2, m1], mie_eps=-10)
+    r = o.tmatrix_solution(solution_eps=1e-20, convergence_eps=1e-12, maxt=10)
+    u = r["order"]
+    nb = 2 * u * (u + 2)
+    qe, qs = oracle_mod.tmatrix_qext_qsca(u, np.asfortranarray(r["tmat"][:nb, :nb]), y)
+    qe0, qs0 = coated_sphere(x, y, m1, m2, 10)
+    # T entries are single precision in the orientation average
+    assert abs(qe / qe0 - 1) < 1e-7 and abs(qs / qs0 - 1) < 1e-7
+
+
 def test_oracle_host_bicg_matches_dense_solve(oracle_mod):
     pos, rad, ri = host_cluster()
     o = oracle_mod.Oracle(pos, rad, ri, mie_eps=1e-6)
@@ -223,6 +240,29 @@ def test_host_scattering_matrix(pair):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_host_t_matrix(pair, precision):
+    """tmatrix_solution with host spheres: the excitation distributed to the
+    spheres outside every other, the per-column efficiencies through the
+    interaction, the merge of the outside spheres; FP64 against the oracle to
+    1e-9 (T matrix, sums, order kept), mixed GMRES to 1e-6."""
+    from mstm_b200 import api
+    _, o = pair
+    pos, rad, ri = host_cluster()
+    g = api.SphereCluster(pos, rad, ri, mie_epsilon=1e-6, precision=precision)
+    ro = o.tmatrix_solution(convergence_eps=1e-6, solution_eps=1e-12 if precision == "fp64" else 1e-16)
+    T = g.t_matrix_order()
+    assert T == ro["tmo"]
+    rg = g.tmatrix_solution(T, solution_eps=1e-12, convergence_eps=1e-6)
+    assert rg["istat"] == 0 and rg["order"] == ro["order"]
+    tol = 1e-9 if precision == "fp64" else 1e-6
+    assert np.abs(rg["tmat"] - ro["tmat"]).max() <= tol * np.abs(ro["tmat"]).max()
+    assert np.abs(rg["qtot"] - ro["qtot"]).max() <= tol * ro["qtot"][0]
+    assert np.abs(rg["sphere_qeff"] - ro["sphere_qeff"]).max() <= tol * np.abs(ro["sphere_qeff"]).max()
+    g.close()
+
+
+@pytest.mark.gpu
 def test_host_solver_modes(pair):
     """niter 0 (the host couplings applied twice, solver:509-518) and the
     order-of-scattering iteration (niter < 0)."""
@@ -268,8 +308,6 @@ def test_host_contexts_refuse_the_medium_only_paths(pair):
     with pytest.raises(MstmgError):
         m.fixedorsoln(eps=1e-8)
     m.close()
-    with pytest.raises(MstmgError):
-        g.tmatrix_solution(4)
     with pytest.raises(MstmgError):
         g.fft_setup(d_cell=2.0)
     with pytest.raises(MstmgError):
