@@ -13,9 +13,10 @@ solver path through the library:
   fft_translation_option  the FFT translation for clusters of at least
                       min_fft_nsphere spheres (input:1114)
 
-Options outside this path (plane boundaries, periodic lattices, host spheres,
-near fields, Gaussian beams, random configurations, ...) are rejected with a
-clear error rather than ignored.
+Spheres inside other spheres are detected by the library (host spheres) and
+solved with their couplings.  Options outside this path (plane boundaries,
+periodic lattices, near fields, Gaussian beams, random configurations, ...)
+are rejected with a clear error rather than ignored.
 
     python -m mstm_b200.inputfile run.inp [--precision fp64|mixed]
 """
@@ -327,8 +328,11 @@ def execute(run, precision="fp64"):
     out = dict(number_spheres=len(rad), neqns=g.number_eqns, vol_radius=g.vol_radius, medium=med,
                max_mie_order=int(g.sphere_order.max()), run_number=run.get("_run_number", 1))
     _, mqe, mqa = g.miecoefcalc()
+    host, nh = g.host_spheres()
+    if nh > 0:
+        out["host"] = host
     from .output import mean_mie
-    out["mean_mie"] = mean_mie(rad, mqe, mqa)
+    out["mean_mie"] = mean_mie(rad, mqe, mqa, host if nh > 0 else None)
     t0 = time.perf_counter()
     try:
         if run["fft_translation_option"] and len(rad) >= run["min_fft_nsphere"]:

@@ -61,24 +61,30 @@ def listed_int(n):
 
 
 # ---- geometry and Mie summaries as the reference forms them -------------------
-def cluster_radii(pos, rad):
+def cluster_radii(pos, rad, host=None):
     """(volume radius, area-mean radius, circumscribing radius) as spheredata's
     set-up forms them (mstm-modules-33.f90:5257-5379): circumscribing about the
-    mean sphere position."""
+    mean position of the spheres outside every other; the volume and
+    area-mean radii over those spheres (host: the holding sphere of each
+    sphere, -1 for none; None: every sphere is outside)."""
     pos = np.asarray(pos, np.float64).reshape(-1, 3)
     rad = np.asarray(rad, np.float64)
-    vol = float(np.sum(rad ** 3) ** (1.0 / 3.0))
-    area = float(math.sqrt(np.mean(rad ** 2)))
-    org = pos.mean(axis=0)
+    out = np.ones(len(rad), bool) if host is None else (np.asarray(host) < 0)
+    vol = float(np.sum(rad[out] ** 3) ** (1.0 / 3.0))
+    area = float(math.sqrt(np.mean(rad[out] ** 2)))
+    org = pos[out].mean(axis=0)
     circ = float(np.max(np.sqrt(((pos - org) ** 2).sum(axis=1)) + rad))
     return vol, area, circ
 
 
-def mean_mie(rad, qext, qabs):
-    """Area-weighted mean Mie efficiencies (mstm-modules-33.f90:5364-5379)."""
+def mean_mie(rad, qext, qabs, host=None):
+    """Area-weighted mean Mie efficiencies of the spheres outside every other
+    (mstm-modules-33.f90:5364-5379)."""
     rad = np.asarray(rad, np.float64)
-    a2 = float(np.mean(rad ** 2))
-    return float(np.sum(np.asarray(qext) * rad ** 2) / a2 / len(rad)), float(np.sum(np.asarray(qabs) * rad ** 2) / a2 / len(rad))
+    out = np.ones(len(rad), bool) if host is None else (np.asarray(host) < 0)
+    r, qe, qa = rad[out], np.asarray(qext)[out], np.asarray(qabs)[out]
+    a2 = float(np.mean(r ** 2))
+    return float(np.sum(qe * r ** 2) / a2 / len(r)), float(np.sum(qa * r ** 2) / a2 / len(r))
 
 
 def scaled_scat_mat(s):
@@ -110,7 +116,8 @@ def run_variables(run, out):
     from .inputfile import cluster_arrays, medium_index
     pos, rad, ri = cluster_arrays(run)
     n = len(rad)
-    vol, area, circ = cluster_radii(pos, rad)
+    host = out.get("host")
+    vol, area, circ = cluster_radii(pos, rad, host)
     med = medium_index(run)
     L = ["*" * 52, label(f"input variables for run {iw(out.get('run_number', 1), 5)}")]
     L += [label("sphere data input file:"), run["sphere_data_input_file"] or ""]
@@ -124,7 +131,8 @@ def run_variables(run, out):
         L += [label("sphere properties and associations"),
               label("  sphere    host   layer radius     x       y       z           ref indx")]
         for i in range(n):
-            L.append(iw(i + 1, 8) + iw(0, 8) + iw(0, 8) + fd(rad[i], 8, 3) + fd(pos[i, 0], 8, 3) + fd(pos[i, 1], 8, 3)
+            h = 0 if host is None else int(host[i]) + 1   # 1-based, 0 outside every sphere
+            L.append(iw(i + 1, 8) + iw(h, 8) + iw(0, 8) + fd(rad[i], 8, 3) + fd(pos[i, 0], 8, 3) + fd(pos[i, 1], 8, 3)
                      + fd(pos[i, 2], 8, 3) + es(ri[i].real) + es(ri[i].imag))
     if out["kind"] == "random_orientation":
         L += [label("random orientation, estimated t matrix order:"), iw(out["t_matrix_order_estimate"], 6)]

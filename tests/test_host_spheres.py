@@ -331,3 +331,39 @@ def test_moving_a_sphere_inside_another_needs_a_new_context():
         g.set_positions(moved)
     g.set_positions(pos + 0.25)    # still outside: accepted
     g.close()
+
+
+COATED_DECK = """! a coated sphere: core concentric in a shell, read as host spheres
+number_spheres
+2
+sphere_data
+0.d0,0.d0,0.d0,2.d0,(1.33d0,0.01d0)
+0.d0,0.d0,0.d0,1.2d0,(1.6d0,0.05d0)
+end_of_sphere_data
+mie_epsilon
+-14.d0
+solution_epsilon
+1.d-16
+incident_beta_deg
+0.d0
+end_of_options
+"""
+
+
+@pytest.mark.gpu
+def test_coated_sphere_deck():
+    """An input deck with a core inside a shell runs through the library's
+    host-sphere path: Qext and Qsca are the Aden-Kerker values, the run's
+    sphere table names the host."""
+    from mstm_b200 import inputfile as I
+    from mstm_b200.output import run_variables
+    run = I.parse(COATED_DECK)[0]
+    out = I.execute(run, "fp64")
+    qe, qs = coated_sphere(1.2, 2.0, 1.6 + 0.05j, 1.33 + 0.01j, 14)
+    xg = out["vol_radius"]
+    assert abs(out["qtot"][0, 0] * xg ** 2 / (qe * 4.0) - 1) < 1e-9
+    assert abs(out["qtot"][2, 0] * xg ** 2 / (qs * 4.0) - 1) < 1e-9
+    assert list(out["host"]) == [-1, 0]
+    L = run_variables(run, out)
+    i = L.index(" sphere properties and associations")
+    assert L[i + 3][:16] == "       2       1"
