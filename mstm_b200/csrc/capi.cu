@@ -174,16 +174,18 @@ int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const std::v
 {
     std::vector<long long> off(np > 0 ? np : 1);
     long long u = 0;
-    int maxrec = 4, pl = 1;
+    int maxrec = 4, pl = 1, lo = 1 << 30;
     for (int t = 0; t < np; t++) {
         off[t] = u;
         int rec = op_record_units(c->order[pr[t].x], c->order[pr[t].y]);
         maxrec = std::max(maxrec, rec);
         pl = std::max(pl, std::max(c->order[pr[t].x], c->order[pr[t].y]));
+        lo = std::min(lo, std::min(c->order[pr[t].x], c->order[pr[t].y]));
         u += rec;
     }
     c->npairs = np;
     c->pair_lmax = pl;
+    c->pair_uniform = np > 0 && lo == pl;
     c->tiles_host = tl;
     if (!c->tiled) {   // shards need tiles; a re-layout without them drops the shard
         c->shard = 0;

@@ -226,6 +226,7 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
     a.nrhs = nrhs;
     a.contran = contran;
     a.lmax = c->pair_lmax;
+    a.uniform = c->pair_uniform ? 1 : 0;
     a.maxrec = c->maxrec;
     a.err = c->err.p;
     TiledArgs<T> ta;

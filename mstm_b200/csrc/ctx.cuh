@@ -324,6 +324,7 @@ struct mstmg_ctx {
     unsigned long long layout_gen = 0;
     int n = 0, neqns = 0, lmax = 0, npairs = 0, maxrec = 0;
     int pair_lmax = 0;   // largest order among the spheres of the rotation pairs (the order-generic kernel's strides)
+    bool pair_uniform = false;   // every rotation pair has both orders pair_lmax
     long long op_units = 0;
     double xg = 1.0;
     std::vector<int> order, offset, mie_offset;

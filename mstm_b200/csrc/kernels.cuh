@@ -42,6 +42,7 @@ template <typename T> struct TransArgs {
     int lmax;                // largest order (smem strides)
     int maxrec;              // largest operator record, storage units
     int* err;
+    int uniform = 0;         // 1: every pair has both orders lmax
 };
 template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cudaStream_t st);
 template <typename T> size_t translate_smem_bytes(int lmax, int nrhs, int maxrec);

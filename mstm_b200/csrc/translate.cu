@@ -59,8 +59,9 @@ template <typename T> __device__ __forceinline__ void atomic_add_c(cpx<T>* p, cp
 template <typename T> __device__ __forceinline__ cpx<T> ldc(const cpx<T>* p) { return *p; }
 
 // LM: the largest order among the launch's pairs, a compile-time constant so
-// that the index decodes of every phase are multiplications, not divisions
-template <typename T, int NT, int LM> __global__ void __launch_bounds__(NT) translate_kernel(TransArgs<T> a)
+// that the index decodes of every phase are multiplications, not divisions;
+// UNI: every pair has both orders LM (the order tests fold away)
+template <typename T, int NT, int LM, bool UNI> __global__ void __launch_bounds__(NT) translate_kernel(TransArgs<T> a)
 {
     extern __shared__ __align__(128) unsigned char sm[];
     const int tid = threadIdx.x;
@@ -112,7 +113,7 @@ template <typename T, int NT, int LM> __global__ void __launch_bounds__(NT) tran
         }
         const T* rec = opb + (size_t)b * a.maxrec;
         const int i = a.pairs[q].x, j = a.pairs[q].y;
-        const int noi = a.order[i], noj = a.order[j];
+        const int noi = UNI ? LM : a.order[i], noj = UNI ? LM : a.order[j];
         const int nmin = noi < noj ? noi : noj, nmax = noi > noj ? noi : noj;
         if (noi != prev_noi || noj != prev_noj) {
             if (tid <= lm + 1) {
@@ -287,10 +288,10 @@ template <typename T> size_t translate_smem_bytes(int lmax, int nrhs, int maxrec
     return head + ops + bufs;
 }
 
-template <typename T, int NT, int LM> static void launch_translate_lm(const TransArgs<T>& a, int nsm, cudaStream_t st)
+template <typename T, int NT, int LM, bool UNI = false> static void launch_translate_lm(const TransArgs<T>& a, int nsm, cudaStream_t st)
 {
     size_t smem = translate_smem_bytes<T>(LM, a.nrhs, a.maxrec);
-    auto kern = translate_kernel<T, NT, LM>;
+    auto kern = translate_kernel<T, NT, LM, UNI>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // as many CTAs per SM as registers and shared memory allow
     int per_sm = 0;
@@ -312,6 +313,15 @@ template <typename T, int NT, int LM> static void launch_translate_lm(const Tran
 template <typename T> void launch_translate(const TransArgs<T>& a, int nsm, cudaStream_t st)
 {
     static_assert(MSTMG_LMAX == 16, "one instance per order up to MSTMG_LMAX");
+    if (a.uniform) {
+        switch (a.lmax) {
+        case 3: launch_translate_lm<T, 64, 3, true>(a, nsm, st); return;
+        case 4: launch_translate_lm<T, 64, 4, true>(a, nsm, st); return;
+        case 5: launch_translate_lm<T, 64, 5, true>(a, nsm, st); return;
+        case 6: launch_translate_lm<T, 64, 6, true>(a, nsm, st); return;
+        default: break;
+        }
+    }
     switch (a.lmax) {
     case 1: launch_translate_lm<T, 64, 1>(a, nsm, st); break;
     case 2: launch_translate_lm<T, 64, 2>(a, nsm, st); break;
