@@ -398,6 +398,18 @@ int setup_layout(mstmg_ctx* c)
         CK(cudaMemcpyAsync(h.d_hoff.p, hoff.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
         CK(cudaMemcpyAsync(h.d_outside.p, outside.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
         CK(cudaMemcpyAsync(h.d_host.p, h.host.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+        std::vector<int> hst(n + 1, 0), held;
+        for (int i = 0; i < n; i++)
+            if (h.host[i] >= 0) hst[h.host[i] + 1]++;
+        for (int i = 0; i < n; i++) hst[i + 1] += hst[i];
+        held.assign(std::max(hst[n], 1), 0);
+        std::vector<int> fill(hst.begin(), hst.end() - 1);
+        for (int j = 0; j < n; j++)
+            if (h.host[j] >= 0) held[fill[h.host[j]]++] = j;
+        CK(h.d_hstart.alloc(n + 1));
+        CK(h.d_held.alloc(held.size()));
+        CK(cudaMemcpy(h.d_hstart.p, hst.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h.d_held.p, held.data(), sizeof(int) * held.size(), cudaMemcpyHostToDevice));
     }
     launch_mie_coefs(n, c->rad.p, c->ri.p, c->opts.medium_re, c->opts.medium_im, hs.on() ? hs.d_rext.p : nullptr, c->d_order.p,
                      c->d_mie_offset.p, hs.on() ? hs.d_hoff.p : nullptr, c->an.p, c->an_inv.p, c->an32.p, c->hs.dn.p, c->hs.un.p,

@@ -30,7 +30,7 @@ static int qeff_ctx(mstmg_ctx* c, const zd* amnp)
     }
     launch_qeff(c->n, c->d_order.p, c->d_offset.p, c->d_mie_offset.p, c->rad.p, mk(c->opts.medium_re, c->opts.medium_im), c->an_inv.p,
                 amnp, c->pmnp.p, ne, c->qeff.p, c->xg, c->qtot.p, c->st, c->hs.on() ? c->hs.d_rext.p : nullptr, g,
-                c->hs.on() ? c->hs.d_host.p : nullptr, c->hs.on() ? c->hs.qv.p : nullptr);
+                c->hs.on() ? c->hs.d_host.p : nullptr, c->hs.on() ? c->hs.qv.p : nullptr, c->hs.d_hstart.p, c->hs.d_held.p);
     CK(cudaGetLastError());
     return MSTMG_OK;
 }

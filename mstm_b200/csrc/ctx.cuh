@@ -298,6 +298,7 @@ struct HostSpheres {
     std::vector<double> rext;    // per sphere: re, im of the index around it (exteriorrefindex)
     DevBuf<double> d_rext, qv, xpos;   // xpos: positions of the device sphere arrays (internal blocks at their host's centre)
     DevBuf<int> d_host, d_hoff, d_outside;   // holding sphere; offset of the internal block (-1 none); 1 outside every sphere
+    DevBuf<int> d_hstart, d_held;            // the spheres each sphere holds: held[hstart[i] .. hstart[i+1])
     DevBuf<zd> dn, un, vn;       // the holding spheres' D, U, V Mie coefficients (mie_offset)
     DevBuf<zf> dn32, un32, vn32; // the same in FP32 (the mixed solver's passes)
     DevBuf<double> pmed, dmed;   // the index of each same-host pair's medium: rotation pairs, dense pairs

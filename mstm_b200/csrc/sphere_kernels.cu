@@ -579,23 +579,28 @@ void launch_qtot_configs(int nc, const int* cfg_start, const double* radius, con
 // both scaled by the area ratio, written into qeff's absorption rows as the
 // reference does; the totals over the spheres outside every other.
 // qv: scratch of 3 nsph doubles.
-__global__ void __launch_bounds__(QTOT_NT) qtot_hosts_kernel(int nsph, const double* radius, const int* host, double* qeff, double* qv,
-                                                             double xg, double* qtot)
+// held[hstart[i] .. hstart[i+1]): the spheres sphere i holds, in order
+__global__ void __launch_bounds__(QTOT_NT) qtot_hosts_kernel(int nsph, const double* radius, const int* host, const int* hstart,
+                                                             const int* held, double* qeff, double* qv, double xg, double* qtot)
 {
     __shared__ double red[9][QTOT_NT];
     for (int i = threadIdx.x; i < nsph; i += QTOT_NT)
         for (int p = 0; p < 3; p++) {
             double v = qeff[1 + 3 * (p + 3 * i)];
-            for (int j = 0; j < nsph; j++)
-                if (host[j] == i) v = v - qeff[1 + 3 * (p + 3 * j)] * radius[j] * radius[j] / (radius[i] * radius[i]);
+            for (int q = hstart[i]; q < hstart[i + 1]; q++) {
+                const int j = held[q];
+                v = v - qeff[1 + 3 * (p + 3 * j)] * radius[j] * radius[j] / (radius[i] * radius[i]);
+            }
             qv[p + 3 * i] = v;
         }
     __syncthreads();
     for (int i = threadIdx.x; i < nsph; i += QTOT_NT)
         for (int p = 0; p < 3; p++) {
             double v = qv[p + 3 * i];
-            for (int j = 0; j < nsph; j++)
-                if (host[j] == i) v = v + qv[p + 3 * j] * radius[j] * radius[j] / (radius[i] * radius[i]);
+            for (int q = hstart[i]; q < hstart[i + 1]; q++) {
+                const int j = held[q];
+                v = v + qv[p + 3 * j] * radius[j] * radius[j] / (radius[i] * radius[i]);
+            }
             qeff[1 + 3 * (p + 3 * i)] = v;
         }
     __syncthreads();
@@ -620,10 +625,10 @@ __global__ void __launch_bounds__(QTOT_NT) qtot_hosts_kernel(int nsph, const dou
 
 void launch_qeff(int nsph, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed, const zd* an_inv,
                  const zd* amnp, const zd* pmnp0, int ld, double* qeff, double xg, double* qtot, cudaStream_t st, const double* rext,
-                 const zd* gmnp, const int* host, double* qv)
+                 const zd* gmnp, const int* host, double* qv, const int* hstart, const int* held)
 {
     qeff_kernel<<<(nsph + 63) / 64, 64, 0, st>>>(nsph, order, offset, mie_offset, radius, rimed, an_inv, amnp, pmnp0, ld, qeff, rext, gmnp);
-    if (host) qtot_hosts_kernel<<<1, QTOT_NT, 0, st>>>(nsph, radius, host, qeff, qv, xg, qtot);
+    if (host) qtot_hosts_kernel<<<1, QTOT_NT, 0, st>>>(nsph, radius, host, hstart, held, qeff, qv, xg, qtot);
     else qtot_kernel<<<1, QTOT_NT, 0, st>>>(nsph, radius, qeff, xg, qtot);
     launch_counter() += 2;
 }

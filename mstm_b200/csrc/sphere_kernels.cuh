@@ -24,8 +24,9 @@ void launch_hmie(int nslots, int nreal, const int* slot_sphere, const int* order
 void launch_qtot_configs(int nc, const int* cfg_start, const double* radius, const double* qeff, const double* xg, double* qtot, cudaStream_t st);
 // with host spheres: rext the index around each sphere, gmnp the exciting
 // fields (interaction without the Mie multiply plus incident), host the
-// holding sphere (-1 none) and qv a scratch of 3 nsph doubles
+// holding sphere (-1 none), held[hstart[i] .. hstart[i+1]) the spheres
+// sphere i holds and qv a scratch of 3 nsph doubles
 void launch_qeff(int nsph, const int* order, const int* offset, const int* mie_offset, const double* radius, zd rimed,
                  const zd* an_inv, const zd* amnp, const zd* pmnp0, int ld, double* qeff, double xg, double* qtot,
                  cudaStream_t st, const double* rext = nullptr, const zd* gmnp = nullptr, const int* host = nullptr,
-                 double* qv = nullptr);
+                 double* qv = nullptr, const int* hstart = nullptr, const int* held = nullptr);
