@@ -109,7 +109,8 @@ static void find_hosts(mstmg_ctx* c, const std::vector<double>& ri)
     h.vid.assign(n, -1);
     h.rext.assign(2 * (size_t)n, 0.0);
     h.nhosted = h.nv = 0;
-    for (int i = 0; i < n; i++) {
+    const bool equal = std::all_of(c->radius.begin(), c->radius.end(), [&](double r) { return r == c->radius[0]; });
+    for (int i = 0; i < n && !equal; i++) {   // equal spheres hold none
         double xspmin = 1.0e6;
         for (int j = 0; j < n; j++) {
             if (!(c->radius[j] > c->radius[i])) continue;
