@@ -197,7 +197,7 @@ int upload_pairs(mstmg_ctx* c, const std::vector<int2>& pr, int np, const std::v
     c->maxrec = maxrec;
     // FP32 passes of the tiled path run the row kernel on row records unless
     // the rotation-tiled kernel is asked for (tile_pairs 1 or 2)
-    c->row32 = (c->tiled && c->opts.tile_pairs == 0 && rows_supported(c->lmax, 1)) ? row_record_units(c->lmax) : 0;
+    c->row32 = (c->tiled && c->opts.tile_pairs == 0 && rows_supported(c->tile_L, 1)) ? row_record_units(c->tile_L) : 0;
     c->layout_gen++;
     if (np > 0) {
         CK(c->pairs.alloc(np));
@@ -546,8 +546,27 @@ int setup_layout(mstmg_ctx* c)
         set_err("internal error: pair schedule incomplete");
         return MSTMG_ERR_ARG;
     }
+    c->tile_L = lm;
     c->tsph.release();   // block tiles
     c->pslot.release();
+    if (hs.on() && !c->opts.generic_kernel && np > 0) {
+        // host spheres: when the pairs inside the hosts all have one order
+        // the tiled kernels take them on grouped tiles (the spheres of each
+        // host in groups, each sphere's block at its own offset)
+        const int L0 = c->order[pr[0].x];
+        bool uni = true;
+        for (long long q = 0; q < np && uni; q++) uni = c->order[pr[q].x] == L0 && c->order[pr[q].y] == L0;
+        if (uni && L0 >= tso && tiled_supported(L0, 1)) {
+            std::vector<char> inp(n, 0);
+            for (long long q = 0; q < np; q++) inp[pr[q].x] = inp[pr[q].y] = 1;
+            std::vector<std::vector<int>> members(n + 1);   // by host, the spheres outside every other first
+            for (int i = 0; i < n; i++)
+                if (inp[i]) members[hs.host[i] + 1].push_back(i);
+            if (int rg = group_tiles(c, members, pr, tl)) return rg;
+            c->tiled = true;
+            c->tile_L = L0;
+        }
+    }
     (void)off;
     (void)maxrec;
     int rc_ = upload_pairs(c, pr, (int)np, tl);

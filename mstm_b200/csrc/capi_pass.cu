@@ -177,7 +177,7 @@ template <> const float* ops_ptr<float>(mstmg_ctx* c) { return c->op32.p; }
 template <typename T> static int rows_pass(mstmg_ctx*, const TiledArgs<T>&, int, int, unsigned) { return -1; }
 template <> int rows_pass<float>(mstmg_ctx* c, const TiledArgs<float>& tf, int nrhs, int nchunk, unsigned contran)
 {
-    if (rows_supported(c->lmax, nrhs)) return launch_translate_rows(tf, c->lmax, c->nsm, c->st);
+    if (rows_supported(c->tile_L, nrhs)) return launch_translate_rows(tf, c->tile_L, c->nsm, c->st);
     if (nchunk != 1) return -1;
     int rc = 0;
     for (int c0 = 0; c0 < nrhs && rc == 0;) {
@@ -187,7 +187,7 @@ template <> int rows_pass<float>(mstmg_ctx* c, const TiledArgs<float>& tf, int n
         tw.y = tf.y + (size_t)c0 * c->neqns;
         tw.nrhs = w;
         tw.contran = (contran >> c0) & ((1u << w) - 1u);
-        rc = launch_translate_rows(tw, c->lmax, c->nsm, c->st);
+        rc = launch_translate_rows(tw, c->tile_L, c->nsm, c->st);
         c0 += w;
     }
     return rc;
@@ -230,7 +230,10 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
     a.maxrec = c->maxrec;
     a.err = c->err.p;
     TiledArgs<T> ta;
-    bool use_tiled = c->tiled && (tiled_supported(c->lmax, nrhs) || (sizeof(T) == 4 && c->row32));
+    // FP64 passes of orders 3 and 4 run the order-generic kernel on the tile
+    // ordered pairs (faster there than the rotation-tiled kernel); FP32 passes
+    // take the row kernel from order 3
+    bool use_tiled = c->tiled && (sizeof(T) == 4 || c->tile_L >= 5) && (tiled_supported(c->tile_L, nrhs) || (sizeof(T) == 4 && c->row32));
     if (use_tiled) {
         ta.ntiles = c->ntiles;
         ta.tiles = c->tiles.p;
@@ -248,6 +251,7 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
         ta.tsph = c->tsph.p;
         ta.pslot = c->pslot.p;
         ta.pairs_per_step = c->opts.tile_pairs;
+        ta.soff = c->hs.on() ? c->d_offset.p : nullptr;
     }
     if (nchunk > 1 && !use_tiled) return MSTMG_ERR_UNSUPPORTED;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -266,7 +270,7 @@ template <typename T> int translate(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, in
             set_err("FP32 translation pass: no row-kernel configuration for this order and column count");
             return MSTMG_ERR_UNSUPPORTED;
         }
-    } else if (!use_tiled || launch_translate_tiled<T>(ta, c->lmax, c->nsm, c->st) != 0) {
+    } else if (!use_tiled || launch_translate_tiled<T>(ta, c->tile_L, c->nsm, c->st) != 0) {
         if (nchunk > 1) {
             if (e0) c->ev_pool.push_back(e0);
             if (e1) c->ev_pool.push_back(e1);
@@ -295,7 +299,7 @@ int fp32_chunk(mstmg_ctx* c, const zf* x, zf* y, int ncols, unsigned pattern2)
 {
     if (c->opts.fp32_chunk == 2 || c->opts.fp32_chunk == 4) return c->opts.fp32_chunk;
     if (c->chunk32 > 0) return c->chunk32;
-    if (!c->tiled || ncols < 4 || ncols % 4 != 0 || !tiled_supported(c->lmax, 2) || !tiled_supported(c->lmax, 4)) return 4;
+    if (!c->tiled || ncols < 4 || ncols % 4 != 0 || !tiled_supported(c->tile_L, 2) || !tiled_supported(c->tile_L, 4)) return 4;
     auto expand = [&](int w) {
         unsigned m = 0;
         for (int r = 0; r < w; r++)
@@ -341,7 +345,7 @@ int fp32_chunk(mstmg_ctx* c, const zf* x, zf* y, int ncols, unsigned pattern2)
 // pairs): the cases the dense TF32 images serve.
 bool tc_eligible(const mstmg_ctx* c)
 {
-    if (c->opts.tensor_core < 0 || c->tc_state < 0 || c->nshards > 1) return false;
+    if (c->opts.tensor_core < 0 || c->tc_state < 0 || c->nshards > 1 || c->hs.on()) return false;
     if (!c->tiled || c->ndense > 0 || (c->fft && c->fft->on) || c->npairs == 0) return false;
     return c->lmax >= 5 && tc_geom(c->lmax).NP <= 128;
 }
@@ -490,7 +494,7 @@ template <typename T> int translate_many(mstmg_ctx* c, const cpx<T>* x, cpx<T>* 
         }
         NR = fp32_chunk(c, x, y, ncols, pattern2);
     }
-    if (c->tiled && ncols > NR && ncols % NR == 0 && tiled_supported(c->lmax, NR)) {
+    if (c->tiled && (sizeof(T) == 4 || c->tile_L >= 5) && ncols > NR && ncols % NR == 0 && tiled_supported(c->tile_L, NR)) {
         int rc = translate<T>(c, x, y, NR, expand(NR), ncols / NR);
         if (rc != MSTMG_ERR_UNSUPPORTED) return rc;
     }
@@ -665,6 +669,85 @@ template <typename T> int fft_far(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int 
 
 // node_selection (fft:654-825) with target box = the sphere-centre extents,
 // the near-pair list, the node translations and the kernel spectra.
+// Grouped tiles (the tiled kernels' tiles over listed spheres): the spheres
+// of `members`, taken list by list, form groups of TILE_B; a tile holds the pairs
+// of pr between two groups (or inside one), its spheres listed by slot
+// (c->tsph) and each pair's slots (c->pslot).  pr is reordered tile by tile,
+// the pairs of a tile in slot-disjoint couples where it has them (the row
+// kernel runs such a couple as one step); tl gets the tiles.
+int group_tiles(mstmg_ctx* c, const std::vector<std::vector<int>>& members, std::vector<int2>& pr, std::vector<int4>& tl)
+{
+    const int B = TILE_B, n = c->n;
+    c->tsph.release();
+    c->pslot.release();
+    tl.clear();
+    std::vector<int> grp(n, -1), gs(n, 0);
+    int k = 0;
+    for (const auto& cm : members)
+        for (int i : cm) {
+            grp[i] = k / B;
+            gs[i] = k % B;
+            k++;
+        }
+    const long long ng = (k + B - 1) / B;
+    std::vector<int> gmem((size_t)std::max(ng, 1LL) * B, -1);
+    for (int i = 0; i < n; i++)
+        if (grp[i] >= 0) gmem[(size_t)grp[i] * B + gs[i]] = i;
+    std::vector<long long> key(pr.size());
+    std::vector<int> idx(pr.size());
+    for (size_t q = 0; q < pr.size(); q++) {
+        if (grp[pr[q].x] < 0 || grp[pr[q].y] < 0) {
+            set_err("internal error: a pair's sphere is in no tile group");
+            return MSTMG_ERR_ARG;
+        }
+        const long long ga = std::min(grp[pr[q].x], grp[pr[q].y]), gb = std::max(grp[pr[q].x], grp[pr[q].y]);
+        key[q] = ga * ng + gb;
+        idx[q] = (int)q;
+    }
+    std::stable_sort(idx.begin(), idx.end(), [&](int u, int v) { return key[u] < key[v]; });
+    std::vector<int2> pr2(pr.size());
+    std::vector<int> ts;
+    std::vector<short2> ps(pr.size());
+    size_t q = 0;
+    while (q < idx.size()) {
+        const long long kk = key[idx[q]];
+        const int ga = (int)(kk / ng), gb = (int)(kk % ng);
+        const size_t start = q;
+        for (int s = 0; s < B; s++) ts.push_back(gmem[(size_t)ga * B + s]);
+        for (int s = 0; s < B; s++) ts.push_back(ga == gb ? -1 : gmem[(size_t)gb * B + s]);
+        for (; q < idx.size() && key[idx[q]] == kk; q++) {
+            const int2 p2 = pr[idx[q]];
+            pr2[q] = p2;
+            const short si = (short)(grp[p2.x] == ga ? gs[p2.x] : B + gs[p2.x]);
+            const short sj = (short)(grp[p2.y] == ga ? gs[p2.y] : B + gs[p2.y]);
+            ps[q] = make_short2(si, sj);
+        }
+        for (size_t u = start; u + 1 < q;) {
+            const short2 a0 = ps[u];
+            bool found = false;
+            for (size_t v = u + 1; v < q && !found; v++) {
+                const short2 b0 = ps[v];
+                if (a0.x != b0.x && a0.x != b0.y && a0.y != b0.x && a0.y != b0.y) {
+                    std::swap(ps[u + 1], ps[v]);
+                    std::swap(pr2[u + 1], pr2[v]);
+                    found = true;
+                }
+            }
+            u += found ? 2 : 1;
+        }
+        // z: the tile's row of the sphere lists (tiles may be dealt to shards)
+        tl.push_back(make_int4((int)start, (int)(q - start), (int)tl.size(), ga == gb ? 1 : 0));
+    }
+    pr.swap(pr2);
+    if (!ts.empty()) {
+        CK(c->tsph.alloc(ts.size()));
+        CK(c->pslot.alloc(ps.size()));
+        CK(cudaMemcpy(c->tsph.p, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->pslot.p, ps.data(), sizeof(short2) * ps.size(), cudaMemcpyHostToDevice));
+    }
+    return MSTMG_OK;
+}
+
 int fft_build(mstmg_ctx* c)
 {
     FftState& F = *c->fft;
@@ -754,75 +837,17 @@ int fft_build(mstmg_ctx* c)
     // near pairs between two groups (or inside one), its spheres listed by
     // slot, so the near pairs of nearby spheres share the tiles' output
     // accumulation as the block tiles of a whole cluster do.
-    c->tsph.release();
-    c->pslot.release();
     std::vector<int4> tl;
     {
-        const int B = TILE_B;
         const int lmin = *std::min_element(c->order.begin(), c->order.end());
         c->tiled = !c->opts.generic_kernel && lmin == c->lmax && lmin >= c->opts.translation_switch_order && tiled_supported(c->lmax, 1) &&
                    !pr.empty();
+        c->tile_L = c->lmax;
         if (c->tiled) {
-            std::vector<int> grp(n), gs(n);
-            int k = 0;
-            for (const auto& cm : members)
-                for (int i : cm) {
-                    grp[i] = k / B;
-                    gs[i] = k % B;
-                    k++;
-                }
-            const long long ng = (n + B - 1) / B;
-            std::vector<int> gmem((size_t)ng * B, -1);
-            for (int i = 0; i < n; i++) gmem[(size_t)grp[i] * B + gs[i]] = i;
-            std::vector<long long> key(pr.size());
-            std::vector<int> idx(pr.size());
-            for (size_t q = 0; q < pr.size(); q++) {
-                const long long ga = std::min(grp[pr[q].x], grp[pr[q].y]), gb = std::max(grp[pr[q].x], grp[pr[q].y]);
-                key[q] = ga * ng + gb;
-                idx[q] = (int)q;
-            }
-            std::stable_sort(idx.begin(), idx.end(), [&](int u, int v) { return key[u] < key[v]; });
-            std::vector<int2> pr2(pr.size());
-            std::vector<int> ts;
-            std::vector<short2> ps(pr.size());
-            size_t q = 0;
-            while (q < idx.size()) {
-                const long long kk = key[idx[q]];
-                const int ga = (int)(kk / ng), gb = (int)(kk % ng);
-                const size_t start = q;
-                for (int s = 0; s < B; s++) ts.push_back(gmem[(size_t)ga * B + s]);
-                for (int s = 0; s < B; s++) ts.push_back(ga == gb ? -1 : gmem[(size_t)gb * B + s]);
-                for (; q < idx.size() && key[idx[q]] == kk; q++) {
-                    const int2 p2 = pr[idx[q]];
-                    pr2[q] = p2;
-                    const short si = (short)(grp[p2.x] == ga ? gs[p2.x] : B + gs[p2.x]);
-                    const short sj = (short)(grp[p2.y] == ga ? gs[p2.y] : B + gs[p2.y]);
-                    ps[q] = make_short2(si, sj);
-                }
-                // couples of consecutive pairs with four different output
-                // slots where the tile has them (the row kernel runs such a
-                // couple as one step)
-                for (size_t u = start; u + 1 < q;) {
-                    const short2 a0 = ps[u];
-                    bool found = false;
-                    for (size_t v = u + 1; v < q && !found; v++) {
-                        const short2 b0 = ps[v];
-                        if (a0.x != b0.x && a0.x != b0.y && a0.y != b0.x && a0.y != b0.y) {
-                            std::swap(ps[u + 1], ps[v]);
-                            std::swap(pr2[u + 1], pr2[v]);
-                            found = true;
-                        }
-                    }
-                    u += found ? 2 : 1;
-                }
-                // z: the tile's row of the sphere lists (tiles may be dealt to shards)
-                tl.push_back(make_int4((int)start, (int)(q - start), (int)tl.size(), ga == gb ? 1 : 0));
-            }
-            pr.swap(pr2);
-            CK(c->tsph.alloc(ts.size()));
-            CK(c->pslot.alloc(ps.size()));
-            CK(cudaMemcpyAsync(c->tsph.p, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice, c->st));
-            CK(cudaMemcpyAsync(c->pslot.p, ps.data(), sizeof(short2) * ps.size(), cudaMemcpyHostToDevice, c->st));
+            if (int rg = group_tiles(c, members, pr, tl)) return rg;
+        } else {
+            c->tsph.release();
+            c->pslot.release();
         }
     }
     int rc = upload_pairs(c, pr, (int)pr.size(), tl);   // synchronises: the host vectors above are done with

@@ -345,6 +345,7 @@ struct mstmg_ctx {
     DevBuf<int> tsph;
     DevBuf<short2> pslot;
     bool tiled = false;   // monodisperse cluster: pairs stored in tile order for the fast kernel
+    int tile_L = 0;       // the sphere order of the tiled pairs (the cluster's; with host spheres, the held spheres')
     int row32 = 0;        // tiled: floats per FP32 row record (translate_rows.cuh); 0: FP32 records as FP64
     // pair shard (mstmg_set_pair_shard): this context translates the tiles
     // t with t % nshards == shard; all tiles kept on the host
@@ -469,6 +470,7 @@ template <typename T> int translate_hosts(mstmg_ctx* c, const cpx<T>* x, cpx<T>*
 template <typename T> void mie_all(mstmg_ctx* c, int idir, int conj_in, const cpx<T>* x, cpx<T>* y);
 template <typename T> int fft_far(mstmg_ctx* c, const cpx<T>* x, cpx<T>* y, int ncols, unsigned contran);
 int fft_build(mstmg_ctx* c);
+int group_tiles(mstmg_ctx* c, const std::vector<std::vector<int>>& members, std::vector<int2>& pr, std::vector<int4>& tl);
 // capi_origin.cu
 mstmg::Tables& big_tables();   // the reference's large constant tables (this thread's copy)
 // capi_solve.cu

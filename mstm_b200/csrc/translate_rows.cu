@@ -474,8 +474,8 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
             const int2 pr = u ? pf_p1 : pf_p0;
             zf* w = SRC + (size_t)bb * CW + (size_t)u * C * NB2;
             for (int rr = 0; rr < NR; rr++) {
-                bulk_copy(w + (size_t)(0 * NR + rr) * NB, xs + (size_t)rr * a.ld + (size_t)pr.y * NB, XB, &bar[2 + bb]);   // source of j -> i
-                bulk_copy(w + (size_t)(1 * NR + rr) * NB, xs + (size_t)rr * a.ld + (size_t)pr.x * NB, XB, &bar[2 + bb]);   // source of i -> j
+                bulk_copy(w + (size_t)(0 * NR + rr) * NB, xs + (size_t)rr * a.ld + tile_sphere_base(a, pr.y, NB), XB, &bar[2 + bb]);   // source of j -> i
+                bulk_copy(w + (size_t)(1 * NR + rr) * NB, xs + (size_t)rr * a.ld + tile_sphere_base(a, pr.x, NB), XB, &bar[2 + bb]);   // source of i -> j
             }
         }
     };
@@ -560,7 +560,7 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
                 // grouped tiles carry their sphere-list row in z (i0 << 16 | j0 here)
                 const int sph = a.tsph ? a.tsph[(size_t)((cm.i0 << 16) | cm.j0) * NSLOT + slot] : ((slot < TILE_B) ? (cm.i0 + slot) : (cm.j0 + slot - TILE_B));
                 zf* av = ACC + (size_t)slot * SS + rem;
-                if (a.tsph ? sph >= 0 : (!(cm.diag && slot >= TILE_B) && sph < a.nsph)) red_add<float>(yc + (size_t)rr * a.ld + (size_t)sph * NB + el, *av);
+                if (a.tsph ? sph >= 0 : (!(cm.diag && slot >= TILE_B) && sph < a.nsph)) red_add<float>(yc + (size_t)rr * a.ld + tile_sphere_base(a, sph, NB) + el, *av);
                 *av = mk(0.f, 0.f);
             }
             if (cm.item + G >= NI) break;
@@ -688,11 +688,13 @@ template <int L> static int launch_L(const TiledArgs<float>& a, int nsm, cudaStr
 
 }  // namespace
 
-bool rows_supported(int L, int nrhs) { return L >= 5 && L <= 10 && (nrhs == 1 || nrhs == 2 || nrhs == 4); }
+bool rows_supported(int L, int nrhs) { return L >= 3 && L <= 10 && (nrhs == 1 || nrhs == 2 || nrhs == 4); }
 
 int launch_translate_rows(const TiledArgs<float>& a, int L, int nsm, cudaStream_t st)
 {
     switch (L) {
+    case 3: return launch_L<3>(a, nsm, st);
+    case 4: return launch_L<4>(a, nsm, st);
     case 5: return launch_L<5>(a, nsm, st);
     case 6: return launch_L<6>(a, nsm, st);
     case 7: return launch_L<7>(a, nsm, st);

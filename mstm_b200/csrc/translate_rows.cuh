@@ -41,7 +41,7 @@ __host__ __device__ constexpr int row_record_units(int L)
     return u + (((4 - u) % 32) + 32) % 32;
 }
 
-// The row pass covers every FP32 pass of the tiled path: L = 5..10 and
+// The row pass covers every FP32 pass of the tiled path: L = 3..10 and
 // 1, 2 or 4 columns per chunk.
 bool rows_supported(int L, int nrhs);
 int launch_translate_rows(const TiledArgs<float>& a, int L, int nsm, cudaStream_t st);

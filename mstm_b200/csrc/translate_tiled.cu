@@ -166,8 +166,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
             const int2 pr = a.pairs[qq + u];
             cpx<T>* w = W2 + (size_t)u * WP;
             for (int r = 0; r < NR; r++) {
-                bulk_copy(w + (size_t)(0 * NR + r) * NB, xs + (size_t)r * a.ld + (size_t)pr.y * NB, XB, &bar[2]);   // source of j -> i
-                bulk_copy(w + (size_t)(1 * NR + r) * NB, xs + (size_t)r * a.ld + (size_t)pr.x * NB, XB, &bar[2]);   // source of i -> j
+                bulk_copy(w + (size_t)(0 * NR + r) * NB, xs + (size_t)r * a.ld + tile_sphere_base(a, pr.y, NB), XB, &bar[2]);   // source of j -> i
+                bulk_copy(w + (size_t)(1 * NR + r) * NB, xs + (size_t)r * a.ld + tile_sphere_base(a, pr.x, NB), XB, &bar[2]);   // source of i -> j
             }
         }
     };
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
                 const int sph = a.tsph ? a.tsph[(size_t)tinfo.z * NSLOT + slot] : ((slot < B) ? (i0 + slot) : (j0 + slot - B));
                 if (a.tsph ? sph >= 0 : (!(diag && slot >= B) && sph < a.nsph)) {
                     cpx<T> v = ACC[idx];
-                    red_add<T>(yc + (size_t)r * a.ld + (size_t)sph * NB + el, v);
+                    red_add<T>(yc + (size_t)r * a.ld + tile_sphere_base(a, sph, NB) + el, v);
                 }
                 ACC[idx] = mk((T)0, (T)0);
             }
@@ -503,6 +503,8 @@ template <typename T, int L> static int launch_L(const TiledArgs<T>& a, int nsm,
 template <typename T> int launch_translate_tiled(const TiledArgs<T>& a, int L, int nsm, cudaStream_t st)
 {
     switch (L) {
+    case 3: return launch_L<T, 3>(a, nsm, st);
+    case 4: return launch_L<T, 4>(a, nsm, st);
     case 5: return launch_L<T, 5>(a, nsm, st);
     case 6: return launch_L<T, 6>(a, nsm, st);
     case 7: return launch_L<T, 7>(a, nsm, st);
@@ -512,7 +514,7 @@ template <typename T> int launch_translate_tiled(const TiledArgs<T>& a, int L, i
     default: return -1;
     }
 }
-bool tiled_supported(int L, int nrhs) { return L >= 5 && L <= 10 && (nrhs == 1 || nrhs == 2 || nrhs == 4); }
+bool tiled_supported(int L, int nrhs) { return L >= 3 && L <= 10 && (nrhs == 1 || nrhs == 2 || nrhs == 4); }
 
 template int launch_translate_tiled<double>(const TiledArgs<double>&, int, int, cudaStream_t);
 template int launch_translate_tiled<float>(const TiledArgs<float>&, int, int, cudaStream_t);

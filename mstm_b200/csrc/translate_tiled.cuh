@@ -21,7 +21,16 @@ template <typename T> struct TiledArgs {
     const int* tsph = nullptr;
     const short2* pslot = nullptr;
     int pairs_per_step = 0;  // 2: two slot-disjoint pairs a step (FP32, one or two columns); otherwise one
+    // sphere i's block at soff[i] (complex units; null: i * 2L(L+2), the
+    // layout of a cluster of one order; set with host spheres, whose internal
+    // blocks sit between the others')
+    const int* soff = nullptr;
 };
+// start of sphere i's block in a vector of the tiled path
+template <typename T> __device__ __forceinline__ size_t tile_sphere_base(const TiledArgs<T>& a, int i, int NB)
+{
+    return a.soff ? (size_t)a.soff[i] : (size_t)i * NB;
+}
 
 bool tiled_supported(int L, int nrhs);
 // one CTA runs the kernels' bounded mbarrier wait on a barrier no copy completes

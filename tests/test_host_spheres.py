@@ -367,3 +367,35 @@ def test_coated_sphere_deck():
     L = run_variables(run, out)
     i = L.index(" sphere properties and associations")
     assert L[i + 3][:16] == "       2       1"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [4, 6])
+def test_host_inclusions_on_tiles(oracle_mod, order):
+    """Inclusions of one order inside a host: their pairs run on the tiled
+    kernels (grouped tiles, each sphere's block at its own offset): the
+    interaction to 1e-12, the FP64 solve (same iterations, 1e-9) and the
+    mixed one (1e-6) against the oracle."""
+    from mstm_b200 import api, configs as C
+    w = C.host_inclusions(40, 0.5, 0.15, seed=order)
+    # the host's order is raised to the inclusions' (forced) order
+    g = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=-order, precision="fp64")
+    o = oracle_mod.Oracle(w["pos"], w["radius"], w["ref_index"], mie_eps=-order, nthreads=4)
+    assert np.array_equal(g.sphere_offset, o.offset)
+    rng = np.random.default_rng(order)
+    x = rng.standard_normal((g.number_eqns, 2)) + 1j * rng.standard_normal((g.number_eqns, 2))
+    yg = g.sphereinteraction(x, con_tran=[0, 1], initial_run=True)
+    yo = o.sphereinteraction(x, con_tran=[0, 1], initial_run=True)
+    assert np.abs(yg - yo).max() <= 1e-12 * np.abs(yo).max()
+    y32 = g.translation_pass(x, [0, 1], "fp32")
+    y64 = g.translation_pass(x, [0, 1], "fp64")
+    assert np.abs(y32 - y64).max() <= 2e-6 * np.abs(y64).max()
+    ro = o.fixedorsoln(eps=1e-12, niter=500)
+    rg = g.fixedorsoln(eps=1e-12, niter=500)
+    assert rg["iterations"] == ro["iterations"]
+    assert np.allclose(rg["qtot"], ro["qtot"], rtol=1e-9)
+    m = api.SphereCluster(w["pos"], w["radius"], w["ref_index"], mie_epsilon=-order, precision="mixed")
+    rm = m.fixedorsoln(eps=1e-12, niter=500)
+    assert np.abs(rm["qtot"] - ro["qtot"]).max() <= 5e-6 * ro["qtot"][0, 0]
+    for k in (g, m, o):
+        k.close()

@@ -5,7 +5,9 @@ and the i -> j axial product rewritten as row sweeps through the symmetries
 of the Wigner functions and the axial blocks, from FP32 row records.  Checked
 against the FP64 pass at 2e-6 of the largest output (FP32 rounding of
 records and sums) and against the rotation-tiled kernel's FP32 pass
-(tile_pairs 1), for every sphere order the tiled path takes (5..10), column
+(tile_pairs 1), for every sphere order the tiled path takes (3..10; for
+3 and 4 the FP64 pass runs the order-generic kernel on the tile-ordered
+pairs, checked against a context of the generic pair order), column
 counts the kernel runs directly (1, 2, 4) and in groups (3, 5, 8), plain and
 conjugate-transpose columns, cluster sizes with partial tiles, and the FFT
 path's grouped tiles of near pairs.
@@ -20,20 +22,32 @@ pytestmark = pytest.mark.gpu
 TOL = 2e-6
 
 
+def _cluster_arrays(n, seed):
+    pos, _ = C.rsa_sphere(n, 1.0, 0.15, seed=seed)
+    return pos, np.full(n, 1.0), np.full(n, 1.45 + 0.01j)
+
+
 def _pair(L, n, seed, **kw):
     from mstm_b200 import api
-    pos, _ = C.rsa_sphere(n, 1.0, 0.15, seed=seed)
-    rad = np.full(n, 1.0)
-    ri = np.full(n, 1.45 + 0.01j)
+    pos, rad, ri = _cluster_arrays(n, seed)
     rows = api.SphereCluster(pos, rad, ri, mie_epsilon=-L, precision="mixed", **kw)
     rot = api.SphereCluster(pos, rad, ri, mie_epsilon=-L, precision="mixed", tile_pairs=1, **kw)
     return rows, rot
 
 
-@pytest.mark.parametrize("L,n", [(5, 30), (6, 17), (7, 30), (8, 22), (9, 30), (10, 13)])
+@pytest.mark.parametrize("L,n", [(3, 24), (4, 30), (5, 30), (6, 17), (7, 30), (8, 22), (9, 30), (10, 13)])
 def test_row_kernel_matches_fp64_and_rotation_kernel(L, n):
     rows, rot = _pair(L, n, seed=L)
     rng = np.random.default_rng(L)
+    if L < 5:
+        # small orders: the FP64 pass on the tile-ordered pairs against the generic pair order
+        from mstm_b200 import api
+        gen = api.SphereCluster(*_cluster_arrays(n, L), mie_epsilon=-L, precision="fp64", generic_kernel=1)
+        x = rng.normal(size=(rows.number_eqns, 2)) + 1j * rng.normal(size=(rows.number_eqns, 2))
+        yt = rows.translation_pass(x, [0, 1], "fp64")
+        yg = gen.translation_pass(x, [0, 1], "fp64")
+        assert np.abs(yt - yg).max() <= 1e-12 * np.abs(yg).max()
+        gen.close()
     for ct in ([0], [1], [0, 1], [1, 0], [0, 1, 1], [1, 0, 0, 1], [0, 0, 1, 1, 0], [0, 1] * 4):
         x = rng.normal(size=(rows.number_eqns, len(ct))) + 1j * rng.normal(size=(rows.number_eqns, len(ct)))
         y64 = rows.translation_pass(x, ct, "fp64")
