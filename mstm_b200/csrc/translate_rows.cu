@@ -67,16 +67,21 @@ template <int L> __host__ __device__ constexpr int goff(int m) { return m == 0 ?
 template <int L> __host__ __device__ constexpr int gidx(int m, int n) { return goff<L>(m) + n - (m < 1 ? 1 : m); }
 
 // strides padded for the shared-memory banks: (s', t') columns an odd number
-// of 16-byte units apart, tile-output slots an odd number of complex values
+// of 16-byte units apart, tile-output slots an odd number of complex values.
+// A column of sources, of a' or of a tile output holds L(L+2) complex values;
+// for even L that is a multiple of 16 words and the 8 columns a lane group
+// reads at once would share one bank, so their stride gets 2 more (still
+// 16-byte aligned for the bulk copies: 4 words apart in the banks)
+__host__ __device__ constexpr int rows_cs(int L) { return (L & 1) ? L * (L + 2) : L * (L + 2) + 2; }
 __host__ __device__ constexpr int rows_gs(int L) { return (L * (L + 3) / 2) | 1; }
-__host__ __device__ constexpr int rows_ss(int L, int NR) { return NR * 2 * L * (L + 2) + 1; }
+__host__ __device__ constexpr int rows_ss(int L, int NR) { return NR * 2 * rows_cs(L) + 1; }
 
 template <int L, int NR, int PP> __host__ __device__ constexpr size_t rows_smem_pp()
 {
-    constexpr int NB2 = L * (L + 2), C = 4 * NR;
+    constexpr int C = 4 * NR;
     size_t off = 128;                                                   // mbarriers, step descriptors
     off = al128(off + sizeof(float) * 2 * PP * row_record_units(L));    // records, two steps
-    off += sizeof(zf) * 3 * (size_t)PP * C * NB2;                      // sources (two steps), a'
+    off += sizeof(zf) * 3 * (size_t)PP * C * rows_cs(L);               // sources (two steps), a'
     off += sizeof(float4) * (size_t)PP * C * rows_gs(L);               // (s', t') of the axial products
     off += sizeof(zf) * (size_t)2 * TILE_B * rows_ss(L, NR);           // tile outputs
     return off;
@@ -358,12 +363,13 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
     constexpr int NT = 256;
     constexpr int C = 4 * NR, PP = rows_pp<L, NR>(), H = 32 / (PP * C);
     static_assert(PP * C * H == 32, "a warp holds PP pairs x C columns x H row sets");
-    constexpr int NB2 = L * (L + 2), NB = 2 * NB2, GS = rows_gs(L), SS = rows_ss(L, NR);
+    constexpr int NB2 = L * (L + 2), NB = 2 * NB2, GS = rows_gs(L), SS = rows_ss(L, NR), CS = rows_cs(L);
     constexpr int REC = row_record_units(L);
     constexpr int NSLOT = 2 * TILE_B;
     constexpr uint32_t RECB = (uint32_t)(REC * sizeof(float));
     constexpr uint32_t XB = (uint32_t)(NB * sizeof(zf));
-    constexpr int CW = PP * C * NB2;
+    constexpr uint32_t XB2 = (uint32_t)(NB2 * sizeof(zf));
+    constexpr int CW = PP * C * CS;
 
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm);   // [0],[1] records, [2],[3] sources of steps t, t + 1
@@ -386,7 +392,7 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
     ln.swp = (ln.dir != (int)((a.contran >> r) & 1u));
     ln.dsg = ln.dir ? -1.f : 1.f;
     ln.sig = ln.swp ? -1.f : 1.f;
-    ln.ap = AP + (size_t)(qq * C + c) * NB2;
+    ln.ap = AP + (size_t)(qq * C + c) * CS;
     ln.g = GB + (size_t)(qq * C + c) * GS;
 
     for (int e = tid; e < NSLOT * SS; e += NT) ACC[e] = mk(0.f, 0.f);
@@ -472,10 +478,19 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
         mb_expect(&bar[2 + bb], (uint32_t)m.np * 2u * NR * XB);
         for (int u = 0; u < m.np; u++) {
             const int2 pr = u ? pf_p1 : pf_p0;
-            zf* w = SRC + (size_t)bb * CW + (size_t)u * C * NB2;
+            zf* w = SRC + (size_t)bb * CW + (size_t)u * C * CS;
             for (int rr = 0; rr < NR; rr++) {
-                bulk_copy(w + (size_t)(0 * NR + rr) * NB, xs + (size_t)rr * a.ld + tile_sphere_base(a, pr.y, NB), XB, &bar[2 + bb]);   // source of j -> i
-                bulk_copy(w + (size_t)(1 * NR + rr) * NB, xs + (size_t)rr * a.ld + tile_sphere_base(a, pr.x, NB), XB, &bar[2 + bb]);   // source of i -> j
+                const zf* sj = xs + (size_t)rr * a.ld + tile_sphere_base(a, pr.y, NB);   // source of j -> i
+                const zf* si = xs + (size_t)rr * a.ld + tile_sphere_base(a, pr.x, NB);   // source of i -> j
+                if (CS == NB2) {   // both modes' columns in one copy
+                    bulk_copy(w + (size_t)(0 * NR + rr) * NB, sj, XB, &bar[2 + bb]);
+                    bulk_copy(w + (size_t)(1 * NR + rr) * NB, si, XB, &bar[2 + bb]);
+                } else {           // a copy per mode, columns CS apart
+                    for (int pm2 = 0; pm2 < 2; pm2++) {
+                        bulk_copy(w + (size_t)((0 * NR + rr) * 2 + pm2) * CS, sj + (size_t)pm2 * NB2, XB2, &bar[2 + bb]);
+                        bulk_copy(w + (size_t)((1 * NR + rr) * 2 + pm2) * CS, si + (size_t)pm2 * NB2, XB2, &bar[2 + bb]);
+                    }
+                }
             }
         }
     };
@@ -510,10 +525,10 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
         ln.act = qq < cm.np;
         {
             const int sl = (cm.slots >> (16 * qq + (ln.dir ? 8 : 0))) & 255;
-            ln.acc = ACC + (size_t)(ln.act ? sl : 0) * SS + (size_t)r * NB + (size_t)ln.p * NB2;
+            ln.acc = ACC + (size_t)(ln.act ? sl : 0) * SS + (size_t)(r * 2 + ln.p) * CS;
         }
         ln.rec = recs + ((size_t)b * PP + qq) * REC;
-        ln.src = SRC + (size_t)b * CW + (size_t)(qq * C + c) * NB2;
+        ln.src = SRC + (size_t)b * CW + (size_t)(qq * C + c) * CS;
         // the prefetch step's descriptor (thread 0; its loads were issued a phase ago)
         StepMeta pm;
         if (tid == 0 && pf_ok) pm = pf_meta();
@@ -557,9 +572,10 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int rr = rem / NB, el = rem - rr * NB;
+                const int pe = el >= NB2 ? 1 : 0;
                 // grouped tiles carry their sphere-list row in z (i0 << 16 | j0 here)
                 const int sph = a.tsph ? a.tsph[(size_t)((cm.i0 << 16) | cm.j0) * NSLOT + slot] : ((slot < TILE_B) ? (cm.i0 + slot) : (cm.j0 + slot - TILE_B));
-                zf* av = ACC + (size_t)slot * SS + rem;
+                zf* av = ACC + (size_t)slot * SS + (size_t)(rr * 2 + pe) * CS + (el - pe * NB2);
                 if (a.tsph ? sph >= 0 : (!(cm.diag && slot >= TILE_B) && sph < a.nsph)) red_add<float>(yc + (size_t)rr * a.ld + tile_sphere_base(a, sph, NB) + el, *av);
                 *av = mk(0.f, 0.f);
             }
