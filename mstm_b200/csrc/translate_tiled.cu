@@ -45,6 +45,15 @@ __host__ __device__ constexpr int tofs(int n) { return (n - 1) * n / 2; }       
 // FP32 columns slow down at the smaller budget: FP64 2 columns 2.9 -> 4.1 ms).
 // With two pairs a step the shared memory holds two CTAs per SM, which get
 // the 128-register budget.
+// Column stride (complex values) of the sources, S/T, a', g and tile-output
+// columns in shared memory: L(L+2), or for even L (a multiple of 8) one more
+// (FP64: 16-byte values, 4 banks apart) or two more (FP32, 16-byte aligned)
+// so that the columns a group of lanes reads at once fall on different banks
+template <typename T> __host__ __device__ constexpr int tiled_cs(int L)
+{
+    return (L & 1) ? L * (L + 2) : L * (L + 2) + (sizeof(T) == 8 ? 1 : 2);
+}
+
 template <typename T, int NR, int PP> __host__ __device__ constexpr int tiled_minb() { return (sizeof(T) == 4 && NR <= 2 && PP == 1) ? 3 : 2; }
 
 // One CTA works through whole tiles, PP pairs of a tile at a time (a step):
@@ -67,7 +76,9 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
     constexpr int NSLOT = 2 * B;
     constexpr uint32_t RECB = (uint32_t)(REC * sizeof(T));
     constexpr uint32_t XB = (uint32_t)(NB * sizeof(cpx<T>));   // one sphere block of one rhs
-    constexpr int WP = C * NB2;          // one pair's share of W1 / W2
+    constexpr uint32_t XB2 = (uint32_t)(NB2 * sizeof(cpx<T>)); // one mode of it
+    constexpr int CS = tiled_cs<T>(L);   // column stride of W1 / W2 / ACC (bank-spread for even L)
+    constexpr int WP = C * CS;           // one pair's share of W1 / W2
 
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm);          // [0],[1] operators, [2] sources
@@ -82,9 +93,9 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
     T* opb = reinterpret_cast<T*>(sm + off);                  // 2 buffers x PP records
     off += sizeof(T) * 2 * PP * REC;
     off = (off + 127) & ~(size_t)127;
-    cpx<T>* W1 = reinterpret_cast<cpx<T>*>(sm + off);         // PP x C x NB2: S/T, then g
-    cpx<T>* W2 = W1 + PP * WP;                                // PP x C x NB2: sources (2 spheres x NR x NB), then a'
-    cpx<T>* ACC = W2 + PP * WP;                               // NSLOT x NR x NB
+    cpx<T>* W1 = reinterpret_cast<cpx<T>*>(sm + off);         // PP x C x CS: S/T, then g
+    cpx<T>* W2 = W1 + PP * WP;                                // PP x C x CS: sources (2 spheres x NR x 2 modes), then a'
+    cpx<T>* ACC = W2 + PP * WP;                               // NSLOT x NR x 2 modes x CS
 
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -101,7 +112,7 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
             for (int line = m1; line <= L; line++) tabC[e++] = make_short2((short)m, (short)line);
         }
     }
-    for (int e = tid; e < NSLOT * NR * NB; e += NT) ACC[e] = mk((T)0, (T)0);
+    for (int e = tid; e < NSLOT * NR * 2 * CS; e += NT) ACC[e] = mk((T)0, (T)0);
     if (tid == 0) {
         mb_init(&bar[0], 1);
         mb_init(&bar[1], 1);
@@ -166,8 +177,17 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
             const int2 pr = a.pairs[qq + u];
             cpx<T>* w = W2 + (size_t)u * WP;
             for (int r = 0; r < NR; r++) {
-                bulk_copy(w + (size_t)(0 * NR + r) * NB, xs + (size_t)r * a.ld + tile_sphere_base(a, pr.y, NB), XB, &bar[2]);   // source of j -> i
-                bulk_copy(w + (size_t)(1 * NR + r) * NB, xs + (size_t)r * a.ld + tile_sphere_base(a, pr.x, NB), XB, &bar[2]);   // source of i -> j
+                const cpx<T>* sj = xs + (size_t)r * a.ld + tile_sphere_base(a, pr.y, NB);   // source of j -> i
+                const cpx<T>* si = xs + (size_t)r * a.ld + tile_sphere_base(a, pr.x, NB);   // source of i -> j
+                if (CS == NB2) {   // both modes' columns in one copy
+                    bulk_copy(w + (size_t)(0 * NR + r) * NB, sj, XB, &bar[2]);
+                    bulk_copy(w + (size_t)(1 * NR + r) * NB, si, XB, &bar[2]);
+                } else {           // a copy per mode, columns CS apart
+                    for (int pm2 = 0; pm2 < 2; pm2++) {
+                        bulk_copy(w + (size_t)((0 * NR + r) * 2 + pm2) * CS, sj + (size_t)pm2 * NB2, XB2, &bar[2]);
+                        bulk_copy(w + (size_t)((1 * NR + r) * 2 + pm2) * CS, si + (size_t)pm2 * NB2, XB2, &bar[2]);
+                    }
+                }
             }
         }
     };
@@ -227,15 +247,15 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
                     const int n = nm.x, m = nm.y;
                     const int r = (c >> 1) % NR, dir = (c >> 1) / NR;
                     const bool swp = (dir != (int)((a.contran >> r) & 1u));
-                    const cpx<T>* xs = W2 + (size_t)u * WP + (size_t)c * NB2;
+                    const cpx<T>* xs = W2 + (size_t)u * WP + (size_t)c * CS;
                     const cpx<T>* e = ephm + (size_t)u * (2 * L + 1) + L;
                     const int hp = hidx<L>(m, n), hm = m ? hidx<L>(-m, n) : hp;
                     // with the shift the +m and -m sources trade places (and take the sign (-1)^m)
                     U[k] = xs[swp ? hm : hp];
                     V[k] = xs[swp ? hp : hm];
                     EU[k] = e[dir ? -m : m];
-                    sdst[k] = u * WP + c * NB2 + sofs(n) + m;
-                    tdst[k] = u * WP + c * NB2 + NS + tofs(n) + m - 1;
+                    sdst[k] = u * WP + c * CS + sofs(n) + m;
+                    tdst[k] = u * WP + c * CS + NS + tofs(n) + m - 1;
                     mm[k] = swp ? -m - 1 : m;
                 }
             }
@@ -275,8 +295,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
 #pragma unroll
             for (int cc = 0; cc < CB; cc++) {
                 const int c = g * CB + cc;
-                const cpx<T>* sv = W1 + u * WP + c * NB2 + sofs(n);
-                const cpx<T>* tv = W1 + u * WP + c * NB2 + NS + tofs(n);
+                const cpx<T>* sv = W1 + u * WP + c * CS + sofs(n);
+                const cpx<T>* tv = W1 + u * WP + c * CS + NS + tofs(n);
                 cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
 #pragma unroll
                 for (int mm = 0; mm <= L; mm++)
@@ -284,7 +304,7 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
 #pragma unroll
                 for (int mm = 0; mm < L; mm++)
                     if (mm < n) Q = mac_r(Q, orr[mm], tv[mm]);
-                cpx<T>* ap = W2 + u * WP + c * NB2;
+                cpx<T>* ap = W2 + u * WP + c * CS;
                 if (k == 0) {
                     ap[hidx<L>(0, n)] = P;
                 } else {
@@ -313,10 +333,10 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
             const T* z0 = rec + 2 + RS + 2 * op_z_offset(m, L, L) + (dir ? 2 * (line - m1) : 2 * (line - m1) * dim);
             const T* z1 = z0 + 2 * dim * dim;
             const int zst = dir ? 2 * dim : 2;
-            const cpx<T>* a0 = W2 + u * WP + (((dir * NR) + r) * 2 + 0) * NB2;
-            const cpx<T>* a1 = W2 + u * WP + (((dir * NR) + r) * 2 + 1) * NB2;
-            cpx<T>* o0 = W1 + u * WP + (((dir * NR) + r) * 2 + 0) * NB2;
-            cpx<T>* o1 = W1 + u * WP + (((dir * NR) + r) * 2 + 1) * NB2;
+            const cpx<T>* a0 = W2 + u * WP + (((dir * NR) + r) * 2 + 0) * CS;
+            const cpx<T>* a1 = W2 + u * WP + (((dir * NR) + r) * 2 + 1) * CS;
+            cpx<T>* o0 = W1 + u * WP + (((dir * NR) + r) * 2 + 0) * CS;
+            cpx<T>* o1 = W1 + u * WP + (((dir * NR) + r) * 2 + 1) * CS;
             if (m == 0) {
                 cpx<T> g0 = mk((T)0, (T)0), g1 = mk((T)0, (T)0);
                 for (int v = 0; v < dim; v++) {
@@ -385,8 +405,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
             for (int cc = 0; cc < CB; cc++) {
                 const int c = g * CB + cc;
                 const int p = c & 1, r = (c >> 1) % NR, dir = (c >> 1) / NR;
-                const cpx<T>* sv = W1 + u * WP + c * NB2 + sofs(n);
-                const cpx<T>* tv = W1 + u * WP + c * NB2 + NS + tofs(n);
+                const cpx<T>* sv = W1 + u * WP + c * CS + sofs(n);
+                const cpx<T>* tv = W1 + u * WP + c * CS + NS + tofs(n);
                 cpx<T> P = mk((T)0, (T)0), Q = mk((T)0, (T)0);
 #pragma unroll
                 for (int mm = 0; mm <= L; mm++)
@@ -395,7 +415,7 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
                 for (int mm = 0; mm < L; mm++)
                     if (mm < n) Q = mac_r(Q, oc[mm], tv[mm]);
                 const int slot = dir ? (u == 0 ? sj[0] : sj[PP - 1]) : (u == 0 ? si[0] : si[PP - 1]);
-                cpx<T>* acc = ACC + (slot * NR + r) * NB + p * NB2;
+                cpx<T>* acc = ACC + ((slot * NR + r) * 2 + p) * CS;
                 if (k == 0) {
                     acc[hidx<L>(0, n)] = acc[hidx<L>(0, n)] + (T)2 * P;
                 } else {
@@ -425,13 +445,15 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int r = rem / NB, el = rem - r * NB;
+                const int pe = el >= NB2 ? 1 : 0;
+                const int ai = ((slot * NR + r) * 2 + pe) * CS + (el - pe * NB2);
                 // grouped tiles carry their sphere-list row in z
                 const int sph = a.tsph ? a.tsph[(size_t)tinfo.z * NSLOT + slot] : ((slot < B) ? (i0 + slot) : (j0 + slot - B));
                 if (a.tsph ? sph >= 0 : (!(diag && slot >= B) && sph < a.nsph)) {
-                    cpx<T> v = ACC[idx];
+                    cpx<T> v = ACC[ai];
                     red_add<T>(yc + (size_t)r * a.ld + tile_sphere_base(a, sph, NB) + el, v);
                 }
-                ACC[idx] = mk((T)0, (T)0);
+                ACC[ai] = mk((T)0, (T)0);
             }
             __syncthreads();
             tcur += G;
@@ -446,14 +468,14 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
 
 template <typename T, int L, int NR, int B, int PP> static size_t tiled_smem()
 {
-    constexpr int NS = L * (L + 3) / 2, NQ = L * (L + 1) / 2, NB2 = L * (L + 2), NB = 2 * NB2, C = 4 * NR;
+    constexpr int NS = L * (L + 3) / 2, NQ = L * (L + 1) / 2, CS = tiled_cs<T>(L), C = 4 * NR;
     size_t off = 64 + sizeof(short2) * (NS + NQ + NS);
     off = (off + 127) & ~(size_t)127;
     off += sizeof(cpx<T>) * PP * (2 * L + 1);
     off = (off + 127) & ~(size_t)127;
     off += sizeof(T) * 2 * PP * op_record_units(L, L);
     off = (off + 127) & ~(size_t)127;
-    off += sizeof(cpx<T>) * ((size_t)2 * PP * C * NB2 + (size_t)2 * B * NR * NB);
+    off += sizeof(cpx<T>) * ((size_t)2 * PP * C * CS + (size_t)2 * B * NR * 2 * CS);
     return off;
 }
 
