@@ -572,11 +572,19 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int rr = rem / NB, el = rem - rr * NB;
-                const int pe = el >= NB2 ? 1 : 0;
                 // grouped tiles carry their sphere-list row in z (i0 << 16 | j0 here)
                 const int sph = a.tsph ? a.tsph[(size_t)((cm.i0 << 16) | cm.j0) * NSLOT + slot] : ((slot < TILE_B) ? (cm.i0 + slot) : (cm.j0 + slot - TILE_B));
-                zf* av = ACC + (size_t)slot * SS + (size_t)(rr * 2 + pe) * CS + (el - pe * NB2);
-                if (a.tsph ? sph >= 0 : (!(cm.diag && slot >= TILE_B) && sph < a.nsph)) red_add<float>(yc + (size_t)rr * a.ld + tile_sphere_base(a, sph, NB) + el, *av);
+                zf* av;
+                if constexpr (CS == NB2) {
+                    av = ACC + (size_t)slot * SS + rem;
+                } else {
+                    const int pe = el >= NB2 ? 1 : 0;
+                    av = ACC + (size_t)slot * SS + (size_t)(rr * 2 + pe) * CS + (el - pe * NB2);
+                }
+                if (a.tsph ? sph >= 0 : (!(cm.diag && slot >= TILE_B) && sph < a.nsph)) {
+                    const size_t sb = a.soff ? (size_t)a.soff[sph] : (size_t)sph * NB;
+                    red_add<float>(yc + (size_t)rr * a.ld + sb + el, *av);
+                }
                 *av = mk(0.f, 0.f);
             }
             if (cm.item + G >= NI) break;

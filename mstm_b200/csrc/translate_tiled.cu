@@ -445,8 +445,11 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
                 const int slot = idx / (NR * NB);
                 const int rem = idx - slot * (NR * NB);
                 const int r = rem / NB, el = rem - r * NB;
-                const int pe = el >= NB2 ? 1 : 0;
-                const int ai = ((slot * NR + r) * 2 + pe) * CS + (el - pe * NB2);
+                int ai = idx;   // CS == NB2: the accumulators in flush order
+                if constexpr (CS != NB2) {
+                    const int pe = el >= NB2 ? 1 : 0;
+                    ai = ((slot * NR + r) * 2 + pe) * CS + (el - pe * NB2);
+                }
                 // grouped tiles carry their sphere-list row in z
                 const int sph = a.tsph ? a.tsph[(size_t)tinfo.z * NSLOT + slot] : ((slot < B) ? (i0 + slot) : (j0 + slot - B));
                 if (a.tsph ? sph >= 0 : (!(diag && slot >= B) && sph < a.nsph)) {
