@@ -357,7 +357,7 @@ struct StepMeta {
     int i0, j0, diag;   // the tile's block starts and diagonal flag
 };
 
-template <int L, int NR>
+template <int L, int NR, bool SO>
 __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float> a, RowSched sc)
 {
     constexpr int NT = 256;
@@ -480,8 +480,8 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
             const int2 pr = u ? pf_p1 : pf_p0;
             zf* w = SRC + (size_t)bb * CW + (size_t)u * C * CS;
             for (int rr = 0; rr < NR; rr++) {
-                const zf* sj = xs + (size_t)rr * a.ld + tile_sphere_base(a, pr.y, NB);   // source of j -> i
-                const zf* si = xs + (size_t)rr * a.ld + tile_sphere_base(a, pr.x, NB);   // source of i -> j
+                const zf* sj = xs + (size_t)rr * a.ld + tile_sphere_base<SO>(a, pr.y, NB);   // source of j -> i
+                const zf* si = xs + (size_t)rr * a.ld + tile_sphere_base<SO>(a, pr.x, NB);   // source of i -> j
                 if (CS == NB2) {   // both modes' columns in one copy
                     bulk_copy(w + (size_t)(0 * NR + rr) * NB, sj, XB, &bar[2 + bb]);
                     bulk_copy(w + (size_t)(1 * NR + rr) * NB, si, XB, &bar[2 + bb]);
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float>
                     av = ACC + (size_t)slot * SS + (size_t)(rr * 2 + pe) * CS + (el - pe * NB2);
                 }
                 if (a.tsph ? sph >= 0 : (!(cm.diag && slot >= TILE_B) && sph < a.nsph)) {
-                    const size_t sb = a.soff ? (size_t)a.soff[sph] : (size_t)sph * NB;
+                    const size_t sb = tile_sphere_base<SO>(a, sph, NB);
                     red_add<float>(yc + (size_t)rr * a.ld + sb + el, *av);
                 }
                 *av = mk(0.f, 0.f);
@@ -688,7 +688,7 @@ template <int L, int NR> static int launch_LN(const TiledArgs<float>& a, int nsm
     constexpr int H = 32 / (rows_pp<L, NR>() * 4 * NR);
     const RowSched& sc = sched_for(L, H);
     if (!sc.fits) return -1;
-    auto kern = translate_rows_kernel<L, NR>;
+    auto kern = a.soff ? translate_rows_kernel<L, NR, true> : translate_rows_kernel<L, NR, false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = (int)((228 * 1024) / (smem + 1024));
     per_sm = std::max(1, std::min(2, per_sm));

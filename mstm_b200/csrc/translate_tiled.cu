@@ -60,7 +60,7 @@ template <typename T, int NR, int PP> __host__ __device__ constexpr int tiled_mi
 // consecutive pairs whose output slots are disjoint share one step, so the
 // four phases and their barriers serve both (PP = 2), which fills the
 // threads of the rotation phases and halves the barriers per pair.
-template <typename T, int L, int NR, int B, int PP>
+template <typename T, int L, int NR, int B, int PP, bool SO>
 __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_kernel(TiledArgs<T> a)
 {
     constexpr int NT = 256;
@@ -177,8 +177,8 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
             const int2 pr = a.pairs[qq + u];
             cpx<T>* w = W2 + (size_t)u * WP;
             for (int r = 0; r < NR; r++) {
-                const cpx<T>* sj = xs + (size_t)r * a.ld + tile_sphere_base(a, pr.y, NB);   // source of j -> i
-                const cpx<T>* si = xs + (size_t)r * a.ld + tile_sphere_base(a, pr.x, NB);   // source of i -> j
+                const cpx<T>* sj = xs + (size_t)r * a.ld + tile_sphere_base<SO>(a, pr.y, NB);   // source of j -> i
+                const cpx<T>* si = xs + (size_t)r * a.ld + tile_sphere_base<SO>(a, pr.x, NB);   // source of i -> j
                 if (CS == NB2) {   // both modes' columns in one copy
                     bulk_copy(w + (size_t)(0 * NR + r) * NB, sj, XB, &bar[2]);
                     bulk_copy(w + (size_t)(1 * NR + r) * NB, si, XB, &bar[2]);
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_
                 const int sph = a.tsph ? a.tsph[(size_t)tinfo.z * NSLOT + slot] : ((slot < B) ? (i0 + slot) : (j0 + slot - B));
                 if (a.tsph ? sph >= 0 : (!(diag && slot >= B) && sph < a.nsph)) {
                     cpx<T> v = ACC[ai];
-                    red_add<T>(yc + (size_t)r * a.ld + tile_sphere_base(a, sph, NB) + el, v);
+                    red_add<T>(yc + (size_t)r * a.ld + tile_sphere_base<SO>(a, sph, NB) + el, v);
                 }
                 ACC[ai] = mk((T)0, (T)0);
             }
@@ -486,7 +486,7 @@ template <typename T, int L, int NR, int B, int PP> static int launch_pp(const T
 {
     size_t smem = tiled_smem<T, L, NR, B, PP>();
     if (smem > 227 * 1024) return -1;
-    auto kern = translate_tiled_kernel<T, L, NR, B, PP>;
+    auto kern = a.soff ? translate_tiled_kernel<T, L, NR, B, PP, true> : translate_tiled_kernel<T, L, NR, B, PP, false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = (int)((228 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;

@@ -26,10 +26,13 @@ template <typename T> struct TiledArgs {
     // blocks sit between the others')
     const int* soff = nullptr;
 };
-// start of sphere i's block in a vector of the tiled path
-template <typename T> __device__ __forceinline__ size_t tile_sphere_base(const TiledArgs<T>& a, int i, int NB)
+// start of sphere i's block in a vector of the tiled path; SO (per-sphere
+// offsets) is a template argument of the kernels, so the clusters of one
+// order pay no branch on a.soff in their inner loops
+template <bool SO, typename T> __device__ __forceinline__ size_t tile_sphere_base(const TiledArgs<T>& a, int i, int NB)
 {
-    return a.soff ? (size_t)a.soff[i] : (size_t)i * NB;
+    if constexpr (SO) return (size_t)a.soff[i];
+    else return (size_t)i * NB;
 }
 
 bool tiled_supported(int L, int nrhs);
