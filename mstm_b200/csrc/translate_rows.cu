@@ -357,8 +357,13 @@ struct StepMeta {
     int i0, j0, diag;   // the tile's block starts and diagonal flag
 };
 
+// CTAs per SM the register budget is set for: three for the small orders,
+// whose steps are short enough that a third CTA's warps hide the copies' and
+// barriers' latency; two otherwise (the larger orders' register tiles)
+template <int L> __host__ __device__ constexpr int rows_minb() { return L <= 5 ? 3 : 2; }
+
 template <int L, int NR, bool SO>
-__global__ void __launch_bounds__(256, 2) translate_rows_kernel(TiledArgs<float> a, RowSched sc)
+__global__ void __launch_bounds__(256, rows_minb<L>()) translate_rows_kernel(TiledArgs<float> a, RowSched sc)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR, PP = rows_pp<L, NR>(), H = 32 / (PP * C);
@@ -691,7 +696,7 @@ template <int L, int NR> static int launch_LN(const TiledArgs<float>& a, int nsm
     auto kern = a.soff ? translate_rows_kernel<L, NR, true> : translate_rows_kernel<L, NR, false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = (int)((228 * 1024) / (smem + 1024));
-    per_sm = std::max(1, std::min(2, per_sm));
+    per_sm = std::max(1, std::min(rows_minb<L>(), per_sm));
     if (a.ctas_per_sm >= 1 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
     int blocks = std::min(nsm * per_sm, a.ntiles * a.nchunk);
     if (blocks < 1) return 0;
