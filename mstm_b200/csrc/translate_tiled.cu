@@ -41,8 +41,11 @@ __host__ __device__ constexpr int tofs(int n) { return (n - 1) * n / 2; }       
 
 // CTAs per SM the register budget is sized for: 3 for FP32 with one or two
 // columns (80 registers; the extra resident warps hide the pass's latencies:
-// fractal500 FP32, 2 columns, 2.27 -> 1.88 ms), 2 otherwise (FP64 and four
-// FP32 columns slow down at the smaller budget: FP64 2 columns 2.9 -> 4.1 ms).
+// fractal500 FP32, 2 columns, 2.27 -> 1.88 ms) and for FP64 up to order 5
+// (1500 spheres of order 5, FP64, 2 columns: 16.5 -> 14.7 ms), 2 otherwise
+// (FP64 at larger orders and four FP32 columns slow down at the smaller
+// budget: fractal500 FP64, 2 columns, 2.9 -> 4.1 ms).  FP64 below order 5
+// runs the order-generic kernel, faster there than this one at either budget.
 // With two pairs a step the shared memory holds two CTAs per SM, which get
 // the 128-register budget.
 // Column stride (complex values) of the sources, S/T, a', g and tile-output
@@ -54,14 +57,17 @@ template <typename T> __host__ __device__ constexpr int tiled_cs(int L)
     return (L & 1) ? L * (L + 2) : L * (L + 2) + (sizeof(T) == 8 ? 1 : 2);
 }
 
-template <typename T, int NR, int PP> __host__ __device__ constexpr int tiled_minb() { return (sizeof(T) == 4 && NR <= 2 && PP == 1) ? 3 : 2; }
+template <typename T, int L, int NR, int PP> __host__ __device__ constexpr int tiled_minb()
+{
+    return ((sizeof(T) == 4 && NR <= 2 && PP == 1) || (sizeof(T) == 8 && L <= 5)) ? 3 : 2;
+}
 
 // One CTA works through whole tiles, PP pairs of a tile at a time (a step):
 // consecutive pairs whose output slots are disjoint share one step, so the
 // four phases and their barriers serve both (PP = 2), which fills the
 // threads of the rotation phases and halves the barriers per pair.
 template <typename T, int L, int NR, int B, int PP, bool SO>
-__global__ void __launch_bounds__(256, tiled_minb<T, NR, PP>()) translate_tiled_kernel(TiledArgs<T> a)
+__global__ void __launch_bounds__(256, tiled_minb<T, L, NR, PP>()) translate_tiled_kernel(TiledArgs<T> a)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR;            // columns of a pair: ((dir*NR)+r)*2+p
@@ -490,7 +496,7 @@ template <typename T, int L, int NR, int B, int PP> static int launch_pp(const T
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = (int)((228 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
-    if (per_sm > tiled_minb<T, NR, PP>()) per_sm = tiled_minb<T, NR, PP>();
+    if (per_sm > tiled_minb<T, L, NR, PP>()) per_sm = tiled_minb<T, L, NR, PP>();
     if (a.ctas_per_sm >= 1 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
     int blocks = nsm * per_sm;
     if (blocks > a.ntiles * a.nchunk) blocks = a.ntiles * a.nchunk;
