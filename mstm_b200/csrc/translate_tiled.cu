@@ -41,8 +41,9 @@ __host__ __device__ constexpr int tofs(int n) { return (n - 1) * n / 2; }       
 
 // CTAs per SM the register budget is sized for: 3 for FP32 with one or two
 // columns (80 registers; the extra resident warps hide the pass's latencies:
-// fractal500 FP32, 2 columns, 2.27 -> 1.88 ms) and for FP64 up to order 5
-// (1500 spheres of order 5, FP64, 2 columns: 16.5 -> 14.7 ms), 2 otherwise
+// fractal500 FP32, 2 columns, 2.27 -> 1.88 ms) and for FP64 up to order 7
+// (FP64, 2 columns: 1500 spheres of order 5 16.5 -> 14.7 ms, 1000 of order 6
+// 8.32 -> 7.62 ms, 800 of order 7 6.01 -> 5.58 ms), 2 otherwise
 // (FP64 at larger orders and four FP32 columns slow down at the smaller
 // budget: fractal500 FP64, 2 columns, 2.9 -> 4.1 ms).  FP64 below order 5
 // runs the order-generic kernel, faster there than this one at either budget.
@@ -59,15 +60,15 @@ template <typename T> __host__ __device__ constexpr int tiled_cs(int L)
 
 template <typename T, int L, int NR, int PP> __host__ __device__ constexpr int tiled_minb()
 {
-    return ((sizeof(T) == 4 && NR <= 2 && PP == 1) || (sizeof(T) == 8 && L <= 5)) ? 3 : 2;
+    return ((sizeof(T) == 4 && NR <= 2 && PP == 1) || (sizeof(T) == 8 && L <= 7)) ? 3 : 2;
 }
 
 // One CTA works through whole tiles, PP pairs of a tile at a time (a step):
 // consecutive pairs whose output slots are disjoint share one step, so the
 // four phases and their barriers serve both (PP = 2), which fills the
 // threads of the rotation phases and halves the barriers per pair.
-template <typename T, int L, int NR, int B, int PP, bool SO>
-__global__ void __launch_bounds__(256, tiled_minb<T, L, NR, PP>()) translate_tiled_kernel(TiledArgs<T> a)
+template <typename T, int L, int NR, int B, int PP, bool SO, int MB>
+__global__ void __launch_bounds__(256, MB) translate_tiled_kernel(TiledArgs<T> a)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR;            // columns of a pair: ((dir*NR)+r)*2+p
@@ -488,15 +489,15 @@ template <typename T, int L, int NR, int B, int PP> static size_t tiled_smem()
     return off;
 }
 
-template <typename T, int L, int NR, int B, int PP> static int launch_pp(const TiledArgs<T>& a, int nsm, cudaStream_t st)
+template <typename T, int L, int NR, int B, int PP, int MB> static int launch_mb(const TiledArgs<T>& a, int nsm, cudaStream_t st)
 {
     size_t smem = tiled_smem<T, L, NR, B, PP>();
     if (smem > 227 * 1024) return -1;
-    auto kern = a.soff ? translate_tiled_kernel<T, L, NR, B, PP, true> : translate_tiled_kernel<T, L, NR, B, PP, false>;
+    auto kern = a.soff ? translate_tiled_kernel<T, L, NR, B, PP, true, MB> : translate_tiled_kernel<T, L, NR, B, PP, false, MB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = (int)((228 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
-    if (per_sm > tiled_minb<T, L, NR, PP>()) per_sm = tiled_minb<T, L, NR, PP>();
+    if (per_sm > MB) per_sm = MB;
     if (a.ctas_per_sm >= 1 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
     int blocks = nsm * per_sm;
     if (blocks > a.ntiles * a.nchunk) blocks = a.ntiles * a.nchunk;
@@ -504,6 +505,20 @@ template <typename T, int L, int NR, int B, int PP> static int launch_pp(const T
     kern<<<blocks, 256, smem, st>>>(a);
     launch_counter() += 1;
     return 0;
+}
+
+// FP64 passes of orders 5-7 whose work items do not fill one wave of three
+// CTAs per SM run the two-CTA instance: with few CTAs the 128-register budget
+// (no spills) is faster per CTA (20 spheres of order 7, FP64 solve: 3.59 ms
+// with the three-CTA instance, 3.05 ms with this one)
+template <typename T, int L, int NR, int B, int PP> static int launch_pp(const TiledArgs<T>& a, int nsm, cudaStream_t st)
+{
+    constexpr int MB = tiled_minb<T, L, NR, PP>();
+    if constexpr (sizeof(T) == 8 && MB == 3) {
+        if (a.ntiles * a.nchunk < 3 * nsm || (a.ctas_per_sm >= 1 && a.ctas_per_sm < 3))
+            return launch_mb<T, L, NR, B, PP, 2>(a, nsm, st);
+    }
+    return launch_mb<T, L, NR, B, PP, MB>(a, nsm, st);
 }
 
 // Two pairs a step only when asked for (FP32 passes of one or two columns):
