@@ -614,7 +614,7 @@ def report_line(args, ws, R, ne):
         "tuned": {"iterations": it, "outer": m["stats"]["outer"], "passes64": m["stats"]["passes64"],
                   "passes32": m["stats"]["passes32"], "qext": m["qtot"][0, 0], "qext_plain": p["qtot"][0, 0],
                   "qext_rel_diff": abs(m["qtot"][0, 0] / p["qtot"][0, 0] - 1)},
-        "roofline": {"kernel": "translate_rows_kernel<9, 2> (FP32 pair translation pass, row kernel)", "bound": "hbm",
+        "roofline": {"kernel": "translate_rows_kernel<9, 2, 0> (FP32 pair translation pass, row kernel)", "bound": "hbm",
                      "achieved": round(achieved, 1) if achieved else None, "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4) if achieved else None,
                      "traffic": round(TRAFFIC_PER_ALG_BYTE * (stored32 + vec_bytes)),
