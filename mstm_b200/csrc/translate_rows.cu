@@ -362,8 +362,8 @@ struct StepMeta {
 // barriers' latency; two otherwise (the larger orders' register tiles)
 template <int L> __host__ __device__ constexpr int rows_minb() { return L <= 5 ? 3 : 2; }
 
-template <int L, int NR, bool SO>
-__global__ void __launch_bounds__(256, rows_minb<L>()) translate_rows_kernel(TiledArgs<float> a, RowSched sc)
+template <int L, int NR, bool SO, int MB>
+__global__ void __launch_bounds__(256, MB) translate_rows_kernel(TiledArgs<float> a, RowSched sc)
 {
     constexpr int NT = 256;
     constexpr int C = 4 * NR, PP = rows_pp<L, NR>(), H = 32 / (PP * C);
@@ -686,23 +686,36 @@ static const RowSched& sched_for(int L, int H)
     return it->second;
 }
 
-template <int L, int NR> static int launch_LN(const TiledArgs<float>& a, int nsm, cudaStream_t st)
+template <int L, int NR, int MB> static int launch_mb(const TiledArgs<float>& a, int nsm, cudaStream_t st)
 {
     constexpr size_t smem = rows_smem<L, NR>();
     if (smem > 227 * 1024) return -1;
     constexpr int H = 32 / (rows_pp<L, NR>() * 4 * NR);
     const RowSched& sc = sched_for(L, H);
     if (!sc.fits) return -1;
-    auto kern = a.soff ? translate_rows_kernel<L, NR, true> : translate_rows_kernel<L, NR, false>;
+    auto kern = a.soff ? translate_rows_kernel<L, NR, true, MB> : translate_rows_kernel<L, NR, false, MB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = (int)((228 * 1024) / (smem + 1024));
-    per_sm = std::max(1, std::min(rows_minb<L>(), per_sm));
+    per_sm = std::max(1, std::min(MB, per_sm));
     if (a.ctas_per_sm >= 1 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
     int blocks = std::min(nsm * per_sm, a.ntiles * a.nchunk);
     if (blocks < 1) return 0;
     kern<<<blocks, 256, smem, st>>>(a, sc);
     launch_counter() += 1;
     return 0;
+}
+
+// a pass whose work items do not fill one wave of three CTAs per SM runs the
+// two-CTA instance, faster per CTA without the small orders' spills (30
+// spheres of order 5, 2 columns: 33.3 us with the three-CTA instance, 29.2 us
+// with this one)
+template <int L, int NR> static int launch_LN(const TiledArgs<float>& a, int nsm, cudaStream_t st)
+{
+    constexpr int MB = rows_minb<L>();
+    if constexpr (MB == 3) {
+        if (a.ntiles * a.nchunk < 3 * nsm || (a.ctas_per_sm >= 1 && a.ctas_per_sm < 3)) return launch_mb<L, NR, 2>(a, nsm, st);
+    }
+    return launch_mb<L, NR, MB>(a, nsm, st);
 }
 
 template <int L> static int launch_L(const TiledArgs<float>& a, int nsm, cudaStream_t st)
